@@ -1,0 +1,156 @@
+/* C ABI of liboem_b200.so, the sm_100a FDTD step engine that replaces OpenEM's solver step loop.
+ *
+ * OpenEM drives its CUDA side through one Python module, openem/device.py (the Kernels
+ * registry, openem/device.py:145-171, "the one entry point to the CUDA side", :3-10), with the
+ * device tables built by openem/device_tables.py and the step loop in openem/solver.py. This
+ * library is the replacement for that boundary: a *plan* owns every device buffer of one
+ * simulation; the host computes every coefficient in float64 and hands plain host arrays to
+ * the plan, which copies them to the device; stepping and readout are single calls.
+ *
+ * Conventions
+ *   - Every function returns an int status: OEM_OK (0) or a negative OEM_ERR_* code. The text of
+ *     the last error of the calling thread is returned by oem_last_error().
+ *   - Host pointers are borrowed for the duration of the call only.
+ *   - Field arrays are C-order (nx, ny, nz) on the host; on the device z is padded to a multiple
+ *     of 32 floats.
+ *   - A plan is used by one host thread at a time; different plans may run concurrently on
+ *     different streams. The stream argument is a cudaStream_t passed as void* (NULL = the
+ *     legacy default stream).
+ */
+#ifndef OEM_B200_H
+#define OEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OEM_OK 0
+#define OEM_ERR_INVALID (-1)     /* bad argument, shape or range (Python: ValueError) */
+#define OEM_ERR_UNSUPPORTED (-2) /* physics this engine does not run (NotImplementedError) */
+#define OEM_ERR_CUDA (-3)        /* CUDA runtime error (RuntimeError) */
+#define OEM_ERR_TIMEOUT (-4)     /* a bounded device wait gave up (RuntimeError) */
+#define OEM_ERR_STATE (-5)       /* call out of order, e.g. stepping before finalize */
+#define OEM_ERR_NOMEM (-6)       /* device allocation failed */
+
+typedef struct oem_plan oem_plan;
+
+/* Library version (major*10000 + minor*100 + patch) and last error text of this thread. */
+int oem_version(void);
+const char* oem_last_error(void);
+
+/* Create an empty plan for an (nx, ny, nz) grid on CUDA device `device`.
+ * ch = dt/mu0 and cw = eps0/dt are the H-update and dispersion-history scalars
+ * (openem/device_tables.py:174, :284). Replaces the allocation half of
+ * openem/device_tables.py:42-84 (_alloc_fields). */
+int oem_plan_create(int device, int nx, int ny, int nz, double ch, double cw, oem_plan** out);
+int oem_plan_destroy(oem_plan* p);
+
+/* One axis of the grid: 1/primal and 1/dual spacing, neighbour tables and masks
+ * (openem/grid.py:219-304) and the CPML recursion coefficients at E and H positions, each an
+ * (a | b | 1/kappa) triple of n values filled with the identity (0, 1, 1) outside the layers
+ * (openem/coeffs.py:21-42). slab_lo / slab_hi are the numbers of cells at each end where psi
+ * is stored; outside them the coefficients must be the identity. Replaces
+ * openem/device_tables.py:118-165 (_axis_device_tables) and the psi allocation of
+ * openem/coeffs.py:56-95. */
+int oem_plan_set_axis(oem_plan* p, int axis, const double* idl_p, const double* idl_d,
+                      const int32_t* nxt, const int32_t* prv, const double* mnx,
+                      const double* mpv, const double* pml_e, const double* pml_h,
+                      int slab_lo, int slab_hi);
+
+/* Material tuples and the per-cell material index.
+ * table: n_mat records of 16 32-bit words:
+ *   float ca[3], float cb[3], float eps[3], int32 pole_set[3] (-1 = not dispersive),
+ *   int32 pole_count[3], int32 reserved.
+ * index: nx*ny*nz unpadded C-order cell indices into the table, 2 bytes each when
+ * index_bytes == 2, 4 bytes when 4. Replaces the dense ca/cb arrays and the uint16 (ca, cb)
+ * lookup table of openem/coeffs.py:98-208 and openem/device_tables.py:168-219. */
+int oem_plan_set_materials(oem_plan* p, int n_mat, const uint32_t* table, int index_bytes,
+                           const void* index);
+
+/* Pole sets of the ADE (openem/kernels/dispersion.cu:25-114): set s owns poles
+ * set_ofs[s] .. set_ofs[s+1]-1; coef holds 4 floats per pole, (Re(A-1), Im(A-1), Re(B), Im(B)).
+ * seg_ofs: one uint32 per 32-cell z segment of the padded grid, the number of poles stored
+ * before that segment (cell order, then component, then pole). n_pole_total sizes P.
+ * Replaces openem/device_tables.py:235-285 (_dispersion_tables). */
+int oem_plan_set_pole_sets(oem_plan* p, int n_sets, const int32_t* set_ofs, const float* coef,
+                           const uint32_t* seg_ofs, int64_t n_seg, int64_t n_pole_total);
+
+/* One-face TF/SF plane-wave group (openem/kernels/source_dft.cu:39-73,
+ * openem/sources_setup.py:93-119): H correction on plane kh (Hy for pol 0, Hx for pol 1),
+ * E correction on plane ks; tables hold n_tab >= n_total float64 samples. */
+int oem_plan_add_plane_source(oem_plan* p, int pol, int kh, int ks, double coef_h,
+                              double coef_e, int64_t n_tab, const double* ex_tab,
+                              const double* hy_tab);
+
+/* Point dipoles (openem/kernels/source_dft.cu:135-206, openem/sources_setup.py:419-457).
+ * n_pts stencil points: cell (i, j, k) as three int32, component, coef = weight/dV, source
+ * index. amp: (n_src, nsteps1) float64, half-step samples for electric dipoles, whole-step for
+ * magnetic. Points that hit the same (component, cell) are summed in a fixed order. */
+int oem_plan_add_dipoles(oem_plan* p, int magnetic, int n_pts, const int32_t* ijk,
+                         const int32_t* comp, const float* coef, const int32_t* src, int n_src,
+                         int64_t nsteps1, const double* amp);
+
+/* DFT monitors (openem/kernels/source_dft.cu:208-779, openem/monitors_setup.py:74-255).
+ * phase: (n_total, nf, 4) float32 rows (cos, sin at E time (n+1)dt, cos, sin at H time
+ * (n+1/2)dt), apodisation window already multiplied in. Accumulators are float64.
+ * A flux monitor records (E_t1, E_t2, H_t1, H_t2) on the plane km of normal `axis`
+ * (transverse axes ascending) with H colocated as (H[km] + H[km-1]) / 2; a box monitor
+ * records the six components at their Yee positions. batch: snapshot ring depth T (steps
+ * per fp32 partial sum), 1..32. The id of the new monitor is written to *id. */
+int oem_plan_add_flux_monitor(oem_plan* p, int axis, int km, int nf, int64_t n_total,
+                              const float* phase, int batch, int* id);
+int oem_plan_add_box_monitor(oem_plan* p, int i0, int j0, int k0, int ni, int nj, int nk,
+                             int nf, int64_t n_total, const float* phase, int batch, int* id);
+
+/* Field time monitor (openem/kernels/source_dft.cu:273-319): components comps[0..nc-1]
+ * (0..5 = Ex..Hz) in a box, sampled at m = beg, beg+iv, ... < end into nslots slots, H averaged
+ * over the two neighbouring half steps. */
+int oem_plan_add_time_monitor(oem_plan* p, int nc, const int32_t* comps, int i0, int j0, int k0,
+                              int ni, int nj, int nk, int beg, int end, int iv, int nslots,
+                              int* id);
+
+/* Allocate the fields and auxiliary state, upload everything, capture the step graph.
+ * n_total is the nominal number of steps (bounds the source and phase tables). */
+int oem_plan_finalize(oem_plan* p, int64_t n_total);
+
+/* Advance nsteps full time steps on `stream` (asynchronous). One step is
+ * openem/solver.py:1145-1162 (_step_body): H update + H sources, E update with the ADE and
+ * conductivity + E sources, time sampling, DFT. */
+int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream);
+
+/* Fold the partly filled snapshot batch of every DFT monitor into its accumulator
+ * (openem/readout.py:137-157). Idempotent until the next step. */
+int oem_plan_flush(oem_plan* p, void* stream);
+
+/* Steps taken so far (host-side count). */
+int oem_plan_steps(oem_plan* p, int64_t* steps);
+
+/* Readout, synchronous on `stream`: DFT accumulators (ncomp, nf, points) float64 real and
+ * imaginary parts; time samples (nc, nslots, ni, nj, nk) float32; one field component
+ * (0..5) as an unpadded (nx, ny, nz) float32 array. */
+int oem_plan_read_monitor(oem_plan* p, int id, double* re, double* im, void* stream);
+int oem_plan_read_time_monitor(oem_plan* p, int id, float* out, void* stream);
+int oem_plan_read_field(oem_plan* p, int comp, float* out, void* stream);
+int oem_plan_write_field(oem_plan* p, int comp, const float* in, void* stream);
+
+/* Volume-weighted float64 sums for the early-termination criteria
+ * (openem/solver.py:107-121, :160-203): out[0] = sum V |E|^2, out[1] = sum V eps |E|^2,
+ * out[2] = sum V |H|^2, with each component's own Yee dual volume. Synchronous. */
+int oem_plan_energy(oem_plan* p, double out[3], void* stream);
+
+/* Device pointers of the six field arrays (padded layout) and the padded z pitch, for
+ * zero-copy interop with array libraries. */
+int oem_plan_field_ptrs(oem_plan* p, void* ptrs[6], int* nzp);
+
+/* Per-launch timing of the hot kernels accumulated by oem_plan_run when enabled (CUDA events
+ * on the run stream): kernel names, launch counts and total milliseconds. */
+int oem_plan_enable_timing(oem_plan* p, int on);
+int oem_plan_timing(oem_plan* p, int max, char* names /* max*32 */, int64_t* counts,
+                    double* ms, int* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OEM_B200_H */

@@ -1,0 +1,794 @@
+// C ABI of the engine (include/oem_b200.h): plan lifecycle, table upload, CUDA-graph stepping,
+// readout. The host side of OpenEM's step loop (openem/solver.py:403-511, _time_loop
+// :1165-1213) is split here into "build once" (oem_plan_finalize) and "step many"
+// (oem_plan_run); the float64 coefficient math stays in the Python host.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "oem_internal.cuh"
+
+namespace oem {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_error(cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  cudaGetLastError();  // clear a sticky launch error so the next call sees its own status
+  return set_error(OEM_ERR_CUDA, m);
+}
+
+static int check_plan(oem_plan* p, bool want_final) {
+  if (!p) return set_error(OEM_ERR_INVALID, "null plan");
+  if (want_final && !p->finalized) return set_error(OEM_ERR_STATE, "plan is not finalized");
+  if (!want_final && p->finalized)
+    return set_error(OEM_ERR_STATE, "plan is already finalized; tables can no longer change");
+  return OEM_OK;
+}
+
+static int use_device(oem_plan* p) {
+  OEM_CUDA(cudaSetDevice(p->device));
+  return OEM_OK;
+}
+
+static int64_t padded_index(const oem_plan* p, int i, int j, int k) {
+  return ((int64_t)i * p->ny + j) * p->nzp + k;
+}
+
+// Upload one axis (z tables padded to nzp with values that keep padding threads in range).
+static int upload_axis(oem_plan* p, int a) {
+  const AxisHost& h = p->axh[a];
+  const int n = (a == 0) ? p->nx : (a == 1) ? p->ny : p->nz;
+  const int np = (a == 2) ? p->nzp : n;
+  auto pad_f = [&](const std::vector<double>& v, size_t off, double fill) {
+    std::vector<float> o(np, (float)fill);
+    for (int q = 0; q < n; ++q) o[q] = (float)v[off + q];
+    return o;
+  };
+  auto pad_i = [&](const std::vector<int>& v, int fill) {
+    std::vector<int> o(np, fill);
+    for (int q = 0; q < n; ++q) o[q] = v[q];
+    return o;
+  };
+  DevAxis& D = p->yp.ax[a];
+  float* d;
+  int* di;
+  int rc;
+#define UPF(field, vec, off, fill)                                        \
+  {                                                                       \
+    std::vector<float> t_ = pad_f(vec, off, fill);                        \
+    if ((rc = dupload(p, &d, t_.data(), t_.size()))) return rc;           \
+    D.field = d;                                                          \
+  }
+  UPF(idl_p, h.idl_p, 0, 1.0);
+  UPF(idl_d, h.idl_d, 0, 1.0);
+  UPF(mnx, h.mnx, 0, 0.0);
+  UPF(mpv, h.mpv, 0, 0.0);
+  UPF(ae, h.pml_e, 0, 0.0);
+  UPF(be, h.pml_e, n, 1.0);
+  UPF(ke, h.pml_e, 2 * (size_t)n, 1.0);
+  UPF(ah, h.pml_h, 0, 0.0);
+  UPF(bh, h.pml_h, n, 1.0);
+  UPF(kh, h.pml_h, 2 * (size_t)n, 1.0);
+#undef UPF
+  {
+    std::vector<int> t = pad_i(h.nxt, n - 1);
+    if ((rc = dupload(p, &di, t.data(), t.size()))) return rc;
+    D.nxt = di;
+  }
+  {
+    std::vector<int> t = pad_i(h.prv, n - 1);
+    if ((rc = dupload(p, &di, t.data(), t.size()))) return rc;
+    D.prv = di;
+  }
+  D.n = n;
+  D.lo = h.lo;
+  D.hi = h.hi;
+  // float64 primal / dual spacings for the energy sums
+  std::vector<double> dlp(n), dld(n);
+  for (int q = 0; q < n; ++q) {
+    dlp[q] = 1.0 / h.idl_p[q];
+    dld[q] = 1.0 / h.idl_d[q];
+  }
+  if ((rc = dupload(p, &p->d_dl[a][0], dlp.data(), (size_t)n))) return rc;
+  if ((rc = dupload(p, &p->d_dl[a][1], dld.data(), (size_t)n))) return rc;
+  return OEM_OK;
+}
+
+static int alloc_psi(oem_plan* p) {
+  int rc;
+  for (int a = 0; a < 3; ++a) {
+    const AxisHost& h = p->axh[a];
+    for (int side = 0; side < 2; ++side) {
+      const int L = side == 0 ? h.lo : h.hi;
+      size_t cnt = 0;
+      if (L > 0) {
+        if (a == 0) cnt = (size_t)L * p->ny * p->nzp;
+        else if (a == 1) cnt = (size_t)p->nx * L * p->nzp;
+        else cnt = (size_t)p->nx * p->ny * L;
+      }
+      for (int slot = 0; slot < 2; ++slot) {
+        float* ph = nullptr;
+        float* pe = nullptr;
+        if (cnt) {
+          if ((rc = dalloc(p, &ph, cnt))) return rc;
+          if ((rc = dalloc(p, &pe, cnt))) return rc;
+        }
+        p->yp.psih.p[a][slot][side] = ph;
+        p->yp.psie.p[a][slot][side] = pe;
+      }
+    }
+  }
+  return OEM_OK;
+}
+
+// One time step (openem/solver.py:1145-1162).
+static int enqueue_step(oem_plan* p, cudaStream_t s) {
+  const YeeParams& P = p->yp;
+  cudaError_t e;
+  if ((e = launch_update_h(P, s)) != cudaSuccess) return cuda_error(e, "update_h");
+  for (const DipoleSet& d : p->dipoles)
+    if (d.magnetic && (e = launch_dipoles(P, d, p->d_step, s)) != cudaSuccess)
+      return cuda_error(e, "dipoles_h");
+  for (const PlaneSrc& src : p->planes)
+    if ((e = launch_plane_h(P, src, p->d_step, s)) != cudaSuccess)
+      return cuda_error(e, "plane_h");
+  if ((e = launch_update_e(P, s)) != cudaSuccess) return cuda_error(e, "update_e");
+  for (const PlaneSrc& src : p->planes)
+    if ((e = launch_plane_e(P, src, p->d_step, s)) != cudaSuccess)
+      return cuda_error(e, "plane_e");
+  for (const DipoleSet& d : p->dipoles)
+    if (!d.magnetic && (e = launch_dipoles(P, d, p->d_step, s)) != cudaSuccess)
+      return cuda_error(e, "dipoles_e");
+  for (const TimeMon& m : p->tmons) {
+    if ((e = launch_time_sample(P, m, p->d_step, 1, s)) != cudaSuccess)
+      return cuda_error(e, "time_sample");
+    if ((e = launch_time_sample(P, m, p->d_step, 0, s)) != cudaSuccess)
+      return cuda_error(e, "time_sample");
+  }
+  for (const Monitor& m : p->mons) {
+    if ((e = launch_snapshot(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "snapshot");
+    if ((e = launch_flush(m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "flush");
+  }
+  if ((e = launch_step_advance(p->d_step, s)) != cudaSuccess) return cuda_error(e, "step");
+  return OEM_OK;
+}
+
+static int capture(oem_plan* p, int nsteps, cudaGraphExec_t* out) {
+  cudaGraph_t g = nullptr;
+  OEM_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
+  int rc = OEM_OK;
+  for (int q = 0; q < nsteps && rc == OEM_OK; ++q) rc = enqueue_step(p, p->cap_stream);
+  cudaError_t e = cudaStreamEndCapture(p->cap_stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_error(e, "cudaGraphInstantiate");
+  return OEM_OK;
+}
+
+}  // namespace oem
+
+using namespace oem;
+
+extern "C" {
+
+int oem_version(void) { return 100; }
+
+const char* oem_last_error(void) { return g_last_error.c_str(); }
+
+int oem_plan_create(int device, int nx, int ny, int nz, double ch, double cw, oem_plan** out) {
+  if (!out) return set_error(OEM_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  if (nx < 1 || ny < 1 || nz < 1)
+    return set_error(OEM_ERR_INVALID, "grid dimensions must be positive");
+  const int64_t nzp = ((int64_t)nz + 31) / 32 * 32;
+  if ((int64_t)nx * ny * nzp > ((int64_t)1 << 40))
+    return set_error(OEM_ERR_INVALID, "grid too large");
+  if ((int64_t)nx * ny * nzp / 32 > 0xffffffffLL)
+    return set_error(OEM_ERR_INVALID, "grid too large for 32-bit segment offsets");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess) return cuda_error(e, "cudaGetDeviceCount");
+  if (device < 0 || device >= ndev)
+    return set_error(OEM_ERR_INVALID, "device " + std::to_string(device) + " out of range");
+  oem_plan* p = new oem_plan();
+  p->device = device;
+  p->nx = nx;
+  p->ny = ny;
+  p->nz = nz;
+  p->nzp = (int)nzp;
+  p->ch = ch;
+  p->cw = cw;
+  *out = p;
+  return OEM_OK;
+}
+
+int oem_plan_destroy(oem_plan* p) {
+  if (!p) return OEM_OK;
+  cudaSetDevice(p->device);
+  if (p->graph_many) cudaGraphExecDestroy(p->graph_many);
+  if (p->graph_one) cudaGraphExecDestroy(p->graph_one);
+  if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
+  for (void* a : p->allocs) cudaFree(a);
+  delete p;
+  return OEM_OK;
+}
+
+int oem_plan_set_axis(oem_plan* p, int axis, const double* idl_p, const double* idl_d,
+                      const int32_t* nxt, const int32_t* prv, const double* mnx,
+                      const double* mpv, const double* pml_e, const double* pml_h, int slab_lo,
+                      int slab_hi) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (axis < 0 || axis > 2) return set_error(OEM_ERR_INVALID, "axis must be 0, 1 or 2");
+  if (!idl_p || !idl_d || !nxt || !prv || !mnx || !mpv || !pml_e || !pml_h)
+    return set_error(OEM_ERR_INVALID, "null axis table");
+  const int n = axis == 0 ? p->nx : axis == 1 ? p->ny : p->nz;
+  if (slab_lo < 0 || slab_hi < 0 || slab_lo + slab_hi > n)
+    return set_error(OEM_ERR_INVALID, "psi slabs overlap or exceed the axis");
+  AxisHost& h = p->axh[axis];
+  h.idl_p.assign(idl_p, idl_p + n);
+  h.idl_d.assign(idl_d, idl_d + n);
+  h.nxt.assign(nxt, nxt + n);
+  h.prv.assign(prv, prv + n);
+  h.mnx.assign(mnx, mnx + n);
+  h.mpv.assign(mpv, mpv + n);
+  h.pml_e.assign(pml_e, pml_e + 3 * (size_t)n);
+  h.pml_h.assign(pml_h, pml_h + 3 * (size_t)n);
+  for (int q = 0; q < n; ++q) {
+    if (h.nxt[q] < 0 || h.nxt[q] >= n || h.prv[q] < 0 || h.prv[q] >= n)
+      return set_error(OEM_ERR_INVALID, "neighbour index out of range on axis " +
+                                            std::to_string(axis));
+    if (!(h.idl_p[q] > 0.0) || !(h.idl_d[q] > 0.0))
+      return set_error(OEM_ERR_INVALID, "spacings must be positive");
+    const bool in_slab = q < slab_lo || q >= n - slab_hi;
+    if (!in_slab) {
+      for (const std::vector<double>* v : {&h.pml_e, &h.pml_h}) {
+        if ((*v)[q] != 0.0 || (*v)[n + q] != 1.0 || (*v)[2 * (size_t)n + q] != 1.0)
+          return set_error(OEM_ERR_INVALID,
+                           "CPML coefficients are not the identity outside the psi slabs on "
+                           "axis " + std::to_string(axis) + " at index " + std::to_string(q));
+      }
+    }
+  }
+  h.lo = slab_lo;
+  h.hi = slab_hi;
+  h.set = true;
+  return OEM_OK;
+}
+
+int oem_plan_set_materials(oem_plan* p, int n_mat, const uint32_t* table, int index_bytes,
+                           const void* index) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (n_mat < 1 || !table || !index) return set_error(OEM_ERR_INVALID, "empty material table");
+  if (index_bytes != 2 && index_bytes != 4)
+    return set_error(OEM_ERR_INVALID, "index_bytes must be 2 or 4");
+  if (index_bytes == 2 && n_mat > 65535)
+    return set_error(OEM_ERR_INVALID, "more than 65535 materials need a 4-byte index");
+  p->mats.resize((size_t)n_mat + 1);
+  MatRec& v = p->mats[0];  // material 0: padding cells (E held at zero)
+  for (int c = 0; c < 3; ++c) {
+    v.ca[c] = 0.f; v.cb[c] = 0.f; v.eps[c] = 1.f; v.pset[c] = -1; v.np[c] = 0;
+  }
+  v.reserved = 0;
+  memcpy(&p->mats[1], table, sizeof(MatRec) * (size_t)n_mat);
+  for (int m = 1; m <= n_mat; ++m)
+    for (int c = 0; c < 3; ++c) {
+      const MatRec& r = p->mats[m];
+      if (r.pset[c] < 0 && r.np[c] != 0)
+        return set_error(OEM_ERR_INVALID, "non-dispersive material with a pole count");
+      if (r.np[c] < 0 || r.np[c] > 15)
+        return set_error(OEM_ERR_INVALID, "pole count per component must be 0..15");
+    }
+  const size_t ncell = (size_t)p->nx * p->ny * p->nz;
+  p->index_bytes = index_bytes;
+  p->mat_index.resize(ncell * index_bytes);
+  memcpy(p->mat_index.data(), index, ncell * index_bytes);
+  // range check
+  if (index_bytes == 2) {
+    const uint16_t* q = reinterpret_cast<const uint16_t*>(p->mat_index.data());
+    for (size_t t = 0; t < ncell; ++t)
+      if (q[t] >= n_mat) return set_error(OEM_ERR_INVALID, "material index out of range");
+  } else {
+    const uint32_t* q = reinterpret_cast<const uint32_t*>(p->mat_index.data());
+    for (size_t t = 0; t < ncell; ++t)
+      if (q[t] >= (uint32_t)n_mat) return set_error(OEM_ERR_INVALID, "material index out of range");
+  }
+  return OEM_OK;
+}
+
+int oem_plan_set_pole_sets(oem_plan* p, int n_sets, const int32_t* set_ofs, const float* coef,
+                           const uint32_t* seg_ofs, int64_t n_seg, int64_t n_pole_total) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (n_sets < 1 || !set_ofs || !coef || !seg_ofs)
+    return set_error(OEM_ERR_INVALID, "empty pole-set table");
+  const int64_t want_seg = (int64_t)p->nx * p->ny * p->nzp / 32;
+  if (n_seg != want_seg)
+    return set_error(OEM_ERR_INVALID, "seg_ofs must hold one entry per 32-cell segment (" +
+                                          std::to_string(want_seg) + ")");
+  if (n_pole_total < 0 || n_pole_total > 0xffffffffLL)
+    return set_error(OEM_ERR_INVALID, "pole count out of range");
+  p->pset_ofs.assign(set_ofs, set_ofs + n_sets + 1);
+  if (p->pset_ofs[0] != 0) return set_error(OEM_ERR_INVALID, "set_ofs[0] must be 0");
+  for (int s = 0; s < n_sets; ++s)
+    if (p->pset_ofs[s + 1] < p->pset_ofs[s]) return set_error(OEM_ERR_INVALID, "set_ofs not monotone");
+  p->pcoef.assign(coef, coef + 4 * (size_t)p->pset_ofs[n_sets]);
+  p->seg_ofs.assign(seg_ofs, seg_ofs + n_seg);
+  p->n_pole_total = n_pole_total;
+  return OEM_OK;
+}
+
+int oem_plan_add_plane_source(oem_plan* p, int pol, int kh, int ks, double coef_h, double coef_e,
+                              int64_t n_tab, const double* ex_tab, const double* hy_tab) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (pol != 0 && pol != 1) return set_error(OEM_ERR_UNSUPPORTED, "plane wave polarisation must be Ex or Ey");
+  if (kh < 0 || kh >= p->nz || ks < 0 || ks >= p->nz)
+    return set_error(OEM_ERR_INVALID, "plane-wave injection planes out of range");
+  if (n_tab < 1 || !ex_tab || !hy_tab) return set_error(OEM_ERR_INVALID, "empty incident table");
+  if ((rc = use_device(p))) return rc;
+  PlaneSrc s;
+  s.pol = pol;
+  s.kh = kh;
+  s.ks = ks;
+  s.coef_h = (float)coef_h;
+  s.coef_e = (float)coef_e;
+  s.ntab = n_tab;
+  if ((rc = dupload(p, &s.d_ex, ex_tab, (size_t)n_tab))) return rc;
+  if ((rc = dupload(p, &s.d_hy, hy_tab, (size_t)n_tab))) return rc;
+  p->planes.push_back(s);
+  return OEM_OK;
+}
+
+int oem_plan_add_dipoles(oem_plan* p, int magnetic, int n_pts, const int32_t* ijk,
+                         const int32_t* comp, const float* coef, const int32_t* src, int n_src,
+                         int64_t nsteps1, const double* amp) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (n_pts < 1 || n_src < 1 || nsteps1 < 1 || !ijk || !comp || !coef || !src || !amp)
+    return set_error(OEM_ERR_INVALID, "empty dipole table");
+  if ((rc = use_device(p))) return rc;
+  // Group points by (component, cell), keeping their input order inside a group.
+  std::map<std::pair<int64_t, int>, std::vector<int>> groups;
+  std::vector<std::pair<int64_t, int>> order;
+  for (int q = 0; q < n_pts; ++q) {
+    const int i = ijk[3 * q], j = ijk[3 * q + 1], k = ijk[3 * q + 2];
+    if (i < 0 || i >= p->nx || j < 0 || j >= p->ny || k < 0 || k >= p->nz)
+      return set_error(OEM_ERR_INVALID, "dipole stencil point outside the grid");
+    if (comp[q] < 0 || comp[q] > 2) return set_error(OEM_ERR_INVALID, "dipole component out of range");
+    if (src[q] < 0 || src[q] >= n_src) return set_error(OEM_ERR_INVALID, "dipole source index out of range");
+    auto key = std::make_pair(padded_index(p, i, j, k), (int)comp[q]);
+    auto it = groups.find(key);
+    if (it == groups.end()) {
+      order.push_back(key);
+      groups[key] = {q};
+    } else {
+      it->second.push_back(q);
+    }
+  }
+  std::vector<int64_t> tgt;
+  std::vector<int> tcomp, ofs(1, 0), psrc;
+  std::vector<float> pcoef;
+  for (const auto& key : order) {
+    tgt.push_back(key.first);
+    tcomp.push_back(key.second);
+    for (int q : groups[key]) {
+      pcoef.push_back(coef[q]);
+      psrc.push_back(src[q]);
+    }
+    ofs.push_back((int)pcoef.size());
+  }
+  DipoleSet d;
+  d.magnetic = magnetic ? 1 : 0;
+  d.n_targets = (int)tgt.size();
+  d.nsteps1 = nsteps1;
+  d.n_src = n_src;
+  if ((rc = dupload(p, &d.d_target, tgt.data(), tgt.size()))) return rc;
+  if ((rc = dupload(p, &d.d_tcomp, tcomp.data(), tcomp.size()))) return rc;
+  if ((rc = dupload(p, &d.d_ofs, ofs.data(), ofs.size()))) return rc;
+  if ((rc = dupload(p, &d.d_coef, pcoef.data(), pcoef.size()))) return rc;
+  if ((rc = dupload(p, &d.d_src, psrc.data(), psrc.size()))) return rc;
+  if ((rc = dupload(p, &d.d_amp, amp, (size_t)n_src * nsteps1))) return rc;
+  p->dipoles.push_back(d);
+  return OEM_OK;
+}
+
+static int add_monitor_common(oem_plan* p, Monitor& m, int nf, int64_t n_total, const float* phase,
+                              int batch, int* id) {
+  int rc;
+  if (nf < 1 || n_total < 1 || !phase || !id) return set_error(OEM_ERR_INVALID, "empty monitor");
+  if (batch < 1 || batch > 32) return set_error(OEM_ERR_INVALID, "batch must be 1..32");
+  if ((rc = use_device(p))) return rc;
+  m.nf = nf;
+  m.T = batch;
+  m.n_total = n_total;
+  if ((rc = dupload(p, &m.d_phase, phase, (size_t)n_total * nf * 4))) return rc;
+  if ((rc = dalloc(p, &m.d_snap, (size_t)m.T * m.ncomp * m.cells))) return rc;
+  if ((rc = dalloc(p, &m.d_re, (size_t)m.ncomp * nf * m.cells))) return rc;
+  if ((rc = dalloc(p, &m.d_im, (size_t)m.ncomp * nf * m.cells))) return rc;
+  int minus1 = -1;
+  if ((rc = dupload(p, &m.d_done, &minus1, 1))) return rc;
+  *id = (int)p->mons.size();
+  p->mons.push_back(m);
+  return OEM_OK;
+}
+
+int oem_plan_add_flux_monitor(oem_plan* p, int axis, int km, int nf, int64_t n_total,
+                              const float* phase, int batch, int* id) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (axis < 0 || axis > 2) return set_error(OEM_ERR_INVALID, "monitor axis must be 0..2");
+  const int dims[3] = {p->nx, p->ny, p->nz};
+  if (km < 1 || km >= dims[axis])
+    return set_error(OEM_ERR_INVALID, "flux plane index must be in [1, n) of its normal axis");
+  Monitor m;
+  m.kind = 0;
+  m.axis = axis;
+  m.km = km;
+  const int t1 = axis == 0 ? 1 : 0, t2 = axis == 2 ? 1 : 2;
+  m.n1 = dims[t1];
+  m.n2 = dims[t2];
+  m.ncomp = 4;
+  m.cells = (int64_t)m.n1 * m.n2;
+  return add_monitor_common(p, m, nf, n_total, phase, batch, id);
+}
+
+int oem_plan_add_box_monitor(oem_plan* p, int i0, int j0, int k0, int ni, int nj, int nk, int nf,
+                             int64_t n_total, const float* phase, int batch, int* id) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (ni < 1 || nj < 1 || nk < 1 || i0 < 0 || j0 < 0 || k0 < 0 || i0 + ni > p->nx ||
+      j0 + nj > p->ny || k0 + nk > p->nz)
+    return set_error(OEM_ERR_INVALID, "field monitor box outside the grid");
+  Monitor m;
+  m.kind = 1;
+  m.i0 = i0; m.j0 = j0; m.k0 = k0;
+  m.ni = ni; m.nj = nj; m.nk = nk;
+  m.ncomp = 6;
+  m.cells = (int64_t)ni * nj * nk;
+  return add_monitor_common(p, m, nf, n_total, phase, batch, id);
+}
+
+int oem_plan_add_time_monitor(oem_plan* p, int nc, const int32_t* comps, int i0, int j0, int k0,
+                              int ni, int nj, int nk, int beg, int end, int iv, int nslots,
+                              int* id) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (nc < 1 || nc > 6 || !comps || !id) return set_error(OEM_ERR_INVALID, "bad component list");
+  if (ni < 1 || nj < 1 || nk < 1 || i0 < 0 || j0 < 0 || k0 < 0 || i0 + ni > p->nx ||
+      j0 + nj > p->ny || k0 + nk > p->nz)
+    return set_error(OEM_ERR_INVALID, "time monitor box outside the grid");
+  if (iv < 1 || nslots < 0) return set_error(OEM_ERR_INVALID, "bad sampling interval");
+  if ((rc = use_device(p))) return rc;
+  TimeMon m;
+  m.nc = nc;
+  for (int q = 0; q < nc; ++q) {
+    if (comps[q] < 0 || comps[q] > 5) return set_error(OEM_ERR_INVALID, "component out of range");
+    m.comps[q] = comps[q];
+  }
+  m.i0 = i0; m.j0 = j0; m.k0 = k0; m.ni = ni; m.nj = nj; m.nk = nk;
+  m.beg = beg; m.end = end; m.iv = iv; m.nslots = nslots;
+  if ((rc = dalloc(p, &m.d_buf, (size_t)nc * std::max(nslots, 1) * ni * nj * nk))) return rc;
+  *id = (int)p->tmons.size();
+  p->tmons.push_back(m);
+  return OEM_OK;
+}
+
+int oem_plan_finalize(oem_plan* p, int64_t n_total) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  for (int a = 0; a < 3; ++a)
+    if (!p->axh[a].set) return set_error(OEM_ERR_STATE, "axis " + std::to_string(a) + " not set");
+  if (p->mats.empty()) return set_error(OEM_ERR_STATE, "materials not set");
+  if (n_total < 0) return set_error(OEM_ERR_INVALID, "negative step count");
+  for (const PlaneSrc& s : p->planes)
+    if (s.ntab < n_total) return set_error(OEM_ERR_INVALID, "plane-wave table shorter than the run");
+  for (const DipoleSet& d : p->dipoles)
+    if (d.nsteps1 < n_total) return set_error(OEM_ERR_INVALID, "dipole table shorter than the run");
+  for (const Monitor& m : p->mons)
+    if (m.n_total < n_total) return set_error(OEM_ERR_INVALID, "phase table shorter than the run");
+  if ((rc = use_device(p))) return rc;
+  p->n_total = n_total;
+  YeeParams& P = p->yp;
+  P.nx = p->nx; P.ny = p->ny; P.nz = p->nz; P.nzp = p->nzp;
+  P.ch = (float)p->ch;
+  P.cw = (float)p->cw;
+  const size_t ncp = (size_t)p->nx * p->ny * p->nzp;
+  for (int c = 0; c < 6; ++c)
+    if ((rc = dalloc(p, &P.f[c], ncp))) return rc;
+  for (int a = 0; a < 3; ++a)
+    if ((rc = upload_axis(p, a))) return rc;
+  if ((rc = alloc_psi(p))) return rc;
+  // materials: table with the padding material at 0, padded index shifted by one
+  MatRec* dm;
+  if ((rc = dupload(p, &dm, p->mats.data(), p->mats.size()))) return rc;
+  P.mats = dm;
+  const bool wide = p->index_bytes == 4 || p->mats.size() > 65535;
+  {
+    const size_t row = (size_t)p->nz;
+    if (!wide) {
+      std::vector<uint16_t> idx(ncp, 0);
+      const uint16_t* src = reinterpret_cast<const uint16_t*>(p->mat_index.data());
+      for (size_t r = 0; r < (size_t)p->nx * p->ny; ++r)
+        for (size_t k = 0; k < row; ++k) idx[r * p->nzp + k] = (uint16_t)(src[r * row + k] + 1);
+      uint16_t* d;
+      if ((rc = dupload(p, &d, idx.data(), ncp))) return rc;
+      P.mat16 = d;
+      P.mat32 = nullptr;
+    } else {
+      std::vector<uint32_t> idx(ncp, 0);
+      for (size_t r = 0; r < (size_t)p->nx * p->ny; ++r)
+        for (size_t k = 0; k < row; ++k) {
+          const size_t t = r * row + k;
+          uint32_t v;
+          if (p->index_bytes == 2) v = reinterpret_cast<const uint16_t*>(p->mat_index.data())[t];
+          else v = reinterpret_cast<const uint32_t*>(p->mat_index.data())[t];
+          idx[r * p->nzp + k] = v + 1;
+        }
+      uint32_t* d;
+      if ((rc = dupload(p, &d, idx.data(), ncp))) return rc;
+      P.mat32 = d;
+      P.mat16 = nullptr;
+    }
+    std::vector<uint8_t>().swap(p->mat_index);
+  }
+  // ADE
+  bool any_pole = false;
+  for (const MatRec& m : p->mats)
+    for (int c = 0; c < 3; ++c) any_pole |= m.np[c] > 0;
+  P.has_ade = 0;
+  if (any_pole) {
+    if (p->pset_ofs.empty()) return set_error(OEM_ERR_STATE, "dispersive materials without pole sets");
+    const int nsets = (int)p->pset_ofs.size() - 1;
+    for (const MatRec& m : p->mats)
+      for (int c = 0; c < 3; ++c)
+        if (m.np[c] > 0 && (m.pset[c] >= nsets ||
+                            p->pset_ofs[m.pset[c] + 1] - p->pset_ofs[m.pset[c]] != m.np[c]))
+          return set_error(OEM_ERR_INVALID, "material pole count disagrees with its pole set");
+    float4* dc;
+    int* dofs;
+    uint32_t* dseg;
+    float2* dP;
+    if ((rc = dupload(p, &dc, reinterpret_cast<const float4*>(p->pcoef.data()), p->pcoef.size() / 4))) return rc;
+    if ((rc = dupload(p, &dofs, p->pset_ofs.data(), p->pset_ofs.size()))) return rc;
+    if ((rc = dupload(p, &dseg, p->seg_ofs.data(), p->seg_ofs.size()))) return rc;
+    if ((rc = dalloc(p, &dP, (size_t)std::max<int64_t>(p->n_pole_total, 1)))) return rc;
+    P.pcoef = dc;
+    P.pset_ofs = dofs;
+    P.seg_ofs = dseg;
+    P.P = dP;
+    P.has_ade = 1;
+  }
+  if ((rc = dalloc(p, &p->d_step, 1))) return rc;
+  p->energy_blocks = energy_block_count(P);
+  if ((rc = dalloc(p, &p->d_energy_part, 3 * (size_t)p->energy_blocks))) return rc;
+  // capture: G steps per graph for small grids (launch overhead), 1 for large ones
+  OEM_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
+  const double cells = (double)ncp;
+  int G = (int)std::min(32.0, std::max(1.0, 4.0e6 / cells));
+  p->graph_steps = G;
+  if ((rc = capture(p, 1, &p->graph_one))) return rc;
+  if (G > 1 && (rc = capture(p, G, &p->graph_many))) return rc;
+  OEM_CUDA(cudaDeviceSynchronize());
+  p->finalized = true;
+  return OEM_OK;
+}
+
+int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (nsteps < 0) return set_error(OEM_ERR_INVALID, "negative step count");
+  if (p->steps + nsteps > p->n_total)
+    return set_error(OEM_ERR_INVALID, "asked to run past the nominal step count " +
+                                          std::to_string(p->n_total) + " (tables end there)");
+  if ((rc = use_device(p))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int64_t left = nsteps;
+  if (p->timing) {
+    // Direct launches with CUDA events around the two update kernels; events come from a pool
+    // sized for this call and are read once at the end, so the stream never waits on the host.
+    const int64_t n = nsteps;
+    std::vector<cudaEvent_t> ev((size_t)n * 5);
+    for (auto& evq : ev) OEM_CUDA(cudaEventCreate(&evq));
+    for (int64_t q = 0; q < n; ++q) {
+      cudaEvent_t* E = &ev[(size_t)q * 5];
+      OEM_CUDA(cudaEventRecord(E[0], s));
+      cudaError_t e = launch_update_h(p->yp, s);
+      if (e != cudaSuccess) return cuda_error(e, "update_h");
+      OEM_CUDA(cudaEventRecord(E[1], s));
+      for (const DipoleSet& d : p->dipoles)
+        if (d.magnetic && (e = launch_dipoles(p->yp, d, p->d_step, s)) != cudaSuccess)
+          return cuda_error(e, "dipoles_h");
+      for (const PlaneSrc& src : p->planes)
+        if ((e = launch_plane_h(p->yp, src, p->d_step, s)) != cudaSuccess) return cuda_error(e, "plane_h");
+      OEM_CUDA(cudaEventRecord(E[2], s));
+      if ((e = launch_update_e(p->yp, s)) != cudaSuccess) return cuda_error(e, "update_e");
+      OEM_CUDA(cudaEventRecord(E[3], s));
+      for (const PlaneSrc& src : p->planes)
+        if ((e = launch_plane_e(p->yp, src, p->d_step, s)) != cudaSuccess) return cuda_error(e, "plane_e");
+      for (const DipoleSet& d : p->dipoles)
+        if (!d.magnetic && (e = launch_dipoles(p->yp, d, p->d_step, s)) != cudaSuccess)
+          return cuda_error(e, "dipoles_e");
+      for (const TimeMon& m : p->tmons) {
+        if ((e = launch_time_sample(p->yp, m, p->d_step, 1, s)) != cudaSuccess) return cuda_error(e, "ts");
+        if ((e = launch_time_sample(p->yp, m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "ts");
+      }
+      for (const Monitor& m : p->mons) {
+        if ((e = launch_snapshot(p->yp, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "snap");
+        if ((e = launch_flush(m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "flush");
+      }
+      if ((e = launch_step_advance(p->d_step, s)) != cudaSuccess) return cuda_error(e, "step");
+      OEM_CUDA(cudaEventRecord(E[4], s));
+    }
+    if (n > 0) OEM_CUDA(cudaEventSynchronize(ev[(size_t)n * 5 - 1]));
+    auto add = [&](const char* nm, double ms) {
+      for (TimingRec& r : p->trecs)
+        if (r.name == nm) { r.count++; r.ms += ms; return; }
+      TimingRec r; r.name = nm; r.count = 1; r.ms = ms; p->trecs.push_back(r);
+    };
+    for (int64_t q = 0; q < n; ++q) {
+      cudaEvent_t* E = &ev[(size_t)q * 5];
+      float t_h = 0.f, t_e = 0.f, t_all = 0.f;
+      OEM_CUDA(cudaEventElapsedTime(&t_h, E[0], E[1]));
+      OEM_CUDA(cudaEventElapsedTime(&t_e, E[2], E[3]));
+      OEM_CUDA(cudaEventElapsedTime(&t_all, E[0], E[4]));
+      add("update_h", t_h);
+      add("update_e", t_e);
+      add("step", t_all);
+    }
+    for (auto& evq : ev) cudaEventDestroy(evq);
+    p->steps += n;
+    return OEM_OK;
+  }
+  while (left >= p->graph_steps && p->graph_steps > 1) {
+    OEM_CUDA(cudaGraphLaunch(p->graph_many, s));
+    left -= p->graph_steps;
+  }
+  while (left > 0) {
+    OEM_CUDA(cudaGraphLaunch(p->graph_one, s));
+    --left;
+  }
+  p->steps += nsteps;
+  return OEM_OK;
+}
+
+int oem_plan_flush(oem_plan* p, void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if ((rc = use_device(p))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  for (const Monitor& m : p->mons) {
+    cudaError_t e = launch_flush(m, p->d_step, 1, s);
+    if (e != cudaSuccess) return cuda_error(e, "flush");
+  }
+  return OEM_OK;
+}
+
+int oem_plan_steps(oem_plan* p, int64_t* steps) {
+  if (!p || !steps) return set_error(OEM_ERR_INVALID, "null argument");
+  *steps = p->steps;
+  return OEM_OK;
+}
+
+int oem_plan_read_monitor(oem_plan* p, int id, double* re, double* im, void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (id < 0 || id >= (int)p->mons.size()) return set_error(OEM_ERR_INVALID, "monitor id out of range");
+  if ((rc = use_device(p))) return rc;
+  const Monitor& m = p->mons[id];
+  const size_t n = (size_t)m.ncomp * m.nf * m.cells;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  OEM_CUDA(cudaMemcpyAsync(re, m.d_re, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  OEM_CUDA(cudaMemcpyAsync(im, m.d_im, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  OEM_CUDA(cudaStreamSynchronize(s));
+  return OEM_OK;
+}
+
+int oem_plan_read_time_monitor(oem_plan* p, int id, float* out, void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (id < 0 || id >= (int)p->tmons.size()) return set_error(OEM_ERR_INVALID, "time monitor id out of range");
+  if ((rc = use_device(p))) return rc;
+  const TimeMon& m = p->tmons[id];
+  const size_t n = (size_t)m.nc * m.nslots * m.ni * m.nj * m.nk;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (n) OEM_CUDA(cudaMemcpyAsync(out, m.d_buf, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+  OEM_CUDA(cudaStreamSynchronize(s));
+  return OEM_OK;
+}
+
+int oem_plan_read_field(oem_plan* p, int comp, float* out, void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (comp < 0 || comp > 5 || !out) return set_error(OEM_ERR_INVALID, "component must be 0..5");
+  if ((rc = use_device(p))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  OEM_CUDA(cudaMemcpy2DAsync(out, (size_t)p->nz * sizeof(float), p->yp.f[comp],
+                             (size_t)p->nzp * sizeof(float), (size_t)p->nz * sizeof(float),
+                             (size_t)p->nx * p->ny, cudaMemcpyDeviceToHost, s));
+  OEM_CUDA(cudaStreamSynchronize(s));
+  return OEM_OK;
+}
+
+int oem_plan_write_field(oem_plan* p, int comp, const float* in, void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (comp < 0 || comp > 5 || !in) return set_error(OEM_ERR_INVALID, "component must be 0..5");
+  if ((rc = use_device(p))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  OEM_CUDA(cudaMemcpy2DAsync(p->yp.f[comp], (size_t)p->nzp * sizeof(float), in,
+                             (size_t)p->nz * sizeof(float), (size_t)p->nz * sizeof(float),
+                             (size_t)p->nx * p->ny, cudaMemcpyHostToDevice, s));
+  OEM_CUDA(cudaStreamSynchronize(s));
+  return OEM_OK;
+}
+
+int oem_plan_energy(oem_plan* p, double out[3], void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (!out) return set_error(OEM_ERR_INVALID, "null output");
+  if ((rc = use_device(p))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = launch_energy(p->yp, p->d_dl, p->d_energy_part, p->energy_blocks, s);
+  if (e != cudaSuccess) return cuda_error(e, "energy");
+  std::vector<double> part(3 * (size_t)p->energy_blocks);
+  OEM_CUDA(cudaMemcpyAsync(part.data(), p->d_energy_part, part.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, s));
+  OEM_CUDA(cudaStreamSynchronize(s));
+  out[0] = out[1] = out[2] = 0.0;
+  for (int b = 0; b < p->energy_blocks; ++b)
+    for (int c = 0; c < 3; ++c) out[c] += part[3 * (size_t)b + c];
+  return OEM_OK;
+}
+
+int oem_plan_field_ptrs(oem_plan* p, void* ptrs[6], int* nzp) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  for (int c = 0; c < 6; ++c) ptrs[c] = p->yp.f[c];
+  if (nzp) *nzp = p->nzp;
+  return OEM_OK;
+}
+
+int oem_plan_enable_timing(oem_plan* p, int on) {
+  if (!p) return set_error(OEM_ERR_INVALID, "null plan");
+  p->timing = on != 0;
+  p->trecs.clear();
+  return OEM_OK;
+}
+
+int oem_plan_timing(oem_plan* p, int max, char* names, int64_t* counts, double* ms, int* n) {
+  if (!p || !n) return set_error(OEM_ERR_INVALID, "null argument");
+  int cnt = 0;
+  for (const TimingRec& r : p->trecs) {
+    if (cnt >= max) break;
+    if (names) {
+      strncpy(names + 32 * cnt, r.name.c_str(), 31);
+      names[32 * cnt + 31] = 0;
+    }
+    if (counts) counts[cnt] = r.count;
+    if (ms) ms[cnt] = r.ms;
+    ++cnt;
+  }
+  *n = cnt;
+  return OEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,238 @@
+// Internal declarations shared by the engine's translation units: device-side parameter
+// blocks, the plan object, launch helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/oem_b200.h"
+
+namespace oem {
+
+// ---------------------------------------------------------------------------------------------
+// Error reporting (thread-local last error, negative status codes)
+// ---------------------------------------------------------------------------------------------
+int set_error(int code, const std::string& msg);
+int cuda_error(cudaError_t e, const char* what);
+
+#define OEM_CUDA(call)                                               \
+  do {                                                               \
+    cudaError_t e_ = (call);                                         \
+    if (e_ != cudaSuccess) return ::oem::cuda_error(e_, #call);      \
+  } while (0)
+
+// ---------------------------------------------------------------------------------------------
+// Device-side views
+// ---------------------------------------------------------------------------------------------
+
+// One material tuple: update coefficients, permittivity and ADE pole set of the three E
+// components at one cell. 64 bytes.
+struct MatRec {
+  float ca[3];
+  float cb[3];
+  float eps[3];
+  int pset[3];  // -1 = not dispersive
+  int np[3];    // poles of that set (0 when not dispersive)
+  int reserved;
+};
+static_assert(sizeof(MatRec) == 64, "MatRec must be 16 words");
+
+// One grid axis on the device. z tables are padded to nzp entries.
+struct DevAxis {
+  const float* idl_p;  // 1 / primal spacing
+  const float* idl_d;  // 1 / dual spacing
+  const int* nxt;      // forward neighbour
+  const int* prv;      // backward neighbour
+  const float* mnx;    // forward-neighbour mask (0 at an absorbing high wall)
+  const float* mpv;    // backward-neighbour mask
+  const float* ae;     // CPML (a, b, 1/kappa) at E positions
+  const float* be;
+  const float* ke;
+  const float* ah;     // CPML at H positions
+  const float* bh;
+  const float* kh;
+  int n;
+  int lo;  // psi slab cells at the low end  [0, lo)
+  int hi;  // psi slab cells at the high end [n - hi, n)
+};
+
+// psi storage: [derivative axis][component slot][0 = low slab, 1 = high slab]; the component
+// slots of derivative axis a are the two components != a in ascending order.
+struct PsiSet {
+  float* p[3][2][2];
+};
+
+// Everything the Yee kernels need.
+struct YeeParams {
+  float* f[6];  // Ex Ey Ez Hx Hy Hz, padded (nx, ny, nzp)
+  DevAxis ax[3];
+  PsiSet psih;
+  PsiSet psie;
+  int nx, ny, nz, nzp;
+  float ch;  // dt / mu0
+  float cw;  // eps0 / dt
+  const uint16_t* mat16;  // per-cell material index (padded layout), one of the two
+  const uint32_t* mat32;
+  const MatRec* mats;
+  // ADE
+  float2* P;               // pole states, cell order then component then pole
+  const float4* pcoef;     // per pole of a set: (Re(A-1), Im(A-1), Re(B), Im(B))
+  const int* pset_ofs;     // set -> first pole in pcoef
+  const uint32_t* seg_ofs; // poles stored before each 32-cell segment
+  int has_ade;
+};
+
+struct PlaneSrc {
+  int pol, kh, ks;
+  float coef_h, coef_e;
+  int64_t ntab;
+  double* d_ex = nullptr;
+  double* d_hy = nullptr;
+};
+
+struct DipoleSet {
+  int magnetic = 0;
+  int n_targets = 0;
+  int64_t nsteps1 = 0;
+  int n_src = 0;
+  int64_t* d_target = nullptr;  // padded flat index of each distinct (comp, cell)
+  int* d_tcomp = nullptr;
+  int* d_ofs = nullptr;         // target -> its points [ofs[t], ofs[t+1])
+  float* d_coef = nullptr;
+  int* d_src = nullptr;
+  double* d_amp = nullptr;      // (n_src, nsteps1)
+};
+
+struct Monitor {
+  int kind = 0;   // 0 = flux plane, 1 = box
+  int axis = 0, km = 0;
+  int i0 = 0, j0 = 0, k0 = 0, ni = 0, nj = 0, nk = 0;
+  int n1 = 0, n2 = 0;  // plane extent (transverse axes ascending)
+  int nf = 0, T = 1, ncomp = 0;
+  int64_t cells = 0;
+  int64_t n_total = 0;
+  float* d_phase = nullptr;  // (n_total, nf, 4)
+  float* d_snap = nullptr;   // (T, ncomp, cells)
+  double* d_re = nullptr;    // (ncomp, nf, cells)
+  double* d_im = nullptr;
+  int* d_done = nullptr;     // last step already folded into the accumulators
+};
+
+struct TimeMon {
+  int nc = 0;
+  int comps[6] = {0, 0, 0, 0, 0, 0};
+  int i0 = 0, j0 = 0, k0 = 0, ni = 0, nj = 0, nk = 0;
+  int beg = 0, end = 0, iv = 1, nslots = 0;
+  float* d_buf = nullptr;  // (nc, nslots, ni, nj, nk)
+};
+
+struct AxisHost {
+  std::vector<double> idl_p, idl_d, mnx, mpv, pml_e, pml_h;
+  std::vector<int> nxt, prv;
+  int lo = 0, hi = 0;
+  bool set = false;
+};
+
+struct TimingRec {
+  std::string name;
+  int64_t count = 0;
+  double ms = 0.0;
+};
+
+}  // namespace oem
+
+struct oem_plan {
+  int device = 0;
+  int nx = 0, ny = 0, nz = 0, nzp = 0;
+  double ch = 0.0, cw = 0.0;
+  int64_t n_total = 0;
+  int64_t steps = 0;
+  bool finalized = false;
+
+  oem::AxisHost axh[3];
+  // materials (host staging until finalize)
+  std::vector<oem::MatRec> mats;
+  int index_bytes = 0;
+  std::vector<uint8_t> mat_index;  // unpadded, index_bytes per cell
+  // pole sets
+  std::vector<int> pset_ofs;
+  std::vector<float> pcoef;
+  std::vector<uint32_t> seg_ofs;
+  int64_t n_pole_total = 0;
+
+  std::vector<oem::PlaneSrc> planes;
+  std::vector<oem::DipoleSet> dipoles;
+  std::vector<oem::Monitor> mons;
+  std::vector<oem::TimeMon> tmons;
+
+  // device state
+  std::vector<void*> allocs;
+  oem::YeeParams yp{};
+  int* d_step = nullptr;
+  double* d_energy_part = nullptr;
+  int energy_blocks = 0;
+  double* d_dl[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};  // primal, dual
+
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t graph_many = nullptr;
+  cudaGraphExec_t graph_one = nullptr;
+  int graph_steps = 1;
+
+  bool timing = false;
+  std::vector<oem::TimingRec> trecs;
+};
+
+namespace oem {
+
+// Device allocation tracked by the plan (freed in oem_plan_destroy).
+template <class T>
+int dalloc(oem_plan* p, T** out, size_t count, bool zero = true) {
+  void* ptr = nullptr;
+  size_t bytes = count * sizeof(T);
+  if (bytes == 0) bytes = sizeof(T);
+  cudaError_t e = cudaMalloc(&ptr, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(OEM_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(bytes) +
+                                         " bytes failed: " + cudaGetErrorString(e));
+  }
+  p->allocs.push_back(ptr);
+  if (zero) {
+    e = cudaMemset(ptr, 0, bytes);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemset");
+  }
+  *out = static_cast<T*>(ptr);
+  return OEM_OK;
+}
+
+template <class T>
+int dupload(oem_plan* p, T** out, const T* host, size_t count) {
+  int rc = dalloc(p, out, count, false);
+  if (rc) return rc;
+  if (count) OEM_CUDA(cudaMemcpy(*out, host, count * sizeof(T), cudaMemcpyHostToDevice));
+  return OEM_OK;
+}
+
+// Kernel launchers (defined in oem_kernels.cu). All return a cudaError_t of the launch.
+cudaError_t launch_update_h(const YeeParams& P, cudaStream_t s);
+cudaError_t launch_update_e(const YeeParams& P, cudaStream_t s);
+cudaError_t launch_plane_h(const YeeParams& P, const PlaneSrc& src, const int* step,
+                           cudaStream_t s);
+cudaError_t launch_plane_e(const YeeParams& P, const PlaneSrc& src, const int* step,
+                           cudaStream_t s);
+cudaError_t launch_dipoles(const YeeParams& P, const DipoleSet& d, const int* step,
+                           cudaStream_t s);
+cudaError_t launch_time_sample(const YeeParams& P, const TimeMon& m, const int* step, int add,
+                               cudaStream_t s);
+cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* step,
+                            cudaStream_t s);
+cudaError_t launch_flush(const Monitor& m, const int* step, int forced, cudaStream_t s);
+cudaError_t launch_step_advance(int* step, cudaStream_t s);
+cudaError_t launch_energy(const YeeParams& P, double* const dl[3][2], double* part, int nblocks,
+                          cudaStream_t s);
+int energy_block_count(const YeeParams& P);
+
+}  // namespace oem

@@ -1,0 +1,493 @@
+// Step-loop kernels of the sm_100a engine: Yee H and E updates (CPML psi in the boundary slabs,
+// conductivity and PEC folded into per-material coefficients, ADE pole update inlined into the
+// E update), plane-wave and point-dipole injection, field time sampling, batched DFT snapshot
+// and flush, early-termination reductions.
+//
+// The update equations are those of OpenEM (openem/kernels/yee.cu:60-240,
+// dispersion.cu:168-207, source_dft.cu:39-206, 273-319, 440-779); the data layout and the
+// way cells find their coefficients and pole states are this engine's:
+//   * fields are (nx, ny, nzp) with nzp a multiple of 32, so one warp covers one 32-cell z
+//     segment of one row;
+//   * one material index per cell selects a 64-byte tuple (ca, cb, eps, pole set) x 3;
+//   * psi exists only inside the CPML slabs; elsewhere the stretched derivative is the plain
+//     derivative (identity coefficients);
+//   * ADE pole states are packed in cell order; a cell finds its first pole from the offset of
+//     its 32-cell segment plus a warp-ballot prefix sum of the pole counts of the lanes before
+//     it, so no per-entry index arrays are read.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "oem_internal.cuh"
+
+namespace oem {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ float* psi_at(const PsiSet& S, int a, int slot, const DevAxis& A,
+                                        int i, int j, int k, int ny, int nzp) {
+  const int q = (a == 0) ? i : ((a == 1) ? j : k);
+  int side, ql, L;
+  if (q < A.lo) {
+    side = 0; ql = q; L = A.lo;
+  } else if (q >= A.n - A.hi) {
+    side = 1; ql = q - (A.n - A.hi); L = A.hi;
+  } else {
+    return nullptr;
+  }
+  float* base = S.p[a][slot][side];
+  int64_t idx;
+  if (a == 0) idx = ((int64_t)ql * ny + j) * nzp + k;
+  else if (a == 1) idx = ((int64_t)i * L + ql) * nzp + k;
+  else idx = ((int64_t)i * ny + j) * L + ql;
+  return base + idx;
+}
+
+// CPML recursion (openem/kernels/yee.cu:60-74): psi = b psi + a d; return d/kappa + psi.
+// Outside the slabs the coefficients are the identity and psi is identically zero.
+__device__ __forceinline__ float stretch(float d, float* psi, float a, float b, float ik) {
+  if (psi == nullptr) return d;
+  const float p = b * (*psi) + a * d;
+  *psi = p;
+  return ik * d + p;
+}
+
+__device__ __forceinline__ uint32_t mat_id(const YeeParams& P, int64_t id) {
+  return P.mat16 ? (uint32_t)P.mat16[id] : P.mat32[id];
+}
+
+// Deferred ADE of one component: post(n-1) with E^n, then pre(n) with E^n; returns
+// w = sum 2 Re(dP) (openem/kernels/dispersion.cu:168-207, bitwise the same sequence).
+__device__ __forceinline__ float ade(const YeeParams& P, int set, int np, uint32_t poff,
+                                     float en) {
+  float w = 0.0f;
+  const float4* cf = P.pcoef + P.pset_ofs[set];
+  for (int t = 0; t < np; ++t) {
+    const float4 c = __ldg(cf + t);
+    float2 st = P.P[poff + t];
+    const float pr = st.x + c.z * en;
+    const float pi = st.y + c.w * en;
+    const float dr = c.x * pr - c.y * pi + c.z * en;
+    const float di = c.x * pi + c.y * pr + c.w * en;
+    st.x = pr + dr;
+    st.y = pi + di;
+    P.P[poff + t] = st;
+    w += 2.0f * dr;
+  }
+  return w;
+}
+
+// H half step, one thread per cell (openem/kernels/yee.cu:76-137).
+__global__ void __launch_bounds__(128) k_update_h(YeeParams P) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= P.nz || j >= P.ny) return;
+  const int64_t sj = P.nzp, si = (int64_t)P.ny * P.nzp;
+  const int64_t id = i * si + j * sj + k;
+  const DevAxis& X = P.ax[0];
+  const DevAxis& Y = P.ax[1];
+  const DevAxis& Z = P.ax[2];
+  const int ip = X.nxt[i], jp = Y.nxt[j], kp = Z.nxt[k];
+  const float mi = X.mnx[i], mj = Y.mnx[j], mk = Z.mnx[k];
+  const float* Ex = P.f[0];
+  const float* Ey = P.f[1];
+  const float* Ez = P.f[2];
+  const float ex = Ex[id], ey = Ey[id], ez = Ez[id];
+  const int64_t idi = ip * si + j * sj + k;
+  const int64_t idj = i * si + jp * sj + k;
+  const int64_t idk = i * si + j * sj + kp;
+  const float ch = P.ch;
+  {  // Hx: mu0 dHx/dt = -(dEz/dy - dEy/dz)
+    const float dzy = (Ez[idj] * mj - ez) * Y.idl_p[j];
+    const float dyz = (Ey[idk] * mk - ey) * Z.idl_p[k];
+    const float sy = stretch(dzy, psi_at(P.psih, 1, 0, Y, i, j, k, P.ny, P.nzp), Y.ah[j], Y.bh[j], Y.kh[j]);
+    const float sz = stretch(dyz, psi_at(P.psih, 2, 0, Z, i, j, k, P.ny, P.nzp), Z.ah[k], Z.bh[k], Z.kh[k]);
+    P.f[3][id] -= ch * (sy - sz);
+  }
+  {  // Hy: mu0 dHy/dt = -(dEx/dz - dEz/dx)
+    const float dxz = (Ex[idk] * mk - ex) * Z.idl_p[k];
+    const float dzx = (Ez[idi] * mi - ez) * X.idl_p[i];
+    const float sz = stretch(dxz, psi_at(P.psih, 2, 1, Z, i, j, k, P.ny, P.nzp), Z.ah[k], Z.bh[k], Z.kh[k]);
+    const float sx = stretch(dzx, psi_at(P.psih, 0, 0, X, i, j, k, P.ny, P.nzp), X.ah[i], X.bh[i], X.kh[i]);
+    P.f[4][id] -= ch * (sz - sx);
+  }
+  {  // Hz: mu0 dHz/dt = -(dEy/dx - dEx/dy)
+    const float dyx = (Ey[idi] * mi - ey) * X.idl_p[i];
+    const float dxy = (Ex[idj] * mj - ex) * Y.idl_p[j];
+    const float sx = stretch(dyx, psi_at(P.psih, 0, 1, X, i, j, k, P.ny, P.nzp), X.ah[i], X.bh[i], X.kh[i]);
+    const float sy = stretch(dxy, psi_at(P.psih, 1, 1, Y, i, j, k, P.ny, P.nzp), Y.ah[j], Y.bh[j], Y.kh[j]);
+    P.f[5][id] -= ch * (sx - sy);
+  }
+}
+
+// E full step with the ADE inlined, one thread per cell (openem/kernels/yee.cu:154-240 and
+// dispersion.cu:168-207). Block (32, 4): each warp is one aligned 32-cell z segment.
+__global__ void __launch_bounds__(128) k_update_e(YeeParams P) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (j >= P.ny) return;  // warp-uniform: a warp lies in one row
+  const int64_t sj = P.nzp, si = (int64_t)P.ny * P.nzp;
+  const int64_t id = i * si + j * sj + k;
+  const MatRec& M = P.mats[mat_id(P, id)];
+  uint32_t poff = 0;
+  if (P.has_ade) {
+    const int npc = M.np[0] + M.np[1] + M.np[2];
+    const unsigned lt = (1u << (threadIdx.x & 31)) - 1u;
+    int pre = 0;
+#pragma unroll
+    for (int b = 0; b < 6; ++b) pre += __popc(__ballot_sync(kFull, (npc >> b) & 1) & lt) << b;
+    poff = P.seg_ofs[id >> 5] + (uint32_t)pre;
+  }
+  if (k >= P.nz) return;
+  const DevAxis& X = P.ax[0];
+  const DevAxis& Y = P.ax[1];
+  const DevAxis& Z = P.ax[2];
+  const int im = X.prv[i], jm = Y.prv[j], km = Z.prv[k];
+  const float mi = X.mpv[i], mj = Y.mpv[j], mk = Z.mpv[k];
+  const float* Hx = P.f[3];
+  const float* Hy = P.f[4];
+  const float* Hz = P.f[5];
+  const float hx = Hx[id], hy = Hy[id], hz = Hz[id];
+  const int64_t idi = im * si + j * sj + k;
+  const int64_t idj = i * si + jm * sj + k;
+  const int64_t idk = i * si + j * sj + km;
+  const float cw = P.cw;
+  {  // Ex: eps dEx/dt = dHz/dy - dHy/dz
+    const float en = P.f[0][id];
+    const float w = (M.np[0] > 0) ? ade(P, M.pset[0], M.np[0], poff, en) : 0.0f;
+    const float dzy = (hz - Hz[idj] * mj) * Y.idl_d[j];
+    const float dyz = (hy - Hy[idk] * mk) * Z.idl_d[k];
+    const float sy = stretch(dzy, psi_at(P.psie, 1, 0, Y, i, j, k, P.ny, P.nzp), Y.ae[j], Y.be[j], Y.ke[j]);
+    const float sz = stretch(dyz, psi_at(P.psie, 2, 0, Z, i, j, k, P.ny, P.nzp), Z.ae[k], Z.be[k], Z.ke[k]);
+    P.f[0][id] = M.ca[0] * en + M.cb[0] * (sy - sz - cw * w);
+  }
+  {  // Ey: eps dEy/dt = dHx/dz - dHz/dx
+    const float en = P.f[1][id];
+    const float w = (M.np[1] > 0) ? ade(P, M.pset[1], M.np[1], poff + M.np[0], en) : 0.0f;
+    const float dxz = (hx - Hx[idk] * mk) * Z.idl_d[k];
+    const float dzx = (hz - Hz[idi] * mi) * X.idl_d[i];
+    const float sz = stretch(dxz, psi_at(P.psie, 2, 1, Z, i, j, k, P.ny, P.nzp), Z.ae[k], Z.be[k], Z.ke[k]);
+    const float sx = stretch(dzx, psi_at(P.psie, 0, 0, X, i, j, k, P.ny, P.nzp), X.ae[i], X.be[i], X.ke[i]);
+    P.f[1][id] = M.ca[1] * en + M.cb[1] * (sz - sx - cw * w);
+  }
+  {  // Ez: eps dEz/dt = dHy/dx - dHx/dy
+    const float en = P.f[2][id];
+    const float w = (M.np[2] > 0)
+                        ? ade(P, M.pset[2], M.np[2], poff + M.np[0] + M.np[1], en) : 0.0f;
+    const float dyx = (hy - Hy[idi] * mi) * X.idl_d[i];
+    const float dxy = (hx - Hx[idj] * mj) * Y.idl_d[j];
+    const float sx = stretch(dyx, psi_at(P.psie, 0, 1, X, i, j, k, P.ny, P.nzp), X.ae[i], X.be[i], X.ke[i]);
+    const float sy = stretch(dxy, psi_at(P.psie, 1, 1, Y, i, j, k, P.ny, P.nzp), Y.ae[j], Y.be[j], Y.ke[j]);
+    P.f[2][id] = M.ca[2] * en + M.cb[2] * (sx - sy - cw * w);
+  }
+}
+
+// One-face TF/SF plane wave, H side (openem/kernels/source_dft.cu:40-55).
+__global__ void k_plane_h(YeeParams P, PlaneSrc s, const int* step) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  const int n = *step;
+  if (i >= P.nx || j >= P.ny || n < 0 || n >= s.ntab) return;
+  const float inc = (float)s.d_ex[n];
+  float* H = P.f[s.pol == 0 ? 4 : 3];
+  H[((int64_t)i * P.ny + j) * P.nzp + s.kh] += s.coef_h * inc;
+}
+
+// One-face TF/SF plane wave, E side (openem/kernels/source_dft.cu:58-73).
+__global__ void k_plane_e(YeeParams P, PlaneSrc s, const int* step) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  const int n = *step;
+  if (i >= P.nx || j >= P.ny || n < 0 || n >= s.ntab) return;
+  const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + s.ks;
+  const float inc = (float)s.d_hy[n];
+  const float cb = P.mats[mat_id(P, id)].cb[s.pol];
+  P.f[s.pol][id] += cb * s.coef_e * inc;
+}
+
+// Point dipoles, one thread per distinct (component, cell); its stencil points are added in a
+// fixed order, so the result is deterministic (openem/kernels/source_dft.cu:147-206 uses
+// atomicAdd instead).
+__global__ void k_dipoles(YeeParams P, DipoleSet d, const int* step) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = *step;
+  if (t >= d.n_targets || n < 0 || n >= d.nsteps1) return;
+  const int c = d.d_tcomp[t];
+  const int64_t id = d.d_target[t];
+  float* F = P.f[d.magnetic ? 3 + c : c];
+  const float cc = d.magnetic ? P.ch : P.mats[mat_id(P, id)].cb[c];
+  float v = F[id];
+  for (int q = d.d_ofs[t]; q < d.d_ofs[t + 1]; ++q) {
+    const float a = (float)d.d_amp[(int64_t)d.d_src[q] * d.nsteps1 + n];
+    v += -cc * d.d_coef[q] * a;
+  }
+  F[id] = v;
+}
+
+// Field time monitor, one shot of the two-shot H average (openem/kernels/source_dft.cu:282-319).
+__global__ void k_time_sample(YeeParams P, TimeMon m, const int* step, int add) {
+  const int m_ref = (*step + 1) - add;
+  const int soff = m_ref - m.beg;
+  if (soff < 0 || m_ref >= m.end || soff % m.iv) return;
+  const int slot = soff / m.iv;
+  if (slot >= m.nslots) return;
+  const int cc = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y * blockDim.y + threadIdx.y;
+  const int a = blockIdx.z;
+  if (a >= m.ni || b >= m.nj || cc >= m.nk) return;
+  const int64_t id = ((int64_t)(m.i0 + a) * P.ny + (m.j0 + b)) * P.nzp + (m.k0 + cc);
+  const int64_t cells = (int64_t)m.ni * m.nj * m.nk;
+  const int64_t off = ((int64_t)a * m.nj + b) * m.nk + cc;
+  for (int q = 0; q < m.nc; ++q) {
+    const int comp = m.comps[q];
+    const float w = comp < 3 ? (add ? 0.0f : 1.0f) : 0.5f;
+    if (w == 0.0f) continue;
+    const int64_t o = ((int64_t)q * m.nslots + slot) * cells + off;
+    const float v = w * P.f[comp][id];
+    m.d_buf[o] = add ? m.d_buf[o] + v : v;
+  }
+}
+
+// DFT snapshot of a flux plane: (E_t1, E_t2, colocated H_t1, colocated H_t2) into ring row
+// step % T (openem/kernels/source_dft.cu:532-564 stores six raw values; the colocation
+// average (H[k] + H[k-1]) / 2 is taken here in the same fp32 arithmetic).
+__global__ void k_snap_plane(YeeParams P, Monitor m, const int* step) {
+  const int p2 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p1 = blockIdx.y * blockDim.y + threadIdx.y;
+  if (p1 >= m.n1 || p2 >= m.n2) return;
+  const int t1 = (m.axis == 0) ? 1 : 0;
+  const int t2 = (m.axis == 2) ? 1 : 2;
+  int c[3];
+  c[m.axis] = m.km; c[t1] = p1; c[t2] = p2;
+  const int64_t id = ((int64_t)c[0] * P.ny + c[1]) * P.nzp + c[2];
+  c[m.axis] = m.km - 1;
+  const int64_t idm = ((int64_t)c[0] * P.ny + c[1]) * P.nzp + c[2];
+  const int64_t off = (int64_t)p1 * m.n2 + p2;
+  float* row = m.d_snap + (int64_t)((*step) % m.T) * 4 * m.cells;
+  row[off] = P.f[t1][id];
+  row[m.cells + off] = P.f[t2][id];
+  row[2 * m.cells + off] = 0.5f * (P.f[3 + t1][id] + P.f[3 + t1][idm]);
+  row[3 * m.cells + off] = 0.5f * (P.f[3 + t2][id] + P.f[3 + t2][idm]);
+}
+
+// DFT snapshot of a box: the six components at their Yee positions
+// (openem/kernels/source_dft.cu:453-478).
+__global__ void k_snap_box(YeeParams P, Monitor m, const int* step) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m.cells) return;
+  const int64_t njk = (int64_t)m.nj * m.nk;
+  const int a = (int)(t / njk);
+  const int64_t r = t - a * njk;
+  const int b = (int)(r / m.nk);
+  const int cc = (int)(r - (int64_t)b * m.nk);
+  const int64_t id = ((int64_t)(m.i0 + a) * P.ny + (m.j0 + b)) * P.nzp + (m.k0 + cc);
+  float* row = m.d_snap + (int64_t)((*step) % m.T) * 6 * m.cells;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) row[q * m.cells + t] = P.f[q][id];
+}
+
+// Batched DFT flush (openem/kernels/source_dft.cu:440-530): at a batch boundary, or when
+// forced, fold the not-yet-folded snapshot rows into the float64 accumulators. Per
+// (point, frequency) the rows are summed in step order into an fp32 partial, which is then
+// added to the float64 accumulator once. done[0] holds the last step already folded.
+template <int NC>
+__global__ void __launch_bounds__(128) k_flush(Monitor m, const int* step, int forced) {
+  const int64_t pt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (pt >= m.cells) return;
+  const int s_now = forced ? (*step - 1) : *step;
+  if (!forced && ((s_now + 1) % m.T) != 0) return;
+  const int s_lo = *m.d_done + 1;
+  if (s_lo > s_now) return;
+  constexpr int NE = NC / 2;  // E components come first
+  for (int f0 = 0; f0 < m.nf; f0 += 8) {
+    const int nfc = min(8, m.nf - f0);
+    float aR[8][NC], aI[8][NC];
+#pragma unroll
+    for (int ff = 0; ff < 8; ++ff)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) { aR[ff][c] = 0.f; aI[ff][c] = 0.f; }
+    for (int s = s_lo; s <= s_now; ++s) {
+      const float* row = m.d_snap + (int64_t)(s % m.T) * NC * m.cells;
+      float v[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) v[c] = row[c * m.cells + pt];
+      const float4* ph = reinterpret_cast<const float4*>(m.d_phase) + ((int64_t)s * m.nf + f0);
+#pragma unroll
+      for (int ff = 0; ff < 8; ++ff) {
+        if (ff < nfc) {
+          const float4 q = __ldg(ph + ff);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            aR[ff][c] = fmaf(v[c], c < NE ? q.x : q.z, aR[ff][c]);
+            aI[ff][c] = fmaf(v[c], c < NE ? q.y : q.w, aI[ff][c]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int ff = 0; ff < 8; ++ff) {
+      if (ff < nfc) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const int64_t o = ((int64_t)c * m.nf + f0 + ff) * m.cells + pt;
+          m.d_re[o] += (double)aR[ff][c];
+          m.d_im[o] += (double)aI[ff][c];
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_flush_mark(int T, const int* step, int* done, int forced) {
+  const int s_now = forced ? (*step - 1) : *step;
+  if (forced || ((s_now + 1) % T) == 0) {
+    if (s_now > *done) *done = s_now;
+  }
+}
+
+__global__ void k_step_advance(int* step) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) ++*step;
+}
+
+// Float64 volume-weighted sums for early termination (openem/solver.py:107-121, 160-203),
+// one partial per block: [sum V|E|^2, sum V eps |E|^2, sum V |H|^2].
+__global__ void __launch_bounds__(256) k_energy(YeeParams P, const double* dxp, const double* dxd,
+                                                const double* dyp, const double* dyd,
+                                                const double* dzp, const double* dzd,
+                                                double* part) {
+  __shared__ double sh[3][256];
+  const int64_t n = (int64_t)P.nx * P.ny * P.nz;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(t % P.nz);
+    const int64_t r = t / P.nz;
+    const int j = (int)(r % P.ny);
+    const int i = (int)(r / P.ny);
+    const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + k;
+    const MatRec& M = P.mats[mat_id(P, id)];
+    const double vex = dxp[i] * dyd[j] * dzd[k];
+    const double vey = dxd[i] * dyp[j] * dzd[k];
+    const double vez = dxd[i] * dyd[j] * dzp[k];
+    const double vhx = dxd[i] * dyp[j] * dzp[k];
+    const double vhy = dxp[i] * dyd[j] * dzp[k];
+    const double vhz = dxp[i] * dyp[j] * dzd[k];
+    const double ex = P.f[0][id], ey = P.f[1][id], ez = P.f[2][id];
+    const double hx = P.f[3][id], hy = P.f[4][id], hz = P.f[5][id];
+    const double e0 = vex * ex * ex, e1 = vey * ey * ey, e2 = vez * ez * ez;
+    s0 += e0 + e1 + e2;
+    s1 += e0 * M.eps[0] + e1 * M.eps[1] + e2 * M.eps[2];
+    s2 += vhx * hx * hx + vhy * hy * hy + vhz * hz * hz;
+  }
+  sh[0][threadIdx.x] = s0;
+  sh[1][threadIdx.x] = s1;
+  sh[2][threadIdx.x] = s2;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+      sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+      sh[2][threadIdx.x] += sh[2][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x + 0] = sh[0][0];
+    part[3 * blockIdx.x + 1] = sh[1][0];
+    part[3 * blockIdx.x + 2] = sh[2][0];
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------------------------
+
+cudaError_t launch_update_h(const YeeParams& P, cudaStream_t s) {
+  dim3 b(32, 4, 1), g(P.nzp / 32, (P.ny + 3) / 4, P.nx);
+  k_update_h<<<g, b, 0, s>>>(P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_update_e(const YeeParams& P, cudaStream_t s) {
+  dim3 b(32, 4, 1), g(P.nzp / 32, (P.ny + 3) / 4, P.nx);
+  k_update_e<<<g, b, 0, s>>>(P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_plane_h(const YeeParams& P, const PlaneSrc& src, const int* step,
+                           cudaStream_t s) {
+  dim3 b(32, 8, 1), g((P.ny + 31) / 32, (P.nx + 7) / 8, 1);
+  k_plane_h<<<g, b, 0, s>>>(P, src, step);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_plane_e(const YeeParams& P, const PlaneSrc& src, const int* step,
+                           cudaStream_t s) {
+  dim3 b(32, 8, 1), g((P.ny + 31) / 32, (P.nx + 7) / 8, 1);
+  k_plane_e<<<g, b, 0, s>>>(P, src, step);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dipoles(const YeeParams& P, const DipoleSet& d, const int* step,
+                           cudaStream_t s) {
+  if (d.n_targets == 0) return cudaSuccess;
+  k_dipoles<<<(d.n_targets + 63) / 64, 64, 0, s>>>(P, d, step);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_time_sample(const YeeParams& P, const TimeMon& m, const int* step, int add,
+                               cudaStream_t s) {
+  dim3 b(32, 4, 1), g((m.nk + 31) / 32, (m.nj + 3) / 4, m.ni);
+  k_time_sample<<<g, b, 0, s>>>(P, m, step, add);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* step,
+                            cudaStream_t s) {
+  if (m.kind == 0) {
+    dim3 b(32, 4, 1), g((m.n2 + 31) / 32, (m.n1 + 3) / 4, 1);
+    k_snap_plane<<<g, b, 0, s>>>(P, m, step);
+  } else {
+    const int64_t nb = (m.cells + 255) / 256;
+    k_snap_box<<<(unsigned)nb, 256, 0, s>>>(P, m, step);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_flush(const Monitor& m, const int* step, int forced, cudaStream_t s) {
+  const int64_t nb = (m.cells + 127) / 128;
+  if (m.ncomp == 4)
+    k_flush<4><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
+  else
+    k_flush<6><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_flush_mark<<<1, 1, 0, s>>>(m.T, step, m.d_done, forced);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step_advance(int* step, cudaStream_t s) {
+  k_step_advance<<<1, 32, 0, s>>>(step);
+  return cudaGetLastError();
+}
+
+int energy_block_count(const YeeParams& P) {
+  const int64_t n = (int64_t)P.nx * P.ny * P.nz;
+  int64_t nb = (n + 255) / 256;
+  if (nb > 148 * 16) nb = 148 * 16;
+  return (int)(nb < 1 ? 1 : nb);
+}
+
+cudaError_t launch_energy(const YeeParams& P, double* const dl[3][2], double* part, int nblocks,
+                          cudaStream_t s) {
+  k_energy<<<nblocks, 256, 0, s>>>(P, dl[0][0], dl[0][1], dl[1][0], dl[1][1], dl[2][0],
+                                   dl[2][1], part);
+  return cudaGetLastError();
+}
+
+}  // namespace oem

@@ -1,0 +1,361 @@
+"""Synthetic ``Scene`` factory for the workloads the engine is measured and tested on.
+
+Tidy3D is not available, so these builders do the part of OpenEM's scene builder
+(``openem/scene/build.py:224``) that the workloads need, from first principles:
+
+* uniform Yee grids with the 12-layer Tidy3D CPML added outside the simulation domain
+  (``openem/cpml.py:149``), time step at a Courant factor of 0.99;
+* staircased media: a component's cell takes the medium that contains its own Yee position;
+* pole-residue media (Drude, Lorentz) reduced to trapezoidal ADE coefficients, with the DC pole
+  of a Drude term moved onto the conductivity (``openem/scene/poles.py:157-188,284-296``);
+* Gaussian-pulse waveforms sampled at whole and half steps, one-face plane-wave incident tables
+  (``openem/scene/sources.py:19-83``), trilinear point-dipole stencils.
+
+Every builder is deterministic for a given seed.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from openem_b200.model import (
+    C_0, EPSILON_0, ETA_0, Axis, Dispersion, FieldMonitor, FieldTimeMonitor, FluxMonitor,
+    GaussianPulse, Grid, PlaneWaveSource, PMLParams, PointDipole, Scene, pml_build,
+    sample_waveform)
+
+UM = 1e-6
+
+
+def courant_dt(dls, courant: float = 0.99) -> float:
+    """``dt = S / (c sqrt(sum 1/dl^2))`` with the smallest spacing on each axis."""
+    inv = sum(1.0 / float(np.min(d)) ** 2 for d in dls)
+    return courant / (C_0 * np.sqrt(inv))
+
+
+def uniform_axis(n_cells: int, dl: float, lo: float, boundary: str, n_pml: int = 0) -> Axis:
+    """``n_cells`` interior cells starting at ``lo`` (metres) plus ``n_pml`` layers at each end
+    when the boundary is a PML."""
+    extra = n_pml if boundary == "PML" else 0
+    k = np.arange(-extra, n_cells + extra + 1, dtype=np.float64)
+    return Axis(lo + k * dl, boundary, boundary)
+
+
+def pml_dict(grid: Grid, dt: float, n_layers: int = 12) -> dict:
+    """Tidy3D's default ``td.PML()`` coefficients on every PML face, graded with the end cell's
+    spacing and vacuum speed."""
+    params = PMLParams(num_layers=n_layers)
+    out = {}
+    for a, ax in enumerate(grid.axes):
+        if ax.boundary_lo != "PML":
+            continue
+        dl = ax.dl
+        out[(a, "lo")] = pml_build(params, float(dl[0]), "lo", dt)
+        out[(a, "hi")] = pml_build(params, float(dl[-1]), "hi", dt)
+    return out
+
+
+def yee_coords(grid: Grid):
+    """Per-component Yee coordinates ``(x, y, z)`` 1D arrays: Ex(ctr, edge, edge),
+    Ey(edge, ctr, edge), Ez(edge, edge, ctr); H swaps edge and centre."""
+    e = [np.asarray(a.edges[:-1], dtype=np.float64) for a in grid.axes]
+    c = [a.centers for a in grid.axes]
+    on_edge = {0: (False, True, True), 1: (True, False, True), 2: (True, True, False),
+               3: (True, False, False), 4: (False, True, False), 5: (False, False, True)}
+    return {k: tuple(e[a] if v[a] else c[a] for a in range(3)) for k, v in on_edge.items()}
+
+
+def spectrum(source_time, dt: float, num_steps: int, freqs) -> np.ndarray:
+    """Discrete source spectrum ``sum_n a(n dt) e^{i 2 pi f n dt} dt`` (stored with each flux
+    monitor, used only by post-processing)."""
+    t = np.arange(num_steps + 1, dtype=np.float64) * dt
+    a = np.asarray(source_time.amp_time(t))
+    f = np.asarray(freqs, dtype=np.float64)
+    return (a[None, :] * np.exp(2j * np.pi * f[:, None] * t[None, :])).sum(axis=1) * dt
+
+
+def plane_wave_tables(source_time, dt: float, num_steps: int, dl_half: float,
+                      eps_r: float, direction: int = 1):
+    """One-face TF/SF incident tables in a lossless medium: ``Ex_inc(n dt)`` on the source
+    plane, and ``Hy_inc`` on the upstream Hy point sampled at ``(n+1/2) dt + dl_half / v``
+    scaled by ``n / eta0`` (``openem/scene/sources.py:19-83``)."""
+    n_r = np.sqrt(eps_r)
+    v = C_0 / n_r
+    n = np.arange(num_steps + 1, dtype=np.float64)
+    ex_inc = np.real(np.asarray(source_time.amp_time(n * dt)))
+    t_h = (n + 0.5) * dt + dl_half / v
+    hy_inc = direction * np.real(np.asarray(source_time.amp_time(t_h)) * (n_r / ETA_0))
+    return np.ascontiguousarray(ex_inc), np.ascontiguousarray(hy_inc)
+
+
+# ---------------------------------------------------------------------------
+# Pole-residue media
+# ---------------------------------------------------------------------------
+
+def drude_poles(wp: float, gamma: float):
+    """Drude ``-wp^2 / (w^2 + i gamma w)`` as pole-residue pairs ``(a, c)`` in the convention
+    ``chi(s) = sum c/(s-a) + c*/(s-a*)`` (s = -i w): a DC pole ``(0, wp^2/2gamma)`` and
+    ``(-gamma, -wp^2/2gamma)``."""
+    c = wp * wp / (2.0 * gamma)
+    return [(0j, complex(c)), (complex(-gamma), complex(-c))]
+
+
+def lorentz_poles(deps: float, f0: float, delta: float):
+    """Lorentz ``deps f0^2 / (f0^2 - 2 i f delta - f^2)`` (Hz) as one pole-residue pair:
+    ``a = -D + i wd``, ``c = -i deps w0^2 / (2 wd)`` with ``w0 = 2 pi f0``, ``D = 2 pi delta``,
+    ``wd = sqrt(w0^2 - D^2)`` (underdamped)."""
+    w0 = 2.0 * np.pi * f0
+    d = 2.0 * np.pi * delta
+    wd = np.sqrt(w0 * w0 - d * d)
+    return [(complex(-d, wd), complex(0.0, -deps * w0 * w0 / (2.0 * wd)))]
+
+
+def split_dc(poles, dt: float, rtol: float = 1e-9):
+    """Move poles at ``a = 0`` onto a conductivity ``sigma = 2 Re(c) eps0``; return
+    ``(remaining poles, sigma)`` (``openem/scene/poles.py:157-188``)."""
+    keep, sigma = [], 0.0
+    for a, c in poles:
+        if abs(a) <= rtol / dt:
+            sigma += 2.0 * c.real * EPSILON_0
+        else:
+            keep.append((complex(a), complex(c)))
+    return keep, sigma
+
+
+def trap_coeffs(poles, dt: float):
+    """Trapezoidal ``(A - 1, B)`` of ``dP/dt = qP + rE``: ``A = (1 + q dt/2)/(1 - q dt/2)``,
+    ``B = (r dt/2)/(1 - q dt/2)`` (``openem/scene/poles.py:284-296``)."""
+    am1 = np.array([(1.0 + q * dt / 2.0) / (1.0 - q * dt / 2.0) - 1.0 for q, _ in poles],
+                   dtype=np.complex128)
+    b = np.array([(r * dt / 2.0) / (1.0 - q * dt / 2.0) for q, r in poles],
+                 dtype=np.complex128)
+    return am1, b
+
+
+def build_dispersion(masks, am1, b, shape) -> Dispersion | None:
+    """One entry per (component, cell) inside ``masks[c]``, every entry carrying the same
+    poles; entries ordered by component then flat cell index."""
+    comp, cell = [], []
+    for c in range(3):
+        idx = np.flatnonzero(masks[c].ravel())
+        comp.append(np.full(idx.size, c, dtype=np.int32))
+        cell.append(idx.astype(np.int32))
+    comp = np.concatenate(comp)
+    cell = np.concatenate(cell)
+    n = comp.size
+    if n == 0:
+        return None
+    p = am1.size
+    g1 = float(np.sum(2.0 * b.real))
+    return Dispersion(comp=comp, cell=cell,
+                      pole_ofs=(np.arange(n + 1, dtype=np.int64) * p).astype(np.int32),
+                      am1=np.tile(am1, n), b=np.tile(b, n), g=np.full(n, g1))
+
+
+# ---------------------------------------------------------------------------
+# Workload 1: slab plane-wave transmission
+# ---------------------------------------------------------------------------
+
+def slab_plane_wave(nxy: int = 30, dl: float = 0.02 * UM, lz: float = 3.0 * UM,
+                    eps_slab: float = 4.0, d_slab: float = 0.3 * UM,
+                    src_z: float = -1.0 * UM, mon_t: float = 1.0 * UM,
+                    mon_r: float = -1.2 * UM, freq0: float = 2.998e14, nfreq: int = 11,
+                    run_time: float = 4e-13, n_pml: int = 12, with_slab: bool = True,
+                    num_steps: int | None = None) -> Scene:
+    """0.6 x 0.6 x 3.0 um periodic-x/y cell, 12-layer CPML on +/-z, an eps=4 slab 0.3 um thick
+    at z=0, a +z Ex-polarised plane wave at z=-1.0 um (Gaussian pulse f0, fwidth=0.2 f0), flux
+    planes "T" at z=+1.0 um and "R" at z=-1.2 um at 11 frequencies over f0 +/- fwidth.
+
+    ``nxy`` may be reduced to 1: at normal incidence in a periodic cell the fields do not vary
+    along x or y, so the result per unit area is unchanged."""
+    nz_in = int(round(lz / dl))
+    ax = uniform_axis(nxy, dl, -0.5 * nxy * dl, "Periodic")
+    ay = uniform_axis(nxy, dl, -0.5 * nxy * dl, "Periodic")
+    az = uniform_axis(nz_in, dl, -0.5 * lz, "PML", n_pml)
+    grid = Grid(ax, ay, az)
+    dt = courant_dt([ax.dl, ay.dl, az.dl]) if nxy > 1 else courant_dt([az.dl] * 3)
+    n_steps = int(np.floor(run_time / dt + 1e-9)) + 1 if num_steps is None else int(num_steps)
+    shape = grid.shape
+    coords = yee_coords(grid)
+    eps = []
+    for c in range(3):
+        z = coords[c][2]
+        inside = np.abs(z) < 0.5 * d_slab - 1e-9 * dl
+        e = np.ones(shape)
+        if with_slab:
+            e[:, :, inside] = eps_slab
+        eps.append(e)
+    pulse = GaussianPulse(freq0=freq0, fwidth=0.2 * freq0)
+    wf = sample_waveform(pulse, dt, n_steps)
+    edges_z = np.asarray(az.edges)
+    ks = int(np.argmin(np.abs(edges_z - src_z)))
+    ex_inc, hy_inc = plane_wave_tables(pulse, dt, n_steps, 0.5 * float(az.dl[ks - 1]), 1.0, +1)
+    src = PlaneWaveSource(axis=2, plane_index=ks, direction=1, pol_axis=0, waveform=wf,
+                          angle_theta=0.0, num_freqs=1, ex_inc=ex_inc, hy_inc=hy_inc,
+                          center=src_z)
+    freqs = np.linspace(freq0 - 0.2 * freq0, freq0 + 0.2 * freq0, nfreq)
+    spec = spectrum(pulse, dt, n_steps, freqs)
+    mons = []
+    for name, zc in (("T", mon_t), ("R", mon_r)):
+        k = int(np.argmin(np.abs(edges_z - zc)))
+        mons.append(FluxMonitor(name=name, axis=2, plane_index=k, normal_dir=1, freqs=freqs,
+                                source_spectrum=spec))
+    return Scene(grid=grid, dt=dt, num_time_steps=n_steps, shutoff=1e-5,
+                 eps_ex=eps[0], eps_ey=eps[1], eps_ez=eps[2], pml=pml_dict(grid, dt, n_pml),
+                 sources=[src], flux_monitors=mons)
+
+
+def slab_transmission(res_slab, res_empty, name: str = "T") -> np.ndarray:
+    """``T(f) = P_slab / P_empty`` from two results' plane phasors, with the uniform-grid area
+    element (the normalisation ``openem/flux.py:108-134`` uses: a reference run without the
+    structure)."""
+    def p(res):
+        d = res.phasors[name].data
+        return 0.5 * (np.real(d[0] * np.conj(d[3])).sum(axis=(1, 2))
+                      - np.real(d[1] * np.conj(d[2])).sum(axis=(1, 2)))
+    return p(res_slab) / p(res_empty)
+
+
+def slab_analytic_T(freqs, n_slab: float = 2.0, d: float = 0.3 * UM) -> np.ndarray:
+    """Single-layer thin-film transmission at normal incidence in vacuum."""
+    k = 2 * np.pi * np.asarray(freqs) / C_0
+    r = (1 - n_slab) / (1 + n_slab)
+    ph = np.exp(2j * k * n_slab * d)
+    t = (1 - r * r) * np.exp(1j * k * n_slab * d) / (1 - r * r * ph)
+    return np.abs(t) ** 2
+
+
+# ---------------------------------------------------------------------------
+# Workload 2: dispersive bulk (Drude + Lorentz spheres, point dipole, plane DFT monitors)
+# ---------------------------------------------------------------------------
+
+def sphere_centres(n_sph: int, rmin: float, rmax: float, lo: float, hi: float, seed: int):
+    """``n_sph`` non-overlapping spheres by rejection sampling: radius ~ U[rmin, rmax], centre
+    ~ U over the box shrunk by the radius (the spheres stay inside the simulation domain)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    tries = 0
+    while len(out) < n_sph:
+        tries += 1
+        if tries > 200000:
+            raise RuntimeError("could not place the requested spheres")
+        r = rng.uniform(rmin, rmax)
+        c = rng.uniform(lo + r, hi - r, size=3)
+        if all(np.linalg.norm(c - c2) >= r + r2 for c2, r2 in out):
+            out.append((c, r))
+    return out
+
+
+def dipole_stencil(grid: Grid, comp: int, pos, magnetic: bool = False):
+    """Trilinear weights of a point current moment at ``pos`` on the Yee points of ``comp``,
+    divided by each point's dual volume -> ``(indices (nw, 3), coef (nw,))``."""
+    coords = yee_coords(grid)[comp + (3 if magnetic else 0)]
+    per_axis = []
+    for a in range(3):
+        co = coords[a]
+        x = pos[a]
+        i = int(np.argmin(np.abs(co - x)))
+        if abs(co[i] - x) <= 1e-12 * max(abs(x), 1e-9):
+            per_axis.append([(i, 1.0)])
+            continue
+        j = i + 1 if co[i] < x else i - 1
+        w = (x - co[i]) / (co[j] - co[i])
+        per_axis.append([(i, 1.0 - w), (j, w)])
+    vols = (grid.yee_h_dual_volumes() if magnetic else grid.yee_dual_volumes())[comp]
+    idx, coef = [], []
+    for i, wi in per_axis[0]:
+        for j, wj in per_axis[1]:
+            for k, wk in per_axis[2]:
+                idx.append((i, j, k))
+                coef.append(wi * wj * wk / vols[i, j, k])
+    return np.asarray(idx, dtype=np.int64), np.asarray(coef, dtype=np.float64)
+
+
+def dispersive_spheres(n: int = 512, dl: float = 0.02 * UM, n_pml: int = 12, n_sph: int = 64,
+                       rmin: float = 0.2 * UM, rmax: float = 0.6 * UM, seed: int = 0,
+                       num_steps: int = 2000, nfreq: int = 8,
+                       wp: float = 1.4e16, gamma: float = 1e14,
+                       lorentz=(1.5, 4e14, 5e13), dip_freq0: float = 2e14,
+                       dip_fwidth: float = 1e14, monitors: bool = True,
+                       mon_band=(1.5e14, 2.5e14)) -> Scene:
+    """``n^3`` cells in total (CPML included), CPML on all six faces, background eps=1, ``n_sph``
+    non-overlapping spheres of a Drude (wp, gamma in rad/s) + Lorentz (deps, f0, delta in Hz)
+    medium with eps_inf=1, a z-polarised point dipole at the centre, and three mid-plane field
+    monitors (x, y and z normals) at ``nfreq`` frequencies."""
+    n_in = n - 2 * n_pml
+    lo = -0.5 * n_in * dl
+    axes = [uniform_axis(n_in, dl, lo, "PML", n_pml) for _ in range(3)]
+    grid = Grid(*axes)
+    dt = courant_dt([a.dl for a in axes])
+    shape = grid.shape
+    coords = yee_coords(grid)
+    spheres = sphere_centres(n_sph, rmin, rmax, lo, -lo, seed) if n_sph else []
+    masks = []
+    for c in range(3):
+        x, y, z = coords[c]
+        m = np.zeros(shape, dtype=bool)
+        for cen, r in spheres:
+            ix = np.flatnonzero(np.abs(x - cen[0]) <= r)
+            iy = np.flatnonzero(np.abs(y - cen[1]) <= r)
+            iz = np.flatnonzero(np.abs(z - cen[2]) <= r)
+            if not (ix.size and iy.size and iz.size):
+                continue
+            d2 = ((x[ix, None, None] - cen[0]) ** 2 + (y[None, iy, None] - cen[1]) ** 2
+                  + (z[None, None, iz] - cen[2]) ** 2)
+            sub = m[ix[0]:ix[-1] + 1, iy[0]:iy[-1] + 1, iz[0]:iz[-1] + 1]
+            sub |= d2 <= r * r
+        masks.append(m)
+    poles, sigma = split_dc(drude_poles(wp, gamma) + lorentz_poles(*lorentz), dt)
+    am1, b = trap_coeffs(poles, dt)
+    disp = build_dispersion(masks, am1, b, shape)
+    eps = [np.ones(shape) for _ in range(3)]
+    sig = [np.where(masks[c], sigma, 0.0) for c in range(3)]
+    pulse = GaussianPulse(freq0=dip_freq0, fwidth=dip_fwidth)
+    wf = sample_waveform(pulse, dt, num_steps)
+    idx, coef = dipole_stencil(grid, 2, (0.0, 0.0, 0.0))
+    dip = PointDipole(component=2, indices=idx, coef=coef, waveform=wf)
+    fmons = []
+    if monitors:
+        freqs = np.linspace(mon_band[0], mon_band[1], nfreq)
+        h = n // 2
+        for a, name in enumerate(("mid_x", "mid_y", "mid_z")):
+            origin = [0, 0, 0]
+            box = [n, n, n]
+            origin[a] = h - 1
+            box[a] = 2
+            fmons.append(FieldMonitor(name=name, freqs=freqs, origin=tuple(origin),
+                                      box=tuple(box)))
+    return Scene(grid=grid, dt=dt, num_time_steps=num_steps, shutoff=1e-5,
+                 eps_ex=eps[0], eps_ey=eps[1], eps_ez=eps[2], pml=pml_dict(grid, dt, n_pml),
+                 sigma_ex=sig[0], sigma_ey=sig[1], sigma_ez=sig[2], dispersion=disp,
+                 dipoles=[dip], field_monitors=fmons)
+
+
+def small_dispersive(n: int = 40, n_sph: int = 4, seed: int = 0, num_steps: int = 200,
+                     n_pml: int = 8, **kw) -> Scene:
+    """A scaled-down dispersive-spheres scene for oracle parity: same media and source, a
+    smaller grid, fewer spheres, thinner CPML."""
+    n_in = n - 2 * n_pml
+    dl = 0.02 * UM
+    r_hi = min(0.6 * UM, 0.22 * n_in * dl)
+    r_lo = min(0.2 * UM, 0.5 * r_hi)
+    return dispersive_spheres(n=n, dl=dl, n_pml=n_pml, n_sph=n_sph, rmin=r_lo,
+                              rmax=r_hi, seed=seed, num_steps=num_steps, **kw)
+
+
+def with_time_monitor(sc: Scene, name: str = "tmon", comps=(0, 1, 2, 3, 4, 5), origin=None,
+                      box=None, step_begin: int = 0, step_end: int | None = None,
+                      interval: int = 5) -> Scene:
+    """Copy of ``sc`` with one field time monitor added (defaults: a small box at the grid
+    centre, every ``interval`` steps)."""
+    from dataclasses import replace
+    nx, ny, nz = sc.shape
+    if box is None:
+        box = (min(4, nx), min(4, ny), min(4, nz))
+    if origin is None:
+        origin = tuple(max(0, s // 2 - b // 2) for s, b in zip(sc.shape, box))
+    end = sc.num_time_steps if step_end is None else step_end
+    slots = (end - 1 - step_begin) // interval + 1
+    tm = FieldTimeMonitor(name=name, comps=tuple(comps), origin=tuple(origin), box=tuple(box),
+                          step_begin=step_begin, step_end=end, interval=interval,
+                          num_slots=slots)
+    return replace(sc, field_time_monitors=list(sc.field_time_monitors) + [tm])

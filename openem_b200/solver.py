@@ -1,0 +1,330 @@
+"""Drop-in replacement of OpenEM's ``solver.run`` (``openem/solver.py:403-511``).
+
+``run(sc, num_steps, use_shutoff, kernels, verbose, return_fields, policy, force_complex)``
+takes the same ``Scene`` and returns the same ``Result``. The float64 tables are built on the
+host (:mod:`openem_b200.tables`), handed to ``liboem_b200.so`` through its C ABI, and the step
+loop runs there as a captured CUDA graph; Python only decides when to stop.
+
+Physics this engine does not run yet raises ``NotImplementedError`` before anything is
+allocated, the same fail-closed behaviour as OpenEM (``openem/solver.py:1221-1260``).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from openem_b200 import flux as flux_mod
+from openem_b200 import lib as L
+from openem_b200 import shutoff as shutoff_mod
+from openem_b200 import tables as T
+from openem_b200.results import Phasors, Result
+
+SHUTOFF_INTERVAL = 400
+COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+
+
+def refuse_unsupported(sc) -> None:
+    """Fail closed on scene features outside this engine's real-field path."""
+    checks = [
+        (bool(getattr(sc, "tfsf_sources", None)), "TFSF box sources"),
+        (bool(getattr(sc, "mode_sources", None)), "mode / Gaussian-beam sources"),
+        (bool(getattr(sc, "absorbers", None)), "Absorber boundaries"),
+        (bool(getattr(sc, "flux_time_monitors", None)), "flux time monitors"),
+        (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry > 0,
+         "slanted-interface mixed dispersion"),
+        (sc.tensor is not None and sc.tensor.n_entry > 0, "fully anisotropic media"),
+        (sc.modulation is not None and sc.modulation.n_entry > 0, "time-modulated media"),
+        (any(k != 0.0 for k in sc.bloch_k), "Bloch boundaries"),
+    ]
+    for bad, what in checks:
+        if bad:
+            raise NotImplementedError(f"{what} are not supported by the sm_100a engine yet")
+
+
+class Plan:
+    """One simulation resident on the device: owns a ``oem_plan``."""
+
+    def __init__(self, sc, n_total: int | None = None, device: int = 0, stream=None,
+                 batch: int | None = None):
+        refuse_unsupported(sc)
+        self.lib = L.load()
+        self.sc = sc
+        self.n_total = int(sc.num_time_steps if n_total is None else n_total)
+        self.stream = stream
+        self.shape = tuple(int(v) for v in sc.shape)
+        nx, ny, nz = self.shape
+        self._keep = []
+        h = C.c_void_p()
+        L.check(self.lib.oem_plan_create(int(device), nx, ny, nz, float(sc.dt / T.MU_0),
+                                         float(T.EPSILON_0 / sc.dt), C.byref(h)), "plan_create")
+        self.h = h
+        self.h2d_bytes = 0
+        try:
+            self._build(batch)
+        except Exception:
+            self.close()
+            raise
+
+    # ---- construction ------------------------------------------------------------------
+    def _arr(self, a, dtype):
+        a = np.ascontiguousarray(a, dtype=dtype)
+        self._keep.append(a)
+        self.h2d_bytes += a.nbytes
+        return a
+
+    def _build(self, batch):
+        sc, lib, h = self.sc, self.lib, self.h
+        self.tabs = [T.axis_tables(sc, a) for a in range(3)]
+        for a, t in enumerate(self.tabs):
+            L.check(lib.oem_plan_set_axis(
+                h, a, L.ptr(self._arr(t.idl_p, np.float64)), L.ptr(self._arr(t.idl_d, np.float64)),
+                L.ptr(self._arr(t.nxt, np.int32)), L.ptr(self._arr(t.prv, np.int32)),
+                L.ptr(self._arr(np.real(t.mnx), np.float64)),
+                L.ptr(self._arr(np.real(t.mpv), np.float64)),
+                L.ptr(self._arr(t.pml_e, np.float64)), L.ptr(self._arr(t.pml_h, np.float64)),
+                int(t.lo), int(t.hi)), f"set_axis {a}")
+        mt = T.material_tables(sc, self.tabs)
+        self.mt = mt
+        L.check(lib.oem_plan_set_materials(h, int(mt.n_mat), L.ptr(self._arr(mt.table, np.uint32)),
+                                           int(mt.index.dtype.itemsize),
+                                           L.ptr(self._arr(mt.index, mt.index.dtype))),
+                "set_materials")
+        if mt.n_pole_total > 0:
+            L.check(lib.oem_plan_set_pole_sets(
+                h, int(mt.set_ofs.size - 1), L.ptr(self._arr(mt.set_ofs, np.int32)),
+                L.ptr(self._arr(mt.coef, np.float32)), L.ptr(self._arr(mt.seg_ofs, np.uint32)),
+                int(mt.seg_ofs.size), int(mt.n_pole_total)), "set_pole_sets")
+        for ps in T.plane_sources(sc):
+            if ps["ex"].size < self.n_total:
+                raise ValueError(f"asked to run {self.n_total} steps, but the plane-wave table "
+                                 f"holds {ps['ex'].size} samples")
+            L.check(lib.oem_plan_add_plane_source(
+                h, ps["pol"], ps["kh"], ps["ks"], ps["coef_h"], ps["coef_e"], int(ps["ex"].size),
+                L.ptr(self._arr(ps["ex"], np.float64)), L.ptr(self._arr(ps["hy"], np.float64))),
+                "add_plane_source")
+        for mag in (False, True):
+            dt_ = T.dipole_tables(sc, self.n_total, mag)
+            if dt_ is None:
+                continue
+            L.check(lib.oem_plan_add_dipoles(
+                h, int(mag), int(dt_["comp"].size), L.ptr(self._arr(dt_["ijk"], np.int32)),
+                L.ptr(self._arr(dt_["comp"], np.int32)), L.ptr(self._arr(dt_["coef"], np.float32)),
+                L.ptr(self._arr(dt_["src"], np.int32)), int(dt_["n_src"]), int(dt_["nsteps1"]),
+                L.ptr(self._arr(dt_["amp"], np.float64))), "add_dipoles")
+        nt = max(self.n_total, 1)
+        self.flux_mons = []
+        for m in sc.flux_monitors:
+            t1, t2 = [a for a in range(3) if a != m.axis]
+            n1, n2 = self.shape[t1], self.shape[t2]
+            ph = T.phase_table(m.freqs, sc.dt, nt, m.apodization)
+            Tb = batch or T.batch_depth(n1 * n2, 4)
+            mid = C.c_int()
+            L.check(lib.oem_plan_add_flux_monitor(h, int(m.axis), int(m.plane_index),
+                                                  int(np.size(m.freqs)), nt,
+                                                  L.ptr(self._arr(ph, np.float32)), int(Tb),
+                                                  C.byref(mid)), f"flux monitor {m.name}")
+            self.flux_mons.append((m, mid.value, (4, int(np.size(m.freqs)), n1, n2)))
+        self.box_mons = []
+        for m in sc.field_monitors:
+            ni, nj, nk = (int(v) for v in m.box)
+            ph = T.phase_table(m.freqs, sc.dt, nt, m.apodization)
+            Tb = batch or T.batch_depth(ni * nj * nk, 6)
+            mid = C.c_int()
+            i0, j0, k0 = (int(v) for v in m.origin)
+            L.check(lib.oem_plan_add_box_monitor(h, i0, j0, k0, ni, nj, nk,
+                                                 int(np.size(m.freqs)), nt,
+                                                 L.ptr(self._arr(ph, np.float32)), int(Tb),
+                                                 C.byref(mid)), f"field monitor {m.name}")
+            self.box_mons.append((m, mid.value, (6, int(np.size(m.freqs)), ni, nj, nk)))
+        self.time_mons = []
+        for m in sc.field_time_monitors:
+            ni, nj, nk = (int(v) for v in m.box)
+            comps = self._arr(np.asarray(m.comps, np.int32), np.int32)
+            mid = C.c_int()
+            i0, j0, k0 = (int(v) for v in m.origin)
+            L.check(lib.oem_plan_add_time_monitor(h, int(comps.size), L.ptr(comps), i0, j0, k0,
+                                                  ni, nj, nk, int(m.step_begin), int(m.step_end),
+                                                  int(m.interval), int(m.num_slots),
+                                                  C.byref(mid)), f"time monitor {m.name}")
+            self.time_mons.append((m, mid.value, (int(comps.size), int(m.num_slots), ni, nj, nk)))
+        L.check(lib.oem_plan_finalize(h, self.n_total), "finalize")
+        self._keep.clear()
+
+    # ---- stepping / readout ------------------------------------------------------------
+    @property
+    def _s(self):
+        return L.stream_handle(self.stream)
+
+    def run(self, nsteps: int) -> None:
+        L.check(self.lib.oem_plan_run(self.h, int(nsteps), self._s), "run")
+
+    def flush(self) -> None:
+        L.check(self.lib.oem_plan_flush(self.h, self._s), "flush")
+
+    @property
+    def steps(self) -> int:
+        v = C.c_int64()
+        L.check(self.lib.oem_plan_steps(self.h, C.byref(v)))
+        return int(v.value)
+
+    def read_monitor(self, mid: int, shape) -> np.ndarray:
+        re = np.empty(shape, np.float64)
+        im = np.empty(shape, np.float64)
+        L.check(self.lib.oem_plan_read_monitor(self.h, int(mid), L.ptr(re), L.ptr(im), self._s),
+                "read_monitor")
+        return re + 1j * im
+
+    def read_time_monitor(self, mid: int, shape) -> np.ndarray:
+        out = np.empty(shape, np.float32)
+        L.check(self.lib.oem_plan_read_time_monitor(self.h, int(mid), L.ptr(out), self._s),
+                "read_time_monitor")
+        return out
+
+    def read_field(self, comp: int) -> np.ndarray:
+        out = np.empty(self.shape, np.float32)
+        L.check(self.lib.oem_plan_read_field(self.h, int(comp), L.ptr(out), self._s), "read_field")
+        return out
+
+    def write_field(self, comp: int, arr) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float32)
+        if a.shape != self.shape:
+            raise ValueError(f"field shape {a.shape} != {self.shape}")
+        L.check(self.lib.oem_plan_write_field(self.h, int(comp), L.ptr(a), self._s), "write_field")
+
+    def energy(self) -> np.ndarray:
+        out = np.zeros(3, np.float64)
+        L.check(self.lib.oem_plan_energy(self.h, L.ptr(out), self._s), "energy")
+        return out
+
+    def enable_timing(self, on: bool = True) -> None:
+        L.check(self.lib.oem_plan_enable_timing(self.h, int(bool(on))))
+
+    def timing(self) -> dict:
+        names = C.create_string_buffer(32 * 16)
+        counts = np.zeros(16, np.int64)
+        ms = np.zeros(16, np.float64)
+        n = C.c_int()
+        L.check(self.lib.oem_plan_timing(self.h, 16, names, L.ptr(counts), L.ptr(ms), C.byref(n)))
+        out = {}
+        for q in range(n.value):
+            nm = names.raw[32 * q:32 * q + 32].split(b"\0", 1)[0].decode()
+            out[nm] = (int(counts[q]), float(ms[q]))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.oem_plan_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- results -----------------------------------------------------------------------
+    def flux_phasors(self) -> dict:
+        return {m.name: Phasors(name=m.name, data=self.read_monitor(mid, shp),
+                                freqs=np.asarray(m.freqs, dtype=np.float64))
+                for m, mid, shp in self.flux_mons}
+
+    def field_phasors(self) -> dict:
+        return {m.name: self.read_monitor(mid, shp) for m, mid, shp in self.box_mons}
+
+    def time_samples(self, steps_run: int):
+        samples, slots = {}, {}
+        for m, mid, shp in self.time_mons:
+            buf = self.read_time_monitor(mid, shp)
+            m_last = min(steps_run - 1, m.step_end - 1)
+            off = m_last - m.step_begin
+            filled = 0 if off < 0 else min(m.num_slots, off // m.interval + 1)
+            samples[m.name] = buf[:, :filled].copy()
+            slots[m.name] = filled
+        return samples, slots
+
+
+def _time_mon_guard(sc) -> int:
+    tm = list(sc.field_time_monitors) + list(getattr(sc, "flux_time_monitors", []))
+    return max([int(m.step_begin) + 1 for m in tm] + [0])
+
+
+def run(sc, num_steps: int | None = None, use_shutoff: bool = True, kernels=None,
+        verbose: bool = True, return_fields: bool = False, policy=None,
+        force_complex: bool = False, device: int = 0, stream=None) -> Result:
+    """Run one FDTD simulation on the GPU (signature of ``openem/solver.py:403-412``; the
+    ``kernels`` argument is accepted for call compatibility and unused)."""
+    del kernels
+    if force_complex or any(k != 0.0 for k in sc.bloch_k):
+        from openem_b200 import bloch
+        return bloch.run(sc, num_steps=num_steps, use_shutoff=use_shutoff, verbose=verbose,
+                         return_fields=return_fields, policy=policy, device=device,
+                         stream=stream)
+    n_total = int(num_steps if num_steps is not None else sc.num_time_steps)
+    plan = Plan(sc, n_total, device=device, stream=stream)
+    try:
+        return _loop(plan, sc, n_total, use_shutoff, verbose, return_fields, policy)
+    finally:
+        plan.close()
+
+
+def _loop(plan: Plan, sc, n_total: int, use_shutoff: bool, verbose: bool, return_fields: bool,
+          policy) -> Result:
+    pol = policy or shutoff_mod.default_policy(sc.shutoff, interval=SHUTOFF_INTERVAL)
+    interval = int(pol.interval)
+    source_end = shutoff_mod.source_end_step(sc)
+    guard = _time_mon_guard(sc)
+    trace = []
+    t0 = time.time()
+    steps = 0
+    triggered = False
+    if not use_shutoff:
+        plan.run(n_total)
+        steps = n_total
+    else:
+        grid = sc.grid
+        while steps < n_total:
+            chunk = min(interval - steps % interval, n_total - steps)
+            plan.run(chunk)
+            steps += chunk
+            if steps % interval:
+                continue
+            e = plan.energy()
+            m_u = 0.5 * (T.EPSILON_0 * e[1] + T.MU_0 * e[2])
+            fl = np.zeros(0)
+            if plan.flux_mons:
+                plan.flush()
+                fl = np.concatenate([flux_mod.plane_flux(plan.read_monitor(mid, shp), grid,
+                                                         axis=int(m.axis))
+                                     for m, mid, shp in plan.flux_mons])
+            stop = pol.check(steps, float(e[0]), float(m_u), fl) and steps > source_end \
+                and steps >= guard
+            trace.append((steps, pol.field_decay.ratio if pol.field_decay else float("nan")))
+            if stop:
+                triggered = True
+                if verbose:
+                    print(f"  early termination at step {steps}: {pol.reason}", flush=True)
+                break
+    plan.flush()
+    wall = time.time() - t0
+    phasors = plan.flux_phasors()
+    fphas = plan.field_phasors()
+    tsamp, tslots = plan.time_samples(steps)
+    fields = {}
+    if return_fields:
+        for c, nm in enumerate(COMPONENTS):
+            fields[nm] = plan.read_field(c)
+    for tag, d in (("mon", phasors), ("fld", fphas)):
+        for nm, obj in d.items():
+            a = np.asarray(obj.data if hasattr(obj, "data") else obj)
+            if a.size and not np.isfinite(a).all():
+                print(f"[openem_b200] warning: monitor {tag}:{nm} holds non-finite values; the "
+                      "field has most likely diverged", flush=True)
+    return Result(phasors=phasors, steps_run=steps, shutoff_triggered=triggered,
+                  decay_trace=trace,
+                  energy_trace=(pol.energy_decay.abs_history if pol.energy_decay else []),
+                  source_end=int(source_end), wall_seconds=wall,
+                  stop_reason=pol.reason, shutoff_summary=pol.summary(), fields=fields,
+                  field_phasors=fphas, time_samples=tsamp, time_slots=tslots, flux_time={})

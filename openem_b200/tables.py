@@ -1,0 +1,379 @@
+"""Host-side float64 table construction: everything the device plan needs, computed from a
+``Scene`` with numpy before upload (OpenEM computes the same quantities in
+``openem/coeffs.py``, ``openem/device_tables.py``, ``openem/sources_setup.py`` and
+``openem/monitors_setup.py``). No device code runs here, so all of it is testable on a CPU.
+
+Layout decisions (the engine's own):
+
+* **materials** -- every cell gets one index into a table of distinct tuples
+  ``(ca, cb, eps, pole set, pole count) x 3 components``; the update coefficients
+  ``ca = (eps - s)/(eps + s + G)``, ``cb = (dt/eps0)/(eps + s + G)`` are evaluated in float64 and
+  rounded once to float32. PEC cells and the tangential E cells on a PEC-backed wall get
+  ``ca = cb = 0`` (OpenEM multiplies by a PEC mask after the update instead).
+* **pole sets** -- ADE entries with identical float32 coefficient lists share one set.
+* **pole storage** -- pole states are packed in padded cell order, then component, then pole;
+  ``seg_ofs`` holds the number of poles before every 32-cell z segment.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+EPSILON_0 = 8.8541878128e-12
+MU_0 = 1.25663706212e-6
+APOD_K = 0.5
+#: one-face TF/SF correction signs by propagation direction (openem/tfsf1d.py:46)
+PLANE_SIGNS = {+1: (1.0, 1.0), -1: (-1.0, -1.0)}
+
+try:  # hash-based factorisation is O(n); numpy's unique sorts
+    import pandas as _pd
+except Exception:  # pragma: no cover
+    _pd = None
+
+
+def factorize(a: np.ndarray):
+    """Dense codes ``0..k-1`` for the distinct values of a 1D array (first-seen order with
+    pandas, sorted order with numpy) and the number of distinct values."""
+    a = np.ascontiguousarray(a).ravel()
+    if _pd is not None:
+        codes, uniq = _pd.factorize(a, sort=False)
+        return codes.astype(np.int64), len(uniq)
+    uniq, inv = np.unique(a, return_inverse=True)
+    return inv.astype(np.int64), uniq.size
+
+
+def factorize_rows(cols):
+    """Codes for the distinct rows of equal-length integer columns, and their count."""
+    code, n = factorize(cols[0])
+    for c in cols[1:]:
+        cc, m = factorize(c)
+        code, n = factorize(code * m + cc)
+    return code, n
+
+
+def pad_z(n: int) -> int:
+    return (n + 31) // 32 * 32
+
+
+def apod_window(t, spec):
+    t = np.asarray(t, dtype=np.float64)
+    w = np.ones_like(t)
+    if spec is None:
+        return w
+    start, end, width = spec
+    if start is not None:
+        m = t < start
+        w[m] = np.exp(-APOD_K * ((t[m] - start) / width) ** 2)
+    if end is not None:
+        m = t > end
+        w[m] = np.exp(-APOD_K * ((t[m] - end) / width) ** 2)
+    return w
+
+
+# ---------------------------------------------------------------------------------------------
+# Axes
+# ---------------------------------------------------------------------------------------------
+
+def pml_axis(sc, axis: int, at: str):
+    """``(a | b | 1/kappa)`` concatenated, identity outside the layers, and the layer counts at
+    the two ends (``openem/coeffs.py:21-42``)."""
+    n = sc.grid.axes[axis].n
+    a, b, k = np.zeros(n), np.ones(n), np.ones(n)
+    lo = hi = 0
+    for side in ("lo", "hi"):
+        c = sc.pml.get((axis, side))
+        if c is None:
+            continue
+        m = int(np.asarray(c.a_E).size)
+        sl = slice(0, m) if side == "lo" else slice(n - m, n)
+        a[sl] = np.asarray(getattr(c, f"a_{at}"), dtype=np.float64)
+        b[sl] = np.asarray(getattr(c, f"b_{at}"), dtype=np.float64)
+        k[sl] = np.asarray(getattr(c, f"inv_kappa_{at}"), dtype=np.float64)
+        if side == "lo":
+            lo = m
+        else:
+            hi = m
+    return np.concatenate([a, b, k]), lo, hi
+
+
+@dataclass
+class AxisTables:
+    idl_p: np.ndarray
+    idl_d: np.ndarray
+    nxt: np.ndarray
+    prv: np.ndarray
+    mnx: np.ndarray
+    mpv: np.ndarray
+    pec: np.ndarray
+    pml_e: np.ndarray
+    pml_h: np.ndarray
+    lo: int
+    hi: int
+
+
+def axis_tables(sc, axis: int, bloch_k: float = 0.0) -> AxisTables:
+    ax = sc.grid.axes[axis]
+    t = ax.index_tables(bloch_k) if bloch_k else ax.index_tables()
+    pe, lo_e, hi_e = pml_axis(sc, axis, "E")
+    ph, _, _ = pml_axis(sc, axis, "H")
+    return AxisTables(idl_p=1.0 / ax.dl, idl_d=1.0 / ax.dl_dual,
+                      nxt=np.ascontiguousarray(t["nxt"], dtype=np.int32),
+                      prv=np.ascontiguousarray(t["prv"], dtype=np.int32),
+                      mnx=np.asarray(t["mnx"]), mpv=np.asarray(t["mpv"]),
+                      pec=np.asarray(t["pec"], dtype=np.float64),
+                      pml_e=pe, pml_h=ph, lo=lo_e, hi=hi_e)
+
+
+# ---------------------------------------------------------------------------------------------
+# Materials and pole sets
+# ---------------------------------------------------------------------------------------------
+
+@dataclass
+class MaterialTables:
+    table: np.ndarray        # (n_mat, 16) uint32 records
+    index: np.ndarray        # (nx, ny, nz) uint16 or uint32
+    n_mat: int
+    set_ofs: np.ndarray      # (n_sets + 1,) int32
+    coef: np.ndarray         # (n_pole_in_sets, 4) float32
+    seg_ofs: np.ndarray      # (n_seg,) uint32
+    n_pole_total: int
+    ca: tuple                # float32 per component (for sources / checks)
+    cb: tuple
+
+
+def _g_dense(sc, shape):
+    d = sc.dispersion
+    out = [np.zeros(int(np.prod(shape))) for _ in range(3)]
+    if d is not None and d.n_entry > 0:
+        comp, cell, g = np.asarray(d.comp), np.asarray(d.cell, dtype=np.int64), np.asarray(d.g)
+        for c in range(3):
+            m = comp == c
+            out[c][cell[m]] = g[m]
+    return [o.reshape(shape) for o in out]
+
+
+def e_coefficients(sc, tabs):
+    """float32 ``(ca, cb)`` per component, PEC cells and PEC-backed wall cells zeroed."""
+    shape = sc.shape
+    gg = _g_dense(sc, shape)
+    sig = (sc.sigma_ex, sc.sigma_ey, sc.sigma_ez)
+    ca, cb = [], []
+    for c, eps in enumerate((sc.eps_ex, sc.eps_ey, sc.eps_ez)):
+        eps = np.asarray(eps, dtype=np.float64)
+        # same operation order as openem/coeffs.py:132-136: den = (eps + s) + G
+        s = (np.zeros_like(eps) if sig[c] is None
+             else np.asarray(sig[c], dtype=np.float64) * sc.dt / (2.0 * EPSILON_0))
+        den = eps + s + gg[c]
+        num = eps - s
+        ca.append((num / den).astype(np.float32))
+        cb.append(((sc.dt / EPSILON_0) / den).astype(np.float32))
+    pecs = (sc.pec_ex, sc.pec_ey, sc.pec_ez)
+    for c in range(3):
+        if pecs[c] is not None and np.asarray(pecs[c]).size:
+            idx = np.asarray(pecs[c], dtype=np.int64)
+            if idx.min() < 0 or idx.max() >= int(np.prod(shape)):
+                raise ValueError(f"pec_e{'xyz'[c]} index out of range")
+            ca[c].ravel()[idx] = 0.0
+            cb[c].ravel()[idx] = 0.0
+    # tangential E on a PEC-backed wall: component c is tangential to the walls of the two
+    # other axes (openem/kernels/yee.cu:208-211)
+    for a in range(3):
+        zero = np.flatnonzero(tabs[a].pec == 0.0)
+        if zero.size == 0:
+            continue
+        for c in range(3):
+            if c == a:
+                continue
+            sl = [slice(None)] * 3
+            sl[a] = zero
+            ca[c][tuple(sl)] = 0.0
+            cb[c][tuple(sl)] = 0.0
+    return ca, cb
+
+
+def pole_sets(sc):
+    """Deduplicate ADE entries by their float32 coefficient lists. Returns per-component dense
+    set-id arrays (-1 = none), ``set_ofs``, ``coef`` and per-set pole counts."""
+    shape = sc.shape
+    ncell = int(np.prod(shape))
+    pset = [None, None, None]
+    d = sc.dispersion
+    if d is None or d.n_entry == 0:
+        return pset, np.zeros(1, np.int32), np.zeros((0, 4), np.float32), np.zeros(0, np.int32)
+    d.validate(shape)
+    comp = np.asarray(d.comp, dtype=np.int64)
+    cell = np.asarray(d.cell, dtype=np.int64)
+    ofs = np.asarray(d.pole_ofs, dtype=np.int64)
+    npole = np.diff(ofs)
+    if npole.max() > 15:
+        raise NotImplementedError("more than 15 poles on one component")
+    am1 = np.asarray(d.am1, dtype=np.complex128)
+    b = np.asarray(d.b, dtype=np.complex128)
+    pc = np.stack([am1.real, am1.imag, b.real, b.imag], axis=1).astype(np.float32)  # (n_pole, 4)
+    set_id = np.full(d.n_entry, -1, dtype=np.int64)
+    set_ofs = [0]
+    coefs = []
+    counts = []
+    for k in np.unique(npole):
+        ent = np.flatnonzero(npole == k)
+        if k == 0:
+            continue
+        rows = pc[(ofs[ent][:, None] + np.arange(k)[None, :]).ravel()].reshape(ent.size, 4 * k)
+        bits = rows.view(np.uint32)
+        code, nu = factorize_rows([bits[:, q].astype(np.int64) for q in range(4 * k)])
+        first = np.full(nu, -1, dtype=np.int64)
+        order = np.arange(ent.size)
+        first[code[::-1]] = order[::-1]
+        base = len(counts)
+        for u in range(nu):
+            coefs.append(rows[first[u]].reshape(k, 4))
+            counts.append(int(k))
+            set_ofs.append(set_ofs[-1] + int(k))
+        set_id[ent] = base + code
+    for c in range(3):
+        arr = np.full(ncell, -1, dtype=np.int32)
+        m = comp == c
+        arr[cell[m]] = set_id[m].astype(np.int32)
+        pset[c] = arr.reshape(shape)
+    coef = np.concatenate(coefs, axis=0).astype(np.float32) if coefs else np.zeros((0, 4), np.float32)
+    return pset, np.asarray(set_ofs, dtype=np.int32), coef, np.asarray(counts, dtype=np.int32)
+
+
+def material_tables(sc, tabs) -> MaterialTables:
+    shape = sc.shape
+    nx, ny, nz = shape
+    ca, cb = e_coefficients(sc, tabs)
+    eps = [np.asarray(e, dtype=np.float32) for e in (sc.eps_ex, sc.eps_ey, sc.eps_ez)]
+    pset, set_ofs, coef, counts = pole_sets(sc)
+    # two 64-bit keys per component: (ca, cb) bit patterns and (eps, pole set)
+    keys = []
+    for c in range(3):
+        k1 = (ca[c].view(np.uint32).ravel().astype(np.uint64) << np.uint64(32)) \
+            | cb[c].view(np.uint32).ravel().astype(np.uint64)
+        keys.append(k1.view(np.int64))
+        k2 = eps[c].view(np.uint32).ravel().astype(np.uint64) << np.uint64(32)
+        if pset[c] is not None:
+            k2 |= (pset[c].ravel().astype(np.int64) + 1).astype(np.uint64)
+        keys.append(k2.view(np.int64))
+    code, n_mat = factorize_rows(keys)
+    first = np.full(n_mat, -1, dtype=np.int64)
+    idx = np.arange(code.size)
+    first[code[::-1]] = idx[::-1]
+    rec = np.zeros((n_mat, 16), dtype=np.uint32)
+    npc_mat = np.zeros(n_mat, dtype=np.int64)
+    for c in range(3):
+        rec[:, c] = ca[c].ravel()[first].view(np.uint32)
+        rec[:, 3 + c] = cb[c].ravel()[first].view(np.uint32)
+        rec[:, 6 + c] = eps[c].ravel()[first].view(np.uint32)
+        ps = pset[c].ravel()[first] if pset[c] is not None else np.full(n_mat, -1, np.int64)
+        rec[:, 9 + c] = ps.astype(np.int32).view(np.uint32)
+        npl = np.where(ps >= 0, counts[np.maximum(ps, 0)] if counts.size else 0, 0)
+        rec[:, 12 + c] = npl.astype(np.int32).view(np.uint32)
+        npc_mat += npl
+    index = code.reshape(shape).astype(np.uint16 if n_mat <= 65535 else np.uint32)
+    # poles before each 32-cell segment of the padded grid
+    nzp = pad_z(nz)
+    npc = np.zeros((nx, ny, nzp), dtype=np.int64)
+    npc[:, :, :nz] = npc_mat[code].reshape(shape)
+    seg = npc.reshape(-1, 32).sum(axis=1)
+    seg_ofs = np.concatenate([[0], np.cumsum(seg)[:-1]]) if seg.size else np.zeros(0)
+    total = int(seg.sum())
+    if total > 0xFFFFFFFF:
+        raise ValueError("more than 2^32 ADE poles")
+    return MaterialTables(table=rec, index=np.ascontiguousarray(index), n_mat=n_mat,
+                          set_ofs=set_ofs, coef=np.ascontiguousarray(coef),
+                          seg_ofs=seg_ofs.astype(np.uint32), n_pole_total=total,
+                          ca=tuple(ca), cb=tuple(cb))
+
+
+# ---------------------------------------------------------------------------------------------
+# Sources
+# ---------------------------------------------------------------------------------------------
+
+def plane_sources(sc):
+    """Plane-wave groups (one per polarisation) with the coefficients of
+    ``openem/sources_setup.py:93-119``."""
+    if not sc.sources:
+        return []
+    az = sc.grid.axes[2]
+    for s in sc.sources:
+        if s.axis != 2 or s.pol_axis not in (0, 1):
+            raise NotImplementedError("plane waves: propagation along z with Ex/Ey polarisation only")
+        if getattr(s, "angle_theta", 0.0):
+            raise NotImplementedError("oblique plane waves need the Bloch path")
+    keys = {(int(s.plane_index), int(s.direction)) for s in sc.sources}
+    if len(keys) != 1:
+        raise NotImplementedError("plane-wave sources must share one plane and one direction")
+    groups = {}
+    for s in sc.sources:
+        groups.setdefault(int(s.pol_axis), []).append(s)
+    out = []
+    for pol, grp in sorted(groups.items()):
+        s0 = grp[0]
+        ks = int(s0.plane_index)
+        kh = ks - 1 if s0.direction > 0 else ks
+        sh, se = PLANE_SIGNS[int(s0.direction)]
+        sp = -1.0 if pol == 1 else 1.0
+        out.append({
+            "pol": pol, "kh": kh, "ks": ks,
+            "coef_h": float(np.float32(sp * sh * sc.dt / MU_0 * float(1.0 / az.dl[kh]))),
+            "coef_e": float(np.float32(se * float(1.0 / az.dl_dual[ks]))),
+            "ex": np.ascontiguousarray(sum(np.asarray(x.ex_inc, np.float64) for x in grp)),
+            "hy": np.ascontiguousarray(sum(np.asarray(x.hy_inc, np.float64) for x in grp)),
+        })
+    return out
+
+
+def dipole_tables(sc, n_total: int, magnetic: bool):
+    dips = [d for d in sc.dipoles if bool(d.magnetic) == magnetic]
+    if not dips:
+        return None
+    tabs = [np.asarray(d.waveform.amp_int if magnetic else d.waveform.amp_half, np.float64)
+            for d in dips]
+    nsteps1 = min(t.size for t in tabs)
+    if n_total > nsteps1 - 1:
+        raise ValueError(f"asked to run {n_total} steps, but the dipole waveform only sampled "
+                         f"{nsteps1} points")
+    ijk, comp, coef, src = [], [], [], []
+    for s, d in enumerate(dips):
+        ind = np.asarray(d.indices, dtype=np.int64).reshape(-1, 3)
+        cf = np.asarray(d.coef, dtype=np.float64).ravel()
+        ijk.append(ind)
+        comp.append(np.full(len(ind), int(d.component), np.int32))
+        coef.append(cf.astype(np.float32))
+        src.append(np.full(len(ind), s, np.int32))
+    return {"ijk": np.ascontiguousarray(np.concatenate(ijk).astype(np.int32)),
+            "comp": np.concatenate(comp), "coef": np.concatenate(coef), "src": np.concatenate(src),
+            "n_src": len(dips), "nsteps1": nsteps1,
+            "amp": np.ascontiguousarray(np.stack([t[:nsteps1] for t in tabs]))}
+
+
+# ---------------------------------------------------------------------------------------------
+# Monitors
+# ---------------------------------------------------------------------------------------------
+
+def phase_table(freqs, dt: float, n_total: int, apod=None) -> np.ndarray:
+    """(n_total, nf, 4) float32: cos/sin of 2 pi f t at E time (n+1) dt and H time (n+1/2) dt,
+    each multiplied by its apodisation window (openem/kernels/source_dft.cu:332-362)."""
+    f = np.asarray(freqs, dtype=np.float64)
+    n = np.arange(n_total, dtype=np.float64)
+    te, th = (n + 1.0) * dt, (n + 0.5) * dt
+    we, wh = apod_window(te, apod), apod_window(th, apod)
+    ae = 2.0 * np.pi * f[None, :] * te[:, None]
+    ah = 2.0 * np.pi * f[None, :] * th[:, None]
+    out = np.empty((n_total, f.size, 4), dtype=np.float32)
+    out[..., 0] = np.cos(ae) * we[:, None]
+    out[..., 1] = np.sin(ae) * we[:, None]
+    out[..., 2] = np.cos(ah) * wh[:, None]
+    out[..., 3] = np.sin(ah) * wh[:, None]
+    return out
+
+
+def batch_depth(points: int, ncomp: int, cap: int = 32, ring_bytes: float = 2e9) -> int:
+    """Snapshot ring depth: up to 32 steps, halved while the ring would exceed ``ring_bytes``."""
+    T = cap
+    while T > 1 and T * ncomp * 4 * points > ring_bytes:
+        T //= 2
+    return max(T, 1)

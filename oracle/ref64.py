@@ -1,0 +1,492 @@
+"""FP64 NumPy transcription of OpenEM's solver step loop -- TEST INFRASTRUCTURE ONLY.
+
+This module is the oracle the CUDA engine is checked against, and the CPU baseline that
+``bench.py`` times. Nothing in the product path imports it. It restates, in float64 and in the
+launch order of ``openem/solver.py:1145-1162``, the update equations of the reference kernels:
+
+* ``update_h`` with the CPML psi recursion ``stretch`` -- ``openem/kernels/yee.cu:60-137``;
+* ``update_e`` (semi-implicit sigma, dispersion history, PEC masks) -- ``yee.cu:139-240``;
+* ``dispersion_pre`` / ``dispersion_post`` -- ``openem/kernels/dispersion.cu:60-158``;
+* plane-wave TF/SF injection ``inject_h`` / ``inject_e`` -- ``openem/kernels/source_dft.cu:39-73``
+  with the coefficients of ``openem/sources_setup.py:93-119``;
+* point dipoles ``inject_dipole(_h)`` -- ``source_dft.cu:135-206``, tables
+  ``openem/sources_setup.py:419-457``;
+* DFT accumulation of flux planes and field boxes -- ``source_dft.cu:208-430`` (E at
+  ``(n+1) dt``, H at ``(n+1/2) dt``, H colocated ``(H[k] + H[k-1]) / 2`` on a flux plane,
+  apodisation window ``openem/apodization.py:27-45``);
+* field time monitors with the two-shot H average -- ``source_dft.cu:273-319``,
+  ``openem/readout.py:184-197``;
+* the complex Bloch path -- ``openem/kernels/bloch.cu:25-221`` and ``openem/solver.py:1263-1483``.
+
+Coefficient tables follow ``openem/coeffs.py:21-136`` (CPML axis arrays filled with the identity
+outside the layers; ``ca = (eps - s)/(eps + s + G)``, ``cb = (dt/eps0)/(eps + s + G)``) and the
+index tables of ``openem/grid.py:219-304``.
+
+The only inputs are the attributes of a ``Scene`` (OpenEM's own class or the engine's mirror).
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+EPSILON_0 = 8.8541878128e-12
+MU_0 = 1.25663706212e-6
+APOD_K = 0.5
+# +z and -z one-face TF/SF correction signs (openem/tfsf1d.py:46)
+_SIGNS = {+1: (1.0, 1.0), -1: (-1.0, -1.0)}
+
+
+def apod_window(t, spec):
+    t = np.asarray(t, dtype=np.float64)
+    w = np.ones_like(t)
+    if spec is None:
+        return w
+    start, end, width = spec
+    if start is not None:
+        m = t < start
+        w[m] = np.exp(-APOD_K * ((t[m] - start) / width) ** 2)
+    if end is not None:
+        m = t > end
+        w[m] = np.exp(-APOD_K * ((t[m] - end) / width) ** 2)
+    return w
+
+
+def pml_axis_arrays(sc, axis: int, at: str):
+    """``(a, b, 1/kappa)`` along one axis, identity ``(0, 1, 1)`` outside the layers."""
+    n = sc.grid.axes[axis].n
+    a, b, k = np.zeros(n), np.ones(n), np.ones(n)
+    for side in ("lo", "hi"):
+        c = sc.pml.get((axis, side))
+        if c is None:
+            continue
+        m = int(np.asarray(c.a_E).size)
+        sl = slice(0, m) if side == "lo" else slice(n - m, n)
+        a[sl] = np.asarray(getattr(c, f"a_{at}"))
+        b[sl] = np.asarray(getattr(c, f"b_{at}"))
+        k[sl] = np.asarray(getattr(c, f"inv_kappa_{at}"))
+    return a, b, k
+
+
+def e_coeffs(sc):
+    """``(ca, cb)`` per component in float64, PEC cells zeroed."""
+    shape = sc.shape
+    if sc.dispersion is not None and sc.dispersion.n_entry > 0:
+        gg = _g_dense(sc.dispersion, shape)
+    else:
+        gg = (np.zeros(shape),) * 3
+    ca, cb = [], []
+    sig = (sc.sigma_ex, sc.sigma_ey, sc.sigma_ez)
+    for c, eps in enumerate((sc.eps_ex, sc.eps_ey, sc.eps_ez)):
+        eps = np.asarray(eps, dtype=np.float64)
+        s = (np.zeros_like(eps) if sig[c] is None
+             else np.asarray(sig[c], dtype=np.float64) * sc.dt / (2.0 * EPSILON_0))
+        den = eps + s + gg[c]
+        ca.append((eps - s) / den)
+        cb.append((sc.dt / EPSILON_0) / den)
+    pecs = (sc.pec_ex, sc.pec_ey, sc.pec_ez)
+    for c in range(3):
+        if pecs[c] is not None and np.asarray(pecs[c]).size:
+            idx = np.asarray(pecs[c], dtype=np.int64)
+            ca[c].ravel()[idx] = 0.0
+            cb[c].ravel()[idx] = 0.0
+    return ca, cb
+
+
+def _g_dense(d, shape):
+    out = [np.zeros(int(np.prod(shape))) for _ in range(3)]
+    comp, cell, g = np.asarray(d.comp), np.asarray(d.cell), np.asarray(d.g)
+    for c in range(3):
+        m = comp == c
+        out[c][cell[m]] = g[m]
+    return tuple(o.reshape(shape) for o in out)
+
+
+@dataclass
+class OracleResult:
+    phasors: dict = field(default_factory=dict)          # name -> (4, nf, n1, n2) complex
+    field_phasors: dict = field(default_factory=dict)    # name -> (6, nf, ni, nj, nk) complex
+    time_samples: dict = field(default_factory=dict)
+    time_slots: dict = field(default_factory=dict)
+    fields: dict = field(default_factory=dict)
+    steps_run: int = 0
+    seconds: float = 0.0
+
+
+class Oracle:
+    """Float64 state of one real-path run. ``step()`` advances one full time step."""
+
+    def __init__(self, sc, n_total: int | None = None):
+        if sc.any_bloch:
+            raise ValueError("use BlochOracle for a scene with a non-zero Bloch vector")
+        for feat in ("tfsf_sources", "mode_sources", "absorbers", "flux_time_monitors"):
+            if getattr(sc, feat, None):
+                raise NotImplementedError(f"oracle: {feat} not transcribed")
+        if sc.any_dispersion_mix or sc.any_tensor or sc.any_modulation:
+            raise NotImplementedError("oracle: mix / tensor / modulation not transcribed")
+        self.sc = sc
+        self.n_total = int(n_total if n_total is not None else sc.num_time_steps)
+        nx, ny, nz = self.shape = sc.shape
+        self.E = [np.zeros(self.shape) for _ in range(3)]
+        self.H = [np.zeros(self.shape) for _ in range(3)]
+        # psi slots in the reference order: hx_y hx_z hy_z hy_x hz_x hz_y (same on E)
+        self.psi_h = [np.zeros(self.shape) for _ in range(6)]
+        self.psi_e = [np.zeros(self.shape) for _ in range(6)]
+        tabs = [a.index_tables() for a in sc.grid.axes]
+        self.nxt = [t["nxt"] for t in tabs]
+        self.prv = [t["prv"] for t in tabs]
+        self.mnx = [np.asarray(t["mnx"], dtype=np.float64) for t in tabs]
+        self.mpv = [np.asarray(t["mpv"], dtype=np.float64) for t in tabs]
+        self.pec = [t["pec"] for t in tabs]
+        self.idl_p = [1.0 / a.dl for a in sc.grid.axes]
+        self.idl_d = [1.0 / a.dl_dual for a in sc.grid.axes]
+        self.pml_e = [pml_axis_arrays(sc, a, "E") for a in range(3)]
+        self.pml_h = [pml_axis_arrays(sc, a, "H") for a in range(3)]
+        self.ch = sc.dt / MU_0
+        self.cw = EPSILON_0 / sc.dt
+        self.ca, self.cb = e_coeffs(sc)
+        self.hist = [np.zeros(self.shape) for _ in range(3)]
+        self._setup_dispersion()
+        self._setup_sources()
+        self._setup_monitors()
+        self.n = 0
+
+    # ---- setup --------------------------------------------------------------------------
+    def _setup_dispersion(self):
+        d = self.sc.dispersion
+        self.disp = None
+        if d is None or d.n_entry == 0:
+            return
+        d.validate(self.shape)
+        ofs = np.asarray(d.pole_ofs, dtype=np.int64)
+        npole = np.diff(ofs)
+        ent = np.repeat(np.arange(d.n_entry), npole)
+        self.disp = {
+            "comp": np.asarray(d.comp, dtype=np.int64),
+            "cell": np.asarray(d.cell, dtype=np.int64),
+            "ent": ent,
+            "am1": np.asarray(d.am1, dtype=np.complex128),
+            "b": np.asarray(d.b, dtype=np.complex128),
+            "P": np.zeros(int(ofs[-1]), dtype=np.complex128),
+        }
+
+    def _entry_field(self, F):
+        d = self.disp
+        out = np.empty(d["comp"].size)
+        for c in range(3):
+            m = d["comp"] == c
+            out[m] = F[c].ravel()[d["cell"][m]]
+        return out
+
+    def _setup_sources(self):
+        sc = self.sc
+        az = sc.grid.axes[2]
+        self.pw = []
+        groups = {}
+        for s in sc.sources:
+            if s.axis != 2 or s.pol_axis not in (0, 1):
+                raise NotImplementedError("plane waves: z propagation, Ex/Ey polarisation only")
+            groups.setdefault(int(s.pol_axis), []).append(s)
+        for pol, grp in sorted(groups.items()):
+            s0 = grp[0]
+            ks = int(s0.plane_index)
+            kh = ks - 1 if s0.direction > 0 else ks
+            sh, se = _SIGNS[int(s0.direction)]
+            sp = -1.0 if pol == 1 else 1.0
+            self.pw.append({
+                "pol": pol, "ks": ks, "kh": kh,
+                "coef_h": sp * sh * sc.dt / MU_0 / float(az.dl[kh]),
+                "coef_e": se / float(az.dl_dual[ks]),
+                "ex": sum(np.asarray(x.ex_inc, dtype=np.float64) for x in grp),
+                "hy": sum(np.asarray(x.hy_inc, dtype=np.float64) for x in grp)})
+        self.dip_e = self._dipole_table([d for d in sc.dipoles if not d.magnetic], half=True)
+        self.dip_h = self._dipole_table([d for d in sc.dipoles if d.magnetic], half=False)
+
+    def _dipole_table(self, dips, half: bool):
+        if not dips:
+            return None
+        tabs = [np.asarray(d.waveform.amp_half if half else d.waveform.amp_int,
+                           dtype=np.float64) for d in dips]
+        nsteps1 = min(t.size for t in tabs)
+        if self.n_total > nsteps1 - 1:
+            raise ValueError(f"asked to run {self.n_total} steps, dipole waveform has "
+                             f"{nsteps1} samples")
+        pts = []
+        for s, d in enumerate(dips):
+            for (i, j, k), cf in zip(np.asarray(d.indices), np.asarray(d.coef)):
+                pts.append((int(d.component), int(i), int(j), int(k), float(cf), s))
+        return {"pts": pts, "amp": np.stack([t[:nsteps1] for t in tabs])}
+
+    def _setup_monitors(self):
+        sc = self.sc
+        nt = self.n_total
+        te = (np.arange(nt, dtype=np.float64) + 1.0) * sc.dt
+        th = (np.arange(nt, dtype=np.float64) + 0.5) * sc.dt
+        self.t_e, self.t_h = te, th
+        nx, ny, nz = self.shape
+        self.fmon = []
+        for m in sc.flux_monitors:
+            f = np.asarray(m.freqs, dtype=np.float64)
+            t1, t2 = [a for a in range(3) if a != m.axis]
+            n1, n2 = self.shape[t1], self.shape[t2]
+            self.fmon.append({"m": m, "f": f, "t1": t1, "t2": t2,
+                              "we": apod_window(te, m.apodization),
+                              "wh": apod_window(th, m.apodization),
+                              "acc": np.zeros((4, f.size, n1, n2), dtype=np.complex128)})
+        self.bmon = []
+        for m in sc.field_monitors:
+            f = np.asarray(m.freqs, dtype=np.float64)
+            (i0, j0, k0), (ni, nj, nk) = m.origin, m.box
+            self.bmon.append({"m": m, "f": f,
+                              "sl": (slice(i0, i0 + ni), slice(j0, j0 + nj), slice(k0, k0 + nk)),
+                              "we": apod_window(te, m.apodization),
+                              "wh": apod_window(th, m.apodization),
+                              "acc": np.zeros((6, f.size, ni, nj, nk), dtype=np.complex128)})
+        self.tmon = []
+        for m in sc.field_time_monitors:
+            (i0, j0, k0), (ni, nj, nk) = m.origin, m.box
+            self.tmon.append({"m": m, "sl": (slice(i0, i0 + ni), slice(j0, j0 + nj),
+                                             slice(k0, k0 + nk)),
+                              "buf": np.zeros((len(m.comps), m.num_slots, ni, nj, nk))})
+        # t = 0 sample, taken before the loop on zero fields (openem/solver.py:492-495)
+        self._sample_time(0)
+
+    # ---- one step -------------------------------------------------------------------------
+    @staticmethod
+    def _take(F, idx, axis):
+        return np.take(F, idx, axis=axis)
+
+    def _stretch(self, psi, d, coef, axis):
+        a, b, k = coef[axis]
+        sh = [1, 1, 1]
+        sh[axis] = -1
+        a, b, k = a.reshape(sh), b.reshape(sh), k.reshape(sh)
+        psi *= b
+        psi += a * d
+        return k * d + psi
+
+    def _bc(self, v, axis):
+        sh = [1, 1, 1]
+        sh[axis] = -1
+        return np.asarray(v).reshape(sh)
+
+    def update_h(self):
+        Ex, Ey, Ez = self.E
+        Hx, Hy, Hz = self.H
+        nxt, mnx, idl = self.nxt, self.mnx, self.idl_p
+        ph, pml = self.psi_h, self.pml_h
+        fwd = lambda F, a: (self._take(F, nxt[a], a) * self._bc(mnx[a], a) - F) * self._bc(idl[a], a)
+        # Hx: -(dEz/dy - dEy/dz)
+        sy = self._stretch(ph[0], fwd(Ez, 1), pml, 1)
+        sz = self._stretch(ph[1], fwd(Ey, 2), pml, 2)
+        dHx = sy - sz
+        sz2 = self._stretch(ph[2], fwd(Ex, 2), pml, 2)
+        sx2 = self._stretch(ph[3], fwd(Ez, 0), pml, 0)
+        dHy = sz2 - sx2
+        sx3 = self._stretch(ph[4], fwd(Ey, 0), pml, 0)
+        sy3 = self._stretch(ph[5], fwd(Ex, 1), pml, 1)
+        dHz = sx3 - sy3
+        Hx -= self.ch * dHx
+        Hy -= self.ch * dHy
+        Hz -= self.ch * dHz
+
+    def inject_h(self, n):
+        for p in self.pw:
+            Ht = self.H[1] if p["pol"] == 0 else self.H[0]
+            Ht[:, :, p["kh"]] += p["coef_h"] * p["ex"][n]
+        if self.dip_h is not None:
+            for c, i, j, k, cf, s in self.dip_h["pts"]:
+                self.H[c][i, j, k] -= self.ch * cf * self.dip_h["amp"][s, n]
+
+    def disp_pre(self):
+        d = self.disp
+        if d is None:
+            return
+        en = self._entry_field(self.E)[d["ent"]]
+        dP = d["am1"] * d["P"] + d["b"] * en
+        d["P"] += dP
+        w = np.zeros(d["comp"].size)
+        np.add.at(w, d["ent"], 2.0 * dP.real)
+        for c in range(3):
+            m = d["comp"] == c
+            self.hist[c].ravel()[d["cell"][m]] = w[m]
+
+    def disp_post(self):
+        d = self.disp
+        if d is None:
+            return
+        en = self._entry_field(self.E)[d["ent"]]
+        d["P"] += d["b"] * en
+
+    def update_e(self):
+        Ex, Ey, Ez = self.E
+        Hx, Hy, Hz = self.H
+        prv, mpv, idl = self.prv, self.mpv, self.idl_d
+        pe, pml = self.psi_e, self.pml_e
+        bwd = lambda F, a: (F - self._take(F, prv[a], a) * self._bc(mpv[a], a)) * self._bc(idl[a], a)
+        px, py, pz = (self._bc(self.pec[a], a) for a in range(3))
+        sy = self._stretch(pe[0], bwd(Hz, 1), pml, 1)
+        sz = self._stretch(pe[1], bwd(Hy, 2), pml, 2)
+        cx = sy - sz
+        sz2 = self._stretch(pe[2], bwd(Hx, 2), pml, 2)
+        sx2 = self._stretch(pe[3], bwd(Hz, 0), pml, 0)
+        cy = sz2 - sx2
+        sx3 = self._stretch(pe[4], bwd(Hy, 0), pml, 0)
+        sy3 = self._stretch(pe[5], bwd(Hx, 1), pml, 1)
+        cz = sx3 - sy3
+        ca, cb, cw, hs = self.ca, self.cb, self.cw, self.hist
+        self.E[0] = (ca[0] * Ex + cb[0] * (cx - cw * hs[0])) * py * pz
+        self.E[1] = (ca[1] * Ey + cb[1] * (cy - cw * hs[1])) * pz * px
+        self.E[2] = (ca[2] * Ez + cb[2] * (cz - cw * hs[2])) * px * py
+
+    def inject_e(self, n):
+        for p in self.pw:
+            c = p["pol"]
+            self.E[c][:, :, p["ks"]] += self.cb[c][:, :, p["ks"]] * p["coef_e"] * p["hy"][n]
+        if self.dip_e is not None:
+            for c, i, j, k, cf, s in self.dip_e["pts"]:
+                self.E[c][i, j, k] -= self.cb[c][i, j, k] * cf * self.dip_e["amp"][s, n]
+
+    def dft(self, n):
+        for mon in self.fmon:
+            m, f = mon["m"], mon["f"]
+            km, ax, t1, t2 = int(m.plane_index), int(m.axis), mon["t1"], mon["t2"]
+            take = lambda F, k: np.take(F, k, axis=ax)
+            vals = (take(self.E[t1], km), take(self.E[t2], km),
+                    0.5 * (take(self.H[t1], km) + take(self.H[t1], km - 1)),
+                    0.5 * (take(self.H[t2], km) + take(self.H[t2], km - 1)))
+            pe = np.exp(2j * np.pi * f * self.t_e[n]) * mon["we"][n]
+            ph = np.exp(2j * np.pi * f * self.t_h[n]) * mon["wh"][n]
+            acc = mon["acc"]
+            for c in range(4):
+                acc[c] += (pe if c < 2 else ph)[:, None, None] * vals[c][None]
+        for mon in self.bmon:
+            f, sl = mon["f"], mon["sl"]
+            pe = np.exp(2j * np.pi * f * self.t_e[n]) * mon["we"][n]
+            ph = np.exp(2j * np.pi * f * self.t_h[n]) * mon["wh"][n]
+            acc = mon["acc"]
+            for c in range(6):
+                F = self.E[c] if c < 3 else self.H[c - 3]
+                acc[c] += (pe if c < 3 else ph)[:, None, None, None] * F[sl][None]
+
+    def _sample_time(self, m_step):
+        """Two-shot H average at m = m_step: E^m + H^{m-1/2}/2 now, H^{m+1/2}/2 one step later."""
+        for tm in self.tmon:
+            m = tm["m"]
+            for add in (1, 0):
+                m_ref = m_step - add
+                if add and m_step == 0:
+                    continue
+                off = m_ref - m.step_begin
+                if off < 0 or m_ref >= m.step_end or off % m.interval:
+                    continue
+                slot = off // m.interval
+                if slot >= m.num_slots:
+                    continue
+                for q, c in enumerate(m.comps):
+                    F = self.E[c] if c < 3 else self.H[c - 3]
+                    w = (1.0 if c < 3 else 0.5) if not add else (0.0 if c < 3 else 0.5)
+                    if w == 0.0:
+                        continue
+                    v = w * F[tm["sl"]]
+                    if add:
+                        tm["buf"][q, slot] += v
+                    else:
+                        tm["buf"][q, slot] = v
+
+    def step(self):
+        n = self.n
+        self.update_h()
+        self.inject_h(n)
+        self.disp_pre()
+        self.update_e()
+        self.inject_e(n)
+        self.disp_post()
+        self._sample_time(n + 1)
+        self.dft(n)
+        self.n += 1
+
+    def run(self, n_steps: int | None = None) -> OracleResult:
+        n_steps = self.n_total if n_steps is None else int(n_steps)
+        t0 = time.perf_counter()
+        for _ in range(n_steps):
+            self.step()
+        return self.result(time.perf_counter() - t0)
+
+    def result(self, seconds: float = 0.0) -> OracleResult:
+        r = OracleResult(steps_run=self.n, seconds=seconds)
+        for mon in self.fmon:
+            r.phasors[mon["m"].name] = mon["acc"].copy()
+        for mon in self.bmon:
+            r.field_phasors[mon["m"].name] = mon["acc"].copy()
+        for tm in self.tmon:
+            m = tm["m"]
+            m_last = min(self.n - 1, m.step_end - 1)
+            off = m_last - m.step_begin
+            filled = 0 if off < 0 else min(m.num_slots, off // m.interval + 1)
+            r.time_samples[m.name] = tm["buf"][:, :filled].copy()
+            r.time_slots[m.name] = filled
+        names = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+        for nm, F in zip(names, (*self.E, *self.H)):
+            r.fields[nm] = F.copy()
+        return r
+
+
+def run(sc, num_steps: int | None = None) -> OracleResult:
+    """Run ``num_steps`` (default: the scene's nominal count) on the FP64 oracle."""
+    if sc.any_bloch:
+        return BlochOracle(sc, num_steps).run()
+    return Oracle(sc, num_steps).run()
+
+
+class BlochOracle(Oracle):
+    """Complex-field Bloch path (``openem/kernels/bloch.cu:25-221``): fields carry re + i im,
+    the periodic seam neighbour is multiplied by ``exp(+/- i 2 pi k)``; the scene subset is
+    lossless and non-dispersive with plane sources excluded (``openem/solver.py:1221-1260``)."""
+
+    def __init__(self, sc, n_total: int | None = None):
+        if sc.any_dispersion or sc.any_loss or sc.any_pec or sc.sources or sc.tfsf_sources:
+            raise NotImplementedError("Bloch subset: lossless, non-dispersive, no plane wave")
+        self.sc = sc
+        self.n_total = int(n_total if n_total is not None else sc.num_time_steps)
+        self.shape = sc.shape
+        self.E = [np.zeros(self.shape, dtype=np.complex128) for _ in range(3)]
+        self.H = [np.zeros(self.shape, dtype=np.complex128) for _ in range(3)]
+        self.psi_h = [np.zeros(self.shape, dtype=np.complex128) for _ in range(6)]
+        self.psi_e = [np.zeros(self.shape, dtype=np.complex128) for _ in range(6)]
+        tabs = [a.index_tables(k) for a, k in zip(sc.grid.axes, sc.bloch_k)]
+        self.nxt = [t["nxt"] for t in tabs]
+        self.prv = [t["prv"] for t in tabs]
+        self.mnx = [np.asarray(t["mnx"], dtype=np.complex128) for t in tabs]
+        self.mpv = [np.asarray(t["mpv"], dtype=np.complex128) for t in tabs]
+        self.pec = [t["pec"] for t in tabs]
+        self.idl_p = [1.0 / a.dl for a in sc.grid.axes]
+        self.idl_d = [1.0 / a.dl_dual for a in sc.grid.axes]
+        self.pml_e = [pml_axis_arrays(sc, a, "E") for a in range(3)]
+        self.pml_h = [pml_axis_arrays(sc, a, "H") for a in range(3)]
+        self.ch = sc.dt / MU_0
+        self.cw = EPSILON_0 / sc.dt
+        self.ca = [np.ones(self.shape) for _ in range(3)]
+        self.cb = [(sc.dt / EPSILON_0) / np.asarray(e, dtype=np.float64)
+                   for e in (sc.eps_ex, sc.eps_ey, sc.eps_ez)]
+        self.hist = [np.zeros(self.shape) for _ in range(3)]
+        self.disp = None
+        self.pw = []
+        self.dip_e = self._dipole_table_c([d for d in sc.dipoles if not d.magnetic], True)
+        self.dip_h = self._dipole_table_c([d for d in sc.dipoles if d.magnetic], False)
+        self._setup_monitors()
+        self.n = 0
+
+    def _dipole_table_c(self, dips, half: bool):
+        if not dips:
+            return None
+        tabs = [np.asarray(d.waveform.amp_half_complex if half else d.waveform.amp_int_complex,
+                           dtype=np.complex128) for d in dips]
+        n1 = min(t.size for t in tabs)
+        pts = []
+        for s, d in enumerate(dips):
+            for (i, j, k), cf in zip(np.asarray(d.indices), np.asarray(d.coef)):
+                pts.append((int(d.component), int(i), int(j), int(k), float(cf), s))
+        return {"pts": pts, "amp": np.stack([t[:n1] for t in tabs])}

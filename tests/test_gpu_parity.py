@@ -1,0 +1,112 @@
+"""CUDA engine against the FP64 oracle on the same seeded scenes.
+
+Tolerances (fp32 fields against float64 arithmetic): final fields within 1e-5 relative L2 on
+the plane-wave slab and 2e-5 on the Drude+Lorentz scene, DFT phasors within 1e-4 relative L2,
+slab transmission within 1e-4 absolute.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import ref64
+from openem_b200 import scenes, solver
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def flux(ph):
+    return 0.5 * (np.real(ph[0] * np.conj(ph[3])).sum(axis=(1, 2))
+                  - np.real(ph[1] * np.conj(ph[2])).sum(axis=(1, 2)))
+
+
+@pytest.fixture(scope="module")
+def slab_runs():
+    sc = scenes.slab_plane_wave(nxy=1)
+    sc0 = scenes.slab_plane_wave(nxy=1, with_slab=False)
+    return {"sc": sc, "sc0": sc0, "ref": ref64.run(sc), "ref0": ref64.run(sc0),
+            "gpu": solver.run(sc, use_shutoff=False, return_fields=True, verbose=False),
+            "gpu0": solver.run(sc0, use_shutoff=False, verbose=False)}
+
+
+def test_slab_phasors_match_oracle(slab_runs):
+    r, g = slab_runs["ref"], slab_runs["gpu"]
+    for name in ("T", "R"):
+        assert rel_l2(g.phasors[name].data, r.phasors[name]) < 1e-4, name
+
+
+def test_slab_fields_match_oracle(slab_runs):
+    """Fields while the pulse is inside the cell (after 2000 steps); at the end of the full run
+    the pulse has left and only an fp32 round-off floor remains."""
+    sc = slab_runs["sc"]
+    r = ref64.run(sc, 2000)
+    g = solver.run(sc, num_steps=2000, use_shutoff=False, return_fields=True, verbose=False)
+    for nm in ("Ex", "Hy"):
+        assert rel_l2(g.fields[nm], r.fields[nm]) < 1e-5, nm
+
+
+def test_slab_transmission_and_energy_balance(slab_runs):
+    g, g0, r, r0 = (slab_runs[k] for k in ("gpu", "gpu0", "ref", "ref0"))
+    T_g = flux(g.phasors["T"].data) / flux(g0.phasors["T"].data)
+    R_g = -flux(g.phasors["R"].data) / flux(g0.phasors["T"].data)
+    T_r = flux(r.phasors["T"]) / flux(r0.phasors["T"])
+    assert np.max(np.abs(T_g - T_r)) < 1e-4
+    # OpenEM prints transmission = 0.8310044973694679 at f0 for this slab (README.md:62)
+    assert abs(T_g[5] - 0.8310044973694679) < 2e-5
+    assert np.all(np.abs(T_g + R_g - 1.0) < 2e-4)
+
+
+def test_wide_periodic_cell_equals_narrow(slab_runs):
+    """At normal incidence the 30x30 periodic cell carries the 1x1 solution in every column."""
+    sc = scenes.slab_plane_wave(nxy=30, num_steps=2000)
+    g = solver.run(sc, use_shutoff=False, verbose=False)
+    sc1 = scenes.slab_plane_wave(nxy=1, num_steps=2000)
+    g1 = solver.run(sc1, use_shutoff=False, verbose=False)
+    d = g.phasors["T"].data
+    assert d.shape == (4, 11, 30, 30)
+    np.testing.assert_allclose(d, np.broadcast_to(g1.phasors["T"].data, d.shape), rtol=1e-6,
+                               atol=1e-12 * np.abs(d).max())
+
+
+@pytest.fixture(scope="module")
+def disp_runs():
+    sc = scenes.with_time_monitor(
+        scenes.small_dispersive(n=32, n_sph=4, num_steps=300, n_pml=8, nfreq=4), interval=7)
+    return {"sc": sc, "ref": ref64.run(sc),
+            "gpu": solver.run(sc, use_shutoff=False, return_fields=True, verbose=False)}
+
+
+def test_dispersive_fields_match_oracle(disp_runs):
+    r, g = disp_runs["ref"], disp_runs["gpu"]
+    for nm in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        assert rel_l2(g.fields[nm], r.fields[nm]) < 2e-5, nm
+
+
+def test_dispersive_field_monitors_match_oracle(disp_runs):
+    r, g = disp_runs["ref"], disp_runs["gpu"]
+    for name, data in r.field_phasors.items():
+        assert g.field_phasors[name].shape == data.shape
+        assert rel_l2(g.field_phasors[name], data) < 1e-4, name
+
+
+def test_time_monitor_matches_oracle(disp_runs):
+    r, g = disp_runs["ref"], disp_runs["gpu"]
+    assert g.time_slots == r.time_slots
+    for name, data in r.time_samples.items():
+        assert rel_l2(g.time_samples[name], data) < 2e-5, name
+
+
+def test_dispersion_changes_the_result(disp_runs):
+    """The ADE is really active: dropping the poles (and the Drude conductivity) moves the
+    fields by far more than the tolerance."""
+    from dataclasses import replace
+    sc = disp_runs["sc"]
+    g = disp_runs["gpu"]
+    plain = replace(sc, dispersion=None, sigma_ex=None, sigma_ey=None, sigma_ez=None)
+    gp = solver.run(plain, use_shutoff=False, return_fields=True, verbose=False)
+    assert rel_l2(gp.fields["Ez"], g.fields["Ez"]) > 1e-2
