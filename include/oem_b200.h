@@ -69,6 +69,11 @@ int oem_plan_set_axis(oem_plan* p, int axis, const double* idl_p, const double* 
 int oem_plan_set_materials(oem_plan* p, int n_mat, const uint32_t* table, int index_bytes,
                            const void* index);
 
+/* Same as oem_plan_set_materials, with the per-cell index already in device memory
+ * (unpadded (nx, ny, nz) C order, index_bytes each). The plan copies it. */
+int oem_plan_set_materials_device(oem_plan* p, int n_mat, const uint32_t* table, int index_bytes,
+                                  const void* d_index);
+
 /* Pole sets of the ADE (openem/kernels/dispersion.cu:25-114): set s owns poles
  * set_ofs[s] .. set_ofs[s+1]-1; coef holds 4 floats per pole, (Re(A-1), Im(A-1), Re(B), Im(B)).
  * seg_ofs: one uint32 per 32-cell z segment of the padded grid, the number of poles stored
@@ -76,6 +81,11 @@ int oem_plan_set_materials(oem_plan* p, int n_mat, const uint32_t* table, int in
  * Replaces openem/device_tables.py:235-285 (_dispersion_tables). */
 int oem_plan_set_pole_sets(oem_plan* p, int n_sets, const int32_t* set_ofs, const float* coef,
                            const uint32_t* seg_ofs, int64_t n_seg, int64_t n_pole_total);
+
+/* Same as oem_plan_set_pole_sets, with seg_ofs already in device memory (copied). */
+int oem_plan_set_pole_sets_device(oem_plan* p, int n_sets, const int32_t* set_ofs,
+                                  const float* coef, const uint32_t* d_seg_ofs, int64_t n_seg,
+                                  int64_t n_pole_total);
 
 /* One-face TF/SF plane-wave group (openem/kernels/source_dft.cu:39-73,
  * openem/sources_setup.py:93-119): H correction on plane kh (Hy for pol 0, Hx for pol 1),
@@ -123,6 +133,13 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream);
 /* Fold the partly filled snapshot batch of every DFT monitor into its accumulator
  * (openem/readout.py:137-157). Idempotent until the next step. */
 int oem_plan_flush(oem_plan* p, void* stream);
+
+/* Synchronise `stream` and report OEM_ERR_TIMEOUT if a kernel's bounded pipeline wait gave up
+ * since the last check (the readout calls report it too). */
+int oem_plan_status(oem_plan* p, void* stream);
+
+/* Number of kernel launches one time step of this plan makes (its captured step graph). */
+int oem_plan_launches_per_step(oem_plan* p, int* n);
 
 /* Steps taken so far (host-side count). */
 int oem_plan_steps(oem_plan* p, int64_t* steps);

@@ -4,6 +4,7 @@
 // (oem_plan_run); the float64 coefficient math stays in the Python host.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -133,18 +134,95 @@ static int alloc_psi(oem_plan* p) {
   return OEM_OK;
 }
 
+static cudaError_t run_h(oem_plan* p, cudaStream_t s) {
+  if (p->basic_kernels == 1) return launch_update_h(p->yp, s);
+  if (p->basic_kernels == 2) return launch_update_h_stream(p->yp, p->xch, s);
+  return launch_update_h_tma(p->tma, p->yp, p->xch, p->d_err, s);
+}
+
+static cudaError_t run_e(oem_plan* p, cudaStream_t s) {
+  if (p->basic_kernels == 1) return launch_update_e(p->yp, s);
+  if (p->basic_kernels == 2) return launch_update_e_stream(p->yp, p->xch, (int)p->mats.size(), s);
+  return launch_update_e_tma(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s);
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+  }
+  return fn;
+}
+
+// 3D tensor map over one padded (nx, ny, nzp) array, box (bz, by, 1), zero fill out of bounds.
+static int encode_map(oem_plan* p, CUtensorMap* m, const void* base, bool u16, bool u32, int bz,
+                      int by) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return set_error(OEM_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  const cuuint64_t es = u16 ? 2 : 4;
+  cuuint64_t dims[3] = {(cuuint64_t)p->nzp, (cuuint64_t)p->ny, (cuuint64_t)p->nx};
+  cuuint64_t strides[2] = {(cuuint64_t)p->nzp * es, (cuuint64_t)p->ny * p->nzp * es};
+  cuuint32_t box[3] = {(cuuint32_t)bz, (cuuint32_t)by, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  const CUtensorMapDataType dt = u16 ? CU_TENSOR_MAP_DATA_TYPE_UINT16
+                                     : (u32 ? CU_TENSOR_MAP_DATA_TYPE_UINT32
+                                            : CU_TENSOR_MAP_DATA_TYPE_FLOAT32);
+  CUresult r = fn(m, dt, 3, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_error(OEM_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return OEM_OK;
+}
+
+int make_tma_maps(oem_plan* p) {
+  int rc;
+  const YeeParams& P = p->yp;
+  for (int c = 0; c < 3; ++c) {
+    if ((rc = encode_map(p, &p->tma.e_wide[c], P.f[c], false, false, 136, 5))) return rc;
+    if ((rc = encode_map(p, &p->tma.e_tile[c], P.f[c], false, false, 128, 4))) return rc;
+    if ((rc = encode_map(p, &p->tma.h_wide[c], P.f[3 + c], false, false, 136, 5))) return rc;
+    if ((rc = encode_map(p, &p->tma.h_tile[c], P.f[3 + c], false, false, 128, 4))) return rc;
+  }
+  if (P.mat16) return encode_map(p, &p->tma.m_tile, P.mat16, true, false, 128, 4);
+  return encode_map(p, &p->tma.m_tile, P.mat32, false, true, 128, 4);
+}
+
+// Non-zero when a kernel's bounded wait gave up since the last check.
+static int check_device_error(oem_plan* p) {
+  int h = 0;
+  OEM_CUDA(cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    cudaMemset(p->d_err, 0, sizeof(int));
+    return set_error(OEM_ERR_TIMEOUT,
+                     "a device pipeline wait exceeded its bound; the results of this run are "
+                     "invalid");
+  }
+  return OEM_OK;
+}
+
 // One time step (openem/solver.py:1145-1162).
 static int enqueue_step(oem_plan* p, cudaStream_t s) {
   const YeeParams& P = p->yp;
   cudaError_t e;
-  if ((e = launch_update_h(P, s)) != cudaSuccess) return cuda_error(e, "update_h");
+  if ((e = run_h(p, s)) != cudaSuccess) return cuda_error(e, "update_h");
   for (const DipoleSet& d : p->dipoles)
     if (d.magnetic && (e = launch_dipoles(P, d, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "dipoles_h");
   for (const PlaneSrc& src : p->planes)
     if ((e = launch_plane_h(P, src, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "plane_h");
-  if ((e = launch_update_e(P, s)) != cudaSuccess) return cuda_error(e, "update_e");
+  if ((e = run_e(p, s)) != cudaSuccess) return cuda_error(e, "update_e");
   for (const PlaneSrc& src : p->planes)
     if ((e = launch_plane_e(P, src, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "plane_e");
@@ -215,6 +293,10 @@ int oem_plan_create(int device, int nx, int ny, int nz, double ch, double cw, oe
   p->nzp = (int)nzp;
   p->ch = ch;
   p->cw = cw;
+  const char* kind = getenv("OEM_B200_KERNELS");
+  p->basic_kernels = 0;
+  if (kind && strcmp(kind, "basic") == 0) p->basic_kernels = 1;
+  if (kind && strcmp(kind, "stream") == 0) p->basic_kernels = 2;
   *out = p;
   return OEM_OK;
 }
@@ -290,6 +372,8 @@ int oem_plan_set_materials(oem_plan* p, int n_mat, const uint32_t* table, int in
   v.reserved = 0;
   memcpy(&p->mats[1], table, sizeof(MatRec) * (size_t)n_mat);
   for (int m = 1; m <= n_mat; ++m)
+    p->mats[m].reserved = p->mats[m].np[0] + p->mats[m].np[1] + p->mats[m].np[2];
+  for (int m = 1; m <= n_mat; ++m)
     for (int c = 0; c < 3; ++c) {
       const MatRec& r = p->mats[m];
       if (r.pset[c] < 0 && r.np[c] != 0)
@@ -332,6 +416,85 @@ int oem_plan_set_pole_sets(oem_plan* p, int n_sets, const int32_t* set_ofs, cons
     if (p->pset_ofs[s + 1] < p->pset_ofs[s]) return set_error(OEM_ERR_INVALID, "set_ofs not monotone");
   p->pcoef.assign(coef, coef + 4 * (size_t)p->pset_ofs[n_sets]);
   p->seg_ofs.assign(seg_ofs, seg_ofs + n_seg);
+  p->n_pole_total = n_pole_total;
+  return OEM_OK;
+}
+
+// Material table from the host, per-cell index already on the device (unpadded C order).
+int oem_plan_set_materials_device(oem_plan* p, int n_mat, const uint32_t* table, int index_bytes,
+                                  const void* d_index) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (n_mat < 1 || !table || !d_index) return set_error(OEM_ERR_INVALID, "empty material table");
+  if (index_bytes != 2 && index_bytes != 4)
+    return set_error(OEM_ERR_INVALID, "index_bytes must be 2 or 4");
+  if (index_bytes == 2 && n_mat > 65535)
+    return set_error(OEM_ERR_INVALID, "more than 65535 materials need a 4-byte index");
+  if ((rc = use_device(p))) return rc;
+  p->mats.resize((size_t)n_mat + 1);
+  MatRec& v = p->mats[0];
+  for (int c = 0; c < 3; ++c) {
+    v.ca[c] = 0.f; v.cb[c] = 0.f; v.eps[c] = 1.f; v.pset[c] = -1; v.np[c] = 0;
+  }
+  v.reserved = 0;
+  memcpy(&p->mats[1], table, sizeof(MatRec) * (size_t)n_mat);
+  for (int m = 1; m <= n_mat; ++m) {
+    MatRec& r = p->mats[m];
+    for (int c = 0; c < 3; ++c) {
+      if (r.pset[c] < 0 && r.np[c] != 0)
+        return set_error(OEM_ERR_INVALID, "non-dispersive material with a pole count");
+      if (r.np[c] < 0 || r.np[c] > 15)
+        return set_error(OEM_ERR_INVALID, "pole count per component must be 0..15");
+    }
+    r.reserved = r.np[0] + r.np[1] + r.np[2];
+  }
+  p->index_bytes = index_bytes;
+  const bool wide = index_bytes == 4 || (size_t)n_mat + 1 > 65535;
+  const size_t ncp = (size_t)p->nx * p->ny * p->nzp;
+  unsigned* bad = nullptr;
+  if ((rc = dalloc(p, &bad, 1))) return rc;
+  cudaError_t e;
+  if (wide) {
+    if ((rc = dalloc(p, &p->dev_mat32, ncp, false))) return rc;
+    e = launch_pad_index(d_index, index_bytes, nullptr, p->dev_mat32, p->nx, p->ny, p->nz, p->nzp,
+                         (uint32_t)n_mat, bad, 0);
+  } else {
+    if ((rc = dalloc(p, &p->dev_mat16, ncp, false))) return rc;
+    e = launch_pad_index(d_index, index_bytes, p->dev_mat16, nullptr, p->nx, p->ny, p->nz, p->nzp,
+                         (uint32_t)n_mat, bad, 0);
+  }
+  if (e != cudaSuccess) return cuda_error(e, "pad_index");
+  unsigned hbad = 0;
+  OEM_CUDA(cudaMemcpy(&hbad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (hbad) return set_error(OEM_ERR_INVALID, "material index out of range");
+  p->dev_index = true;
+  return OEM_OK;
+}
+
+// Pole sets from the host, segment offsets already on the device.
+int oem_plan_set_pole_sets_device(oem_plan* p, int n_sets, const int32_t* set_ofs,
+                                  const float* coef, const uint32_t* d_seg_ofs, int64_t n_seg,
+                                  int64_t n_pole_total) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (n_sets < 1 || !set_ofs || !coef || !d_seg_ofs)
+    return set_error(OEM_ERR_INVALID, "empty pole-set table");
+  const int64_t want_seg = (int64_t)p->nx * p->ny * p->nzp / 32;
+  if (n_seg != want_seg)
+    return set_error(OEM_ERR_INVALID, "seg_ofs must hold one entry per 32-cell segment (" +
+                                          std::to_string(want_seg) + ")");
+  if (n_pole_total < 0 || n_pole_total > 0xffffffffLL)
+    return set_error(OEM_ERR_INVALID, "pole count out of range");
+  if ((rc = use_device(p))) return rc;
+  p->pset_ofs.assign(set_ofs, set_ofs + n_sets + 1);
+  if (p->pset_ofs[0] != 0) return set_error(OEM_ERR_INVALID, "set_ofs[0] must be 0");
+  for (int s = 0; s < n_sets; ++s)
+    if (p->pset_ofs[s + 1] < p->pset_ofs[s]) return set_error(OEM_ERR_INVALID, "set_ofs not monotone");
+  p->pcoef.assign(coef, coef + 4 * (size_t)p->pset_ofs[n_sets]);
+  if ((rc = dalloc(p, &p->dev_seg, (size_t)n_seg, false))) return rc;
+  OEM_CUDA(cudaMemcpy(p->dev_seg, d_seg_ofs, (size_t)n_seg * sizeof(uint32_t),
+                      cudaMemcpyDeviceToDevice));
+  p->seg_ofs.clear();
   p->n_pole_total = n_pole_total;
   return OEM_OK;
 }
@@ -522,7 +685,10 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   if ((rc = dupload(p, &dm, p->mats.data(), p->mats.size()))) return rc;
   P.mats = dm;
   const bool wide = p->index_bytes == 4 || p->mats.size() > 65535;
-  {
+  if (p->dev_index) {
+    P.mat16 = p->dev_mat16;
+    P.mat32 = p->dev_mat32;
+  } else {
     const size_t row = (size_t)p->nz;
     if (!wide) {
       std::vector<uint16_t> idx(ncp, 0);
@@ -569,7 +735,11 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
     float2* dP;
     if ((rc = dupload(p, &dc, reinterpret_cast<const float4*>(p->pcoef.data()), p->pcoef.size() / 4))) return rc;
     if ((rc = dupload(p, &dofs, p->pset_ofs.data(), p->pset_ofs.size()))) return rc;
-    if ((rc = dupload(p, &dseg, p->seg_ofs.data(), p->seg_ofs.size()))) return rc;
+    if (p->dev_seg) {
+      dseg = p->dev_seg;
+    } else if ((rc = dupload(p, &dseg, p->seg_ofs.data(), p->seg_ofs.size()))) {
+      return rc;
+    }
     if ((rc = dalloc(p, &dP, (size_t)std::max<int64_t>(p->n_pole_total, 1)))) return rc;
     P.pcoef = dc;
     P.pset_ofs = dofs;
@@ -578,6 +748,19 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
     P.has_ade = 1;
   }
   if ((rc = dalloc(p, &p->d_step, 1))) return rc;
+  if ((rc = dalloc(p, &p->d_err, 1))) return rc;
+  p->xch = p->basic_kernels == 2 ? stream_xchunk(P) : tma_xchunk(P);
+  if (p->basic_kernels == 0) {
+    // grids the tensor-map encoder refuses run on the register-streaming kernels
+    if (make_tma_maps(p) != OEM_OK) {
+      p->basic_kernels = 2;
+      p->xch = stream_xchunk(P);
+    } else {
+      cudaError_t e = tma_setup_kernels();
+      if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
+    }
+  }
+  if (const char* xs = getenv("OEM_B200_XCHUNK")) p->xch = std::max(1, atoi(xs));
   p->energy_blocks = energy_block_count(P);
   if ((rc = dalloc(p, &p->d_energy_part, 3 * (size_t)p->energy_blocks))) return rc;
   // capture: G steps per graph for small grids (launch overhead), 1 for large ones
@@ -611,7 +794,7 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
     for (int64_t q = 0; q < n; ++q) {
       cudaEvent_t* E = &ev[(size_t)q * 5];
       OEM_CUDA(cudaEventRecord(E[0], s));
-      cudaError_t e = launch_update_h(p->yp, s);
+      cudaError_t e = run_h(p, s);
       if (e != cudaSuccess) return cuda_error(e, "update_h");
       OEM_CUDA(cudaEventRecord(E[1], s));
       for (const DipoleSet& d : p->dipoles)
@@ -620,7 +803,7 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       for (const PlaneSrc& src : p->planes)
         if ((e = launch_plane_h(p->yp, src, p->d_step, s)) != cudaSuccess) return cuda_error(e, "plane_h");
       OEM_CUDA(cudaEventRecord(E[2], s));
-      if ((e = launch_update_e(p->yp, s)) != cudaSuccess) return cuda_error(e, "update_e");
+      if ((e = run_e(p, s)) != cudaSuccess) return cuda_error(e, "update_e");
       OEM_CUDA(cudaEventRecord(E[3], s));
       for (const PlaneSrc& src : p->planes)
         if ((e = launch_plane_e(p->yp, src, p->d_step, s)) != cudaSuccess) return cuda_error(e, "plane_e");
@@ -682,6 +865,27 @@ int oem_plan_flush(oem_plan* p, void* stream) {
   return OEM_OK;
 }
 
+int oem_plan_launches_per_step(oem_plan* p, int* n) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (!n) return set_error(OEM_ERR_INVALID, "null output");
+  int c = 2 + 1;  // update_h, update_e, step counter
+  c += 2 * (int)p->planes.size();
+  for (const DipoleSet& d : p->dipoles) c += d.n_targets > 0 ? 1 : 0;
+  c += 2 * (int)p->tmons.size();
+  c += 3 * (int)p->mons.size();  // snapshot, flush, flush mark
+  *n = c;
+  return OEM_OK;
+}
+
+int oem_plan_status(oem_plan* p, void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if ((rc = use_device(p))) return rc;
+  OEM_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  return check_device_error(p);
+}
+
 int oem_plan_steps(oem_plan* p, int64_t* steps) {
   if (!p || !steps) return set_error(OEM_ERR_INVALID, "null argument");
   *steps = p->steps;
@@ -699,7 +903,7 @@ int oem_plan_read_monitor(oem_plan* p, int id, double* re, double* im, void* str
   OEM_CUDA(cudaMemcpyAsync(re, m.d_re, n * sizeof(double), cudaMemcpyDeviceToHost, s));
   OEM_CUDA(cudaMemcpyAsync(im, m.d_im, n * sizeof(double), cudaMemcpyDeviceToHost, s));
   OEM_CUDA(cudaStreamSynchronize(s));
-  return OEM_OK;
+  return check_device_error(p);
 }
 
 int oem_plan_read_time_monitor(oem_plan* p, int id, float* out, void* stream) {
@@ -725,7 +929,7 @@ int oem_plan_read_field(oem_plan* p, int comp, float* out, void* stream) {
                              (size_t)p->nzp * sizeof(float), (size_t)p->nz * sizeof(float),
                              (size_t)p->nx * p->ny, cudaMemcpyDeviceToHost, s));
   OEM_CUDA(cudaStreamSynchronize(s));
-  return OEM_OK;
+  return check_device_error(p);
 }
 
 int oem_plan_write_field(oem_plan* p, int comp, const float* in, void* stream) {
@@ -756,7 +960,7 @@ int oem_plan_energy(oem_plan* p, double out[3], void* stream) {
   out[0] = out[1] = out[2] = 0.0;
   for (int b = 0; b < p->energy_blocks; ++b)
     for (int c = 0; c < 3; ++c) out[c] += part[3 * (size_t)b + c];
-  return OEM_OK;
+  return check_device_error(p);
 }
 
 int oem_plan_field_ptrs(oem_plan* p, void* ptrs[6], int* nzp) {

@@ -2,6 +2,7 @@
 // blocks, the plan object, launch helpers.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -36,7 +37,7 @@ struct MatRec {
   float eps[3];
   int pset[3];  // -1 = not dispersive
   int np[3];    // poles of that set (0 when not dispersive)
-  int reserved;
+  int reserved;  // np[0] + np[1] + np[2], filled by the plan
 };
 static_assert(sizeof(MatRec) == 64, "MatRec must be 16 words");
 
@@ -83,6 +84,16 @@ struct YeeParams {
   const int* pset_ofs;     // set -> first pole in pcoef
   const uint32_t* seg_ofs; // poles stored before each 32-cell segment
   int has_ade;
+};
+
+// TMA descriptors of the field tiles the pipelined kernels load (see oem_yee_tma.cu):
+// halo boxes 136 (z) x 5 (y) and tiles 128 x 4, plus the material-index tile.
+struct TmaMaps {
+  CUtensorMap e_wide[3];
+  CUtensorMap h_tile[3];
+  CUtensorMap h_wide[3];
+  CUtensorMap e_tile[3];
+  CUtensorMap m_tile;
 };
 
 struct PlaneSrc {
@@ -183,6 +194,16 @@ struct oem_plan {
 
   bool timing = false;
   std::vector<oem::TimingRec> trecs;
+
+  bool dev_index = false;        // material index uploaded from device memory
+  uint16_t* dev_mat16 = nullptr;
+  uint32_t* dev_mat32 = nullptr;
+  uint32_t* dev_seg = nullptr;   // segment offsets uploaded from device memory
+
+  int basic_kernels = 0;  // 1: one-thread-per-cell kernels, 2: register-streaming, 0: TMA
+  oem::TmaMaps tma{};
+  int* d_err = nullptr;   // set by a kernel whose bounded wait gave up
+  int xch = 8;            // x planes per thread in the streaming kernels
 };
 
 namespace oem {
@@ -231,6 +252,19 @@ cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* ste
                             cudaStream_t s);
 cudaError_t launch_flush(const Monitor& m, const int* step, int forced, cudaStream_t s);
 cudaError_t launch_step_advance(int* step, cudaStream_t s);
+int stream_xchunk(const YeeParams& P);
+int tma_xchunk(const YeeParams& P);
+cudaError_t tma_setup_kernels();
+cudaError_t launch_update_h_tma(const TmaMaps& maps, const YeeParams& P, int xch, int* err,
+                                cudaStream_t s);
+cudaError_t launch_update_e_tma(const TmaMaps& maps, const YeeParams& P, int xch, int n_mats,
+                                int* err, cudaStream_t s);
+int make_tma_maps(oem_plan* p);
+cudaError_t launch_pad_index(const void* in, int in_bytes, uint16_t* out16, uint32_t* out32,
+                             int nx, int ny, int nz, int nzp, uint32_t n_mat, unsigned* bad,
+                             cudaStream_t s);
+cudaError_t launch_update_h_stream(const YeeParams& P, int xch, cudaStream_t s);
+cudaError_t launch_update_e_stream(const YeeParams& P, int xch, int n_mats, cudaStream_t s);
 cudaError_t launch_energy(const YeeParams& P, double* const dl[3][2], double* part, int nblocks,
                           cudaStream_t s);
 int energy_block_count(const YeeParams& P);

@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "oem_internal.cuh"
 
 namespace oem {
@@ -401,7 +403,46 @@ __global__ void __launch_bounds__(256) k_energy(YeeParams P, const double* dxp, 
   }
 }
 
+// Copy an unpadded (nx, ny, nz) material index into the padded (nx, ny, nzp) layout, shifted by
+// one (0 is the padding material); flags indices >= n_mat.
+template <class Tin, class Tout>
+__global__ void k_pad_index(const Tin* in, Tout* out, int ny, int nz, int nzp, int64_t total,
+                            uint32_t n_mat, unsigned* bad) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(t % nzp);
+    const int64_t r = t / nzp;
+    Tout v = 0;
+    if (k < nz) {
+      const uint32_t m = (uint32_t)in[r * nz + k];
+      if (m >= n_mat) {
+        atomicOr(bad, 1u);
+      } else {
+        v = (Tout)(m + 1);
+      }
+    }
+    out[t] = v;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_pad_index(const void* in, int in_bytes, uint16_t* out16, uint32_t* out32,
+                             int nx, int ny, int nz, int nzp, uint32_t n_mat, unsigned* bad,
+                             cudaStream_t s) {
+  const int64_t total = (int64_t)nx * ny * nzp;
+  const int nb = (int)std::min<int64_t>((total + 255) / 256, 148 * 64);
+  if (in_bytes == 2) {
+    const uint16_t* a = static_cast<const uint16_t*>(in);
+    if (out16) k_pad_index<<<nb, 256, 0, s>>>(a, out16, ny, nz, nzp, total, n_mat, bad);
+    else k_pad_index<<<nb, 256, 0, s>>>(a, out32, ny, nz, nzp, total, n_mat, bad);
+  } else {
+    const uint32_t* a = static_cast<const uint32_t*>(in);
+    if (out16) k_pad_index<<<nb, 256, 0, s>>>(a, out16, ny, nz, nzp, total, n_mat, bad);
+    else k_pad_index<<<nb, 256, 0, s>>>(a, out32, ny, nz, nzp, total, n_mat, bad);
+  }
+  return cudaGetLastError();
+}
 
 // ---------------------------------------------------------------------------------------------
 // Launchers

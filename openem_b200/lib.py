@@ -29,7 +29,9 @@ SIGNATURES = {
     "oem_plan_destroy": (_I, [_P]),
     "oem_plan_set_axis": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I]),
     "oem_plan_set_materials": (_I, [_P, _I, _P, _I, _P]),
+    "oem_plan_set_materials_device": (_I, [_P, _I, _P, _I, _P]),
     "oem_plan_set_pole_sets": (_I, [_P, _I, _P, _P, _P, _L, _L]),
+    "oem_plan_set_pole_sets_device": (_I, [_P, _I, _P, _P, _P, _L, _L]),
     "oem_plan_add_plane_source": (_I, [_P, _I, _I, _I, _D, _D, _L, _P, _P]),
     "oem_plan_add_dipoles": (_I, [_P, _I, _I, _P, _P, _P, _P, _I, _L, _P]),
     "oem_plan_add_flux_monitor": (_I, [_P, _I, _I, _I, _L, _P, _I, C.POINTER(_I)]),
@@ -40,6 +42,8 @@ SIGNATURES = {
     "oem_plan_finalize": (_I, [_P, _L]),
     "oem_plan_run": (_I, [_P, _L, _P]),
     "oem_plan_flush": (_I, [_P, _P]),
+    "oem_plan_status": (_I, [_P, _P]),
+    "oem_plan_launches_per_step": (_I, [_P, C.POINTER(_I)]),
     "oem_plan_steps": (_I, [_P, C.POINTER(_L)]),
     "oem_plan_read_monitor": (_I, [_P, _I, _P, _P, _P]),
     "oem_plan_read_time_monitor": (_I, [_P, _I, _P, _P]),

@@ -1,0 +1,81 @@
+"""Algorithmic byte counts of the step, used for the HBM roofline.
+
+Per cell-update, the step must read and write the six field components once (48 B), read a
+material description, update the CPML psi auxiliaries of the cells in the boundary slabs (two
+psi arrays per field family per slab axis, read and written: 16 B per slab cell per family),
+update the ADE pole states of the dispersive entries (a complex float32 read and written per
+pole: 16 B), and read the monitored points (six float32 per point per step).
+
+``step_bytes_per_cell`` uses OpenEM's material description (three uint16 coefficient indices,
+6 B per cell) so the figure is comparable across implementations; the per-kernel counts use
+what this engine's kernels must move (one uint16 material index, 2 B per cell, read by the E
+update only).
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import pathlib
+
+import numpy as np
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _slab_cells(sc) -> dict:
+    nx, ny, nz = (int(v) for v in sc.shape)
+    dims = (nx, ny, nz)
+    out = {}
+    for a in range(3):
+        lo = sc.pml.get((a, "lo"))
+        hi = sc.pml.get((a, "hi"))
+        layers = (0 if lo is None else int(np.asarray(lo.a_E).size)) + \
+                 (0 if hi is None else int(np.asarray(hi.a_E).size))
+        out[a] = layers * nx * ny * nz // dims[a]
+    return out
+
+
+def counts(sc) -> dict:
+    ncell = int(np.prod(sc.shape))
+    slabs = _slab_cells(sc)
+    n_pole = 0 if sc.dispersion is None else int(sc.dispersion.n_pole)
+    mon_pts = 0
+    for m in sc.field_monitors:
+        mon_pts += int(np.prod(m.box))
+    for m in sc.flux_monitors:
+        t = [sc.shape[a] for a in range(3) if a != m.axis]
+        mon_pts += int(t[0] * t[1])
+    return {"ncell": ncell, "slab_cells": slabs, "n_pole": n_pole, "monitor_points": mon_pts}
+
+
+def step_bytes_per_cell(sc) -> float:
+    """Algorithmic bytes per cell-update of one full step (OpenEM's 6-byte material form)."""
+    c = counts(sc)
+    n = c["ncell"]
+    psi = 32.0 * sum(c["slab_cells"].values())
+    ade = 16.0 * c["n_pole"]
+    mon = 24.0 * c["monitor_points"]
+    return (48.0 + 6.0) + (psi + ade + mon) / n
+
+
+def kernel_bytes(sc) -> dict:
+    """Algorithmic bytes per launch of this engine's two update kernels."""
+    c = counts(sc)
+    n = c["ncell"]
+    psi = 16.0 * sum(c["slab_cells"].values())
+    return {"update_h": 36.0 * n + psi, "update_e": 38.0 * n + psi + 16.0 * c["n_pole"]}
+
+
+def measured_peaks(root=None) -> dict:
+    """The measured HBM copy bandwidth (GB/s) of this pool's B200s, or the fallback figure."""
+    root = pathlib.Path(root or pathlib.Path(__file__).resolve().parent.parent)
+    p = root / "MEASURED_PEAKS.json"
+    env = os.environ.get("OEM_B200_PEAKS")
+    if env:
+        p = pathlib.Path(env)
+    try:
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    except Exception:
+        return {"hbm_gbs": FALLBACK_HBM_GBS, "source": "fallback"}

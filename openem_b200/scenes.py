@@ -160,7 +160,8 @@ def slab_plane_wave(nxy: int = 30, dl: float = 0.02 * UM, lz: float = 3.0 * UM,
                     src_z: float = -1.0 * UM, mon_t: float = 1.0 * UM,
                     mon_r: float = -1.2 * UM, freq0: float = 2.998e14, nfreq: int = 11,
                     run_time: float = 4e-13, n_pml: int = 12, with_slab: bool = True,
-                    num_steps: int | None = None) -> Scene:
+                    num_steps: int | None = None, direction: int = 1,
+                    fwidth_rel: float = 0.2) -> Scene:
     """0.6 x 0.6 x 3.0 um periodic-x/y cell, 12-layer CPML on +/-z, an eps=4 slab 0.3 um thick
     at z=0, a +z Ex-polarised plane wave at z=-1.0 um (Gaussian pulse f0, fwidth=0.2 f0), flux
     planes "T" at z=+1.0 um and "R" at z=-1.2 um at 11 frequencies over f0 +/- fwidth.
@@ -184,15 +185,17 @@ def slab_plane_wave(nxy: int = 30, dl: float = 0.02 * UM, lz: float = 3.0 * UM,
         if with_slab:
             e[:, :, inside] = eps_slab
         eps.append(e)
-    pulse = GaussianPulse(freq0=freq0, fwidth=0.2 * freq0)
+    pulse = GaussianPulse(freq0=freq0, fwidth=fwidth_rel * freq0)
     wf = sample_waveform(pulse, dt, n_steps)
     edges_z = np.asarray(az.edges)
     ks = int(np.argmin(np.abs(edges_z - src_z)))
-    ex_inc, hy_inc = plane_wave_tables(pulse, dt, n_steps, 0.5 * float(az.dl[ks - 1]), 1.0, +1)
-    src = PlaneWaveSource(axis=2, plane_index=ks, direction=1, pol_axis=0, waveform=wf,
+    # the upstream Hy point is half a cell below the plane for +z, half a cell above for -z
+    dl_half = 0.5 * float(az.dl[ks - 1] if direction > 0 else az.dl[ks])
+    ex_inc, hy_inc = plane_wave_tables(pulse, dt, n_steps, dl_half, 1.0, direction)
+    src = PlaneWaveSource(axis=2, plane_index=ks, direction=direction, pol_axis=0, waveform=wf,
                           angle_theta=0.0, num_freqs=1, ex_inc=ex_inc, hy_inc=hy_inc,
                           center=src_z)
-    freqs = np.linspace(freq0 - 0.2 * freq0, freq0 + 0.2 * freq0, nfreq)
+    freqs = np.linspace(freq0 - fwidth_rel * freq0, freq0 + fwidth_rel * freq0, nfreq)
     spec = spectrum(pulse, dt, n_steps, freqs)
     mons = []
     for name, zc in (("T", mon_t), ("R", mon_r)):

@@ -12,6 +12,7 @@ allocated, the same fail-closed behaviour as OpenEM (``openem/solver.py:1221-126
 from __future__ import annotations
 
 import ctypes as C
+import os
 import time
 
 import numpy as np
@@ -54,6 +55,7 @@ class Plan:
         self.sc = sc
         self.n_total = int(sc.num_time_steps if n_total is None else n_total)
         self.stream = stream
+        self.device = int(device)
         self.shape = tuple(int(v) for v in sc.shape)
         nx, ny, nz = self.shape
         self._keep = []
@@ -69,6 +71,16 @@ class Plan:
             raise
 
     # ---- construction ------------------------------------------------------------------
+    def _device_tables(self) -> bool:
+        """Build the per-cell tables on the GPU for large grids (host numpy otherwise)."""
+        mode = os.environ.get("OEM_B200_TABLES", "auto")
+        if mode == "host":
+            return False
+        from openem_b200 import tables_gpu
+        if mode == "device":
+            return True
+        return int(np.prod(self.shape)) >= 2_000_000 and tables_gpu.available()
+
     def _arr(self, a, dtype):
         a = np.ascontiguousarray(a, dtype=dtype)
         self._keep.append(a)
@@ -86,17 +98,34 @@ class Plan:
                 L.ptr(self._arr(np.real(t.mpv), np.float64)),
                 L.ptr(self._arr(t.pml_e, np.float64)), L.ptr(self._arr(t.pml_h, np.float64)),
                 int(t.lo), int(t.hi)), f"set_axis {a}")
-        mt = T.material_tables(sc, self.tabs)
-        self.mt = mt
-        L.check(lib.oem_plan_set_materials(h, int(mt.n_mat), L.ptr(self._arr(mt.table, np.uint32)),
-                                           int(mt.index.dtype.itemsize),
-                                           L.ptr(self._arr(mt.index, mt.index.dtype))),
-                "set_materials")
-        if mt.n_pole_total > 0:
-            L.check(lib.oem_plan_set_pole_sets(
-                h, int(mt.set_ofs.size - 1), L.ptr(self._arr(mt.set_ofs, np.int32)),
-                L.ptr(self._arr(mt.coef, np.float32)), L.ptr(self._arr(mt.seg_ofs, np.uint32)),
-                int(mt.seg_ofs.size), int(mt.n_pole_total)), "set_pole_sets")
+        if self._device_tables():
+            from openem_b200 import tables_gpu
+            mt = tables_gpu.material_tables_device(sc, self.tabs, self.device)
+            self.h2d_bytes += sum(np.asarray(a).nbytes for a in
+                                  (sc.eps_ex, sc.eps_ey, sc.eps_ez))
+            self.h2d_bytes += sum(np.asarray(a).nbytes for a in
+                                  (sc.sigma_ex, sc.sigma_ey, sc.sigma_ez) if a is not None)
+            L.check(lib.oem_plan_set_materials_device(
+                h, int(mt.n_mat), L.ptr(self._arr(mt.table, np.uint32)), int(mt.index_bytes),
+                C.c_void_p(mt.index.data_ptr())), "set_materials_device")
+            if mt.n_pole_total > 0:
+                L.check(lib.oem_plan_set_pole_sets_device(
+                    h, int(mt.set_ofs.size - 1), L.ptr(self._arr(mt.set_ofs, np.int32)),
+                    L.ptr(self._arr(mt.coef, np.float32)), C.c_void_p(mt.seg_ofs.data_ptr()),
+                    int(mt.seg_ofs.numel()), int(mt.n_pole_total)), "set_pole_sets_device")
+            del mt
+        else:
+            mt = T.material_tables(sc, self.tabs)
+            L.check(lib.oem_plan_set_materials(h, int(mt.n_mat),
+                                               L.ptr(self._arr(mt.table, np.uint32)),
+                                               int(mt.index.dtype.itemsize),
+                                               L.ptr(self._arr(mt.index, mt.index.dtype))),
+                    "set_materials")
+            if mt.n_pole_total > 0:
+                L.check(lib.oem_plan_set_pole_sets(
+                    h, int(mt.set_ofs.size - 1), L.ptr(self._arr(mt.set_ofs, np.int32)),
+                    L.ptr(self._arr(mt.coef, np.float32)), L.ptr(self._arr(mt.seg_ofs, np.uint32)),
+                    int(mt.seg_ofs.size), int(mt.n_pole_total)), "set_pole_sets")
         for ps in T.plane_sources(sc):
             if ps["ex"].size < self.n_total:
                 raise ValueError(f"asked to run {self.n_total} steps, but the plane-wave table "
@@ -199,6 +228,15 @@ class Plan:
         L.check(self.lib.oem_plan_energy(self.h, L.ptr(out), self._s), "energy")
         return out
 
+    def launches_per_step(self) -> int:
+        n = C.c_int()
+        L.check(self.lib.oem_plan_launches_per_step(self.h, C.byref(n)))
+        return int(n.value)
+
+    def status(self) -> None:
+        """Raise if a device pipeline wait timed out since the last check."""
+        L.check(self.lib.oem_plan_status(self.h, self._s), "status")
+
     def enable_timing(self, on: bool = True) -> None:
         L.check(self.lib.oem_plan_enable_timing(self.h, int(bool(on))))
 
@@ -253,19 +291,31 @@ def _time_mon_guard(sc) -> int:
 
 def run(sc, num_steps: int | None = None, use_shutoff: bool = True, kernels=None,
         verbose: bool = True, return_fields: bool = False, policy=None,
-        force_complex: bool = False, device: int = 0, stream=None) -> Result:
+        force_complex: bool = False, device: int = 0, stream=None,
+        stats: dict | None = None) -> Result:
     """Run one FDTD simulation on the GPU (signature of ``openem/solver.py:403-412``; the
-    ``kernels`` argument is accepted for call compatibility and unused)."""
+    ``kernels`` argument is accepted for call compatibility and unused). ``stats``, when
+    given, receives the host-to-device and device-to-host byte counts and the launches per
+    step."""
     del kernels
     if force_complex or any(k != 0.0 for k in sc.bloch_k):
         from openem_b200 import bloch
         return bloch.run(sc, num_steps=num_steps, use_shutoff=use_shutoff, verbose=verbose,
                          return_fields=return_fields, policy=policy, device=device,
-                         stream=stream)
+                         stream=stream, stats=stats)
     n_total = int(num_steps if num_steps is not None else sc.num_time_steps)
     plan = Plan(sc, n_total, device=device, stream=stream)
     try:
-        return _loop(plan, sc, n_total, use_shutoff, verbose, return_fields, policy)
+        res = _loop(plan, sc, n_total, use_shutoff, verbose, return_fields, policy)
+        plan.status()
+        if stats is not None:
+            d2h = sum(np.asarray(p.data).size * 16 for p in res.phasors.values())
+            d2h += sum(np.asarray(a).size * 16 for a in res.field_phasors.values())
+            d2h += sum(np.asarray(a).size * 4 for a in res.time_samples.values())
+            d2h += sum(np.asarray(a).size * 4 for a in res.fields.values())
+            stats.update(h2d_bytes=int(plan.h2d_bytes), d2h_bytes=int(d2h),
+                         launches_per_step=plan.launches_per_step())
+        return res
     finally:
         plan.close()
 

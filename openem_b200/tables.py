@@ -193,16 +193,16 @@ def e_coefficients(sc, tabs):
     return ca, cb
 
 
-def pole_sets(sc):
-    """Deduplicate ADE entries by their float32 coefficient lists. Returns per-component dense
-    set-id arrays (-1 = none), ``set_ofs``, ``coef`` and per-set pole counts."""
-    shape = sc.shape
-    ncell = int(np.prod(shape))
-    pset = [None, None, None]
+def entry_pole_sets(sc):
+    """Deduplicate ADE entries by their float32 coefficient lists.
+
+    Returns ``(comp, cell, set_id, set_ofs, coef, counts)``: per entry its component, flat cell
+    and pole-set id; per set its first pole in ``coef`` ((n, 4) float32 rows
+    ``Re(A-1), Im(A-1), Re(B), Im(B)``) and its pole count. ``None`` without dispersion."""
     d = sc.dispersion
     if d is None or d.n_entry == 0:
-        return pset, np.zeros(1, np.int32), np.zeros((0, 4), np.float32), np.zeros(0, np.int32)
-    d.validate(shape)
+        return None
+    d.validate(sc.shape)
     comp = np.asarray(d.comp, dtype=np.int64)
     cell = np.asarray(d.cell, dtype=np.int64)
     ofs = np.asarray(d.pole_ofs, dtype=np.int64)
@@ -211,34 +211,55 @@ def pole_sets(sc):
         raise NotImplementedError("more than 15 poles on one component")
     am1 = np.asarray(d.am1, dtype=np.complex128)
     b = np.asarray(d.b, dtype=np.complex128)
-    pc = np.stack([am1.real, am1.imag, b.real, b.imag], axis=1).astype(np.float32)  # (n_pole, 4)
+    pc = np.empty((am1.size, 4), dtype=np.float32)
+    pc[:, 0], pc[:, 1], pc[:, 2], pc[:, 3] = am1.real, am1.imag, b.real, b.imag
     set_id = np.full(d.n_entry, -1, dtype=np.int64)
-    set_ofs = [0]
-    coefs = []
-    counts = []
-    for k in np.unique(npole):
-        ent = np.flatnonzero(npole == k)
+    set_ofs, coefs, counts = [0], [], []
+    uniform_k = np.all(npole == npole[0])
+    for k in (np.array([npole[0]]) if uniform_k else np.unique(npole)):
+        k = int(k)
         if k == 0:
             continue
-        rows = pc[(ofs[ent][:, None] + np.arange(k)[None, :]).ravel()].reshape(ent.size, 4 * k)
+        ent = np.arange(d.n_entry) if uniform_k else np.flatnonzero(npole == k)
+        if uniform_k and np.all(ofs[:-1] == np.arange(d.n_entry) * k):
+            rows = pc.reshape(d.n_entry, 4 * k)
+        else:
+            rows = pc[(ofs[ent][:, None] + np.arange(k)[None, :]).ravel()].reshape(ent.size, 4 * k)
         bits = rows.view(np.uint32)
-        code, nu = factorize_rows([bits[:, q].astype(np.int64) for q in range(4 * k)])
-        first = np.full(nu, -1, dtype=np.int64)
-        order = np.arange(ent.size)
-        first[code[::-1]] = order[::-1]
+        if np.all(bits == bits[0]):                       # one coefficient list for all
+            code, nu, first = np.zeros(ent.size, np.int64), 1, np.zeros(1, np.int64)
+        else:
+            code, nu = factorize_rows([bits[:, q].astype(np.int64) for q in range(4 * k)])
+            first = np.full(nu, -1, dtype=np.int64)
+            order = np.arange(ent.size)
+            first[code[::-1]] = order[::-1]
         base = len(counts)
         for u in range(nu):
             coefs.append(rows[first[u]].reshape(k, 4))
-            counts.append(int(k))
-            set_ofs.append(set_ofs[-1] + int(k))
+            counts.append(k)
+            set_ofs.append(set_ofs[-1] + k)
         set_id[ent] = base + code
+    coef = np.concatenate(coefs, axis=0).astype(np.float32) if coefs else np.zeros((0, 4), np.float32)
+    return (comp, cell, set_id, np.asarray(set_ofs, dtype=np.int32), coef,
+            np.asarray(counts, dtype=np.int32))
+
+
+def pole_sets(sc):
+    """Dense per-component pole-set ids (-1 = none) plus ``set_ofs``, ``coef``, ``counts``."""
+    shape = sc.shape
+    ep = entry_pole_sets(sc)
+    if ep is None:
+        return [None, None, None], np.zeros(1, np.int32), np.zeros((0, 4), np.float32), \
+            np.zeros(0, np.int32)
+    comp, cell, set_id, set_ofs, coef, counts = ep
+    ncell = int(np.prod(shape))
+    pset = []
     for c in range(3):
         arr = np.full(ncell, -1, dtype=np.int32)
         m = comp == c
         arr[cell[m]] = set_id[m].astype(np.int32)
-        pset[c] = arr.reshape(shape)
-    coef = np.concatenate(coefs, axis=0).astype(np.float32) if coefs else np.zeros((0, 4), np.float32)
-    return pset, np.asarray(set_ofs, dtype=np.int32), coef, np.asarray(counts, dtype=np.int32)
+        pset.append(arr.reshape(shape))
+    return pset, set_ofs, coef, counts
 
 
 def material_tables(sc, tabs) -> MaterialTables:

@@ -1,0 +1,195 @@
+"""The oracle and the host-side tables against OpenEM's own CPU code and published numbers.
+
+Fixtures under tests/golden/ were written by tests/golden/gen_golden.py from OpenEM's numpy
+modules (cpml, grid, apodization, flux, tfsf1d, shutoff, serialize). The known answers are
+OpenEM's published results: the slab transmission printed in README.md:62 and the PML
+reflection measured in tests/test_pml_reflection.py:58.
+"""
+
+import pathlib
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from oracle import ref64
+from openem_b200 import flux as flux_mod
+from openem_b200 import model as M
+from openem_b200 import scenes
+from openem_b200 import tables as T
+
+GOLD = pathlib.Path(__file__).resolve().parent / "golden"
+
+
+@pytest.fixture(scope="module")
+def gt():
+    return np.load(GOLD / "ref_tables.npz")
+
+
+def test_cpml_coefficients_match_reference(gt):
+    dt = float(gt["cpml_dt"])
+    params = {"a": M.PMLParams(12),
+              "b": M.PMLParams(8, sigma_max=2.0, kappa_max=5.0, alpha_max=0.1, alpha_min=0.01)}
+    for tag, p in params.items():
+        for side in ("lo", "hi"):
+            c = M.pml_build(p, float(gt[f"cpml_{tag}_dl"]), side, dt,
+                            avg_speed=float(gt[f"cpml_{tag}_spd"]))
+            for f in ("a_E", "b_E", "inv_kappa_E", "a_H", "b_H", "inv_kappa_H"):
+                np.testing.assert_allclose(getattr(c, f), gt[f"cpml_{tag}_{side}_{f}"],
+                                           rtol=1e-14, atol=0, err_msg=f"{tag} {side} {f}")
+
+
+@pytest.mark.parametrize("tag,lo,hi,k", [("per", "Periodic", "Periodic", 0.0),
+                                         ("pml", "PML", "PML", 0.0),
+                                         ("pmc", "PMCBoundary", "PMCBoundary", 0.0),
+                                         ("blo", "BlochBoundary", "BlochBoundary", 0.15)])
+def test_axis_tables_match_reference(gt, tag, lo, hi, k):
+    ax = M.Axis(gt["axis_edges"], lo, hi)
+    t = ax.index_tables(k)
+    for key in ("nxt", "prv", "mnx", "mpv", "pec"):
+        np.testing.assert_array_equal(t[key], gt[f"axis_{tag}_{key}"], err_msg=key)
+    np.testing.assert_array_equal(ax.dl_dual, gt[f"axis_{tag}_dl_dual"])
+
+
+def test_apodization_matches_reference(gt):
+    t = gt["apod_t"]
+    for tag, spec in (("none", None), ("both", (2e-13, 7e-13, 5e-14)),
+                      ("start", (3e-13, None, 1e-13))):
+        np.testing.assert_array_equal(T.apod_window(t, spec), gt[f"apod_{tag}"])
+        np.testing.assert_array_equal(ref64.apod_window(t, spec), gt[f"apod_{tag}"])
+
+
+def test_plane_flux_matches_reference(gt):
+    sc = scenes.slab_plane_wave(nxy=4, num_steps=10)
+    np.testing.assert_allclose(flux_mod.plane_flux(gt["flux_data"], sc.grid, axis=2),
+                               gt["flux_val"], rtol=1e-13)
+
+
+@pytest.mark.parametrize("tag", ["ll", "ls"])
+def test_oracle_1d_line_matches_reference_tfsf1d(tag):
+    """OpenEM's numpy 1D Yee line (openem/tfsf1d.py:297-325) and the oracle on a 1x1xN periodic
+    column run the same update and one-face injection; their E and H histories agree."""
+    z = np.load(GOLD / "ref_tfsf1d.npz")
+    dl1 = z[f"{tag}_dl1"]
+    n1 = dl1.size
+    dt = float(z["dt"])
+    n_steps = int(z["n_steps"])
+    inj, col0, n_col_e = int(z["inj"]), int(z["col0"]), int(z["n_col_e"])
+    edges = np.concatenate([[0.0], np.cumsum(dl1)])
+    grid = M.Grid(M.Axis(np.array([0.0, dl1[0]]), "Periodic", "Periodic"),
+                  M.Axis(np.array([0.0, dl1[0]]), "Periodic", "Periodic"),
+                  M.Axis(edges, "PECBoundary", "PECBoundary"))
+    eps = z[f"{tag}_eps1"].reshape(1, 1, n1)
+    sig = z[f"{tag}_sigma1"].reshape(1, 1, n1)
+    wf = M.Waveform(amp_int=z[f"{tag}_ex_inc"], amp_half=z[f"{tag}_ex_inc"],
+                    amp_int_complex=z[f"{tag}_ex_inc"].astype(complex), dt=dt)
+    src = M.PlaneWaveSource(axis=2, plane_index=inj, direction=1, pol_axis=0, waveform=wf,
+                            angle_theta=0.0, num_freqs=1, ex_inc=z[f"{tag}_ex_inc"],
+                            hy_inc=z[f"{tag}_hy_inc"])
+    sc = M.Scene(grid=grid, dt=dt, num_time_steps=n_steps, shutoff=1e-5, eps_ex=eps,
+                 eps_ey=eps.copy(), eps_ez=eps.copy(), pml={},
+                 sigma_ex=sig if np.any(sig) else None,
+                 sigma_ey=sig.copy() if np.any(sig) else None,
+                 sigma_ez=sig.copy() if np.any(sig) else None, sources=[src])
+    o = ref64.Oracle(sc, n_steps)
+    ex_tab = np.zeros((n_steps + 1, n_col_e))
+    hy_tab = np.zeros((n_steps, n_col_e + 1))
+    for n in range(n_steps):
+        o.step()
+        hy_tab[n] = o.H[1][0, 0, col0 - 1:col0 + n_col_e]
+        ex_tab[n + 1] = o.E[0][0, 0, col0:col0 + n_col_e]
+    scale_e = np.abs(z[f"{tag}_ex_tab"]).max()
+    scale_h = np.abs(z[f"{tag}_hy_tab"]).max()
+    assert np.abs(ex_tab - z[f"{tag}_ex_tab"]).max() < 1e-12 * scale_e
+    assert np.abs(hy_tab - z[f"{tag}_hy_tab"]).max() < 1e-12 * scale_h
+
+
+def _flux(ph):
+    return 0.5 * (np.real(ph[0] * np.conj(ph[3])).sum(axis=(1, 2))
+                  - np.real(ph[1] * np.conj(ph[2])).sum(axis=(1, 2)))
+
+
+def test_oracle_reproduces_published_slab_transmission():
+    """README.md:62 prints transmission = 0.8310044973694679 for this slab at f0 (Tidy3D
+    scene, OpenEM solver); docs/tutorial.md:101-103 gives T+R within [1.0000, 1.0001]."""
+    sc = scenes.slab_plane_wave(nxy=1)
+    sc0 = scenes.slab_plane_wave(nxy=1, with_slab=False)
+    r, r0 = ref64.run(sc), ref64.run(sc0)
+    T_ = _flux(r.phasors["T"]) / _flux(r0.phasors["T"])
+    R_ = -_flux(r.phasors["R"]) / _flux(r0.phasors["T"])
+    assert abs(T_[5] - 0.8310044973694679) < 2e-6
+    assert np.all(np.abs(T_ + R_ - 1.0) < 1.2e-4)
+    # and the grid converges towards the analytic thin-film value 0.8373
+    assert abs(T_[5] - scenes.slab_analytic_T(sc.flux_monitors[0].freqs)[5]) < 0.01
+
+
+def _pml_reflection(n_layers: int) -> float:
+    """Vacuum column, -z plane wave at z=0, flux 12 cells downstream vs flux at z=+0.4 um
+    (the reference criterion of tests/test_pml_reflection.py:31-54)."""
+    sc = scenes.slab_plane_wave(nxy=1, dl=0.01e-6, lz=2.0e-6, with_slab=False, src_z=0.0,
+                                direction=-1, freq0=5e14, nfreq=1, mon_t=-0.12e-6,
+                                mon_r=0.4e-6, run_time=1e-13, n_pml=n_layers)
+    mons = [replace(m, freqs=np.array([5e14])) for m in sc.flux_monitors]
+    r = ref64.run(replace(sc, flux_monitors=mons))
+    return abs(_flux(r.phasors["R"])[0]) / abs(_flux(r.phasors["T"])[0])
+
+
+def test_oracle_pml_reflection_known_answer():
+    """tests/test_pml_reflection.py:57-69: below 1e-8 with 12 layers (measured 3.8e-9 there),
+    and at least 100x better than 6 layers."""
+    r12 = _pml_reflection(12)
+    r6 = _pml_reflection(6)
+    assert r12 < 1e-8
+    assert 3.0e-9 < r12 < 4.5e-9
+    assert r12 < r6 / 100
+
+
+def test_trapezoid_chi_converges_second_order():
+    """tests/test_dispersion.py:166-181: the discrete susceptibility of the trapezoidal ADE
+    converges to the analytic one at second order (Drude + Lorentz medium of the bulk
+    workload)."""
+    poles = scenes.drude_poles(1.4e16, 1e14)[1:] + scenes.lorentz_poles(1.5, 4e14, 5e13)
+    freqs = np.linspace(1.0e14, 4.0e14, 9)
+
+    def chi_exact(f):
+        s = -2j * np.pi * f
+        return sum(c / (s - a) + np.conj(c) / (s - np.conj(a)) for a, c in poles)
+
+    def chi_disc(f, dt):
+        am1, b = scenes.trap_coeffs(poles, dt)
+        am1c, bc = scenes.trap_coeffs([(np.conj(a), np.conj(c)) for a, c in poles], dt)
+        zz = np.exp(-2j * np.pi * f * dt)
+        h = lambda A, B: B * (zz + 1) / (zz - A)
+        return sum(h(1 + x, y) + h(1 + xc, yc) for x, y, xc, yc in zip(am1, b, am1c, bc))
+
+    errs = []
+    for dt in (8e-18, 4e-18, 2e-18):
+        num = np.array([chi_disc(f, dt) for f in freqs])
+        ana = np.array([chi_exact(f) for f in freqs])
+        errs.append(float(np.max(np.abs(num - ana) / np.abs(1.0 + ana))))
+    order = np.log2(errs[0] / errs[-1]) / 2.0
+    assert 1.9 < order < 2.1, (order, errs)
+
+
+def test_shutoff_policy_matches_reference():
+    from openem_b200 import shutoff
+    z = np.load(GOLD / "ref_shutoff.npz")
+    pol = shutoff.default_policy(1e-5, interval=400)
+    for q, (s, a, b, f) in enumerate(zip(z["steps"], z["e2"], z["energy"], z["flux"])):
+        fired = pol.check(int(s), float(a), float(b), f)
+        assert fired == bool(z["fired"][q]), q
+        assert pol.field_decay.ratio == pytest.approx(float(z["ratio"][q]), rel=1e-12)
+        tau_ref = float(z["tau"][q])
+        if np.isfinite(tau_ref):
+            assert pol.energy_decay.tau == pytest.approx(tau_ref, rel=1e-9)
+        else:
+            assert not np.isfinite(pol.energy_decay.tau)
+    assert pol.reason.split("(")[0] == str(z["reason"]).split("(")[0]
+
+
+def test_source_end_step():
+    from openem_b200 import shutoff
+    sc = scenes.slab_plane_wave(nxy=1, num_steps=3000)
+    end = shutoff.source_end_step(sc)
+    a = np.abs(sc.sources[0].waveform.amp_int)
+    assert a[end] > 1e-3 * a.max() and np.all(a[end + 1:] <= 1e-3 * a.max())
