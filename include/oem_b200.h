@@ -157,6 +157,22 @@ int oem_plan_write_field(oem_plan* p, int comp, const float* in, void* stream);
  * out[2] = sum V |H|^2, with each component's own Yee dual volume. Synchronous. */
 int oem_plan_energy(oem_plan* p, double out[3], void* stream);
 
+/* Field sums for callers that cannot allocate device memory. This entry point has no
+ * counterpart in OpenEM; it is the allocation-free form of oem_plan_energy, for code that owns
+ * its fields in another framework's memory pool or must not let cudaMalloc synchronise the
+ * device in its step loop. Inputs: six fp32 field arrays (device pointers, (nx, ny, nzp) with
+ * z padded to nzp >= nz), three fp32 relative-permittivity arrays in the same layout (or NULL
+ * for 1), and the host array `spacing` of 2*(nx+ny+nz) doubles: primal then dual spacing of x,
+ * then of y, then of z. Output: out[0] = sum V|E|^2, out[1] = sum V eps|E|^2,
+ * out[2] = sum V|H|^2 with each component's Yee dual volume; synchronous on `stream`.
+ * It allocates nothing: its only scratch is a file-scope device array of 581 KB (held on every
+ * GPU that loads the library until exit), so nx + ny + nz is limited to 32768. The first call
+ * on a device looks that array up (cudaGetSymbolAddress) and should come before any stream
+ * capture. All calls share the array: calls that overlap on the GPU race. */
+int oem_field_energy_noalloc(const float* const fields[6], const float* const eps[3], int nx,
+                             int ny, int nz, int nzp, const double* spacing, double out[3],
+                             void* stream);
+
 /* Device pointers of the six field arrays (padded layout) and the padded z pitch, for
  * zero-copy interop with array libraries. */
 int oem_plan_field_ptrs(oem_plan* p, void* ptrs[6], int* nzp);

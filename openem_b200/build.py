@@ -19,7 +19,8 @@ PKG = pathlib.Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "liboem_b200.so"
-SOURCES = ["oem_api.cu", "oem_kernels.cu", "oem_yee_stream.cu", "oem_yee_tma.cu"]
+SOURCES = ["oem_api.cu", "oem_kernels.cu", "oem_yee_stream.cu", "oem_yee_tma.cu",
+           "oem_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

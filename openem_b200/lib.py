@@ -51,6 +51,7 @@ SIGNATURES = {
     "oem_plan_write_field": (_I, [_P, _I, _P, _P]),
     "oem_plan_energy": (_I, [_P, _P, _P]),
     "oem_plan_field_ptrs": (_I, [_P, _P, C.POINTER(_I)]),
+    "oem_field_energy_noalloc": (_I, [_P, _P, _I, _I, _I, _I, _P, _P, _P]),
     "oem_plan_enable_timing": (_I, [_P, _I]),
     "oem_plan_timing": (_I, [_P, _I, _P, _P, _P, C.POINTER(_I)]),
 }
