@@ -137,12 +137,15 @@ static int alloc_psi(oem_plan* p) {
 static cudaError_t run_h(oem_plan* p, cudaStream_t s) {
   if (p->basic_kernels == 1) return launch_update_h(p->yp, s);
   if (p->basic_kernels == 2) return launch_update_h_stream(p->yp, p->xch, s);
+  if (p->basic_kernels == 3) return launch_update_h_ws(p->tma, p->yp, p->xch, p->d_err, s);
   return launch_update_h_tma(p->tma, p->yp, p->xch, p->d_err, s);
 }
 
 static cudaError_t run_e(oem_plan* p, cudaStream_t s) {
   if (p->basic_kernels == 1) return launch_update_e(p->yp, s);
   if (p->basic_kernels == 2) return launch_update_e_stream(p->yp, p->xch, (int)p->mats.size(), s);
+  if (p->basic_kernels == 3)
+    return launch_update_e_ws(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s);
   return launch_update_e_tma(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s);
 }
 
@@ -294,9 +297,11 @@ int oem_plan_create(int device, int nx, int ny, int nz, double ch, double cw, oe
   p->ch = ch;
   p->cw = cw;
   const char* kind = getenv("OEM_B200_KERNELS");
-  p->basic_kernels = 0;
+  p->basic_kernels = 3;  // warp-specialised TMA kernels unless asked otherwise
   if (kind && strcmp(kind, "basic") == 0) p->basic_kernels = 1;
   if (kind && strcmp(kind, "stream") == 0) p->basic_kernels = 2;
+  if (kind && strcmp(kind, "ws") == 0) p->basic_kernels = 3;
+  if (kind && strcmp(kind, "tma") == 0) p->basic_kernels = 0;
   *out = p;
   return OEM_OK;
 }
@@ -740,27 +745,33 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
     } else if ((rc = dupload(p, &dseg, p->seg_ofs.data(), p->seg_ofs.size()))) {
       return rc;
     }
-    if ((rc = dalloc(p, &dP, (size_t)std::max<int64_t>(p->n_pole_total, 1)))) return rc;
+    // four float2 of slack: bulk copies of a row's poles are widened to 16-byte boundaries
+    if ((rc = dalloc(p, &dP, (size_t)std::max<int64_t>(p->n_pole_total, 1) + 4))) return rc;
     P.pcoef = dc;
     P.pset_ofs = dofs;
     P.seg_ofs = dseg;
     P.P = dP;
+    P.n_pole_total = (uint32_t)p->n_pole_total;
+    P.n_coef = (int)(p->pcoef.size() / 4);
+    P.n_sets = (int)p->pset_ofs.size() - 1;
     P.has_ade = 1;
   }
   if ((rc = dalloc(p, &p->d_step, 1))) return rc;
   if ((rc = dalloc(p, &p->d_err, 1))) return rc;
-  p->xch = p->basic_kernels == 2 ? stream_xchunk(P) : tma_xchunk(P);
-  if (p->basic_kernels == 0) {
+  p->xch = p->basic_kernels == 2 ? stream_xchunk(P)
+                                  : (p->basic_kernels == 3 ? ws_xchunk(P) : tma_xchunk(P));
+  if (p->basic_kernels == 0 || p->basic_kernels == 3) {
     // grids the tensor-map encoder refuses run on the register-streaming kernels
     if (make_tma_maps(p) != OEM_OK) {
       p->basic_kernels = 2;
       p->xch = stream_xchunk(P);
     } else {
-      cudaError_t e = tma_setup_kernels();
+      cudaError_t e = p->basic_kernels == 3 ? ws_setup_kernels() : tma_setup_kernels();
       if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
     }
   }
   if (const char* xs = getenv("OEM_B200_XCHUNK")) p->xch = std::max(1, atoi(xs));
+  if (p->basic_kernels == 3) p->xch = std::min(p->xch, ws_max_xchunk());
   p->energy_blocks = energy_block_count(P);
   if ((rc = dalloc(p, &p->d_energy_part, 3 * (size_t)p->energy_blocks))) return rc;
   // capture: G steps per graph for small grids (launch overhead), 1 for large ones

@@ -83,6 +83,9 @@ struct YeeParams {
   const float4* pcoef;     // per pole of a set: (Re(A-1), Im(A-1), Re(B), Im(B))
   const int* pset_ofs;     // set -> first pole in pcoef
   const uint32_t* seg_ofs; // poles stored before each 32-cell segment
+  uint32_t n_pole_total;
+  int n_coef;              // entries of pcoef
+  int n_sets;              // pole sets (pset_ofs holds n_sets + 1 entries)
   int has_ade;
 };
 
@@ -200,7 +203,7 @@ struct oem_plan {
   uint32_t* dev_mat32 = nullptr;
   uint32_t* dev_seg = nullptr;   // segment offsets uploaded from device memory
 
-  int basic_kernels = 0;  // 1: one-thread-per-cell kernels, 2: register-streaming, 0: TMA
+  int basic_kernels = 3;  // 3: warp-specialised (default), 0: TMA, 1: one-thread-per-cell, 2: register-streaming
   oem::TmaMaps tma{};
   int* d_err = nullptr;   // set by a kernel whose bounded wait gave up
   int xch = 8;            // x planes per thread in the streaming kernels
@@ -264,6 +267,13 @@ cudaError_t launch_pad_index(const void* in, int in_bytes, uint16_t* out16, uint
                              int nx, int ny, int nz, int nzp, uint32_t n_mat, unsigned* bad,
                              cudaStream_t s);
 cudaError_t launch_update_h_stream(const YeeParams& P, int xch, cudaStream_t s);
+int ws_xchunk(const YeeParams& P);
+int ws_max_xchunk();
+cudaError_t ws_setup_kernels();
+cudaError_t launch_update_h_ws(const TmaMaps& maps, const YeeParams& P, int xch, int* err,
+                               cudaStream_t s);
+cudaError_t launch_update_e_ws(const TmaMaps& maps, const YeeParams& P, int xch, int n_mats,
+                               int* err, cudaStream_t s);
 cudaError_t launch_update_e_stream(const YeeParams& P, int xch, int n_mats, cudaStream_t s);
 cudaError_t launch_energy(const YeeParams& P, double* const dl[3][2], double* part, int nblocks,
                           cudaStream_t s);

@@ -20,6 +20,7 @@
 #include <algorithm>
 
 #include "oem_internal.cuh"
+#include "oem_arith.cuh"
 
 namespace oem {
 
@@ -50,9 +51,7 @@ __device__ __forceinline__ float* psi_at(const PsiSet& S, int a, int slot, const
 // Outside the slabs the coefficients are the identity and psi is identically zero.
 __device__ __forceinline__ float stretch(float d, float* psi, float a, float b, float ik) {
   if (psi == nullptr) return d;
-  const float p = b * (*psi) + a * d;
-  *psi = p;
-  return ik * d + p;
+  return cpml_stretch(d, *psi, a, b, ik);
 }
 
 __device__ __forceinline__ uint32_t mat_id(const YeeParams& P, int64_t id) {
@@ -68,14 +67,8 @@ __device__ __forceinline__ float ade(const YeeParams& P, int set, int np, uint32
   for (int t = 0; t < np; ++t) {
     const float4 c = __ldg(cf + t);
     float2 st = P.P[poff + t];
-    const float pr = st.x + c.z * en;
-    const float pi = st.y + c.w * en;
-    const float dr = c.x * pr - c.y * pi + c.z * en;
-    const float di = c.x * pi + c.y * pr + c.w * en;
-    st.x = pr + dr;
-    st.y = pi + di;
+    w = __fadd_rn(w, ade_pole(st, c, en));
     P.P[poff + t] = st;
-    w += 2.0f * dr;
   }
   return w;
 }
@@ -102,25 +95,25 @@ __global__ void __launch_bounds__(128) k_update_h(YeeParams P) {
   const int64_t idk = i * si + j * sj + kp;
   const float ch = P.ch;
   {  // Hx: mu0 dHx/dt = -(dEz/dy - dEy/dz)
-    const float dzy = (Ez[idj] * mj - ez) * Y.idl_p[j];
-    const float dyz = (Ey[idk] * mk - ey) * Z.idl_p[k];
+    const float dzy = fdiff(Ez[idj], mj, ez, Y.idl_p[j]);
+    const float dyz = fdiff(Ey[idk], mk, ey, Z.idl_p[k]);
     const float sy = stretch(dzy, psi_at(P.psih, 1, 0, Y, i, j, k, P.ny, P.nzp), Y.ah[j], Y.bh[j], Y.kh[j]);
     const float sz = stretch(dyz, psi_at(P.psih, 2, 0, Z, i, j, k, P.ny, P.nzp), Z.ah[k], Z.bh[k], Z.kh[k]);
-    P.f[3][id] -= ch * (sy - sz);
+    P.f[3][id] = h_new(P.f[3][id], ch, sy, sz);
   }
   {  // Hy: mu0 dHy/dt = -(dEx/dz - dEz/dx)
-    const float dxz = (Ex[idk] * mk - ex) * Z.idl_p[k];
-    const float dzx = (Ez[idi] * mi - ez) * X.idl_p[i];
+    const float dxz = fdiff(Ex[idk], mk, ex, Z.idl_p[k]);
+    const float dzx = fdiff(Ez[idi], mi, ez, X.idl_p[i]);
     const float sz = stretch(dxz, psi_at(P.psih, 2, 1, Z, i, j, k, P.ny, P.nzp), Z.ah[k], Z.bh[k], Z.kh[k]);
     const float sx = stretch(dzx, psi_at(P.psih, 0, 0, X, i, j, k, P.ny, P.nzp), X.ah[i], X.bh[i], X.kh[i]);
-    P.f[4][id] -= ch * (sz - sx);
+    P.f[4][id] = h_new(P.f[4][id], ch, sz, sx);
   }
   {  // Hz: mu0 dHz/dt = -(dEy/dx - dEx/dy)
-    const float dyx = (Ey[idi] * mi - ey) * X.idl_p[i];
-    const float dxy = (Ex[idj] * mj - ex) * Y.idl_p[j];
+    const float dyx = fdiff(Ey[idi], mi, ey, X.idl_p[i]);
+    const float dxy = fdiff(Ex[idj], mj, ex, Y.idl_p[j]);
     const float sx = stretch(dyx, psi_at(P.psih, 0, 1, X, i, j, k, P.ny, P.nzp), X.ah[i], X.bh[i], X.kh[i]);
     const float sy = stretch(dxy, psi_at(P.psih, 1, 1, Y, i, j, k, P.ny, P.nzp), Y.ah[j], Y.bh[j], Y.kh[j]);
-    P.f[5][id] -= ch * (sx - sy);
+    P.f[5][id] = h_new(P.f[5][id], ch, sx, sy);
   }
 }
 
@@ -160,30 +153,30 @@ __global__ void __launch_bounds__(128) k_update_e(YeeParams P) {
   {  // Ex: eps dEx/dt = dHz/dy - dHy/dz
     const float en = P.f[0][id];
     const float w = (M.np[0] > 0) ? ade(P, M.pset[0], M.np[0], poff, en) : 0.0f;
-    const float dzy = (hz - Hz[idj] * mj) * Y.idl_d[j];
-    const float dyz = (hy - Hy[idk] * mk) * Z.idl_d[k];
+    const float dzy = bdiff(hz, Hz[idj], mj, Y.idl_d[j]);
+    const float dyz = bdiff(hy, Hy[idk], mk, Z.idl_d[k]);
     const float sy = stretch(dzy, psi_at(P.psie, 1, 0, Y, i, j, k, P.ny, P.nzp), Y.ae[j], Y.be[j], Y.ke[j]);
     const float sz = stretch(dyz, psi_at(P.psie, 2, 0, Z, i, j, k, P.ny, P.nzp), Z.ae[k], Z.be[k], Z.ke[k]);
-    P.f[0][id] = M.ca[0] * en + M.cb[0] * (sy - sz - cw * w);
+    P.f[0][id] = e_new(M.ca[0], en, M.cb[0], sy, sz, cw, w);
   }
   {  // Ey: eps dEy/dt = dHx/dz - dHz/dx
     const float en = P.f[1][id];
     const float w = (M.np[1] > 0) ? ade(P, M.pset[1], M.np[1], poff + M.np[0], en) : 0.0f;
-    const float dxz = (hx - Hx[idk] * mk) * Z.idl_d[k];
-    const float dzx = (hz - Hz[idi] * mi) * X.idl_d[i];
+    const float dxz = bdiff(hx, Hx[idk], mk, Z.idl_d[k]);
+    const float dzx = bdiff(hz, Hz[idi], mi, X.idl_d[i]);
     const float sz = stretch(dxz, psi_at(P.psie, 2, 1, Z, i, j, k, P.ny, P.nzp), Z.ae[k], Z.be[k], Z.ke[k]);
     const float sx = stretch(dzx, psi_at(P.psie, 0, 0, X, i, j, k, P.ny, P.nzp), X.ae[i], X.be[i], X.ke[i]);
-    P.f[1][id] = M.ca[1] * en + M.cb[1] * (sz - sx - cw * w);
+    P.f[1][id] = e_new(M.ca[1], en, M.cb[1], sz, sx, cw, w);
   }
   {  // Ez: eps dEz/dt = dHy/dx - dHx/dy
     const float en = P.f[2][id];
     const float w = (M.np[2] > 0)
                         ? ade(P, M.pset[2], M.np[2], poff + M.np[0] + M.np[1], en) : 0.0f;
-    const float dyx = (hy - Hy[idi] * mi) * X.idl_d[i];
-    const float dxy = (hx - Hx[idj] * mj) * Y.idl_d[j];
+    const float dyx = bdiff(hy, Hy[idi], mi, X.idl_d[i]);
+    const float dxy = bdiff(hx, Hx[idj], mj, Y.idl_d[j]);
     const float sx = stretch(dyx, psi_at(P.psie, 0, 1, X, i, j, k, P.ny, P.nzp), X.ae[i], X.be[i], X.ke[i]);
     const float sy = stretch(dxy, psi_at(P.psie, 1, 1, Y, i, j, k, P.ny, P.nzp), Y.ae[j], Y.be[j], Y.ke[j]);
-    P.f[2][id] = M.ca[2] * en + M.cb[2] * (sx - sy - cw * w);
+    P.f[2][id] = e_new(M.ca[2], en, M.cb[2], sx, sy, cw, w);
   }
 }
 

@@ -14,6 +14,7 @@
 #include <stdint.h>
 
 #include "oem_internal.cuh"
+#include "oem_arith.cuh"
 
 namespace oem {
 
@@ -193,14 +194,8 @@ __device__ __forceinline__ float ade_cell(const YeeParams& P, int set, int np, u
   for (int t = 0; t < np; ++t) {
     const float4 c = __ldg(cf + t);
     float2 st = P.P[poff + t];
-    const float pr = st.x + c.z * en;
-    const float pi = st.y + c.w * en;
-    const float dr = c.x * pr - c.y * pi + c.z * en;
-    const float di = c.x * pi + c.y * pr + c.w * en;
-    st.x = pr + dr;
-    st.y = pi + di;
+    w = __fadd_rn(w, ade_pole(st, c, en));
     P.P[poff + t] = st;
-    w += 2.0f * dr;
   }
   return w;
 }
@@ -327,7 +322,7 @@ __global__ void __launch_bounds__(128) k_e_stream(YeeParams P, int xch, int smem
         const float dyz = (hy.v[e] - zhy[e] * mkz[e]) * idz[e];
         const float sy = ysl ? stretch_slab(dzy, psi_slab(P.psie, 1, 0, Y, i, j, k, P.ny, P.nzp), ay, by, ky) : dzy;
         const float sz = zsl[e] ? stretch_slab(dyz, psi_slab(P.psie, 2, 0, Z, i, j, k, P.ny, P.nzp), az[e], bz[e], kz[e]) : dyz;
-        ex.v[e] = cab.x * en + cab.w * (sy - sz - cw * w);
+        ex.v[e] = e_new(cab.x, en, cab.w, sy, sz, cw, w);
       }
       {  // Ey: dHx/dz - dHz/dx
         const float en = ey.v[e];
@@ -337,7 +332,7 @@ __global__ void __launch_bounds__(128) k_e_stream(YeeParams P, int xch, int smem
         const float dzx = (hz.v[e] - phz.v[e] * mi) * idx_;
         const float sz = zsl[e] ? stretch_slab(dxz, psi_slab(P.psie, 2, 1, Z, i, j, k, P.ny, P.nzp), az[e], bz[e], kz[e]) : dxz;
         const float sx = xsl ? stretch_slab(dzx, psi_slab(P.psie, 0, 0, X, i, j, k, P.ny, P.nzp), ax_, bx_, kx_) : dzx;
-        ey.v[e] = cab.y * en + cb12.x * (sz - sx - cw * w);
+        ey.v[e] = e_new(cab.y, en, cb12.x, sz, sx, cw, w);
       }
       {  // Ez: dHy/dx - dHx/dy
         const float en = ez.v[e];
@@ -347,7 +342,7 @@ __global__ void __launch_bounds__(128) k_e_stream(YeeParams P, int xch, int smem
         const float dxy = (hx.v[e] - yhx.v[e] * mj) * idy;
         const float sx = xsl ? stretch_slab(dyx, psi_slab(P.psie, 0, 1, X, i, j, k, P.ny, P.nzp), ax_, bx_, kx_) : dyx;
         const float sy = ysl ? stretch_slab(dxy, psi_slab(P.psie, 1, 1, Y, i, j, k, P.ny, P.nzp), ay, by, ky) : dxy;
-        ez.v[e] = cab.z * en + cb12.y * (sx - sy - cw * w);
+        ez.v[e] = e_new(cab.z, en, cb12.y, sx, sy, cw, w);
       }
       poff += (uint32_t)np;
     }

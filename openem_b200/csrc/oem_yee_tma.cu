@@ -20,6 +20,7 @@
 #include <stdint.h>
 
 #include "oem_internal.cuh"
+#include "oem_arith.cuh"
 
 namespace oem {
 
@@ -324,14 +325,8 @@ __device__ __forceinline__ float ade_cell(const YeeParams& P, int set, int np, u
   for (int t = 0; t < np; ++t) {
     const float4 c = __ldg(cf + t);
     float2 st = P.P[poff + t];
-    const float pr = st.x + c.z * en;
-    const float pi = st.y + c.w * en;
-    const float dr = c.x * pr - c.y * pi + c.z * en;
-    const float di = c.x * pi + c.y * pr + c.w * en;
-    st.x = pr + dr;
-    st.y = pi + di;
+    w = __fadd_rn(w, ade_pole(st, c, en));
     P.P[poff + t] = st;
-    w += 2.0f * dr;
   }
   return w;
 }
@@ -508,7 +503,7 @@ __global__ void __launch_bounds__(128) k_e_tma(const __grid_constant__ TmaMaps m
           const float dyz = (hye - zhy * mkz[e]) * idz[e];
           const float sy = ysl ? stretch_reg(dzy, py0.v[e], ay, by, ky) : dzy;
           const float sz = zsl[e] ? stretch_slab(dyz, psi_slab(P.psie, 2, 0, Z, i, j, k, P.ny, P.nzp), az[e], bz[e], kz[e]) : dyz;
-          ex[e] = cab.x * en + cab.w * (sy - sz - cw * wv);
+          ex[e] = e_new(cab.x, en, cab.w, sy, sz, cw, wv);
         }
         {  // Ey: dHx/dz - dHz/dx
           const float en = ey[e];
@@ -518,7 +513,7 @@ __global__ void __launch_bounds__(128) k_e_tma(const __grid_constant__ TmaMaps m
           const float dzx = (hze - comp4(phz, e) * mi) * idx_;
           const float sz = zsl[e] ? stretch_slab(dxz, psi_slab(P.psie, 2, 1, Z, i, j, k, P.ny, P.nzp), az[e], bz[e], kz[e]) : dxz;
           const float sx = xsl ? stretch_reg(dzx, px0.v[e], ax_, bx_, kx_) : dzx;
-          ey[e] = cab.y * en + cb12.x * (sz - sx - cw * wv);
+          ey[e] = e_new(cab.y, en, cb12.x, sz, sx, cw, wv);
         }
         {  // Ez: dHy/dx - dHx/dy
           const float en = ez[e];
@@ -528,7 +523,7 @@ __global__ void __launch_bounds__(128) k_e_tma(const __grid_constant__ TmaMaps m
           const float dxy = (hxe - comp4(yhx, e) * mj) * idy;
           const float sx = xsl ? stretch_reg(dyx, px1.v[e], ax_, bx_, kx_) : dyx;
           const float sy = ysl ? stretch_reg(dxy, py1.v[e], ay, by, ky) : dxy;
-          ez[e] = cab.z * en + cb12.y * (sx - sy - cw * wv);
+          ez[e] = e_new(cab.z, en, cb12.y, sx, sy, cw, wv);
         }
         poff += (uint32_t)np;
       }

@@ -1,0 +1,933 @@
+// Warp-specialised, fully asynchronous Yee kernels for sm_100a (the default step kernels).
+//
+// A block owns a 128 (z) x 4 (y) tile and walks a chunk of x planes. Warp 4 is the producer:
+// its lane 0 stages everything one plane needs into a 3-deep shared-memory ring -- field tiles
+// with cp.async.bulk.tensor (TMA), the CPML psi rows of slab cells and the ADE pole states of a
+// row with 1D cp.async.bulk copies -- ahead of the four consumer warps, one per tile row, four z
+// cells per lane. A stage is published by a "full" mbarrier (producer arrival + transaction
+// bytes) and recycled through an "empty" mbarrier that each consumer warp arrives on once it is
+// done with it. Consumers issue no synchronous global load except for the rare boundary cells
+// whose neighbour is not the adjacent index (periodic wrap, PMC, symmetry) and pole rows that
+// do not fit the stage's pole window; they write H/E, psi and the pole states straight back.
+//
+// Every mbarrier wait is bounded (2^20 polls); a wait that gives up sets *err, stops the
+// issuing side and the waiting side, and the producer drains what it issued (again bounded).
+//
+// The arithmetic per cell is that of the basic kernels (openem/kernels/yee.cu:60-240,
+// dispersion.cu:168-207).
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "oem_internal.cuh"
+#include "oem_arith.cuh"
+
+namespace oem {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kTY = 4;
+constexpr int kTZ = 128;
+constexpr int kBZ = 136;
+constexpr int kS = 3;
+constexpr int kBoxW = 704;                      // floats per 136 x 5 halo-box slot (128-B aligned)
+constexpr uint32_t kWideBytes = 5 * kBZ * 4;    // bytes a halo box transfers
+constexpr uint32_t kTileBytes = kTY * kTZ * 4;  // bytes a 128 x 4 tile transfers
+constexpr int kZMax = 32;                       // z-slab depths staged when <= this and % 4 == 0
+constexpr int kSmemMats = 64;
+constexpr int kXMax = 64;                       // x planes per block (segment table size)
+constexpr int kSmemCoef = 64;                   // pole coefficients kept in shared memory
+constexpr int kSmemSets = 32;
+
+// H kernel stage (floats)
+constexpr int kH_EB = 0;                  // E halo box x3
+constexpr int kH_EN = kH_EB + 3 * kBoxW;  // E tile of the x-neighbour plane x3
+constexpr int kH_HT = kH_EN + 3 * 512;    // H tile x3
+constexpr int kH_PX = kH_HT + 3 * 512;    // psi x-slab rows [2][4][128]
+constexpr int kH_PY = kH_PX + 1024;       // psi y-slab rows [2][4][128]
+constexpr int kH_PZ = kH_PY + 1024;       // psi z-slab rows [2 slots][2 sides][4 x depth]
+constexpr int kHStage = kH_PZ + 512;
+// E kernel stage (32-bit words)
+constexpr int kE_HB = 0;                  // H halo box x3 (rows j0-1.., cols k0-4..)
+constexpr int kE_HP = kE_HB + 3 * kBoxW;  // Hy, Hz tiles of the previous plane
+constexpr int kE_ET = kE_HP + 2 * 512;    // E tile x3
+constexpr int kE_MT = kE_ET + 3 * 512;    // material tile (uint16 or uint32)
+// A per-plane pool: the psi rows the plane needs (x rows 1024 floats, y rows 1024, z rows 512,
+// each only when present), then the pole-state window in the rest.
+constexpr int kE_POOL = kE_MT + 512;
+constexpr int kEPool = 3328;
+constexpr int kE_PT = kE_POOL + kEPool;   // [2r]: pole start of row r, [2r+1]: window offset,
+                                          // [8..10]: psi x/y/z offsets, [11]: window start
+constexpr int kEStage = kE_PT + 32;
+static_assert((kHStage * 4) % 128 == 0 && (kEStage * 4) % 128 == 0, "stage alignment");
+static_assert((kH_EN * 4) % 128 == 0 && (kH_HT * 4) % 128 == 0 && (kH_PX * 4) % 128 == 0 &&
+                  (kH_PY * 4) % 128 == 0 && (kH_PZ * 4) % 128 == 0,
+              "H slots aligned");
+static_assert((kE_HP * 4) % 128 == 0 && (kE_ET * 4) % 128 == 0 && (kE_MT * 4) % 128 == 0 &&
+                  (kE_POOL * 4) % 128 == 0 && (kE_PT * 4) % 128 == 0,
+              "E slots aligned");
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+  for (uint32_t it = 0; it < (1u << 20); ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicExch(err, 1);
+  return false;
+}
+__device__ __forceinline__ void tma3(void* dst, const CUtensorMap* map, uint64_t* bar, int c0,
+                                     int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+// 1D bulk copy global -> shared; both addresses 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool in_slab(const DevAxis& A, int q) {
+  return q < A.lo || q >= A.n - A.hi;
+}
+
+// Global address of the psi row (4 consecutive cells at k) of slab array (a, slot).
+__device__ __forceinline__ float* psi_addr(const PsiSet& S, int a, int slot, const DevAxis& A,
+                                          int i, int j, int k, int ny, int nzp) {
+  const int q = (a == 0) ? i : ((a == 1) ? j : k);
+  int side, ql, L;
+  if (q < A.lo) {
+    side = 0; ql = q; L = A.lo;
+  } else {
+    side = 1; ql = q - (A.n - A.hi); L = A.hi;
+  }
+  float* base = S.p[a][slot][side];
+  int64_t idx;
+  if (a == 0) idx = ((int64_t)ql * ny + j) * nzp + k;
+  else if (a == 1) idx = ((int64_t)i * L + ql) * nzp + k;
+  else idx = ((int64_t)i * ny + j) * L + ql;
+  return base + idx;
+}
+
+__device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+
+// Does the tile's z range [k0, k0+128) overlap the z slab of side `side`, with stageable depth?
+__device__ __forceinline__ bool zslab_staged(const DevAxis& Z, int side, int k0) {
+  const int L = side ? Z.hi : Z.lo;
+  if (L <= 0 || L > kZMax || (L & 3)) return false;
+  return side ? (k0 + kTZ > Z.n - L && k0 < Z.n) : (k0 < L);
+}
+
+// Producer helper: issue the psi rows of plane i for one field family into a stage.
+// Returns the bytes issued.
+__device__ uint32_t stage_psi(const PsiSet& S, const YeeParams& P, float* px, float* py,
+                              float* pz, uint64_t* bar, int i, int j0, int k0) {
+  const DevAxis& X = P.ax[0];
+  const DevAxis& Y = P.ax[1];
+  const DevAxis& Z = P.ax[2];
+  const uint32_t rowb = (uint32_t)min(kTZ, P.nzp - k0) * 4;
+  uint32_t bytes = 0;
+  const bool xsl = in_slab(X, i);
+  for (int r = 0; r < kTY; ++r) {
+    const int j = j0 + r;
+    if (j >= P.ny) break;
+    if (xsl)
+      for (int s = 0; s < 2; ++s) {
+        bulk(px + (s * 4 + r) * kTZ, psi_addr(S, 0, s, X, i, j, k0, P.ny, P.nzp), rowb, bar);
+        bytes += rowb;
+      }
+    if (in_slab(Y, j))
+      for (int s = 0; s < 2; ++s) {
+        bulk(py + (s * 4 + r) * kTZ, psi_addr(S, 1, s, Y, i, j, k0, P.ny, P.nzp), rowb, bar);
+        bytes += rowb;
+      }
+  }
+  // z slabs: the rows of the tile are adjacent in memory, one copy per (slot, side)
+  const int nrows = min(kTY, P.ny - j0);
+  for (int side = 0; side < 2; ++side) {
+    if (!zslab_staged(Z, side, k0)) continue;
+    const int L = side ? Z.hi : Z.lo;
+    const int kk = side ? Z.n - L : 0;
+    for (int s = 0; s < 2; ++s) {
+      bulk(pz + (s * 2 + side) * kTY * kZMax, psi_addr(S, 2, s, Z, i, j0, kk, P.ny, P.nzp),
+           (uint32_t)(nrows * L) * 4, bar);
+      bytes += (uint32_t)(nrows * L) * 4;
+    }
+  }
+  return bytes;
+}
+
+// Bytes stage_psi would issue (the producer arms the barrier before issuing).
+__device__ uint32_t psi_bytes(const YeeParams& P, int i, int j0, int k0) {
+  const DevAxis& X = P.ax[0];
+  const DevAxis& Y = P.ax[1];
+  const DevAxis& Z = P.ax[2];
+  const uint32_t rowb = (uint32_t)min(kTZ, P.nzp - k0) * 4;
+  uint32_t bytes = 0;
+  const bool xsl = in_slab(X, i);
+  for (int r = 0; r < kTY; ++r) {
+    const int j = j0 + r;
+    if (j >= P.ny) break;
+    if (xsl) bytes += 2 * rowb;
+    if (in_slab(Y, j)) bytes += 2 * rowb;
+  }
+  const int nrows = min(kTY, P.ny - j0);
+  for (int side = 0; side < 2; ++side)
+    if (zslab_staged(Z, side, k0)) bytes += 2u * (uint32_t)(nrows * (side ? Z.hi : Z.lo)) * 4;
+  return bytes;
+}
+
+// Offsets (floats) of the psi rows of plane i in the E kernel's pool, -1 where absent; returns
+// the floats they take (a multiple of 512, so the pole window after them stays aligned).
+__device__ int psi_pool_layout(const YeeParams& P, int i, int j0, int k0, int offs[3]) {
+  int cur = 0;
+  offs[0] = offs[1] = offs[2] = -1;
+  if (in_slab(P.ax[0], i)) {
+    offs[0] = cur;
+    cur += 1024;
+  }
+  bool y = false;
+#pragma unroll
+  for (int r = 0; r < kTY; ++r) y |= (j0 + r < P.ny) && in_slab(P.ax[1], j0 + r);
+  if (y) {
+    offs[1] = cur;
+    cur += 1024;
+  }
+  if (zslab_staged(P.ax[2], 0, k0) || zslab_staged(P.ax[2], 1, k0)) {
+    offs[2] = cur;
+    cur += 512;
+  }
+  return cur;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Shared consumer helpers
+// ---------------------------------------------------------------------------------------------
+
+// z coefficients of the block's 128 cells in shared memory: [0] 1/dl, [1] wall mask,
+// [2] CPML a, [3] CPML b, [4] CPML 1/kappa, [5] neighbour index (as int bits).
+constexpr int kZTab = 6 * kTZ;
+
+__device__ __forceinline__ void load_ztab(float* zt, const DevAxis& Z, bool h_side, int k0,
+                                          int nzp, int tid, int nthreads) {
+  for (int t = tid; t < kZTab; t += nthreads) {
+    const int c = t / kTZ;
+    const int k = k0 + (t - c * kTZ);
+    const int kk = k < nzp ? k : 0;
+    float v;
+    switch (c) {
+      case 0: v = h_side ? Z.idl_p[kk] : Z.idl_d[kk]; break;
+      case 1: v = h_side ? Z.mnx[kk] : Z.mpv[kk]; break;
+      case 2: v = h_side ? Z.ah[kk] : Z.ae[kk]; break;
+      case 3: v = h_side ? Z.bh[kk] : Z.be[kk]; break;
+      case 4: v = h_side ? Z.kh[kk] : Z.ke[kk]; break;
+      default: v = __int_as_float(h_side ? Z.nxt[kk] : Z.prv[kk]); break;
+    }
+    zt[t] = v;
+  }
+}
+
+__device__ __forceinline__ uint32_t mid_at(const float* mt, bool wide, int idx) {
+  return wide ? reinterpret_cast<const uint32_t*>(mt)[idx]
+              : (uint32_t)reinterpret_cast<const uint16_t*>(mt)[idx];
+}
+
+__device__ __forceinline__ void unpack4(const float4 v, float (&a)[4]) {
+  a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
+}
+
+// The poles of one cell: deferred ADE of its dispersive components, polarisation currents out.
+// ps/wp: the stage's pole window and this cell's first entry in it (-1: global memory).
+__device__ __forceinline__ void ade_cell(const YeeParams& P, const float4* coef,
+                                         const int* set_ofs, const MatRec& M, const float2* ps,
+                                         int wp, uint32_t gp, const float en[3], float wv[3]) {
+  int po = 0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    wv[c] = 0.f;
+    const int n = M.np[c];
+    if (n == 0) continue;
+    const float4* cf = coef + set_ofs[M.pset[c]];
+    float acc = 0.f;
+    for (int tt = 0; tt < n; ++tt) {
+      const uint32_t g = gp + (uint32_t)(po + tt);
+      float2 s2 = (wp >= 0) ? ps[wp + po + tt] : P.P[g];
+      acc = __fadd_rn(acc, ade_pole(s2, cf[tt], en[c]));
+      P.P[g] = s2;
+    }
+    wv[c] = acc;
+    po += n;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// H half step
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(160, 2) k_h_ws(const __grid_constant__ TmaMaps maps, YeeParams P,
+                                                 int xch, int* err) {
+  extern __shared__ __align__(128) float smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kS * kHStage);
+  uint64_t* empty = full + kS;
+  float* zt = reinterpret_cast<float*>(empty + kS);
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int k0 = blockIdx.x * kTZ;
+  const int j0 = blockIdx.y * kTY;
+  const int ib = blockIdx.z * xch;
+  const int ie = min(ib + xch, P.nx);
+  const int np = ie - ib;
+  const DevAxis& X = P.ax[0];
+  const DevAxis& Y = P.ax[1];
+  const DevAxis& Z = P.ax[2];
+  load_ztab(zt, Z, true, k0, P.nzp, w * 32 + lane, 160);
+  if (w == 4 && lane == 0) {
+    for (int s = 0; s < kS; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kTY);
+    }
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  if (w == 4) {  // ------------------------------------------------------------ producer
+    if (lane != 0) return;
+    int issued = 0;
+    bool ok = true;
+    for (int q = 0; q < np && ok; ++q) {
+      const int slot = q % kS;
+      if (q >= kS) ok = mbar_wait(&empty[slot], (uint32_t)((q / kS - 1) & 1), err);
+      if (!ok) break;
+      float* st = smem + slot * kHStage;
+      const int i = ib + q;
+      const int inext = (i + 1 < P.nx) ? i + 1 : X.nxt[P.nx - 1];
+      const uint32_t bytes = 3 * kWideBytes + 5 * kTileBytes + psi_bytes(P, i, j0, k0);
+      mbar_expect_tx(&full[slot], bytes);
+      for (int c = 0; c < 3; ++c) {
+        tma3(st + kH_EB + c * kBoxW, &maps.e_wide[c], &full[slot], k0, j0, i);
+        tma3(st + kH_HT + c * 512, &maps.h_tile[c], &full[slot], k0, j0, i);
+      }
+      // only Ey, Ez of the next plane enter the x derivatives
+      tma3(st + kH_EN + 512, &maps.e_tile[1], &full[slot], k0, j0, inext);
+      tma3(st + kH_EN + 1024, &maps.e_tile[2], &full[slot], k0, j0, inext);
+      stage_psi(P.psih, P, st + kH_PX, st + kH_PY, st + kH_PZ, &full[slot], i, j0, k0);
+      issued = q + 1;
+    }
+    for (int q = max(0, issued - kS); q < issued; ++q)  // drain (no-op when consumed)
+      mbar_wait(&full[q % kS], (uint32_t)((q / kS) & 1), err);
+    return;
+  }
+
+  // --------------------------------------------------------------------------- consumers
+  const int j = j0 + w;
+  const bool row_ok = j < P.ny;
+  const int jj = row_ok ? j : 0;
+  const int jp = Y.nxt[jj];
+  const float mj = Y.mnx[jj], idy = Y.idl_p[jj];
+  const bool ysl = row_ok && in_slab(Y, j);
+  const bool yspecial = row_ok && jp != j + 1;
+  const int kq = k0 + 4 * lane;
+  unsigned kvm = 0, zslm = 0, zspm = 0;
+  bool zunit = true;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int k = kq + e;
+    const bool kv = row_ok && k < P.nz;
+    kvm |= (unsigned)kv << e;
+    zslm |= (unsigned)(kv && in_slab(Z, k)) << e;
+    zspm |= (unsigned)(kv && __float_as_int(zt[5 * kTZ + 4 * lane + e]) != k + 1) << e;
+    zunit &= zt[kTZ + 4 * lane + e] == 1.0f;
+  }
+  // a plain row: every cell interior in y and z (adjacent neighbours, unit masks, no CPML)
+  const bool wplain = __all_sync(kFull, row_ok && !ysl && !yspecial && mj == 1.0f &&
+                                            kvm == 0xFu && zslm == 0u && zspm == 0u && zunit);
+  const int64_t sj = P.nzp, si = (int64_t)P.ny * P.nzp;
+  const float ch = P.ch;
+  const int ro = w * kBZ + 4 * lane;  // this quad in a halo box
+  const int to = w * kTZ + 4 * lane;  // this quad in a tile
+  for (int t = 0; t < np; ++t) {
+    const int slot = t % kS;
+    const bool got = mbar_wait(&full[slot], (uint32_t)((t / kS) & 1), err);
+    if (!__all_sync(kFull, got)) break;
+    const float* st = smem + slot * kHStage;
+    const int i = ib + t;
+    const bool xsl = in_slab(X, i);
+    const float mi = X.mnx[i], idx_ = X.idl_p[i];
+    const int64_t row = i * si + (int64_t)j * sj;
+    if (wplain && !xsl && i + 1 < P.nx && X.nxt[i] == i + 1 && mi == 1.0f) {
+      // interior fast path: fdiff with unit masks and no CPML, the same bits as below
+      float ex[4], ey[4], ez[4], yex[4], yez[4], ney[4], nez[4], hx[4], hy[4], hz[4], idz[4];
+      unpack4(lds4(st + kH_EB + ro), ex);
+      unpack4(lds4(st + kH_EB + kBoxW + ro), ey);
+      unpack4(lds4(st + kH_EB + 2 * kBoxW + ro), ez);
+      unpack4(lds4(st + kH_EB + ro + kBZ), yex);
+      unpack4(lds4(st + kH_EB + 2 * kBoxW + ro + kBZ), yez);
+      unpack4(lds4(st + kH_EN + 512 + to), ney);
+      unpack4(lds4(st + kH_EN + 1024 + to), nez);
+      unpack4(lds4(st + kH_HT + to), hx);
+      unpack4(lds4(st + kH_HT + 512 + to), hy);
+      unpack4(lds4(st + kH_HT + 1024 + to), hz);
+      unpack4(lds4(zt + 4 * lane), idz);
+      const float ex4 = st[kH_EB + ro + 4];
+      const float ey4 = st[kH_EB + kBoxW + ro + 4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float zex = (e < 3) ? ex[e + 1] : ex4;
+        const float zey = (e < 3) ? ey[e + 1] : ey4;
+        hx[e] = h_new(hx[e], ch, __fmul_rn(__fsub_rn(yez[e], ez[e]), idy),
+                      __fmul_rn(__fsub_rn(zey, ey[e]), idz[e]));
+        hy[e] = h_new(hy[e], ch, __fmul_rn(__fsub_rn(zex, ex[e]), idz[e]),
+                      __fmul_rn(__fsub_rn(nez[e], ez[e]), idx_));
+        hz[e] = h_new(hz[e], ch, __fmul_rn(__fsub_rn(ney[e], ey[e]), idx_),
+                      __fmul_rn(__fsub_rn(yex[e], ex[e]), idy));
+      }
+      *reinterpret_cast<float4*>(P.f[3] + row + kq) = make_float4(hx[0], hx[1], hx[2], hx[3]);
+      *reinterpret_cast<float4*>(P.f[4] + row + kq) = make_float4(hy[0], hy[1], hy[2], hy[3]);
+      *reinterpret_cast<float4*>(P.f[5] + row + kq) = make_float4(hz[0], hz[1], hz[2], hz[3]);
+    } else if (kvm) {
+      const float ay = Y.ah[jj], by = Y.bh[jj], ky = Y.kh[jj];
+      const float ax_ = X.ah[i], bx_ = X.bh[i], kx_ = X.kh[i];
+      float ex[4], ey[4], ez[4], yex[4], yez[4], ney[4], nez[4], hx[4], hy[4], hz[4];
+      unpack4(lds4(st + kH_EB + ro), ex);
+      unpack4(lds4(st + kH_EB + kBoxW + ro), ey);
+      unpack4(lds4(st + kH_EB + 2 * kBoxW + ro), ez);
+      if (yspecial) {
+        const int64_t oy = i * si + (int64_t)jp * sj + kq;
+        unpack4(*reinterpret_cast<const float4*>(P.f[0] + oy), yex);
+        unpack4(*reinterpret_cast<const float4*>(P.f[2] + oy), yez);
+      } else {
+        unpack4(lds4(st + kH_EB + ro + kBZ), yex);
+        unpack4(lds4(st + kH_EB + 2 * kBoxW + ro + kBZ), yez);
+      }
+      unpack4(lds4(st + kH_EN + 512 + to), ney);
+      unpack4(lds4(st + kH_EN + 1024 + to), nez);
+      unpack4(lds4(st + kH_HT + to), hx);
+      unpack4(lds4(st + kH_HT + 512 + to), hy);
+      unpack4(lds4(st + kH_HT + 1024 + to), hz);
+      const float ex4 = st[kH_EB + ro + 4];
+      const float ey4 = st[kH_EB + kBoxW + ro + 4];
+      // psi of this quad (x: Hy, Hz; y: Hx, Hz; z: Hx, Hy)
+      float px[2][4], py[2][4], pz[2][4];
+      if (xsl)
+        for (int s = 0; s < 2; ++s) unpack4(lds4(st + kH_PX + (s * 4 + w) * kTZ + 4 * lane), px[s]);
+      if (ysl)
+        for (int s = 0; s < 2; ++s) unpack4(lds4(st + kH_PY + (s * 4 + w) * kTZ + 4 * lane), py[s]);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (!((zslm >> e) & 1u)) continue;
+        const int k = kq + e;
+        const int side = k < Z.lo ? 0 : 1;
+        const int zq = side ? k - (Z.n - Z.hi) : k;
+        const bool staged = zslab_staged(Z, side, k0);
+        for (int s = 0; s < 2; ++s)
+          pz[s][e] = staged ? st[kH_PZ + (s * 2 + side) * kTY * kZMax + w * (side ? Z.hi : Z.lo) + zq]
+                            : *psi_addr(P.psih, 2, s, Z, i, j, k, P.ny, P.nzp);
+      }
+      float idz4[4], mkz4[4];
+      unpack4(lds4(zt + 4 * lane), idz4);
+      unpack4(lds4(zt + kTZ + 4 * lane), mkz4);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (!((kvm >> e) & 1u)) continue;
+        const int zi = 4 * lane + e;
+        const float idz = idz4[e], mkz = mkz4[e];
+        const bool zsl = (zslm >> e) & 1u;
+        float zex = (e < 3) ? ex[e + 1] : ex4;
+        float zey = (e < 3) ? ey[e + 1] : ey4;
+        if ((zspm >> e) & 1u) {
+          const int kp = __float_as_int(zt[5 * kTZ + zi]);
+          zex = P.f[0][row + kp];
+          zey = P.f[1][row + kp];
+        }
+        const float az = zsl ? zt[2 * kTZ + zi] : 0.f;
+        const float bz = zsl ? zt[3 * kTZ + zi] : 0.f;
+        const float kz = zsl ? zt[4 * kTZ + zi] : 0.f;
+        {  // Hx: -(dEz/dy - dEy/dz)
+          const float dzy = fdiff(yez[e], mj, ez[e], idy);
+          const float dyz = fdiff(zey, mkz, ey[e], idz);
+          const float sy = ysl ? cpml_stretch(dzy, py[0][e], ay, by, ky) : dzy;
+          const float sz = zsl ? cpml_stretch(dyz, pz[0][e], az, bz, kz) : dyz;
+          hx[e] = h_new(hx[e], ch, sy, sz);
+        }
+        {  // Hy: -(dEx/dz - dEz/dx)
+          const float dxz = fdiff(zex, mkz, ex[e], idz);
+          const float dzx = fdiff(nez[e], mi, ez[e], idx_);
+          const float sz = zsl ? cpml_stretch(dxz, pz[1][e], az, bz, kz) : dxz;
+          const float sx = xsl ? cpml_stretch(dzx, px[0][e], ax_, bx_, kx_) : dzx;
+          hy[e] = h_new(hy[e], ch, sz, sx);
+        }
+        {  // Hz: -(dEy/dx - dEx/dy)
+          const float dyx = fdiff(ney[e], mi, ey[e], idx_);
+          const float dxy = fdiff(yex[e], mj, ex[e], idy);
+          const float sx = xsl ? cpml_stretch(dyx, px[1][e], ax_, bx_, kx_) : dyx;
+          const float sy = ysl ? cpml_stretch(dxy, py[1][e], ay, by, ky) : dxy;
+          hz[e] = h_new(hz[e], ch, sx, sy);
+        }
+      }
+      if (xsl)
+        for (int s = 0; s < 2; ++s)
+          *reinterpret_cast<float4*>(psi_addr(P.psih, 0, s, X, i, j, kq, P.ny, P.nzp)) =
+              make_float4(px[s][0], px[s][1], px[s][2], px[s][3]);
+      if (ysl)
+        for (int s = 0; s < 2; ++s)
+          *reinterpret_cast<float4*>(psi_addr(P.psih, 1, s, Y, i, j, kq, P.ny, P.nzp)) =
+              make_float4(py[s][0], py[s][1], py[s][2], py[s][3]);
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if ((zslm >> e) & 1u)
+          for (int s = 0; s < 2; ++s)
+            *psi_addr(P.psih, 2, s, Z, i, j, kq + e, P.ny, P.nzp) = pz[s][e];
+      *reinterpret_cast<float4*>(P.f[3] + row + kq) = make_float4(hx[0], hx[1], hx[2], hx[3]);
+      *reinterpret_cast<float4*>(P.f[4] + row + kq) = make_float4(hy[0], hy[1], hy[2], hy[3]);
+      *reinterpret_cast<float4*>(P.f[5] + row + kq) = make_float4(hz[0], hz[1], hz[2], hz[3]);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[slot]);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// E full step with the deferred ADE
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps maps, YeeParams P,
+                                                 int xch, int n_mats, int* err) {
+  extern __shared__ __align__(128) float smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kS * kEStage);
+  uint64_t* empty = full + kS;
+  float* zt = reinterpret_cast<float*>(empty + kS);
+  MatRec* smats = reinterpret_cast<MatRec*>(zt + kZTab);
+  uint32_t* segt = reinterpret_cast<uint32_t*>(smats + kSmemMats);  // [plane][row][start, end]
+  float4* scoef = reinterpret_cast<float4*>(segt + kXMax * kTY * 2);
+  int* sofs = reinterpret_cast<int*>(scoef + kSmemCoef);
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int tid = w * 32 + lane;
+  const int k0 = blockIdx.x * kTZ;
+  const int j0 = blockIdx.y * kTY;
+  const int ib = blockIdx.z * xch;
+  const int ie = min(ib + xch, P.nx);
+  const int np = ie - ib;
+  const DevAxis& X = P.ax[0];
+  const DevAxis& Y = P.ax[1];
+  const DevAxis& Z = P.ax[2];
+  const bool wide = P.mat32 != nullptr;
+  const MatRec* mats = P.mats;
+  if (n_mats <= kSmemMats) {
+    const uint4* src = reinterpret_cast<const uint4*>(P.mats);
+    uint4* dst = reinterpret_cast<uint4*>(smats);
+    for (int q = tid; q < n_mats * 4; q += 160) dst[q] = src[q];
+    mats = smats;
+  }
+  const float4* coef = P.pcoef;
+  const int* set_ofs = P.pset_ofs;
+  if (P.has_ade && P.n_coef <= kSmemCoef && P.n_sets < kSmemSets) {
+    for (int q = tid; q < P.n_coef; q += 160) scoef[q] = P.pcoef[q];
+    for (int q = tid; q <= P.n_sets; q += 160) sofs[q] = P.pset_ofs[q];
+    coef = scoef;
+    set_ofs = sofs;
+  }
+  load_ztab(zt, Z, false, k0, P.nzp, tid, 160);
+  if (w == 4 && lane == 0) {
+    for (int s = 0; s < kS; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kTY);
+    }
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  if (w == 4) {  // ------------------------------------------------------------ producer
+    // pole ranges of every (plane, row) of the chunk: the first pole of the tile row and the
+    // end of its last segment, all fetched at once by the producer warp
+    const int64_t nseg = (int64_t)P.nx * P.ny * P.nzp / 32;
+    const int nst = min(4, (P.nzp - k0) / 32);
+    if (P.has_ade) {
+      for (int t = lane; t < np * kTY; t += 32) {
+        const int i = ib + t / kTY, j = j0 + t % kTY;
+        uint32_t a = 0u, b = 0u;
+        if (j < P.ny) {
+          const int64_t s0 = (((int64_t)i * P.ny + j) * P.nzp + k0) >> 5;
+          a = __ldg(P.seg_ofs + s0);
+          b = (s0 + nst < nseg) ? __ldg(P.seg_ofs + s0 + nst) : P.n_pole_total;
+        }
+        segt[2 * t] = a;
+        segt[2 * t + 1] = b;
+      }
+      __syncwarp();
+    }
+    if (lane != 0) return;
+    int issued = 0;
+    bool ok = true;
+    const uint32_t mbytes = (uint32_t)(kTY * kTZ * (wide ? 4 : 2));
+    for (int q = 0; q < np && ok; ++q) {
+      const int slot = q % kS;
+      const int i = ib + q;
+      int offs[3];
+      const int wbase = psi_pool_layout(P, i, j0, k0, offs);
+      const int cap = (kEPool - wbase) / 2;  // float2 pole states this plane can stage
+      int pstart[kTY], poff[kTY], pcnt[kTY];
+      int used = 0;
+#pragma unroll
+      for (int r = 0; r < kTY; ++r) {
+        const uint32_t a = P.has_ade ? segt[2 * (q * kTY + r)] : 0u;
+        const uint32_t b = P.has_ade ? segt[2 * (q * kTY + r) + 1] : 0u;
+        pstart[r] = (int)a; poff[r] = -2; pcnt[r] = 0;
+        if (b <= a) continue;
+        const int a16 = (int)(a & ~1u);
+        const int n2 = (int)(((b - (uint32_t)a16) + 1u) & ~1u);
+        if (used + n2 <= cap) {
+          poff[r] = used + ((int)a - a16);
+          pcnt[r] = n2;
+          used += n2;
+        } else {
+          poff[r] = -1;  // consumers read this row's poles from global memory
+        }
+      }
+      if (q >= kS) ok = mbar_wait(&empty[slot], (uint32_t)((q / kS - 1) & 1), err);
+      if (!ok) break;
+      float* st = smem + slot * kEStage;
+      int* tab = reinterpret_cast<int*>(st + kE_PT);
+      const int iprev = (i > 0) ? i - 1 : X.prv[0];
+      uint32_t bytes = 3 * kWideBytes + 5 * kTileBytes + mbytes + psi_bytes(P, i, j0, k0) +
+                       (uint32_t)used * 8;
+#pragma unroll
+      for (int r = 0; r < kTY; ++r) {
+        tab[2 * r] = pstart[r];
+        tab[2 * r + 1] = poff[r];
+      }
+      tab[8] = offs[0];
+      tab[9] = offs[1];
+      tab[10] = offs[2];
+      tab[11] = wbase;
+      mbar_expect_tx(&full[slot], bytes);
+      for (int c = 0; c < 3; ++c) {
+        tma3(st + kE_HB + c * kBoxW, &maps.h_wide[c], &full[slot], k0 - 4, j0 - 1, i);
+        tma3(st + kE_ET + c * 512, &maps.e_tile[c], &full[slot], k0, j0, i);
+      }
+      tma3(st + kE_HP, &maps.h_tile[1], &full[slot], k0, j0, iprev);
+      tma3(st + kE_HP + 512, &maps.h_tile[2], &full[slot], k0, j0, iprev);
+      tma3(st + kE_MT, &maps.m_tile, &full[slot], k0, j0, i);
+      float* pool = st + kE_POOL;
+      stage_psi(P.psie, P, pool + offs[0], pool + offs[1], pool + offs[2], &full[slot], i, j0, k0);
+#pragma unroll
+      for (int r = 0; r < kTY; ++r)
+        if (pcnt[r] > 0) {
+          const int a16 = pstart[r] & ~1;
+          bulk(pool + wbase + 2 * (poff[r] - (pstart[r] - a16)), P.P + a16,
+               (uint32_t)pcnt[r] * 8, &full[slot]);
+        }
+      issued = q + 1;
+    }
+    for (int q = max(0, issued - kS); q < issued; ++q)
+      mbar_wait(&full[q % kS], (uint32_t)((q / kS) & 1), err);
+    return;
+  }
+
+  // --------------------------------------------------------------------------- consumers
+  const int j = j0 + w;
+  const bool row_ok = j < P.ny;
+  const int jj = row_ok ? j : 0;
+  const int jm = Y.prv[jj];
+  const float mj = Y.mpv[jj], idy = Y.idl_d[jj];
+  const bool ysl = row_ok && in_slab(Y, j);
+  const bool yspecial = row_ok && jm != j - 1;
+  const int kq = k0 + 4 * lane;
+  unsigned kvm = 0, zslm = 0, zspm = 0;
+  bool zunit = true;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int k = kq + e;
+    const bool kv = row_ok && k < P.nz;
+    kvm |= (unsigned)kv << e;
+    zslm |= (unsigned)(kv && in_slab(Z, k)) << e;
+    zspm |= (unsigned)(kv && __float_as_int(zt[5 * kTZ + 4 * lane + e]) != k - 1) << e;
+    zunit &= zt[kTZ + 4 * lane + e] == 1.0f;
+  }
+  const bool wplain = __all_sync(kFull, row_ok && !ysl && !yspecial && mj == 1.0f &&
+                                            kvm == 0xFu && zslm == 0u && zspm == 0u && zunit);
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t sj = P.nzp, si = (int64_t)P.ny * P.nzp;
+  const float cw = P.cw;
+  const int ro = (w + 1) * kBZ + 4 + 4 * lane;  // this quad in the H halo box
+  const int to = w * kTZ + 4 * lane;
+  for (int t = 0; t < np; ++t) {
+    const int slot = t % kS;
+    const bool got = mbar_wait(&full[slot], (uint32_t)((t / kS) & 1), err);
+    if (!__all_sync(kFull, got)) break;
+    float* stw = smem + slot * kEStage;
+    const float* st = stw;
+    const int* tab = reinterpret_cast<const int*>(st + kE_PT);
+    const float* pool = st + kE_POOL;
+    const float2* ps = reinterpret_cast<const float2*>(pool + tab[11]);
+    const int i = ib + t;
+    uint32_t mid[4] = {0u, 0u, 0u, 0u};
+    if (row_ok) {
+      if (wide) {
+        const uint4 m = *reinterpret_cast<const uint4*>(reinterpret_cast<const uint32_t*>(st + kE_MT) + to);
+        mid[0] = m.x; mid[1] = m.y; mid[2] = m.z; mid[3] = m.w;
+      } else {
+        const uint2 m = *reinterpret_cast<const uint2*>(reinterpret_cast<const uint16_t*>(st + kE_MT) + to);
+        mid[0] = m.x & 0xffffu; mid[1] = m.x >> 16; mid[2] = m.y & 0xffffu; mid[3] = m.y >> 16;
+      }
+    }
+    int lane_np = 0;
+    if (P.has_ade) {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) lane_np += mats[mid[e]].reserved;
+    }
+    // poles of this lane: global index gp, window index wp (-1: read from global memory)
+    uint32_t gp = 0;
+    int wp = -1;
+    const bool any_poles = P.has_ade && __any_sync(kFull, lane_np > 0);
+    if (any_poles) {
+      int pre = 0;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) pre += __popc(__ballot_sync(kFull, (lane_np >> b) & 1) & lt) << b;
+      gp = (uint32_t)tab[2 * w] + (uint32_t)pre;
+      if (tab[2 * w + 1] >= 0) wp = tab[2 * w + 1] + pre;
+    }
+    float ex[4], ey[4], ez[4];
+    unpack4(lds4(st + kE_ET + to), ex);
+    unpack4(lds4(st + kE_ET + 512 + to), ey);
+    unpack4(lds4(st + kE_ET + 1024 + to), ez);
+    if (lane_np > 0) {
+      // deferred ADE of this lane's dispersive cells, one rolled loop; the polarisation
+      // currents replace E^n in the warp's own row of the stage (E^n is in registers now)
+      float* et = stw + kE_ET + to;
+#pragma unroll 1
+      for (int e = 0; e < 4; ++e) {
+        const MatRec& M = mats[mid_at(st + kE_MT, wide, to + e)];
+        const int npc = M.reserved;
+        if (npc == 0) continue;
+        const float en[3] = {et[e], et[512 + e], et[1024 + e]};
+        float wv[3];
+        ade_cell(P, coef, set_ofs, M, ps, wp, gp, en, wv);
+        et[e] = wv[0];
+        et[512 + e] = wv[1];
+        et[1024 + e] = wv[2];
+        gp += (uint32_t)npc;
+        if (wp >= 0) wp += npc;
+      }
+    }
+    const bool xsl = in_slab(X, i);
+    const float mi = X.mpv[i], idx_ = X.idl_d[i];
+    const int64_t row = i * si + (int64_t)j * sj;
+    if (wplain && !xsl && i > 0 && X.prv[i] == i - 1 && mi == 1.0f) {
+      float hx[4], hy[4], hz[4], yhx[4], yhz[4], phy[4], phz[4], idz[4];
+      unpack4(lds4(st + kE_HB + ro), hx);
+      unpack4(lds4(st + kE_HB + kBoxW + ro), hy);
+      unpack4(lds4(st + kE_HB + 2 * kBoxW + ro), hz);
+      unpack4(lds4(st + kE_HB + ro - kBZ), yhx);
+      unpack4(lds4(st + kE_HB + 2 * kBoxW + ro - kBZ), yhz);
+      unpack4(lds4(st + kE_HP + to), phy);
+      unpack4(lds4(st + kE_HP + 512 + to), phz);
+      unpack4(lds4(zt + 4 * lane), idz);
+      const float hxm = st[kE_HB + ro - 1];
+      const float hym = st[kE_HB + kBoxW + ro - 1];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const MatRec& M = mats[mid[e]];
+        const float4 cab = *reinterpret_cast<const float4*>(&M.ca[0]);
+        const float2 cb12 = *reinterpret_cast<const float2*>(&M.cb[1]);
+        const float zhx = (e > 0) ? hx[e - 1] : hxm;
+        const float zhy = (e > 0) ? hy[e - 1] : hym;
+        float wv[3] = {0.f, 0.f, 0.f};
+        if (lane_np > 0 && M.reserved > 0) {
+          wv[0] = st[kE_ET + to + e];
+          wv[1] = st[kE_ET + 512 + to + e];
+          wv[2] = st[kE_ET + 1024 + to + e];
+        }
+        ex[e] = e_new(cab.x, ex[e], cab.w, __fmul_rn(__fsub_rn(hz[e], yhz[e]), idy),
+                      __fmul_rn(__fsub_rn(hy[e], zhy), idz[e]), cw, wv[0]);
+        ey[e] = e_new(cab.y, ey[e], cb12.x, __fmul_rn(__fsub_rn(hx[e], zhx), idz[e]),
+                      __fmul_rn(__fsub_rn(hz[e], phz[e]), idx_), cw, wv[1]);
+        ez[e] = e_new(cab.z, ez[e], cb12.y, __fmul_rn(__fsub_rn(hy[e], phy[e]), idx_),
+                      __fmul_rn(__fsub_rn(hx[e], yhx[e]), idy), cw, wv[2]);
+      }
+      *reinterpret_cast<float4*>(P.f[0] + row + kq) = make_float4(ex[0], ex[1], ex[2], ex[3]);
+      *reinterpret_cast<float4*>(P.f[1] + row + kq) = make_float4(ey[0], ey[1], ey[2], ey[3]);
+      *reinterpret_cast<float4*>(P.f[2] + row + kq) = make_float4(ez[0], ez[1], ez[2], ez[3]);
+    } else if (kvm) {
+      const float ay = Y.ae[jj], by = Y.be[jj], ky = Y.ke[jj];
+      const float ax_ = X.ae[i], bx_ = X.be[i], kx_ = X.ke[i];
+      float hx[4], hy[4], hz[4], yhx[4], yhz[4], phy[4], phz[4];
+      unpack4(lds4(st + kE_HB + ro), hx);
+      unpack4(lds4(st + kE_HB + kBoxW + ro), hy);
+      unpack4(lds4(st + kE_HB + 2 * kBoxW + ro), hz);
+      if (yspecial) {
+        const int64_t oy = i * si + (int64_t)jm * sj + kq;
+        unpack4(*reinterpret_cast<const float4*>(P.f[3] + oy), yhx);
+        unpack4(*reinterpret_cast<const float4*>(P.f[5] + oy), yhz);
+      } else {
+        unpack4(lds4(st + kE_HB + ro - kBZ), yhx);
+        unpack4(lds4(st + kE_HB + 2 * kBoxW + ro - kBZ), yhz);
+      }
+      unpack4(lds4(st + kE_HP + to), phy);
+      unpack4(lds4(st + kE_HP + 512 + to), phz);
+      const float hxm = st[kE_HB + ro - 1];
+      const float hym = st[kE_HB + kBoxW + ro - 1];
+      float px[2][4], py[2][4], pz[2][4];
+      if (xsl)
+        for (int s = 0; s < 2; ++s) unpack4(lds4(pool + tab[8] + (s * 4 + w) * kTZ + 4 * lane), px[s]);
+      if (ysl)
+        for (int s = 0; s < 2; ++s) unpack4(lds4(pool + tab[9] + (s * 4 + w) * kTZ + 4 * lane), py[s]);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (!((zslm >> e) & 1u)) continue;
+        const int k = kq + e;
+        const int side = k < Z.lo ? 0 : 1;
+        const int zq = side ? k - (Z.n - Z.hi) : k;
+        const bool staged = zslab_staged(Z, side, k0);
+        for (int s = 0; s < 2; ++s)
+          pz[s][e] = staged ? pool[tab[10] + (s * 2 + side) * kTY * kZMax + w * (side ? Z.hi : Z.lo) + zq]
+                            : *psi_addr(P.psie, 2, s, Z, i, j, k, P.ny, P.nzp);
+      }
+      float idz4[4], mkz4[4];
+      unpack4(lds4(zt + 4 * lane), idz4);
+      unpack4(lds4(zt + kTZ + 4 * lane), mkz4);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (!((kvm >> e) & 1u)) continue;
+        const int zi = 4 * lane + e;
+        const float idz = idz4[e], mkz = mkz4[e];
+        const bool zsl = (zslm >> e) & 1u;
+        const MatRec& M = mats[mid[e]];
+        const float4 cab = *reinterpret_cast<const float4*>(&M.ca[0]);
+        const float2 cb12 = *reinterpret_cast<const float2*>(&M.cb[1]);
+        float zhx = (e > 0) ? hx[e - 1] : hxm;
+        float zhy = (e > 0) ? hy[e - 1] : hym;
+        if ((zspm >> e) & 1u) {
+          const int km = __float_as_int(zt[5 * kTZ + zi]);
+          zhx = P.f[3][row + km];
+          zhy = P.f[4][row + km];
+        }
+        float wv[3] = {0.f, 0.f, 0.f};
+        if (lane_np > 0 && M.reserved > 0) {
+          wv[0] = st[kE_ET + to + e];
+          wv[1] = st[kE_ET + 512 + to + e];
+          wv[2] = st[kE_ET + 1024 + to + e];
+        }
+        const float az = zsl ? zt[2 * kTZ + zi] : 0.f;
+        const float bz = zsl ? zt[3 * kTZ + zi] : 0.f;
+        const float kz = zsl ? zt[4 * kTZ + zi] : 0.f;
+        {  // Ex: dHz/dy - dHy/dz
+          const float dzy = bdiff(hz[e], yhz[e], mj, idy);
+          const float dyz = bdiff(hy[e], zhy, mkz, idz);
+          const float sy = ysl ? cpml_stretch(dzy, py[0][e], ay, by, ky) : dzy;
+          const float sz = zsl ? cpml_stretch(dyz, pz[0][e], az, bz, kz) : dyz;
+          ex[e] = e_new(cab.x, ex[e], cab.w, sy, sz, cw, wv[0]);
+        }
+        {  // Ey: dHx/dz - dHz/dx
+          const float dxz = bdiff(hx[e], zhx, mkz, idz);
+          const float dzx = bdiff(hz[e], phz[e], mi, idx_);
+          const float sz = zsl ? cpml_stretch(dxz, pz[1][e], az, bz, kz) : dxz;
+          const float sx = xsl ? cpml_stretch(dzx, px[0][e], ax_, bx_, kx_) : dzx;
+          ey[e] = e_new(cab.y, ey[e], cb12.x, sz, sx, cw, wv[1]);
+        }
+        {  // Ez: dHy/dx - dHx/dy
+          const float dyx = bdiff(hy[e], phy[e], mi, idx_);
+          const float dxy = bdiff(hx[e], yhx[e], mj, idy);
+          const float sx = xsl ? cpml_stretch(dyx, px[1][e], ax_, bx_, kx_) : dyx;
+          const float sy = ysl ? cpml_stretch(dxy, py[1][e], ay, by, ky) : dxy;
+          ez[e] = e_new(cab.z, ez[e], cb12.y, sx, sy, cw, wv[2]);
+        }
+      }
+      if (xsl)
+        for (int s = 0; s < 2; ++s)
+          *reinterpret_cast<float4*>(psi_addr(P.psie, 0, s, X, i, j, kq, P.ny, P.nzp)) =
+              make_float4(px[s][0], px[s][1], px[s][2], px[s][3]);
+      if (ysl)
+        for (int s = 0; s < 2; ++s)
+          *reinterpret_cast<float4*>(psi_addr(P.psie, 1, s, Y, i, j, kq, P.ny, P.nzp)) =
+              make_float4(py[s][0], py[s][1], py[s][2], py[s][3]);
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if ((zslm >> e) & 1u)
+          for (int s = 0; s < 2; ++s)
+            *psi_addr(P.psie, 2, s, Z, i, j, kq + e, P.ny, P.nzp) = pz[s][e];
+      *reinterpret_cast<float4*>(P.f[0] + row + kq) = make_float4(ex[0], ex[1], ex[2], ex[3]);
+      *reinterpret_cast<float4*>(P.f[1] + row + kq) = make_float4(ey[0], ey[1], ey[2], ey[3]);
+      *reinterpret_cast<float4*>(P.f[2] + row + kq) = make_float4(ez[0], ez[1], ez[2], ez[3]);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[slot]);
+  }
+}
+
+}  // namespace
+
+size_t ws_h_smem() { return (size_t)kS * kHStage * 4 + 2 * kS * sizeof(uint64_t) + kZTab * 4; }
+size_t ws_e_smem() {
+  return (size_t)kS * kEStage * 4 + 2 * kS * sizeof(uint64_t) + kZTab * 4 +
+         kSmemMats * sizeof(MatRec) + kXMax * kTY * 2 * sizeof(uint32_t) +
+         kSmemCoef * sizeof(float4) + kSmemSets * sizeof(int);
+}
+
+int ws_max_xchunk() { return kXMax; }
+
+int ws_xchunk(const YeeParams& P) {
+  const int64_t tiles = (int64_t)((P.nzp + kTZ - 1) / kTZ) * ((P.ny + kTY - 1) / kTY);
+  const int64_t want = 148LL * 2 * 4;  // ~4 waves of 2 resident blocks per SM
+  int64_t chunks = (want + tiles - 1) / tiles;
+  int xch = (int)((P.nx + chunks - 1) / chunks);
+  if (xch < 8) xch = 8;
+  if (xch > kXMax) xch = kXMax;
+  if (xch > P.nx) xch = P.nx;
+  return xch;
+}
+
+// Two blocks of each kernel share an SM; the largest shared-memory carveout makes room for both.
+cudaError_t ws_setup_kernels() {
+  cudaError_t e = cudaFuncSetAttribute(k_h_ws, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)ws_h_smem());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_h_ws, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_e_ws, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ws_e_smem());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_e_ws, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+  return e;
+}
+
+cudaError_t launch_update_h_ws(const TmaMaps& maps, const YeeParams& P, int xch, int* err,
+                               cudaStream_t s) {
+  dim3 b(32, kTY + 1, 1), g((P.nzp + kTZ - 1) / kTZ, (P.ny + kTY - 1) / kTY, (P.nx + xch - 1) / xch);
+  k_h_ws<<<g, b, ws_h_smem(), s>>>(maps, P, xch, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_update_e_ws(const TmaMaps& maps, const YeeParams& P, int xch, int n_mats,
+                               int* err, cudaStream_t s) {
+  dim3 b(32, kTY + 1, 1), g((P.nzp + kTZ - 1) / kTZ, (P.ny + kTY - 1) / kTY, (P.nx + xch - 1) / xch);
+  k_e_ws<<<g, b, ws_e_smem(), s>>>(maps, P, xch, n_mats, err);
+  return cudaGetLastError();
+}
+
+}  // namespace oem

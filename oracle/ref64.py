@@ -441,6 +441,36 @@ def run(sc, num_steps: int | None = None) -> OracleResult:
     return Oracle(sc, num_steps).run()
 
 
+class PerturbedOracle(Oracle):
+    """The FP64 oracle with float32-sized rounding noise: after every step each field value
+    is multiplied by ``1 + u * U(-1, 1)`` with ``u = 2**-24`` (half an ulp of float32). The
+    distance of its result from the clean run is the rounding floor of a float32 engine on
+    that scene: how far one float32 rounding per value and step moves the fields. Resonant
+    dispersive scenes amplify it well above 2**-24; a float32 engine cannot be held closer
+    to the FP64 oracle than this floor."""
+
+    def __init__(self, sc, n_total: int | None = None, seed: int = 0):
+        super().__init__(sc, n_total)
+        self._rng = np.random.default_rng(seed)
+
+    def step(self):
+        super().step()
+        u = 2.0 ** -24
+        for F in (*self.E, *self.H):
+            F *= 1.0 + u * self._rng.uniform(-1.0, 1.0, F.shape)
+
+
+def fp32_floor(sc, num_steps: int | None = None, seed: int = 1, clean=None) -> dict:
+    """Per-field relative L2 distance between a ``PerturbedOracle`` run and the clean run."""
+    ref = clean if clean is not None else Oracle(sc, num_steps).run()
+    pert = PerturbedOracle(sc, num_steps, seed).run()
+    out = {}
+    for nm, a in pert.fields.items():
+        b = ref.fields[nm]
+        out[nm] = float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+    return out
+
+
 class BlochOracle(Oracle):
     """Complex-field Bloch path (``openem/kernels/bloch.cu:25-221``): fields carry re + i im,
     the periodic seam neighbour is multiplied by ``exp(+/- i 2 pi k)``; the scene subset is

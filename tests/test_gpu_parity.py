@@ -1,7 +1,8 @@
 """CUDA engine against the FP64 oracle on the same seeded scenes.
 
 Tolerances (fp32 fields against float64 arithmetic): final fields within 1e-5 relative L2 on
-the plane-wave slab and 2e-5 on the Drude+Lorentz scene, DFT phasors within 1e-4 relative L2,
+the plane-wave slab; on the resonant Drude+Lorentz scene within max(2e-5, 3 x the float32
+rounding floor the oracle measures for that component); DFT phasors within 1e-4 relative L2,
 slab transmission within 1e-4 absolute.
 """
 
@@ -18,6 +19,13 @@ def rel_l2(a, b):
     a = np.asarray(a)
     b = np.asarray(b)
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def family_err(fa, fb, names):
+    """Largest per-component L2 difference relative to the norm of the whole field family
+    (E or H): a component that is nearly zero by symmetry does not magnify round-off."""
+    den = np.sqrt(sum(float(np.linalg.norm(fb[n].ravel())) ** 2 for n in names))
+    return max(float(np.linalg.norm((fa[n] - fb[n]).ravel())) for n in names) / max(den, 1e-300)
 
 
 def flux(ph):
@@ -82,9 +90,14 @@ def disp_runs():
 
 
 def test_dispersive_fields_match_oracle(disp_runs):
+    """Each component within max(2e-5, 3 x its float32 rounding floor) of the FP64 oracle.
+    The floor is measured on this scene by the oracle itself, with half-ulp float32 noise
+    injected into every field value each step (``ref64.fp32_floor``); on this resonant
+    Drude+Lorentz scene it reaches ~1.5e-5 for Hx/Hy and ~4.7e-5 for Hz after 300 steps."""
     r, g = disp_runs["ref"], disp_runs["gpu"]
+    floor = ref64.fp32_floor(disp_runs["sc"], clean=r)
     for nm in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
-        assert rel_l2(g.fields[nm], r.fields[nm]) < 2e-5, nm
+        assert rel_l2(g.fields[nm], r.fields[nm]) < max(2e-5, 3.0 * floor[nm]), (nm, floor[nm])
 
 
 def test_dispersive_field_monitors_match_oracle(disp_runs):
@@ -112,18 +125,34 @@ def test_dispersion_changes_the_result(disp_runs):
     assert rel_l2(gp.fields["Ez"], g.fields["Ez"]) > 1e-2
 
 
-def test_streaming_kernels_equal_basic_kernels(monkeypatch):
-    """The streaming kernels (default) and the one-thread-per-cell kernels do the same
-    arithmetic per cell; their results agree to float32 round-off."""
-    sc = scenes.small_dispersive(n=40, n_sph=5, num_steps=120, n_pml=8, nfreq=3)
+@pytest.mark.parametrize("kind", ["stream", "tma", "ws"])
+@pytest.mark.parametrize("n,n_pml", [(40, 8), (42, 8), (44, 6)])
+def test_pipelined_kernels_equal_basic_kernels(monkeypatch, kind, n, n_pml):
+    """Each pipelined kernel pair does the arithmetic of the one-thread-per-cell kernels per
+    cell; their results agree to float32 round-off. CPML depth 8 has its z-slab psi staged in
+    shared memory, depth 6 read directly; 42 cells leave a partial tile of rows."""
+    sc = scenes.small_dispersive(n=n, n_sph=5, num_steps=120, n_pml=n_pml, nfreq=3)
     monkeypatch.setenv("OEM_B200_KERNELS", "basic")
     a = solver.run(sc, use_shutoff=False, return_fields=True, verbose=False)
-    monkeypatch.setenv("OEM_B200_KERNELS", "stream")
+    monkeypatch.setenv("OEM_B200_KERNELS", kind)
     b = solver.run(sc, use_shutoff=False, return_fields=True, verbose=False)
-    for nm in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
-        assert rel_l2(b.fields[nm], a.fields[nm]) < 1e-6, nm
+    assert family_err(b.fields, a.fields, ("Ex", "Ey", "Ez")) < 1e-6
+    assert family_err(b.fields, a.fields, ("Hx", "Hy", "Hz")) < 1e-6
     for name in a.field_phasors:
         assert rel_l2(b.field_phasors[name], a.field_phasors[name]) < 1e-6, name
+
+
+@pytest.mark.parametrize("kind", ["stream", "tma", "ws"])
+def test_pipelined_kernels_periodic_slab(monkeypatch, kind):
+    """Periodic x/y walls of a one-cell-wide column (every neighbour wraps) and a plane-wave
+    source, against the one-thread-per-cell kernels."""
+    sc = scenes.slab_plane_wave(nxy=1, num_steps=400)
+    monkeypatch.setenv("OEM_B200_KERNELS", "basic")
+    a = solver.run(sc, num_steps=400, use_shutoff=False, return_fields=True, verbose=False)
+    monkeypatch.setenv("OEM_B200_KERNELS", kind)
+    b = solver.run(sc, num_steps=400, use_shutoff=False, return_fields=True, verbose=False)
+    for nm in ("Ex", "Hy"):
+        assert rel_l2(b.fields[nm], a.fields[nm]) < 1e-6, nm
 
 
 def test_device_tables_match_host_tables():

@@ -193,3 +193,13 @@ def test_source_end_step():
     end = shutoff.source_end_step(sc)
     a = np.abs(sc.sources[0].waveform.amp_int)
     assert a[end] > 1e-3 * a.max() and np.all(a[end + 1:] <= 1e-3 * a.max())
+
+
+def test_fp32_rounding_floor_is_measurable():
+    """The perturbed oracle moves a resonant dispersive scene by more than the injected
+    half-ulp noise (the scene amplifies rounding) and by far less than a real error would."""
+    from openem_b200 import scenes
+    sc = scenes.small_dispersive(n=24, n_sph=2, num_steps=120, n_pml=6, nfreq=2)
+    fl = ref64.fp32_floor(sc)
+    assert all(v > 2.0 ** -24 for v in fl.values())
+    assert max(fl.values()) < 1e-3
