@@ -144,8 +144,13 @@ static cudaError_t run_h(oem_plan* p, cudaStream_t s) {
 static cudaError_t run_e(oem_plan* p, cudaStream_t s) {
   if (p->basic_kernels == 1) return launch_update_e(p->yp, s);
   if (p->basic_kernels == 2) return launch_update_e_stream(p->yp, p->xch, (int)p->mats.size(), s);
-  if (p->basic_kernels == 3)
+  if (p->basic_kernels == 3) {
+    if (p->yp.has_ade) {
+      cudaError_t e = launch_ade_segments(p->yp, p->d_ade_segs, p->n_ade_segs, s);
+      if (e != cudaSuccess) return e;
+    }
     return launch_update_e_ws(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s);
+  }
   return launch_update_e_tma(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s);
 }
 
@@ -754,6 +759,22 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
     P.n_pole_total = (uint32_t)p->n_pole_total;
     P.n_coef = (int)(p->pcoef.size() / 4);
     P.n_sets = (int)p->pset_ofs.size() - 1;
+    if (p->basic_kernels == 3) {
+      // separate pole pass: pole-indexed currents (four floats of slack for 16-byte-aligned
+      // bulk reads) and the list of segments that hold poles
+      if ((rc = dalloc(p, &P.J, (size_t)std::max<int64_t>(p->n_pole_total, 1) + 4))) return rc;
+      const int64_t nseg = (int64_t)p->nx * p->ny * p->nzp / 32;
+      unsigned long long* dcount = nullptr;
+      if ((rc = dalloc(p, &dcount, 1))) return rc;
+      OEM_CUDA(launch_list_pole_segments(P, nseg, nullptr, dcount, 0));
+      unsigned long long h = 0;
+      OEM_CUDA(cudaMemcpy(&h, dcount, sizeof(h), cudaMemcpyDeviceToHost));
+      p->n_ade_segs = (int64_t)h;
+      if ((rc = dalloc(p, &p->d_ade_segs, (size_t)std::max<int64_t>(p->n_ade_segs, 1)))) return rc;
+      OEM_CUDA(cudaMemset(dcount, 0, sizeof(h)));
+      OEM_CUDA(launch_list_pole_segments(P, nseg, p->d_ade_segs, dcount, 0));
+      OEM_CUDA(cudaDeviceSynchronize());
+    }
     P.has_ade = 1;
   }
   if ((rc = dalloc(p, &p->d_step, 1))) return rc;
@@ -800,10 +821,10 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
     // Direct launches with CUDA events around the two update kernels; events come from a pool
     // sized for this call and are read once at the end, so the stream never waits on the host.
     const int64_t n = nsteps;
-    std::vector<cudaEvent_t> ev((size_t)n * 5);
+    std::vector<cudaEvent_t> ev((size_t)n * 6);
     for (auto& evq : ev) OEM_CUDA(cudaEventCreate(&evq));
     for (int64_t q = 0; q < n; ++q) {
-      cudaEvent_t* E = &ev[(size_t)q * 5];
+      cudaEvent_t* E = &ev[(size_t)q * 6];
       OEM_CUDA(cudaEventRecord(E[0], s));
       cudaError_t e = run_h(p, s);
       if (e != cudaSuccess) return cuda_error(e, "update_h");
@@ -814,7 +835,17 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       for (const PlaneSrc& src : p->planes)
         if ((e = launch_plane_h(p->yp, src, p->d_step, s)) != cudaSuccess) return cuda_error(e, "plane_h");
       OEM_CUDA(cudaEventRecord(E[2], s));
-      if ((e = run_e(p, s)) != cudaSuccess) return cuda_error(e, "update_e");
+      const bool split = p->basic_kernels == 3 && p->yp.has_ade;
+      if (split) {
+        // the pole pass and the E kernel timed apart
+        if ((e = launch_ade_segments(p->yp, p->d_ade_segs, p->n_ade_segs, s)) != cudaSuccess)
+          return cuda_error(e, "ade");
+        OEM_CUDA(cudaEventRecord(E[5], s));
+        e = launch_update_e_ws(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s);
+      } else {
+        e = run_e(p, s);
+      }
+      if (e != cudaSuccess) return cuda_error(e, "update_e");
       OEM_CUDA(cudaEventRecord(E[3], s));
       for (const PlaneSrc& src : p->planes)
         if ((e = launch_plane_e(p->yp, src, p->d_step, s)) != cudaSuccess) return cuda_error(e, "plane_e");
@@ -832,18 +863,24 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       if ((e = launch_step_advance(p->d_step, s)) != cudaSuccess) return cuda_error(e, "step");
       OEM_CUDA(cudaEventRecord(E[4], s));
     }
-    if (n > 0) OEM_CUDA(cudaEventSynchronize(ev[(size_t)n * 5 - 1]));
+    if (n > 0) OEM_CUDA(cudaEventSynchronize(ev[(size_t)n * 6 - 2]));
     auto add = [&](const char* nm, double ms) {
       for (TimingRec& r : p->trecs)
         if (r.name == nm) { r.count++; r.ms += ms; return; }
       TimingRec r; r.name = nm; r.count = 1; r.ms = ms; p->trecs.push_back(r);
     };
     for (int64_t q = 0; q < n; ++q) {
-      cudaEvent_t* E = &ev[(size_t)q * 5];
-      float t_h = 0.f, t_e = 0.f, t_all = 0.f;
+      cudaEvent_t* E = &ev[(size_t)q * 6];
+      float t_h = 0.f, t_e = 0.f, t_all = 0.f, t_ade = 0.f;
       OEM_CUDA(cudaEventElapsedTime(&t_h, E[0], E[1]));
-      OEM_CUDA(cudaEventElapsedTime(&t_e, E[2], E[3]));
       OEM_CUDA(cudaEventElapsedTime(&t_all, E[0], E[4]));
+      if (p->basic_kernels == 3 && p->yp.has_ade) {
+        OEM_CUDA(cudaEventElapsedTime(&t_ade, E[2], E[5]));
+        OEM_CUDA(cudaEventElapsedTime(&t_e, E[5], E[3]));
+        add("ade", t_ade);
+      } else {
+        OEM_CUDA(cudaEventElapsedTime(&t_e, E[2], E[3]));
+      }
       add("update_h", t_h);
       add("update_e", t_e);
       add("step", t_all);
@@ -881,6 +918,7 @@ int oem_plan_launches_per_step(oem_plan* p, int* n) {
   if (rc) return rc;
   if (!n) return set_error(OEM_ERR_INVALID, "null output");
   int c = 2 + 1;  // update_h, update_e, step counter
+  if (p->basic_kernels == 3 && p->yp.has_ade) c += 1;  // separate pole pass
   c += 2 * (int)p->planes.size();
   for (const DipoleSet& d : p->dipoles) c += d.n_targets > 0 ? 1 : 0;
   c += 2 * (int)p->tmons.size();

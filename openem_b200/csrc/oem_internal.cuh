@@ -80,6 +80,7 @@ struct YeeParams {
   const MatRec* mats;
   // ADE
   float2* P;               // pole states, cell order then component then pole
+  float* J;                // pole-indexed polarisation currents of the separate pole pass
   const float4* pcoef;     // per pole of a set: (Re(A-1), Im(A-1), Re(B), Im(B))
   const int* pset_ofs;     // set -> first pole in pcoef
   const uint32_t* seg_ofs; // poles stored before each 32-cell segment
@@ -206,6 +207,8 @@ struct oem_plan {
   int basic_kernels = 3;  // 3: warp-specialised (default), 0: TMA, 1: one-thread-per-cell, 2: register-streaming
   oem::TmaMaps tma{};
   int* d_err = nullptr;   // set by a kernel whose bounded wait gave up
+  int64_t* d_ade_segs = nullptr;  // segments with poles (separate pole pass)
+  int64_t n_ade_segs = 0;
   int xch = 8;            // x planes per thread in the streaming kernels
 };
 
@@ -275,6 +278,10 @@ cudaError_t launch_update_h_ws(const TmaMaps& maps, const YeeParams& P, int xch,
 cudaError_t launch_update_e_ws(const TmaMaps& maps, const YeeParams& P, int xch, int n_mats,
                                int* err, cudaStream_t s);
 cudaError_t launch_update_e_stream(const YeeParams& P, int xch, int n_mats, cudaStream_t s);
+cudaError_t launch_list_pole_segments(const YeeParams& P, int64_t nseg, int64_t* list,
+                                      unsigned long long* count, cudaStream_t s);
+cudaError_t launch_ade_segments(const YeeParams& P, const int64_t* segs, int64_t nsegs,
+                                cudaStream_t s);
 cudaError_t launch_energy(const YeeParams& P, double* const dl[3][2], double* part, int nblocks,
                           cudaStream_t s);
 int energy_block_count(const YeeParams& P);

@@ -2,19 +2,20 @@
 //
 // A block owns a 128 (z) x 4 (y) tile and walks a chunk of x planes. Warp 4 is the producer:
 // its lane 0 stages everything one plane needs into a 3-deep shared-memory ring -- field tiles
-// with cp.async.bulk.tensor (TMA), the CPML psi rows of slab cells and the ADE pole states of a
-// row with 1D cp.async.bulk copies -- ahead of the four consumer warps, one per tile row, four z
-// cells per lane. A stage is published by a "full" mbarrier (producer arrival + transaction
-// bytes) and recycled through an "empty" mbarrier that each consumer warp arrives on once it is
-// done with it. Consumers issue no synchronous global load except for the rare boundary cells
-// whose neighbour is not the adjacent index (periodic wrap, PMC, symmetry) and pole rows that
-// do not fit the stage's pole window; they write H/E, psi and the pole states straight back.
+// with cp.async.bulk.tensor (TMA), the CPML psi rows of slab cells and the polarisation
+// currents of the plane's dispersive cells with 1D cp.async.bulk copies -- ahead of the four
+// consumer warps, one per tile row, four z cells per lane. A stage is published by a "full"
+// mbarrier (producer arrival + transaction bytes) and recycled through an "empty" mbarrier
+// that each consumer warp arrives on once it is done with it. Consumers issue no synchronous
+// global load except for wrapped neighbours (periodic seams) and rows whose currents do not fit
+// the stage's window; they write H/E and psi straight back. The ADE pole states are advanced
+// by a separate pass (oem_ade.cu) that runs between the two updates and leaves J behind.
 //
 // Every mbarrier wait is bounded (2^20 polls); a wait that gives up sets *err, stops the
 // issuing side and the waiting side, and the producer drains what it issued (again bounded).
 //
-// The arithmetic per cell is that of the basic kernels (openem/kernels/yee.cu:60-240,
-// dispersion.cu:168-207).
+// The arithmetic per cell is that of the basic kernels (openem/kernels/yee.cu:60-240), pinned
+// in oem_arith.cuh, so both produce the same bits.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -37,8 +38,6 @@ constexpr uint32_t kTileBytes = kTY * kTZ * 4;  // bytes a 128 x 4 tile transfer
 constexpr int kZMax = 32;                       // z-slab depths staged when <= this and % 4 == 0
 constexpr int kSmemMats = 64;
 constexpr int kXMax = 64;                       // x planes per block (segment table size)
-constexpr int kSmemCoef = 64;                   // pole coefficients kept in shared memory
-constexpr int kSmemSets = 32;
 
 // H kernel stage (floats)
 constexpr int kH_EB = 0;                  // E halo box x3
@@ -254,36 +253,74 @@ __device__ __forceinline__ void load_ztab(float* zt, const DevAxis& Z, bool h_si
   }
 }
 
-__device__ __forceinline__ uint32_t mid_at(const float* mt, bool wide, int idx) {
-  return wide ? reinterpret_cast<const uint32_t*>(mt)[idx]
-              : (uint32_t)reinterpret_cast<const uint16_t*>(mt)[idx];
+// J of the three components of one cell: stored at the cell's first pole of each component.
+__device__ __forceinline__ void cell_currents(const MatRec& M, const float* jw, int wp,
+                                              const float* J, uint32_t gp, float wv[3]) {
+  int po = 0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const int n = M.np[c];
+    if (n > 0) wv[c] = (wp >= 0) ? jw[wp + po] : J[gp + (uint32_t)po];
+    po += n;
+  }
 }
 
 __device__ __forceinline__ void unpack4(const float4 v, float (&a)[4]) {
   a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
 }
 
-// The poles of one cell: deferred ADE of its dispersive components, polarisation currents out.
-// ps/wp: the stage's pole window and this cell's first entry in it (-1: global memory).
-__device__ __forceinline__ void ade_cell(const YeeParams& P, const float4* coef,
-                                         const int* set_ofs, const MatRec& M, const float2* ps,
-                                         int wp, uint32_t gp, const float en[3], float wv[3]) {
-  int po = 0;
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    wv[c] = 0.f;
-    const int n = M.np[c];
-    if (n == 0) continue;
-    const float4* cf = coef + set_ofs[M.pset[c]];
-    float acc = 0.f;
-    for (int tt = 0; tt < n; ++tt) {
-      const uint32_t g = gp + (uint32_t)(po + tt);
-      float2 s2 = (wp >= 0) ? ps[wp + po + tt] : P.P[g];
-      acc = __fadd_rn(acc, ade_pole(s2, cf[tt], en[c]));
-      P.P[g] = s2;
+// z CPML of one lane's four cells (the two z derivatives da, db of the slots 0 and 1): psi
+// from the stage when the slab depth is staged, else from global memory, written back to
+// global memory. A lane whose four cells all lie in one slab at a 16-byte-aligned offset does
+// it with vector loads and stores; other slab lanes cell by cell.
+__device__ __forceinline__ void z_cpml(float (&da)[4], float (&db)[4], unsigned zslm,
+                                    const float* zrows, const float* zt, const PsiSet& S,
+                                    const YeeParams& P, const DevAxis& Z, int i, int j, int kq,
+                                    int k0, int w, int lane) {
+  const int side = kq < Z.lo ? 0 : 1;
+  const int L = side ? Z.hi : Z.lo;
+  const int zq = side ? kq - (Z.n - Z.hi) : kq;
+  const int64_t base = ((int64_t)i * P.ny + j) * L;
+  if (zslm == 0xFu && (L & 3) == 0 && (zq & 3) == 0) {
+    float* g0 = S.p[2][0][side] + base + zq;
+    float* g1 = S.p[2][1][side] + base + zq;
+    float p0[4], p1[4], a[4], b[4], k[4];
+    if (zslab_staged(Z, side, k0)) {
+      unpack4(lds4(zrows + (0 * 2 + side) * kTY * kZMax + w * L + zq), p0);
+      unpack4(lds4(zrows + (1 * 2 + side) * kTY * kZMax + w * L + zq), p1);
+    } else {
+      unpack4(*reinterpret_cast<const float4*>(g0), p0);
+      unpack4(*reinterpret_cast<const float4*>(g1), p1);
     }
-    wv[c] = acc;
-    po += n;
+    unpack4(lds4(zt + 2 * kTZ + 4 * lane), a);
+    unpack4(lds4(zt + 3 * kTZ + 4 * lane), b);
+    unpack4(lds4(zt + 4 * kTZ + 4 * lane), k);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      da[e] = cpml_stretch(da[e], p0[e], a[e], b[e], k[e]);
+      db[e] = cpml_stretch(db[e], p1[e], a[e], b[e], k[e]);
+    }
+    *reinterpret_cast<float4*>(g0) = make_float4(p0[0], p0[1], p0[2], p0[3]);
+    *reinterpret_cast<float4*>(g1) = make_float4(p1[0], p1[1], p1[2], p1[3]);
+    return;
+  }
+  for (int e = 0; e < 4; ++e) {
+    if (!((zslm >> e) & 1u)) continue;
+    const int kk = kq + e;
+    const int sd = kk < Z.lo ? 0 : 1;
+    const int Ls = sd ? Z.hi : Z.lo;
+    const int q = sd ? kk - (Z.n - Z.hi) : kk;
+    const int zi = 4 * lane + e;
+    const bool staged = zslab_staged(Z, sd, k0);
+    float* g0 = psi_addr(S, 2, 0, Z, i, j, kk, P.ny, P.nzp);
+    float* g1 = psi_addr(S, 2, 1, Z, i, j, kk, P.ny, P.nzp);
+    float p0 = staged ? zrows[(0 * 2 + sd) * kTY * kZMax + w * Ls + q] : *g0;
+    float p1 = staged ? zrows[(1 * 2 + sd) * kTY * kZMax + w * Ls + q] : *g1;
+    const float a = zt[2 * kTZ + zi], b = zt[3 * kTZ + zi], k = zt[4 * kTZ + zi];
+    da[e] = cpml_stretch(da[e], p0, a, b, k);
+    db[e] = cpml_stretch(db[e], p1, a, b, k);
+    *g0 = p0;
+    *g1 = p1;
   }
 }
 
@@ -350,22 +387,23 @@ __global__ void __launch_bounds__(160, 2) k_h_ws(const __grid_constant__ TmaMaps
   const int jp = Y.nxt[jj];
   const float mj = Y.mnx[jj], idy = Y.idl_p[jj];
   const bool ysl = row_ok && in_slab(Y, j);
-  const bool yspecial = row_ok && jp != j + 1;
+  // a neighbour that is not the adjacent index is fetched from global memory, unless its wall
+  // mask is 0: then the staged adjacent value (finite: a field or the zero fill) times 0 gives
+  // the same difference
+  const bool yspecial = row_ok && jp != j + 1 && mj != 0.0f;
   const int kq = k0 + 4 * lane;
   unsigned kvm = 0, zslm = 0, zspm = 0;
-  bool zunit = true;
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
     const int k = kq + e;
     const bool kv = row_ok && k < P.nz;
     kvm |= (unsigned)kv << e;
     zslm |= (unsigned)(kv && in_slab(Z, k)) << e;
-    zspm |= (unsigned)(kv && __float_as_int(zt[5 * kTZ + 4 * lane + e]) != k + 1) << e;
-    zunit &= zt[kTZ + 4 * lane + e] == 1.0f;
+    zspm |= (unsigned)(kv && __float_as_int(zt[5 * kTZ + 4 * lane + e]) != k + 1 &&
+                       zt[kTZ + 4 * lane + e] != 0.0f) << e;
   }
   // a plain row: every cell interior in y and z (adjacent neighbours, unit masks, no CPML)
-  const bool wplain = __all_sync(kFull, row_ok && !ysl && !yspecial && mj == 1.0f &&
-                                            kvm == 0xFu && zslm == 0u && zspm == 0u && zunit);
+  const bool yplain = row_ok && !ysl && !yspecial && mj == 1.0f;  // uniform over the warp
   const int64_t sj = P.nzp, si = (int64_t)P.ny * P.nzp;
   const float ch = P.ch;
   const int ro = w * kBZ + 4 * lane;  // this quad in a halo box
@@ -379,40 +417,9 @@ __global__ void __launch_bounds__(160, 2) k_h_ws(const __grid_constant__ TmaMaps
     const bool xsl = in_slab(X, i);
     const float mi = X.mnx[i], idx_ = X.idl_p[i];
     const int64_t row = i * si + (int64_t)j * sj;
-    if (wplain && !xsl && i + 1 < P.nx && X.nxt[i] == i + 1 && mi == 1.0f) {
-      // interior fast path: fdiff with unit masks and no CPML, the same bits as below
-      float ex[4], ey[4], ez[4], yex[4], yez[4], ney[4], nez[4], hx[4], hy[4], hz[4], idz[4];
-      unpack4(lds4(st + kH_EB + ro), ex);
-      unpack4(lds4(st + kH_EB + kBoxW + ro), ey);
-      unpack4(lds4(st + kH_EB + 2 * kBoxW + ro), ez);
-      unpack4(lds4(st + kH_EB + ro + kBZ), yex);
-      unpack4(lds4(st + kH_EB + 2 * kBoxW + ro + kBZ), yez);
-      unpack4(lds4(st + kH_EN + 512 + to), ney);
-      unpack4(lds4(st + kH_EN + 1024 + to), nez);
-      unpack4(lds4(st + kH_HT + to), hx);
-      unpack4(lds4(st + kH_HT + 512 + to), hy);
-      unpack4(lds4(st + kH_HT + 1024 + to), hz);
-      unpack4(lds4(zt + 4 * lane), idz);
-      const float ex4 = st[kH_EB + ro + 4];
-      const float ey4 = st[kH_EB + kBoxW + ro + 4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const float zex = (e < 3) ? ex[e + 1] : ex4;
-        const float zey = (e < 3) ? ey[e + 1] : ey4;
-        hx[e] = h_new(hx[e], ch, __fmul_rn(__fsub_rn(yez[e], ez[e]), idy),
-                      __fmul_rn(__fsub_rn(zey, ey[e]), idz[e]));
-        hy[e] = h_new(hy[e], ch, __fmul_rn(__fsub_rn(zex, ex[e]), idz[e]),
-                      __fmul_rn(__fsub_rn(nez[e], ez[e]), idx_));
-        hz[e] = h_new(hz[e], ch, __fmul_rn(__fsub_rn(ney[e], ey[e]), idx_),
-                      __fmul_rn(__fsub_rn(yex[e], ex[e]), idy));
-      }
-      *reinterpret_cast<float4*>(P.f[3] + row + kq) = make_float4(hx[0], hx[1], hx[2], hx[3]);
-      *reinterpret_cast<float4*>(P.f[4] + row + kq) = make_float4(hy[0], hy[1], hy[2], hy[3]);
-      *reinterpret_cast<float4*>(P.f[5] + row + kq) = make_float4(hz[0], hz[1], hz[2], hz[3]);
-    } else if (kvm) {
-      const float ay = Y.ah[jj], by = Y.bh[jj], ky = Y.kh[jj];
-      const float ax_ = X.ah[i], bx_ = X.bh[i], kx_ = X.kh[i];
+    if (kvm) {
       float ex[4], ey[4], ez[4], yex[4], yez[4], ney[4], nez[4], hx[4], hy[4], hz[4];
+      float idz[4], mkz[4];
       unpack4(lds4(st + kH_EB + ro), ex);
       unpack4(lds4(st + kH_EB + kBoxW + ro), ey);
       unpack4(lds4(st + kH_EB + 2 * kBoxW + ro), ez);
@@ -429,79 +436,76 @@ __global__ void __launch_bounds__(160, 2) k_h_ws(const __grid_constant__ TmaMaps
       unpack4(lds4(st + kH_HT + to), hx);
       unpack4(lds4(st + kH_HT + 512 + to), hy);
       unpack4(lds4(st + kH_HT + 1024 + to), hz);
+      unpack4(lds4(zt + 4 * lane), idz);
+      unpack4(lds4(zt + kTZ + 4 * lane), mkz);
       const float ex4 = st[kH_EB + ro + 4];
       const float ey4 = st[kH_EB + kBoxW + ro + 4];
-      // psi of this quad (x: Hy, Hz; y: Hx, Hz; z: Hx, Hy)
-      float px[2][4], py[2][4], pz[2][4];
-      if (xsl)
-        for (int s = 0; s < 2; ++s) unpack4(lds4(st + kH_PX + (s * 4 + w) * kTZ + 4 * lane), px[s]);
-      if (ysl)
-        for (int s = 0; s < 2; ++s) unpack4(lds4(st + kH_PY + (s * 4 + w) * kTZ + 4 * lane), py[s]);
+      // z derivatives of all four cells, then the z CPML of the slab lanes in one block
+      float dyz[4], dxz[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        if (!((zslm >> e) & 1u)) continue;
-        const int k = kq + e;
-        const int side = k < Z.lo ? 0 : 1;
-        const int zq = side ? k - (Z.n - Z.hi) : k;
-        const bool staged = zslab_staged(Z, side, k0);
-        for (int s = 0; s < 2; ++s)
-          pz[s][e] = staged ? st[kH_PZ + (s * 2 + side) * kTY * kZMax + w * (side ? Z.hi : Z.lo) + zq]
-                            : *psi_addr(P.psih, 2, s, Z, i, j, k, P.ny, P.nzp);
-      }
-      float idz4[4], mkz4[4];
-      unpack4(lds4(zt + 4 * lane), idz4);
-      unpack4(lds4(zt + kTZ + 4 * lane), mkz4);
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        if (!((kvm >> e) & 1u)) continue;
-        const int zi = 4 * lane + e;
-        const float idz = idz4[e], mkz = mkz4[e];
-        const bool zsl = (zslm >> e) & 1u;
         float zex = (e < 3) ? ex[e + 1] : ex4;
         float zey = (e < 3) ? ey[e + 1] : ey4;
         if ((zspm >> e) & 1u) {
-          const int kp = __float_as_int(zt[5 * kTZ + zi]);
+          const int kp = __float_as_int(zt[5 * kTZ + 4 * lane + e]);
           zex = P.f[0][row + kp];
           zey = P.f[1][row + kp];
         }
-        const float az = zsl ? zt[2 * kTZ + zi] : 0.f;
-        const float bz = zsl ? zt[3 * kTZ + zi] : 0.f;
-        const float kz = zsl ? zt[4 * kTZ + zi] : 0.f;
-        {  // Hx: -(dEz/dy - dEy/dz)
+        dyz[e] = fdiff(zey, mkz[e], ey[e], idz[e]);
+        dxz[e] = fdiff(zex, mkz[e], ex[e], idz[e]);
+      }
+      if (zslm) z_cpml(dyz, dxz, zslm, st + kH_PZ, zt, P.psih, P, Z, i, j, kq, k0, w, lane);
+      if (yplain && !xsl && i + 1 < P.nx && X.nxt[i] == i + 1 && mi == 1.0f) {
+        // x and y interior: unit masks, no x/y CPML (the same bits as below, n * 1 == n)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float nhx = h_new(hx[e], ch, __fmul_rn(__fsub_rn(yez[e], ez[e]), idy), dyz[e]);
+          const float nhy = h_new(hy[e], ch, dxz[e], __fmul_rn(__fsub_rn(nez[e], ez[e]), idx_));
+          const float nhz = h_new(hz[e], ch, __fmul_rn(__fsub_rn(ney[e], ey[e]), idx_),
+                                  __fmul_rn(__fsub_rn(yex[e], ex[e]), idy));
+          const bool kv = (kvm >> e) & 1u;
+          hx[e] = kv ? nhx : hx[e];
+          hy[e] = kv ? nhy : hy[e];
+          hz[e] = kv ? nhz : hz[e];
+        }
+      } else {
+        const float ay = Y.ah[jj], by = Y.bh[jj], ky = Y.kh[jj];
+        const float ax_ = X.ah[i], bx_ = X.bh[i], kx_ = X.kh[i];
+        // psi of this quad (x: Hy, Hz; y: Hx, Hz)
+        float px[2][4], py[2][4];
+        if (xsl)
+          for (int s = 0; s < 2; ++s) unpack4(lds4(st + kH_PX + (s * 4 + w) * kTZ + 4 * lane), px[s]);
+        if (ysl)
+          for (int s = 0; s < 2; ++s) unpack4(lds4(st + kH_PY + (s * 4 + w) * kTZ + 4 * lane), py[s]);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
           const float dzy = fdiff(yez[e], mj, ez[e], idy);
-          const float dyz = fdiff(zey, mkz, ey[e], idz);
-          const float sy = ysl ? cpml_stretch(dzy, py[0][e], ay, by, ky) : dzy;
-          const float sz = zsl ? cpml_stretch(dyz, pz[0][e], az, bz, kz) : dyz;
-          hx[e] = h_new(hx[e], ch, sy, sz);
-        }
-        {  // Hy: -(dEx/dz - dEz/dx)
-          const float dxz = fdiff(zex, mkz, ex[e], idz);
           const float dzx = fdiff(nez[e], mi, ez[e], idx_);
-          const float sz = zsl ? cpml_stretch(dxz, pz[1][e], az, bz, kz) : dxz;
-          const float sx = xsl ? cpml_stretch(dzx, px[0][e], ax_, bx_, kx_) : dzx;
-          hy[e] = h_new(hy[e], ch, sz, sx);
-        }
-        {  // Hz: -(dEy/dx - dEx/dy)
           const float dyx = fdiff(ney[e], mi, ey[e], idx_);
           const float dxy = fdiff(yex[e], mj, ex[e], idy);
-          const float sx = xsl ? cpml_stretch(dyx, px[1][e], ax_, bx_, kx_) : dyx;
-          const float sy = ysl ? cpml_stretch(dxy, py[1][e], ay, by, ky) : dxy;
-          hz[e] = h_new(hz[e], ch, sx, sy);
+          float sy0 = dzy, sy1 = dxy, sx0 = dzx, sx1 = dyx;
+          if (ysl) {
+            sy0 = cpml_stretch(dzy, py[0][e], ay, by, ky);
+            sy1 = cpml_stretch(dxy, py[1][e], ay, by, ky);
+          }
+          if (xsl) {
+            sx0 = cpml_stretch(dzx, px[0][e], ax_, bx_, kx_);
+            sx1 = cpml_stretch(dyx, px[1][e], ax_, bx_, kx_);
+          }
+          const bool kv = (kvm >> e) & 1u;
+          hx[e] = kv ? h_new(hx[e], ch, sy0, dyz[e]) : hx[e];  // -(dEz/dy - dEy/dz)
+          hy[e] = kv ? h_new(hy[e], ch, dxz[e], sx0) : hy[e];  // -(dEx/dz - dEz/dx)
+          hz[e] = kv ? h_new(hz[e], ch, sx1, sy1) : hz[e];     // -(dEy/dx - dEx/dy)
         }
-      }
-      if (xsl)
-        for (int s = 0; s < 2; ++s)
-          *reinterpret_cast<float4*>(psi_addr(P.psih, 0, s, X, i, j, kq, P.ny, P.nzp)) =
-              make_float4(px[s][0], px[s][1], px[s][2], px[s][3]);
-      if (ysl)
-        for (int s = 0; s < 2; ++s)
-          *reinterpret_cast<float4*>(psi_addr(P.psih, 1, s, Y, i, j, kq, P.ny, P.nzp)) =
-              make_float4(py[s][0], py[s][1], py[s][2], py[s][3]);
-#pragma unroll
-      for (int e = 0; e < 4; ++e)
-        if ((zslm >> e) & 1u)
+        if (xsl)
           for (int s = 0; s < 2; ++s)
-            *psi_addr(P.psih, 2, s, Z, i, j, kq + e, P.ny, P.nzp) = pz[s][e];
+            *reinterpret_cast<float4*>(psi_addr(P.psih, 0, s, X, i, j, kq, P.ny, P.nzp)) =
+                make_float4(px[s][0], px[s][1], px[s][2], px[s][3]);
+        if (ysl)
+          for (int s = 0; s < 2; ++s)
+            *reinterpret_cast<float4*>(psi_addr(P.psih, 1, s, Y, i, j, kq, P.ny, P.nzp)) =
+                make_float4(py[s][0], py[s][1], py[s][2], py[s][3]);
+      }
       *reinterpret_cast<float4*>(P.f[3] + row + kq) = make_float4(hx[0], hx[1], hx[2], hx[3]);
       *reinterpret_cast<float4*>(P.f[4] + row + kq) = make_float4(hy[0], hy[1], hy[2], hy[3]);
       *reinterpret_cast<float4*>(P.f[5] + row + kq) = make_float4(hz[0], hz[1], hz[2], hz[3]);
@@ -522,8 +526,6 @@ __global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps
   float* zt = reinterpret_cast<float*>(empty + kS);
   MatRec* smats = reinterpret_cast<MatRec*>(zt + kZTab);
   uint32_t* segt = reinterpret_cast<uint32_t*>(smats + kSmemMats);  // [plane][row][start, end]
-  float4* scoef = reinterpret_cast<float4*>(segt + kXMax * kTY * 2);
-  int* sofs = reinterpret_cast<int*>(scoef + kSmemCoef);
   const int lane = threadIdx.x, w = threadIdx.y;
   const int tid = w * 32 + lane;
   const int k0 = blockIdx.x * kTZ;
@@ -541,14 +543,6 @@ __global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps
     uint4* dst = reinterpret_cast<uint4*>(smats);
     for (int q = tid; q < n_mats * 4; q += 160) dst[q] = src[q];
     mats = smats;
-  }
-  const float4* coef = P.pcoef;
-  const int* set_ofs = P.pset_ofs;
-  if (P.has_ade && P.n_coef <= kSmemCoef && P.n_sets < kSmemSets) {
-    for (int q = tid; q < P.n_coef; q += 160) scoef[q] = P.pcoef[q];
-    for (int q = tid; q <= P.n_sets; q += 160) sofs[q] = P.pset_ofs[q];
-    coef = scoef;
-    set_ofs = sofs;
   }
   load_ztab(zt, Z, false, k0, P.nzp, tid, 160);
   if (w == 4 && lane == 0) {
@@ -588,7 +582,7 @@ __global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps
       const int i = ib + q;
       int offs[3];
       const int wbase = psi_pool_layout(P, i, j0, k0, offs);
-      const int cap = (kEPool - wbase) / 2;  // float2 pole states this plane can stage
+      const int cap = kEPool - wbase;  // pole currents (floats) this plane can stage
       int pstart[kTY], poff[kTY], pcnt[kTY];
       int used = 0;
 #pragma unroll
@@ -597,12 +591,12 @@ __global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps
         const uint32_t b = P.has_ade ? segt[2 * (q * kTY + r) + 1] : 0u;
         pstart[r] = (int)a; poff[r] = -2; pcnt[r] = 0;
         if (b <= a) continue;
-        const int a16 = (int)(a & ~1u);
-        const int n2 = (int)(((b - (uint32_t)a16) + 1u) & ~1u);
-        if (used + n2 <= cap) {
+        const int a16 = (int)(a & ~3u);  // 16-byte aligned start
+        const int n4 = (int)(((b - (uint32_t)a16) + 3u) & ~3u);
+        if (used + n4 <= cap) {
           poff[r] = used + ((int)a - a16);
-          pcnt[r] = n2;
-          used += n2;
+          pcnt[r] = n4;
+          used += n4;
         } else {
           poff[r] = -1;  // consumers read this row's poles from global memory
         }
@@ -613,7 +607,7 @@ __global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps
       int* tab = reinterpret_cast<int*>(st + kE_PT);
       const int iprev = (i > 0) ? i - 1 : X.prv[0];
       uint32_t bytes = 3 * kWideBytes + 5 * kTileBytes + mbytes + psi_bytes(P, i, j0, k0) +
-                       (uint32_t)used * 8;
+                       (uint32_t)used * 4;
 #pragma unroll
       for (int r = 0; r < kTY; ++r) {
         tab[2 * r] = pstart[r];
@@ -636,9 +630,9 @@ __global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps
 #pragma unroll
       for (int r = 0; r < kTY; ++r)
         if (pcnt[r] > 0) {
-          const int a16 = pstart[r] & ~1;
-          bulk(pool + wbase + 2 * (poff[r] - (pstart[r] - a16)), P.P + a16,
-               (uint32_t)pcnt[r] * 8, &full[slot]);
+          const int a16 = pstart[r] & ~3;
+          bulk(pool + wbase + (poff[r] - (pstart[r] - a16)), P.J + a16, (uint32_t)pcnt[r] * 4,
+               &full[slot]);
         }
       issued = q + 1;
     }
@@ -654,21 +648,19 @@ __global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps
   const int jm = Y.prv[jj];
   const float mj = Y.mpv[jj], idy = Y.idl_d[jj];
   const bool ysl = row_ok && in_slab(Y, j);
-  const bool yspecial = row_ok && jm != j - 1;
+  const bool yspecial = row_ok && jm != j - 1 && mj != 0.0f;  // see the H kernel
   const int kq = k0 + 4 * lane;
   unsigned kvm = 0, zslm = 0, zspm = 0;
-  bool zunit = true;
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
     const int k = kq + e;
     const bool kv = row_ok && k < P.nz;
     kvm |= (unsigned)kv << e;
     zslm |= (unsigned)(kv && in_slab(Z, k)) << e;
-    zspm |= (unsigned)(kv && __float_as_int(zt[5 * kTZ + 4 * lane + e]) != k - 1) << e;
-    zunit &= zt[kTZ + 4 * lane + e] == 1.0f;
+    zspm |= (unsigned)(kv && __float_as_int(zt[5 * kTZ + 4 * lane + e]) != k - 1 &&
+                       zt[kTZ + 4 * lane + e] != 0.0f) << e;
   }
-  const bool wplain = __all_sync(kFull, row_ok && !ysl && !yspecial && mj == 1.0f &&
-                                            kvm == 0xFu && zslm == 0u && zspm == 0u && zunit);
+  const bool yplain = row_ok && !ysl && !yspecial && mj == 1.0f;  // uniform over the warp
   const unsigned lt = (1u << lane) - 1u;
   const int64_t sj = P.nzp, si = (int64_t)P.ny * P.nzp;
   const float cw = P.cw;
@@ -678,11 +670,10 @@ __global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps
     const int slot = t % kS;
     const bool got = mbar_wait(&full[slot], (uint32_t)((t / kS) & 1), err);
     if (!__all_sync(kFull, got)) break;
-    float* stw = smem + slot * kEStage;
-    const float* st = stw;
+    const float* st = smem + slot * kEStage;
     const int* tab = reinterpret_cast<const int*>(st + kE_PT);
     const float* pool = st + kE_POOL;
-    const float2* ps = reinterpret_cast<const float2*>(pool + tab[11]);
+    const float* jw = pool + tab[11];  // pole currents of the plane's rows
     const int i = ib + t;
     uint32_t mid[4] = {0u, 0u, 0u, 0u};
     if (row_ok) {
@@ -699,82 +690,25 @@ __global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps
 #pragma unroll
       for (int e = 0; e < 4; ++e) lane_np += mats[mid[e]].reserved;
     }
-    // poles of this lane: global index gp, window index wp (-1: read from global memory)
+    // poles of this lane: global index gp, window index wp (-1: read J from global memory)
     uint32_t gp = 0;
     int wp = -1;
-    const bool any_poles = P.has_ade && __any_sync(kFull, lane_np > 0);
-    if (any_poles) {
+    if (P.has_ade && __any_sync(kFull, lane_np > 0)) {
       int pre = 0;
 #pragma unroll
       for (int b = 0; b < 8; ++b) pre += __popc(__ballot_sync(kFull, (lane_np >> b) & 1) & lt) << b;
       gp = (uint32_t)tab[2 * w] + (uint32_t)pre;
       if (tab[2 * w + 1] >= 0) wp = tab[2 * w + 1] + pre;
     }
-    float ex[4], ey[4], ez[4];
-    unpack4(lds4(st + kE_ET + to), ex);
-    unpack4(lds4(st + kE_ET + 512 + to), ey);
-    unpack4(lds4(st + kE_ET + 1024 + to), ez);
-    if (lane_np > 0) {
-      // deferred ADE of this lane's dispersive cells, one rolled loop; the polarisation
-      // currents replace E^n in the warp's own row of the stage (E^n is in registers now)
-      float* et = stw + kE_ET + to;
-#pragma unroll 1
-      for (int e = 0; e < 4; ++e) {
-        const MatRec& M = mats[mid_at(st + kE_MT, wide, to + e)];
-        const int npc = M.reserved;
-        if (npc == 0) continue;
-        const float en[3] = {et[e], et[512 + e], et[1024 + e]};
-        float wv[3];
-        ade_cell(P, coef, set_ofs, M, ps, wp, gp, en, wv);
-        et[e] = wv[0];
-        et[512 + e] = wv[1];
-        et[1024 + e] = wv[2];
-        gp += (uint32_t)npc;
-        if (wp >= 0) wp += npc;
-      }
-    }
     const bool xsl = in_slab(X, i);
     const float mi = X.mpv[i], idx_ = X.idl_d[i];
     const int64_t row = i * si + (int64_t)j * sj;
-    if (wplain && !xsl && i > 0 && X.prv[i] == i - 1 && mi == 1.0f) {
-      float hx[4], hy[4], hz[4], yhx[4], yhz[4], phy[4], phz[4], idz[4];
-      unpack4(lds4(st + kE_HB + ro), hx);
-      unpack4(lds4(st + kE_HB + kBoxW + ro), hy);
-      unpack4(lds4(st + kE_HB + 2 * kBoxW + ro), hz);
-      unpack4(lds4(st + kE_HB + ro - kBZ), yhx);
-      unpack4(lds4(st + kE_HB + 2 * kBoxW + ro - kBZ), yhz);
-      unpack4(lds4(st + kE_HP + to), phy);
-      unpack4(lds4(st + kE_HP + 512 + to), phz);
-      unpack4(lds4(zt + 4 * lane), idz);
-      const float hxm = st[kE_HB + ro - 1];
-      const float hym = st[kE_HB + kBoxW + ro - 1];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const MatRec& M = mats[mid[e]];
-        const float4 cab = *reinterpret_cast<const float4*>(&M.ca[0]);
-        const float2 cb12 = *reinterpret_cast<const float2*>(&M.cb[1]);
-        const float zhx = (e > 0) ? hx[e - 1] : hxm;
-        const float zhy = (e > 0) ? hy[e - 1] : hym;
-        float wv[3] = {0.f, 0.f, 0.f};
-        if (lane_np > 0 && M.reserved > 0) {
-          wv[0] = st[kE_ET + to + e];
-          wv[1] = st[kE_ET + 512 + to + e];
-          wv[2] = st[kE_ET + 1024 + to + e];
-        }
-        ex[e] = e_new(cab.x, ex[e], cab.w, __fmul_rn(__fsub_rn(hz[e], yhz[e]), idy),
-                      __fmul_rn(__fsub_rn(hy[e], zhy), idz[e]), cw, wv[0]);
-        ey[e] = e_new(cab.y, ey[e], cb12.x, __fmul_rn(__fsub_rn(hx[e], zhx), idz[e]),
-                      __fmul_rn(__fsub_rn(hz[e], phz[e]), idx_), cw, wv[1]);
-        ez[e] = e_new(cab.z, ez[e], cb12.y, __fmul_rn(__fsub_rn(hy[e], phy[e]), idx_),
-                      __fmul_rn(__fsub_rn(hx[e], yhx[e]), idy), cw, wv[2]);
-      }
-      *reinterpret_cast<float4*>(P.f[0] + row + kq) = make_float4(ex[0], ex[1], ex[2], ex[3]);
-      *reinterpret_cast<float4*>(P.f[1] + row + kq) = make_float4(ey[0], ey[1], ey[2], ey[3]);
-      *reinterpret_cast<float4*>(P.f[2] + row + kq) = make_float4(ez[0], ez[1], ez[2], ez[3]);
-    } else if (kvm) {
-      const float ay = Y.ae[jj], by = Y.be[jj], ky = Y.ke[jj];
-      const float ax_ = X.ae[i], bx_ = X.be[i], kx_ = X.ke[i];
-      float hx[4], hy[4], hz[4], yhx[4], yhz[4], phy[4], phz[4];
+    if (kvm) {
+      float ex[4], ey[4], ez[4], hx[4], hy[4], hz[4], yhx[4], yhz[4], phy[4], phz[4];
+      float idz[4], mkz[4];
+      unpack4(lds4(st + kE_ET + to), ex);
+      unpack4(lds4(st + kE_ET + 512 + to), ey);
+      unpack4(lds4(st + kE_ET + 1024 + to), ez);
       unpack4(lds4(st + kE_HB + ro), hx);
       unpack4(lds4(st + kE_HB + kBoxW + ro), hy);
       unpack4(lds4(st + kE_HB + 2 * kBoxW + ro), hz);
@@ -788,87 +722,86 @@ __global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps
       }
       unpack4(lds4(st + kE_HP + to), phy);
       unpack4(lds4(st + kE_HP + 512 + to), phz);
+      unpack4(lds4(zt + 4 * lane), idz);
+      unpack4(lds4(zt + kTZ + 4 * lane), mkz);
       const float hxm = st[kE_HB + ro - 1];
       const float hym = st[kE_HB + kBoxW + ro - 1];
-      float px[2][4], py[2][4], pz[2][4];
-      if (xsl)
-        for (int s = 0; s < 2; ++s) unpack4(lds4(pool + tab[8] + (s * 4 + w) * kTZ + 4 * lane), px[s]);
-      if (ysl)
-        for (int s = 0; s < 2; ++s) unpack4(lds4(pool + tab[9] + (s * 4 + w) * kTZ + 4 * lane), py[s]);
+      // z derivatives of all four cells, then the z CPML of the slab lanes in one block
+      float dyz[4], dxz[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        if (!((zslm >> e) & 1u)) continue;
-        const int k = kq + e;
-        const int side = k < Z.lo ? 0 : 1;
-        const int zq = side ? k - (Z.n - Z.hi) : k;
-        const bool staged = zslab_staged(Z, side, k0);
-        for (int s = 0; s < 2; ++s)
-          pz[s][e] = staged ? pool[tab[10] + (s * 2 + side) * kTY * kZMax + w * (side ? Z.hi : Z.lo) + zq]
-                            : *psi_addr(P.psie, 2, s, Z, i, j, k, P.ny, P.nzp);
-      }
-      float idz4[4], mkz4[4];
-      unpack4(lds4(zt + 4 * lane), idz4);
-      unpack4(lds4(zt + kTZ + 4 * lane), mkz4);
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        if (!((kvm >> e) & 1u)) continue;
-        const int zi = 4 * lane + e;
-        const float idz = idz4[e], mkz = mkz4[e];
-        const bool zsl = (zslm >> e) & 1u;
-        const MatRec& M = mats[mid[e]];
-        const float4 cab = *reinterpret_cast<const float4*>(&M.ca[0]);
-        const float2 cb12 = *reinterpret_cast<const float2*>(&M.cb[1]);
         float zhx = (e > 0) ? hx[e - 1] : hxm;
         float zhy = (e > 0) ? hy[e - 1] : hym;
         if ((zspm >> e) & 1u) {
-          const int km = __float_as_int(zt[5 * kTZ + zi]);
+          const int km = __float_as_int(zt[5 * kTZ + 4 * lane + e]);
           zhx = P.f[3][row + km];
           zhy = P.f[4][row + km];
         }
+        dyz[e] = bdiff(hy[e], zhy, mkz[e], idz[e]);  // dHy/dz
+        dxz[e] = bdiff(hx[e], zhx, mkz[e], idz[e]);  // dHx/dz
+      }
+      if (zslm) z_cpml(dyz, dxz, zslm, pool + tab[10], zt, P.psie, P, Z, i, j, kq, k0, w, lane);
+      // x and y derivatives (CPML on the x/y slab planes and rows)
+      float sy0[4], sy1[4], sx0[4], sx1[4];
+      if (yplain && !xsl && i > 0 && X.prv[i] == i - 1 && mi == 1.0f) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          sy0[e] = __fmul_rn(__fsub_rn(hz[e], yhz[e]), idy);   // dHz/dy
+          sx0[e] = __fmul_rn(__fsub_rn(hz[e], phz[e]), idx_);  // dHz/dx
+          sx1[e] = __fmul_rn(__fsub_rn(hy[e], phy[e]), idx_);  // dHy/dx
+          sy1[e] = __fmul_rn(__fsub_rn(hx[e], yhx[e]), idy);   // dHx/dy
+        }
+      } else {
+        const float ay = Y.ae[jj], by = Y.be[jj], ky = Y.ke[jj];
+        const float ax_ = X.ae[i], bx_ = X.be[i], kx_ = X.ke[i];
+        float px[2][4], py[2][4];
+        if (xsl)
+          for (int s = 0; s < 2; ++s) unpack4(lds4(pool + tab[8] + (s * 4 + w) * kTZ + 4 * lane), px[s]);
+        if (ysl)
+          for (int s = 0; s < 2; ++s) unpack4(lds4(pool + tab[9] + (s * 4 + w) * kTZ + 4 * lane), py[s]);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          sy0[e] = bdiff(hz[e], yhz[e], mj, idy);
+          sx0[e] = bdiff(hz[e], phz[e], mi, idx_);
+          sx1[e] = bdiff(hy[e], phy[e], mi, idx_);
+          sy1[e] = bdiff(hx[e], yhx[e], mj, idy);
+          if (ysl) {
+            sy0[e] = cpml_stretch(sy0[e], py[0][e], ay, by, ky);
+            sy1[e] = cpml_stretch(sy1[e], py[1][e], ay, by, ky);
+          }
+          if (xsl) {
+            sx0[e] = cpml_stretch(sx0[e], px[0][e], ax_, bx_, kx_);
+            sx1[e] = cpml_stretch(sx1[e], px[1][e], ax_, bx_, kx_);
+          }
+        }
+        if (xsl)
+          for (int s = 0; s < 2; ++s)
+            *reinterpret_cast<float4*>(psi_addr(P.psie, 0, s, X, i, j, kq, P.ny, P.nzp)) =
+                make_float4(px[s][0], px[s][1], px[s][2], px[s][3]);
+        if (ysl)
+          for (int s = 0; s < 2; ++s)
+            *reinterpret_cast<float4*>(psi_addr(P.psie, 1, s, Y, i, j, kq, P.ny, P.nzp)) =
+                make_float4(py[s][0], py[s][1], py[s][2], py[s][3]);
+      }
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const MatRec& M = mats[mid[e]];
+        const float4 cab = *reinterpret_cast<const float4*>(&M.ca[0]);
+        const float2 cb12 = *reinterpret_cast<const float2*>(&M.cb[1]);
         float wv[3] = {0.f, 0.f, 0.f};
         if (lane_np > 0 && M.reserved > 0) {
-          wv[0] = st[kE_ET + to + e];
-          wv[1] = st[kE_ET + 512 + to + e];
-          wv[2] = st[kE_ET + 1024 + to + e];
+          cell_currents(M, jw, wp, P.J, gp, wv);
+          gp += (uint32_t)M.reserved;
+          if (wp >= 0) wp += M.reserved;
         }
-        const float az = zsl ? zt[2 * kTZ + zi] : 0.f;
-        const float bz = zsl ? zt[3 * kTZ + zi] : 0.f;
-        const float kz = zsl ? zt[4 * kTZ + zi] : 0.f;
-        {  // Ex: dHz/dy - dHy/dz
-          const float dzy = bdiff(hz[e], yhz[e], mj, idy);
-          const float dyz = bdiff(hy[e], zhy, mkz, idz);
-          const float sy = ysl ? cpml_stretch(dzy, py[0][e], ay, by, ky) : dzy;
-          const float sz = zsl ? cpml_stretch(dyz, pz[0][e], az, bz, kz) : dyz;
-          ex[e] = e_new(cab.x, ex[e], cab.w, sy, sz, cw, wv[0]);
-        }
-        {  // Ey: dHx/dz - dHz/dx
-          const float dxz = bdiff(hx[e], zhx, mkz, idz);
-          const float dzx = bdiff(hz[e], phz[e], mi, idx_);
-          const float sz = zsl ? cpml_stretch(dxz, pz[1][e], az, bz, kz) : dxz;
-          const float sx = xsl ? cpml_stretch(dzx, px[0][e], ax_, bx_, kx_) : dzx;
-          ey[e] = e_new(cab.y, ey[e], cb12.x, sz, sx, cw, wv[1]);
-        }
-        {  // Ez: dHy/dx - dHx/dy
-          const float dyx = bdiff(hy[e], phy[e], mi, idx_);
-          const float dxy = bdiff(hx[e], yhx[e], mj, idy);
-          const float sx = xsl ? cpml_stretch(dyx, px[1][e], ax_, bx_, kx_) : dyx;
-          const float sy = ysl ? cpml_stretch(dxy, py[1][e], ay, by, ky) : dxy;
-          ez[e] = e_new(cab.z, ez[e], cb12.y, sx, sy, cw, wv[2]);
-        }
+        const bool kv = (kvm >> e) & 1u;
+        const float nex = e_new(cab.x, ex[e], cab.w, sy0[e], dyz[e], cw, wv[0]);   // dHz/dy - dHy/dz
+        const float ney = e_new(cab.y, ey[e], cb12.x, dxz[e], sx0[e], cw, wv[1]);  // dHx/dz - dHz/dx
+        const float nez = e_new(cab.z, ez[e], cb12.y, sx1[e], sy1[e], cw, wv[2]);  // dHy/dx - dHx/dy
+        ex[e] = kv ? nex : ex[e];
+        ey[e] = kv ? ney : ey[e];
+        ez[e] = kv ? nez : ez[e];
       }
-      if (xsl)
-        for (int s = 0; s < 2; ++s)
-          *reinterpret_cast<float4*>(psi_addr(P.psie, 0, s, X, i, j, kq, P.ny, P.nzp)) =
-              make_float4(px[s][0], px[s][1], px[s][2], px[s][3]);
-      if (ysl)
-        for (int s = 0; s < 2; ++s)
-          *reinterpret_cast<float4*>(psi_addr(P.psie, 1, s, Y, i, j, kq, P.ny, P.nzp)) =
-              make_float4(py[s][0], py[s][1], py[s][2], py[s][3]);
-#pragma unroll
-      for (int e = 0; e < 4; ++e)
-        if ((zslm >> e) & 1u)
-          for (int s = 0; s < 2; ++s)
-            *psi_addr(P.psie, 2, s, Z, i, j, kq + e, P.ny, P.nzp) = pz[s][e];
       *reinterpret_cast<float4*>(P.f[0] + row + kq) = make_float4(ex[0], ex[1], ex[2], ex[3]);
       *reinterpret_cast<float4*>(P.f[1] + row + kq) = make_float4(ey[0], ey[1], ey[2], ey[3]);
       *reinterpret_cast<float4*>(P.f[2] + row + kq) = make_float4(ez[0], ez[1], ez[2], ez[3]);
@@ -883,8 +816,7 @@ __global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps
 size_t ws_h_smem() { return (size_t)kS * kHStage * 4 + 2 * kS * sizeof(uint64_t) + kZTab * 4; }
 size_t ws_e_smem() {
   return (size_t)kS * kEStage * 4 + 2 * kS * sizeof(uint64_t) + kZTab * 4 +
-         kSmemMats * sizeof(MatRec) + kXMax * kTY * 2 * sizeof(uint32_t) +
-         kSmemCoef * sizeof(float4) + kSmemSets * sizeof(int);
+         kSmemMats * sizeof(MatRec) + kXMax * kTY * 2 * sizeof(uint32_t);
 }
 
 int ws_max_xchunk() { return kXMax; }
