@@ -32,22 +32,12 @@ __global__ void k_list_pole_segments(const uint32_t* seg, int64_t nseg, uint32_t
   }
 }
 
-__global__ void __launch_bounds__(256) k_ade_segments(YeeParams P, const int64_t* segs,
-                                                      int64_t nsegs) {
-  const int lane = threadIdx.x & 31;
-  const int64_t q = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
-  if (q >= nsegs) return;  // warp-uniform
-  const int64_t s = segs[q];
-  const int64_t cell = s * 32 + lane;
-  const uint32_t m = P.mat16 ? (uint32_t)P.mat16[cell] : P.mat32[cell];
-  const MatRec& M = P.mats[m];
-  const int npc = M.reserved;
-  const unsigned lt = (1u << lane) - 1u;
-  int pre = 0;
-#pragma unroll
-  for (int b = 0; b < 6; ++b) pre += __popc(__ballot_sync(kFull, (npc >> b) & 1) & lt) << b;
-  if (npc == 0) return;
-  const uint32_t gp = P.seg_ofs[s] + (uint32_t)pre;
+constexpr int kSegPoles = 256;  // pole states of one segment staged per warp
+
+// The pole update of one cell on states held in `st` (shared or global memory), J written to
+// the cell's first pole of each component.
+__device__ __forceinline__ void ade_cell_poles(const YeeParams& P, const MatRec& M, float2* st,
+                                               uint32_t gp, int64_t cell) {
   int po = 0;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -58,23 +48,60 @@ __global__ void __launch_bounds__(256) k_ade_segments(YeeParams P, const int64_t
     float acc = 0.f;
     int tt = 0;
     for (; tt + 1 < n; tt += 2) {
-      const uint32_t g = gp + (uint32_t)(po + tt);
-      float2 s0 = P.P[g], s1 = P.P[g + 1];
+      float2 s0 = st[po + tt], s1 = st[po + tt + 1];
       const float d0 = ade_pole(s0, __ldg(cf + tt), en);
       const float d1 = ade_pole(s1, __ldg(cf + tt + 1), en);
-      P.P[g] = s0;
-      P.P[g + 1] = s1;
+      st[po + tt] = s0;
+      st[po + tt + 1] = s1;
       acc = __fadd_rn(__fadd_rn(acc, d0), d1);
     }
     if (tt < n) {
-      const uint32_t g = gp + (uint32_t)(po + tt);
-      float2 s0 = P.P[g];
+      float2 s0 = st[po + tt];
       acc = __fadd_rn(acc, ade_pole(s0, __ldg(cf + tt), en));
-      P.P[g] = s0;
+      st[po + tt] = s0;
     }
     P.J[gp + (uint32_t)po] = acc;
     po += n;
   }
+}
+
+// One segment on one warp: its poles (contiguous in memory) are read into shared memory with
+// coalesced loads, updated there cell by cell, and written back coalesced; a segment with more
+// poles than the buffer holds is updated in place in global memory.
+__device__ __forceinline__ void ade_segment(const YeeParams& P, int64_t s, int64_t nseg,
+                                            float2* st, int lane) {
+  const int64_t cell = s * 32 + lane;
+  const uint32_t a = P.seg_ofs[s];
+  const uint32_t b = (s + 1 < nseg) ? P.seg_ofs[s + 1] : P.n_pole_total;
+  const int n = (int)(b - a);
+  const uint32_t m = P.mat16 ? (uint32_t)P.mat16[cell] : P.mat32[cell];
+  const MatRec& M = P.mats[m];
+  const int npc = M.reserved;
+  const unsigned lt = (1u << lane) - 1u;
+  int pre = 0;
+#pragma unroll
+  for (int bb = 0; bb < 6; ++bb) pre += __popc(__ballot_sync(kFull, (npc >> bb) & 1) & lt) << bb;
+  if (n <= kSegPoles) {
+    for (int t = lane; t < n; t += 32) st[t] = P.P[a + t];
+    __syncwarp();
+    if (npc > 0) ade_cell_poles(P, M, st + pre, a + (uint32_t)pre, cell);
+    __syncwarp();
+    for (int t = lane; t < n; t += 32) P.P[a + t] = st[t];
+    __syncwarp();
+  } else if (npc > 0) {
+    ade_cell_poles(P, M, P.P + a + pre, a + (uint32_t)pre, cell);
+  }
+}
+
+// One warp per listed segment (a grid-stride loop when the grid is capped). In the captured
+// step it runs on its own graph branch beside the H update.
+__global__ void __launch_bounds__(256) k_ade_segments(YeeParams P, const int64_t* segs,
+                                                      int64_t nsegs, int64_t nseg) {
+  __shared__ float2 buf[8][kSegPoles];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  for (int64_t q = (int64_t)blockIdx.x * 8 + w; q < nsegs; q += (int64_t)gridDim.x * 8)
+    ade_segment(P, segs[q], nseg, buf[w], lane);
 }
 
 }  // namespace
@@ -88,10 +115,11 @@ cudaError_t launch_list_pole_segments(const YeeParams& P, int64_t nseg, int64_t*
 }
 
 cudaError_t launch_ade_segments(const YeeParams& P, const int64_t* segs, int64_t nsegs,
-                                cudaStream_t s) {
+                                int64_t nseg, int max_blocks, cudaStream_t s) {
   if (nsegs <= 0) return cudaSuccess;
-  const int64_t blocks = (nsegs + 7) / 8;
-  k_ade_segments<<<(unsigned)blocks, 256, 0, s>>>(P, segs, nsegs);
+  int64_t blocks = (nsegs + 7) / 8;
+  if (max_blocks > 0 && blocks > max_blocks) blocks = max_blocks;
+  k_ade_segments<<<(unsigned)blocks, 256, 0, s>>>(P, segs, nsegs, nseg);
   return cudaGetLastError();
 }
 

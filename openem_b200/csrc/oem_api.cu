@@ -146,7 +146,8 @@ static cudaError_t run_e(oem_plan* p, cudaStream_t s) {
   if (p->basic_kernels == 2) return launch_update_e_stream(p->yp, p->xch, (int)p->mats.size(), s);
   if (p->basic_kernels == 3) {
     if (p->yp.has_ade) {
-      cudaError_t e = launch_ade_segments(p->yp, p->d_ade_segs, p->n_ade_segs, s);
+      cudaError_t e = launch_ade_segments(p->yp, p->d_ade_segs, p->n_ade_segs,
+                                          (int64_t)p->nx * p->ny * p->nzp / 32, 0, s);
       if (e != cudaSuccess) return e;
     }
     return launch_update_e_ws(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s);
@@ -223,6 +224,18 @@ static int check_device_error(oem_plan* p) {
 static int enqueue_step(oem_plan* p, cudaStream_t s) {
   const YeeParams& P = p->yp;
   cudaError_t e;
+  // the pole pass depends on E^n only: it runs on a branch beside the H update and joins
+  // before the E update
+  const bool fork = p->side_stream != nullptr;
+  if (fork) {
+    OEM_CUDA(cudaEventRecord(p->ev_fork, s));
+    OEM_CUDA(cudaStreamWaitEvent(p->side_stream, p->ev_fork, 0));
+    if ((e = launch_ade_segments(P, p->d_ade_segs, p->n_ade_segs,
+                                 (int64_t)p->nx * p->ny * p->nzp / 32, 0, p->side_stream)) !=
+        cudaSuccess)
+      return cuda_error(e, "ade");
+    OEM_CUDA(cudaEventRecord(p->ev_join, p->side_stream));
+  }
   if ((e = run_h(p, s)) != cudaSuccess) return cuda_error(e, "update_h");
   for (const DipoleSet& d : p->dipoles)
     if (d.magnetic && (e = launch_dipoles(P, d, p->d_step, s)) != cudaSuccess)
@@ -230,7 +243,13 @@ static int enqueue_step(oem_plan* p, cudaStream_t s) {
   for (const PlaneSrc& src : p->planes)
     if ((e = launch_plane_h(P, src, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "plane_h");
-  if ((e = run_e(p, s)) != cudaSuccess) return cuda_error(e, "update_e");
+  if (fork) {
+    OEM_CUDA(cudaStreamWaitEvent(s, p->ev_join, 0));
+    e = launch_update_e_ws(p->tma, P, p->xch, (int)p->mats.size(), p->d_err, s);
+  } else {
+    e = run_e(p, s);
+  }
+  if (e != cudaSuccess) return cuda_error(e, "update_e");
   for (const PlaneSrc& src : p->planes)
     if ((e = launch_plane_e(P, src, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "plane_e");
@@ -317,6 +336,9 @@ int oem_plan_destroy(oem_plan* p) {
   if (p->graph_many) cudaGraphExecDestroy(p->graph_many);
   if (p->graph_one) cudaGraphExecDestroy(p->graph_one);
   if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
+  if (p->side_stream) cudaStreamDestroy(p->side_stream);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  if (p->ev_join) cudaEventDestroy(p->ev_join);
   for (void* a : p->allocs) cudaFree(a);
   delete p;
   return OEM_OK;
@@ -797,6 +819,11 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   if ((rc = dalloc(p, &p->d_energy_part, 3 * (size_t)p->energy_blocks))) return rc;
   // capture: G steps per graph for small grids (launch overhead), 1 for large ones
   OEM_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
+  if (p->basic_kernels == 3 && P.has_ade && p->n_ade_segs > 0) {
+    OEM_CUDA(cudaStreamCreateWithFlags(&p->side_stream, cudaStreamNonBlocking));
+    OEM_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+    OEM_CUDA(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
+  }
   const double cells = (double)ncp;
   int G = (int)std::min(32.0, std::max(1.0, 4.0e6 / cells));
   p->graph_steps = G;
@@ -838,7 +865,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       const bool split = p->basic_kernels == 3 && p->yp.has_ade;
       if (split) {
         // the pole pass and the E kernel timed apart
-        if ((e = launch_ade_segments(p->yp, p->d_ade_segs, p->n_ade_segs, s)) != cudaSuccess)
+        if ((e = launch_ade_segments(p->yp, p->d_ade_segs, p->n_ade_segs,
+                                     (int64_t)p->nx * p->ny * p->nzp / 32, 0, s)) != cudaSuccess)
           return cuda_error(e, "ade");
         OEM_CUDA(cudaEventRecord(E[5], s));
         e = launch_update_e_ws(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s);

@@ -209,6 +209,8 @@ struct oem_plan {
   int* d_err = nullptr;   // set by a kernel whose bounded wait gave up
   int64_t* d_ade_segs = nullptr;  // segments with poles (separate pole pass)
   int64_t n_ade_segs = 0;
+  cudaStream_t side_stream = nullptr;  // branch of the captured step that runs the pole pass
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int xch = 8;            // x planes per thread in the streaming kernels
 };
 
@@ -281,7 +283,7 @@ cudaError_t launch_update_e_stream(const YeeParams& P, int xch, int n_mats, cuda
 cudaError_t launch_list_pole_segments(const YeeParams& P, int64_t nseg, int64_t* list,
                                       unsigned long long* count, cudaStream_t s);
 cudaError_t launch_ade_segments(const YeeParams& P, const int64_t* segs, int64_t nsegs,
-                                cudaStream_t s);
+                                int64_t nseg, int max_blocks, cudaStream_t s);
 cudaError_t launch_energy(const YeeParams& P, double* const dl[3][2], double* part, int nblocks,
                           cudaStream_t s);
 int energy_block_count(const YeeParams& P);

@@ -269,19 +269,21 @@ __global__ void k_snap_plane(YeeParams P, Monitor m, const int* step) {
 }
 
 // DFT snapshot of a box: the six components at their Yee positions
-// (openem/kernels/source_dft.cu:453-478).
+// (openem/kernels/source_dft.cu:453-478). Threads cover one (j, k) plane of the box with a
+// 32-bit index; blockIdx.y walks the x planes.
 __global__ void k_snap_box(YeeParams P, Monitor m, const int* step) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= m.cells) return;
-  const int64_t njk = (int64_t)m.nj * m.nk;
-  const int a = (int)(t / njk);
-  const int64_t r = t - a * njk;
-  const int b = (int)(r / m.nk);
-  const int cc = (int)(r - (int64_t)b * m.nk);
-  const int64_t id = ((int64_t)(m.i0 + a) * P.ny + (m.j0 + b)) * P.nzp + (m.k0 + cc);
+  const uint32_t njk = (uint32_t)m.nj * (uint32_t)m.nk;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= njk) return;
+  const uint32_t b = t / (uint32_t)m.nk;
+  const uint32_t cc = t - b * (uint32_t)m.nk;
   float* row = m.d_snap + (int64_t)((*step) % m.T) * 6 * m.cells;
+  for (int a = blockIdx.y; a < m.ni; a += gridDim.y) {
+    const int64_t id = ((int64_t)(m.i0 + a) * P.ny + (m.j0 + (int)b)) * P.nzp + (m.k0 + (int)cc);
+    const int64_t o = (int64_t)a * njk + t;
 #pragma unroll
-  for (int q = 0; q < 6; ++q) row[q * m.cells + t] = P.f[q][id];
+    for (int q = 0; q < 6; ++q) row[q * m.cells + o] = P.f[q][id];
+  }
 }
 
 // Batched DFT flush (openem/kernels/source_dft.cu:440-530): at a batch boundary, or when
@@ -290,13 +292,15 @@ __global__ void k_snap_box(YeeParams P, Monitor m, const int* step) {
 // added to the float64 accumulator once. done[0] holds the last step already folded.
 template <int NC>
 __global__ void __launch_bounds__(128) k_flush(Monitor m, const int* step, int forced) {
-  const int64_t pt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (pt >= m.cells) return;
   const int s_now = forced ? (*step - 1) : *step;
   if (!forced && ((s_now + 1) % m.T) != 0) return;
   const int s_lo = *m.d_done + 1;
   if (s_lo > s_now) return;
   constexpr int NE = NC / 2;  // E components come first
+  // grid-stride over the points: a few blocks per SM, so that the launch of a step without a
+  // batch boundary costs little
+  for (int64_t pt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pt < m.cells;
+       pt += (int64_t)gridDim.x * blockDim.x)
   for (int f0 = 0; f0 < m.nf; f0 += 8) {
     const int nfc = min(8, m.nf - f0);
     float aR[8][NC], aI[8][NC];
@@ -487,14 +491,16 @@ cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* ste
     dim3 b(32, 4, 1), g((m.n2 + 31) / 32, (m.n1 + 3) / 4, 1);
     k_snap_plane<<<g, b, 0, s>>>(P, m, step);
   } else {
-    const int64_t nb = (m.cells + 255) / 256;
-    k_snap_box<<<(unsigned)nb, 256, 0, s>>>(P, m, step);
+    const int64_t njk = (int64_t)m.nj * m.nk;
+    if (njk >= (1LL << 31)) return cudaErrorInvalidValue;  // one box plane per 32-bit index
+    dim3 g((unsigned)((njk + 255) / 256), (unsigned)std::min(m.ni, 65535), 1);
+    k_snap_box<<<g, 256, 0, s>>>(P, m, step);
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_flush(const Monitor& m, const int* step, int forced, cudaStream_t s) {
-  const int64_t nb = (m.cells + 127) / 128;
+  const int64_t nb = std::min<int64_t>((m.cells + 127) / 128, 148 * 8);
   if (m.ncomp == 4)
     k_flush<4><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
   else

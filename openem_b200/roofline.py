@@ -60,11 +60,20 @@ def step_bytes_per_cell(sc) -> float:
 
 
 def kernel_bytes(sc) -> dict:
-    """Algorithmic bytes per launch of this engine's two update kernels."""
+    """Algorithmic bytes per launch of this engine's step kernels.
+
+    ``update_h``: E read, H read and written (36 B per cell) plus the H-side psi of the slab
+    cells. ``update_e``: H read, E read and written, the material index (38 B per cell), the
+    E-side psi, and one float32 polarisation current per dispersive (component, cell) entry.
+    ``ade`` (the separate pole pass): each pole state read and written (16 B), and per entry
+    E^n read and the current written (8 B)."""
     c = counts(sc)
     n = c["ncell"]
     psi = 16.0 * sum(c["slab_cells"].values())
-    return {"update_h": 36.0 * n + psi, "update_e": 38.0 * n + psi + 16.0 * c["n_pole"]}
+    n_entry = 0 if sc.dispersion is None else int(sc.dispersion.n_entry)
+    return {"update_h": 36.0 * n + psi,
+            "update_e": 38.0 * n + psi + 4.0 * n_entry,
+            "ade": 16.0 * c["n_pole"] + 8.0 * n_entry}
 
 
 def measured_peaks(root=None) -> dict:
