@@ -102,6 +102,38 @@ int oem_plan_add_dipoles(oem_plan* p, int magnetic, int n_pts, const int32_t* ij
                          const int32_t* comp, const float* coef, const int32_t* src, int n_src,
                          int64_t nsteps1, const double* amp);
 
+/* Mode / Gaussian-beam / oblique plane-wave source: one-plane TF/SF injection with 2D complex
+ * profiles (replaces inject_mode_h/_e, openem/kernels/source_dft.cu:84-128, their complex
+ * variants inject_mode_h_c/_e_c, openem/kernels/bloch.cu:326-384, and the host tables of
+ * openem/sources_setup.py:321-416). The tangential pair is cyclic, t1 = (axis+1)%3,
+ * t2 = (axis+2)%3; n1 x n2 is the whole plane (n_t1, n_t2). profiles: (n_terms, 8, n1, n2)
+ * float32 = E_t1 re, E_t1 im, E_t2 re, E_t2 im, H_t1 re, H_t1 im, H_t2 re, H_t2 im for the base
+ * term then the broadband corrections; amp_e / amp_h: (n_terms, ntab, 2) float64 (re, im) of
+ * amp(n dt) and amp((n+1/2) dt). After the H update of step n, H_t1[kh] += coef_h1 * E_t2 amp_e,
+ * H_t2[kh] += coef_h2 * E_t1 amp_e; after the E update, E_t1[ks] += cb * coef_e1 * H_t2 amp_h,
+ * E_t2[ks] += cb * coef_e2 * H_t1 amp_h. A real plan adds the real part of each product, a
+ * complex plan the whole product. */
+int oem_plan_add_mode_source(oem_plan* p, int axis, int kh, int ks, int n1, int n2,
+                             double coef_h1, double coef_h2, double coef_e1, double coef_e2,
+                             int n_terms, const float* profiles, int64_t ntab,
+                             const double* amp_e, const double* amp_h);
+
+/* Complex (Bloch) plan: imaginary parts of the neighbour masks of one axis (the real parts come
+ * from oem_plan_set_axis), exp(+-i 2 pi k) at the periodic seam of a Bloch axis
+ * (openem/grid.py:219-252). The first call makes the plan complex: every field and psi gets an
+ * imaginary array, the updates become openem/kernels/bloch.cu:38-221, and monitors and time
+ * samples record complex values. Call after oem_plan_set_axis and before adding sources or
+ * monitors. Complex plans take no dispersive media (OEM_ERR_UNSUPPORTED at finalize), the
+ * subset of openem/solver.py:1221-1260. */
+int oem_plan_set_axis_phase(oem_plan* p, int axis, const double* mnx_im, const double* mpv_im);
+
+/* Point dipoles on a complex plan: as oem_plan_add_dipoles with the complex amplitude split in
+ * two tables (openem/kernels/bloch.cu:226-278). */
+int oem_plan_add_dipoles_complex(oem_plan* p, int magnetic, int n_pts, const int32_t* ijk,
+                                 const int32_t* comp, const float* coef, const int32_t* src,
+                                 int n_src, int64_t nsteps1, const double* amp_re,
+                                 const double* amp_im);
+
 /* DFT monitors (openem/kernels/source_dft.cu:208-779, openem/monitors_setup.py:74-255).
  * phase: (n_total, nf, 4) float32 rows (cos, sin at E time (n+1)dt, cos, sin at H time
  * (n+1/2)dt), apodisation window already multiplied in. Accumulators are float64.
@@ -143,6 +175,12 @@ int oem_plan_launches_per_step(oem_plan* p, int* n);
 
 /* Steps taken so far (host-side count). */
 int oem_plan_steps(oem_plan* p, int64_t* steps);
+
+/* Complex plan readout: the real and imaginary (nx, ny, nz) float32 parts of one field
+ * component; and the real and imaginary sample buffers of a time monitor
+ * (openem/solver.py:1410-1436, _readout_c). */
+int oem_plan_read_field_complex(oem_plan* p, int comp, float* re, float* im, void* stream);
+int oem_plan_read_time_monitor_complex(oem_plan* p, int id, float* re, float* im, void* stream);
 
 /* Readout, synchronous on `stream`: DFT accumulators (ncomp, nf, points) float64 real and
  * imaginary parts; time samples (nc, nslots, ni, nj, nk) float32; one field component

@@ -76,6 +76,11 @@ static int upload_axis(oem_plan* p, int a) {
   UPF(idl_d, h.idl_d, 0, 1.0);
   UPF(mnx, h.mnx, 0, 0.0);
   UPF(mpv, h.mpv, 0, 0.0);
+  if (p->is_complex) {
+    const std::vector<double> zero(n, 0.0);
+    UPF(mnx_i, (h.mnx_i.empty() ? zero : h.mnx_i), 0, 0.0);
+    UPF(mpv_i, (h.mpv_i.empty() ? zero : h.mpv_i), 0, 0.0);
+  }
   UPF(ae, h.pml_e, 0, 0.0);
   UPF(be, h.pml_e, n, 1.0);
   UPF(ke, h.pml_e, 2 * (size_t)n, 1.0);
@@ -122,12 +127,20 @@ static int alloc_psi(oem_plan* p) {
       for (int slot = 0; slot < 2; ++slot) {
         float* ph = nullptr;
         float* pe = nullptr;
+        float* phi = nullptr;
+        float* pei = nullptr;
         if (cnt) {
           if ((rc = dalloc(p, &ph, cnt))) return rc;
           if ((rc = dalloc(p, &pe, cnt))) return rc;
+          if (p->is_complex) {
+            if ((rc = dalloc(p, &phi, cnt))) return rc;
+            if ((rc = dalloc(p, &pei, cnt))) return rc;
+          }
         }
         p->yp.psih.p[a][slot][side] = ph;
         p->yp.psie.p[a][slot][side] = pe;
+        p->yp.psih_i.p[a][slot][side] = phi;
+        p->yp.psie_i.p[a][slot][side] = pei;
       }
     }
   }
@@ -135,6 +148,7 @@ static int alloc_psi(oem_plan* p) {
 }
 
 static cudaError_t run_h(oem_plan* p, cudaStream_t s) {
+  if (p->is_complex) return launch_update_h_c(p->yp, s);
   if (p->basic_kernels == 1) return launch_update_h(p->yp, s);
   if (p->basic_kernels == 2) return launch_update_h_stream(p->yp, p->xch, s);
   if (p->basic_kernels == 3) return launch_update_h_ws(p->tma, p->yp, p->xch, p->d_err, s);
@@ -142,6 +156,7 @@ static cudaError_t run_h(oem_plan* p, cudaStream_t s) {
 }
 
 static cudaError_t run_e(oem_plan* p, cudaStream_t s) {
+  if (p->is_complex) return launch_update_e_c(p->yp, s);
   if (p->basic_kernels == 1) return launch_update_e(p->yp, s);
   if (p->basic_kernels == 2) return launch_update_e_stream(p->yp, p->xch, (int)p->mats.size(), s);
   if (p->basic_kernels == 3) {
@@ -243,6 +258,8 @@ static int enqueue_step(oem_plan* p, cudaStream_t s) {
   for (const PlaneSrc& src : p->planes)
     if ((e = launch_plane_h(P, src, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "plane_h");
+  for (const ModeSrc& m : p->modesrcs)
+    if ((e = launch_mode_h(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_h");
   if (fork) {
     OEM_CUDA(cudaStreamWaitEvent(s, p->ev_join, 0));
     e = launch_update_e_ws(p->tma, P, p->xch, (int)p->mats.size(), p->d_err, s);
@@ -253,6 +270,8 @@ static int enqueue_step(oem_plan* p, cudaStream_t s) {
   for (const PlaneSrc& src : p->planes)
     if ((e = launch_plane_e(P, src, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "plane_e");
+  for (const ModeSrc& m : p->modesrcs)
+    if ((e = launch_mode_e(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_e");
   for (const DipoleSet& d : p->dipoles)
     if (!d.magnetic && (e = launch_dipoles(P, d, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "dipoles_e");
@@ -553,9 +572,9 @@ int oem_plan_add_plane_source(oem_plan* p, int pol, int kh, int ks, double coef_
   return OEM_OK;
 }
 
-int oem_plan_add_dipoles(oem_plan* p, int magnetic, int n_pts, const int32_t* ijk,
-                         const int32_t* comp, const float* coef, const int32_t* src, int n_src,
-                         int64_t nsteps1, const double* amp) {
+static int add_dipoles_impl(oem_plan* p, int magnetic, int n_pts, const int32_t* ijk,
+                            const int32_t* comp, const float* coef, const int32_t* src, int n_src,
+                            int64_t nsteps1, const double* amp, const double* amp_im) {
   int rc = check_plan(p, false);
   if (rc) return rc;
   if (n_pts < 1 || n_src < 1 || nsteps1 < 1 || !ijk || !comp || !coef || !src || !amp)
@@ -602,7 +621,71 @@ int oem_plan_add_dipoles(oem_plan* p, int magnetic, int n_pts, const int32_t* ij
   if ((rc = dupload(p, &d.d_coef, pcoef.data(), pcoef.size()))) return rc;
   if ((rc = dupload(p, &d.d_src, psrc.data(), psrc.size()))) return rc;
   if ((rc = dupload(p, &d.d_amp, amp, (size_t)n_src * nsteps1))) return rc;
+  if (amp_im && (rc = dupload(p, &d.d_amp_im, amp_im, (size_t)n_src * nsteps1))) return rc;
   p->dipoles.push_back(d);
+  return OEM_OK;
+}
+
+int oem_plan_add_dipoles(oem_plan* p, int magnetic, int n_pts, const int32_t* ijk,
+                         const int32_t* comp, const float* coef, const int32_t* src, int n_src,
+                         int64_t nsteps1, const double* amp) {
+  if (p && p->is_complex)
+    return set_error(OEM_ERR_STATE, "a complex plan takes complex dipole amplitudes");
+  return add_dipoles_impl(p, magnetic, n_pts, ijk, comp, coef, src, n_src, nsteps1, amp,
+                          nullptr);
+}
+
+int oem_plan_add_dipoles_complex(oem_plan* p, int magnetic, int n_pts, const int32_t* ijk,
+                                 const int32_t* comp, const float* coef, const int32_t* src,
+                                 int n_src, int64_t nsteps1, const double* amp_re,
+                                 const double* amp_im) {
+  if (!p || !p->is_complex)
+    return set_error(OEM_ERR_STATE, "complex dipole amplitudes need a complex plan");
+  if (!amp_im) return set_error(OEM_ERR_INVALID, "null imaginary amplitude table");
+  return add_dipoles_impl(p, magnetic, n_pts, ijk, comp, coef, src, n_src, nsteps1, amp_re,
+                          amp_im);
+}
+
+int oem_plan_set_axis_phase(oem_plan* p, int axis, const double* mnx_im, const double* mpv_im) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (axis < 0 || axis > 2) return set_error(OEM_ERR_INVALID, "axis must be 0, 1 or 2");
+  if (!mnx_im || !mpv_im) return set_error(OEM_ERR_INVALID, "null mask table");
+  if (!p->axh[axis].set) return set_error(OEM_ERR_STATE, "set the axis tables first");
+  if (!p->dipoles.empty() || !p->mons.empty() || !p->tmons.empty() || !p->planes.empty())
+    return set_error(OEM_ERR_STATE, "mark the plan complex before adding sources and monitors");
+  const int n = axis == 0 ? p->nx : axis == 1 ? p->ny : p->nz;
+  p->axh[axis].mnx_i.assign(mnx_im, mnx_im + n);
+  p->axh[axis].mpv_i.assign(mpv_im, mpv_im + n);
+  p->is_complex = true;
+  return OEM_OK;
+}
+
+int oem_plan_add_mode_source(oem_plan* p, int axis, int kh, int ks, int n1, int n2,
+                             double coef_h1, double coef_h2, double coef_e1, double coef_e2,
+                             int n_terms, const float* profiles, int64_t ntab,
+                             const double* amp_e, const double* amp_h) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (axis < 0 || axis > 2) return set_error(OEM_ERR_INVALID, "mode axis must be 0, 1 or 2");
+  const int dims[3] = {p->nx, p->ny, p->nz};
+  const int t1 = (axis + 1) % 3, t2 = (axis + 2) % 3;
+  if (n1 != dims[t1] || n2 != dims[t2])
+    return set_error(OEM_ERR_INVALID, "mode profile must cover the whole plane (n_t1, n_t2)");
+  if (kh < 0 || kh >= dims[axis] || ks < 0 || ks >= dims[axis])
+    return set_error(OEM_ERR_INVALID, "mode injection plane outside the grid");
+  if (n_terms < 1 || ntab < 1 || !profiles || !amp_e || !amp_h)
+    return set_error(OEM_ERR_INVALID, "empty mode source");
+  if ((rc = use_device(p))) return rc;
+  ModeSrc m;
+  m.axis = axis; m.kh = kh; m.ks = ks; m.n1 = n1; m.n2 = n2; m.nterms = n_terms;
+  m.ch1 = (float)coef_h1; m.ch2 = (float)coef_h2; m.ce1 = (float)coef_e1; m.ce2 = (float)coef_e2;
+  m.ntab = ntab;
+  const size_t plane = (size_t)n1 * n2;
+  if ((rc = dupload(p, &m.d_prof, profiles, (size_t)n_terms * 8 * plane))) return rc;
+  if ((rc = dupload(p, &m.d_amp_e, amp_e, (size_t)n_terms * ntab * 2))) return rc;
+  if ((rc = dupload(p, &m.d_amp_h, amp_h, (size_t)n_terms * ntab * 2))) return rc;
+  p->modesrcs.push_back(m);
   return OEM_OK;
 }
 
@@ -616,7 +699,8 @@ static int add_monitor_common(oem_plan* p, Monitor& m, int nf, int64_t n_total, 
   m.T = batch;
   m.n_total = n_total;
   if ((rc = dupload(p, &m.d_phase, phase, (size_t)n_total * nf * 4))) return rc;
-  if ((rc = dalloc(p, &m.d_snap, (size_t)m.T * m.ncomp * m.cells))) return rc;
+  m.cplx = p->is_complex ? 1 : 0;
+  if ((rc = dalloc(p, &m.d_snap, (size_t)m.T * m.ncomp * (m.cplx ? 2 : 1) * m.cells))) return rc;
   if ((rc = dalloc(p, &m.d_re, (size_t)m.ncomp * nf * m.cells))) return rc;
   if ((rc = dalloc(p, &m.d_im, (size_t)m.ncomp * nf * m.cells))) return rc;
   int minus1 = -1;
@@ -682,6 +766,9 @@ int oem_plan_add_time_monitor(oem_plan* p, int nc, const int32_t* comps, int i0,
   m.i0 = i0; m.j0 = j0; m.k0 = k0; m.ni = ni; m.nj = nj; m.nk = nk;
   m.beg = beg; m.end = end; m.iv = iv; m.nslots = nslots;
   if ((rc = dalloc(p, &m.d_buf, (size_t)nc * std::max(nslots, 1) * ni * nj * nk))) return rc;
+  if (p->is_complex &&
+      (rc = dalloc(p, &m.d_buf_i, (size_t)nc * std::max(nslots, 1) * ni * nj * nk)))
+    return rc;
   *id = (int)p->tmons.size();
   p->tmons.push_back(m);
   return OEM_OK;
@@ -698,6 +785,10 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
     if (s.ntab < n_total) return set_error(OEM_ERR_INVALID, "plane-wave table shorter than the run");
   for (const DipoleSet& d : p->dipoles)
     if (d.nsteps1 < n_total) return set_error(OEM_ERR_INVALID, "dipole table shorter than the run");
+  for (const ModeSrc& m : p->modesrcs)
+    if (m.ntab < n_total) return set_error(OEM_ERR_INVALID, "mode amplitude table shorter than the run");
+  if (p->is_complex && (p->n_pole_total > 0 || !p->pset_ofs.empty()))
+    return set_error(OEM_ERR_UNSUPPORTED, "dispersive media on a complex (Bloch) plan");
   for (const Monitor& m : p->mons)
     if (m.n_total < n_total) return set_error(OEM_ERR_INVALID, "phase table shorter than the run");
   if ((rc = use_device(p))) return rc;
@@ -709,6 +800,12 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   const size_t ncp = (size_t)p->nx * p->ny * p->nzp;
   for (int c = 0; c < 6; ++c)
     if ((rc = dalloc(p, &P.f[c], ncp))) return rc;
+  if (p->is_complex) {
+    for (int c = 0; c < 6; ++c)
+      if ((rc = dalloc(p, &P.fi[c], ncp))) return rc;
+    P.cplx = 1;
+    p->basic_kernels = 1;  // the complex update kernels; no pipelined variant
+  }
   for (int a = 0; a < 3; ++a)
     if ((rc = upload_axis(p, a))) return rc;
   if ((rc = alloc_psi(p))) return rc;
@@ -861,6 +958,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
           return cuda_error(e, "dipoles_h");
       for (const PlaneSrc& src : p->planes)
         if ((e = launch_plane_h(p->yp, src, p->d_step, s)) != cudaSuccess) return cuda_error(e, "plane_h");
+      for (const ModeSrc& m : p->modesrcs)
+        if ((e = launch_mode_h(p->yp, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_h");
       OEM_CUDA(cudaEventRecord(E[2], s));
       const bool split = p->basic_kernels == 3 && p->yp.has_ade;
       if (split) {
@@ -877,6 +976,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       OEM_CUDA(cudaEventRecord(E[3], s));
       for (const PlaneSrc& src : p->planes)
         if ((e = launch_plane_e(p->yp, src, p->d_step, s)) != cudaSuccess) return cuda_error(e, "plane_e");
+      for (const ModeSrc& m : p->modesrcs)
+        if ((e = launch_mode_e(p->yp, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_e");
       for (const DipoleSet& d : p->dipoles)
         if (!d.magnetic && (e = launch_dipoles(p->yp, d, p->d_step, s)) != cudaSuccess)
           return cuda_error(e, "dipoles_e");
@@ -948,6 +1049,7 @@ int oem_plan_launches_per_step(oem_plan* p, int* n) {
   int c = 2 + 1;  // update_h, update_e, step counter
   if (p->basic_kernels == 3 && p->yp.has_ade) c += 1;  // separate pole pass
   c += 2 * (int)p->planes.size();
+  c += 2 * (int)p->modesrcs.size();
   for (const DipoleSet& d : p->dipoles) c += d.n_targets > 0 ? 1 : 0;
   c += 2 * (int)p->tmons.size();
   c += 3 * (int)p->mons.size();  // snapshot, flush, flush mark
@@ -1007,6 +1109,41 @@ int oem_plan_read_field(oem_plan* p, int comp, float* out, void* stream) {
                              (size_t)p->nx * p->ny, cudaMemcpyDeviceToHost, s));
   OEM_CUDA(cudaStreamSynchronize(s));
   return check_device_error(p);
+}
+
+int oem_plan_read_field_complex(oem_plan* p, int comp, float* re, float* im, void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (!p->is_complex) return set_error(OEM_ERR_STATE, "not a complex plan");
+  if (comp < 0 || comp > 5 || !re || !im) return set_error(OEM_ERR_INVALID, "component must be 0..5");
+  if ((rc = use_device(p))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const float* src[2] = {p->yp.f[comp], p->yp.fi[comp]};
+  float* dst[2] = {re, im};
+  for (int q = 0; q < 2; ++q)
+    OEM_CUDA(cudaMemcpy2DAsync(dst[q], (size_t)p->nz * sizeof(float), src[q],
+                               (size_t)p->nzp * sizeof(float), (size_t)p->nz * sizeof(float),
+                               (size_t)p->nx * p->ny, cudaMemcpyDeviceToHost, s));
+  OEM_CUDA(cudaStreamSynchronize(s));
+  return check_device_error(p);
+}
+
+int oem_plan_read_time_monitor_complex(oem_plan* p, int id, float* re, float* im, void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (!p->is_complex) return set_error(OEM_ERR_STATE, "not a complex plan");
+  if (id < 0 || id >= (int)p->tmons.size()) return set_error(OEM_ERR_INVALID, "time monitor id out of range");
+  if (!re || !im) return set_error(OEM_ERR_INVALID, "null output");
+  if ((rc = use_device(p))) return rc;
+  const TimeMon& m = p->tmons[id];
+  const size_t n = (size_t)m.nc * m.nslots * m.ni * m.nj * m.nk;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (n) {
+    OEM_CUDA(cudaMemcpyAsync(re, m.d_buf, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    OEM_CUDA(cudaMemcpyAsync(im, m.d_buf_i, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+  }
+  OEM_CUDA(cudaStreamSynchronize(s));
+  return OEM_OK;
 }
 
 int oem_plan_write_field(oem_plan* p, int comp, const float* in, void* stream) {

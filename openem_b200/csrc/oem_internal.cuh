@@ -55,6 +55,8 @@ struct DevAxis {
   const float* ah;     // CPML at H positions
   const float* bh;
   const float* kh;
+  const float* mnx_i;  // imaginary parts of the masks (complex plans: the Bloch phase at the
+  const float* mpv_i;  // periodic seam), nullptr on the real path
   int n;
   int lo;  // psi slab cells at the low end  [0, lo)
   int hi;  // psi slab cells at the high end [n - hi, n)
@@ -69,9 +71,13 @@ struct PsiSet {
 // Everything the Yee kernels need.
 struct YeeParams {
   float* f[6];  // Ex Ey Ez Hx Hy Hz, padded (nx, ny, nzp)
+  float* fi[6];  // imaginary parts on a complex (Bloch) plan, nullptr otherwise
   DevAxis ax[3];
   PsiSet psih;
   PsiSet psie;
+  PsiSet psih_i;  // imaginary psi on a complex plan
+  PsiSet psie_i;
+  int cplx;
   int nx, ny, nz, nzp;
   float ch;  // dt / mu0
   float cw;  // eps0 / dt
@@ -119,6 +125,19 @@ struct DipoleSet {
   float* d_coef = nullptr;
   int* d_src = nullptr;
   double* d_amp = nullptr;      // (n_src, nsteps1)
+  double* d_amp_im = nullptr;   // imaginary part on a complex plan
+};
+
+// One mode-source injection entry (one-plane TF/SF with 2D complex profiles): the tangential
+// pair t1 = axis+1, t2 = axis+2 (cyclic); profiles per term [8][n1][n2] = E_t1, E_t2, H_t1,
+// H_t2 as (re, im) planes; amplitudes per term (ntab, 2).
+struct ModeSrc {
+  int axis = 0, kh = 0, ks = 0, n1 = 0, n2 = 0, nterms = 0;
+  float ch1 = 0.f, ch2 = 0.f, ce1 = 0.f, ce2 = 0.f;
+  int64_t ntab = 0;
+  float* d_prof = nullptr;
+  double* d_amp_e = nullptr;  // amp at n dt, paired with the E profiles on the H side
+  double* d_amp_h = nullptr;  // amp at (n + 1/2) dt, paired with the H profiles on the E side
 };
 
 struct Monitor {
@@ -134,6 +153,7 @@ struct Monitor {
   double* d_re = nullptr;    // (ncomp, nf, cells)
   double* d_im = nullptr;
   int* d_done = nullptr;     // last step already folded into the accumulators
+  int cplx = 0;              // complex fields: the ring holds ncomp real then ncomp imaginary rows
 };
 
 struct TimeMon {
@@ -142,10 +162,12 @@ struct TimeMon {
   int i0 = 0, j0 = 0, k0 = 0, ni = 0, nj = 0, nk = 0;
   int beg = 0, end = 0, iv = 1, nslots = 0;
   float* d_buf = nullptr;  // (nc, nslots, ni, nj, nk)
+  float* d_buf_i = nullptr;  // imaginary samples on a complex plan
 };
 
 struct AxisHost {
   std::vector<double> idl_p, idl_d, mnx, mpv, pml_e, pml_h;
+  std::vector<double> mnx_i, mpv_i;  // complex plans: imaginary parts of the masks
   std::vector<int> nxt, prv;
   int lo = 0, hi = 0;
   bool set = false;
@@ -180,6 +202,8 @@ struct oem_plan {
 
   std::vector<oem::PlaneSrc> planes;
   std::vector<oem::DipoleSet> dipoles;
+  std::vector<oem::ModeSrc> modesrcs;
+  bool is_complex = false;  // Bloch / forced complex fields
   std::vector<oem::Monitor> mons;
   std::vector<oem::TimeMon> tmons;
 
@@ -284,6 +308,10 @@ cudaError_t launch_list_pole_segments(const YeeParams& P, int64_t nseg, int64_t*
                                       unsigned long long* count, cudaStream_t s);
 cudaError_t launch_ade_segments(const YeeParams& P, const int64_t* segs, int64_t nsegs,
                                 int64_t nseg, int max_blocks, cudaStream_t s);
+cudaError_t launch_update_h_c(const YeeParams& P, cudaStream_t s);
+cudaError_t launch_update_e_c(const YeeParams& P, cudaStream_t s);
+cudaError_t launch_mode_h(const YeeParams& P, const ModeSrc& m, const int* step, cudaStream_t s);
+cudaError_t launch_mode_e(const YeeParams& P, const ModeSrc& m, const int* step, cudaStream_t s);
 cudaError_t launch_energy(const YeeParams& P, double* const dl[3][2], double* part, int nblocks,
                           cudaStream_t s);
 int energy_block_count(const YeeParams& P);

@@ -220,6 +220,15 @@ __global__ void k_dipoles(YeeParams P, DipoleSet d, const int* step) {
     v += -cc * d.d_coef[q] * a;
   }
   F[id] = v;
+  if (d.d_amp_im) {  // complex plan: the imaginary part of the amplitude drives the im field
+    float* Fi = P.fi[d.magnetic ? 3 + c : c];
+    float w = Fi[id];
+    for (int q = d.d_ofs[t]; q < d.d_ofs[t + 1]; ++q) {
+      const float a = (float)d.d_amp_im[(int64_t)d.d_src[q] * d.nsteps1 + n];
+      w += -cc * d.d_coef[q] * a;
+    }
+    Fi[id] = w;
+  }
 }
 
 // Field time monitor, one shot of the two-shot H average (openem/kernels/source_dft.cu:282-319).
@@ -243,6 +252,10 @@ __global__ void k_time_sample(YeeParams P, TimeMon m, const int* step, int add) 
     const int64_t o = ((int64_t)q * m.nslots + slot) * cells + off;
     const float v = w * P.f[comp][id];
     m.d_buf[o] = add ? m.d_buf[o] + v : v;
+    if (m.d_buf_i) {
+      const float vi = w * P.fi[comp][id];
+      m.d_buf_i[o] = add ? m.d_buf_i[o] + vi : vi;
+    }
   }
 }
 
@@ -261,11 +274,17 @@ __global__ void k_snap_plane(YeeParams P, Monitor m, const int* step) {
   c[m.axis] = m.km - 1;
   const int64_t idm = ((int64_t)c[0] * P.ny + c[1]) * P.nzp + c[2];
   const int64_t off = (int64_t)p1 * m.n2 + p2;
-  float* row = m.d_snap + (int64_t)((*step) % m.T) * 4 * m.cells;
+  float* row = m.d_snap + (int64_t)((*step) % m.T) * (m.cplx ? 8 : 4) * m.cells;
   row[off] = P.f[t1][id];
   row[m.cells + off] = P.f[t2][id];
   row[2 * m.cells + off] = 0.5f * (P.f[3 + t1][id] + P.f[3 + t1][idm]);
   row[3 * m.cells + off] = 0.5f * (P.f[3 + t2][id] + P.f[3 + t2][idm]);
+  if (m.cplx) {
+    row[4 * m.cells + off] = P.fi[t1][id];
+    row[5 * m.cells + off] = P.fi[t2][id];
+    row[6 * m.cells + off] = 0.5f * (P.fi[3 + t1][id] + P.fi[3 + t1][idm]);
+    row[7 * m.cells + off] = 0.5f * (P.fi[3 + t2][id] + P.fi[3 + t2][idm]);
+  }
 }
 
 // DFT snapshot of a box: the six components at their Yee positions
@@ -277,12 +296,16 @@ __global__ void k_snap_box(YeeParams P, Monitor m, const int* step) {
   if (t >= njk) return;
   const uint32_t b = t / (uint32_t)m.nk;
   const uint32_t cc = t - b * (uint32_t)m.nk;
-  float* row = m.d_snap + (int64_t)((*step) % m.T) * 6 * m.cells;
+  float* row = m.d_snap + (int64_t)((*step) % m.T) * (m.cplx ? 12 : 6) * m.cells;
   for (int a = blockIdx.y; a < m.ni; a += gridDim.y) {
     const int64_t id = ((int64_t)(m.i0 + a) * P.ny + (m.j0 + (int)b)) * P.nzp + (m.k0 + (int)cc);
     const int64_t o = (int64_t)a * njk + t;
 #pragma unroll
     for (int q = 0; q < 6; ++q) row[q * m.cells + o] = P.f[q][id];
+    if (m.cplx) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) row[(6 + q) * m.cells + o] = P.fi[q][id];
+    }
   }
 }
 
@@ -340,6 +363,61 @@ __global__ void __launch_bounds__(128) k_flush(Monitor m, const int* step, int f
   }
 }
 
+// Complex-field variant (openem/kernels/bloch.cu:389-481): the ring holds NC real rows then
+// NC imaginary rows; phasor += (u_re + i u_im)(cos + i sin) with the apodised phase.
+template <int NC>
+__global__ void __launch_bounds__(128) k_flush_c(Monitor m, const int* step, int forced) {
+  const int s_now = forced ? (*step - 1) : *step;
+  if (!forced && ((s_now + 1) % m.T) != 0) return;
+  const int s_lo = *m.d_done + 1;
+  if (s_lo > s_now) return;
+  constexpr int NE = NC / 2;
+  for (int64_t pt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pt < m.cells;
+       pt += (int64_t)gridDim.x * blockDim.x) {
+    for (int f0 = 0; f0 < m.nf; f0 += 4) {
+      const int nfc = min(4, m.nf - f0);
+      float aR[4][NC], aI[4][NC];
+#pragma unroll
+      for (int ff = 0; ff < 4; ++ff)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) { aR[ff][c] = 0.f; aI[ff][c] = 0.f; }
+      for (int s = s_lo; s <= s_now; ++s) {
+        const float* row = m.d_snap + (int64_t)(s % m.T) * 2 * NC * m.cells;
+        float vr[NC], vi[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          vr[c] = row[c * m.cells + pt];
+          vi[c] = row[(NC + c) * m.cells + pt];
+        }
+        const float4* ph = reinterpret_cast<const float4*>(m.d_phase) + ((int64_t)s * m.nf + f0);
+#pragma unroll
+        for (int ff = 0; ff < 4; ++ff) {
+          if (ff < nfc) {
+            const float4 q = __ldg(ph + ff);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              const float co = c < NE ? q.x : q.z, si = c < NE ? q.y : q.w;
+              aR[ff][c] = fmaf(-vi[c], si, fmaf(vr[c], co, aR[ff][c]));
+              aI[ff][c] = fmaf(vi[c], co, fmaf(vr[c], si, aI[ff][c]));
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int ff = 0; ff < 4; ++ff) {
+        if (ff < nfc) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            const int64_t o = ((int64_t)c * m.nf + f0 + ff) * m.cells + pt;
+            m.d_re[o] += (double)aR[ff][c];
+            m.d_im[o] += (double)aI[ff][c];
+          }
+        }
+      }
+    }
+  }
+}
+
 __global__ void k_flush_mark(int T, const int* step, int* done, int forced) {
   const int s_now = forced ? (*step - 1) : *step;
   if (forced || ((s_now + 1) % T) == 0) {
@@ -376,10 +454,18 @@ __global__ void __launch_bounds__(256) k_energy(YeeParams P, const double* dxp, 
     const double vhz = dxp[i] * dyp[j] * dzd[k];
     const double ex = P.f[0][id], ey = P.f[1][id], ez = P.f[2][id];
     const double hx = P.f[3][id], hy = P.f[4][id], hz = P.f[5][id];
-    const double e0 = vex * ex * ex, e1 = vey * ey * ey, e2 = vez * ez * ez;
+    double ax2 = ex * ex, ay2 = ey * ey, az2 = ez * ez;
+    double bx2 = hx * hx, by2 = hy * hy, bz2 = hz * hz;
+    if (P.cplx) {  // |u|^2 of complex fields
+      const double exi = P.fi[0][id], eyi = P.fi[1][id], ezi = P.fi[2][id];
+      const double hxi = P.fi[3][id], hyi = P.fi[4][id], hzi = P.fi[5][id];
+      ax2 += exi * exi; ay2 += eyi * eyi; az2 += ezi * ezi;
+      bx2 += hxi * hxi; by2 += hyi * hyi; bz2 += hzi * hzi;
+    }
+    const double e0 = vex * ax2, e1 = vey * ay2, e2 = vez * az2;
     s0 += e0 + e1 + e2;
     s1 += e0 * M.eps[0] + e1 * M.eps[1] + e2 * M.eps[2];
-    s2 += vhx * hx * hx + vhy * hy * hy + vhz * hz * hz;
+    s2 += vhx * bx2 + vhy * by2 + vhz * bz2;
   }
   sh[0][threadIdx.x] = s0;
   sh[1][threadIdx.x] = s1;
@@ -501,10 +587,16 @@ cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* ste
 
 cudaError_t launch_flush(const Monitor& m, const int* step, int forced, cudaStream_t s) {
   const int64_t nb = std::min<int64_t>((m.cells + 127) / 128, 148 * 8);
-  if (m.ncomp == 4)
+  if (m.cplx) {
+    if (m.ncomp == 4)
+      k_flush_c<4><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
+    else
+      k_flush_c<6><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
+  } else if (m.ncomp == 4) {
     k_flush<4><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
-  else
+  } else {
     k_flush<6><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_flush_mark<<<1, 1, 0, s>>>(m.T, step, m.d_done, forced);

@@ -34,6 +34,10 @@ SIGNATURES = {
     "oem_plan_set_pole_sets_device": (_I, [_P, _I, _P, _P, _P, _L, _L]),
     "oem_plan_add_plane_source": (_I, [_P, _I, _I, _I, _D, _D, _L, _P, _P]),
     "oem_plan_add_dipoles": (_I, [_P, _I, _I, _P, _P, _P, _P, _I, _L, _P]),
+    "oem_plan_add_dipoles_complex": (_I, [_P, _I, _I, _P, _P, _P, _P, _I, _L, _P, _P]),
+    "oem_plan_add_mode_source": (_I, [_P, _I, _I, _I, _I, _I, _D, _D, _D, _D, _I, _P, _L,
+                                      _P, _P]),
+    "oem_plan_set_axis_phase": (_I, [_P, _I, _P, _P]),
     "oem_plan_add_flux_monitor": (_I, [_P, _I, _I, _I, _L, _P, _I, C.POINTER(_I)]),
     "oem_plan_add_box_monitor": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _L, _P, _I,
                                       C.POINTER(_I)]),
@@ -48,6 +52,8 @@ SIGNATURES = {
     "oem_plan_read_monitor": (_I, [_P, _I, _P, _P, _P]),
     "oem_plan_read_time_monitor": (_I, [_P, _I, _P, _P]),
     "oem_plan_read_field": (_I, [_P, _I, _P, _P]),
+    "oem_plan_read_field_complex": (_I, [_P, _I, _P, _P, _P]),
+    "oem_plan_read_time_monitor_complex": (_I, [_P, _I, _P, _P, _P]),
     "oem_plan_write_field": (_I, [_P, _I, _P, _P]),
     "oem_plan_energy": (_I, [_P, _P, _P]),
     "oem_plan_field_ptrs": (_I, [_P, _P, C.POINTER(_I)]),

@@ -20,7 +20,7 @@ import numpy as np
 
 from openem_b200.model import (
     C_0, EPSILON_0, ETA_0, Axis, Dispersion, FieldMonitor, FieldTimeMonitor, FluxMonitor,
-    GaussianPulse, Grid, PlaneWaveSource, PMLParams, PointDipole, Scene, pml_build,
+    GaussianPulse, Grid, ModeSource, PlaneWaveSource, PMLParams, PointDipole, Scene, pml_build,
     sample_waveform)
 
 UM = 1e-6
@@ -362,3 +362,205 @@ def with_time_monitor(sc: Scene, name: str = "tmon", comps=(0, 1, 2, 3, 4, 5), o
                           step_begin=step_begin, step_end=end, interval=interval,
                           num_slots=slots)
     return replace(sc, field_time_monitors=list(sc.field_time_monitors) + [tm])
+
+
+# ---------------------------------------------------------------------------------------------
+# Mode-source carriers: oblique plane waves (Bloch cells) and Gaussian beams
+# ---------------------------------------------------------------------------------------------
+
+def _z_plane_coords(grid: Grid):
+    """Transverse Yee coordinates of the z-normal tangential components: Ex (x ctr, y edge),
+    Ey (x edge, y ctr), Hx (x edge, y ctr), Hy (x ctr, y edge)."""
+    ax, ay = grid.axes[0], grid.axes[1]
+    xe, ye = np.asarray(ax.edges[:-1], np.float64), np.asarray(ay.edges[:-1], np.float64)
+    xc, yc = np.asarray(ax.centers, np.float64), np.asarray(ay.centers, np.float64)
+    return {"Ex": (xc, ye), "Ey": (xe, yc), "Hx": (xe, yc), "Hy": (xc, ye)}
+
+
+def _mode_amplitudes(source_time, dt: float, num_steps: int, delay_h: float):
+    """amp_e = a(n dt), amp_h = a((n + 1/2) dt + delay_h) for n = 0..num_steps; the H delay is
+    the travel time from the upstream H plane to the source plane."""
+    n = np.arange(num_steps + 1, dtype=np.float64)
+    amp_e = np.asarray(source_time.amp_time(n * dt), np.complex128)
+    amp_h = np.asarray(source_time.amp_time((n + 0.5) * dt + delay_h), np.complex128)
+    return amp_e, amp_h
+
+
+def oblique_plane_wave(grid: Grid, dt: float, num_steps: int, plane_index: int, bloch_k,
+                       source_time, pol: str = "s", direction: int = 1,
+                       eps_r: float = 1.0) -> ModeSource:
+    """z-normal mode source carrying a plane wave whose transverse wavevector is the Bloch
+    vector of the cell, ``k_t = 2 pi (k_x / L_x, k_y / L_y)``: ``E = e exp(i k_t . r_t)``,
+    ``H = n (k_hat x e) / eta0`` sampled at each component's Yee position, with
+    ``k_z = sqrt(k^2 - |k_t|^2)`` at ``freq0`` (the angle of incidence at the carrier). ``pol``
+    ``"s"``: E perpendicular to the plane of incidence (y at normal incidence); ``"p"``: in it.
+    The H profile sits on the upstream H plane; its amplitude table is delayed by the half-cell
+    travel time along z at the carrier angle (exact at normal incidence)."""
+    ax, ay, az = grid.axes
+    lx = float(ax.edges[-1] - ax.edges[0])
+    ly = float(ay.edges[-1] - ay.edges[0])
+    n_r = float(np.sqrt(eps_r))
+    k0 = 2.0 * np.pi * source_time.freq0 * n_r / C_0
+    kx = 2.0 * np.pi * float(bloch_k[0]) / lx
+    ky = 2.0 * np.pi * float(bloch_k[1]) / ly
+    kz2 = k0 * k0 - kx * kx - ky * ky
+    if kz2 <= 0.0:
+        raise ValueError("the Bloch vector is evanescent at the carrier frequency")
+    kz = float(np.sqrt(kz2)) * (1 if direction > 0 else -1)
+    khat = np.array([kx, ky, kz]) / k0
+    zhat = np.array([0.0, 0.0, 1.0])
+    s_vec = np.cross(zhat, khat)
+    s_vec = np.array([0.0, 1.0, 0.0]) if np.linalg.norm(s_vec) < 1e-12 else s_vec / np.linalg.norm(s_vec)
+    e = s_vec if pol == "s" else np.cross(khat, s_vec) * -1.0
+    h = n_r * np.cross(khat, e) / ETA_0
+    c = _z_plane_coords(grid)
+
+    def prof(amp, name):
+        x, y = c[name]
+        return amp * np.exp(1j * (kx * x[:, None] + ky * y[None, :]))
+
+    ks = int(plane_index)
+    dl_half = 0.5 * float(az.dl[ks - 1] if direction > 0 else az.dl[ks])
+    delay = dl_half * abs(khat[2]) * n_r / C_0
+    amp_e, amp_h = _mode_amplitudes(source_time, dt, num_steps, delay)
+    return ModeSource(plane_index=ks, direction=int(direction),
+                      ey_inc=prof(e[0], "Ex"), ez_inc=prof(e[1], "Ey"),
+                      hy_inc=prof(h[0], "Hx"), hz_inc=prof(h[1], "Hy"),
+                      amp_e=amp_e, amp_h=amp_h, n_eff=complex(n_r), axis=2)
+
+
+def gaussian_beam(grid: Grid, dt: float, num_steps: int, plane_index: int, waist: float,
+                  source_time, pol_axis: int = 1, center=(0.0, 0.0), direction: int = 1,
+                  eps_r: float = 1.0) -> ModeSource:
+    """z-normal mode source of a Gaussian beam at its waist plane: E = e exp(-r^2 / w0^2)
+    polarised along ``pol_axis`` (0 or 1), H = n (z_hat x E) / eta0 (paraxial), amplitude
+    tables as :func:`oblique_plane_wave` at normal incidence."""
+    az = grid.axes[2]
+    n_r = float(np.sqrt(eps_r))
+    c = _z_plane_coords(grid)
+    e = np.zeros(3)
+    e[pol_axis] = 1.0
+    khat = np.array([0.0, 0.0, 1.0 if direction > 0 else -1.0])
+    h = n_r * np.cross(khat, e) / ETA_0
+
+    def prof(amp, name):
+        x, y = c[name]
+        r2 = (x[:, None] - center[0]) ** 2 + (y[None, :] - center[1]) ** 2
+        return (amp * np.exp(-r2 / (waist * waist))).astype(np.complex128)
+
+    ks = int(plane_index)
+    dl_half = 0.5 * float(az.dl[ks - 1] if direction > 0 else az.dl[ks])
+    amp_e, amp_h = _mode_amplitudes(source_time, dt, num_steps, dl_half * n_r / C_0)
+    return ModeSource(plane_index=ks, direction=int(direction),
+                      ey_inc=prof(e[0], "Ex"), ez_inc=prof(e[1], "Ey"),
+                      hy_inc=prof(h[0], "Hx"), hz_inc=prof(h[1], "Hy"),
+                      amp_e=amp_e, amp_h=amp_h, n_eff=complex(n_r), axis=2)
+
+
+def _pixel_eps(grid: Grid, shape, npix: int, layer, lo_hi, rng):
+    """Diagonal permittivity of a pixelated layer: per pixel (npix x npix in the x-y plane)
+    eps_xx, eps_yy, eps_zz ~ U[lo, hi], staircased per component at its Yee position; layer =
+    (z0, z1) in metres."""
+    pix = rng.uniform(lo_hi[0], lo_hi[1], size=(3, npix, npix))
+    ax, ay = grid.axes[0], grid.axes[1]
+    x0, x1 = float(ax.edges[0]), float(ax.edges[-1])
+    y0, y1 = float(ay.edges[0]), float(ay.edges[-1])
+    coords = yee_coords(grid)
+    eps = []
+    for comp in range(3):
+        x, y, z = coords[comp]
+        px = np.clip(((x - x0) / (x1 - x0) * npix).astype(int), 0, npix - 1)
+        py = np.clip(((y - y0) / (y1 - y0) * npix).astype(int), 0, npix - 1)
+        inz = (z >= layer[0]) & (z < layer[1])
+        e = np.ones(shape)
+        vals = pix[comp][px[:, None], py[None, :]]
+        e[:, :, inz] = vals[:, :, None]
+        eps.append(e)
+    return eps
+
+
+def bloch_metasurface(nx: int = 256, ny: int = 256, nz: int = 1024, dl: float = 0.01 * UM,
+                      n_pml: int = 12, bloch_k=(0.15, 0.0, 0.0), freq0: float = 3e14,
+                      fwidth_rel: float = 0.3, npix: int = 64, layer_cells: int = 40,
+                      nfreq: int = 200, num_steps: int = 20000, seed: int = 1,
+                      field_monitor: bool = False) -> Scene:
+    """Bloch unit cell with a pixelated diagonal-anisotropic layer: ``nx x ny x nz`` cells in
+    total (CPML on +-z included), Bloch vector ``bloch_k`` (in units of 2 pi / L) on x and y,
+    a ``layer_cells``-thick layer at mid-z whose ``npix x npix`` pixels draw eps_xx, eps_yy,
+    eps_zz from U[2, 12] (``seed``), an s-polarised oblique plane wave (transverse wavevector =
+    Bloch vector) injected upward from below the layer, and a flux monitor above it with
+    ``nfreq`` frequencies over freq0 +- fwidth."""
+    n_in = nz - 2 * n_pml
+    axes = [Axis(np.arange(nx + 1) * dl, "BlochBoundary", "BlochBoundary"),
+            Axis(np.arange(ny + 1) * dl, "Periodic", "Periodic"),
+            uniform_axis(n_in, dl, -0.5 * n_in * dl, "PML", n_pml)]
+    grid = Grid(*axes)
+    dt = courant_dt([a.dl for a in axes])
+    shape = grid.shape
+    zc = 0.0
+    layer = (zc - 0.5 * layer_cells * dl, zc + 0.5 * layer_cells * dl)
+    eps = _pixel_eps(grid, shape, npix, layer, (2.0, 12.0), np.random.default_rng(seed))
+    pulse = GaussianPulse(freq0=freq0, fwidth=fwidth_rel * freq0)
+    edges_z = np.asarray(axes[2].edges)
+    z_src = layer[0] - 0.25 * n_in * dl
+    ks = int(np.argmin(np.abs(edges_z - z_src)))
+    src = oblique_plane_wave(grid, dt, num_steps, ks, bloch_k, pulse, pol="s")
+    freqs = np.linspace(freq0 * (1 - fwidth_rel), freq0 * (1 + fwidth_rel), nfreq)
+    km = int(np.argmin(np.abs(edges_z - (layer[1] + 0.2 * n_in * dl))))
+    mons = [FluxMonitor(name="T", axis=2, plane_index=km, normal_dir=1, freqs=freqs,
+                        source_spectrum=spectrum(pulse, dt, num_steps, freqs))]
+    fmons = []
+    if field_monitor:
+        fmons.append(FieldMonitor(name="layer_mid", freqs=freqs[:: max(1, nfreq // 4)],
+                                  origin=(0, 0, nz // 2), box=(nx, ny, 1)))
+    return Scene(grid=grid, dt=dt, num_time_steps=num_steps, shutoff=1e-5,
+                 eps_ex=eps[0], eps_ey=eps[1], eps_ez=eps[2], pml=pml_dict(grid, dt, n_pml),
+                 bloch_k=tuple(float(v) for v in bloch_k), mode_sources=[src],
+                 flux_monitors=mons, field_monitors=fmons)
+
+
+def beam_slab(nx: int = 200, ny: int = 200, nz: int = 120, dl: float = 0.025 * UM,
+              n_pml: int = 12, eps_slab: float = 12.1, eps_bg: float = 2.1,
+              slab_cells: int = 9, design=(80, 80), seed: int = 2, waist: float = 1.0 * UM,
+              freq0: float = 1.94e14, fwidth_rel: float = 0.15, nfreq: int = 5,
+              num_steps: int = 2000) -> Scene:
+    """A slab (``slab_cells`` thick, eps_slab) in a background eps_bg with a ``design`` pixel
+    region of the slab drawn from U[eps_bg, eps_slab] (``seed``), CPML on all faces, a
+    y-polarised Gaussian beam (``waist``) injected upward below the slab and a flux monitor
+    above it at ``nfreq`` frequencies over freq0 +- fwidth."""
+    dims = (nx, ny, nz)
+    axes = [uniform_axis(d - 2 * n_pml, dl, -0.5 * (d - 2 * n_pml) * dl, "PML", n_pml)
+            for d in dims]
+    grid = Grid(*axes)
+    dt = courant_dt([a.dl for a in axes])
+    shape = grid.shape
+    rng = np.random.default_rng(seed)
+    coords = yee_coords(grid)
+    zlo, zhi = -0.5 * slab_cells * dl, 0.5 * slab_cells * dl
+    dx, dy = design[0] * dl, design[1] * dl
+    pix = rng.uniform(eps_bg, eps_slab, size=design)
+    eps = []
+    for comp in range(3):
+        x, y, z = coords[comp]
+        e = np.full(shape, eps_bg)
+        inz = (z >= zlo) & (z < zhi)
+        e[:, :, inz] = eps_slab
+        ix = np.flatnonzero(np.abs(x) < 0.5 * dx)
+        iy = np.flatnonzero(np.abs(y) < 0.5 * dy)
+        px = np.clip(((x[ix] + 0.5 * dx) / dx * design[0]).astype(int), 0, design[0] - 1)
+        py = np.clip(((y[iy] + 0.5 * dy) / dy * design[1]).astype(int), 0, design[1] - 1)
+        sub = e[ix[0]:ix[-1] + 1, iy[0]:iy[-1] + 1, :]
+        sub[:, :, inz] = pix[px[:, None], py[None, :]][:, :, None]
+        eps.append(e)
+    pulse = GaussianPulse(freq0=freq0, fwidth=fwidth_rel * freq0)
+    edges_z = np.asarray(axes[2].edges)
+    n_in = nz - 2 * n_pml
+    ks = int(np.argmin(np.abs(edges_z - (zlo - 0.3 * n_in * dl))))
+    src = gaussian_beam(grid, dt, num_steps, ks, waist, pulse, pol_axis=1, eps_r=eps_bg)
+    freqs = np.linspace(freq0 * (1 - fwidth_rel), freq0 * (1 + fwidth_rel), nfreq)
+    km = int(np.argmin(np.abs(edges_z - (zhi + 0.3 * n_in * dl))))
+    mons = [FluxMonitor(name="T", axis=2, plane_index=km, normal_dir=1, freqs=freqs,
+                        source_spectrum=spectrum(pulse, dt, num_steps, freqs))]
+    return Scene(grid=grid, dt=dt, num_time_steps=num_steps, shutoff=1e-5,
+                 eps_ex=eps[0], eps_ey=eps[1], eps_ez=eps[2], pml=pml_dict(grid, dt, n_pml),
+                 mode_sources=[src], flux_monitors=mons)

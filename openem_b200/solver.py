@@ -31,7 +31,6 @@ def refuse_unsupported(sc) -> None:
     """Fail closed on scene features outside this engine's real-field path."""
     checks = [
         (bool(getattr(sc, "tfsf_sources", None)), "TFSF box sources"),
-        (bool(getattr(sc, "mode_sources", None)), "mode / Gaussian-beam sources"),
         (bool(getattr(sc, "absorbers", None)), "Absorber boundaries"),
         (bool(getattr(sc, "flux_time_monitors", None)), "flux time monitors"),
         (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry > 0,
@@ -45,12 +44,51 @@ def refuse_unsupported(sc) -> None:
             raise NotImplementedError(f"{what} are not supported by the sm_100a engine yet")
 
 
+def refuse_unsupported_bloch(sc) -> None:
+    """Fail closed outside the complex-field subset (openem/solver.py:1221-1260): point dipoles,
+    mode sources (oblique plane waves, beams), DFT and time monitors, CPML and periodic / Bloch
+    axes; lossless, non-dispersive media without PEC."""
+    bad = []
+    if sc.sources:
+        bad.append("plane wave sources")
+    if getattr(sc, "tfsf_sources", None):
+        bad.append("TFSF sources")
+    if (sc.dispersion is not None and sc.dispersion.n_entry > 0) or \
+            (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry > 0):
+        bad.append("dispersive media")
+    if sc.modulation is not None and sc.modulation.n_entry > 0:
+        bad.append("time-varying media")
+    if sc.tensor is not None and sc.tensor.n_entry > 0:
+        bad.append("tensor media")
+    if sc.sigma_ex is not None:
+        bad.append("conductivity")
+    if sc.pec_ex is not None:
+        bad.append("PEC cells")
+    if getattr(sc, "flux_time_monitors", None):
+        bad.append("FluxTimeMonitor")
+    if getattr(sc, "absorbers", None):
+        bad.append("Absorber boundaries")
+    if bad:
+        raise NotImplementedError(
+            "the Bloch complex-field path does not support: " + ", ".join(bad)
+            + ". The supported subset is point dipoles (electric/magnetic), mode sources, DFT "
+            "and time monitors, CPML / periodic / Bloch boundaries")
+    if not sc.dipoles and not getattr(sc, "mode_sources", None):
+        raise NotImplementedError(
+            "the Bloch complex-field path needs a point dipole source or an (oblique) mode "
+            "source, and this scene has neither")
+
+
 class Plan:
     """One simulation resident on the device: owns a ``oem_plan``."""
 
     def __init__(self, sc, n_total: int | None = None, device: int = 0, stream=None,
-                 batch: int | None = None):
-        refuse_unsupported(sc)
+                 batch: int | None = None, cplx: bool = False):
+        self.cplx = bool(cplx)
+        if self.cplx:
+            refuse_unsupported_bloch(sc)
+        else:
+            refuse_unsupported(sc)
         self.lib = L.load()
         self.sc = sc
         self.n_total = int(sc.num_time_steps if n_total is None else n_total)
@@ -89,7 +127,10 @@ class Plan:
 
     def _build(self, batch):
         sc, lib, h = self.sc, self.lib, self.h
-        self.tabs = [T.axis_tables(sc, a) for a in range(3)]
+        if self.cplx:
+            self.tabs = [T.axis_tables(sc, a, float(sc.bloch_k[a])) for a in range(3)]
+        else:
+            self.tabs = [T.axis_tables(sc, a) for a in range(3)]
         for a, t in enumerate(self.tabs):
             L.check(lib.oem_plan_set_axis(
                 h, a, L.ptr(self._arr(t.idl_p, np.float64)), L.ptr(self._arr(t.idl_d, np.float64)),
@@ -98,6 +139,11 @@ class Plan:
                 L.ptr(self._arr(np.real(t.mpv), np.float64)),
                 L.ptr(self._arr(t.pml_e, np.float64)), L.ptr(self._arr(t.pml_h, np.float64)),
                 int(t.lo), int(t.hi)), f"set_axis {a}")
+        if self.cplx:
+            for a, t in enumerate(self.tabs):
+                L.check(lib.oem_plan_set_axis_phase(
+                    h, a, L.ptr(self._arr(np.imag(t.mnx), np.float64)),
+                    L.ptr(self._arr(np.imag(t.mpv), np.float64))), f"set_axis_phase {a}")
         if self._device_tables():
             from openem_b200 import tables_gpu
             mt = tables_gpu.material_tables_device(sc, self.tabs, self.device)
@@ -135,14 +181,25 @@ class Plan:
                 L.ptr(self._arr(ps["ex"], np.float64)), L.ptr(self._arr(ps["hy"], np.float64))),
                 "add_plane_source")
         for mag in (False, True):
-            dt_ = T.dipole_tables(sc, self.n_total, mag)
+            dt_ = T.dipole_tables(sc, self.n_total, mag, complex_amp=self.cplx)
             if dt_ is None:
                 continue
-            L.check(lib.oem_plan_add_dipoles(
-                h, int(mag), int(dt_["comp"].size), L.ptr(self._arr(dt_["ijk"], np.int32)),
-                L.ptr(self._arr(dt_["comp"], np.int32)), L.ptr(self._arr(dt_["coef"], np.float32)),
-                L.ptr(self._arr(dt_["src"], np.int32)), int(dt_["n_src"]), int(dt_["nsteps1"]),
-                L.ptr(self._arr(dt_["amp"], np.float64))), "add_dipoles")
+            head = (h, int(mag), int(dt_["comp"].size), L.ptr(self._arr(dt_["ijk"], np.int32)),
+                    L.ptr(self._arr(dt_["comp"], np.int32)),
+                    L.ptr(self._arr(dt_["coef"], np.float32)),
+                    L.ptr(self._arr(dt_["src"], np.int32)), int(dt_["n_src"]),
+                    int(dt_["nsteps1"]), L.ptr(self._arr(dt_["amp"], np.float64)))
+            if self.cplx:
+                L.check(lib.oem_plan_add_dipoles_complex(
+                    *head, L.ptr(self._arr(dt_["amp_im"], np.float64))), "add_dipoles_complex")
+            else:
+                L.check(lib.oem_plan_add_dipoles(*head), "add_dipoles")
+        for ms in T.mode_tables(sc, self.n_total):
+            L.check(lib.oem_plan_add_mode_source(
+                h, ms["axis"], ms["kh"], ms["ks"], ms["n1"], ms["n2"], *ms["coef_h"],
+                *ms["coef_e"], int(ms["prof"].shape[0]), L.ptr(self._arr(ms["prof"], np.float32)),
+                ms["ntab"], L.ptr(self._arr(ms["amp_e"], np.float64)),
+                L.ptr(self._arr(ms["amp_h"], np.float64))), "add_mode_source")
         nt = max(self.n_total, 1)
         self.flux_mons = []
         for m in sc.flux_monitors:
@@ -208,12 +265,23 @@ class Plan:
 
     def read_time_monitor(self, mid: int, shape) -> np.ndarray:
         out = np.empty(shape, np.float32)
+        if self.cplx:
+            im = np.empty(shape, np.float32)
+            L.check(self.lib.oem_plan_read_time_monitor_complex(self.h, int(mid), L.ptr(out),
+                                                                L.ptr(im), self._s),
+                    "read_time_monitor_complex")
+            return out + 1j * im
         L.check(self.lib.oem_plan_read_time_monitor(self.h, int(mid), L.ptr(out), self._s),
                 "read_time_monitor")
         return out
 
     def read_field(self, comp: int) -> np.ndarray:
         out = np.empty(self.shape, np.float32)
+        if self.cplx:
+            im = np.empty(self.shape, np.float32)
+            L.check(self.lib.oem_plan_read_field_complex(self.h, int(comp), L.ptr(out),
+                                                         L.ptr(im), self._s), "read_field_complex")
+            return out + 1j * im
         L.check(self.lib.oem_plan_read_field(self.h, int(comp), L.ptr(out), self._s), "read_field")
         return out
 
@@ -303,16 +371,24 @@ def run(sc, num_steps: int | None = None, use_shutoff: bool = True, kernels=None
         return bloch.run(sc, num_steps=num_steps, use_shutoff=use_shutoff, verbose=verbose,
                          return_fields=return_fields, policy=policy, device=device,
                          stream=stream, stats=stats)
+    return run_plan(sc, num_steps, use_shutoff, verbose, return_fields, policy, device, stream,
+                    stats, cplx=False)
+
+
+def run_plan(sc, num_steps, use_shutoff, verbose, return_fields, policy, device, stream, stats,
+             cplx: bool) -> Result:
+    """Build a plan (real or complex fields), step it with the shutoff cadence, read out."""
     n_total = int(num_steps if num_steps is not None else sc.num_time_steps)
-    plan = Plan(sc, n_total, device=device, stream=stream)
+    plan = Plan(sc, n_total, device=device, stream=stream, cplx=cplx)
     try:
         res = _loop(plan, sc, n_total, use_shutoff, verbose, return_fields, policy)
         plan.status()
         if stats is not None:
             d2h = sum(np.asarray(p.data).size * 16 for p in res.phasors.values())
             d2h += sum(np.asarray(a).size * 16 for a in res.field_phasors.values())
-            d2h += sum(np.asarray(a).size * 4 for a in res.time_samples.values())
-            d2h += sum(np.asarray(a).size * 4 for a in res.fields.values())
+            width = 8 if cplx else 4  # float32 parts read back per value
+            d2h += sum(np.asarray(a).size * width for a in res.time_samples.values())
+            d2h += sum(np.asarray(a).size * width for a in res.fields.values())
             stats.update(h2d_bytes=int(plan.h2d_bytes), d2h_bytes=int(d2h),
                          launches_per_step=plan.launches_per_step())
         return res
@@ -344,7 +420,8 @@ def _loop(plan: Plan, sc, n_total: int, use_shutoff: bool, verbose: bool, return
             e = plan.energy()
             m_u = 0.5 * (T.EPSILON_0 * e[1] + T.MU_0 * e[2])
             fl = np.zeros(0)
-            if plan.flux_mons:
+            # the complex path checks no flux criterion (openem/solver.py:1325-1328)
+            if plan.flux_mons and not plan.cplx:
                 plan.flush()
                 fl = np.concatenate([flux_mod.plane_flux(plan.read_monitor(mid, shp), grid,
                                                          axis=int(m.axis))

@@ -347,12 +347,20 @@ def plane_sources(sc):
     return out
 
 
-def dipole_tables(sc, n_total: int, magnetic: bool):
+def dipole_tables(sc, n_total: int, magnetic: bool, complex_amp: bool = False):
+    """Flattened stencils of the electric (half-step table) or magnetic (whole-step table)
+    dipoles (openem/sources_setup.py:419-470). ``complex_amp`` takes the complex analytic
+    amplitude of a Bloch run: ``amp`` then holds its real and ``amp_im`` its imaginary part."""
     dips = [d for d in sc.dipoles if bool(d.magnetic) == magnetic]
     if not dips:
         return None
-    tabs = [np.asarray(d.waveform.amp_int if magnetic else d.waveform.amp_half, np.float64)
-            for d in dips]
+    if complex_amp:
+        ctabs = [np.asarray(d.waveform.amp_int_complex if magnetic
+                            else d.waveform.amp_half_complex, np.complex128) for d in dips]
+        tabs = [np.real(t) for t in ctabs]
+    else:
+        tabs = [np.asarray(d.waveform.amp_int if magnetic else d.waveform.amp_half, np.float64)
+                for d in dips]
     nsteps1 = min(t.size for t in tabs)
     if n_total > nsteps1 - 1:
         raise ValueError(f"asked to run {n_total} steps, but the dipole waveform only sampled "
@@ -365,10 +373,64 @@ def dipole_tables(sc, n_total: int, magnetic: bool):
         comp.append(np.full(len(ind), int(d.component), np.int32))
         coef.append(cf.astype(np.float32))
         src.append(np.full(len(ind), s, np.int32))
-    return {"ijk": np.ascontiguousarray(np.concatenate(ijk).astype(np.int32)),
-            "comp": np.concatenate(comp), "coef": np.concatenate(coef), "src": np.concatenate(src),
-            "n_src": len(dips), "nsteps1": nsteps1,
-            "amp": np.ascontiguousarray(np.stack([t[:nsteps1] for t in tabs]))}
+    out = {"ijk": np.ascontiguousarray(np.concatenate(ijk).astype(np.int32)),
+           "comp": np.concatenate(comp), "coef": np.concatenate(coef), "src": np.concatenate(src),
+           "n_src": len(dips), "nsteps1": nsteps1,
+           "amp": np.ascontiguousarray(np.stack([t[:nsteps1] for t in tabs]))}
+    if complex_amp:
+        out["amp_im"] = np.ascontiguousarray(np.stack([np.imag(t[:nsteps1]) for t in ctabs]))
+    return out
+
+
+# one-plane TF/SF signs of a mode source per direction: (H_t1, H_t2, E_t1, E_t2)
+# (openem/sources_setup.py:51-54)
+MODE_SIGNS = {+1: (-1.0, +1.0, +1.0, -1.0), -1: (+1.0, -1.0, +1.0, -1.0)}
+
+
+def mode_tables(sc, n_total: int) -> list:
+    """One injection entry per mode source (openem/sources_setup.py:376-416): planes, the
+    four float32 coefficients, the (n_terms, 8, n_t1, n_t2) float32 profiles (E_t1, E_t2, H_t1,
+    H_t2 as re/im planes; base term then broadband corrections) and the (n_terms, ntab, 2)
+    float64 amplitude tables. Sources are injected one entry each: the injection is linear, so
+    the sum over entries is the superposition OpenEM forms by merging same-face sources."""
+    out = []
+    for m in getattr(sc, "mode_sources", None) or []:
+        a = int(m.axis)
+        ax = sc.grid.axes[a]
+        ks = int(m.plane_index)
+        kh = ks - 1 if int(m.direction) > 0 else ks
+        s_h1, s_h2, s_e1, s_e2 = MODE_SIGNS[int(m.direction)]
+        ch = sc.dt / MU_0 * float(1.0 / ax.dl[kh])
+        ce = float(1.0 / ax.dl_dual[ks])
+        terms = [(m.ey_inc, m.ez_inc, m.hy_inc, m.hz_inc, m.amp_e, m.amp_h)]
+        for k in range(0 if m.bb_ey is None else len(m.bb_ey)):
+            terms.append((m.bb_ey[k], m.bb_ez[k], m.bb_hy[k], m.bb_hz[k], m.bb_amp_e[k],
+                          m.bb_amp_h[k]))
+        t1, t2 = (a + 1) % 3, (a + 2) % 3
+        n1, n2 = int(sc.shape[t1]), int(sc.shape[t2])
+        ntab = min(min(np.size(t[4]), np.size(t[5])) for t in terms)
+        if n_total > ntab:
+            raise ValueError(f"asked to run {n_total} steps, but the mode amplitude tables hold "
+                             f"{ntab} samples")
+        prof = np.empty((len(terms), 8, n1, n2), np.float32)
+        amp_e = np.empty((len(terms), ntab, 2), np.float64)
+        amp_h = np.empty((len(terms), ntab, 2), np.float64)
+        for q, (e1, e2, h1, h2, ae, ah) in enumerate(terms):
+            for r, pr in enumerate((e1, e2, h1, h2)):
+                pr = np.asarray(pr, np.complex128)
+                if pr.shape != (n1, n2):
+                    raise ValueError(f"mode profile shape {pr.shape} != plane {(n1, n2)}")
+                prof[q, 2 * r] = pr.real
+                prof[q, 2 * r + 1] = pr.imag
+            ae = np.asarray(ae, np.complex128)[:ntab]
+            ah = np.asarray(ah, np.complex128)[:ntab]
+            amp_e[q, :, 0], amp_e[q, :, 1] = ae.real, ae.imag
+            amp_h[q, :, 0], amp_h[q, :, 1] = ah.real, ah.imag
+        out.append({"axis": a, "kh": kh, "ks": ks, "n1": n1, "n2": n2,
+                    "coef_h": (float(np.float32(s_h1 * ch)), float(np.float32(s_h2 * ch))),
+                    "coef_e": (float(np.float32(s_e1 * ce)), float(np.float32(s_e2 * ce))),
+                    "prof": prof, "amp_e": amp_e, "amp_h": amp_h, "ntab": int(ntab)})
+    return out
 
 
 # ---------------------------------------------------------------------------------------------

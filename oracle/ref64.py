@@ -37,6 +37,9 @@ MU_0 = 1.25663706212e-6
 APOD_K = 0.5
 # +z and -z one-face TF/SF correction signs (openem/tfsf1d.py:46)
 _SIGNS = {+1: (1.0, 1.0), -1: (-1.0, -1.0)}
+# one-plane TF/SF signs of a mode source per direction: (H_t1, H_t2, E_t1, E_t2)
+# (openem/sources_setup.py:51-54)
+_MODE_SIGNS = {+1: (-1.0, +1.0, +1.0, -1.0), -1: (+1.0, -1.0, +1.0, -1.0)}
 
 
 def apod_window(t, spec):
@@ -121,7 +124,7 @@ class Oracle:
     def __init__(self, sc, n_total: int | None = None):
         if sc.any_bloch:
             raise ValueError("use BlochOracle for a scene with a non-zero Bloch vector")
-        for feat in ("tfsf_sources", "mode_sources", "absorbers", "flux_time_monitors"):
+        for feat in ("tfsf_sources", "absorbers", "flux_time_monitors"):
             if getattr(sc, feat, None):
                 raise NotImplementedError(f"oracle: {feat} not transcribed")
         if sc.any_dispersion_mix or sc.any_tensor or sc.any_modulation:
@@ -203,6 +206,66 @@ class Oracle:
                 "hy": sum(np.asarray(x.hy_inc, dtype=np.float64) for x in grp)})
         self.dip_e = self._dipole_table([d for d in sc.dipoles if not d.magnetic], half=True)
         self.dip_h = self._dipole_table([d for d in sc.dipoles if d.magnetic], half=False)
+        self.modes = self._mode_tables()
+
+    def _mode_tables(self):
+        """One entry per mode source (openem/sources_setup.py:376-416): the cyclic tangential
+        pair t1 = axis+1, t2 = axis+2, H plane kh and E plane ks, the four coefficients and the
+        (profile, amplitude) terms, the base term followed by the broadband corrections."""
+        sc = self.sc
+        out = []
+        for m in getattr(sc, "mode_sources", None) or []:
+            a = int(m.axis)
+            ax = sc.grid.axes[a]
+            ks = int(m.plane_index)
+            kh = ks - 1 if m.direction > 0 else ks
+            s_h1, s_h2, s_e1, s_e2 = _MODE_SIGNS[int(m.direction)]
+            ch = sc.dt / MU_0 * (1.0 / float(ax.dl[kh]))
+            ce = 1.0 / float(ax.dl_dual[ks])
+            terms_h = [(np.asarray(m.ey_inc), np.asarray(m.ez_inc), np.asarray(m.amp_e))]
+            terms_e = [(np.asarray(m.hy_inc), np.asarray(m.hz_inc), np.asarray(m.amp_h))]
+            for k in range(0 if m.bb_ey is None else len(m.bb_ey)):
+                terms_h.append((np.asarray(m.bb_ey[k]), np.asarray(m.bb_ez[k]),
+                                np.asarray(m.bb_amp_e[k])))
+                terms_e.append((np.asarray(m.bb_hy[k]), np.asarray(m.bb_hz[k]),
+                                np.asarray(m.bb_amp_h[k])))
+            out.append({"axis": a, "t1": (a + 1) % 3, "t2": (a + 2) % 3, "ks": ks, "kh": kh,
+                        "ch": (s_h1 * ch, s_h2 * ch), "ce": (s_e1 * ce, s_e2 * ce),
+                        "th": terms_h, "te": terms_e})
+        return out
+
+    @staticmethod
+    def _plane(F, axis, k):
+        """The (n_t1, n_t2) view of plane ``k`` along ``axis`` in cyclic tangential order."""
+        if axis == 0:
+            return F[k, :, :]          # (y, z)
+        if axis == 1:
+            return F[:, k, :].T        # (z, x)
+        return F[:, :, k]              # (x, y)
+
+    def _mode_value(self, prof, amp):
+        """Real path: Re(profile * amp) (openem/kernels/source_dft.cu:84-128)."""
+        return (prof * amp).real
+
+    def inject_mode_h(self, n):
+        """H side: H_t1 += c_h1 * E_t2 profile * amp_e[n], H_t2 += c_h2 * E_t1 profile."""
+        for md in self.modes:
+            H1 = self._plane(self.H[md["t1"]], md["axis"], md["kh"])
+            H2 = self._plane(self.H[md["t2"]], md["axis"], md["kh"])
+            for e1, e2, amp in md["th"]:
+                H1 += md["ch"][0] * self._mode_value(e2, amp[n])
+                H2 += md["ch"][1] * self._mode_value(e1, amp[n])
+
+    def inject_mode_e(self, n):
+        """E side: E_t1 += cb_t1 * c_e1 * H_t2 profile * amp_h[n], E_t2 likewise with H_t1."""
+        for md in self.modes:
+            E1 = self._plane(self.E[md["t1"]], md["axis"], md["ks"])
+            E2 = self._plane(self.E[md["t2"]], md["axis"], md["ks"])
+            cb1 = self._plane(self.cb[md["t1"]], md["axis"], md["ks"])
+            cb2 = self._plane(self.cb[md["t2"]], md["axis"], md["ks"])
+            for h1, h2, amp in md["te"]:
+                E1 += cb1 * md["ce"][0] * self._mode_value(h2, amp[n])
+                E2 += cb2 * md["ce"][1] * self._mode_value(h1, amp[n])
 
     def _dipole_table(self, dips, half: bool):
         if not dips:
@@ -249,7 +312,8 @@ class Oracle:
             (i0, j0, k0), (ni, nj, nk) = m.origin, m.box
             self.tmon.append({"m": m, "sl": (slice(i0, i0 + ni), slice(j0, j0 + nj),
                                              slice(k0, k0 + nk)),
-                              "buf": np.zeros((len(m.comps), m.num_slots, ni, nj, nk))})
+                              "buf": np.zeros((len(m.comps), m.num_slots, ni, nj, nk),
+                                              dtype=self.E[0].dtype)})
         # t = 0 sample, taken before the loop on zero fields (openem/solver.py:492-495)
         self._sample_time(0)
 
@@ -293,12 +357,15 @@ class Oracle:
         Hz -= self.ch * dHz
 
     def inject_h(self, n):
-        for p in self.pw:
-            Ht = self.H[1] if p["pol"] == 0 else self.H[0]
-            Ht[:, :, p["kh"]] += p["coef_h"] * p["ex"][n]
+        """H-side sources in OpenEM's order (openem/solver.py:876-918): magnetic dipoles, plane
+        waves, mode sources."""
         if self.dip_h is not None:
             for c, i, j, k, cf, s in self.dip_h["pts"]:
                 self.H[c][i, j, k] -= self.ch * cf * self.dip_h["amp"][s, n]
+        for p in self.pw:
+            Ht = self.H[1] if p["pol"] == 0 else self.H[0]
+            Ht[:, :, p["kh"]] += p["coef_h"] * p["ex"][n]
+        self.inject_mode_h(n)
 
     def disp_pre(self):
         d = self.disp
@@ -342,9 +409,12 @@ class Oracle:
         self.E[2] = (ca[2] * Ez + cb[2] * (cz - cw * hs[2])) * px * py
 
     def inject_e(self, n):
+        """E-side sources in OpenEM's order (openem/solver.py:955-969): plane waves, mode
+        sources, electric dipoles."""
         for p in self.pw:
             c = p["pol"]
             self.E[c][:, :, p["ks"]] += self.cb[c][:, :, p["ks"]] * p["coef_e"] * p["hy"][n]
+        self.inject_mode_e(n)
         if self.dip_e is not None:
             for c, i, j, k, cf, s in self.dip_e["pts"]:
                 self.E[c][i, j, k] -= self.cb[c][i, j, k] * cf * self.dip_e["amp"][s, n]
@@ -479,6 +549,8 @@ class BlochOracle(Oracle):
     def __init__(self, sc, n_total: int | None = None):
         if sc.any_dispersion or sc.any_loss or sc.any_pec or sc.sources or sc.tfsf_sources:
             raise NotImplementedError("Bloch subset: lossless, non-dispersive, no plane wave")
+        if getattr(sc, "absorbers", None) or getattr(sc, "flux_time_monitors", None):
+            raise NotImplementedError("oracle: absorbers / flux time monitors not transcribed")
         self.sc = sc
         self.n_total = int(n_total if n_total is not None else sc.num_time_steps)
         self.shape = sc.shape
@@ -506,8 +578,13 @@ class BlochOracle(Oracle):
         self.pw = []
         self.dip_e = self._dipole_table_c([d for d in sc.dipoles if not d.magnetic], True)
         self.dip_h = self._dipole_table_c([d for d in sc.dipoles if d.magnetic], False)
-        self._setup_monitors()
+        self.modes = self._mode_tables()
+        self._setup_monitors()  # complex time samples (openem/kernels/bloch.cu:280-318)
         self.n = 0
+
+    def _mode_value(self, prof, amp):
+        """Complex path: the full product profile * amp (openem/kernels/bloch.cu:326-384)."""
+        return prof * amp
 
     def _dipole_table_c(self, dips, half: bool):
         if not dips:

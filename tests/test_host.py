@@ -119,12 +119,11 @@ def test_phase_table():
     assert ph.dtype == np.float32 and ph.shape == (5, 2, 4)
 
 
-@pytest.mark.parametrize("feature", ["tfsf", "mode", "absorber", "modulation", "tensor"])
+@pytest.mark.parametrize("feature", ["tfsf", "absorber", "modulation", "tensor"])
 def test_unsupported_physics_fails_closed(feature):
     sc = scenes.slab_plane_wave(nxy=1, num_steps=10)
     bad = {
         "tfsf": replace(sc, tfsf_sources=[object()]),
-        "mode": replace(sc, mode_sources=[object()]),
         "absorber": replace(sc, absorbers=[object()]),
         "modulation": replace(sc, modulation=M.TimeModulation(
             1e14, np.array([0]), np.array([0]), np.array([0.1]), np.array([0.0]))),
@@ -133,6 +132,22 @@ def test_unsupported_physics_fails_closed(feature):
     }[feature]
     with pytest.raises(NotImplementedError):
         solver.refuse_unsupported(bad)
+
+
+@pytest.mark.parametrize("feature", ["plane", "dispersion", "loss", "nosource"])
+def test_bloch_subset_fails_closed(feature):
+    """The complex path refuses what OpenEM's does (openem/solver.py:1221-1260)."""
+    sd = scenes.small_dispersive(n=20, n_sph=1, n_pml=4, num_steps=10)
+    plain = replace(sd, dispersion=None, sigma_ex=None, sigma_ey=None, sigma_ez=None)
+    bad = {
+        "plane": scenes.slab_plane_wave(nxy=1, num_steps=10),
+        "dispersion": replace(sd, sigma_ex=None, sigma_ey=None, sigma_ez=None),
+        "loss": replace(sd, dispersion=None),
+        "nosource": replace(plain, dipoles=[]),
+    }[feature]
+    with pytest.raises(NotImplementedError):
+        solver.refuse_unsupported_bloch(bad)
+    solver.refuse_unsupported_bloch(plain)
 
 
 def test_dipole_table_refuses_short_waveform():
