@@ -118,6 +118,16 @@ int oem_plan_add_mode_source(oem_plan* p, int axis, int kh, int ks, int n1, int 
                              int n_terms, const float* profiles, int64_t ntab,
                              const double* amp_e, const double* amp_h);
 
+/* Absorber boundary slab (Tidy3D's Absorber; replaces absorb_slab / absorb_batch,
+ * openem/kernels/absorber.cu:20-70, absorb_batch.cu:15-110, and the host tables of
+ * openem/dispersion_setup.py:89-120): layers [g0, g0 + nlay) along `axis`. After the H-side
+ * sources of every step the H family in the layers is multiplied by the per-layer decay
+ * exp(-Gamma dt) (tangential H at half-cell positions: decay_half, normal H: decay_int), after
+ * the E-side updates the E family (normal E: decay_half, tangential E: decay_int). Several slabs
+ * multiply in the order they were added. Factors must lie in (0, 1]. */
+int oem_plan_add_absorber(oem_plan* p, int axis, int g0, int nlay, const double* decay_int,
+                          const double* decay_half);
+
 /* Complex (Bloch) plan: imaginary parts of the neighbour masks of one axis (the real parts come
  * from oem_plan_set_axis), exp(+-i 2 pi k) at the periodic seam of a Bloch axis
  * (openem/grid.py:219-252). The first call makes the plan complex: every field and psi gets an

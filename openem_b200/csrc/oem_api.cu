@@ -260,6 +260,8 @@ static int enqueue_step(oem_plan* p, cudaStream_t s) {
       return cuda_error(e, "plane_h");
   for (const ModeSrc& m : p->modesrcs)
     if ((e = launch_mode_h(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_h");
+  for (const Absorber& a : p->absorbers)
+    if ((e = launch_absorb(P, a, 0, s)) != cudaSuccess) return cuda_error(e, "absorb_h");
   if (fork) {
     OEM_CUDA(cudaStreamWaitEvent(s, p->ev_join, 0));
     e = launch_update_e_ws(p->tma, P, p->xch, (int)p->mats.size(), p->d_err, s);
@@ -275,6 +277,8 @@ static int enqueue_step(oem_plan* p, cudaStream_t s) {
   for (const DipoleSet& d : p->dipoles)
     if (!d.magnetic && (e = launch_dipoles(P, d, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "dipoles_e");
+  for (const Absorber& a : p->absorbers)
+    if ((e = launch_absorb(P, a, 1, s)) != cudaSuccess) return cuda_error(e, "absorb_e");
   for (const TimeMon& m : p->tmons) {
     if ((e = launch_time_sample(P, m, p->d_step, 1, s)) != cudaSuccess)
       return cuda_error(e, "time_sample");
@@ -646,6 +650,28 @@ int oem_plan_add_dipoles_complex(oem_plan* p, int magnetic, int n_pts, const int
                           amp_im);
 }
 
+int oem_plan_add_absorber(oem_plan* p, int axis, int g0, int nlay, const double* decay_int,
+                          const double* decay_half) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (axis < 0 || axis > 2) return set_error(OEM_ERR_INVALID, "absorber axis must be 0, 1 or 2");
+  const int n = axis == 0 ? p->nx : axis == 1 ? p->ny : p->nz;
+  if (nlay < 1 || g0 < 0 || g0 + nlay > n)
+    return set_error(OEM_ERR_INVALID, "absorber layers outside the axis");
+  if (!decay_int || !decay_half) return set_error(OEM_ERR_INVALID, "null decay profile");
+  for (int l = 0; l < nlay; ++l)
+    if (!(decay_int[l] > 0.0 && decay_int[l] <= 1.0) || !(decay_half[l] > 0.0 && decay_half[l] <= 1.0))
+      return set_error(OEM_ERR_INVALID, "absorber decay factors must lie in (0, 1]");
+  if ((rc = use_device(p))) return rc;
+  Absorber a;
+  a.axis = axis; a.g0 = g0; a.nlay = nlay;
+  std::vector<float> di(decay_int, decay_int + nlay), dh(decay_half, decay_half + nlay);
+  if ((rc = dupload(p, &a.d_int, di.data(), di.size()))) return rc;
+  if ((rc = dupload(p, &a.d_half, dh.data(), dh.size()))) return rc;
+  p->absorbers.push_back(a);
+  return OEM_OK;
+}
+
 int oem_plan_set_axis_phase(oem_plan* p, int axis, const double* mnx_im, const double* mpv_im) {
   int rc = check_plan(p, false);
   if (rc) return rc;
@@ -960,6 +986,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
         if ((e = launch_plane_h(p->yp, src, p->d_step, s)) != cudaSuccess) return cuda_error(e, "plane_h");
       for (const ModeSrc& m : p->modesrcs)
         if ((e = launch_mode_h(p->yp, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_h");
+      for (const Absorber& a : p->absorbers)
+        if ((e = launch_absorb(p->yp, a, 0, s)) != cudaSuccess) return cuda_error(e, "absorb_h");
       OEM_CUDA(cudaEventRecord(E[2], s));
       const bool split = p->basic_kernels == 3 && p->yp.has_ade;
       if (split) {
@@ -981,6 +1009,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       for (const DipoleSet& d : p->dipoles)
         if (!d.magnetic && (e = launch_dipoles(p->yp, d, p->d_step, s)) != cudaSuccess)
           return cuda_error(e, "dipoles_e");
+      for (const Absorber& a : p->absorbers)
+        if ((e = launch_absorb(p->yp, a, 1, s)) != cudaSuccess) return cuda_error(e, "absorb_e");
       for (const TimeMon& m : p->tmons) {
         if ((e = launch_time_sample(p->yp, m, p->d_step, 1, s)) != cudaSuccess) return cuda_error(e, "ts");
         if ((e = launch_time_sample(p->yp, m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "ts");
@@ -1050,6 +1080,7 @@ int oem_plan_launches_per_step(oem_plan* p, int* n) {
   if (p->basic_kernels == 3 && p->yp.has_ade) c += 1;  // separate pole pass
   c += 2 * (int)p->planes.size();
   c += 2 * (int)p->modesrcs.size();
+  c += 2 * (int)p->absorbers.size();
   for (const DipoleSet& d : p->dipoles) c += d.n_targets > 0 ? 1 : 0;
   c += 2 * (int)p->tmons.size();
   c += 3 * (int)p->mons.size();  // snapshot, flush, flush mark

@@ -156,6 +156,14 @@ struct Monitor {
   int cplx = 0;              // complex fields: the ring holds ncomp real then ncomp imaginary rows
 };
 
+// One absorber slab (Tidy3D's Absorber): the layers [g0, g0 + nlay) along `axis`, whole- and
+// half-cell decay factors exp(-Gamma dt) per layer.
+struct Absorber {
+  int axis = 0, g0 = 0, nlay = 0;
+  float* d_int = nullptr;
+  float* d_half = nullptr;
+};
+
 struct TimeMon {
   int nc = 0;
   int comps[6] = {0, 0, 0, 0, 0, 0};
@@ -203,6 +211,7 @@ struct oem_plan {
   std::vector<oem::PlaneSrc> planes;
   std::vector<oem::DipoleSet> dipoles;
   std::vector<oem::ModeSrc> modesrcs;
+  std::vector<oem::Absorber> absorbers;
   bool is_complex = false;  // Bloch / forced complex fields
   std::vector<oem::Monitor> mons;
   std::vector<oem::TimeMon> tmons;
@@ -310,6 +319,7 @@ cudaError_t launch_ade_segments(const YeeParams& P, const int64_t* segs, int64_t
                                 int64_t nseg, int max_blocks, cudaStream_t s);
 cudaError_t launch_update_h_c(const YeeParams& P, cudaStream_t s);
 cudaError_t launch_update_e_c(const YeeParams& P, cudaStream_t s);
+cudaError_t launch_absorb(const YeeParams& P, const Absorber& a, int is_e, cudaStream_t s);
 cudaError_t launch_mode_h(const YeeParams& P, const ModeSrc& m, const int* step, cudaStream_t s);
 cudaError_t launch_mode_e(const YeeParams& P, const ModeSrc& m, const int* step, cudaStream_t s);
 cudaError_t launch_energy(const YeeParams& P, double* const dl[3][2], double* part, int nblocks,

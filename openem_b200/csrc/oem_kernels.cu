@@ -231,6 +231,32 @@ __global__ void k_dipoles(YeeParams P, DipoleSet d, const int* step) {
   }
 }
 
+// Absorber decay of one slab and one field family (openem/kernels/absorber.cu:20-70): the
+// bounding box spans the whole grid except nlay layers along the axis; (j, k) flattened with k
+// innermost, i on blockIdx.y. E: the normal component sits at the half cell; H: the tangential
+// ones. Complex plans decay both parts.
+__global__ void k_absorb(YeeParams P, Absorber a, int is_e, int bj, int bk) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ii = blockIdx.y;
+  if (tid >= bj * bk) return;
+  const int jj = tid / bk;
+  const int kk = tid - jj * bk;
+  const int i = a.axis == 0 ? a.g0 + ii : ii;
+  const int j = a.axis == 1 ? a.g0 + jj : jj;
+  const int k = a.axis == 2 ? a.g0 + kk : kk;
+  const int l = a.axis == 0 ? ii : (a.axis == 1 ? jj : kk);
+  const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + k;
+  const float di = a.d_int[l], dh = a.d_half[l];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const bool half = is_e ? (c == a.axis) : (c != a.axis);
+    const float d = half ? dh : di;
+    const int q = is_e ? c : 3 + c;
+    P.f[q][id] = __fmul_rn(P.f[q][id], d);
+    if (P.cplx) P.fi[q][id] = __fmul_rn(P.fi[q][id], d);
+  }
+}
+
 // Field time monitor, one shot of the two-shot H average (openem/kernels/source_dft.cu:282-319).
 __global__ void k_time_sample(YeeParams P, TimeMon m, const int* step, int add) {
   const int m_ref = (*step + 1) - add;
@@ -568,6 +594,15 @@ cudaError_t launch_time_sample(const YeeParams& P, const TimeMon& m, const int* 
                                cudaStream_t s) {
   dim3 b(32, 4, 1), g((m.nk + 31) / 32, (m.nj + 3) / 4, m.ni);
   k_time_sample<<<g, b, 0, s>>>(P, m, step, add);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_absorb(const YeeParams& P, const Absorber& a, int is_e, cudaStream_t s) {
+  const int box[3] = {a.axis == 0 ? a.nlay : P.nx, a.axis == 1 ? a.nlay : P.ny,
+                      a.axis == 2 ? a.nlay : P.nz};
+  const int64_t njk = (int64_t)box[1] * box[2];
+  dim3 g((unsigned)((njk + 255) / 256), (unsigned)box[0], 1);
+  k_absorb<<<g, 256, 0, s>>>(P, a, is_e, box[1], box[2]);
   return cudaGetLastError();
 }
 

@@ -38,6 +38,7 @@ SIGNATURES = {
     "oem_plan_add_mode_source": (_I, [_P, _I, _I, _I, _I, _I, _D, _D, _D, _D, _I, _P, _L,
                                       _P, _P]),
     "oem_plan_set_axis_phase": (_I, [_P, _I, _P, _P]),
+    "oem_plan_add_absorber": (_I, [_P, _I, _I, _I, _P, _P]),
     "oem_plan_add_flux_monitor": (_I, [_P, _I, _I, _I, _L, _P, _I, C.POINTER(_I)]),
     "oem_plan_add_box_monitor": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _L, _P, _I,
                                       C.POINTER(_I)]),

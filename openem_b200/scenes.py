@@ -564,3 +564,21 @@ def beam_slab(nx: int = 200, ny: int = 200, nz: int = 120, dl: float = 0.025 * U
     return Scene(grid=grid, dt=dt, num_time_steps=num_steps, shutoff=1e-5,
                  eps_ex=eps[0], eps_ey=eps[1], eps_ez=eps[2], pml=pml_dict(grid, dt, n_pml),
                  mode_sources=[src], flux_monitors=mons)
+
+
+def absorber_slabs(grid: Grid, axis: int, n_layers: int, strength: float = 0.05,
+                   order: int = 3) -> list:
+    """Graded absorber slabs on both ends of ``axis``: per step decay ``exp(-s d^order)`` with
+    ``d`` the depth into the absorber (0 at its inner face, 1 at the wall), sampled at the
+    whole-cell and half-cell positions of each layer in global index order."""
+    from openem_b200.model import AbsorberSlab
+    n = int(grid.shape[axis])
+    lay = np.arange(n_layers, dtype=np.float64)
+    lo_int = (n_layers - lay) / n_layers
+    lo_half = (n_layers - lay - 0.5) / n_layers
+    hi_int = lay / n_layers
+    hi_half = (lay + 0.5) / n_layers
+    dec = lambda d: np.exp(-strength * d ** order)
+    return [AbsorberSlab(axis=axis, g0=0, decay_int=dec(lo_int), decay_half=dec(lo_half)),
+            AbsorberSlab(axis=axis, g0=n - n_layers, decay_int=dec(hi_int),
+                         decay_half=dec(hi_half))]

@@ -31,7 +31,7 @@ def refuse_unsupported(sc) -> None:
     """Fail closed on scene features outside this engine's real-field path."""
     checks = [
         (bool(getattr(sc, "tfsf_sources", None)), "TFSF box sources"),
-        (bool(getattr(sc, "absorbers", None)), "Absorber boundaries"),
+        (T.dispersion_in_absorbers(sc), "dispersive media inside Absorber layers"),
         (bool(getattr(sc, "flux_time_monitors", None)), "flux time monitors"),
         (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry > 0,
          "slanted-interface mixed dispersion"),
@@ -66,8 +66,6 @@ def refuse_unsupported_bloch(sc) -> None:
         bad.append("PEC cells")
     if getattr(sc, "flux_time_monitors", None):
         bad.append("FluxTimeMonitor")
-    if getattr(sc, "absorbers", None):
-        bad.append("Absorber boundaries")
     if bad:
         raise NotImplementedError(
             "the Bloch complex-field path does not support: " + ", ".join(bad)
@@ -194,6 +192,9 @@ class Plan:
                     *head, L.ptr(self._arr(dt_["amp_im"], np.float64))), "add_dipoles_complex")
             else:
                 L.check(lib.oem_plan_add_dipoles(*head), "add_dipoles")
+        for axis, g0, nlay, di, dh in T.absorber_tables(sc):
+            L.check(lib.oem_plan_add_absorber(h, axis, g0, nlay, L.ptr(self._arr(di, np.float64)),
+                                              L.ptr(self._arr(dh, np.float64))), "add_absorber")
         for ms in T.mode_tables(sc, self.n_total):
             L.check(lib.oem_plan_add_mode_source(
                 h, ms["axis"], ms["kh"], ms["ks"], ms["n1"], ms["n2"], *ms["coef_h"],

@@ -460,3 +460,31 @@ def batch_depth(points: int, ncomp: int, cap: int = 32, ring_bytes: float = 2e9)
     while T > 1 and T * ncomp * 4 * points > ring_bytes:
         T //= 2
     return max(T, 1)
+
+
+def absorber_tables(sc) -> list:
+    """Absorber slabs in scene order: ``(axis, g0, nlay, decay_int, decay_half)``
+    (openem/dispersion_setup.py:89-120)."""
+    out = []
+    for sl in getattr(sc, "absorbers", None) or []:
+        sl.validate()
+        di = np.asarray(sl.decay_int, np.float64)
+        dh = np.asarray(sl.decay_half, np.float64)
+        if di.size != dh.size:
+            raise ValueError("absorber decay profiles differ in length")
+        out.append((int(sl.axis), int(sl.g0), int(di.size), di, dh))
+    return out
+
+
+def dispersion_in_absorbers(sc) -> bool:
+    """True when a dispersive (component, cell) entry lies inside an absorber's layers."""
+    d = sc.dispersion
+    if d is None or d.n_entry == 0 or not getattr(sc, "absorbers", None):
+        return False
+    cells = np.asarray(d.cell, dtype=np.int64)
+    ijk = np.unravel_index(cells, tuple(int(v) for v in sc.shape))
+    for sl in sc.absorbers:
+        q = ijk[int(sl.axis)]
+        if np.any((q >= int(sl.g0)) & (q < int(sl.g0) + np.size(sl.decay_int))):
+            return True
+    return False

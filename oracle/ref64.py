@@ -124,7 +124,7 @@ class Oracle:
     def __init__(self, sc, n_total: int | None = None):
         if sc.any_bloch:
             raise ValueError("use BlochOracle for a scene with a non-zero Bloch vector")
-        for feat in ("tfsf_sources", "absorbers", "flux_time_monitors"):
+        for feat in ("tfsf_sources", "flux_time_monitors"):
             if getattr(sc, feat, None):
                 raise NotImplementedError(f"oracle: {feat} not transcribed")
         if sc.any_dispersion_mix or sc.any_tensor or sc.any_modulation:
@@ -466,14 +466,33 @@ class Oracle:
                     else:
                         tm["buf"][q, slot] = v
 
+    def absorb(self, family):
+        """Absorber decay (openem/kernels/absorber.cu:20-70): every slab in scene order
+        multiplies the family inside its layers; E normal / H tangential components sit at the
+        half cell (decay_half), the others at the whole cell (decay_int)."""
+        F = self.E if family == "E" else self.H
+        for sl in getattr(self.sc, "absorbers", None) or []:
+            a, g0 = int(sl.axis), int(sl.g0)
+            di = np.asarray(sl.decay_int, np.float64)
+            dh = np.asarray(sl.decay_half, np.float64)
+            sl_ = [slice(None)] * 3
+            sl_[a] = slice(g0, g0 + di.size)
+            sh = [1, 1, 1]
+            sh[a] = -1
+            for c in range(3):
+                half = (c == a) if family == "E" else (c != a)
+                F[c][tuple(sl_)] *= (dh if half else di).reshape(sh)
+
     def step(self):
         n = self.n
         self.update_h()
         self.inject_h(n)
+        self.absorb("H")
         self.disp_pre()
         self.update_e()
         self.inject_e(n)
         self.disp_post()
+        self.absorb("E")
         self._sample_time(n + 1)
         self.dft(n)
         self.n += 1
@@ -549,8 +568,8 @@ class BlochOracle(Oracle):
     def __init__(self, sc, n_total: int | None = None):
         if sc.any_dispersion or sc.any_loss or sc.any_pec or sc.sources or sc.tfsf_sources:
             raise NotImplementedError("Bloch subset: lossless, non-dispersive, no plane wave")
-        if getattr(sc, "absorbers", None) or getattr(sc, "flux_time_monitors", None):
-            raise NotImplementedError("oracle: absorbers / flux time monitors not transcribed")
+        if getattr(sc, "flux_time_monitors", None):
+            raise NotImplementedError("oracle: flux time monitors not transcribed")
         self.sc = sc
         self.n_total = int(n_total if n_total is not None else sc.num_time_steps)
         self.shape = sc.shape

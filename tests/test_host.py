@@ -119,12 +119,13 @@ def test_phase_table():
     assert ph.dtype == np.float32 and ph.shape == (5, 2, 4)
 
 
-@pytest.mark.parametrize("feature", ["tfsf", "absorber", "modulation", "tensor"])
+@pytest.mark.parametrize("feature", ["tfsf", "disp_in_absorber", "modulation", "tensor"])
 def test_unsupported_physics_fails_closed(feature):
     sc = scenes.slab_plane_wave(nxy=1, num_steps=10)
+    sd = scenes.small_dispersive(n=20, n_sph=1, n_pml=4, num_steps=10)
     bad = {
         "tfsf": replace(sc, tfsf_sources=[object()]),
-        "absorber": replace(sc, absorbers=[object()]),
+        "disp_in_absorber": replace(sd, absorbers=scenes.absorber_slabs(sd.grid, 0, 10)),
         "modulation": replace(sc, modulation=M.TimeModulation(
             1e14, np.array([0]), np.array([0]), np.array([0.1]), np.array([0.0]))),
         "tensor": replace(sc, tensor=M.TensorEps(np.array([0]), np.array([0]),
