@@ -118,6 +118,11 @@ int oem_plan_add_mode_source(oem_plan* p, int axis, int kh, int ks, int n1, int 
                              int n_terms, const float* profiles, int64_t ntab,
                              const double* amp_e, const double* amp_h);
 
+/* Tile shape of the pipelined update kernels: x planes walked by one block (0 = the plan's
+ * automatic choice; the warp-specialised kernels cap it at 64). No OpenEM counterpart: set by the
+ * serving autotuner per grid-size class before oem_plan_finalize. */
+int oem_plan_set_xchunk(oem_plan* p, int xch);
+
 /* Absorber boundary slab (Tidy3D's Absorber; replaces absorb_slab / absorb_batch,
  * openem/kernels/absorber.cu:20-70, absorb_batch.cu:15-110, and the host tables of
  * openem/dispersion_setup.py:89-120): layers [g0, g0 + nlay) along `axis`. After the H-side

@@ -650,6 +650,14 @@ int oem_plan_add_dipoles_complex(oem_plan* p, int magnetic, int n_pts, const int
                           amp_im);
 }
 
+int oem_plan_set_xchunk(oem_plan* p, int xch) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (xch < 0 || xch > 4096) return set_error(OEM_ERR_INVALID, "x chunk must be 0..4096");
+  p->xch_user = xch;
+  return OEM_OK;
+}
+
 int oem_plan_add_absorber(oem_plan* p, int axis, int g0, int nlay, const double* decay_int,
                           const double* decay_half) {
   int rc = check_plan(p, false);
@@ -918,7 +926,7 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
       if ((rc = dalloc(p, &p->d_ade_segs, (size_t)std::max<int64_t>(p->n_ade_segs, 1)))) return rc;
       OEM_CUDA(cudaMemset(dcount, 0, sizeof(h)));
       OEM_CUDA(launch_list_pole_segments(P, nseg, p->d_ade_segs, dcount, 0));
-      OEM_CUDA(cudaDeviceSynchronize());
+      OEM_CUDA(cudaStreamSynchronize(0));
     }
     P.has_ade = 1;
   }
@@ -936,6 +944,7 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
       if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
     }
   }
+  if (p->xch_user > 0) p->xch = p->xch_user;
   if (const char* xs = getenv("OEM_B200_XCHUNK")) p->xch = std::max(1, atoi(xs));
   if (p->basic_kernels == 3) p->xch = std::min(p->xch, ws_max_xchunk());
   p->energy_blocks = energy_block_count(P);
@@ -952,7 +961,9 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   p->graph_steps = G;
   if ((rc = capture(p, 1, &p->graph_one))) return rc;
   if (G > 1 && (rc = capture(p, G, &p->graph_many))) return rc;
-  OEM_CUDA(cudaDeviceSynchronize());
+  // setup work runs on the legacy default stream; waiting for it alone leaves other plans'
+  // (non-blocking) streams running, which a server with several plans in flight relies on
+  OEM_CUDA(cudaStreamSynchronize(0));
   p->finalized = true;
   return OEM_OK;
 }

@@ -245,6 +245,7 @@ struct oem_plan {
   cudaStream_t side_stream = nullptr;  // branch of the captured step that runs the pole pass
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int xch = 8;            // x planes per thread in the streaming kernels
+  int xch_user = 0;       // tile shape chosen by the caller (0: automatic)
 };
 
 namespace oem {

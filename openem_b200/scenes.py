@@ -582,3 +582,83 @@ def absorber_slabs(grid: Grid, axis: int, n_layers: int, strength: float = 0.05,
     return [AbsorberSlab(axis=axis, g0=0, decay_int=dec(lo_int), decay_half=dec(lo_half)),
             AbsorberSlab(axis=axis, g0=n - n_layers, decay_int=dec(hi_int),
                          decay_half=dec(hi_half))]
+
+
+def serving_request(n: int, rng, num_steps: int, dl: float = 0.02 * UM,
+                    n_pml: int = 12) -> Scene:
+    """One request of a serving stream: an ``n^3`` grid (CPML on all faces included), a medium
+    drawn from {non-dispersive eps ~ U[1, 12]; 1-pole Drude; 2-pole Lorentz} filling 1 to 16
+    random boxes, a z dipole at a random interior point or a +z plane wave, and one flux
+    monitor near the top face at 4 to 32 frequencies. ``rng`` is a numpy Generator."""
+    n_pml = min(n_pml, max(4, n // 8))
+    n_in = n - 2 * n_pml
+    lo = -0.5 * n_in * dl
+    axes = [uniform_axis(n_in, dl, lo, "PML", n_pml) for _ in range(3)]
+    grid = Grid(*axes)
+    dt = courant_dt([a.dl for a in axes])
+    shape = grid.shape
+    kind = int(rng.integers(0, 3))
+    nbox = int(rng.integers(1, 17))
+    coords = yee_coords(grid)
+    boxes = []
+    for _ in range(nbox):
+        c = rng.uniform(lo * 0.8, -lo * 0.8, size=3)
+        h = rng.uniform(0.05, 0.25, size=3) * (-2.0 * lo)
+        boxes.append((c - h, c + h))
+    masks = []
+    for comp in range(3):
+        x, y, z = coords[comp]
+        m = np.zeros(shape, dtype=bool)
+        for b0, b1 in boxes:
+            ix = (x >= b0[0]) & (x <= b1[0])
+            iy = (y >= b0[1]) & (y <= b1[1])
+            iz = (z >= b0[2]) & (z <= b1[2])
+            m |= ix[:, None, None] & iy[None, :, None] & iz[None, None, :]
+        masks.append(m)
+    eps = [np.ones(shape) for _ in range(3)]
+    sig = None
+    disp = None
+    if kind == 0:
+        v = float(rng.uniform(1.0, 12.0))
+        for c in range(3):
+            eps[c][masks[c]] = v
+    else:
+        if kind == 1:
+            poles = drude_poles(float(rng.uniform(5e15, 1.5e16)), float(rng.uniform(5e13, 2e14)))
+        else:
+            poles = lorentz_poles(float(rng.uniform(0.5, 3.0)), float(rng.uniform(1e14, 4e14)),
+                                  float(rng.uniform(1e13, 5e13))) + \
+                lorentz_poles(float(rng.uniform(0.5, 3.0)), float(rng.uniform(1e14, 4e14)),
+                              float(rng.uniform(1e13, 5e13)))
+        poles, sigma = split_dc(poles, dt)
+        am1, b = trap_coeffs(poles, dt)
+        disp = build_dispersion(masks, am1, b, shape)
+        if sigma:
+            sig = [np.where(masks[c], sigma, 0.0) for c in range(3)]
+    freq0, fwidth = 2e14, 1e14
+    pulse = GaussianPulse(freq0=freq0, fwidth=fwidth)
+    wf = sample_waveform(pulse, dt, num_steps)
+    edges_z = np.asarray(axes[2].edges)
+    sources, dipoles = [], []
+    if rng.integers(0, 2) == 0:
+        pos = rng.uniform(lo * 0.5, -lo * 0.5, size=3)
+        idx, coef = dipole_stencil(grid, 2, tuple(pos))
+        dipoles.append(PointDipole(component=2, indices=idx, coef=coef, waveform=wf))
+    else:
+        ks = n_pml + max(2, n_in // 8)
+        dl_half = 0.5 * float(axes[2].dl[ks - 1])
+        ex_inc, hy_inc = plane_wave_tables(pulse, dt, num_steps, dl_half, 1.0, 1)
+        sources.append(PlaneWaveSource(axis=2, plane_index=ks, direction=1, pol_axis=0,
+                                       waveform=wf, angle_theta=0.0, num_freqs=1,
+                                       ex_inc=ex_inc, hy_inc=hy_inc,
+                                       center=float(edges_z[ks])))
+    nf = int(rng.integers(4, 33))
+    freqs = np.linspace(freq0 - 0.5 * fwidth, freq0 + 0.5 * fwidth, nf)
+    km = n - n_pml - max(2, n_in // 8)
+    mons = [FluxMonitor(name="T", axis=2, plane_index=km, normal_dir=1, freqs=freqs,
+                        source_spectrum=spectrum(pulse, dt, num_steps, freqs))]
+    sig = sig or [None, None, None]
+    return Scene(grid=grid, dt=dt, num_time_steps=num_steps, shutoff=1e-5,
+                 eps_ex=eps[0], eps_ey=eps[1], eps_ez=eps[2], pml=pml_dict(grid, dt, n_pml),
+                 sigma_ex=sig[0], sigma_ey=sig[1], sigma_ez=sig[2], dispersion=disp,
+                 sources=sources, dipoles=dipoles, flux_monitors=mons)

@@ -1,0 +1,360 @@
+"""Continuous-batching simulation server on one GPU.
+
+A request is a ``Scene`` and a step count with an arrival time. The server admits requests as
+they arrive while a slot and HBM are free (admission by the plan's estimated device footprint),
+builds each admitted simulation's plan (host tables, upload, graph capture) on a worker thread
+while the device steps the plans already resident, gives every plan its own non-blocking CUDA
+stream, and advances each in chunks of captured step graphs, so that the work of requests that
+arrive while others run overlaps on the device. A finished plan is read out on its
+own stream and its memory released lazily, in batches (``cudaFree`` waits for the whole device,
+so freeing one plan at a time would stall every stream in flight).
+
+Tile shapes: the warp-specialised update kernels walk a chunk of x planes per block; an
+autotuner (:class:`Tuner`) times the candidate chunks once per grid-size class on a probe plan
+and the server builds every plan of that class with the winner.
+
+Each request's result is exactly what it would be alone: plans share nothing but the device.
+
+    python -m openem_b200.serve --requests 48 --min-n 48 --max-n 192 --min-steps 500 \\
+        --max-steps 1500 --load 4.0
+
+prints one JSON line with sims/s and p50/p99 latency of the served stream against the same
+requests run one at a time through :func:`openem_b200.solver.run`.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from openem_b200 import solver
+from openem_b200.results import Result
+
+
+@dataclass
+class Request:
+    rid: int
+    scene: object
+    num_steps: int
+    arrival: float = 0.0  # seconds after the start of serving
+
+
+@dataclass
+class Done:
+    rid: int
+    result: Result
+    arrival: float
+    start: float
+    finish: float
+
+    @property
+    def latency(self) -> float:
+        return self.finish - self.arrival
+
+
+def footprint(sc, num_steps: int) -> int:
+    """Estimated device bytes of a plan of ``sc``: fields, material index, CPML psi, pole states
+    and currents, monitor rings, accumulators and phase tables, plus a fixed margin."""
+    nx, ny, nz = (int(v) for v in sc.shape)
+    nzp = (nz + 31) // 32 * 32
+    ncp = nx * ny * nzp
+    b = 24 * ncp + 2 * ncp
+    for a, n in enumerate((nx, ny, nz)):
+        layers = sum(int(np.asarray(sc.pml[(a, s)].a_E).size) for s in ("lo", "hi")
+                     if (a, s) in sc.pml)
+        b += 16 * layers * (ncp // max(n, 1))
+    if sc.dispersion is not None:
+        npole = int(sc.dispersion.n_pole)
+        b += 12 * npole + ncp // 8
+    for m in sc.flux_monitors:
+        t = [int(sc.shape[a]) for a in range(3) if a != m.axis]
+        pts, nf = t[0] * t[1], int(np.size(m.freqs))
+        b += 32 * 4 * 4 * pts + 2 * 4 * nf * pts * 8 + num_steps * nf * 16
+    for m in sc.field_monitors:
+        pts, nf = int(np.prod(m.box)), int(np.size(m.freqs))
+        b += 32 * 6 * 4 * pts + 2 * 6 * nf * pts * 8 + num_steps * nf * 16
+    return int(b + (32 << 20))
+
+
+class Tuner:
+    """Per grid-size class, the x-plane chunk of the update kernels that steps a probe plan
+    fastest. A class is the padded grid shape; the probe is a vacuum scene of that shape with
+    CPML on all faces, timed over ``steps`` steps per candidate with CUDA events."""
+
+    def __init__(self, device: int = 0, candidates=(8, 16, 32, 64), steps: int = 30):
+        self.device = int(device)
+        self.candidates = tuple(int(c) for c in candidates)
+        self.steps = int(steps)
+        self.cache: dict = {}
+
+    @staticmethod
+    def size_class(sc) -> tuple:
+        nx, ny, nz = (int(v) for v in sc.shape)
+        return (nx, ny, (nz + 31) // 32 * 32)
+
+    def xchunk(self, sc) -> int:
+        key = self.size_class(sc)
+        if key not in self.cache:
+            self.cache[key] = self._tune(sc)
+        return self.cache[key]
+
+    def _tune(self, sc) -> int:
+        from dataclasses import replace
+        probe = replace(sc, dispersion=None, sigma_ex=None, sigma_ey=None, sigma_ez=None,
+                        sources=[], field_monitors=[], flux_monitors=[],
+                        field_time_monitors=[], num_time_steps=3 * self.steps)
+        best, best_ms = 0, math.inf
+        for c in self.candidates:
+            if c > int(sc.shape[0]):
+                continue
+            p = solver.Plan(probe, 3 * self.steps, device=self.device, xchunk=c)
+            try:
+                p.run(self.steps)
+                p.enable_timing(True)
+                p.run(self.steps)
+                p.status()
+                tm = p.timing()
+                ms = tm["update_h"][1] + tm["update_e"][1]
+            finally:
+                p.close()
+            if ms < best_ms:
+                best, best_ms = c, ms
+        return best
+
+
+def _plan_factory(req: Request, device: int, stream, tuner: Tuner | None):
+    xch = tuner.xchunk(req.scene) if tuner is not None else 0
+    return solver.Plan(req.scene, req.num_steps, device=device, stream=stream, xchunk=xch)
+
+
+class Server:
+    """Admit, step and read out requests with continuous batching (see the module docstring).
+
+    ``max_slots`` bounds the simulations in flight, ``mem_budget`` (bytes) their summed
+    footprint; ``chunk`` is the number of steps issued to a plan at a time."""
+
+    def __init__(self, device: int = 0, max_slots: int = 16, mem_budget: int | None = None,
+                 chunk: int = 256, tuner: Tuner | None = None, plan_factory=None,
+                 clock=time.perf_counter, stream_factory=None, event_factory=None,
+                 build_workers: int = 4):
+        self.device = int(device)
+        self.build_workers = int(build_workers)
+        self.max_slots = int(max_slots)
+        self.chunk = int(chunk)
+        self.tuner = tuner
+        self.clock = clock
+        self.plan_factory = plan_factory or (lambda r, s: _plan_factory(r, self.device, s,
+                                                                         self.tuner))
+        if mem_budget is None:
+            import torch
+            free, _total = torch.cuda.mem_get_info(self.device)
+            mem_budget = int(0.85 * free)
+        self.mem_budget = int(mem_budget)
+        if stream_factory is None:
+            import torch
+            stream_factory = lambda: torch.cuda.Stream(device=self.device)  # noqa: E731
+            event_factory = lambda: torch.cuda.Event()  # noqa: E731
+            self.device_ctx = lambda: torch.cuda.set_device(self.device)  # noqa: E731
+        self.stream_factory = stream_factory
+        self.event_factory = event_factory
+        self.log: list = []  # (time, event, rid) for tests and reports
+
+    def serve(self, requests) -> list:
+        from concurrent.futures import ThreadPoolExecutor
+        pool = ThreadPoolExecutor(max_workers=max(1, self.build_workers))
+        try:
+            return self._serve(requests, pool)
+        finally:
+            pool.shutdown(wait=True)
+
+    def _build(self, req, stream):
+        if self.device_ctx is not None:
+            self.device_ctx()
+        return self.plan_factory(req, stream)
+
+    device_ctx = None
+
+    def _serve(self, requests, pool) -> list:
+        pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
+        active = []       # dicts: req, plan (or its future), stream, event, steps, start, bytes
+        graveyard = []    # finished plans whose memory is released in batches
+        used = 0
+        dead_bytes = 0
+        done = []
+        t0 = self.clock()
+        while pending or active:
+            now = self.clock() - t0
+            progressed = False
+            # admission: arrived requests, while a slot and the memory budget allow
+            while pending and pending[0].arrival <= now and len(active) < self.max_slots:
+                req = pending[0]
+                need = footprint(req.scene, req.num_steps)
+                if used + dead_bytes + need > self.mem_budget and graveyard:
+                    for p in graveyard:
+                        p.close()
+                    graveyard.clear()
+                    dead_bytes = 0
+                if used + need > self.mem_budget and active:
+                    break  # wait for a simulation to finish and free its memory
+                pending.pop(0)
+                stream = self.stream_factory()
+                ent = {"req": req, "plan": None, "stream": stream, "event": self.event_factory(),
+                       "steps": 0, "start": self.clock() - t0, "bytes": need,
+                       "future": pool.submit(self._build, req, stream)}
+                active.append(ent)
+                used += need
+                self.log.append((ent["start"], "admit", req.rid))
+                progressed = True
+            # step: a built plan whose previous chunk has drained gets the next one
+            for ent in list(active):
+                if ent["plan"] is None:
+                    if not ent["future"].done():
+                        continue
+                    ent["plan"] = ent["future"].result()  # re-raises a failed build
+                    self._issue(ent)
+                    progressed = True
+                    continue
+                if not ent["event"].query():
+                    continue
+                req = ent["req"]
+                if ent["steps"] < req.num_steps:
+                    self._issue(ent)
+                    progressed = True
+                    continue
+                res = self._readout(ent)
+                fin = self.clock() - t0
+                done.append(Done(req.rid, res, req.arrival, ent["start"], fin))
+                self.log.append((fin, "done", req.rid))
+                active.remove(ent)
+                used -= ent["bytes"]
+                dead_bytes += ent["bytes"]
+                graveyard.append(ent["plan"])
+                progressed = True
+            if not progressed:
+                if not active and pending:
+                    wait = pending[0].arrival - (self.clock() - t0)
+                    if wait > 0:
+                        time.sleep(min(wait, 0.01))
+                else:
+                    time.sleep(5e-5)
+        for p in graveyard:
+            p.close()
+        return sorted(done, key=lambda d: d.rid)
+
+
+
+    def _issue(self, ent) -> None:
+        req = ent["req"]
+        n = min(self.chunk, req.num_steps - ent["steps"])
+        ent["plan"].run(n)
+        ent["steps"] += n
+        ent["event"].record(ent["stream"])
+
+    @staticmethod
+    def _readout(ent) -> Result:
+        plan = ent["plan"]
+        plan.flush()
+        plan.status()
+        tsamp, tslots = plan.time_samples(ent["steps"])
+        return Result(phasors=plan.flux_phasors(), steps_run=ent["steps"],
+                      shutoff_triggered=False, field_phasors=plan.field_phasors(),
+                      time_samples=tsamp, time_slots=tslots)
+
+
+def serial(requests, device: int = 0) -> list:
+    """The same requests one at a time through the plain engine (``solver.run``), back to back
+    from t = 0; returns Done records with the serial completion times."""
+    import torch
+    out = []
+    t0 = time.perf_counter()
+    for req in sorted(requests, key=lambda r: r.rid):
+        start = time.perf_counter() - t0
+        res = solver.run(req.scene, num_steps=req.num_steps, use_shutoff=False, verbose=False,
+                         device=device)
+        torch.cuda.synchronize(device)
+        out.append(Done(req.rid, res, 0.0, start, time.perf_counter() - t0))
+    return out
+
+
+def make_stream(n_requests: int, seed: int = 3, n_range=(64, 384), step_range=(1000, 6000)):
+    """The request stream: N log-uniform in ``n_range``, steps uniform in ``step_range``, each
+    scene from :func:`openem_b200.scenes.serving_request` (seeded)."""
+    from openem_b200 import scenes
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for q in range(n_requests):
+        n = int(round(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1])))))
+        steps = int(rng.integers(step_range[0], step_range[1] + 1))
+        reqs.append(Request(q, scenes.serving_request(n, rng, steps), steps))
+    return reqs
+
+
+def poisson_arrivals(requests, rate: float, seed: int = 3) -> None:
+    """Arrival times of a Poisson process of ``rate`` requests per second, in place."""
+    rng = np.random.default_rng(seed + 1)
+    t = 0.0
+    for r in requests:
+        r.arrival = t
+        t += float(rng.exponential(1.0 / rate))
+
+
+def _percentiles(lat):
+    lat = np.sort(np.asarray(lat))
+    return float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--min-n", type=int, default=48)
+    ap.add_argument("--max-n", type=int, default=192)
+    ap.add_argument("--min-steps", type=int, default=500)
+    ap.add_argument("--max-steps", type=int, default=1500)
+    ap.add_argument("--load", type=float, default=4.0,
+                    help="offered load as a multiple of the serial capacity")
+    ap.add_argument("--slots", type=int, default=16)
+    ap.add_argument("--workers", type=int, default=4, help="plan-building threads")
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args()
+    import torch
+    torch.cuda.set_device(a.device)
+    reqs = make_stream(a.requests, a.seed, (a.min_n, a.max_n), (a.min_steps, a.max_steps))
+    # warm-up: the library, the first graph capture and the tuner's probes
+    tuner = Tuner(a.device)
+    for r in reqs:
+        tuner.xchunk(r.scene)
+    solver.run(reqs[0].scene, num_steps=10, use_shutoff=False, verbose=False, device=a.device)
+    ser = serial(reqs, a.device)
+    t_ser = ser[-1].finish
+    rate = a.load * len(reqs) / t_ser
+    poisson_arrivals(reqs, rate, a.seed)
+    srv = Server(a.device, max_slots=a.slots, tuner=tuner, build_workers=a.workers)
+    got = srv.serve(reqs)
+    t_srv = max(d.finish for d in got) - min(r.arrival for r in reqs)
+    same = all(np.array_equal(g.result.phasors["T"].data, s.result.phasors["T"].data)
+               for g, s in zip(got, ser))
+    p50, p99 = _percentiles([d.latency for d in got])
+    s50, s99 = _percentiles([d.finish for d in ser])
+    cells = sum(int(np.prod(r.scene.shape)) * r.num_steps for r in reqs)
+    print(json.dumps({
+        "metric": "served sims/s", "requests": len(reqs),
+        "sims_per_s": len(reqs) / t_srv, "serial_sims_per_s": len(reqs) / t_ser,
+        "ratio": t_ser / t_srv, "p50_latency_s": p50, "p99_latency_s": p99,
+        "serial_p50_completion_s": s50, "serial_p99_completion_s": s99,
+        "offered_load_x_serial": a.load, "arrival_rate_per_s": rate,
+        "gcell_updates": cells / 1e9, "identical_to_alone": bool(same),
+        "config": {"n_range": [a.min_n, a.max_n], "step_range": [a.min_steps, a.max_steps],
+                   "slots": a.slots, "build_workers": a.workers, "seed": a.seed,
+                   "tuned_xchunk": {
+                       "x".join(str(v) for v in k): c for k, c in tuner.cache.items()}}}),
+          flush=True)
+
+
+if __name__ == "__main__":
+    main()

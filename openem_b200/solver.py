@@ -81,8 +81,9 @@ class Plan:
     """One simulation resident on the device: owns a ``oem_plan``."""
 
     def __init__(self, sc, n_total: int | None = None, device: int = 0, stream=None,
-                 batch: int | None = None, cplx: bool = False):
+                 batch: int | None = None, cplx: bool = False, xchunk: int = 0):
         self.cplx = bool(cplx)
+        self.xchunk = int(xchunk)
         if self.cplx:
             refuse_unsupported_bloch(sc)
         else:
@@ -237,6 +238,8 @@ class Plan:
                                                   int(m.interval), int(m.num_slots),
                                                   C.byref(mid)), f"time monitor {m.name}")
             self.time_mons.append((m, mid.value, (int(comps.size), int(m.num_slots), ni, nj, nk)))
+        if self.xchunk:
+            L.check(lib.oem_plan_set_xchunk(h, self.xchunk), "set_xchunk")
         L.check(lib.oem_plan_finalize(h, self.n_total), "finalize")
         self._keep.clear()
 
