@@ -173,9 +173,14 @@ class Server:
             pool.shutdown(wait=True)
 
     def _build(self, req, stream):
-        if self.device_ctx is not None:
-            self.device_ctx()
-        return self.plan_factory(req, stream)
+        if self.device_ctx is None:
+            return self.plan_factory(req, stream)
+        import torch
+        self.device_ctx()
+        # device-side table builds run on a high-priority stream, so that their small kernels
+        # are scheduled ahead of the pending blocks of the simulations in flight
+        with torch.cuda.stream(torch.cuda.Stream(device=self.device, priority=-1)):
+            return self.plan_factory(req, stream)
 
     device_ctx = None
 

@@ -116,7 +116,7 @@ class Plan:
         from openem_b200 import tables_gpu
         if mode == "device":
             return True
-        return int(np.prod(self.shape)) >= 2_000_000 and tables_gpu.available()
+        return int(np.prod(self.shape)) >= 100_000 and tables_gpu.available()
 
     def _arr(self, a, dtype):
         a = np.ascontiguousarray(a, dtype=dtype)

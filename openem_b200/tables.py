@@ -39,17 +39,47 @@ def factorize(a: np.ndarray):
     a = np.ascontiguousarray(a).ravel()
     if _pd is not None:
         codes, uniq = _pd.factorize(a, sort=False)
-        return codes.astype(np.int64), len(uniq)
+        return codes.astype(np.int64, copy=False), len(uniq)
     uniq, inv = np.unique(a, return_inverse=True)
-    return inv.astype(np.int64), uniq.size
+    return inv.astype(np.int64, copy=False), uniq.size
 
 
-def factorize_rows(cols):
-    """Codes for the distinct rows of equal-length integer columns, and their count."""
+def _factorize_rows_exact(cols):
     code, n = factorize(cols[0])
     for c in cols[1:]:
         cc, m = factorize(c)
         code, n = factorize(code * m + cc)
+    return code, n
+
+
+def factorize_rows(cols):
+    """Codes for the distinct rows of equal-length integer columns, and their count.
+
+    One 64-bit hash per row (a multiply-xor mix of the columns, finished with the splitmix64
+    avalanche) is factorised once; every row is then compared column by column with the first
+    row of its code, and any collision falls back to the exact column-by-column factorisation,
+    so the codes are always exact."""
+    if len(cols) == 1:
+        return factorize(cols[0])
+    u = [np.ascontiguousarray(c).ravel().view(np.uint64) for c in cols]
+    h = np.zeros(u[0].size, np.uint64)
+    with np.errstate(over="ignore"):
+        for c in u:
+            h ^= c
+            h *= np.uint64(0x9E3779B97F4A7C15)
+            h ^= h >> np.uint64(29)
+        h ^= h >> np.uint64(30)
+        h *= np.uint64(0xBF58476D1CE4E5B9)
+        h ^= h >> np.uint64(27)
+        h *= np.uint64(0x94D049BB133111EB)
+        h ^= h >> np.uint64(31)
+    code, n = factorize(h)
+    first = np.empty(n, dtype=np.int64)
+    first[code[::-1]] = np.arange(code.size - 1, -1, -1, dtype=np.int64)
+    rep = first[code]
+    for c in u:
+        if not np.array_equal(c[rep], c):
+            return _factorize_rows_exact(cols)
     return code, n
 
 

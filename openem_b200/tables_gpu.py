@@ -152,6 +152,7 @@ def material_tables_device(sc, tabs, device: int = 0) -> DeviceTables:
         raise ValueError("more than 2^32 ADE poles")
     seg_ofs = (torch.cumsum(seg, 0) - seg).to(torch.int64) & mask32
     seg_ofs = seg_ofs.to(torch.int32).contiguous()
-    torch.cuda.synchronize(dev)
+    # the stream the tables were built on, not the whole device: other plans may be stepping
+    torch.cuda.current_stream(dev).synchronize()
     return DeviceTables(table=rec, index=index, n_mat=n_mat, set_ofs=set_ofs,
                         coef=np.ascontiguousarray(coef), seg_ofs=seg_ofs, n_pole_total=total)
