@@ -123,6 +123,21 @@ int oem_plan_add_mode_source(oem_plan* p, int axis, int kh, int ks, int n1, int 
  * serving autotuner per grid-size class before oem_plan_finalize. */
 int oem_plan_set_xchunk(oem_plan* p, int xch);
 
+/* Discrete adjoint of a flux objective (the reference computes gradients with forward and
+ * adjoint solves through tidy3d's VJP, openem/nb/autograd_hook.py:184-221; this engine adds a
+ * time-reversed discrete adjoint with K-step checkpoints). oem_plan_enable_checkpoints (before
+ * finalize) makes every oem_plan_run save the fields and CPML psi at steps 0, K, 2K, ...;
+ * after the whole forward pass, oem_plan_adjoint_flux differentiates
+ *   J = sum_f weights[f] * P_f,  P_f = 1/2 sum_plane [Re(E_t1 H_t2*) dA_1 - Re(E_t2 H_t1*) dA_2]
+ * of flux monitor mon_id (the phasors it accumulated; dA1, dA2 the (n1, n2) face elements of the
+ * two terms, transverse axes ascending) with respect to the E-update coefficients:
+ * g_ca, g_cb receive dJ/dca and dJ/dcb per component and cell, (3, nx, ny, nz) float64 each. It
+ * recomputes each segment from its checkpoint (the plan's fields are overwritten) and runs the
+ * transposed step backward. Real, non-dispersive plans without absorbers. */
+int oem_plan_enable_checkpoints(oem_plan* p, int k);
+int oem_plan_adjoint_flux(oem_plan* p, int mon_id, const double* weights, const double* dA1,
+                          const double* dA2, double* g_ca, double* g_cb, void* stream);
+
 /* Absorber boundary slab (Tidy3D's Absorber; replaces absorb_slab / absorb_batch,
  * openem/kernels/absorber.cu:20-70, absorb_batch.cu:15-110, and the host tables of
  * openem/dispersion_setup.py:89-120): layers [g0, g0 + nlay) along `axis`. After the H-side

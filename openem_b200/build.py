@@ -20,7 +20,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "liboem_b200.so"
 SOURCES = ["oem_api.cu", "oem_kernels.cu", "oem_yee_stream.cu", "oem_yee_tma.cu",
-           "oem_noalloc.cu", "oem_yee_ws.cu", "oem_ade.cu", "oem_complex.cu"]
+           "oem_noalloc.cu", "oem_yee_ws.cu", "oem_ade.cu", "oem_complex.cu", "oem_adjoint.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1,0 +1,277 @@
+// Discrete adjoint of the real-field step: the transpose of the forward update, run backward in
+// time, for an objective that is a weighted sum of flux-plane powers at monitor frequencies.
+//
+// Forward step n (the kernels of oem_kernels.cu / oem_yee_ws.cu, same arithmetic):
+//   H^{n+1/2} = H^{n-1/2} - ch (S_a - S_b),   S = d / kappa + psi',  psi' = b psi + a d,
+//                                             d = (E[nxt] m - E) / dl        (forward differences)
+//   E^{n+1}   = ca E^n + cb (S_a - S_b) [+ sources, all proportional to cb],
+//                                             d = (H - H[prv] m) / dl        (backward differences)
+// is linear in (E, H, psi). Its transpose, applied from step N-1 down to 0 to the adjoint
+// state (lambda_E, lambda_H, lambda_psi):
+//   1. objective sources of step n: lambda_E += dJ/dE^{n+1}, lambda_H += dJ/dH^{n+1/2};
+//   2. reverse E update: gradient terms, S_bar = +-cb lambda_E, psi: psi_bar = lambda_psi +
+//      S_bar, d_bar = S_bar / kappa + a psi_bar, lambda_psi <- b psi_bar; lambda_E <- ca lambda_E;
+//      lambda_H gathers the transposed backward differences of d_bar;
+//   3. reverse H update: S_bar = -+ch lambda_H, same psi rule; lambda_E gathers the transposed
+//      forward differences; lambda_H passes through.
+// Gradients: with T^n = (E^{n+1} - ca E^n) / cb (the curl term including every cb-proportional
+// source), dJ/dca = sum_n lambda_E^{n+1} E^n and dJ/dcb = sum_n lambda_E^{n+1} T^n per
+// component and cell, accumulated in float64.
+//
+// The transposed differences are gathers (one thread per cell): a cell receives its own term
+// and the terms of the cells whose neighbour it is; at a clamped wall or a PMC / symmetry plane a
+// cell can be its own neighbour, so the inverse neighbour relation is checked explicitly.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "oem_internal.cuh"
+
+namespace oem {
+
+namespace {
+
+__device__ __forceinline__ int64_t psi_index(const DevAxis& A, int a, int i, int j, int k,
+                                             int ny, int nzp, int* side) {
+  const int q = (a == 0) ? i : ((a == 1) ? j : k);
+  int ql, L;
+  if (q < A.lo) {
+    *side = 0; ql = q; L = A.lo;
+  } else if (q >= A.n - A.hi) {
+    *side = 1; ql = q - (A.n - A.hi); L = A.hi;
+  } else {
+    return -1;
+  }
+  if (a == 0) return ((int64_t)ql * ny + j) * nzp + k;
+  if (a == 1) return ((int64_t)i * L + ql) * nzp + k;
+  return ((int64_t)i * ny + j) * L + ql;
+}
+
+// adjoint of S = d / kappa + (b psi + a d) for one slab array (or S = d outside the slabs)
+__device__ __forceinline__ float dbar_of(float sbar, const PsiSet& LP, int a, int slot,
+                                         const DevAxis& A, const float* ca, const float* cb,
+                                         const float* ck, int q, int i, int j, int k, int ny,
+                                         int nzp) {
+  int side = 0;
+  const int64_t pi = psi_index(A, a, i, j, k, ny, nzp, &side);
+  if (pi < 0) return sbar;
+  float* lp = LP.p[a][slot][side] + pi;
+  const float pbar = *lp + sbar;
+  *lp = cb[q] * pbar;
+  return ck[q] * sbar + ca[q] * pbar;
+}
+
+__device__ __forceinline__ uint32_t mat_of(const YeeParams& P, int64_t id) {
+  return P.mat16 ? (uint32_t)P.mat16[id] : P.mat32[id];
+}
+
+// objective sources of step n on one flux plane: coef (4, nf, n1, n2, 2) per term (E_t1, E_t2,
+// H_t1, H_t2 colocated) the weights of (cos, sin) of the forward phase table row n
+__global__ void k_adj_src(YeeParams P, AdjFlux af, AdjState S, int n) {
+  const int o2 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int o1 = blockIdx.y * blockDim.y + threadIdx.y;
+  if (o1 >= af.n1 || o2 >= af.n2) return;
+  const int t1 = (af.axis == 0) ? 1 : 0;
+  const int t2 = (af.axis == 2) ? 1 : 2;
+  int c[3];
+  c[af.axis] = af.km; c[t1] = o1; c[t2] = o2;
+  const int64_t id = ((int64_t)c[0] * P.ny + c[1]) * P.nzp + c[2];
+  c[af.axis] = af.km - 1;
+  const int64_t idm = ((int64_t)c[0] * P.ny + c[1]) * P.nzp + c[2];
+  const int64_t plane = (int64_t)af.n1 * af.n2;
+  const int64_t p = (int64_t)o1 * af.n2 + o2;
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int f = 0; f < af.nf; ++f) {
+    const float* ph = af.phase + ((int64_t)n * af.nf + f) * 4;
+    for (int t = 0; t < 4; ++t) {
+      const double* w = af.coef + (((int64_t)t * af.nf + f) * plane + p) * 2;
+      const double co = t < 2 ? ph[0] : ph[2], si = t < 2 ? ph[1] : ph[3];
+      a[t] += co * w[0] + si * w[1];
+    }
+  }
+  S.lam[t1][id] += (float)a[0];
+  S.lam[t2][id] += (float)a[1];
+  S.lam[3 + t1][id] += (float)(0.5 * a[2]);
+  S.lam[3 + t1][idm] += (float)(0.5 * a[2]);
+  S.lam[3 + t2][id] += (float)(0.5 * a[3]);
+  S.lam[3 + t2][idm] += (float)(0.5 * a[3]);
+}
+
+// reverse E update, part 1: gradient terms, adjoint psi, the six d_bar, lambda_E <- ca lambda_E
+__global__ void __launch_bounds__(128) k_adj_e_a(YeeParams P, AdjState S, const float* en0,
+                                                 const float* en1_, const float* en2,
+                                                 const float* e10, const float* e11,
+                                                 const float* e12) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= P.nz || j >= P.ny) return;
+  const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + k;
+  const MatRec& M = P.mats[mat_of(P, id)];
+  const float* en[3] = {en0, en1_, en2};
+  const float* e1[3] = {e10, e11, e12};
+  // (axis a, psi slot) of the S_a and S_b terms of each component, d_bar index 2c and 2c+1
+  const int ax_a[3] = {1, 2, 0}, ax_b[3] = {2, 0, 1};
+  const int sl_a[3] = {0, 1, 1}, sl_b[3] = {0, 0, 1};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float lam = S.lam[c][id];
+    const float ca = M.ca[c], cb = M.cb[c];
+    if (lam != 0.f) {
+      const double e0 = en[c][id], e1v = e1[c][id];
+      S.gca[c][id] += (double)lam * e0;
+      if (cb != 0.f) S.gcb[c][id] += (double)lam * (e1v - (double)ca * e0) / (double)cb;
+    }
+    const float sa = cb * lam, sb = -cb * lam;
+    const int aa = ax_a[c], ab = ax_b[c];
+    const DevAxis& Aa = P.ax[aa];
+    const DevAxis& Ab = P.ax[ab];
+    const int qa = aa == 0 ? i : (aa == 1 ? j : k);
+    const int qb = ab == 0 ? i : (ab == 1 ? j : k);
+    S.dbar[2 * c][id] = dbar_of(sa, S.lpsie, aa, sl_a[c], Aa, Aa.ae, Aa.be, Aa.ke, qa, i, j, k,
+                                P.ny, P.nzp);
+    S.dbar[2 * c + 1][id] = dbar_of(sb, S.lpsie, ab, sl_b[c], Ab, Ab.ae, Ab.be, Ab.ke, qb, i,
+                                    j, k, P.ny, P.nzp);
+    S.lam[c][id] = ca * lam;
+  }
+}
+
+// index of cell (i, j, k) moved to q along axis a
+__device__ __forceinline__ int64_t moved(const YeeParams& P, int a, int i, int j, int k, int q) {
+  if (a == 0) i = q;
+  else if (a == 1) j = q;
+  else k = q;
+  return ((int64_t)i * P.ny + j) * P.nzp + k;
+}
+
+// The cells q' of an axis that can name q as a neighbour: q - 1, q, q + 1 and, on a periodic
+// axis, the wrap partner (prv / nxt of q); each listed once.
+__device__ __forceinline__ int neighbour_candidates(const DevAxis& A, int q, int* c) {
+  int n = 0;
+  const int raw[5] = {q - 1, q, q + 1, A.prv[q], A.nxt[q]};
+#pragma unroll
+  for (int t = 0; t < 5; ++t) {
+    const int v = raw[t];
+    if (v < 0 || v >= A.n) continue;
+    bool seen = false;
+    for (int u = 0; u < n; ++u) seen |= (c[u] == v);
+    if (!seen) c[n++] = v;
+  }
+  return n;
+}
+
+// transposed backward difference along axis a of term array db into lambda at (i, j, k):
+// own idl d_bar, minus m idl d_bar of every cell c' with prv(c') = this cell
+__device__ __forceinline__ float gather_bwd(const YeeParams& P, const float* db, int a, int i,
+                                            int j, int k) {
+  const DevAxis& A = P.ax[a];
+  const int q = a == 0 ? i : (a == 1 ? j : k);
+  float v = A.idl_d[q] * db[moved(P, a, i, j, k, q)];
+  int cand[5];
+  const int nc = neighbour_candidates(A, q, cand);
+  for (int t = 0; t < nc; ++t) {
+    const int qq = cand[t];
+    if (A.prv[qq] != q) continue;
+    v -= A.mpv[qq] * A.idl_d[qq] * db[moved(P, a, i, j, k, qq)];
+  }
+  return v;
+}
+
+// transposed forward difference along axis a: minus own idl d_bar, plus m idl d_bar of every
+// cell c' with nxt(c') = this cell
+__device__ __forceinline__ float gather_fwd(const YeeParams& P, const float* db, int a, int i,
+                                            int j, int k) {
+  const DevAxis& A = P.ax[a];
+  const int q = a == 0 ? i : (a == 1 ? j : k);
+  float v = -A.idl_p[q] * db[moved(P, a, i, j, k, q)];
+  int cand[5];
+  const int nc = neighbour_candidates(A, q, cand);
+  for (int t = 0; t < nc; ++t) {
+    const int qq = cand[t];
+    if (A.nxt[qq] != q) continue;
+    v += A.mnx[qq] * A.idl_p[qq] * db[moved(P, a, i, j, k, qq)];
+  }
+  return v;
+}
+
+// reverse E update, part 2: lambda_H gathers the transposed backward differences
+__global__ void __launch_bounds__(128) k_adj_e_b(YeeParams P, AdjState S) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= P.nz || j >= P.ny) return;
+  const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + k;
+  // Hz: Ex y-term (0), Ey x-term (3); Hy: Ex z-term (1), Ez x-term (4); Hx: Ey z-term (2),
+  // Ez y-term (5)
+  S.lam[5][id] += gather_bwd(P, S.dbar[0], 1, i, j, k) + gather_bwd(P, S.dbar[3], 0, i, j, k);
+  S.lam[4][id] += gather_bwd(P, S.dbar[1], 2, i, j, k) + gather_bwd(P, S.dbar[4], 0, i, j, k);
+  S.lam[3][id] += gather_bwd(P, S.dbar[2], 2, i, j, k) + gather_bwd(P, S.dbar[5], 1, i, j, k);
+}
+
+// reverse H update, part 1: adjoint psi and the six d_bar (lambda_H passes through)
+__global__ void __launch_bounds__(128) k_adj_h_a(YeeParams P, AdjState S) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= P.nz || j >= P.ny) return;
+  const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + k;
+  const int ax_a[3] = {1, 2, 0}, ax_b[3] = {2, 0, 1};
+  const int sl_a[3] = {0, 1, 1}, sl_b[3] = {0, 0, 1};
+#pragma unroll
+  for (int h = 0; h < 3; ++h) {
+    const float lam = S.lam[3 + h][id];
+    const float sa = -P.ch * lam, sb = P.ch * lam;
+    const int aa = ax_a[h], ab = ax_b[h];
+    const DevAxis& Aa = P.ax[aa];
+    const DevAxis& Ab = P.ax[ab];
+    const int qa = aa == 0 ? i : (aa == 1 ? j : k);
+    const int qb = ab == 0 ? i : (ab == 1 ? j : k);
+    S.dbar[2 * h][id] = dbar_of(sa, S.lpsih, aa, sl_a[h], Aa, Aa.ah, Aa.bh, Aa.kh, qa, i, j, k,
+                                P.ny, P.nzp);
+    S.dbar[2 * h + 1][id] = dbar_of(sb, S.lpsih, ab, sl_b[h], Ab, Ab.ah, Ab.bh, Ab.kh, qb, i,
+                                    j, k, P.ny, P.nzp);
+  }
+}
+
+// reverse H update, part 2: lambda_E gathers the transposed forward differences
+__global__ void __launch_bounds__(128) k_adj_h_b(YeeParams P, AdjState S) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= P.nz || j >= P.ny) return;
+  const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + k;
+  // Ez: Hx y-term (0), Hy x-term (3); Ey: Hx z-term (1), Hz x-term (4); Ex: Hy z-term (2),
+  // Hz y-term (5)
+  S.lam[2][id] += gather_fwd(P, S.dbar[0], 1, i, j, k) + gather_fwd(P, S.dbar[3], 0, i, j, k);
+  S.lam[1][id] += gather_fwd(P, S.dbar[1], 2, i, j, k) + gather_fwd(P, S.dbar[4], 0, i, j, k);
+  S.lam[0][id] += gather_fwd(P, S.dbar[2], 2, i, j, k) + gather_fwd(P, S.dbar[5], 1, i, j, k);
+}
+
+}  // namespace
+
+cudaError_t launch_adj_src(const YeeParams& P, const AdjFlux& a, const AdjState& S, int n,
+                           cudaStream_t s) {
+  dim3 b(32, 4, 1), g((a.n2 + 31) / 32, (a.n1 + 3) / 4, 1);
+  k_adj_src<<<g, b, 0, s>>>(P, a, S, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adj_e(const YeeParams& P, const AdjState& S, const float* const en[3],
+                         const float* const en1[3], cudaStream_t s) {
+  dim3 b(32, 4, 1), g((P.nzp + 31) / 32, (P.ny + 3) / 4, P.nx);
+  k_adj_e_a<<<g, b, 0, s>>>(P, S, en[0], en[1], en[2], en1[0], en1[1], en1[2]);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_adj_e_b<<<g, b, 0, s>>>(P, S);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adj_h(const YeeParams& P, const AdjState& S, cudaStream_t s) {
+  dim3 b(32, 4, 1), g((P.nzp + 31) / 32, (P.ny + 3) / 4, P.nx);
+  k_adj_h_a<<<g, b, 0, s>>>(P, S);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_adj_h_b<<<g, b, 0, s>>>(P, S);
+  return cudaGetLastError();
+}
+
+}  // namespace oem

@@ -236,7 +236,7 @@ static int check_device_error(oem_plan* p) {
 }
 
 // One time step (openem/solver.py:1145-1162).
-static int enqueue_step(oem_plan* p, cudaStream_t s) {
+static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
   const YeeParams& P = p->yp;
   cudaError_t e;
   // the pole pass depends on E^n only: it runs on a branch beside the H update and joins
@@ -280,16 +280,64 @@ static int enqueue_step(oem_plan* p, cudaStream_t s) {
   for (const Absorber& a : p->absorbers)
     if ((e = launch_absorb(P, a, 1, s)) != cudaSuccess) return cuda_error(e, "absorb_e");
   for (const TimeMon& m : p->tmons) {
+    if (!monitors) break;
     if ((e = launch_time_sample(P, m, p->d_step, 1, s)) != cudaSuccess)
       return cuda_error(e, "time_sample");
     if ((e = launch_time_sample(P, m, p->d_step, 0, s)) != cudaSuccess)
       return cuda_error(e, "time_sample");
   }
   for (const Monitor& m : p->mons) {
+    if (!monitors) break;
     if ((e = launch_snapshot(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "snapshot");
     if ((e = launch_flush(m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "flush");
   }
   if ((e = launch_step_advance(p->d_step, s)) != cudaSuccess) return cuda_error(e, "step");
+  return OEM_OK;
+}
+
+// ---- checkpoints: the six fields and every CPML psi array, copied device to device ----
+static void state_arrays(oem_plan* p, std::vector<std::pair<float*, size_t>>& v) {
+  const size_t ncp = (size_t)p->nx * p->ny * p->nzp;
+  for (int c = 0; c < 6; ++c) v.push_back({p->yp.f[c], ncp});
+  for (int a = 0; a < 3; ++a) {
+    const AxisHost& h = p->axh[a];
+    for (int side = 0; side < 2; ++side) {
+      const int L = side == 0 ? h.lo : h.hi;
+      if (L <= 0) continue;
+      size_t cnt = a == 0 ? (size_t)L * p->ny * p->nzp
+                          : (a == 1 ? (size_t)p->nx * L * p->nzp : (size_t)p->nx * p->ny * L);
+      for (int slot = 0; slot < 2; ++slot) {
+        v.push_back({p->yp.psih.p[a][slot][side], cnt});
+        v.push_back({p->yp.psie.p[a][slot][side], cnt});
+      }
+    }
+  }
+}
+
+static int save_state(oem_plan* p, int slot, cudaStream_t s) {
+  if (slot < 0 || slot >= (int)p->ckpt.size()) return OEM_OK;  // past the planned step count
+  std::vector<std::pair<float*, size_t>> v;
+  state_arrays(p, v);
+  float* dst = p->ckpt[slot];
+  for (auto& a : v) {
+    OEM_CUDA(cudaMemcpyAsync(dst, a.first, a.second * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    dst += a.second;
+  }
+  p->ckpt_step[slot] = p->steps;
+  return OEM_OK;
+}
+
+static int load_state(oem_plan* p, int slot, cudaStream_t s) {
+  std::vector<std::pair<float*, size_t>> v;
+  state_arrays(p, v);
+  const float* src = p->ckpt[slot];
+  for (auto& a : v) {
+    OEM_CUDA(cudaMemcpyAsync(a.first, src, a.second * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    src += a.second;
+  }
+  const int n = (int)p->ckpt_step[slot];
+  OEM_CUDA(cudaMemcpyAsync(p->d_step, &n, sizeof(int), cudaMemcpyHostToDevice, s));
+  OEM_CUDA(cudaStreamSynchronize(s));
   return OEM_OK;
 }
 
@@ -658,6 +706,150 @@ int oem_plan_set_xchunk(oem_plan* p, int xch) {
   return OEM_OK;
 }
 
+int oem_plan_enable_checkpoints(oem_plan* p, int k) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (k < 1) return set_error(OEM_ERR_INVALID, "checkpoint interval must be >= 1");
+  p->ckpt_k = k;
+  return OEM_OK;
+}
+
+int oem_plan_adjoint_flux(oem_plan* p, int mon_id, const double* weights, const double* dA1,
+                          const double* dA2, double* g_ca, double* g_cb, void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (p->ckpt_k < 1) return set_error(OEM_ERR_STATE, "checkpoints were not enabled");
+  if (p->steps != p->n_total) return set_error(OEM_ERR_STATE, "run the whole forward pass first");
+  if (mon_id < 0 || mon_id >= (int)p->mons.size() || p->mons[mon_id].kind != 0)
+    return set_error(OEM_ERR_INVALID, "not a flux monitor id");
+  if (p->mons[mon_id].n_total < p->n_total)
+    return set_error(OEM_ERR_INVALID, "the monitor's phase table is shorter than the run");
+  if (!weights || !dA1 || !dA2 || !g_ca || !g_cb) return set_error(OEM_ERR_INVALID, "null argument");
+  if (p->is_complex || p->yp.has_ade || !p->absorbers.empty())
+    return set_error(OEM_ERR_UNSUPPORTED,
+                     "the adjoint covers real, non-dispersive plans without absorbers");
+  for (int64_t q = 0; q < (int64_t)p->ckpt.size(); ++q)
+    if (p->ckpt_step[q] != q * p->ckpt_k) return set_error(OEM_ERR_STATE, "missing checkpoint");
+  if ((rc = use_device(p))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Monitor& m = p->mons[mon_id];
+  if ((rc = oem_plan_flush(p, stream))) return rc;
+  const int64_t plane = m.cells, nf = m.nf;
+  std::vector<double> re((size_t)4 * nf * plane), im(re.size());
+  OEM_CUDA(cudaMemcpy(re.data(), m.d_re, re.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  OEM_CUDA(cudaMemcpy(im.data(), m.d_im, im.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  // objective J = sum_f w_f 1/2 sum_p [Re(E1 H2*) dA1 - Re(E2 H1*) dA2] (transverse axes
+  // ascending): per term the weights of (cos, sin) of the phase table
+  std::vector<double> coef((size_t)4 * nf * plane * 2);
+  auto at = [&](int c, int64_t f, int64_t q) { return ((size_t)c * nf + f) * plane + q; };
+  for (int64_t f = 0; f < nf; ++f)
+    for (int o1 = 0; o1 < m.n1; ++o1)
+      for (int o2 = 0; o2 < m.n2; ++o2) {
+        const int64_t q = (int64_t)o1 * m.n2 + o2;
+        const double a1 = dA1[q], a2 = dA2[q];
+        const double w = 0.5 * weights[f];
+        const double e1r = re[at(0, f, q)], e1i = im[at(0, f, q)];
+        const double e2r = re[at(1, f, q)], e2i = im[at(1, f, q)];
+        const double h1r = re[at(2, f, q)], h1i = im[at(2, f, q)];
+        const double h2r = re[at(3, f, q)], h2i = im[at(3, f, q)];
+        const double v[4][2] = {{w * a1 * h2r, w * a1 * h2i}, {-w * a2 * h1r, -w * a2 * h1i},
+                                {-w * a2 * e2r, -w * a2 * e2i}, {w * a1 * e1r, w * a1 * e1i}};
+        for (int c = 0; c < 4; ++c) {
+          coef[2 * at(c, f, q)] = v[c][0];
+          coef[2 * at(c, f, q) + 1] = v[c][1];
+        }
+      }
+  // adjoint buffers for this call
+  std::vector<void*> tmp;
+  auto alloc = [&](auto** ptr, size_t count) -> int {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(**ptr));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(OEM_ERR_NOMEM, "adjoint buffers do not fit in device memory");
+    }
+    tmp.push_back(q);
+    OEM_CUDA(cudaMemsetAsync(q, 0, std::max<size_t>(count, 1) * sizeof(**ptr), s));
+    *ptr = static_cast<std::remove_reference_t<decltype(*ptr)>>(q);
+    return OEM_OK;
+  };
+  auto release = [&]() { cudaStreamSynchronize(s); for (void* q : tmp) cudaFree(q); };
+  const size_t ncp = (size_t)p->nx * p->ny * p->nzp;
+  const int K = p->ckpt_k;
+  AdjState S{};
+  AdjFlux af{};
+  double* dcoef = nullptr;
+  float* seg = nullptr;
+  rc = OEM_OK;
+  for (int c = 0; c < 6 && !rc; ++c) rc = alloc(&S.lam[c], ncp);
+  for (int c = 0; c < 6 && !rc; ++c) rc = alloc(&S.dbar[c], ncp);
+  for (int c = 0; c < 3 && !rc; ++c) rc = alloc(&S.gca[c], ncp);
+  for (int c = 0; c < 3 && !rc; ++c) rc = alloc(&S.gcb[c], ncp);
+  for (int a = 0; a < 3 && !rc; ++a)
+    for (int side = 0; side < 2 && !rc; ++side) {
+      const int L = side == 0 ? p->axh[a].lo : p->axh[a].hi;
+      if (L <= 0) continue;
+      size_t cnt = a == 0 ? (size_t)L * p->ny * p->nzp
+                          : (a == 1 ? (size_t)p->nx * L * p->nzp : (size_t)p->nx * p->ny * L);
+      for (int slot = 0; slot < 2 && !rc; ++slot) {
+        rc = alloc(&S.lpsih.p[a][slot][side], cnt);
+        if (!rc) rc = alloc(&S.lpsie.p[a][slot][side], cnt);
+      }
+    }
+  if (!rc) rc = alloc(&dcoef, coef.size());
+  if (!rc) rc = alloc(&seg, (size_t)(K + 1) * 3 * ncp);
+  if (rc) {
+    release();
+    return rc;
+  }
+  OEM_CUDA(cudaMemcpyAsync(dcoef, coef.data(), coef.size() * sizeof(double),
+                           cudaMemcpyHostToDevice, s));
+  af.axis = m.axis; af.km = m.km; af.n1 = m.n1; af.n2 = m.n2; af.nf = (int)nf;
+  af.phase = m.d_phase;
+  af.coef = dcoef;
+  const int64_t N = p->n_total;
+  const int64_t nseg = (N + K - 1) / K;
+  const YeeParams& P = p->yp;
+  cudaError_t e = cudaSuccess;
+  for (int64_t sg = nseg - 1; sg >= 0 && !rc; --sg) {
+    const int64_t n0 = sg * K, n1 = std::min<int64_t>(N, n0 + K);
+    // recompute the segment from its checkpoint, keeping E at every step
+    if ((rc = load_state(p, (int)sg, s))) break;
+    for (int64_t t = 0; t <= n1 - n0 && !rc; ++t) {
+      if (t > 0) rc = enqueue_step(p, s, false);
+      for (int c = 0; c < 3 && !rc; ++c)
+        if ((e = cudaMemcpyAsync(seg + ((size_t)t * 3 + c) * ncp, P.f[c], ncp * sizeof(float),
+                                 cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+          rc = cuda_error(e, "segment copy");
+    }
+    for (int64_t n = n1 - 1; n >= n0 && !rc; --n) {
+      const float* en[3];
+      const float* en1[3];
+      for (int c = 0; c < 3; ++c) {
+        en[c] = seg + ((size_t)(n - n0) * 3 + c) * ncp;
+        en1[c] = seg + ((size_t)(n - n0 + 1) * 3 + c) * ncp;
+      }
+      if ((e = launch_adj_src(P, af, S, (int)n, s)) != cudaSuccess) rc = cuda_error(e, "adj_src");
+      if (!rc && (e = launch_adj_e(P, S, en, en1, s)) != cudaSuccess) rc = cuda_error(e, "adj_e");
+      if (!rc && (e = launch_adj_h(P, S, s)) != cudaSuccess) rc = cuda_error(e, "adj_h");
+    }
+  }
+  if (!rc) {
+    for (int c = 0; c < 3 && !rc; ++c) {
+      const size_t plane_bytes = (size_t)p->nz * sizeof(double);
+      if ((e = cudaMemcpy2DAsync(g_ca + (size_t)c * p->nx * p->ny * p->nz, plane_bytes, S.gca[c],
+                                 (size_t)p->nzp * sizeof(double), plane_bytes,
+                                 (size_t)p->nx * p->ny, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+          (e = cudaMemcpy2DAsync(g_cb + (size_t)c * p->nx * p->ny * p->nz, plane_bytes, S.gcb[c],
+                                 (size_t)p->nzp * sizeof(double), plane_bytes,
+                                 (size_t)p->nx * p->ny, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        rc = cuda_error(e, "gradient readout");
+    }
+  }
+  release();
+  return rc;
+}
+
 int oem_plan_add_absorber(oem_plan* p, int axis, int g0, int nlay, const double* decay_int,
                           const double* decay_half) {
   int rc = check_plan(p, false);
@@ -843,6 +1035,17 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   for (int a = 0; a < 3; ++a)
     if ((rc = upload_axis(p, a))) return rc;
   if ((rc = alloc_psi(p))) return rc;
+  if (p->ckpt_k > 0) {
+    std::vector<std::pair<float*, size_t>> v;
+    state_arrays(p, v);
+    p->ckpt_floats = 0;
+    for (auto& a : v) p->ckpt_floats += a.second;
+    const int64_t nslot = (n_total + p->ckpt_k - 1) / p->ckpt_k;
+    p->ckpt.assign((size_t)std::max<int64_t>(nslot, 1), nullptr);
+    p->ckpt_step.assign(p->ckpt.size(), -1);
+    for (float*& b : p->ckpt)
+      if ((rc = dalloc(p, &b, p->ckpt_floats, false))) return rc;
+  }
   // materials: table with the padding material at 0, padded index shifted by one
   MatRec* dm;
   if ((rc = dupload(p, &dm, p->mats.data(), p->mats.size()))) return rc;
@@ -978,6 +1181,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
   if ((rc = use_device(p))) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int64_t left = nsteps;
+  if (p->timing && p->ckpt_k > 0)
+    return set_error(OEM_ERR_STATE, "timing mode does not save adjoint checkpoints");
   if (p->timing) {
     // Direct launches with CUDA events around the two update kernels; events come from a pool
     // sized for this call and are read once at the end, so the stream never waits on the host.
@@ -1059,15 +1264,26 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
     p->steps += n;
     return OEM_OK;
   }
-  while (left >= p->graph_steps && p->graph_steps > 1) {
-    OEM_CUDA(cudaGraphLaunch(p->graph_many, s));
-    left -= p->graph_steps;
-  }
   while (left > 0) {
-    OEM_CUDA(cudaGraphLaunch(p->graph_one, s));
-    --left;
+    // with checkpoints, every K-step segment starts from a saved state
+    int64_t chunk = left;
+    if (p->ckpt_k > 0) {
+      if (p->steps % p->ckpt_k == 0 && (rc = save_state(p, (int)(p->steps / p->ckpt_k), s)))
+        return rc;
+      chunk = std::min<int64_t>(left, p->ckpt_k - p->steps % p->ckpt_k);
+    }
+    int64_t c = chunk;
+    while (c >= p->graph_steps && p->graph_steps > 1) {
+      OEM_CUDA(cudaGraphLaunch(p->graph_many, s));
+      c -= p->graph_steps;
+    }
+    while (c > 0) {
+      OEM_CUDA(cudaGraphLaunch(p->graph_one, s));
+      --c;
+    }
+    p->steps += chunk;
+    left -= chunk;
   }
-  p->steps += nsteps;
   return OEM_OK;
 }
 

@@ -212,6 +212,11 @@ struct oem_plan {
   std::vector<oem::DipoleSet> dipoles;
   std::vector<oem::ModeSrc> modesrcs;
   std::vector<oem::Absorber> absorbers;
+  // checkpoints of the state every ckpt_k steps (discrete adjoint): fields and CPML psi
+  int ckpt_k = 0;
+  std::vector<float*> ckpt;        // one buffer per checkpoint, ckpt_floats floats each
+  size_t ckpt_floats = 0;
+  std::vector<int64_t> ckpt_step;  // step held by each buffer (-1: empty)
   bool is_complex = false;  // Bloch / forced complex fields
   std::vector<oem::Monitor> mons;
   std::vector<oem::TimeMon> tmons;
@@ -321,6 +326,26 @@ cudaError_t launch_ade_segments(const YeeParams& P, const int64_t* segs, int64_t
 cudaError_t launch_update_h_c(const YeeParams& P, cudaStream_t s);
 cudaError_t launch_update_e_c(const YeeParams& P, cudaStream_t s);
 cudaError_t launch_absorb(const YeeParams& P, const Absorber& a, int is_e, cudaStream_t s);
+
+// Discrete adjoint (oem_adjoint.cu): adjoint fields, their CPML psi, scratch for the transposed
+// differences, and the gradient accumulators of ca and cb per component.
+struct AdjState {
+  float* lam[6];      // adjoint of Ex Ey Ez Hx Hy Hz (padded)
+  PsiSet lpsih, lpsie;  // adjoint psi
+  float* dbar[6];     // per-cell adjoint of the six differences of one half step
+  double* gca[3];     // sum over steps of lambda_E^{n+1} E^n
+  double* gcb[3];     // sum over steps of lambda_E^{n+1} T^n, T^n = (E^{n+1} - ca E^n) / cb
+};
+struct AdjFlux {      // objective sources of one flux plane (see oem_adjoint.cu)
+  int axis, km, n1, n2, nf;
+  const float* phase;   // (n_total, nf, 4) forward phase table
+  const double* coef;   // (4, nf, n1, n2, 2): per term and frequency the (cos, sin) weights
+};
+cudaError_t launch_adj_src(const YeeParams& P, const AdjFlux& a, const AdjState& S, int n,
+                           cudaStream_t s);
+cudaError_t launch_adj_e(const YeeParams& P, const AdjState& S, const float* const en[3],
+                         const float* const en1[3], cudaStream_t s);
+cudaError_t launch_adj_h(const YeeParams& P, const AdjState& S, cudaStream_t s);
 cudaError_t launch_mode_h(const YeeParams& P, const ModeSrc& m, const int* step, cudaStream_t s);
 cudaError_t launch_mode_e(const YeeParams& P, const ModeSrc& m, const int* step, cudaStream_t s);
 cudaError_t launch_energy(const YeeParams& P, double* const dl[3][2], double* part, int nblocks,

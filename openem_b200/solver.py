@@ -81,9 +81,11 @@ class Plan:
     """One simulation resident on the device: owns a ``oem_plan``."""
 
     def __init__(self, sc, n_total: int | None = None, device: int = 0, stream=None,
-                 batch: int | None = None, cplx: bool = False, xchunk: int = 0):
+                 batch: int | None = None, cplx: bool = False, xchunk: int = 0,
+                 checkpoint_every: int = 0):
         self.cplx = bool(cplx)
         self.xchunk = int(xchunk)
+        self.checkpoint_every = int(checkpoint_every)
         if self.cplx:
             refuse_unsupported_bloch(sc)
         else:
@@ -240,6 +242,8 @@ class Plan:
             self.time_mons.append((m, mid.value, (int(comps.size), int(m.num_slots), ni, nj, nk)))
         if self.xchunk:
             L.check(lib.oem_plan_set_xchunk(h, self.xchunk), "set_xchunk")
+        if self.checkpoint_every:
+            L.check(lib.oem_plan_enable_checkpoints(h, self.checkpoint_every), "checkpoints")
         L.check(lib.oem_plan_finalize(h, self.n_total), "finalize")
         self._keep.clear()
 
@@ -266,6 +270,19 @@ class Plan:
         L.check(self.lib.oem_plan_read_monitor(self.h, int(mid), L.ptr(re), L.ptr(im), self._s),
                 "read_monitor")
         return re + 1j * im
+
+    def adjoint_flux(self, mid: int, weights, dA1, dA2):
+        """dJ/dca and dJ/dcb, (3, nx, ny, nz) float64 each, of ``J = sum_f weights[f] P_f``
+        for the flux monitor ``mid`` (face elements ``dA1``, ``dA2`` of its two terms)."""
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        a1 = np.ascontiguousarray(dA1, dtype=np.float64)
+        a2 = np.ascontiguousarray(dA2, dtype=np.float64)
+        g_ca = np.empty((3,) + self.shape, np.float64)
+        g_cb = np.empty((3,) + self.shape, np.float64)
+        L.check(self.lib.oem_plan_adjoint_flux(self.h, int(mid), L.ptr(w), L.ptr(a1), L.ptr(a2),
+                                               L.ptr(g_ca), L.ptr(g_cb), self._s),
+                "adjoint_flux")
+        return g_ca, g_cb
 
     def read_time_monitor(self, mid: int, shape) -> np.ndarray:
         out = np.empty(shape, np.float32)

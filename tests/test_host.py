@@ -151,6 +151,52 @@ def test_bloch_subset_fails_closed(feature):
     solver.refuse_unsupported_bloch(plain)
 
 
+@pytest.mark.parametrize("feature", ["dispersion", "absorber", "bloch"])
+def test_adjoint_fails_closed(feature):
+    """The discrete adjoint covers real, non-dispersive scenes without absorbers; the rest is
+    refused before anything reaches the device."""
+    from openem_b200 import adjoint
+    sd = scenes.small_dispersive(n=20, n_sph=1, n_pml=4, num_steps=10)
+    plain = replace(sd, dispersion=None)
+    bad = {
+        "dispersion": sd,
+        "absorber": replace(plain, absorbers=scenes.absorber_slabs(plain.grid, 0, 3)),
+        "bloch": replace(plain, bloch_k=(0.1, 0.0, 0.0)),
+    }[feature]
+    with pytest.raises(NotImplementedError):
+        adjoint._refuse(bad)
+    adjoint._refuse(plain)
+
+
+def test_adjoint_coefficient_jacobian_matches_differences():
+    """d(ca, cb)/d(eps, sigma) of the float64 coefficient formula against central
+    differences."""
+    from openem_b200 import adjoint
+    sd = scenes.small_dispersive(n=12, n_sph=1, n_pml=3, num_steps=10)
+    sc = replace(sd, dispersion=None)
+    jac = adjoint.coefficient_jacobian(sc)
+    eps0 = T.EPSILON_0
+    c, cell = 1, (5, 6, 7)
+    e = float(np.asarray(sc.eps_ey)[cell])
+    sg = 0.0 if sc.sigma_ey is None else float(np.asarray(sc.sigma_ey)[cell])
+    G = float(T._g_dense(sc, sc.shape)[c][cell])
+
+    def coef(ev, sv):
+        s = sv * sc.dt / (2 * eps0)
+        den = ev + s + G
+        return (ev - s) / den, (sc.dt / eps0) / den
+    h = 1e-6
+    ca_p, cb_p = coef(e + h, sg)
+    ca_m, cb_m = coef(e - h, sg)
+    np.testing.assert_allclose(jac[c][0][cell], (ca_p - ca_m) / (2 * h), rtol=1e-6, atol=1e-12)
+    np.testing.assert_allclose(jac[c][1][cell], (cb_p - cb_m) / (2 * h), rtol=1e-6)
+    hs = 1e-3
+    ca_p, cb_p = coef(e, sg + hs)
+    ca_m, cb_m = coef(e, sg - hs)
+    np.testing.assert_allclose(jac[c][2][cell], (ca_p - ca_m) / (2 * hs), rtol=1e-6)
+    np.testing.assert_allclose(jac[c][3][cell], (cb_p - cb_m) / (2 * hs), rtol=1e-6)
+
+
 def test_dipole_table_refuses_short_waveform():
     sc = scenes.small_dispersive(n=20, n_sph=1, n_pml=4, num_steps=30)
     with pytest.raises(ValueError):
