@@ -138,6 +138,18 @@ int oem_plan_enable_checkpoints(oem_plan* p, int k);
 int oem_plan_adjoint_flux(oem_plan* p, int mon_id, const double* weights, const double* dA1,
                           const double* dA2, double* g_ca, double* g_cb, void* stream);
 
+/* Time-modulated permittivity (openem/kernels/modulation.cu:40-79,
+ * openem/sources_setup.py:460-518, 640-650): eps(t) = eps_s + amp cos(omega t - phi) on n_entry
+ * (comp, cell) entries, cell = (i ny + j) nz + k, each (comp, cell) at most once. Every step the
+ * D-form coefficients ca = (eps(t_n) - sd) / (eps(t_n+1) + sd + gg), cb = dte / (same) replace
+ * the cell's update coefficients before the E update; cph / sph are cos / sin of phi, cs_tab holds
+ * ntab >= n_total rows (cos w t_n, sin w t_n, cos w t_n+1, sin w t_n+1), dte = dt / eps0. Each
+ * modulated cell must own its material record (no other cell may use its material index). */
+int oem_plan_add_modulation(oem_plan* p, int n_entry, const int* comp, const int64_t* cell,
+                            const float* amp, const float* cph, const float* sph,
+                            const float* eps_s, const float* sd, const float* gg, int ntab,
+                            const float* cs_tab, double dte);
+
 /* Absorber boundary slab (Tidy3D's Absorber; replaces absorb_slab / absorb_batch,
  * openem/kernels/absorber.cu:20-70, absorb_batch.cu:15-110, and the host tables of
  * openem/dispersion_setup.py:89-120): layers [g0, g0 + nlay) along `axis`. After the H-side

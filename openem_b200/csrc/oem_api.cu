@@ -8,6 +8,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <map>
 #include <string>
 #include <utility>
@@ -242,6 +243,8 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
   // the pole pass depends on E^n only: it runs on a branch beside the H update and joins
   // before the E update
   const bool fork = p->side_stream != nullptr;
+  for (const Modulation& m : p->mods)
+    if ((e = launch_modulate(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "modulate");
   if (fork) {
     OEM_CUDA(cudaEventRecord(p->ev_fork, s));
     OEM_CUDA(cudaStreamWaitEvent(p->side_stream, p->ev_fork, 0));
@@ -872,6 +875,51 @@ int oem_plan_add_absorber(oem_plan* p, int axis, int g0, int nlay, const double*
   return OEM_OK;
 }
 
+int oem_plan_add_modulation(oem_plan* p, int n_entry, const int* comp, const int64_t* cell,
+                            const float* amp, const float* cph, const float* sph,
+                            const float* eps_s, const float* sd, const float* gg, int ntab,
+                            const float* cs_tab, double dte) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (n_entry < 1 || ntab < 1) return set_error(OEM_ERR_INVALID, "empty modulation");
+  if (!comp || !cell || !amp || !cph || !sph || !eps_s || !sd || !gg || !cs_tab)
+    return set_error(OEM_ERR_INVALID, "null modulation table");
+  if (p->is_complex) return set_error(OEM_ERR_UNSUPPORTED, "time modulation on a complex plan");
+  const int64_t ncell = (int64_t)p->nx * p->ny * p->nz;
+  std::vector<uint8_t> seen((size_t)3 * ncell, 0);
+  for (int e = 0; e < n_entry; ++e) {
+    if (comp[e] < 0 || comp[e] > 2 || cell[e] < 0 || cell[e] >= ncell)
+      return set_error(OEM_ERR_INVALID, "modulation entry outside the grid");
+    uint8_t& f = seen[(size_t)comp[e] * ncell + cell[e]];
+    if (f) return set_error(OEM_ERR_INVALID, "duplicate (comp, cell) modulation entry");
+    f = 1;
+    if (!(eps_s[e] - std::fabs(amp[e]) > 0.f))
+      return set_error(OEM_ERR_INVALID, "eps_s - |amp| must stay positive");
+  }
+  if ((rc = use_device(p))) return rc;
+  Modulation m;
+  m.n = n_entry;
+  m.ntab = ntab;
+  m.dte = (float)dte;
+  std::vector<int64_t> padded(n_entry);
+  for (int e = 0; e < n_entry; ++e) {
+    const int64_t r = cell[e] / p->nz, k = cell[e] % p->nz;
+    padded[e] = r * p->nzp + k;
+  }
+  if ((rc = dupload(p, &m.comp, comp, n_entry))) return rc;
+  if ((rc = dupload(p, &m.cell, padded.data(), n_entry))) return rc;
+  if ((rc = dupload(p, &m.amp, amp, n_entry))) return rc;
+  if ((rc = dupload(p, &m.cph, cph, n_entry))) return rc;
+  if ((rc = dupload(p, &m.sph, sph, n_entry))) return rc;
+  if ((rc = dupload(p, &m.eps, eps_s, n_entry))) return rc;
+  if ((rc = dupload(p, &m.sd, sd, n_entry))) return rc;
+  if ((rc = dupload(p, &m.gg, gg, n_entry))) return rc;
+  if ((rc = dupload(p, &m.cs, reinterpret_cast<const float4*>(cs_tab), (size_t)ntab))) return rc;
+  p->mods.push_back(m);
+  p->mod_cells.emplace_back(cell, cell + n_entry);
+  return OEM_OK;
+}
+
 int oem_plan_set_axis_phase(oem_plan* p, int axis, const double* mnx_im, const double* mpv_im) {
   int rc = check_plan(p, false);
   if (rc) return rc;
@@ -1017,6 +1065,30 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
     return set_error(OEM_ERR_UNSUPPORTED, "dispersive media on a complex (Bloch) plan");
   for (const Monitor& m : p->mons)
     if (m.n_total < n_total) return set_error(OEM_ERR_INVALID, "phase table shorter than the run");
+  for (const Modulation& m : p->mods)
+    if (m.ntab < n_total) return set_error(OEM_ERR_INVALID, "modulation table shorter than the run");
+  if (!p->mods.empty() && !p->dev_index) {
+    // every modulated cell owns its material record: the kernel rewrites it in place
+    std::vector<int64_t> owner(p->mats.size(), -1);
+    auto idx_of = [&](int64_t c) -> int64_t {
+      return p->index_bytes == 2 ? reinterpret_cast<const uint16_t*>(p->mat_index.data())[c]
+                                 : reinterpret_cast<const uint32_t*>(p->mat_index.data())[c];
+    };
+    for (const auto& cells : p->mod_cells)
+      for (int64_t c : cells) {
+        int64_t& o = owner[(size_t)idx_of(c) + 1];
+        if (o >= 0 && o != c)
+          return set_error(OEM_ERR_INVALID, "two modulated cells share a material record");
+        o = c;
+      }
+    const int64_t ncell = (int64_t)p->nx * p->ny * p->nz;
+    for (int64_t c = 0; c < ncell; ++c) {
+      const int64_t o = owner[(size_t)idx_of(c) + 1];
+      if (o >= 0 && o != c)
+        return set_error(OEM_ERR_INVALID, "a modulated cell shares its material record");
+    }
+  }
+  p->mod_cells.clear();
   if ((rc = use_device(p))) return rc;
   p->n_total = n_total;
   YeeParams& P = p->yp;
@@ -1050,6 +1122,7 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   MatRec* dm;
   if ((rc = dupload(p, &dm, p->mats.data(), p->mats.size()))) return rc;
   P.mats = dm;
+  for (Modulation& m : p->mods) m.mats = dm;
   const bool wide = p->index_bytes == 4 || p->mats.size() > 65535;
   if (p->dev_index) {
     P.mat16 = p->dev_mat16;
@@ -1191,8 +1264,12 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
     for (auto& evq : ev) OEM_CUDA(cudaEventCreate(&evq));
     for (int64_t q = 0; q < n; ++q) {
       cudaEvent_t* E = &ev[(size_t)q * 6];
+      cudaError_t e;
+      for (const Modulation& m : p->mods)
+        if ((e = launch_modulate(p->yp, m, p->d_step, s)) != cudaSuccess)
+          return cuda_error(e, "modulate");
       OEM_CUDA(cudaEventRecord(E[0], s));
-      cudaError_t e = run_h(p, s);
+      e = run_h(p, s);
       if (e != cudaSuccess) return cuda_error(e, "update_h");
       OEM_CUDA(cudaEventRecord(E[1], s));
       for (const DipoleSet& d : p->dipoles)
@@ -1308,6 +1385,7 @@ int oem_plan_launches_per_step(oem_plan* p, int* n) {
   c += 2 * (int)p->planes.size();
   c += 2 * (int)p->modesrcs.size();
   c += 2 * (int)p->absorbers.size();
+  c += (int)p->mods.size();
   for (const DipoleSet& d : p->dipoles) c += d.n_targets > 0 ? 1 : 0;
   c += 2 * (int)p->tmons.size();
   c += 3 * (int)p->mons.size();  // snapshot, flush, flush mark

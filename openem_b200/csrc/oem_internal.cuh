@@ -164,6 +164,25 @@ struct Absorber {
   float* d_half = nullptr;
 };
 
+// Time-modulated permittivity eps(t) = eps_s + amp cos(omega t - phi) on (comp, cell) entries:
+// every step the D-form coefficients ca = (eps(t_n) - s) / (eps(t_n+1) + s + G),
+// cb = (dt / eps0) / (eps(t_n+1) + s + G) are written into the cell's own material record (each
+// modulated cell owns one). cs holds (cos w t_n, sin w t_n, cos w t_n+1, sin w t_n+1) per step.
+struct Modulation {
+  int n = 0, ntab = 0;
+  float dte = 0.f;
+  int* comp = nullptr;
+  int64_t* cell = nullptr;  // padded index
+  float* amp = nullptr;
+  float* cph = nullptr;
+  float* sph = nullptr;
+  float* eps = nullptr;
+  float* sd = nullptr;
+  float* gg = nullptr;
+  float4* cs = nullptr;
+  MatRec* mats = nullptr;   // the plan's records (writable), set at finalize
+};
+
 struct TimeMon {
   int nc = 0;
   int comps[6] = {0, 0, 0, 0, 0, 0};
@@ -212,6 +231,8 @@ struct oem_plan {
   std::vector<oem::DipoleSet> dipoles;
   std::vector<oem::ModeSrc> modesrcs;
   std::vector<oem::Absorber> absorbers;
+  std::vector<oem::Modulation> mods;
+  std::vector<std::vector<int64_t>> mod_cells;  // unpadded cells of each, kept until finalize
   // checkpoints of the state every ckpt_k steps (discrete adjoint): fields and CPML psi
   int ckpt_k = 0;
   std::vector<float*> ckpt;        // one buffer per checkpoint, ckpt_floats floats each
@@ -326,6 +347,8 @@ cudaError_t launch_ade_segments(const YeeParams& P, const int64_t* segs, int64_t
 cudaError_t launch_update_h_c(const YeeParams& P, cudaStream_t s);
 cudaError_t launch_update_e_c(const YeeParams& P, cudaStream_t s);
 cudaError_t launch_absorb(const YeeParams& P, const Absorber& a, int is_e, cudaStream_t s);
+cudaError_t launch_modulate(const YeeParams& P, const Modulation& m, const int* step,
+                            cudaStream_t s);
 
 // Discrete adjoint (oem_adjoint.cu): adjoint fields, their CPML psi, scratch for the transposed
 // differences, and the gradient accumulators of ca and cb per component.

@@ -606,6 +606,33 @@ cudaError_t launch_absorb(const YeeParams& P, const Absorber& a, int is_e, cudaS
   return cudaGetLastError();
 }
 
+// Time-modulated coefficients of step n (openem/kernels/modulation.cu:40-79): eps at t_n and
+// t_n+1 from the per-entry phase (cos phi, sin phi) and the step's (cos, sin) of omega t, the
+// D-form ca / cb written into the cell's own material record before the E update reads it.
+__global__ void k_modulate(YeeParams P, Modulation m, const int* step) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = *step;
+  if (e >= m.n || n < 0 || n >= m.ntab) return;
+  const float4 cs = m.cs[n];
+  const float a = m.amp[e], cp = m.cph[e], sp = m.sph[e], es = m.eps[e];
+  const float e0 = __fadd_rn(es, __fmul_rn(a, __fadd_rn(__fmul_rn(cs.x, cp), __fmul_rn(cs.y, sp))));
+  const float e1 = __fadd_rn(es, __fmul_rn(a, __fadd_rn(__fmul_rn(cs.z, cp), __fmul_rn(cs.w, sp))));
+  const float sd = m.sd[e];
+  const float den = __fadd_rn(__fadd_rn(e1, sd), m.gg[e]);
+  const int64_t id = m.cell[e];
+  MatRec& M = m.mats[mat_id(P, id)];
+  const int c = m.comp[e];
+  M.ca[c] = __fdiv_rn(__fsub_rn(e0, sd), den);
+  M.cb[c] = __fdiv_rn(m.dte, den);
+}
+
+cudaError_t launch_modulate(const YeeParams& P, const Modulation& m, const int* step,
+                            cudaStream_t s) {
+  if (m.n <= 0) return cudaSuccess;
+  k_modulate<<<(m.n + 127) / 128, 128, 0, s>>>(P, m, step);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* step,
                             cudaStream_t s) {
   if (m.kind == 0) {

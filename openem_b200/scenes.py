@@ -20,8 +20,8 @@ import numpy as np
 
 from openem_b200.model import (
     C_0, EPSILON_0, ETA_0, Axis, Dispersion, FieldMonitor, FieldTimeMonitor, FluxMonitor,
-    GaussianPulse, Grid, ModeSource, PlaneWaveSource, PMLParams, PointDipole, Scene, pml_build,
-    sample_waveform)
+    GaussianPulse, Grid, ModeSource, PlaneWaveSource, PMLParams, PointDipole, Scene,
+    TimeModulation, pml_build, sample_waveform)
 
 UM = 1e-6
 
@@ -205,6 +205,55 @@ def slab_plane_wave(nxy: int = 30, dl: float = 0.02 * UM, lz: float = 3.0 * UM,
     return Scene(grid=grid, dt=dt, num_time_steps=n_steps, shutoff=1e-5,
                  eps_ex=eps[0], eps_ey=eps[1], eps_ez=eps[2], pml=pml_dict(grid, dt, n_pml),
                  sources=[src], flux_monitors=mons)
+
+
+def modulated_slab(eps_s: float = 1.0, delta: float = 0.01, fm_rel: float = 0.1,
+                   phase=0.0, nxy: int = 1, dl: float = 0.025 * UM, lz: float = 4.0 * UM,
+                   d_slab: float = 1.0 * UM, freq0: float = C_0 / (1.0 * UM),
+                   fwidth_rel: float = 0.02, freqs=None, num_steps: int | None = None,
+                   run_time: float | None = None) -> Scene:
+    """A periodic-x/y cell with CPML on +-z, a +z Ex plane wave at z = -lz/2 + 0.4 um and a flux
+    plane "T" at z = +lz/2 - 0.4 um, and a 1 um slab at z = 0 whose permittivity is
+    ``eps_s + delta cos(2 pi fm t - phase)`` at every Yee point inside the slab, both faces
+    included (so eps(t) >= eps_s - delta everywhere: below 1 the Courant step of the vacuum
+    grid would be unstable). ``phase`` is a
+    scalar or a function of the Yee point's (x, y, z). Monitor frequencies default to
+    (f0 - fm, f0, f0 + fm)."""
+    fm = fm_rel * freq0
+    fwidth = fwidth_rel * freq0
+    rt = run_time if run_time is not None else 10.0 / fwidth
+    base = slab_plane_wave(nxy=nxy, dl=dl, lz=lz, eps_slab=eps_s, d_slab=d_slab,
+                           src_z=-0.5 * lz + 0.4 * UM, mon_t=0.5 * lz - 0.4 * UM,
+                           mon_r=-0.5 * lz + 0.2 * UM, freq0=freq0, nfreq=3, run_time=rt,
+                           with_slab=eps_s != 1.0, num_steps=num_steps, fwidth_rel=fwidth_rel)
+    f = np.asarray(freqs if freqs is not None else (freq0 - fm, freq0, freq0 + fm), np.float64)
+    pulse = GaussianPulse(freq0=freq0, fwidth=fwidth)
+    spec = spectrum(pulse, base.dt, base.num_time_steps, f)
+    mons = [FluxMonitor(name=m.name, axis=2, plane_index=m.plane_index, normal_dir=1, freqs=f,
+                        source_spectrum=spec) for m in base.flux_monitors]
+    grid = base.grid
+    nx, ny, nz = grid.shape
+    coords = yee_coords(grid)
+    comp, cell, ph = [], [], []
+    eps = [np.array(e, dtype=np.float64) for e in (base.eps_ex, base.eps_ey, base.eps_ez)]
+    for c in range(3):
+        x, y, z = coords[c]
+        kk = np.flatnonzero(np.abs(z) <= 0.5 * d_slab + 1e-6 * dl)
+        eps[c][:, :, kk] = eps_s
+        I, J, K = np.meshgrid(np.arange(nx), np.arange(ny), kk, indexing="ij")
+        comp.append(np.full(I.size, c))
+        cell.append(((I * ny + J) * nz + K).ravel())
+        if callable(phase):
+            ph.append(np.asarray(phase(x[I.ravel()], y[J.ravel()], z[K.ravel()]), np.float64))
+        else:
+            ph.append(np.full(I.size, float(phase)))
+    comp = np.concatenate(comp).astype(np.int32)
+    cell = np.concatenate(cell).astype(np.int64)
+    mod = TimeModulation(freq=fm, comp=comp, cell=cell, amp=np.full(comp.size, float(delta)),
+                         phase=np.concatenate(ph))
+    from dataclasses import replace
+    return replace(base, flux_monitors=mons, modulation=mod, eps_ex=eps[0], eps_ey=eps[1],
+                   eps_ez=eps[2])
 
 
 def slab_transmission(res_slab, res_empty, name: str = "T") -> np.ndarray:

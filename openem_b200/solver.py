@@ -36,7 +36,9 @@ def refuse_unsupported(sc) -> None:
         (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry > 0,
          "slanted-interface mixed dispersion"),
         (sc.tensor is not None and sc.tensor.n_entry > 0, "fully anisotropic media"),
-        (sc.modulation is not None and sc.modulation.n_entry > 0, "time-modulated media"),
+        (sc.modulation is not None and sc.modulation.n_entry > 0
+         and (sc.pec_ex is not None or sc.tensor is not None or sc.dispersion_mix is not None),
+         "time-modulated media together with PEC, tensor or mixed media"),
         (any(k != 0.0 for k in sc.bloch_k), "Bloch boundaries"),
     ]
     for bad, what in checks:
@@ -145,9 +147,12 @@ class Plan:
                 L.check(lib.oem_plan_set_axis_phase(
                     h, a, L.ptr(self._arr(np.imag(t.mnx), np.float64)),
                     L.ptr(self._arr(np.imag(t.mpv), np.float64))), f"set_axis_phase {a}")
+        mod = None if self.cplx else T.modulation_tables(sc, self.tabs, self.n_total)
         if self._device_tables():
             from openem_b200 import tables_gpu
             mt = tables_gpu.material_tables_device(sc, self.tabs, self.device)
+            if mod is not None:
+                tables_gpu.isolate_cells_device(mt, mod["cell"])
             self.h2d_bytes += sum(np.asarray(a).nbytes for a in
                                   (sc.eps_ex, sc.eps_ey, sc.eps_ez))
             self.h2d_bytes += sum(np.asarray(a).nbytes for a in
@@ -163,16 +168,27 @@ class Plan:
             del mt
         else:
             mt = T.material_tables(sc, self.tabs)
-            L.check(lib.oem_plan_set_materials(h, int(mt.n_mat),
-                                               L.ptr(self._arr(mt.table, np.uint32)),
-                                               int(mt.index.dtype.itemsize),
-                                               L.ptr(self._arr(mt.index, mt.index.dtype))),
+            table, index, n_mat = mt.table, mt.index, mt.n_mat
+            if mod is not None:
+                table, index, n_mat = T.isolate_cells(table, index, mod["cell"])
+            L.check(lib.oem_plan_set_materials(h, int(n_mat),
+                                               L.ptr(self._arr(table, np.uint32)),
+                                               int(index.dtype.itemsize),
+                                               L.ptr(self._arr(index, index.dtype))),
                     "set_materials")
             if mt.n_pole_total > 0:
                 L.check(lib.oem_plan_set_pole_sets(
                     h, int(mt.set_ofs.size - 1), L.ptr(self._arr(mt.set_ofs, np.int32)),
                     L.ptr(self._arr(mt.coef, np.float32)), L.ptr(self._arr(mt.seg_ofs, np.uint32)),
                     int(mt.seg_ofs.size), int(mt.n_pole_total)), "set_pole_sets")
+        if mod is not None and mod["comp"].size:
+            L.check(lib.oem_plan_add_modulation(
+                h, int(mod["comp"].size), L.ptr(self._arr(mod["comp"], np.int32)),
+                L.ptr(self._arr(mod["cell"], np.int64)), L.ptr(self._arr(mod["amp"], np.float32)),
+                L.ptr(self._arr(mod["cph"], np.float32)), L.ptr(self._arr(mod["sph"], np.float32)),
+                L.ptr(self._arr(mod["eps"], np.float32)), L.ptr(self._arr(mod["sd"], np.float32)),
+                L.ptr(self._arr(mod["gg"], np.float32)), int(mod["cs"].shape[0]),
+                L.ptr(self._arr(mod["cs"], np.float32)), float(mod["dte"])), "modulation")
         for ps in T.plane_sources(sc):
             if ps["ex"].size < self.n_total:
                 raise ValueError(f"asked to run {self.n_total} steps, but the plane-wave table "

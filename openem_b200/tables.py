@@ -492,6 +492,71 @@ def batch_depth(points: int, ncomp: int, cap: int = 32, ring_bytes: float = 2e9)
     return max(T, 1)
 
 
+def modulation_tables(sc, tabs, n_total: int) -> dict | None:
+    """Per-entry tables of a time-modulated permittivity and the per-step (cos, sin) of the
+    modulation phase at t_n and t_n+1, computed in float64 and narrowed to float32
+    (``openem/sources_setup.py:460-518, 640-650``). Entries whose static ``cb`` is zero (the
+    tangential E on a PEC-backed wall, which OpenEM masks after the update) are dropped: their
+    coefficients stay zero."""
+    mo = sc.modulation
+    if mo is None or mo.n_entry == 0:
+        return None
+    mo.validate(sc.shape)
+    if sc.any_pec or (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry > 0) \
+            or (sc.tensor is not None and sc.tensor.n_entry > 0):
+        raise NotImplementedError(
+            "a time-varying medium together with PEC/mix/tensor in one scene is not supported")
+    comp = np.asarray(mo.comp, np.int64)
+    cell = np.asarray(mo.cell, np.int64)
+    amp = np.asarray(mo.amp, np.float64)
+    phase = np.asarray(mo.phase, np.float64)
+    es = np.empty(comp.size)
+    sd = np.zeros(comp.size)
+    gg = np.zeros(comp.size)
+    sig = (sc.sigma_ex, sc.sigma_ey, sc.sigma_ez)
+    g_maps = _g_dense(sc, sc.shape)
+    for c, eps in enumerate((sc.eps_ex, sc.eps_ey, sc.eps_ez)):
+        m = comp == c
+        es[m] = np.asarray(eps, np.float64).ravel()[cell[m]]
+        if sig[c] is not None:
+            sd[m] = np.asarray(sig[c], np.float64).ravel()[cell[m]] * sc.dt / (2.0 * EPSILON_0)
+        gg[m] = np.asarray(g_maps[c]).ravel()[cell[m]]
+    if float(np.min(es - np.abs(amp))) <= 0.0:
+        raise ValueError(f"modulated cells: min of eps_s - |amp| is "
+                         f"{float(np.min(es - np.abs(amp))):.4f} <= 0, so eps(t) would go "
+                         "non-positive, which is unstable")
+    _, cb = e_coefficients(sc, tabs)
+    keep = np.ones(comp.size, bool)
+    for c in range(3):
+        m = comp == c
+        keep[m] = cb[c].ravel()[cell[m]] != 0.0
+    om = 2.0 * np.pi * float(mo.freq)
+    t = np.arange(n_total, dtype=np.float64)
+    w0, w1 = om * (t * sc.dt), om * ((t + 1.0) * sc.dt)
+    cs = np.ascontiguousarray(np.stack([np.cos(w0), np.sin(w0), np.cos(w1), np.sin(w1)],
+                                       axis=1).astype(np.float32))
+    f32 = lambda a: np.ascontiguousarray(a[keep], dtype=np.float32)
+    return {"comp": np.ascontiguousarray(comp[keep], np.int32),
+            "cell": np.ascontiguousarray(cell[keep], np.int64),
+            "amp": f32(amp), "cph": f32(np.cos(phase)), "sph": f32(np.sin(phase)),
+            "eps": f32(es), "sd": f32(sd), "gg": f32(gg), "cs": cs,
+            "dte": float(sc.dt / EPSILON_0)}
+
+
+def isolate_cells(table, index, cells):
+    """Give each listed cell its own copy of its material record, appended after the existing
+    ones: the per-step modulation kernel rewrites a modulated cell's record in place, so no other
+    cell may share it. Returns the new table, index and record count."""
+    cells = np.unique(np.asarray(cells, np.int64))
+    flat = np.asarray(index).reshape(-1)
+    n0 = int(table.shape[0])
+    table = np.concatenate([table, table[flat[cells].astype(np.int64)]])
+    n_mat = int(table.shape[0])
+    out = flat.astype(np.uint16 if n_mat <= 65535 else np.uint32)
+    out[cells] = n0 + np.arange(cells.size)
+    return table, np.ascontiguousarray(out.reshape(np.asarray(index).shape)), n_mat
+
+
 def absorber_tables(sc) -> list:
     """Absorber slabs in scene order: ``(axis, g0, nlay, decay_int, decay_half)``
     (openem/dispersion_setup.py:89-120)."""

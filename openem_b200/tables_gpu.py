@@ -156,3 +156,21 @@ def material_tables_device(sc, tabs, device: int = 0) -> DeviceTables:
     torch.cuda.current_stream(dev).synchronize()
     return DeviceTables(table=rec, index=index, n_mat=n_mat, set_ofs=set_ofs,
                         coef=np.ascontiguousarray(coef), seg_ofs=seg_ofs, n_pole_total=total)
+
+
+def isolate_cells_device(mt: DeviceTables, cells) -> None:
+    """:func:`openem_b200.tables.isolate_cells` on a device index, in place."""
+    import torch
+    cells = np.unique(np.asarray(cells, np.int64))
+    flat = mt.index.view(-1)
+    cd = torch.as_tensor(cells, device=flat.device)
+    old = flat[cd].to(torch.int64).cpu().numpy()
+    n0 = int(mt.n_mat)
+    table = np.concatenate([mt.table, mt.table[old]])
+    n_mat = int(table.shape[0])
+    index = mt.index if (n_mat <= 32767 or mt.index.dtype == torch.int32) \
+        else mt.index.to(torch.int32)
+    index.view(-1)[cd] = torch.arange(n0, n_mat, device=flat.device, dtype=torch.int64) \
+        .to(index.dtype)
+    torch.cuda.current_stream(flat.device).synchronize()
+    mt.table, mt.index, mt.n_mat = table, index, n_mat

@@ -127,8 +127,8 @@ class Oracle:
         for feat in ("tfsf_sources", "flux_time_monitors"):
             if getattr(sc, feat, None):
                 raise NotImplementedError(f"oracle: {feat} not transcribed")
-        if sc.any_dispersion_mix or sc.any_tensor or sc.any_modulation:
-            raise NotImplementedError("oracle: mix / tensor / modulation not transcribed")
+        if sc.any_dispersion_mix or sc.any_tensor:
+            raise NotImplementedError("oracle: mix / tensor not transcribed")
         self.sc = sc
         self.n_total = int(n_total if n_total is not None else sc.num_time_steps)
         nx, ny, nz = self.shape = sc.shape
@@ -152,11 +152,52 @@ class Oracle:
         self.ca, self.cb = e_coeffs(sc)
         self.hist = [np.zeros(self.shape) for _ in range(3)]
         self._setup_dispersion()
+        self._setup_modulation()
         self._setup_sources()
         self._setup_monitors()
         self.n = 0
 
     # ---- setup --------------------------------------------------------------------------
+    def _setup_modulation(self):
+        """Time-modulated permittivity (openem/sources_setup.py:460-518): per entry eps_s, amp,
+        phase, s = sigma dt / (2 eps0) and the dispersion coupling G, all float64."""
+        sc = self.sc
+        self.mod = None
+        mo = sc.modulation
+        if mo is None or mo.n_entry == 0:
+            return
+        comp = np.asarray(mo.comp, np.int64)
+        cell = np.asarray(mo.cell, np.int64)
+        es, sd, gg = np.empty(comp.size), np.zeros(comp.size), np.zeros(comp.size)
+        g = _g_dense(sc.dispersion, self.shape) if sc.any_dispersion else None
+        sig = (sc.sigma_ex, sc.sigma_ey, sc.sigma_ez)
+        for c, eps in enumerate((sc.eps_ex, sc.eps_ey, sc.eps_ez)):
+            m = comp == c
+            es[m] = np.asarray(eps, np.float64).ravel()[cell[m]]
+            if sig[c] is not None:
+                sd[m] = np.asarray(sig[c], np.float64).ravel()[cell[m]] * sc.dt / (2 * EPSILON_0)
+            if g is not None:
+                gg[m] = g[c].ravel()[cell[m]]
+        self.mod = {"comp": comp, "cell": cell, "es": es, "sd": sd, "gg": gg,
+                    "amp": np.asarray(mo.amp, np.float64),
+                    "phase": np.asarray(mo.phase, np.float64), "om": 2 * np.pi * float(mo.freq)}
+
+    def modulate(self, n):
+        """D-form coefficients of step n on the modulated entries
+        (openem/kernels/modulation.cu:40-79): ca = (eps(t_n) - s) / (eps(t_n+1) + s + G),
+        cb = (dt / eps0) / (eps(t_n+1) + s + G), eps(t) = eps_s + amp cos(omega t - phi)."""
+        md = getattr(self, "mod", None)  # the complex path has no modulation
+        if md is None:
+            return
+        dt = self.sc.dt
+        e0 = md["es"] + md["amp"] * np.cos(md["om"] * (n * dt) - md["phase"])
+        e1 = md["es"] + md["amp"] * np.cos(md["om"] * ((n + 1) * dt) - md["phase"])
+        den = e1 + md["sd"] + md["gg"]
+        for c in range(3):
+            m = md["comp"] == c
+            self.ca[c].ravel()[md["cell"][m]] = ((e0 - md["sd"]) / den)[m]
+            self.cb[c].ravel()[md["cell"][m]] = ((dt / EPSILON_0) / den)[m]
+
     def _setup_dispersion(self):
         d = self.sc.dispersion
         self.disp = None
@@ -489,6 +530,7 @@ class Oracle:
         self.inject_h(n)
         self.absorb("H")
         self.disp_pre()
+        self.modulate(n)
         self.update_e()
         self.inject_e(n)
         self.disp_post()

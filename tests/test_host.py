@@ -119,14 +119,14 @@ def test_phase_table():
     assert ph.dtype == np.float32 and ph.shape == (5, 2, 4)
 
 
-@pytest.mark.parametrize("feature", ["tfsf", "disp_in_absorber", "modulation", "tensor"])
+@pytest.mark.parametrize("feature", ["tfsf", "disp_in_absorber", "modulation_pec", "tensor"])
 def test_unsupported_physics_fails_closed(feature):
     sc = scenes.slab_plane_wave(nxy=1, num_steps=10)
     sd = scenes.small_dispersive(n=20, n_sph=1, n_pml=4, num_steps=10)
     bad = {
         "tfsf": replace(sc, tfsf_sources=[object()]),
         "disp_in_absorber": replace(sd, absorbers=scenes.absorber_slabs(sd.grid, 0, 10)),
-        "modulation": replace(sc, modulation=M.TimeModulation(
+        "modulation_pec": replace(sc, pec_ex=np.array([5]), modulation=M.TimeModulation(
             1e14, np.array([0]), np.array([0]), np.array([0.1]), np.array([0.0]))),
         "tensor": replace(sc, tensor=M.TensorEps(np.array([0]), np.array([0]),
                                                   np.eye(3)[None], np.zeros((1, 3, 3)))),
@@ -195,6 +195,49 @@ def test_adjoint_coefficient_jacobian_matches_differences():
     ca_m, cb_m = coef(e, sg - hs)
     np.testing.assert_allclose(jac[c][2][cell], (ca_p - ca_m) / (2 * hs), rtol=1e-6)
     np.testing.assert_allclose(jac[c][3][cell], (cb_p - cb_m) / (2 * hs), rtol=1e-6)
+
+
+def test_modulation_tables():
+    """Per-step (cos, sin) rows at t_n and t_n+1 in float64 narrowed to float32, entries on a
+    PEC-backed wall dropped, eps_s - |amp| <= 0 and PEC cells refused
+    (openem/sources_setup.py:460-518, 640-650)."""
+    sc = scenes.modulated_slab(nxy=2, num_steps=50, phase=lambda x, y, z: 3e6 * x)
+    tabs = [T.axis_tables(sc, a) for a in range(3)]
+    md = T.modulation_tables(sc, tabs, 50)
+    om = 2 * np.pi * sc.modulation.freq
+    n = np.arange(50.0)
+    np.testing.assert_array_equal(md["cs"][:, 0], np.cos(om * n * sc.dt).astype(np.float32))
+    np.testing.assert_array_equal(md["cs"][:, 3], np.sin(om * (n + 1) * sc.dt).astype(np.float32))
+    assert md["comp"].size == sc.modulation.n_entry
+    assert np.ptp(md["cph"]) > 0
+    with pytest.raises(ValueError):
+        T.modulation_tables(replace(sc, modulation=replace(
+            sc.modulation, amp=np.full(sc.modulation.n_entry, 1.5))), tabs, 50)
+    with pytest.raises(NotImplementedError):
+        T.modulation_tables(replace(sc, pec_ex=np.array([0])), tabs, 50)
+    # a PEC-backed z wall: the tangential entries on it keep ca = cb = 0
+    ax = sc.grid.axes
+    g2 = M.Grid(ax[0], ax[1], M.Axis(ax[2].edges, "PEC", "PEC"))
+    nz = sc.shape[2]
+    mo = M.TimeModulation(sc.modulation.freq, np.array([0, 2]), np.array([0, 0]),
+                          np.array([0.1, 0.1]), np.zeros(2))
+    sc2 = replace(sc, grid=g2, pml={}, modulation=mo)
+    tabs2 = [T.axis_tables(sc2, a) for a in range(3)]
+    md2 = T.modulation_tables(sc2, tabs2, 5)
+    assert md2["comp"].tolist() == [2] and nz > 0
+
+
+def test_isolate_cells_gives_each_cell_its_own_record():
+    table = np.arange(3 * 16, dtype=np.uint32).reshape(3, 16)
+    index = np.array([[0, 1, 1], [2, 1, 0]], dtype=np.uint16)
+    t2, i2, n = T.isolate_cells(table, index, np.array([1, 4, 1]))
+    assert n == 5 and t2.shape == (5, 16)
+    flat = i2.ravel()
+    assert flat[1] == 3 and flat[4] == 4
+    np.testing.assert_array_equal(t2[3], table[1])
+    np.testing.assert_array_equal(t2[4], table[1])
+    keep = [0, 2, 3, 5]
+    np.testing.assert_array_equal(flat[keep], index.ravel()[keep])
 
 
 def test_dipole_table_refuses_short_waveform():

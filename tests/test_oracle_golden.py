@@ -225,3 +225,40 @@ def test_mode_source_one_plane_tfsf_is_unidirectional():
         pb = flux_mod.plane_flux(r.phasors["B"], sc.grid, axis=2)
         assert np.all(pu > 0)
         assert abs(pb[2] / pu[2]) < 1e-6, (k, pb / pu)
+
+
+def test_oracle_modulation_first_order_sidebands():
+    """Known answer from OpenEM's own modulation test (tests/test_timemod.py:255-300): an
+    index-matched slab with eps(t) = 1 + 0.01 cos(Omega t) transmits sidebands at f0 +- Omega
+    whose flux ratio to the carrier is (k+- delta S / 4)^2, S = |sum dz exp(i (k0 - k+-) z)| over
+    the modulated Ex planes; 5% tolerance there. The FP64 oracle lands within 1%."""
+    C0 = 2.99792458e8
+    sc = scenes.modulated_slab(num_steps=12000)
+    r = ref64.run(sc)
+    fl = flux_mod.plane_flux(r.phasors["T"], sc.grid, axis=2)
+    f = sc.flux_monitors[0].freqs
+    mo = sc.modulation
+    nz = sc.shape[2]
+    kk = np.unique(mo.cell[mo.comp == 0] % nz)
+    z = sc.grid.axes[2].edges[kk]
+    dz = sc.grid.axes[2].dl_dual[kk]
+    k0 = 2 * np.pi * f[1] / C0
+    for i in (0, 2):
+        kpm = 2 * np.pi * f[i] / C0
+        S = abs(np.sum(dz * np.exp(1j * (k0 - kpm) * z)))
+        pred = (kpm * 0.01 / 4.0 * S) ** 2
+        assert fl[i] / fl[1] == pytest.approx(pred, rel=0.01)
+    assert fl[2] / fl[1] > fl[0] / fl[1]
+
+
+def test_oracle_zero_amplitude_modulation_is_identity():
+    """With amp = 0 the D-form coefficients reduce to the static ones expression for expression,
+    so the FP64 oracle is bitwise unchanged (the reference's criterion,
+    tests/test_timemod.py:155-190, with loss and dispersion folded in)."""
+    sd = scenes.small_dispersive(n=16, n_sph=1, n_pml=3, num_steps=60)
+    mo = M.TimeModulation(3e13, np.array([0, 1, 2, 2]), np.array([100, 2000, 2001, 3000]),
+                          np.zeros(4), np.array([0.0, 0.3, 1.0, 2.0]))
+    a = ref64.run(replace(sd, modulation=mo))
+    b = ref64.run(sd)
+    for nm in a.fields:
+        np.testing.assert_array_equal(a.fields[nm], b.fields[nm])
