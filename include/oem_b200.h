@@ -150,6 +150,24 @@ int oem_plan_add_modulation(oem_plan* p, int n_entry, const int* comp, const int
                             const float* eps_s, const float* sd, const float* gg, int ntab,
                             const float* cs_tab, double dte);
 
+/* Instantaneous flux through a plane (FluxTimeMonitor; openem/readout.py:20-73,
+ * openem/flux.py:146-164, 307-578): per sampled step m (m = beg + iv q < end, q < nslots)
+ *   s(m) = sum_planes w sum_(u,v) dS[u,v] (E_t1 Hbar_t2 - E_t2 Hbar_t1),  Hbar = (H^{m-1/2} +
+ * H^{m+1/2}) / 2, with the components colocated onto the samples: per plane q (1 or 2) E from
+ * layer ke[q] of the normal axis, H from layers kh[q], kh[q] + 1 with weights wh[2q], wh[2q+1];
+ * along t1 (the lower transverse axis) E_t1 and H_t2 interpolate between cells lo1[u] and hi1[u]
+ * with low weights wlo1[0][u] (E) / wlo1[1][u] (H) and high weight whi1[u], the others sit on
+ * edge e1[u]; the same along t2 with (E_t2, H_t1). dS is (n1, n2), signed. Read with
+ * oem_plan_read_flux_time (nslots float64). */
+int oem_plan_add_flux_time_monitor(oem_plan* p, int axis, int nplanes, const double* w,
+                                   const int* ke, const int* kh, const double* wh, int n1,
+                                   const int* e1, const int* lo1, const int* hi1,
+                                   const double* wlo1, const double* whi1, int n2, const int* e2,
+                                   const int* lo2, const int* hi2, const double* wlo2,
+                                   const double* whi2, const double* dS, int beg, int end, int iv,
+                                   int nslots, int* id);
+int oem_plan_read_flux_time(oem_plan* p, int id, double* out, void* stream);
+
 /* Absorber boundary slab (Tidy3D's Absorber; replaces absorb_slab / absorb_batch,
  * openem/kernels/absorber.cu:20-70, absorb_batch.cu:15-110, and the host tables of
  * openem/dispersion_setup.py:89-120): layers [g0, g0 + nlay) along `axis`. After the H-side

@@ -289,6 +289,10 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
     if ((e = launch_time_sample(P, m, p->d_step, 0, s)) != cudaSuccess)
       return cuda_error(e, "time_sample");
   }
+  for (const FluxTimeMon& m : p->ftmons) {
+    if (!monitors) break;
+    if ((e = launch_flux_time(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "flux_time");
+  }
   for (const Monitor& m : p->mons) {
     if (!monitors) break;
     if ((e = launch_snapshot(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "snapshot");
@@ -1048,6 +1052,80 @@ int oem_plan_add_time_monitor(oem_plan* p, int nc, const int32_t* comps, int i0,
   return OEM_OK;
 }
 
+int oem_plan_add_flux_time_monitor(oem_plan* p, int axis, int nplanes, const double* w,
+                                   const int* ke, const int* kh, const double* wh, int n1,
+                                   const int* e1, const int* lo1, const int* hi1,
+                                   const double* wlo1, const double* whi1, int n2, const int* e2,
+                                   const int* lo2, const int* hi2, const double* wlo2,
+                                   const double* whi2, const double* dS, int beg, int end, int iv,
+                                   int nslots, int* id) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (p->is_complex) return set_error(OEM_ERR_UNSUPPORTED, "flux time monitors on a complex plan");
+  if (axis < 0 || axis > 2) return set_error(OEM_ERR_INVALID, "monitor axis must be 0..2");
+  if (nplanes < 1 || nplanes > 2 || n1 < 1 || n2 < 1 || iv < 1 || nslots < 0 || !id)
+    return set_error(OEM_ERR_INVALID, "bad flux time monitor shape");
+  if (!w || !ke || !kh || !wh || !e1 || !lo1 || !hi1 || !wlo1 || !whi1 || !e2 || !lo2 || !hi2 ||
+      !wlo2 || !whi2 || !dS)
+    return set_error(OEM_ERR_INVALID, "null flux time table");
+  const int dims[3] = {p->nx, p->ny, p->nz};
+  const int t1 = axis == 0 ? 1 : 0, t2 = axis == 2 ? 1 : 2;
+  for (int q = 0; q < nplanes; ++q)
+    if (ke[q] < 0 || ke[q] >= dims[axis] || kh[q] < 0 || kh[q] + 1 >= dims[axis])
+      return set_error(OEM_ERR_INVALID, "flux time plane outside the grid");
+  auto inside = [](const int* a, int n, int lim) {
+    for (int q = 0; q < n; ++q)
+      if (a[q] < 0 || a[q] >= lim) return false;
+    return true;
+  };
+  if (!inside(e1, n1, dims[t1]) || !inside(lo1, n1, dims[t1]) || !inside(hi1, n1, dims[t1]) ||
+      !inside(e2, n2, dims[t2]) || !inside(lo2, n2, dims[t2]) || !inside(hi2, n2, dims[t2]))
+    return set_error(OEM_ERR_INVALID, "flux time sample outside the grid");
+  if ((rc = use_device(p))) return rc;
+  FluxTimeMon m;
+  m.axis = axis;
+  m.nplanes = nplanes;
+  for (int q = 0; q < nplanes; ++q) {
+    m.w[q] = w[q];
+    m.ke[q] = ke[q];
+    m.kh[q] = kh[q];
+    m.wh[q][0] = wh[2 * q];
+    m.wh[q][1] = wh[2 * q + 1];
+  }
+  m.n1 = n1; m.n2 = n2;
+  m.beg = beg; m.end = end; m.iv = iv; m.slots = nslots;
+  const int64_t samples = (int64_t)nplanes * n1 * n2;
+  m.nblocks = (int)std::max<int64_t>(1, std::min<int64_t>((samples + 255) / 256, 148 * 4));
+  if ((rc = dupload(p, &m.e1, e1, n1)) || (rc = dupload(p, &m.lo1, lo1, n1)) ||
+      (rc = dupload(p, &m.hi1, hi1, n1)) || (rc = dupload(p, &m.wlo1, wlo1, 2 * (size_t)n1)) ||
+      (rc = dupload(p, &m.whi1, whi1, n1)) || (rc = dupload(p, &m.e2, e2, n2)) ||
+      (rc = dupload(p, &m.lo2, lo2, n2)) || (rc = dupload(p, &m.hi2, hi2, n2)) ||
+      (rc = dupload(p, &m.wlo2, wlo2, 2 * (size_t)n2)) || (rc = dupload(p, &m.whi2, whi2, n2)) ||
+      (rc = dupload(p, &m.dS, dS, (size_t)n1 * n2)))
+    return rc;
+  if ((rc = dalloc(p, &m.ekeep, (size_t)samples * 2)) ||
+      (rc = dalloc(p, &m.part, (size_t)m.nblocks * 2)) ||
+      (rc = dalloc(p, &m.buf, (size_t)std::max(nslots, 1))))
+    return rc;
+  *id = (int)p->ftmons.size();
+  p->ftmons.push_back(m);
+  return OEM_OK;
+}
+
+int oem_plan_read_flux_time(oem_plan* p, int id, double* out, void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (id < 0 || id >= (int)p->ftmons.size() || !out)
+    return set_error(OEM_ERR_INVALID, "flux time monitor id out of range");
+  if ((rc = use_device(p))) return rc;
+  const FluxTimeMon& m = p->ftmons[id];
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (m.slots)
+    OEM_CUDA(cudaMemcpyAsync(out, m.buf, (size_t)m.slots * sizeof(double), cudaMemcpyDeviceToHost, s));
+  OEM_CUDA(cudaStreamSynchronize(s));
+  return check_device_error(p);
+}
+
 int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   int rc = check_plan(p, false);
   if (rc) return rc;
@@ -1308,6 +1386,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
         if ((e = launch_time_sample(p->yp, m, p->d_step, 1, s)) != cudaSuccess) return cuda_error(e, "ts");
         if ((e = launch_time_sample(p->yp, m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "ts");
       }
+      for (const FluxTimeMon& m : p->ftmons)
+        if ((e = launch_flux_time(p->yp, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "ft");
       for (const Monitor& m : p->mons) {
         if ((e = launch_snapshot(p->yp, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "snap");
         if ((e = launch_flush(m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "flush");
@@ -1389,6 +1469,7 @@ int oem_plan_launches_per_step(oem_plan* p, int* n) {
   for (const DipoleSet& d : p->dipoles) c += d.n_targets > 0 ? 1 : 0;
   c += 2 * (int)p->tmons.size();
   c += 3 * (int)p->mons.size();  // snapshot, flush, flush mark
+  c += 2 * (int)p->ftmons.size();
   *n = c;
   return OEM_OK;
 }

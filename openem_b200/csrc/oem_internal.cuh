@@ -183,6 +183,30 @@ struct Modulation {
   MatRec* mats = nullptr;   // the plan's records (writable), set at finalize
 };
 
+// Instantaneous colocated flux of one plane (FluxTimeMonitor): per sample step m,
+// s(m) = sum_planes w sum dS (E_t1 Hbar_t2 - E_t2 Hbar_t1), Hbar = (H^{m-1/2} + H^{m+1/2}) / 2,
+// accumulated in two shots: at step m the E^m half with H^{m-1/2} (E colocated and kept), at step
+// m + 1 the kept E with H^{m+1/2}. Per transverse axis: edge index, low / high interpolation
+// cells, low weights of the two labels interpolated along it (E_t1, H_t2 along t1; E_t2, H_t1
+// along t2) and high weights.
+struct FluxTimeMon {
+  int axis = 0, nplanes = 1;
+  double w[2] = {1.0, 0.0};
+  int ke[2] = {0, 0}, kh[2] = {0, 0};
+  double wh[2][2] = {{1.0, 0.0}, {1.0, 0.0}};
+  int n1 = 0, n2 = 0;
+  int *e1 = nullptr, *lo1 = nullptr, *hi1 = nullptr;
+  int *e2 = nullptr, *lo2 = nullptr, *hi2 = nullptr;
+  double *wlo1 = nullptr, *whi1 = nullptr;  // wlo1: (2, n1) = (E_t1, H_t2)
+  double *wlo2 = nullptr, *whi2 = nullptr;  // wlo2: (2, n2) = (E_t2, H_t1)
+  double* dS = nullptr;                     // (n1, n2), signed
+  double* ekeep = nullptr;                  // (nplanes, 2, n1, n2) colocated E of the last shot
+  double* part = nullptr;                   // (nblocks, 2) block partial sums
+  double* buf = nullptr;                    // (slots,)
+  int nblocks = 0;
+  int beg = 0, end = 0, iv = 1, slots = 0;
+};
+
 struct TimeMon {
   int nc = 0;
   int comps[6] = {0, 0, 0, 0, 0, 0};
@@ -241,6 +265,7 @@ struct oem_plan {
   bool is_complex = false;  // Bloch / forced complex fields
   std::vector<oem::Monitor> mons;
   std::vector<oem::TimeMon> tmons;
+  std::vector<oem::FluxTimeMon> ftmons;
 
   // device state
   std::vector<void*> allocs;
@@ -349,6 +374,8 @@ cudaError_t launch_update_e_c(const YeeParams& P, cudaStream_t s);
 cudaError_t launch_absorb(const YeeParams& P, const Absorber& a, int is_e, cudaStream_t s);
 cudaError_t launch_modulate(const YeeParams& P, const Modulation& m, const int* step,
                             cudaStream_t s);
+cudaError_t launch_flux_time(const YeeParams& P, const FluxTimeMon& m, const int* step,
+                             cudaStream_t s);
 
 // Discrete adjoint (oem_adjoint.cu): adjoint fields, their CPML psi, scratch for the transposed
 // differences, and the gradient accumulators of ca and cb per component.

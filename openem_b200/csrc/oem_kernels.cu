@@ -633,6 +633,101 @@ cudaError_t launch_modulate(const YeeParams& P, const Modulation& m, const int* 
   return cudaGetLastError();
 }
 
+// Instantaneous colocated flux (openem/readout.py:20-73 with the geometry of
+// openem/flux.py:146-164, 534-578): one thread per (plane, sample); the second shot of step
+// m = n (kept E^n with H^{n+1/2}) and the first shot of m = n + 1 (E^{n+1} with H^{n+1/2}, E kept)
+// each reduce to one block partial; k_flux_time_fold sums the partials in block order.
+__device__ __forceinline__ bool ft_slot(const FluxTimeMon& m, int mref, int* slot) {
+  const int off = mref - m.beg;
+  if (off < 0 || mref >= m.end || off % m.iv) return false;
+  *slot = off / m.iv;
+  return *slot < m.slots;
+}
+
+__device__ __forceinline__ double ft_field(const YeeParams& P, const float* F, int ax, int kn,
+                                           int q1, int q2, int t1, int t2) {
+  int c[3];
+  c[ax] = kn; c[t1] = q1; c[t2] = q2;
+  return (double)F[((int64_t)c[0] * P.ny + c[1]) * P.nzp + c[2]];
+}
+
+__global__ void __launch_bounds__(256) k_flux_time(YeeParams P, FluxTimeMon m, const int* step) {
+  const int n = *step;
+  int slot1, slot0;
+  const bool s1 = ft_slot(m, n, &slot1), s0 = ft_slot(m, n + 1, &slot0);
+  if (!s1 && !s0) return;  // uniform over the grid
+  const int t1 = m.axis == 0 ? 1 : 0, t2 = m.axis == 2 ? 1 : 2;
+  const int64_t per = (int64_t)m.n1 * m.n2, total = per * m.nplanes;
+  double c1 = 0.0, c0 = 0.0;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int p = (int)(q / per);
+    const int64_t r = q - p * per;
+    const int u = (int)(r / m.n2), v = (int)(r - (int64_t)u * m.n2);
+    const int kh = m.kh[p];
+    const double h0 = m.wh[p][0], h1 = m.wh[p][1];
+    const float* Ht1 = P.f[3 + t1];
+    const float* Ht2 = P.f[3 + t2];
+    // H_t2 along t1 (cells lo1 / hi1 at edge e2), H_t1 along t2 (cells lo2 / hi2 at edge e1)
+    auto hnorm = [&](const float* H, int q1, int q2) {
+      return h0 * ft_field(P, H, m.axis, kh, q1, q2, t1, t2) +
+             h1 * ft_field(P, H, m.axis, kh + 1, q1, q2, t1, t2);
+    };
+    const double hv = m.wlo1[m.n1 + u] * hnorm(Ht2, m.lo1[u], m.e2[v]) +
+                      m.whi1[u] * hnorm(Ht2, m.hi1[u], m.e2[v]);
+    const double hu = m.wlo2[m.n2 + v] * hnorm(Ht1, m.e1[u], m.lo2[v]) +
+                      m.whi2[v] * hnorm(Ht1, m.e1[u], m.hi2[v]);
+    const double wd = 0.5 * m.w[p] * m.dS[r];
+    double* keep = m.ekeep + ((int64_t)p * 2) * per + r;
+    if (s1) c1 += wd * (keep[0] * hv - keep[per] * hu);
+    if (s0) {
+      const int ke = m.ke[p];
+      const double eu = m.wlo1[u] * ft_field(P, P.f[t1], m.axis, ke, m.lo1[u], m.e2[v], t1, t2) +
+                        m.whi1[u] * ft_field(P, P.f[t1], m.axis, ke, m.hi1[u], m.e2[v], t1, t2);
+      const double ev = m.wlo2[v] * ft_field(P, P.f[t2], m.axis, ke, m.e1[u], m.lo2[v], t1, t2) +
+                        m.whi2[v] * ft_field(P, P.f[t2], m.axis, ke, m.e1[u], m.hi2[v], t1, t2);
+      keep[0] = eu;
+      keep[per] = ev;
+      c0 += wd * (eu * hv - ev * hu);
+    }
+  }
+  // block reduction in a fixed order
+  __shared__ double red[2][8];
+  for (int o = 16; o > 0; o >>= 1) {
+    c1 += __shfl_down_sync(0xffffffffu, c1, o);
+    c0 += __shfl_down_sync(0xffffffffu, c0, o);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) { red[0][w] = c1; red[1][w] = c0; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { a += red[0][k]; b += red[1][k]; }
+    m.part[2 * blockIdx.x] = a;
+    m.part[2 * blockIdx.x + 1] = b;
+  }
+}
+
+__global__ void k_flux_time_fold(FluxTimeMon m, const int* step) {
+  const int n = *step;
+  int slot1, slot0;
+  const bool s1 = ft_slot(m, n, &slot1), s0 = ft_slot(m, n + 1, &slot0);
+  if (threadIdx.x != 0 || (!s1 && !s0)) return;
+  double a = 0.0, b = 0.0;
+  for (int k = 0; k < m.nblocks; ++k) { a += m.part[2 * k]; b += m.part[2 * k + 1]; }
+  if (s1) m.buf[slot1] += a;  // the second shot completes slot m = n
+  if (s0) m.buf[slot0] = b;   // the first shot opens slot m = n + 1
+}
+
+cudaError_t launch_flux_time(const YeeParams& P, const FluxTimeMon& m, const int* step,
+                             cudaStream_t s) {
+  k_flux_time<<<m.nblocks, 256, 0, s>>>(P, m, step);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_flux_time_fold<<<1, 32, 0, s>>>(m, step);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* step,
                             cudaStream_t s) {
   if (m.kind == 0) {

@@ -20,7 +20,7 @@ import numpy as np
 
 from openem_b200.model import (
     C_0, EPSILON_0, ETA_0, Axis, Dispersion, FieldMonitor, FieldTimeMonitor, FluxMonitor,
-    GaussianPulse, Grid, ModeSource, PlaneWaveSource, PMLParams, PointDipole, Scene,
+    FluxTimeMonitor, GaussianPulse, Grid, ModeSource, PlaneWaveSource, PMLParams, PointDipole, Scene,
     TimeModulation, pml_build, sample_waveform)
 
 UM = 1e-6
@@ -254,6 +254,47 @@ def modulated_slab(eps_s: float = 1.0, delta: float = 0.01, fm_rel: float = 0.1,
     from dataclasses import replace
     return replace(base, flux_monitors=mons, modulation=mod, eps_ex=eps[0], eps_ey=eps[1],
                    eps_ez=eps[2])
+
+
+def flux_time_plane(nxy: int = 16, dl: float = 0.025 * UM, plane_z: float = 0.3 * UM,
+                    center=(0.013 * UM, -0.017 * UM), size=(0.27 * UM, 0.29 * UM),
+                    interval: int = 1, start_step: int = 0, nfreq: int = 181,
+                    run_time: float = 1.5e-13, num_steps: int | None = None,
+                    full_span: bool = False) -> Scene:
+    """Vacuum 0.4 x 0.4 x 1.6 um cell, periodic x/y, CPML z, a +z plane wave (GaussianPulse
+    3e14 Hz, fwidth 0.6e14 Hz) at z = -0.55 um; a FluxTimeMonitor "ft" on the plane through
+    ``plane_z`` (its position between two Yee boundaries sets ``frac``) with transverse bounds
+    ``center +- size / 2`` (or the whole periodic cross section), a FluxMonitor "fx" at
+    ``nfreq`` frequencies over f0 +- 4.5 fwidth on the boundary below it, and a FieldTimeMonitor
+    "ftm" of E_x, E_y, H_x, H_y around the plane."""
+    freq0, fwidth = 3.0e14, 0.6e14
+    base = slab_plane_wave(nxy=nxy, dl=dl, lz=1.6 * UM, src_z=-0.55 * UM, mon_t=plane_z,
+                           mon_r=-0.7 * UM, freq0=freq0, nfreq=3, run_time=run_time,
+                           with_slab=False, num_steps=num_steps, fwidth_rel=fwidth / freq0)
+    grid = base.grid
+    ez = np.asarray(grid.axes[2].edges)
+    km = int(np.searchsorted(ez, plane_z + 1e-6 * dl, side="right")) - 1
+    frac = float((plane_z - ez[km]) / (ez[km + 1] - ez[km]))
+    if abs(frac) < 1e-9:
+        frac = 0.0
+    if full_span:
+        tb = tuple((float(grid.axes[a].edges[0]), float(grid.axes[a].edges[-1])) for a in (0, 1))
+    else:
+        tb = tuple((center[a] - 0.5 * size[a], center[a] + 0.5 * size[a]) for a in (0, 1))
+    n = base.num_time_steps
+    slots = (n - start_step + interval - 1) // interval
+    ft = FluxTimeMonitor(name="ft", axis=2, plane_index=km, normal_dir=1, step_begin=start_step,
+                         step_end=n, interval=interval, num_slots=slots, t_bounds=tb, frac=frac)
+    freqs = np.linspace(freq0 - 4.5 * fwidth, freq0 + 4.5 * fwidth, nfreq)
+    pulse = GaussianPulse(freq0=freq0, fwidth=fwidth)
+    fx = FluxMonitor(name="fx", axis=2, plane_index=km, normal_dir=1, freqs=freqs,
+                     source_spectrum=spectrum(pulse, base.dt, n, freqs))
+    nx, ny, _ = grid.shape
+    tm = FieldTimeMonitor(name="ftm", comps=(0, 1, 3, 4), origin=(0, 0, km - 1),
+                          box=(nx, ny, 3), step_begin=start_step, step_end=n, interval=interval,
+                          num_slots=slots)
+    from dataclasses import replace
+    return replace(base, flux_monitors=[fx], flux_time_monitors=[ft], field_time_monitors=[tm])
 
 
 def slab_transmission(res_slab, res_empty, name: str = "T") -> np.ndarray:

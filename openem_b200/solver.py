@@ -32,7 +32,6 @@ def refuse_unsupported(sc) -> None:
     checks = [
         (bool(getattr(sc, "tfsf_sources", None)), "TFSF box sources"),
         (T.dispersion_in_absorbers(sc), "dispersive media inside Absorber layers"),
-        (bool(getattr(sc, "flux_time_monitors", None)), "flux time monitors"),
         (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry > 0,
          "slanted-interface mixed dispersion"),
         (sc.tensor is not None and sc.tensor.n_entry > 0, "fully anisotropic media"),
@@ -256,6 +255,22 @@ class Plan:
                                                   int(m.interval), int(m.num_slots),
                                                   C.byref(mid)), f"time monitor {m.name}")
             self.time_mons.append((m, mid.value, (int(comps.size), int(m.num_slots), ni, nj, nk)))
+        self.ft_mons = []
+        if not self.cplx:
+            from openem_b200 import flux_time as FT
+            for m in getattr(sc, "flux_time_monitors", []):
+                t = FT.device_tables(FT.geometry(sc.grid, m))
+                mid = C.c_int()
+                a = lambda k, dt: L.ptr(self._arr(t[k], dt))
+                L.check(lib.oem_plan_add_flux_time_monitor(
+                    h, int(m.axis), int(t["nplanes"]), a("w", np.float64), a("ke", np.int32),
+                    a("kh", np.int32), a("wh", np.float64), int(t["n1"]), a("e1", np.int32),
+                    a("lo1", np.int32), a("hi1", np.int32), a("wlo1", np.float64),
+                    a("whi1", np.float64), int(t["n2"]), a("e2", np.int32), a("lo2", np.int32),
+                    a("hi2", np.int32), a("wlo2", np.float64), a("whi2", np.float64),
+                    a("dS", np.float64), int(m.step_begin), int(m.step_end), int(m.interval),
+                    int(m.num_slots), C.byref(mid)), f"flux time monitor {m.name}")
+                self.ft_mons.append((m, mid.value))
         if self.xchunk:
             L.check(lib.oem_plan_set_xchunk(h, self.xchunk), "set_xchunk")
         if self.checkpoint_every:
@@ -377,6 +392,18 @@ class Plan:
     def field_phasors(self) -> dict:
         return {m.name: self.read_monitor(mid, shp) for m, mid, shp in self.box_mons}
 
+    def flux_time(self, steps_run: int) -> dict:
+        """``{name: (filled,) float64}`` of the flux time monitors after ``steps_run`` steps."""
+        out = {}
+        for m, mid in self.ft_mons:
+            buf = np.zeros(max(int(m.num_slots), 1), np.float64)
+            L.check(self.lib.oem_plan_read_flux_time(self.h, int(mid), L.ptr(buf), self._s),
+                    "read_flux_time")
+            off = min(steps_run - 1, m.step_end - 1) - m.step_begin
+            filled = 0 if off < 0 else min(m.num_slots, off // m.interval + 1)
+            out[m.name] = buf[:filled].copy()
+        return out
+
     def time_samples(self, steps_run: int):
         samples, slots = {}, {}
         for m, mid, shp in self.time_mons:
@@ -491,4 +518,5 @@ def _loop(plan: Plan, sc, n_total: int, use_shutoff: bool, verbose: bool, return
                   energy_trace=(pol.energy_decay.abs_history if pol.energy_decay else []),
                   source_end=int(source_end), wall_seconds=wall,
                   stop_reason=pol.reason, shutoff_summary=pol.summary(), fields=fields,
-                  field_phasors=fphas, time_samples=tsamp, time_slots=tslots, flux_time={})
+                  field_phasors=fphas, time_samples=tsamp, time_slots=tslots,
+                  flux_time=plan.flux_time(steps))

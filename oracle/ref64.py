@@ -113,6 +113,7 @@ class OracleResult:
     field_phasors: dict = field(default_factory=dict)    # name -> (6, nf, ni, nj, nk) complex
     time_samples: dict = field(default_factory=dict)
     time_slots: dict = field(default_factory=dict)
+    flux_time: dict = field(default_factory=dict)        # name -> (filled,) float64
     fields: dict = field(default_factory=dict)
     steps_run: int = 0
     seconds: float = 0.0
@@ -124,7 +125,7 @@ class Oracle:
     def __init__(self, sc, n_total: int | None = None):
         if sc.any_bloch:
             raise ValueError("use BlochOracle for a scene with a non-zero Bloch vector")
-        for feat in ("tfsf_sources", "flux_time_monitors"):
+        for feat in ("tfsf_sources",):
             if getattr(sc, feat, None):
                 raise NotImplementedError(f"oracle: {feat} not transcribed")
         if sc.any_dispersion_mix or sc.any_tensor:
@@ -355,8 +356,43 @@ class Oracle:
                                              slice(k0, k0 + nk)),
                               "buf": np.zeros((len(m.comps), m.num_slots, ni, nj, nk),
                                               dtype=self.E[0].dtype)})
+        # flux time monitors: the colocated geometry (openem/flux.py:480-531) is a scene input
+        from openem_b200 import flux_time as FT
+        self.ftmon = [{"m": m, "g": FT.geometry(sc.grid, m), "buf": np.zeros(m.num_slots),
+                       "ekeep": None} for m in getattr(sc, "flux_time_monitors", [])]
         # t = 0 sample, taken before the loop on zero fields (openem/solver.py:492-495)
         self._sample_time(0)
+        self._sample_flux_time(0)
+
+    def _sample_flux_time(self, m_step):
+        """Instantaneous colocated flux in two shots (openem/readout.py:20-73): the second shot
+        of m_step - 1 (its kept colocated E with the current H^{m-1/2}) runs before the first
+        shot of m_step (E^m with H^{m-1/2}, E kept)."""
+        from openem_b200 import flux_time as FT
+        for ft in self.ftmon:
+            m, g = ft["m"], ft["g"]
+            t1, t2 = g["tax"]
+            for phase, m_ref in ((1, m_step - 1), (0, m_step)):
+                off = m_ref - m.step_begin
+                if m_ref < 0 or off < 0 or m_ref >= m.step_end or off % m.interval:
+                    continue
+                slot = off // m.interval
+                if slot >= m.num_slots:
+                    continue
+                if phase == 0:
+                    ft["ekeep"] = [(FT.colocate(self.E[t1], g, "Eu", p),
+                                    FT.colocate(self.E[t2], g, "Ev", p))
+                                   for p in range(len(g["planes"]))]
+                s = 0.0
+                for p, pe in enumerate(g["planes"]):
+                    eu, ev = ft["ekeep"][p]
+                    hu = FT.colocate(self.H[t1], g, "Hu", p)
+                    hv = FT.colocate(self.H[t2], g, "Hv", p)
+                    s += pe["w"] * 0.5 * float(((eu * hv - ev * hu) * g["dS"]).sum())
+                if phase == 0:
+                    ft["buf"][slot] = s
+                else:
+                    ft["buf"][slot] += s
 
     # ---- one step -------------------------------------------------------------------------
     @staticmethod
@@ -537,6 +573,7 @@ class Oracle:
         self.absorb("E")
         self._sample_time(n + 1)
         self.dft(n)
+        self._sample_flux_time(n + 1)
         self.n += 1
 
     def run(self, n_steps: int | None = None) -> OracleResult:
@@ -559,6 +596,11 @@ class Oracle:
             filled = 0 if off < 0 else min(m.num_slots, off // m.interval + 1)
             r.time_samples[m.name] = tm["buf"][:, :filled].copy()
             r.time_slots[m.name] = filled
+        for ft in getattr(self, "ftmon", []):
+            m = ft["m"]
+            off = min(self.n - 1, m.step_end - 1) - m.step_begin
+            filled = 0 if off < 0 else min(m.num_slots, off // m.interval + 1)
+            r.flux_time[m.name] = ft["buf"][:filled].copy()
         names = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
         for nm, F in zip(names, (*self.E, *self.H)):
             r.fields[nm] = F.copy()

@@ -262,3 +262,56 @@ def test_oracle_zero_amplitude_modulation_is_identity():
     b = ref64.run(sd)
     for nm in a.fields:
         np.testing.assert_array_equal(a.fields[nm], b.fields[nm])
+
+
+@pytest.fixture(scope="module")
+def flux_time_run():
+    sc = scenes.flux_time_plane()
+    return sc, ref64.run(sc)
+
+
+def test_oracle_flux_time_parseval(flux_time_run):
+    """Parseval (OpenEM tests/test_fluxtime.py, 2e-2 there): sum_m s(m) = 4 dt int_0^inf P(f) df
+    with P from the plane phasors put through the same colocation geometry."""
+    from openem_b200 import flux_time as FT
+    sc, r = flux_time_run
+    m = sc.flux_time_monitors[0]
+    g = FT.geometry(sc.grid, m)
+    ph = r.phasors["fx"]
+    a0, a1 = g["t"]
+
+    def tang(a, along, lbl):
+        if along == 0:
+            b = a[:, :, a1["edges"]]
+            return (a0["wlo"][lbl][None, :, None] * b[:, a0["lo"], :]
+                    + a0["whi"][None, :, None] * b[:, a0["hi"], :])
+        b = a[:, a0["edges"], :]
+        return (a1["wlo"][lbl][None, None, :] * b[:, :, a1["lo"]]
+                + a1["whi"][None, None, :] * b[:, :, a1["hi"]])
+    eu, ev = tang(ph[0], 0, "Eu"), tang(ph[1], 1, "Ev")
+    hu, hv = tang(ph[2], 1, "Hu"), tang(ph[3], 0, "Hv")
+    p = 0.5 * np.real(np.einsum("fuv,uv->f", eu * np.conj(hv) - ev * np.conj(hu), g["dS"]))
+    f = sc.flux_monitors[0].freqs
+    lhs = float(np.sum(r.flux_time["ft"]))
+    rhs = 4.0 * sc.dt * float(np.sum((p[1:] + p[:-1]) * np.diff(f)) / 2.0)
+    assert lhs > 0 and rhs > 0
+    assert abs(lhs - rhs) / rhs < 2e-2
+
+
+def test_oracle_flux_time_equals_time_monitor_samples(flux_time_run):
+    """Step by step, the two-shot flux series equals the FieldTimeMonitor samples (E^m and the
+    averaged H) of the same plane put through the same colocation and integration."""
+    from openem_b200 import flux_time as FT
+    sc, r = flux_time_run
+    m = sc.flux_time_monitors[0]
+    g = FT.geometry(sc.grid, m)
+    ts = r.time_samples["ftm"]
+    km = m.plane_index
+    s = r.flux_time["ft"]
+    assert s.size == ts.shape[1] == m.num_slots
+    scale = float(np.abs(s).max())
+    for q in range(0, s.size, 7):
+        F = [np.zeros(sc.shape) for _ in range(4)]
+        for c in range(4):
+            F[c][:, :, km - 1:km + 2] = ts[c, q]
+        assert abs(FT.sample(F[:2], F[2:], g) - s[q]) <= 1e-12 * scale
