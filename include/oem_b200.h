@@ -36,6 +36,20 @@ extern "C" {
 
 typedef struct oem_plan oem_plan;
 
+/* One face of a TFSF box correction (openem/kernels/tfsf.cu:49-86): for p < np, q < nq the
+ * padded cell base + p sp + q sq of field component comp (0..5) gets coef x the incident table
+ * row interpolated at column c0 + cp p + cq q (E faces also x the cell's cb). Faces of one group
+ * touch disjoint cells; groups apply in order. */
+typedef struct oem_tfsf_face {
+  int32_t comp;
+  int32_t group;
+  float coef;
+  float reserved;
+  double c0, cp, cq;
+  int64_t base, sp, sq;
+  int32_t np, nq;
+} oem_tfsf_face;
+
 /* Library version (major*10000 + minor*100 + patch) and last error text of this thread. */
 int oem_version(void);
 const char* oem_last_error(void);
@@ -167,6 +181,15 @@ int oem_plan_add_flux_time_monitor(oem_plan* p, int axis, int nplanes, const dou
                                    const double* whi2, const double* dS, int beg, int end, int iv,
                                    int nslots, int* id);
 int oem_plan_read_flux_time(oem_plan* p, int id, double* out, void* stream);
+
+/* TFSF box (openem/sources_setup.py:120-318, openem/kernels/tfsf.cu): incident tables of the 1D
+ * auxiliary line, ex_tab (ex_rows >= n_total + 1, ex_n columns) = E^n on the box edges read by
+ * the H faces after the H update of step n, hy_tab (hy_rows >= n_total, hy_n) = H^{n+1/2} on the
+ * box cells read by the E faces after the E update. Faces are grouped and ordered as described
+ * at oem_tfsf_face; H-side corrections follow the plane waves, E-side ones likewise. */
+int oem_plan_add_tfsf(oem_plan* p, int n_e, const oem_tfsf_face* e_faces, int n_h,
+                      const oem_tfsf_face* h_faces, int ex_rows, int ex_n, const double* ex_tab,
+                      int hy_rows, int hy_n, const double* hy_tab);
 
 /* Absorber boundary slab (Tidy3D's Absorber; replaces absorb_slab / absorb_batch,
  * openem/kernels/absorber.cu:20-70, absorb_batch.cu:15-110, and the host tables of

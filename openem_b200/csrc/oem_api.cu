@@ -261,6 +261,8 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
   for (const PlaneSrc& src : p->planes)
     if ((e = launch_plane_h(P, src, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "plane_h");
+  for (const Tfsf& t : p->tfsfs)
+    if ((e = launch_tfsf(P, t, 0, p->d_step, s)) != cudaSuccess) return cuda_error(e, "tfsf_h");
   for (const ModeSrc& m : p->modesrcs)
     if ((e = launch_mode_h(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_h");
   for (const Absorber& a : p->absorbers)
@@ -275,6 +277,8 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
   for (const PlaneSrc& src : p->planes)
     if ((e = launch_plane_e(P, src, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "plane_e");
+  for (const Tfsf& t : p->tfsfs)
+    if ((e = launch_tfsf(P, t, 1, p->d_step, s)) != cudaSuccess) return cuda_error(e, "tfsf_e");
   for (const ModeSrc& m : p->modesrcs)
     if ((e = launch_mode_e(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_e");
   for (const DipoleSet& d : p->dipoles)
@@ -1126,6 +1130,58 @@ int oem_plan_read_flux_time(oem_plan* p, int id, double* out, void* stream) {
   return check_device_error(p);
 }
 
+static int tfsf_side(oem_plan* p, int n, const oem_tfsf_face* faces, oem_tfsf_face** dfaces,
+                     int64_t** dofs, std::vector<std::pair<int, int>>& groups,
+                     std::vector<int64_t>& points) {
+  int rc;
+  const int64_t ncp = (int64_t)p->nx * p->ny * p->nzp;
+  std::vector<int64_t> ofs;
+  for (int f = 0; f < n; ++f) {
+    const oem_tfsf_face& F = faces[f];
+    if (F.comp < 0 || F.comp > 5 || F.np < 0 || F.nq < 0)
+      return set_error(OEM_ERR_INVALID, "bad TFSF face");
+    if (F.np > 0 && F.nq > 0) {
+      const int64_t last = F.base + (int64_t)(F.np - 1) * F.sp + (int64_t)(F.nq - 1) * F.sq;
+      if (F.base < 0 || last < 0 || F.base >= ncp || last >= ncp)
+        return set_error(OEM_ERR_INVALID, "TFSF face outside the grid");
+    }
+    if (f > 0 && F.group < faces[f - 1].group)
+      return set_error(OEM_ERR_INVALID, "TFSF faces must be ordered by group");
+    if (f == 0 || F.group != faces[f - 1].group) {
+      groups.push_back({f, 0});
+      points.push_back(0);
+      ofs.push_back(0);
+    }
+    groups.back().second += 1;
+    points.back() += (int64_t)F.np * F.nq;
+    ofs.push_back(points.back());
+  }
+  if (n == 0) return OEM_OK;
+  if ((rc = dupload(p, dfaces, faces, (size_t)n))) return rc;
+  if ((rc = dupload(p, dofs, ofs.data(), ofs.size()))) return rc;
+  return OEM_OK;
+}
+
+int oem_plan_add_tfsf(oem_plan* p, int n_e, const oem_tfsf_face* e_faces, int n_h,
+                      const oem_tfsf_face* h_faces, int ex_rows, int ex_n, const double* ex_tab,
+                      int hy_rows, int hy_n, const double* hy_tab) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (p->is_complex) return set_error(OEM_ERR_UNSUPPORTED, "TFSF boxes on a complex plan");
+  if (n_e < 0 || n_h < 0 || (n_e && !e_faces) || (n_h && !h_faces) || !ex_tab || !hy_tab ||
+      ex_rows < 1 || ex_n < 1 || hy_rows < 1 || hy_n < 1)
+    return set_error(OEM_ERR_INVALID, "bad TFSF tables");
+  if ((rc = use_device(p))) return rc;
+  Tfsf t;
+  if ((rc = tfsf_side(p, n_e, e_faces, &t.e_faces, &t.e_ofs, t.e_groups, t.e_points))) return rc;
+  if ((rc = tfsf_side(p, n_h, h_faces, &t.h_faces, &t.h_ofs, t.h_groups, t.h_points))) return rc;
+  t.ex_rows = ex_rows; t.ex_n = ex_n; t.hy_rows = hy_rows; t.hy_n = hy_n;
+  if ((rc = dupload(p, &t.ex_tab, ex_tab, (size_t)ex_rows * ex_n))) return rc;
+  if ((rc = dupload(p, &t.hy_tab, hy_tab, (size_t)hy_rows * hy_n))) return rc;
+  p->tfsfs.push_back(std::move(t));
+  return OEM_OK;
+}
+
 int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   int rc = check_plan(p, false);
   if (rc) return rc;
@@ -1145,6 +1201,9 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
     if (m.n_total < n_total) return set_error(OEM_ERR_INVALID, "phase table shorter than the run");
   for (const Modulation& m : p->mods)
     if (m.ntab < n_total) return set_error(OEM_ERR_INVALID, "modulation table shorter than the run");
+  for (const Tfsf& t : p->tfsfs)
+    if (t.ex_rows < n_total + 1 || t.hy_rows < n_total)
+      return set_error(OEM_ERR_INVALID, "TFSF incident table shorter than the run");
   if (!p->mods.empty() && !p->dev_index) {
     // every modulated cell owns its material record: the kernel rewrites it in place
     std::vector<int64_t> owner(p->mats.size(), -1);
@@ -1355,6 +1414,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
           return cuda_error(e, "dipoles_h");
       for (const PlaneSrc& src : p->planes)
         if ((e = launch_plane_h(p->yp, src, p->d_step, s)) != cudaSuccess) return cuda_error(e, "plane_h");
+      for (const Tfsf& t : p->tfsfs)
+        if ((e = launch_tfsf(p->yp, t, 0, p->d_step, s)) != cudaSuccess) return cuda_error(e, "tfsf_h");
       for (const ModeSrc& m : p->modesrcs)
         if ((e = launch_mode_h(p->yp, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_h");
       for (const Absorber& a : p->absorbers)
@@ -1375,6 +1436,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       OEM_CUDA(cudaEventRecord(E[3], s));
       for (const PlaneSrc& src : p->planes)
         if ((e = launch_plane_e(p->yp, src, p->d_step, s)) != cudaSuccess) return cuda_error(e, "plane_e");
+      for (const Tfsf& t : p->tfsfs)
+        if ((e = launch_tfsf(p->yp, t, 1, p->d_step, s)) != cudaSuccess) return cuda_error(e, "tfsf_e");
       for (const ModeSrc& m : p->modesrcs)
         if ((e = launch_mode_e(p->yp, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_e");
       for (const DipoleSet& d : p->dipoles)
@@ -1470,6 +1533,7 @@ int oem_plan_launches_per_step(oem_plan* p, int* n) {
   c += 2 * (int)p->tmons.size();
   c += 3 * (int)p->mons.size();  // snapshot, flush, flush mark
   c += 2 * (int)p->ftmons.size();
+  for (const Tfsf& t : p->tfsfs) c += (int)(t.e_groups.size() + t.h_groups.size());
   *n = c;
   return OEM_OK;
 }

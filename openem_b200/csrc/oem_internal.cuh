@@ -207,6 +207,20 @@ struct FluxTimeMon {
   int beg = 0, end = 0, iv = 1, slots = 0;
 };
 
+// TFSF box: faces (device copies) and the two incident tables; one launch per face group.
+struct Tfsf {
+  oem_tfsf_face* e_faces = nullptr;
+  oem_tfsf_face* h_faces = nullptr;
+  std::vector<std::pair<int, int>> e_groups, h_groups;  // [first face, count) per group
+  std::vector<int64_t> e_points, h_points;             // points per group
+  std::vector<std::vector<int64_t>> e_ofs_h, h_ofs_h;  // host prefix offsets per group
+  int64_t* e_ofs = nullptr;                            // device prefix offsets, per face + 1
+  int64_t* h_ofs = nullptr;
+  double* ex_tab = nullptr;
+  double* hy_tab = nullptr;
+  int ex_rows = 0, ex_n = 0, hy_rows = 0, hy_n = 0;
+};
+
 struct TimeMon {
   int nc = 0;
   int comps[6] = {0, 0, 0, 0, 0, 0};
@@ -266,6 +280,7 @@ struct oem_plan {
   std::vector<oem::Monitor> mons;
   std::vector<oem::TimeMon> tmons;
   std::vector<oem::FluxTimeMon> ftmons;
+  std::vector<oem::Tfsf> tfsfs;
 
   // device state
   std::vector<void*> allocs;
@@ -376,6 +391,8 @@ cudaError_t launch_modulate(const YeeParams& P, const Modulation& m, const int* 
                             cudaStream_t s);
 cudaError_t launch_flux_time(const YeeParams& P, const FluxTimeMon& m, const int* step,
                              cudaStream_t s);
+cudaError_t launch_tfsf(const YeeParams& P, const Tfsf& t, int is_e, const int* step,
+                        cudaStream_t s);
 
 // Discrete adjoint (oem_adjoint.cu): adjoint fields, their CPML psi, scratch for the transposed
 // differences, and the gradient accumulators of ca and cb per component.

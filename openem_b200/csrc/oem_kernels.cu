@@ -728,6 +728,59 @@ cudaError_t launch_flux_time(const YeeParams& P, const FluxTimeMon& m, const int
   return cudaGetLastError();
 }
 
+// TFSF box face corrections (openem/kernels/tfsf.cu:31-86): one thread per point of a group of
+// faces that touch disjoint cells; the table row of the step interpolated at the point's column.
+__global__ void k_tfsf(YeeParams P, const oem_tfsf_face* faces, const int64_t* ofs, int nfaces,
+                       int64_t total, const double* tab, int rows, int row_n, const int* step,
+                       int is_e) {
+  const int n = *step;
+  if (n < 0 || n >= rows) return;
+  const double* row = tab + (int64_t)n * row_n;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int f = 0;
+    while (f + 1 < nfaces && t >= ofs[f + 1]) ++f;
+    const oem_tfsf_face& F = faces[f];
+    const int64_t r = t - ofs[f];
+    const int p = (int)(r / F.nq), q = (int)(r - (int64_t)p * F.nq);
+    const double pos = F.c0 + F.cp * (double)p + F.cq * (double)q;
+    int i0 = (int)floor(pos);
+    double w = pos - (double)i0;
+    if (i0 < 0) { i0 = 0; w = 0.0; }
+    else if (i0 >= row_n - 1) { i0 = row_n - 1; w = 0.0; }
+    const int i1 = i0 + 1 < row_n ? i0 + 1 : i0;
+    const float val = (float)(row[i0] + w * (row[i1] - row[i0]));
+    const int64_t id = F.base + (int64_t)p * F.sp + (int64_t)q * F.sq;
+    float* Fd = P.f[F.comp];
+    if (is_e) {
+      const float cb = P.mats[mat_id(P, id)].cb[F.comp];
+      Fd[id] = __fadd_rn(Fd[id], __fmul_rn(__fmul_rn(cb, F.coef), val));
+    } else {
+      Fd[id] = __fadd_rn(Fd[id], __fmul_rn(F.coef, val));
+    }
+  }
+}
+
+cudaError_t launch_tfsf(const YeeParams& P, const Tfsf& t, int is_e, const int* step,
+                        cudaStream_t s) {
+  const auto& groups = is_e ? t.e_groups : t.h_groups;
+  const auto& points = is_e ? t.e_points : t.h_points;
+  const oem_tfsf_face* faces = is_e ? t.e_faces : t.h_faces;
+  const int64_t* ofs = is_e ? t.e_ofs : t.h_ofs;
+  for (size_t g = 0; g < groups.size(); ++g) {
+    const int64_t total = points[g];
+    if (total <= 0) continue;
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 8);
+    const int first = groups[g].first;
+    k_tfsf<<<blocks, 256, 0, s>>>(P, faces + first, ofs + first + (int64_t)g, groups[g].second,
+                                  total, is_e ? t.hy_tab : t.ex_tab, is_e ? t.hy_rows : t.ex_rows,
+                                  is_e ? t.hy_n : t.ex_n, step, is_e);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* step,
                             cudaStream_t s) {
   if (m.kind == 0) {

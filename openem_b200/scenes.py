@@ -20,8 +20,8 @@ import numpy as np
 
 from openem_b200.model import (
     C_0, EPSILON_0, ETA_0, Axis, Dispersion, FieldMonitor, FieldTimeMonitor, FluxMonitor,
-    FluxTimeMonitor, GaussianPulse, Grid, ModeSource, PlaneWaveSource, PMLParams, PointDipole, Scene,
-    TimeModulation, pml_build, sample_waveform)
+    FluxTimeMonitor, GaussianPulse, Grid, ModeSource, PlaneWaveSource, PMLParams, PointDipole,
+    Scene, TFSFSource, TimeModulation, pml_build, sample_waveform)
 
 UM = 1e-6
 
@@ -295,6 +295,87 @@ def flux_time_plane(nxy: int = 16, dl: float = 0.025 * UM, plane_z: float = 0.3 
                           num_slots=slots)
     from dataclasses import replace
     return replace(base, flux_monitors=[fx], flux_time_monitors=[ft], field_time_monitors=[tm])
+
+
+def tfsf_source(grid: Grid, dt: float, num_steps: int, eps_u: np.ndarray, box_lo, box_hi,
+                axis: int = 2, direction: int = 1, pol=(1.0, 0.0), source_time=None,
+                sigma_u: np.ndarray | None = None) -> TFSFSource:
+    """A normal-incidence TFSF box source: the 1D auxiliary line copies the spacing of the box
+    column (4 cells beyond each face) with a runway at both ends, its permittivity from the
+    u-component profile at the box corner column, the injection point 2 cells outside the
+    entry face, and incident tables with the wave impedance there
+    (``openem/scene/sources.py:999-1232``). ``pol`` = (beta_u, beta_v) on the cyclic transverse
+    axes u = (axis+1) % 3, v = (axis+2) % 3."""
+    from openem_b200 import tfsf as TF
+    a = axis
+    u, v = TF.cyclic_axes(a)
+    lo, hi = [int(x) for x in box_lo], [int(x) for x in box_hi]
+    alo, ahi = lo[a], hi[a]
+    c0, c1 = alo - TF.GAP, ahi + TF.GAP - 1
+    na = grid.shape[a]
+    if c0 < 0 or c1 > na - 1:
+        raise ValueError(f"the TFSF box column [{c0}, {c1}] runs past the axis (n={na})")
+    dl_col = np.asarray(grid.axes[a].dl, np.float64)[c0:c1 + 1]
+
+    def column(arr):
+        col = np.moveaxis(np.asarray(arr, np.float64), (u, v, a), (0, 1, 2))[lo[u], lo[v], :]
+        return col[c0:c1 + 2] if c1 + 1 < col.size else np.concatenate([col[c0:], [col[-1]]])
+    n_lo = TF.runway_cells(num_steps, dt, float(dl_col[0]))
+    n_hi = TF.runway_cells(num_steps, dt, float(dl_col[-1]))
+    dl1 = np.concatenate([np.full(n_lo, dl_col[0]), dl_col, np.full(n_hi, dl_col[-1])])
+    seg = column(eps_u)
+    eps1 = np.concatenate([np.full(n_lo, seg[0]), seg, np.full(n_hi - 1, seg[-1])])
+    sigma1 = None
+    if sigma_u is not None:
+        sg = column(sigma_u)
+        if np.abs(sg).max() > 0:
+            sigma1 = np.concatenate([np.full(n_lo, sg[0]), sg, np.full(n_hi - 1, sg[-1])])
+    col0 = n_lo + (alo - c0)
+    inj = col0 - TF.GAP // 2 if direction > 0 else n_lo + (ahi - c0) + TF.GAP // 2
+    kh1 = inj - 1 if direction > 0 else inj
+    pulse = source_time or GaussianPulse(freq0=3e14, fwidth=1e14)
+    ex_inc, hy_inc = plane_wave_tables(pulse, dt, num_steps, 0.5 * float(dl1[kh1]),
+                                       float(eps1[inj]), direction)
+    return TFSFSource(direction=direction, box_lo=tuple(lo), box_hi=tuple(hi), dl1=dl1,
+                      eps1=eps1, inj=int(inj), col0=int(col0), ex_inc=ex_inc, hy_inc=hy_inc,
+                      waveform=sample_waveform(pulse, dt, num_steps), axis=a,
+                      pol_u=float(pol[0]), pol_v=float(pol[1]), sigma1=sigma1)
+
+
+def tfsf_box_scene(n: int = 40, n_pml: int = 8, dl: float = 0.02 * UM, axis: int = 2,
+                   direction: int = 1, pol=(1.0, 0.0), margin: int = 5, sphere_eps: float = 0.0,
+                   sphere_r: float = 0.1 * UM, substrate_eps: float = 0.0,
+                   num_steps: int = 300) -> Scene:
+    """An n^3 grid with CPML on every face and a TFSF box ``margin`` cells inside the CPML; a
+    dielectric sphere at the centre (``sphere_eps`` > 0), a substrate filling the lower half
+    along ``axis`` (``substrate_eps`` > 0, transversely uniform so it crosses the box), and a
+    normal-incidence pulse along ``axis`` with polarisation ``pol`` on (u, v)."""
+    n_in = n - 2 * n_pml
+    axes = [uniform_axis(n_in, dl, -0.5 * n_in * dl, "PML", n_pml) for _ in range(3)]
+    grid = Grid(*axes)
+    dt = courant_dt([ax.dl for ax in axes])
+    coords = yee_coords(grid)
+    eps = []
+    for c in range(3):
+        x, y, z = coords[c]
+        e = np.ones(grid.shape)
+        if substrate_eps > 0:
+            w = (x, y, z)[axis]
+            sl = [slice(None)] * 3
+            sl[axis] = w < -2.0 * dl
+            e[tuple(sl)] = substrate_eps
+        if sphere_eps > 0:
+            r2 = x[:, None, None] ** 2 + y[None, :, None] ** 2 + z[None, None, :] ** 2
+            e[r2 < sphere_r ** 2] = sphere_eps
+        eps.append(e)
+    lo = (n_pml + margin,) * 3
+    hi = (n - n_pml - margin,) * 3
+    u = (axis + 1) % 3
+    src = tfsf_source(grid, dt, num_steps, eps[u], lo, hi, axis=axis, direction=direction,
+                      pol=pol)
+    return Scene(grid=grid, dt=dt, num_time_steps=num_steps, shutoff=1e-5, eps_ex=eps[0],
+                 eps_ey=eps[1], eps_ez=eps[2], pml=pml_dict(grid, dt, n_pml),
+                 tfsf_sources=[src])
 
 
 def slab_transmission(res_slab, res_empty, name: str = "T") -> np.ndarray:

@@ -30,8 +30,10 @@ COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 def refuse_unsupported(sc) -> None:
     """Fail closed on scene features outside this engine's real-field path."""
     checks = [
-        (bool(getattr(sc, "tfsf_sources", None)), "TFSF box sources"),
         (T.dispersion_in_absorbers(sc), "dispersive media inside Absorber layers"),
+        (any(getattr(t, "k_hat", None) is not None or getattr(t, "open_axes", ())
+             for t in getattr(sc, "tfsf_sources", [])), "oblique or open-axis TFSF boxes"),
+        (len(getattr(sc, "tfsf_sources", [])) > 1, "several TFSF boxes in one scene"),
         (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry > 0,
          "slanted-interface mixed dispersion"),
         (sc.tensor is not None and sc.tensor.n_entry > 0, "fully anisotropic media"),
@@ -196,6 +198,17 @@ class Plan:
                 h, ps["pol"], ps["kh"], ps["ks"], ps["coef_h"], ps["coef_e"], int(ps["ex"].size),
                 L.ptr(self._arr(ps["ex"], np.float64)), L.ptr(self._arr(ps["hy"], np.float64))),
                 "add_plane_source")
+        if getattr(sc, "tfsf_sources", None) and not self.cplx:
+            from openem_b200 import tfsf as TF
+            tb = TF.box_tables(sc, self.n_total)
+            nzp = T.pad_z(self.shape[2])
+            ef = self._arr(TF.device_faces(tb["e_faces"], self.shape[1], nzp), TF.FACE_DTYPE)
+            hf = self._arr(TF.device_faces(tb["h_faces"], self.shape[1], nzp), TF.FACE_DTYPE)
+            ex, hy = self._arr(tb["ex_tab"], np.float64), self._arr(tb["hy_tab"], np.float64)
+            L.check(lib.oem_plan_add_tfsf(h, int(ef.size), L.ptr(ef), int(hf.size), L.ptr(hf),
+                                          int(ex.shape[0]), int(ex.shape[1]), L.ptr(ex),
+                                          int(hy.shape[0]), int(hy.shape[1]), L.ptr(hy)),
+                    "add_tfsf")
         for mag in (False, True):
             dt_ = T.dipole_tables(sc, self.n_total, mag, complex_amp=self.cplx)
             if dt_ is None:

@@ -125,9 +125,6 @@ class Oracle:
     def __init__(self, sc, n_total: int | None = None):
         if sc.any_bloch:
             raise ValueError("use BlochOracle for a scene with a non-zero Bloch vector")
-        for feat in ("tfsf_sources",):
-            if getattr(sc, feat, None):
-                raise NotImplementedError(f"oracle: {feat} not transcribed")
         if sc.any_dispersion_mix or sc.any_tensor:
             raise NotImplementedError("oracle: mix / tensor not transcribed")
         self.sc = sc
@@ -155,6 +152,7 @@ class Oracle:
         self._setup_dispersion()
         self._setup_modulation()
         self._setup_sources()
+        self._setup_tfsf()
         self._setup_monitors()
         self.n = 0
 
@@ -198,6 +196,116 @@ class Oracle:
             m = md["comp"] == c
             self.ca[c].ravel()[md["cell"][m]] = ((e0 - md["sd"]) / den)[m]
             self.cb[c].ravel()[md["cell"][m]] = ((dt / EPSILON_0) / den)[m]
+
+    def _setup_tfsf(self):
+        """TFSF box at normal incidence: the 1D auxiliary line (openem/tfsf1d.py:297-325, run
+        over the whole line here) and the box geometry (openem/sources_setup.py:120-233)."""
+        sc = self.sc
+        self.tfsf = None
+        if not getattr(sc, "tfsf_sources", None):
+            return
+        t = sc.tfsf_sources[0]
+        if getattr(t, "k_hat", None) is not None:
+            raise NotImplementedError("oracle: oblique TFSF not transcribed")
+        a = int(t.axis)
+        lo, hi = [int(x) for x in t.box_lo], [int(x) for x in t.box_hi]
+        nk = hi[a] - lo[a] + 1
+        dl1 = np.asarray(t.dl1, np.float64)
+        eps1 = np.asarray(t.eps1, np.float64)
+        n1 = dl1.size
+        dld1 = np.concatenate([[dl1[0]], 0.5 * (dl1[1:] + dl1[:-1])])
+        dt = sc.dt
+        s1 = (np.zeros(n1) if t.sigma1 is None
+              else np.asarray(t.sigma1, np.float64) * dt / (2 * EPSILON_0))
+        ca1 = (eps1 - s1) / (eps1 + s1)
+        cb1 = dt / EPSILON_0 / (eps1 + s1) / dld1
+        ch1 = dt / MU_0 / dl1
+        d = int(t.direction)
+        inj = int(t.inj)
+        kh = inj - 1 if d > 0 else inj
+        sgn = _SIGNS[d]
+        scale = float(getattr(t, "amp_scale", 1.0))
+        ch_inj = sgn[0] * dt / MU_0 / dl1[kh]
+        ce_inj = sgn[1] * dt / EPSILON_0 / (eps1[inj] + s1[inj]) / dld1[inj]
+        col0 = int(t.col0)
+        e1, h1 = np.zeros(n1), np.zeros(n1)
+        ex_tab = np.zeros((self.n_total + 1, nk))
+        hy_tab = np.zeros((self.n_total, nk + 1))
+        for n in range(self.n_total):
+            h1[:-1] -= ch1[:-1] * (e1[1:] - e1[:-1])
+            h1[kh] += ch_inj * scale * float(t.ex_inc[n])
+            hy_tab[n] = h1[col0 - 1:col0 + nk]
+            e1[1:] = ca1[1:] * e1[1:] - cb1[1:] * (h1[1:] - h1[:-1])
+            e1[inj] += ce_inj * scale * float(t.hy_inc[n])
+            ex_tab[n + 1] = e1[col0:col0 + nk]
+        self.tfsf = {"t": t, "a": a, "lo": lo, "hi": hi, "nk": nk, "ex": ex_tab, "hy": hy_tab}
+
+    def inject_tfsf(self, side, n):
+        """The box-face corrections of step n (the 16 terms of
+        openem/sources_setup.py:236-272): H side with row E^n, E side (times cb) with row
+        H^{n+1/2}."""
+        tf = getattr(self, "tfsf", None)  # the complex path has no TFSF box
+        if tf is None:
+            return
+        t, a, lo, hi, nk = tf["t"], tf["a"], tf["lo"], tf["hi"], tf["nk"]
+        u, v = (a + 1) % 3, (a + 2) % 3
+        bu, bv = float(t.pol_u), float(t.pol_v)
+        dl = [np.asarray(ax.dl, np.float64) for ax in self.sc.grid.axes]
+        dld = [np.asarray(ax.dl_dual, np.float64) for ax in self.sc.grid.axes]
+
+        def region(fixed_ax, fixed_idx, p_ax, p_end, q_ax, q_end):
+            sl = [None, None, None]
+            sl[fixed_ax] = fixed_idx
+            sl[p_ax] = slice(lo[p_ax], p_end)
+            sl[q_ax] = slice(lo[q_ax], q_end)
+            return tuple(sl)
+
+        def col_along_a(vals, q_ax, p_ax):
+            # table values along a broadcast over the face (p_ax, q_ax order of the slice)
+            shape = [1, 1]
+            order = sorted([p_ax, q_ax])
+            shape[order.index(a)] = -1
+            return vals.reshape(shape)
+
+        if side == "h":
+            row = tf["ex"][n]
+            ch = self.ch
+            H = self.H
+            if bu:
+                H[v][region(a, lo[a] - 1, u, hi[u], v, hi[v] + 1)] += bu * ch / dl[a][lo[a] - 1] * row[0]
+                H[v][region(a, hi[a], u, hi[u], v, hi[v] + 1)] -= bu * ch / dl[a][hi[a]] * row[nk - 1]
+            if bv:
+                H[u][region(a, lo[a] - 1, u, hi[u] + 1, v, hi[v])] -= bv * ch / dl[a][lo[a] - 1] * row[0]
+                H[u][region(a, hi[a], u, hi[u] + 1, v, hi[v])] += bv * ch / dl[a][hi[a]] * row[nk - 1]
+            ra = row[:nk]
+            if bu:
+                for idx, sg in ((lo[v] - 1, -1.0), (hi[v], 1.0)):
+                    r = region(v, idx, u, hi[u], a, hi[a] + 1)
+                    H[a][r] += sg * bu * ch / dl[v][idx] * col_along_a(ra, a, u)
+            if bv:
+                for idx, sg in ((lo[u] - 1, 1.0), (hi[u], -1.0)):
+                    r = region(u, idx, v, hi[v], a, hi[a] + 1)
+                    H[a][r] += sg * bv * ch / dl[u][idx] * col_along_a(ra, a, v)
+        else:
+            row = tf["hy"][n]
+            E, cb = self.E, self.cb
+            if bu:
+                for idx, sg, col in ((lo[a], 1.0, 0), (hi[a], -1.0, nk)):
+                    r = region(a, idx, u, hi[u], v, hi[v] + 1)
+                    E[u][r] += cb[u][r] * sg * bu / dld[a][idx] * row[col]
+            if bv:
+                for idx, sg, col in ((lo[a], 1.0, 0), (hi[a], -1.0, nk)):
+                    r = region(a, idx, u, hi[u] + 1, v, hi[v])
+                    E[v][r] += cb[v][r] * sg * bv / dld[a][idx] * row[col]
+            ra = row[1:nk]
+            if bu:
+                for idx, sg in ((lo[u], -1.0), (hi[u], 1.0)):
+                    r = region(u, idx, v, hi[v] + 1, a, hi[a])
+                    E[a][r] += cb[a][r] * sg * bu / dld[u][idx] * col_along_a(ra, a, v)
+            if bv:
+                for idx, sg in ((lo[v], -1.0), (hi[v], 1.0)):
+                    r = region(v, idx, u, hi[u] + 1, a, hi[a])
+                    E[a][r] += cb[a][r] * sg * bv / dld[v][idx] * col_along_a(ra, a, u)
 
     def _setup_dispersion(self):
         d = self.sc.dispersion
@@ -442,6 +550,7 @@ class Oracle:
         for p in self.pw:
             Ht = self.H[1] if p["pol"] == 0 else self.H[0]
             Ht[:, :, p["kh"]] += p["coef_h"] * p["ex"][n]
+        self.inject_tfsf("h", n)
         self.inject_mode_h(n)
 
     def disp_pre(self):
@@ -491,6 +600,7 @@ class Oracle:
         for p in self.pw:
             c = p["pol"]
             self.E[c][:, :, p["ks"]] += self.cb[c][:, :, p["ks"]] * p["coef_e"] * p["hy"][n]
+        self.inject_tfsf("e", n)
         self.inject_mode_e(n)
         if self.dip_e is not None:
             for c, i, j, k, cf, s in self.dip_e["pts"]:

@@ -1,0 +1,52 @@
+"""TFSF box on the GPU: the empty-box criterion (inside equals the 1D line, outside only
+float32 rounding leaks) and scatterers against the FP64 oracle (fields within 1e-5 of their
+family's norm) on several injection axes, directions, polarisations and a crossing substrate."""
+
+import numpy as np
+import pytest
+
+from oracle import ref64
+from openem_b200 import scenes, solver
+from openem_b200 import tfsf as TF
+
+pytestmark = pytest.mark.gpu
+
+
+def family_err(fa, fb, names):
+    den = np.sqrt(sum(float(np.linalg.norm(np.asarray(fb[n]).ravel())) ** 2 for n in names))
+    return max(float(np.linalg.norm((np.asarray(fa[n]) - np.asarray(fb[n])).ravel()))
+               for n in names) / max(den, 1e-300)
+
+
+@pytest.mark.parametrize("axis,direction,pol", [(2, 1, (1.0, 0.0)), (0, -1, (0.6, 0.8))])
+def test_empty_tfsf_box_on_gpu(axis, direction, pol):
+    steps = 260
+    sc = scenes.tfsf_box_scene(n=40, axis=axis, direction=direction, pol=pol, num_steps=steps)
+    t = sc.tfsf_sources[0]
+    g = solver.run(sc, use_shutoff=False, return_fields=True, verbose=False)
+    tb = TF.box_tables(sc, steps)
+    row = tb["ex_tab"][steps]
+    scale = float(np.abs(row).max())
+    u, v = TF.cyclic_axes(axis)
+    lo, hi = t.box_lo, t.box_hi
+    names = ("Ex", "Ey", "Ez")
+    for comp, beta in ((u, pol[0]), (v, pol[1])):
+        F = np.moveaxis(g.fields[names[comp]], (u, v, axis), (0, 1, 2)).astype(np.float64)
+        cu, cv = (0, 1) if comp == u else (1, 0)
+        ins = F[lo[u]:hi[u] + cu, lo[v]:hi[v] + cv, lo[axis]:hi[axis] + 1]
+        assert np.abs(ins - beta * row[None, None, :]).max() <= 2e-5 * scale
+    for nm in names:
+        F = g.fields[nm].astype(np.float64)
+        F[tuple(slice(lo[q] - 1, hi[q] + 2) for q in range(3))] = 0.0
+        assert np.abs(F).max() <= 2e-6 * scale, nm
+
+
+@pytest.mark.parametrize("kw", [dict(axis=2, direction=1, pol=(1.0, 0.0), sphere_eps=6.0),
+                                dict(axis=1, direction=-1, pol=(0.8, -0.6), sphere_eps=4.0,
+                                     substrate_eps=2.25)])
+def test_tfsf_scatterer_matches_oracle(kw):
+    sc = scenes.tfsf_box_scene(n=40, num_steps=300, **kw)
+    r = ref64.run(sc)
+    g = solver.run(sc, use_shutoff=False, return_fields=True, verbose=False)
+    for fam in (("Ex", "Ey", "Ez"), ("Hx", "Hy", "Hz")):
+        assert family_err(g.fields, r.fields, fam) < 1e-5

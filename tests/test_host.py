@@ -124,7 +124,8 @@ def test_unsupported_physics_fails_closed(feature):
     sc = scenes.slab_plane_wave(nxy=1, num_steps=10)
     sd = scenes.small_dispersive(n=20, n_sph=1, n_pml=4, num_steps=10)
     bad = {
-        "tfsf": replace(sc, tfsf_sources=[object()]),
+        "tfsf": replace(sc, tfsf_sources=[replace(
+            scenes.tfsf_box_scene(n=30, num_steps=10).tfsf_sources[0], k_hat=(0.0, 0.5, 0.87))]),
         "disp_in_absorber": replace(sd, absorbers=scenes.absorber_slabs(sd.grid, 0, 10)),
         "modulation_pec": replace(sc, pec_ex=np.array([5]), modulation=M.TimeModulation(
             1e14, np.array([0]), np.array([0]), np.array([0.1]), np.array([0.0]))),

@@ -315,3 +315,54 @@ def test_oracle_flux_time_equals_time_monitor_samples(flux_time_run):
         for c in range(4):
             F[c][:, :, km - 1:km + 2] = ts[c, q]
         assert abs(FT.sample(F[:2], F[2:], g) - s[q]) <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("tag", ["ll", "ls"])
+def test_tfsf_line_tables_match_reference(tag):
+    """The engine's 1D auxiliary line (causal window on) reproduces OpenEM's tfsf1d.tables on
+    the lossless-slab and lossy profiles."""
+    from openem_b200 import tfsf as TF
+    z = np.load(GOLD / "ref_tfsf1d.npz")
+    sig = z[f"{tag}_sigma1"]
+    ex, hy = TF.line_tables(z[f"{tag}_dl1"], z[f"{tag}_eps1"], float(z["dt"]), int(z["inj"]), 1,
+                            z[f"{tag}_ex_inc"], z[f"{tag}_hy_inc"], int(z["n_steps"]),
+                            int(z["col0"]), int(z["n_col_e"]),
+                            sigma1=sig if np.any(sig) else None)
+    np.testing.assert_allclose(ex, z[f"{tag}_ex_tab"], rtol=0, atol=1e-15 * np.abs(ex).max())
+    np.testing.assert_allclose(hy, z[f"{tag}_hy_tab"], rtol=0, atol=1e-15 * np.abs(hy).max())
+
+
+@pytest.mark.parametrize("axis,direction,pol,sub", [
+    (2, 1, (1.0, 0.0), 0.0), (0, -1, (0.6, 0.8), 0.0), (1, 1, (0.0, 1.0), 2.25)])
+def test_oracle_empty_tfsf_box(axis, direction, pol, sub):
+    """OpenEM's TFSF criterion (openem/sources_setup.py:244-248): with nothing inside the box the
+    total field inside equals the polarisation component times the 1D line at every point, and
+    outside the box only rounding leaks (here float64). A substrate that crosses the box is
+    carried by the line itself."""
+    from openem_b200 import tfsf as TF
+    n = 36
+    sc = scenes.tfsf_box_scene(n=n, axis=axis, direction=direction, pol=pol, substrate_eps=sub,
+                               num_steps=220)
+    t = sc.tfsf_sources[0]
+    r = ref64.run(sc)
+    tb = TF.box_tables(sc, 220)
+    a = axis
+    u, v = TF.cyclic_axes(a)
+    lo, hi = t.box_lo, t.box_hi
+    row = tb["ex_tab"][220]
+    scale = float(np.abs(row).max())
+    assert scale > 0
+    names = ("Ex", "Ey", "Ez")
+    for comp, beta in ((u, pol[0]), (v, pol[1])):
+        F = np.moveaxis(r.fields[names[comp]], (u, v, a), (0, 1, 2))
+        lo_t = [lo[u], lo[v], lo[a]]
+        hi_t = [hi[u], hi[v], hi[a]]
+        # E_u sits at u cells / v edges / a edges; E_v at u edges / v cells / a edges
+        cu = 0 if comp == u else 1
+        cv = 1 if comp == u else 0
+        ins = F[lo_t[0]:hi_t[0] + cu, lo_t[1]:hi_t[1] + cv, lo_t[2]:hi_t[2] + 1]
+        assert np.abs(ins - beta * row[None, None, :]).max() <= 1e-12 * scale
+    for nm in names:
+        F = r.fields[nm].copy()
+        F[tuple(slice(lo[q] - 1, hi[q] + 2) for q in range(3))] = 0.0
+        assert np.abs(F).max() <= 1e-12 * scale, nm
