@@ -244,7 +244,8 @@ def run_ours(args):
     # roofline of the dominant kernel
     kb = roofline.kernel_bytes(sc)
     peaks = roofline.measured_peaks(ROOT)
-    dom = max(("update_h", "update_e"), key=lambda k: tm[k][1])
+    dom = max((k for k in ("update_he", "update_h", "update_e") if k in tm),
+              key=lambda k: tm[k][1])
     t_launch = tm[dom][1] / tm[dom][0] * 1e-3
     achieved = kb[dom] / t_launch / 1e9
     traffic = None

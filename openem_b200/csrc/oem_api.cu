@@ -223,6 +223,42 @@ int make_tma_maps(oem_plan* p) {
   return encode_map(p, &p->tma.m_tile, P.mat32, false, true, 128, 4);
 }
 
+// Tensor maps of the fused kernel reading bank b.
+static int make_fused_maps(oem_plan* p, int b) {
+  int rc;
+  FusedMaps& m = p->fmaps[b];
+  for (int c = 0; c < 3; ++c) {
+    if ((rc = encode_map(p, &m.e6[c], p->bank_f[b][c], false, false, 136, 6))) return rc;
+    if ((rc = encode_map(p, &m.h5[c], p->bank_f[b][3 + c], false, false, 128, 5))) return rc;
+  }
+  for (int c = 0; c < 2; ++c)
+    if ((rc = encode_map(p, &m.e5[c], p->bank_f[b][1 + c], false, false, 128, 5))) return rc;
+  const YeeParams& P = p->yp;
+  if (P.mat16) return encode_map(p, &m.m, P.mat16, true, false, 128, 4);
+  return encode_map(p, &m.m, P.mat32, false, true, 128, 4);
+}
+
+// The fused step applies when the warp-specialised kernels run on a real plan whose y and z axes
+// do not wrap and nothing is injected on the H side.
+static bool fused_eligible(oem_plan* p) {
+  if (!p->want_fused || p->basic_kernels != 3 || p->is_complex) return false;
+  if (!p->planes.empty() || !p->modesrcs.empty() || !p->tfsfs.empty() || !p->absorbers.empty())
+    return false;
+  for (const DipoleSet& d : p->dipoles)
+    if (d.magnetic) return false;
+  for (int a = 1; a < 3; ++a) {
+    const AxisHost& h = p->axh[a];
+    const int n = (int)h.prv.size();
+    if (n < 1 || h.prv[0] != 0) return false;  // periodic wrap at the low end
+    for (int q = 1; q < n; ++q)
+      if (h.prv[q] != q - 1) return false;
+  }
+  const AxisHost& x = p->axh[0];
+  for (int q = 1; q < (int)x.prv.size(); ++q)
+    if (x.prv[q] != q - 1) return false;
+  return true;
+}
+
 // Non-zero when a kernel's bounded wait gave up since the last check.
 static int check_device_error(oem_plan* p) {
   int h = 0;
@@ -237,9 +273,36 @@ static int check_device_error(oem_plan* p) {
 }
 
 // One time step (openem/solver.py:1145-1162).
+static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors);
+
+// The current field bank becomes b: every kernel enqueued afterwards (sources, monitors,
+// readouts) reads and writes that bank.
+static void set_bank(oem_plan* p, int b) {
+  p->bank = b;
+  for (int c = 0; c < 6; ++c) p->yp.f[c] = p->bank_f[b][c];
+  p->yp.psih = p->bank_psih[b];
+}
+
 static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
   const YeeParams& P = p->yp;
   cudaError_t e;
+  if (p->fused) {
+    for (const Modulation& m : p->mods)
+      if ((e = launch_modulate(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "modulate");
+    if (P.has_ade && (e = launch_ade_segments(P, p->d_ade_segs, p->n_ade_segs,
+                                              (int64_t)p->nx * p->ny * p->nzp / 32, 0, s)) !=
+                         cudaSuccess)
+      return cuda_error(e, "ade");
+    const int nb = p->bank ^ 1;
+    FieldOut out;
+    for (int c = 0; c < 6; ++c) out.f[c] = p->bank_f[nb][c];
+    out.psih = p->bank_psih[nb];
+    if ((e = launch_update_he_fused(p->fmaps[p->bank], P, out, p->xch, (int)p->mats.size(),
+                                    p->d_err, s)) != cudaSuccess)
+      return cuda_error(e, "update_he");
+    set_bank(p, nb);
+    return enqueue_e_side(p, s, monitors);
+  }
   // the pole pass depends on E^n only: it runs on a branch beside the H update and joins
   // before the E update
   const bool fork = p->side_stream != nullptr;
@@ -274,6 +337,14 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
     e = run_e(p, s);
   }
   if (e != cudaSuccess) return cuda_error(e, "update_e");
+  return enqueue_e_side(p, s, monitors);
+}
+
+// After the E update: E-side injection, absorber, time / flux-time samples, DFT snapshots and
+// flushes, the step counter.
+static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors) {
+  const YeeParams& P = p->yp;
+  cudaError_t e;
   for (const PlaneSrc& src : p->planes)
     if ((e = launch_plane_e(P, src, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "plane_e");
@@ -354,9 +425,11 @@ static int load_state(oem_plan* p, int slot, cudaStream_t s) {
 
 static int capture(oem_plan* p, int nsteps, cudaGraphExec_t* out) {
   cudaGraph_t g = nullptr;
+  const int bank0 = p->bank;
   OEM_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
   int rc = OEM_OK;
   for (int q = 0; q < nsteps && rc == OEM_OK; ++q) rc = enqueue_step(p, p->cap_stream);
+  if (p->fused) set_bank(p, bank0);  // capturing ran nothing: the fields are still in bank0
   cudaError_t e = cudaStreamEndCapture(p->cap_stream, &g);
   if (rc) {
     if (g) cudaGraphDestroy(g);
@@ -408,6 +481,10 @@ int oem_plan_create(int device, int nx, int ny, int nz, double ch, double cw, oe
   if (kind && strcmp(kind, "stream") == 0) p->basic_kernels = 2;
   if (kind && strcmp(kind, "ws") == 0) p->basic_kernels = 3;
   if (kind && strcmp(kind, "tma") == 0) p->basic_kernels = 0;
+  // the fused H + E step (two field banks) only when asked for: it is exact but latency-bound
+  // and slower than the two pipelined kernels on the grids measured so far
+  p->want_fused = kind && strcmp(kind, "fused") == 0;
+  if (const char* fz = getenv("OEM_B200_FUSED")) p->want_fused = p->want_fused && strcmp(fz, "0") != 0;
   *out = p;
   return OEM_OK;
 }
@@ -415,8 +492,10 @@ int oem_plan_create(int device, int nx, int ny, int nz, double ch, double cw, oe
 int oem_plan_destroy(oem_plan* p) {
   if (!p) return OEM_OK;
   cudaSetDevice(p->device);
-  if (p->graph_many) cudaGraphExecDestroy(p->graph_many);
-  if (p->graph_one) cudaGraphExecDestroy(p->graph_one);
+  for (int b = 0; b < 2; ++b) {
+    if (p->graph_many[b]) cudaGraphExecDestroy(p->graph_many[b]);
+    if (p->graph_one[b]) cudaGraphExecDestroy(p->graph_one[b]);
+  }
   if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
   if (p->side_stream) cudaStreamDestroy(p->side_stream);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
@@ -1360,11 +1439,32 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   if (p->xch_user > 0) p->xch = p->xch_user;
   if (const char* xs = getenv("OEM_B200_XCHUNK")) p->xch = std::max(1, atoi(xs));
   if (p->basic_kernels == 3) p->xch = std::min(p->xch, ws_max_xchunk());
+  if (fused_eligible(p)) {
+    // the second field bank and H-side psi the fused step writes into
+    for (int c = 0; c < 6; ++c) {
+      p->bank_f[0][c] = P.f[c];
+      if ((rc = dalloc(p, &p->bank_f[1][c], ncp))) return rc;
+    }
+    p->bank_psih[0] = P.psih;
+    for (int a = 0; a < 3; ++a)
+      for (int side = 0; side < 2; ++side) {
+        const int L = side == 0 ? p->axh[a].lo : p->axh[a].hi;
+        if (L <= 0) continue;
+        const size_t cnt = a == 0 ? (size_t)L * p->ny * p->nzp
+                                  : (a == 1 ? (size_t)p->nx * L * p->nzp
+                                            : (size_t)p->nx * p->ny * L);
+        for (int slot = 0; slot < 2; ++slot)
+          if ((rc = dalloc(p, &p->bank_psih[1].p[a][slot][side], cnt))) return rc;
+      }
+    if ((rc = make_fused_maps(p, 0)) || (rc = make_fused_maps(p, 1))) return rc;
+    p->fused = true;
+    set_bank(p, 0);
+  }
   p->energy_blocks = energy_block_count(P);
   if ((rc = dalloc(p, &p->d_energy_part, 3 * (size_t)p->energy_blocks))) return rc;
   // capture: G steps per graph for small grids (launch overhead), 1 for large ones
   OEM_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
-  if (p->basic_kernels == 3 && P.has_ade && p->n_ade_segs > 0) {
+  if (p->basic_kernels == 3 && !p->fused && P.has_ade && p->n_ade_segs > 0) {
     OEM_CUDA(cudaStreamCreateWithFlags(&p->side_stream, cudaStreamNonBlocking));
     OEM_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
     OEM_CUDA(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
@@ -1372,8 +1472,12 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   const double cells = (double)ncp;
   int G = (int)std::min(32.0, std::max(1.0, 4.0e6 / cells));
   p->graph_steps = G;
-  if ((rc = capture(p, 1, &p->graph_one))) return rc;
-  if (G > 1 && (rc = capture(p, G, &p->graph_many))) return rc;
+  for (int b = 0; b < (p->fused ? 2 : 1); ++b) {
+    if (p->fused) set_bank(p, b);
+    if ((rc = capture(p, 1, &p->graph_one[b]))) return rc;
+    if (G > 1 && (rc = capture(p, G, &p->graph_many[b]))) return rc;
+  }
+  if (p->fused) set_bank(p, 0);
   // setup work runs on the legacy default stream; waiting for it alone leaves other plans'
   // (non-blocking) streams running, which a server with several plans in flight relies on
   OEM_CUDA(cudaStreamSynchronize(0));
@@ -1402,6 +1506,30 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
     for (int64_t q = 0; q < n; ++q) {
       cudaEvent_t* E = &ev[(size_t)q * 6];
       cudaError_t e;
+      if (p->fused) {
+        // E[0] ade E[5] fused E[1] ... E[4]: the pole pass and the fused kernel timed apart
+        OEM_CUDA(cudaEventRecord(E[0], s));
+        for (const Modulation& m : p->mods)
+          if ((e = launch_modulate(p->yp, m, p->d_step, s)) != cudaSuccess)
+            return cuda_error(e, "modulate");
+        if (p->yp.has_ade &&
+            (e = launch_ade_segments(p->yp, p->d_ade_segs, p->n_ade_segs,
+                                     (int64_t)p->nx * p->ny * p->nzp / 32, 0, s)) != cudaSuccess)
+          return cuda_error(e, "ade");
+        OEM_CUDA(cudaEventRecord(E[5], s));
+        const int nb = p->bank ^ 1;
+        FieldOut out;
+        for (int c = 0; c < 6; ++c) out.f[c] = p->bank_f[nb][c];
+        out.psih = p->bank_psih[nb];
+        if ((e = launch_update_he_fused(p->fmaps[p->bank], p->yp, out, p->xch,
+                                        (int)p->mats.size(), p->d_err, s)) != cudaSuccess)
+          return cuda_error(e, "update_he");
+        OEM_CUDA(cudaEventRecord(E[1], s));
+        set_bank(p, nb);
+        if ((rc = enqueue_e_side(p, s, true))) return rc;
+        OEM_CUDA(cudaEventRecord(E[4], s));
+        continue;
+      }
       for (const Modulation& m : p->mods)
         if ((e = launch_modulate(p->yp, m, p->d_step, s)) != cudaSuccess)
           return cuda_error(e, "modulate");
@@ -1467,6 +1595,16 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
     for (int64_t q = 0; q < n; ++q) {
       cudaEvent_t* E = &ev[(size_t)q * 6];
       float t_h = 0.f, t_e = 0.f, t_all = 0.f, t_ade = 0.f;
+      if (p->fused) {
+        float t_he = 0.f;
+        OEM_CUDA(cudaEventElapsedTime(&t_ade, E[0], E[5]));
+        OEM_CUDA(cudaEventElapsedTime(&t_he, E[5], E[1]));
+        OEM_CUDA(cudaEventElapsedTime(&t_all, E[0], E[4]));
+        if (p->yp.has_ade) add("ade", t_ade);
+        add("update_he", t_he);
+        add("step", t_all);
+        continue;
+      }
       OEM_CUDA(cudaEventElapsedTime(&t_h, E[0], E[1]));
       OEM_CUDA(cudaEventElapsedTime(&t_all, E[0], E[4]));
       if (p->basic_kernels == 3 && p->yp.has_ade) {
@@ -1494,11 +1632,13 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
     }
     int64_t c = chunk;
     while (c >= p->graph_steps && p->graph_steps > 1) {
-      OEM_CUDA(cudaGraphLaunch(p->graph_many, s));
+      OEM_CUDA(cudaGraphLaunch(p->graph_many[p->bank], s));
+      if (p->fused && (p->graph_steps & 1)) set_bank(p, p->bank ^ 1);
       c -= p->graph_steps;
     }
     while (c > 0) {
-      OEM_CUDA(cudaGraphLaunch(p->graph_one, s));
+      OEM_CUDA(cudaGraphLaunch(p->graph_one[p->bank], s));
+      if (p->fused) set_bank(p, p->bank ^ 1);
       --c;
     }
     p->steps += chunk;
@@ -1523,7 +1663,7 @@ int oem_plan_launches_per_step(oem_plan* p, int* n) {
   int rc = check_plan(p, true);
   if (rc) return rc;
   if (!n) return set_error(OEM_ERR_INVALID, "null output");
-  int c = 2 + 1;  // update_h, update_e, step counter
+  int c = p->fused ? 1 + 1 : 2 + 1;  // update_h, update_e (or the fused pair), step counter
   if (p->basic_kernels == 3 && p->yp.has_ade) c += 1;  // separate pole pass
   c += 2 * (int)p->planes.size();
   c += 2 * (int)p->modesrcs.size();

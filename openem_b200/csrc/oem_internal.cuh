@@ -106,6 +106,21 @@ struct TmaMaps {
   CUtensorMap m_tile;
 };
 
+// Tensor maps of the fused H + E kernel over one field bank: E boxes 136 x 6, E (y, z) and H
+// tiles 128 x 5, the material tile 128 x 4.
+struct FusedMaps {
+  CUtensorMap e6[3];
+  CUtensorMap e5[2];
+  CUtensorMap h5[3];
+  CUtensorMap m;
+};
+
+// Where the fused kernel writes: the other bank's fields and H-side psi.
+struct FieldOut {
+  float* f[6];
+  PsiSet psih;
+};
+
 struct PlaneSrc {
   int pol, kh, ks;
   float coef_h, coef_e;
@@ -291,8 +306,8 @@ struct oem_plan {
   double* d_dl[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};  // primal, dual
 
   cudaStream_t cap_stream = nullptr;
-  cudaGraphExec_t graph_many = nullptr;
-  cudaGraphExec_t graph_one = nullptr;
+  cudaGraphExec_t graph_many[2] = {nullptr, nullptr};  // per starting field bank
+  cudaGraphExec_t graph_one[2] = {nullptr, nullptr};
   int graph_steps = 1;
 
   bool timing = false;
@@ -312,6 +327,13 @@ struct oem_plan {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int xch = 8;            // x planes per thread in the streaming kernels
   int xch_user = 0;       // tile shape chosen by the caller (0: automatic)
+  // fused H + E step: two field banks (fields and H-side psi), swapped every step
+  bool want_fused = true;
+  bool fused = false;
+  int bank = 0;
+  float* bank_f[2][6] = {};
+  oem::PsiSet bank_psih[2] = {};
+  oem::FusedMaps fmaps[2];
 };
 
 namespace oem {
@@ -391,6 +413,8 @@ cudaError_t launch_modulate(const YeeParams& P, const Modulation& m, const int* 
                             cudaStream_t s);
 cudaError_t launch_flux_time(const YeeParams& P, const FluxTimeMon& m, const int* step,
                              cudaStream_t s);
+cudaError_t launch_update_he_fused(const FusedMaps& maps, const YeeParams& P, const FieldOut& out,
+                                   int xch, int n_mats, int* err, cudaStream_t s);
 cudaError_t launch_tfsf(const YeeParams& P, const Tfsf& t, int is_e, const int* step,
                         cudaStream_t s);
 

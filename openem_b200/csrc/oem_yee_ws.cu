@@ -31,7 +31,20 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kTY = 4;
 constexpr int kTZ = 128;
 constexpr int kBZ = 136;
-constexpr int kS = 3;
+// Ring depth, blocks per SM and the E kernel's psi / current pool (build-time knobs). Two
+// stages let three blocks of each kernel share an SM (<= 136 registers, <= 75 KB of shared
+// memory per block): on the 512^3 dispersive grid the E update runs 12% faster than with three
+// stages and two blocks, the latency of the shallower ring hidden by the third block.
+#ifndef OEM_WS_STAGES
+#define OEM_WS_STAGES 2
+#endif
+#ifndef OEM_WS_MINBLOCKS
+#define OEM_WS_MINBLOCKS 3
+#endif
+#ifndef OEM_WS_EPOOL
+#define OEM_WS_EPOOL 2560
+#endif
+constexpr int kS = OEM_WS_STAGES;
 constexpr int kBoxW = 704;                      // floats per 136 x 5 halo-box slot (128-B aligned)
 constexpr uint32_t kWideBytes = 5 * kBZ * 4;    // bytes a halo box transfers
 constexpr uint32_t kTileBytes = kTY * kTZ * 4;  // bytes a 128 x 4 tile transfers
@@ -55,7 +68,8 @@ constexpr int kE_MT = kE_ET + 3 * 512;    // material tile (uint16 or uint32)
 // A per-plane pool: the psi rows the plane needs (x rows 1024 floats, y rows 1024, z rows 512,
 // each only when present), then the pole-state window in the rest.
 constexpr int kE_POOL = kE_MT + 512;
-constexpr int kEPool = 3328;
+constexpr int kEPool = OEM_WS_EPOOL;
+static_assert(kEPool >= 2560, "the pool must hold the x, y and z psi rows of a plane");
 constexpr int kE_PT = kE_POOL + kEPool;   // [2r]: pole start of row r, [2r+1]: window offset,
                                           // [8..10]: psi x/y/z offsets, [11]: window start
 constexpr int kEStage = kE_PT + 32;
@@ -327,7 +341,7 @@ __device__ __forceinline__ void z_cpml(float (&da)[4], float (&db)[4], unsigned 
 // ---------------------------------------------------------------------------------------------
 // H half step
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(160, 2) k_h_ws(const __grid_constant__ TmaMaps maps, YeeParams P,
+__global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_h_ws(const __grid_constant__ TmaMaps maps, YeeParams P,
                                                  int xch, int* err) {
   extern __shared__ __align__(128) float smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kS * kHStage);
@@ -518,7 +532,7 @@ __global__ void __launch_bounds__(160, 2) k_h_ws(const __grid_constant__ TmaMaps
 // ---------------------------------------------------------------------------------------------
 // E full step with the deferred ADE
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps maps, YeeParams P,
+__global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_constant__ TmaMaps maps, YeeParams P,
                                                  int xch, int n_mats, int* err) {
   extern __shared__ __align__(128) float smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kS * kEStage);
@@ -811,6 +825,491 @@ __global__ void __launch_bounds__(160, 2) k_e_ws(const __grid_constant__ TmaMaps
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Fused H + E step over two field banks
+// ---------------------------------------------------------------------------------------------
+// One pass reads E^n, H^{n-1/2} (and the H-side psi) from the current bank and writes H^{n+1/2},
+// E^{n+1} (and the H-side psi) to the other bank, so every field value crosses HBM once each
+// way. Per x plane i a block computes H^{n+1/2}(i) on its four rows plus the row below them
+// (warp 4, needed by the E update's y difference) and on the cell before its z range (the
+// producer warp, ahead of time, for the z difference), keeps the planes i and i-1 of H^{n+1/2}
+// in shared memory, and
+// then updates E(i) on its four rows. The first plane of a chunk is preceded by an H-only pass
+// over the x neighbour plane X.prv[ib] (own rows). The E-side psi is updated in place (cells are
+// owned by one block); the H-side psi goes to the other bank because the halo row and cell read
+// psi of cells another block owns. The arithmetic is that of the two-kernel path, bit for bit.
+//
+// Eligible grids: y and z without periodic wrap (the halo row and cell are the adjacent ones);
+// no H-side injection (the H update's result is consumed inside the kernel).
+constexpr int kFS = 3;
+constexpr int kF_EBS = 832;                   // floats per 136 x 6 E box (128-B aligned)
+constexpr int kF_T5 = 640;                    // floats per 128 x 5 tile
+constexpr int kF_EB = 0;                      // E^n box x3: rows j0-1 .. j0+4, cols k0 .. k0+135
+constexpr int kF_EN = kF_EB + 3 * kF_EBS;     // Ey, Ez of plane X.nxt[i]: rows j0-1 .. j0+3
+constexpr int kF_HO = kF_EN + 2 * kF_T5;      // H^{n-1/2} x3: rows j0-1 .. j0+3
+constexpr int kF_MT = kF_HO + 3 * kF_T5;      // material tile, rows j0 .. j0+3
+constexpr int kF_ZS = kF_MT + 512;            // Hx, Hy of H^{n+1/2} at (rows, k0 - 1) [c][row]
+constexpr int kFStage = kF_ZS + 32;
+constexpr uint32_t kF_EBBytes = 6 * kBZ * 4;
+constexpr uint32_t kF_T5Bytes = 5 * kTZ * 4;
+constexpr int kF_HN = 2 * 3 * 5 * kTZ;        // H^{n+1/2} of two planes [parity][comp][row][z]
+static_assert((kF_EN * 4) % 128 == 0 && (kF_HO * 4) % 128 == 0 && (kF_MT * 4) % 128 == 0 &&
+                  (kFStage * 4) % 128 == 0 && (kF_EBS * 4) % 128 == 0,
+              "fused stage slots aligned");
+
+__device__ __forceinline__ float* hn_row(float* hn, int par, int c, int r) {
+  return hn + ((par * 3 + c) * 5 + r) * kTZ;
+}
+
+// z CPML of the slab cells of one quad with psi read from `in` and, when `commit`, written to
+// `out` (cell by cell; slab lanes are few).
+__device__ __forceinline__ void zcpml_io(float (&da)[4], float (&db)[4], unsigned zslm,
+                                         const float* zt, const PsiSet& in, const PsiSet& out,
+                                         bool commit, const YeeParams& P, int i, int j, int kq,
+                                         int lane) {
+  const DevAxis& Z = P.ax[2];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    if (!((zslm >> e) & 1u)) continue;
+    const int kk = kq + e;
+    float p0 = *psi_addr(in, 2, 0, Z, i, j, kk, P.ny, P.nzp);
+    float p1 = *psi_addr(in, 2, 1, Z, i, j, kk, P.ny, P.nzp);
+    const int zi = 4 * lane + e;
+    const float a = zt[2 * kTZ + zi], b = zt[3 * kTZ + zi], k = zt[4 * kTZ + zi];
+    da[e] = cpml_stretch(da[e], p0, a, b, k);
+    db[e] = cpml_stretch(db[e], p1, a, b, k);
+    if (commit) {
+      *psi_addr(out, 2, 0, Z, i, j, kk, P.ny, P.nzp) = p0;
+      *psi_addr(out, 2, 1, Z, i, j, kk, P.ny, P.nzp) = p1;
+    }
+  }
+}
+
+// H^{n+1/2} of one quad of row jrow (box / tile row hr) of plane i from the stage; written to
+// the other bank (field and psi) when `commit`.
+__device__ __forceinline__ void fused_h_quad(const YeeParams& P, const FieldOut& out,
+                                             const float* st, const float* zt, int i, int jrow,
+                                             int hr, int k0, int lane, bool commit,
+                                             float (&hx)[4], float (&hy)[4], float (&hz)[4]) {
+  const DevAxis& X = P.ax[0];
+  const DevAxis& Y = P.ax[1];
+  const DevAxis& Z = P.ax[2];
+  const int jp = Y.nxt[jrow];
+  const float mj = Y.mnx[jrow], idy = Y.idl_p[jrow];
+  const bool ysl = in_slab(Y, jrow);
+  const bool yspecial = jp != jrow + 1 && mj != 0.0f;
+  const int kq = k0 + 4 * lane;
+  unsigned kvm = 0, zslm = 0, zspm = 0;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int k = kq + e;
+    const bool kv = k < P.nz;
+    kvm |= (unsigned)kv << e;
+    zslm |= (unsigned)(kv && in_slab(Z, k)) << e;
+    zspm |= (unsigned)(kv && __float_as_int(zt[5 * kTZ + 4 * lane + e]) != k + 1 &&
+                       zt[kTZ + 4 * lane + e] != 0.0f) << e;
+  }
+  const bool yplain = !ysl && !yspecial && mj == 1.0f;
+  const int64_t sj = P.nzp, si = (int64_t)P.ny * P.nzp;
+  const int64_t row = i * si + (int64_t)jrow * sj;
+  const int ro = hr * kBZ + 4 * lane;
+  const int to = hr * kTZ + 4 * lane;
+  const float ch = P.ch;
+  const bool xsl = in_slab(X, i);
+  const float mi = X.mnx[i], idx_ = X.idl_p[i];
+  unpack4(lds4(st + kF_HO + to), hx);
+  unpack4(lds4(st + kF_HO + kF_T5 + to), hy);
+  unpack4(lds4(st + kF_HO + 2 * kF_T5 + to), hz);
+  if (!kvm) return;  // the quad lies past nz: no global access (its row may end before it)
+  float ex[4], ey[4], ez[4], yex[4], yez[4], ney[4], nez[4], idz[4], mkz[4];
+  unpack4(lds4(st + kF_EB + ro), ex);
+  unpack4(lds4(st + kF_EB + kF_EBS + ro), ey);
+  unpack4(lds4(st + kF_EB + 2 * kF_EBS + ro), ez);
+  if (yspecial) {
+    const int64_t oy = i * si + (int64_t)jp * sj + kq;
+    unpack4(*reinterpret_cast<const float4*>(P.f[0] + oy), yex);
+    unpack4(*reinterpret_cast<const float4*>(P.f[2] + oy), yez);
+  } else {
+    unpack4(lds4(st + kF_EB + ro + kBZ), yex);
+    unpack4(lds4(st + kF_EB + 2 * kF_EBS + ro + kBZ), yez);
+  }
+  unpack4(lds4(st + kF_EN + to), ney);
+  unpack4(lds4(st + kF_EN + kF_T5 + to), nez);
+  unpack4(lds4(zt + 4 * lane), idz);
+  unpack4(lds4(zt + kTZ + 4 * lane), mkz);
+  const float ex4 = st[kF_EB + ro + 4];
+  const float ey4 = st[kF_EB + kF_EBS + ro + 4];
+  float dyz[4], dxz[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    float zex = (e < 3) ? ex[e + 1] : ex4;
+    float zey = (e < 3) ? ey[e + 1] : ey4;
+    if ((zspm >> e) & 1u) {
+      const int kp = __float_as_int(zt[5 * kTZ + 4 * lane + e]);
+      zex = P.f[0][row + kp];
+      zey = P.f[1][row + kp];
+    }
+    dyz[e] = fdiff(zey, mkz[e], ey[e], idz[e]);
+    dxz[e] = fdiff(zex, mkz[e], ex[e], idz[e]);
+  }
+  if (zslm) zcpml_io(dyz, dxz, zslm, zt, P.psih, out.psih, commit, P, i, jrow, kq, lane);
+  if (yplain && !xsl && i + 1 < P.nx && X.nxt[i] == i + 1 && mi == 1.0f) {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const float nhx = h_new(hx[e], ch, __fmul_rn(__fsub_rn(yez[e], ez[e]), idy), dyz[e]);
+      const float nhy = h_new(hy[e], ch, dxz[e], __fmul_rn(__fsub_rn(nez[e], ez[e]), idx_));
+      const float nhz = h_new(hz[e], ch, __fmul_rn(__fsub_rn(ney[e], ey[e]), idx_),
+                              __fmul_rn(__fsub_rn(yex[e], ex[e]), idy));
+      const bool kv = (kvm >> e) & 1u;
+      hx[e] = kv ? nhx : hx[e];
+      hy[e] = kv ? nhy : hy[e];
+      hz[e] = kv ? nhz : hz[e];
+    }
+  } else {
+    const float ay = Y.ah[jrow], by = Y.bh[jrow], ky = Y.kh[jrow];
+    const float ax_ = X.ah[i], bx_ = X.bh[i], kx_ = X.kh[i];
+    float px[2][4], py[2][4];
+    if (xsl)
+      for (int s = 0; s < 2; ++s)
+        unpack4(*reinterpret_cast<const float4*>(psi_addr(P.psih, 0, s, X, i, jrow, kq, P.ny, P.nzp)), px[s]);
+    if (ysl)
+      for (int s = 0; s < 2; ++s)
+        unpack4(*reinterpret_cast<const float4*>(psi_addr(P.psih, 1, s, Y, i, jrow, kq, P.ny, P.nzp)), py[s]);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const float dzy = fdiff(yez[e], mj, ez[e], idy);
+      const float dzx = fdiff(nez[e], mi, ez[e], idx_);
+      const float dyx = fdiff(ney[e], mi, ey[e], idx_);
+      const float dxy = fdiff(yex[e], mj, ex[e], idy);
+      float sy0 = dzy, sy1 = dxy, sx0 = dzx, sx1 = dyx;
+      if (ysl) {
+        sy0 = cpml_stretch(dzy, py[0][e], ay, by, ky);
+        sy1 = cpml_stretch(dxy, py[1][e], ay, by, ky);
+      }
+      if (xsl) {
+        sx0 = cpml_stretch(dzx, px[0][e], ax_, bx_, kx_);
+        sx1 = cpml_stretch(dyx, px[1][e], ax_, bx_, kx_);
+      }
+      const bool kv = (kvm >> e) & 1u;
+      hx[e] = kv ? h_new(hx[e], ch, sy0, dyz[e]) : hx[e];
+      hy[e] = kv ? h_new(hy[e], ch, dxz[e], sx0) : hy[e];
+      hz[e] = kv ? h_new(hz[e], ch, sx1, sy1) : hz[e];
+    }
+    if (commit && xsl)
+      for (int s = 0; s < 2; ++s)
+        *reinterpret_cast<float4*>(psi_addr(out.psih, 0, s, X, i, jrow, kq, P.ny, P.nzp)) =
+            make_float4(px[s][0], px[s][1], px[s][2], px[s][3]);
+    if (commit && ysl)
+      for (int s = 0; s < 2; ++s)
+        *reinterpret_cast<float4*>(psi_addr(out.psih, 1, s, Y, i, jrow, kq, P.ny, P.nzp)) =
+            make_float4(py[s][0], py[s][1], py[s][2], py[s][3]);
+  }
+  if (commit) {
+    *reinterpret_cast<float4*>(out.f[3] + row + kq) = make_float4(hx[0], hx[1], hx[2], hx[3]);
+    *reinterpret_cast<float4*>(out.f[4] + row + kq) = make_float4(hy[0], hy[1], hy[2], hy[3]);
+    *reinterpret_cast<float4*>(out.f[5] + row + kq) = make_float4(hz[0], hz[1], hz[2], hz[3]);
+  }
+}
+
+// Hx, Hy of H^{n+1/2} at (i, j, k) from global memory of the current bank (the halo cell before
+// a tile's z range); the same operations as the tile path.
+__device__ __forceinline__ void fused_h_cell(const YeeParams& P, int i, int j, int k, float* hxo,
+                                             float* hyo) {
+  const DevAxis& X = P.ax[0];
+  const DevAxis& Y = P.ax[1];
+  const DevAxis& Z = P.ax[2];
+  const int64_t sj = P.nzp, si = (int64_t)P.ny * P.nzp;
+  const int64_t id = i * si + (int64_t)j * sj + k;
+  const int jp = Y.nxt[j], kp = Z.nxt[k], ip = X.nxt[i];
+  const float ex = P.f[0][id], ey = P.f[1][id], ez = P.f[2][id];
+  const float dzy0 = fdiff(P.f[2][i * si + (int64_t)jp * sj + k], Y.mnx[j], ez, Y.idl_p[j]);
+  float dyz = fdiff(P.f[1][i * si + (int64_t)j * sj + kp], Z.mnx[k], ey, Z.idl_p[k]);
+  float dxz = fdiff(P.f[0][i * si + (int64_t)j * sj + kp], Z.mnx[k], ex, Z.idl_p[k]);
+  const float dzx0 = fdiff(P.f[2][ip * si + (int64_t)j * sj + k], X.mnx[i], ez, X.idl_p[i]);
+  float sy0 = dzy0, sx0 = dzx0;
+  if (in_slab(Y, j)) {
+    float ps = *psi_addr(P.psih, 1, 0, Y, i, j, k, P.ny, P.nzp);
+    sy0 = cpml_stretch(dzy0, ps, Y.ah[j], Y.bh[j], Y.kh[j]);
+  }
+  if (in_slab(Z, k)) {
+    float p0 = *psi_addr(P.psih, 2, 0, Z, i, j, k, P.ny, P.nzp);
+    float p1 = *psi_addr(P.psih, 2, 1, Z, i, j, k, P.ny, P.nzp);
+    dyz = cpml_stretch(dyz, p0, Z.ah[k], Z.bh[k], Z.kh[k]);
+    dxz = cpml_stretch(dxz, p1, Z.ah[k], Z.bh[k], Z.kh[k]);
+  }
+  if (in_slab(X, i)) {
+    float ps = *psi_addr(P.psih, 0, 0, X, i, j, k, P.ny, P.nzp);
+    sx0 = cpml_stretch(dzx0, ps, X.ah[i], X.bh[i], X.kh[i]);
+  }
+  *hxo = h_new(P.f[3][id], P.ch, sy0, dyz);
+  *hyo = h_new(P.f[4][id], P.ch, dxz, sx0);
+}
+
+__global__ void __launch_bounds__(192, 2) k_he_ws(const __grid_constant__ FusedMaps maps,
+                                                  YeeParams P, FieldOut out, int xch,
+                                                  int n_mats, int* err) {
+  extern __shared__ __align__(128) float smem[];
+  float* hn = smem + kFS * kFStage;
+  float* zth = hn + kF_HN;
+  float* zte = zth + kZTab;
+  MatRec* smats = reinterpret_cast<MatRec*>(zte + kZTab);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smats + kSmemMats);
+  uint64_t* empty = full + kFS;
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int tid = w * 32 + lane;
+  const int k0 = blockIdx.x * kTZ;
+  const int j0 = blockIdx.y * kTY;
+  const int ib = blockIdx.z * xch;
+  const int ie = min(ib + xch, P.nx);
+  const int np = ie - ib;
+  const DevAxis& X = P.ax[0];
+  const DevAxis& Y = P.ax[1];
+  const DevAxis& Z = P.ax[2];
+  const int pp = X.prv[ib];
+  const bool pre = pp != ib;  // the E update of plane ib needs H^{n+1/2} of another plane
+  const int nst = np + (pre ? 1 : 0);
+  const bool wide = P.mat32 != nullptr;
+  const MatRec* mats = P.mats;
+  if (n_mats <= kSmemMats) {
+    const uint4* src = reinterpret_cast<const uint4*>(P.mats);
+    uint4* dst = reinterpret_cast<uint4*>(smats);
+    for (int q = tid; q < n_mats * 4; q += 192) dst[q] = src[q];
+    mats = smats;
+  }
+  load_ztab(zth, Z, true, k0, P.nzp, tid, 192);
+  load_ztab(zte, Z, false, k0, P.nzp, tid, 192);
+  if (w == 5 && lane == 0) {
+    for (int s = 0; s < kFS; ++s) {
+      // lane 0's arrival with the transaction bytes, and one per halo-cell lane
+      mbar_init(&full[s], 1 + kTY);
+      mbar_init(&empty[s], kTY + 1);
+    }
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  if (w == 5) {  // ------------------------------------------------------------ producer
+    // lane 0 issues the stage's copies; lanes 0..3 compute the halo cell (row j0 + lane,
+    // k0 - 1) of the stage's plane from global memory, stage depths ahead of the consumers
+    if (lane >= kTY) return;
+    int issued = 0;
+    bool ok = true;
+    const uint32_t mbytes = (uint32_t)(kTY * kTZ * (wide ? 4 : 2));
+    for (int q = 0; q < nst && ok; ++q) {
+      const int slot = q % kFS;
+      if (q >= kFS) ok = mbar_wait(&empty[slot], (uint32_t)((q / kFS - 1) & 1), err);
+      if (!__all_sync(0xfu, ok)) break;
+      float* st = smem + slot * kFStage;
+      const bool main = !(pre && q == 0);
+      const int i = main ? ib + q - (pre ? 1 : 0) : pp;
+      if (lane == 0) {
+        const int inext = X.nxt[i];
+        mbar_expect_tx(&full[slot], 3 * kF_EBBytes + 5 * kF_T5Bytes + mbytes);
+        for (int c = 0; c < 3; ++c) {
+          tma3(st + kF_EB + c * kF_EBS, &maps.e6[c], &full[slot], k0, j0 - 1, i);
+          tma3(st + kF_HO + c * kF_T5, &maps.h5[c], &full[slot], k0, j0 - 1, i);
+        }
+        tma3(st + kF_EN, &maps.e5[0], &full[slot], k0, j0 - 1, inext);
+        tma3(st + kF_EN + kF_T5, &maps.e5[1], &full[slot], k0, j0 - 1, inext);
+        tma3(st + kF_MT, &maps.m, &full[slot], k0, j0, i);
+      }
+      if (main && k0 > 0 && j0 + lane < P.ny) {
+        float a, b;
+        fused_h_cell(P, i, j0 + lane, k0 - 1, &a, &b);
+        st[kF_ZS + lane] = a;
+        st[kF_ZS + kTY + lane] = b;
+      }
+      mbar_arrive(&full[slot]);
+      issued = q + 1;
+    }
+    if (lane == 0)
+      for (int q = max(0, issued - kFS); q < issued; ++q)  // drain (no-op when consumed)
+        mbar_wait(&full[q % kFS], (uint32_t)((q / kFS) & 1), err);
+    return;
+  }
+
+  // ------------------------------------------------------------------- consumers (warps 0-4)
+  // warps 0..3 own rows j0 + w (box row w + 1); warp 4 is the row below (box row 0) and the
+  // cell before k0. Every consumer passes every named barrier, also after a failed wait.
+  const bool owner = w < kTY;
+  const int hr = owner ? w + 1 : 0;
+  const int jrow = j0 - 1 + hr;
+  const bool row_ok = jrow >= 0 && jrow < P.ny;
+  const int64_t sj = P.nzp, si = (int64_t)P.ny * P.nzp;
+  const float cw = P.cw;
+  const unsigned lt = (1u << lane) - 1u;
+  bool alive = true;
+  for (int t = 0; t < nst; ++t) {
+    const int slot = t % kFS;
+    if (alive) alive = mbar_wait(&full[slot], (uint32_t)((t / kFS) & 1), err);
+    alive = __all_sync(kFull, alive);
+    const float* st = smem + slot * kFStage;
+    const bool main = !(pre && t == 0);
+    const int i = main ? (ib + t - (pre ? 1 : 0)) : pp;
+    const int par = t & 1;
+    // ---- H^{n+1/2}(i): owners on their rows (committed on main planes), warp 4 below them
+    if (alive && row_ok && (owner || main)) {
+      float hx[4], hy[4], hz[4];
+      fused_h_quad(P, out, st, zth, i, jrow, hr, k0, lane, owner && main, hx, hy, hz);
+      *reinterpret_cast<float4*>(hn_row(hn, par, 0, hr) + 4 * lane) = make_float4(hx[0], hx[1], hx[2], hx[3]);
+      *reinterpret_cast<float4*>(hn_row(hn, par, 1, hr) + 4 * lane) = make_float4(hy[0], hy[1], hy[2], hy[3]);
+      *reinterpret_cast<float4*>(hn_row(hn, par, 2, hr) + 4 * lane) = make_float4(hz[0], hz[1], hz[2], hz[3]);
+    }
+    __syncwarp();
+    if (!owner && lane == 0) mbar_arrive(&empty[slot]);
+    asm volatile("bar.sync 1, 160;" ::: "memory");
+    // ---- E^{n+1}(i) on the owned rows
+    if (owner) {
+      if (alive && main && row_ok) {
+        const int j = jrow;
+        const int jm = Y.prv[j];
+        const float mj = Y.mpv[j], idy = Y.idl_d[j];
+        const bool ysl = in_slab(Y, j);
+        const int hrm = (jm == j) ? hr : hr - 1;
+        const int xpar = (X.prv[i] == i) ? par : (par ^ 1);
+        const int kq = k0 + 4 * lane;
+        unsigned kvm = 0, zslm = 0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int k = kq + e;
+          const bool kv = k < P.nz;
+          kvm |= (unsigned)kv << e;
+          zslm |= (unsigned)(kv && in_slab(Z, k)) << e;
+        }
+        const int to = w * kTZ + 4 * lane;
+        uint32_t mid[4] = {0u, 0u, 0u, 0u};
+        if (wide) {
+          const uint4 m = *reinterpret_cast<const uint4*>(reinterpret_cast<const uint32_t*>(st + kF_MT) + to);
+          mid[0] = m.x; mid[1] = m.y; mid[2] = m.z; mid[3] = m.w;
+        } else {
+          const uint2 m = *reinterpret_cast<const uint2*>(reinterpret_cast<const uint16_t*>(st + kF_MT) + to);
+          mid[0] = m.x & 0xffffu; mid[1] = m.x >> 16; mid[2] = m.y & 0xffffu; mid[3] = m.y >> 16;
+        }
+        int lane_np = 0;
+        if (P.has_ade) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) lane_np += mats[mid[e]].reserved;
+        }
+        uint32_t gp = 0;
+        if (P.has_ade && __any_sync(kFull, lane_np > 0)) {
+          int pre_n = 0;
+#pragma unroll
+          for (int bb = 0; bb < 8; ++bb)
+            pre_n += __popc(__ballot_sync(kFull, (lane_np >> bb) & 1) & lt) << bb;
+          gp = P.seg_ofs[(((int64_t)i * P.ny + j) * P.nzp + k0) >> 5] + (uint32_t)pre_n;
+        }
+        const bool xsl = in_slab(X, i);
+        const float mi = X.mpv[i], idx_ = X.idl_d[i];
+        const int64_t row = i * si + (int64_t)j * sj;
+        const int ro = hr * kBZ + 4 * lane;
+        if (kvm) {
+        float ex[4], ey[4], ez[4], hx[4], hy[4], hz[4], yhx[4], yhz[4], phy[4], phz[4];
+        float idz[4], mkz[4];
+        unpack4(lds4(st + kF_EB + ro), ex);
+        unpack4(lds4(st + kF_EB + kF_EBS + ro), ey);
+        unpack4(lds4(st + kF_EB + 2 * kF_EBS + ro), ez);
+        unpack4(lds4(hn_row(hn, par, 0, hr) + 4 * lane), hx);
+        unpack4(lds4(hn_row(hn, par, 1, hr) + 4 * lane), hy);
+        unpack4(lds4(hn_row(hn, par, 2, hr) + 4 * lane), hz);
+        unpack4(lds4(hn_row(hn, par, 0, hrm) + 4 * lane), yhx);
+        unpack4(lds4(hn_row(hn, par, 2, hrm) + 4 * lane), yhz);
+        unpack4(lds4(hn_row(hn, xpar, 1, hr) + 4 * lane), phy);
+        unpack4(lds4(hn_row(hn, xpar, 2, hr) + 4 * lane), phz);
+        unpack4(lds4(zte + 4 * lane), idz);
+        unpack4(lds4(zte + kTZ + 4 * lane), mkz);
+        float hxm, hym;
+        if (lane > 0) {
+          hxm = hn_row(hn, par, 0, hr)[4 * lane - 1];
+          hym = hn_row(hn, par, 1, hr)[4 * lane - 1];
+        } else if (k0 > 0) {
+          hxm = st[kF_ZS + w];
+          hym = st[kF_ZS + kTY + w];
+        } else {  // k = 0: the clamped neighbour is the cell itself
+          hxm = hx[0];
+          hym = hy[0];
+        }
+        float dyz[4], dxz[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float zhx = (e > 0) ? hx[e - 1] : hxm;
+          const float zhy = (e > 0) ? hy[e - 1] : hym;
+          dyz[e] = bdiff(hy[e], zhy, mkz[e], idz[e]);
+          dxz[e] = bdiff(hx[e], zhx, mkz[e], idz[e]);
+        }
+        if (zslm) zcpml_io(dyz, dxz, zslm, zte, P.psie, P.psie, true, P, i, j, kq, lane);
+        float sy0[4], sy1[4], sx0[4], sx1[4];
+        const bool yplain = !ysl && jm == j - 1 && mj == 1.0f;
+        if (yplain && !xsl && i > 0 && X.prv[i] == i - 1 && mi == 1.0f) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            sy0[e] = __fmul_rn(__fsub_rn(hz[e], yhz[e]), idy);
+            sx0[e] = __fmul_rn(__fsub_rn(hz[e], phz[e]), idx_);
+            sx1[e] = __fmul_rn(__fsub_rn(hy[e], phy[e]), idx_);
+            sy1[e] = __fmul_rn(__fsub_rn(hx[e], yhx[e]), idy);
+          }
+        } else {
+          const float ay = Y.ae[j], by = Y.be[j], ky = Y.ke[j];
+          const float ax_ = X.ae[i], bx_ = X.be[i], kx_ = X.ke[i];
+          float px[2][4], py[2][4];
+          if (xsl)
+            for (int s = 0; s < 2; ++s)
+              unpack4(*reinterpret_cast<const float4*>(psi_addr(P.psie, 0, s, X, i, j, kq, P.ny, P.nzp)), px[s]);
+          if (ysl)
+            for (int s = 0; s < 2; ++s)
+              unpack4(*reinterpret_cast<const float4*>(psi_addr(P.psie, 1, s, Y, i, j, kq, P.ny, P.nzp)), py[s]);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            sy0[e] = bdiff(hz[e], yhz[e], mj, idy);
+            sx0[e] = bdiff(hz[e], phz[e], mi, idx_);
+            sx1[e] = bdiff(hy[e], phy[e], mi, idx_);
+            sy1[e] = bdiff(hx[e], yhx[e], mj, idy);
+            if (ysl) {
+              sy0[e] = cpml_stretch(sy0[e], py[0][e], ay, by, ky);
+              sy1[e] = cpml_stretch(sy1[e], py[1][e], ay, by, ky);
+            }
+            if (xsl) {
+              sx0[e] = cpml_stretch(sx0[e], px[0][e], ax_, bx_, kx_);
+              sx1[e] = cpml_stretch(sx1[e], px[1][e], ax_, bx_, kx_);
+            }
+          }
+          if (xsl)
+            for (int s = 0; s < 2; ++s)
+              *reinterpret_cast<float4*>(psi_addr(P.psie, 0, s, X, i, j, kq, P.ny, P.nzp)) =
+                  make_float4(px[s][0], px[s][1], px[s][2], px[s][3]);
+          if (ysl)
+            for (int s = 0; s < 2; ++s)
+              *reinterpret_cast<float4*>(psi_addr(P.psie, 1, s, Y, i, j, kq, P.ny, P.nzp)) =
+                  make_float4(py[s][0], py[s][1], py[s][2], py[s][3]);
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const MatRec& M = mats[mid[e]];
+          const float4 cab = *reinterpret_cast<const float4*>(&M.ca[0]);
+          const float2 cb12 = *reinterpret_cast<const float2*>(&M.cb[1]);
+          float wv[3] = {0.f, 0.f, 0.f};
+          if (lane_np > 0 && M.reserved > 0) {
+            cell_currents(M, nullptr, -1, P.J, gp, wv);
+            gp += (uint32_t)M.reserved;
+          }
+          const bool kv = (kvm >> e) & 1u;
+          const float nex = e_new(cab.x, ex[e], cab.w, sy0[e], dyz[e], cw, wv[0]);
+          const float ney = e_new(cab.y, ey[e], cb12.x, dxz[e], sx0[e], cw, wv[1]);
+          const float nez = e_new(cab.z, ez[e], cb12.y, sx1[e], sy1[e], cw, wv[2]);
+          ex[e] = kv ? nex : ex[e];
+          ey[e] = kv ? ney : ey[e];
+          ez[e] = kv ? nez : ez[e];
+        }
+        *reinterpret_cast<float4*>(out.f[0] + row + kq) = make_float4(ex[0], ex[1], ex[2], ex[3]);
+        *reinterpret_cast<float4*>(out.f[1] + row + kq) = make_float4(ey[0], ey[1], ey[2], ey[3]);
+        *reinterpret_cast<float4*>(out.f[2] + row + kq) = make_float4(ez[0], ez[1], ez[2], ez[3]);
+        }  // kvm
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[slot]);
+    }
+  }
+}
+
 }  // namespace
 
 size_t ws_h_smem() { return (size_t)kS * kHStage * 4 + 2 * kS * sizeof(uint64_t) + kZTab * 4; }
@@ -821,9 +1320,14 @@ size_t ws_e_smem() {
 
 int ws_max_xchunk() { return kXMax; }
 
+size_t he_smem() {
+  return (size_t)kFS * kFStage * 4 + (size_t)(kF_HN + 2 * kZTab) * 4 +
+         kSmemMats * sizeof(MatRec) + 2 * kFS * sizeof(uint64_t);
+}
+
 int ws_xchunk(const YeeParams& P) {
   const int64_t tiles = (int64_t)((P.nzp + kTZ - 1) / kTZ) * ((P.ny + kTY - 1) / kTY);
-  const int64_t want = 148LL * 2 * 4;  // ~4 waves of 2 resident blocks per SM
+  const int64_t want = 148LL * OEM_WS_MINBLOCKS * 4;  // ~4 waves of the resident blocks
   int64_t chunks = (want + tiles - 1) / tiles;
   int xch = (int)((P.nx + chunks - 1) / chunks);
   if (xch < 8) xch = 8;
@@ -845,6 +1349,11 @@ cudaError_t ws_setup_kernels() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_e_ws, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_he_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)he_smem());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_he_ws, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
   return e;
 }
 
@@ -859,6 +1368,13 @@ cudaError_t launch_update_e_ws(const TmaMaps& maps, const YeeParams& P, int xch,
                                int* err, cudaStream_t s) {
   dim3 b(32, kTY + 1, 1), g((P.nzp + kTZ - 1) / kTZ, (P.ny + kTY - 1) / kTY, (P.nx + xch - 1) / xch);
   k_e_ws<<<g, b, ws_e_smem(), s>>>(maps, P, xch, n_mats, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_update_he_fused(const FusedMaps& maps, const YeeParams& P, const FieldOut& out,
+                                   int xch, int n_mats, int* err, cudaStream_t s) {
+  dim3 b(32, kTY + 2, 1), g((P.nzp + kTZ - 1) / kTZ, (P.ny + kTY - 1) / kTY, (P.nx + xch - 1) / xch);
+  k_he_ws<<<g, b, he_smem(), s>>>(maps, P, out, xch, n_mats, err);
   return cudaGetLastError();
 }
 

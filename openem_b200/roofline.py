@@ -66,14 +66,17 @@ def kernel_bytes(sc) -> dict:
     cells. ``update_e``: H read, E read and written, the material index (38 B per cell), the
     E-side psi, and one float32 polarisation current per dispersive (component, cell) entry.
     ``ade`` (the separate pole pass): each pole state read and written (16 B), and per entry
-    E^n read and the current written (8 B)."""
+    E^n read and the current written (8 B). ``update_he`` (the fused step over two field banks):
+    E and H each read once and written once (48 B per cell), the material index, both families'
+    psi, and the polarisation currents."""
     c = counts(sc)
     n = c["ncell"]
     psi = 16.0 * sum(c["slab_cells"].values())
     n_entry = 0 if sc.dispersion is None else int(sc.dispersion.n_entry)
     return {"update_h": 36.0 * n + psi,
             "update_e": 38.0 * n + psi + 4.0 * n_entry,
-            "ade": 16.0 * c["n_pole"] + 8.0 * n_entry}
+            "ade": 16.0 * c["n_pole"] + 8.0 * n_entry,
+            "update_he": 50.0 * n + 2.0 * psi + 4.0 * n_entry}
 
 
 def measured_peaks(root=None) -> dict:
