@@ -20,6 +20,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <cmath>
+
 #include "oem_internal.cuh"
 #include "oem_arith.cuh"
 
@@ -1325,18 +1328,29 @@ size_t he_smem() {
          kSmemMats * sizeof(MatRec) + 2 * kFS * sizeof(uint64_t);
 }
 
+// x planes per block: the chunk length whose block count fills the last wave of resident blocks
+// best, less a cost for short chunks (each block fills its ring before the first plane; about two
+// planes' worth). Grids smaller than a wave get the shortest chunks (the most blocks).
 int ws_xchunk(const YeeParams& P) {
   const int64_t tiles = (int64_t)((P.nzp + kTZ - 1) / kTZ) * ((P.ny + kTY - 1) / kTY);
-  const int64_t want = 148LL * OEM_WS_MINBLOCKS * 4;  // ~4 waves of the resident blocks
-  int64_t chunks = (want + tiles - 1) / tiles;
-  int xch = (int)((P.nx + chunks - 1) / chunks);
-  if (xch < 8) xch = 8;
-  if (xch > kXMax) xch = kXMax;
-  if (xch > P.nx) xch = P.nx;
-  return xch;
+  const double slots = 148.0 * OEM_WS_MINBLOCKS;
+  const int hi = std::min(kXMax, P.nx);
+  int best = hi;
+  double best_score = -1e30;
+  for (int xch = std::min(8, hi); xch <= hi; ++xch) {
+    const int64_t chunks = (P.nx + xch - 1) / xch;
+    const double waves = (double)(tiles * chunks) / slots;
+    const double fill = waves / std::ceil(waves);
+    const double score = fill - 2.0 / xch;
+    if (score > best_score + 1e-12) {
+      best_score = score;
+      best = xch;
+    }
+  }
+  return best;
 }
 
-// Two blocks of each kernel share an SM; the largest shared-memory carveout makes room for both.
+// Several blocks of each kernel share an SM; the largest shared-memory carveout makes room.
 cudaError_t ws_setup_kernels() {
   cudaError_t e = cudaFuncSetAttribute(k_h_ws, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)ws_h_smem());
