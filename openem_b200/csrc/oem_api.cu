@@ -476,10 +476,12 @@ int oem_plan_create(int device, int nx, int ny, int nz, double ch, double cw, oe
   p->ch = ch;
   p->cw = cw;
   const char* kind = getenv("OEM_B200_KERNELS");
-  p->basic_kernels = 3;  // warp-specialised TMA kernels unless asked otherwise
+  // warp-specialised TMA kernels unless asked otherwise; below ~1.5M cells the one-thread-per-
+  // cell kernels finish a step sooner (a pipelined block needs several planes to fill its ring)
+  p->basic_kernels = (double)nx * ny * nz < 1.5e6 ? 1 : 3;
   if (kind && strcmp(kind, "basic") == 0) p->basic_kernels = 1;
   if (kind && strcmp(kind, "stream") == 0) p->basic_kernels = 2;
-  if (kind && strcmp(kind, "ws") == 0) p->basic_kernels = 3;
+  if (kind && (strcmp(kind, "ws") == 0 || strcmp(kind, "fused") == 0)) p->basic_kernels = 3;
   if (kind && strcmp(kind, "tma") == 0) p->basic_kernels = 0;
   // the fused H + E step (two field banks) only when asked for: it is exact but latency-bound
   // and slower than the two pipelined kernels on the grids measured so far

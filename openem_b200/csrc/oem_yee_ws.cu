@@ -1328,13 +1328,20 @@ size_t he_smem() {
          kSmemMats * sizeof(MatRec) + 2 * kFS * sizeof(uint64_t);
 }
 
-// x planes per block: the chunk length whose block count fills the last wave of resident blocks
-// best, less a cost for short chunks (each block fills its ring before the first plane; about two
-// planes' worth). Grids smaller than a wave get the shortest chunks (the most blocks).
+// x planes per block. A block streams its planes one after another (about 2 us each) after
+// filling its ring (about six planes' worth), so a grid too small to fill the resident block
+// slots even at 8-plane chunks gets as many chunks as there are slots (down to 2 planes per
+// block: every block runs at once and the step lasts one short chunk). Larger grids take the
+// chunk length whose block count fills the last wave best, less a cost for short chunks.
 int ws_xchunk(const YeeParams& P) {
   const int64_t tiles = (int64_t)((P.nzp + kTZ - 1) / kTZ) * ((P.ny + kTY - 1) / kTY);
   const double slots = 148.0 * OEM_WS_MINBLOCKS;
   const int hi = std::min(kXMax, P.nx);
+  if ((double)(tiles * ((P.nx + 7) / 8)) <= slots) {
+    const int64_t chunks = std::max<int64_t>(1, (int64_t)slots / tiles);
+    const int xch = (int)((P.nx + chunks - 1) / chunks);
+    return std::min(hi, std::max(std::min(2, hi), xch));
+  }
   int best = hi;
   double best_score = -1e30;
   for (int xch = std::min(8, hi); xch <= hi; ++xch) {

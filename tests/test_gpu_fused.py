@@ -89,6 +89,8 @@ def run_both(sc, monkeypatch, steps=None, xchunk=None):
         out[kind] = solver.run(sc, num_steps=steps, use_shutoff=False, return_fields=True,
                                verbose=False, stats=stats)
         out[kind + "_launches"] = stats["launches_per_step"]
+    # the fused pair replaces the two update kernels (and a separate pole pass stays)
+    assert out["fused_launches"] == out["ws_launches"] - 1
     return out
 
 
@@ -114,7 +116,6 @@ def assert_same(a, b):
 def test_fused_equals_two_kernel_path(monkeypatch, bounds, xchunk):
     sc = mixed_scene(bounds=bounds)
     r = run_both(sc, monkeypatch, xchunk=xchunk)
-    assert r["fused_launches"] < r["ws_launches"]  # the fused path really ran
     assert_same(r["fused"], r["ws"])
     assert np.abs(r["fused"].fields["Ez"]).max() > 0
 
@@ -126,7 +127,6 @@ def test_fused_with_modulation_equals_two_kernel_path(monkeypatch):
     mo = TimeModulation(3e13, np.repeat([0, 1, 2], cells.size)[:cells.size],
                         cells, np.full(cells.size, 0.2), np.linspace(0, 2, cells.size))
     r = run_both(replace(sc, modulation=mo), monkeypatch)
-    assert r["fused_launches"] < r["ws_launches"]
     assert_same(r["fused"], r["ws"])
 
 
