@@ -151,6 +151,12 @@ int oem_plan_set_xchunk(oem_plan* p, int xch);
 int oem_plan_enable_checkpoints(oem_plan* p, int k);
 int oem_plan_adjoint_flux(oem_plan* p, int mon_id, const double* weights, const double* dA1,
                           const double* dA2, double* g_ca, double* g_cb, void* stream);
+/* The same with the gradients kept for the cells of one box only, box = (i0, j0, k0, ni, nj, nk):
+ * g_ca, g_cb are (3, ni, nj, nk); the box of a design region keeps the per-step gradient work
+ * and the stored E of each segment to that region. */
+int oem_plan_adjoint_flux_box(oem_plan* p, int mon_id, const double* weights, const double* dA1,
+                              const double* dA2, const int* box, double* g_ca, double* g_cb,
+                              void* stream);
 
 /* Time-modulated permittivity (openem/kernels/modulation.cu:40-79,
  * openem/sources_setup.py:460-518, 640-650): eps(t) = eps_s + amp cos(omega t - phi) on n_entry

@@ -41,12 +41,13 @@ def default_interval(n_steps: int) -> int:
 class FluxGradient:
     value: float          # J
     flux: np.ndarray      # P_f per monitor frequency
-    d_ca: np.ndarray      # dJ/dca, (3, nx, ny, nz)
+    d_ca: np.ndarray      # dJ/dca, (3, ni, nj, nk) over the gradient box
     d_cb: np.ndarray      # dJ/dcb
     d_eps: np.ndarray     # dJ/d eps_r per component and cell
     d_sigma: np.ndarray   # dJ/d sigma (S/m) per component and cell
     steps: int
     checkpoint_every: int
+    box: tuple = ()       # (i0, j0, k0, ni, nj, nk)
 
 
 def _refuse(sc) -> None:
@@ -93,12 +94,15 @@ def coefficient_jacobian(sc):
 
 
 def flux_gradient(sc, monitor: str | None = None, weights=None, num_steps: int | None = None,
-                  checkpoint_every: int | None = None, device: int = 0,
-                  stream=None) -> FluxGradient:
+                  checkpoint_every: int | None = None, device: int = 0, stream=None,
+                  box=None) -> FluxGradient:
     """Run the scene forward for a fixed step count with checkpoints, then the discrete adjoint;
     return ``J`` and its gradient with respect to the E-update coefficients, the relative
-    permittivity and the conductivity of every E component and cell."""
+    permittivity and the conductivity of every E component and cell of ``box = (i0, j0, k0,
+    ni, nj, nk)`` (default: the whole grid; a design region's box keeps the adjoint's gradient
+    work to that region)."""
     _refuse(sc)
+    box = tuple(int(v) for v in (box if box is not None else (0, 0, 0) + tuple(sc.shape)))
     n = int(sc.num_time_steps if num_steps is None else num_steps)
     K = int(checkpoint_every or default_interval(n))
     plan = Plan(sc, n, device=device, stream=stream, checkpoint_every=K)
@@ -114,15 +118,16 @@ def flux_gradient(sc, monitor: str | None = None, weights=None, num_steps: int |
             raise ValueError(f"{w.size} weights for {P.size} monitor frequencies")
         J = float(np.dot(w, P))
         dA1, dA2 = flux_mod.area_weights(sc.grid, axis)
-        g_ca, g_cb = plan.adjoint_flux(mid, w, dA1, dA2)
+        g_ca, g_cb = plan.adjoint_flux(mid, w, dA1, dA2, box=box)
         plan.status()
     finally:
         plan.close()
     jac = coefficient_jacobian(sc)
-    d_eps = np.stack([g_ca[c] * jac[c][0] + g_cb[c] * jac[c][1] for c in range(3)])
-    d_sig = np.stack([g_ca[c] * jac[c][2] + g_cb[c] * jac[c][3] for c in range(3)])
+    sl = tuple(slice(box[a], box[a] + box[3 + a]) for a in range(3))
+    d_eps = np.stack([g_ca[c] * jac[c][0][sl] + g_cb[c] * jac[c][1][sl] for c in range(3)])
+    d_sig = np.stack([g_ca[c] * jac[c][2][sl] + g_cb[c] * jac[c][3][sl] for c in range(3)])
     return FluxGradient(value=J, flux=P, d_ca=g_ca, d_cb=g_cb, d_eps=d_eps, d_sigma=d_sig,
-                        steps=n, checkpoint_every=K)
+                        steps=n, checkpoint_every=K, box=box)
 
 
 try:  # the torch binding is optional: the numpy API above does not need it

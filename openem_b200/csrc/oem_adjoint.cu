@@ -21,8 +21,15 @@
 // The transposed differences are gathers (one thread per cell): a cell receives its own term
 // and the terms of the cells whose neighbour it is; at a clamped wall or a PMC / symmetry plane a
 // cell can be its own neighbour, so the inverse neighbour relation is checked explicitly.
+//
+// Two launches per reverse step: k_adj_ka gathers lambda_E from the previous H-side d_bar (the
+// transposed H update of step n + 1) and then runs the E part of step n; k_adj_kb gathers
+// lambda_H from the E-side d_bar and runs the H part. Gradients are kept for the cells of one
+// box (the design region) only, from E^n and E^{n+1} of that box.
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "oem_internal.cuh"
 
@@ -96,45 +103,6 @@ __global__ void k_adj_src(YeeParams P, AdjFlux af, AdjState S, int n) {
   S.lam[3 + t2][idm] += (float)(0.5 * a[3]);
 }
 
-// reverse E update, part 1: gradient terms, adjoint psi, the six d_bar, lambda_E <- ca lambda_E
-__global__ void __launch_bounds__(128) k_adj_e_a(YeeParams P, AdjState S, const float* en0,
-                                                 const float* en1_, const float* en2,
-                                                 const float* e10, const float* e11,
-                                                 const float* e12) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z;
-  if (k >= P.nz || j >= P.ny) return;
-  const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + k;
-  const MatRec& M = P.mats[mat_of(P, id)];
-  const float* en[3] = {en0, en1_, en2};
-  const float* e1[3] = {e10, e11, e12};
-  // (axis a, psi slot) of the S_a and S_b terms of each component, d_bar index 2c and 2c+1
-  const int ax_a[3] = {1, 2, 0}, ax_b[3] = {2, 0, 1};
-  const int sl_a[3] = {0, 1, 1}, sl_b[3] = {0, 0, 1};
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const float lam = S.lam[c][id];
-    const float ca = M.ca[c], cb = M.cb[c];
-    if (lam != 0.f) {
-      const double e0 = en[c][id], e1v = e1[c][id];
-      S.gca[c][id] += (double)lam * e0;
-      if (cb != 0.f) S.gcb[c][id] += (double)lam * (e1v - (double)ca * e0) / (double)cb;
-    }
-    const float sa = cb * lam, sb = -cb * lam;
-    const int aa = ax_a[c], ab = ax_b[c];
-    const DevAxis& Aa = P.ax[aa];
-    const DevAxis& Ab = P.ax[ab];
-    const int qa = aa == 0 ? i : (aa == 1 ? j : k);
-    const int qb = ab == 0 ? i : (ab == 1 ? j : k);
-    S.dbar[2 * c][id] = dbar_of(sa, S.lpsie, aa, sl_a[c], Aa, Aa.ae, Aa.be, Aa.ke, qa, i, j, k,
-                                P.ny, P.nzp);
-    S.dbar[2 * c + 1][id] = dbar_of(sb, S.lpsie, ab, sl_b[c], Ab, Ab.ae, Ab.be, Ab.ke, qb, i,
-                                    j, k, P.ny, P.nzp);
-    S.lam[c][id] = ca * lam;
-  }
-}
-
 // index of cell (i, j, k) moved to q along axis a
 __device__ __forceinline__ int64_t moved(const YeeParams& P, int a, int i, int j, int k, int q) {
   if (a == 0) i = q;
@@ -193,47 +161,11 @@ __device__ __forceinline__ float gather_fwd(const YeeParams& P, const float* db,
   return v;
 }
 
-// reverse E update, part 2: lambda_H gathers the transposed backward differences
-__global__ void __launch_bounds__(128) k_adj_e_b(YeeParams P, AdjState S) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z;
-  if (k >= P.nz || j >= P.ny) return;
-  const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + k;
-  // Hz: Ex y-term (0), Ey x-term (3); Hy: Ex z-term (1), Ez x-term (4); Hx: Ey z-term (2),
-  // Ez y-term (5)
-  S.lam[5][id] += gather_bwd(P, S.dbar[0], 1, i, j, k) + gather_bwd(P, S.dbar[3], 0, i, j, k);
-  S.lam[4][id] += gather_bwd(P, S.dbar[1], 2, i, j, k) + gather_bwd(P, S.dbar[4], 0, i, j, k);
-  S.lam[3][id] += gather_bwd(P, S.dbar[2], 2, i, j, k) + gather_bwd(P, S.dbar[5], 1, i, j, k);
-}
-
-// reverse H update, part 1: adjoint psi and the six d_bar (lambda_H passes through)
-__global__ void __launch_bounds__(128) k_adj_h_a(YeeParams P, AdjState S) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z;
-  if (k >= P.nz || j >= P.ny) return;
-  const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + k;
-  const int ax_a[3] = {1, 2, 0}, ax_b[3] = {2, 0, 1};
-  const int sl_a[3] = {0, 1, 1}, sl_b[3] = {0, 0, 1};
-#pragma unroll
-  for (int h = 0; h < 3; ++h) {
-    const float lam = S.lam[3 + h][id];
-    const float sa = -P.ch * lam, sb = P.ch * lam;
-    const int aa = ax_a[h], ab = ax_b[h];
-    const DevAxis& Aa = P.ax[aa];
-    const DevAxis& Ab = P.ax[ab];
-    const int qa = aa == 0 ? i : (aa == 1 ? j : k);
-    const int qb = ab == 0 ? i : (ab == 1 ? j : k);
-    S.dbar[2 * h][id] = dbar_of(sa, S.lpsih, aa, sl_a[h], Aa, Aa.ah, Aa.bh, Aa.kh, qa, i, j, k,
-                                P.ny, P.nzp);
-    S.dbar[2 * h + 1][id] = dbar_of(sb, S.lpsih, ab, sl_b[h], Ab, Ab.ah, Ab.bh, Ab.kh, qb, i,
-                                    j, k, P.ny, P.nzp);
-  }
-}
-
-// reverse H update, part 2: lambda_E gathers the transposed forward differences
-__global__ void __launch_bounds__(128) k_adj_h_b(YeeParams P, AdjState S) {
+// reverse step n, E side: lambda_E += transposed forward differences of the H-side d_bar (the
+// H update of step n + 1), then the gradient terms (box cells), the adjoint psi, the six E-side
+// d_bar and lambda_E <- ca lambda_E
+__global__ void __launch_bounds__(128) k_adj_ka(YeeParams P, AdjState S, const float* en_box,
+                                                const float* en1_box) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
@@ -241,9 +173,86 @@ __global__ void __launch_bounds__(128) k_adj_h_b(YeeParams P, AdjState S) {
   const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + k;
   // Ez: Hx y-term (0), Hy x-term (3); Ey: Hx z-term (1), Hz x-term (4); Ex: Hy z-term (2),
   // Hz y-term (5)
-  S.lam[2][id] += gather_fwd(P, S.dbar[0], 1, i, j, k) + gather_fwd(P, S.dbar[3], 0, i, j, k);
-  S.lam[1][id] += gather_fwd(P, S.dbar[1], 2, i, j, k) + gather_fwd(P, S.dbar[4], 0, i, j, k);
-  S.lam[0][id] += gather_fwd(P, S.dbar[2], 2, i, j, k) + gather_fwd(P, S.dbar[5], 1, i, j, k);
+  float lam[3];
+  lam[2] = S.lam[2][id] + (gather_fwd(P, S.dbarh[0], 1, i, j, k) + gather_fwd(P, S.dbarh[3], 0, i, j, k));
+  lam[1] = S.lam[1][id] + (gather_fwd(P, S.dbarh[1], 2, i, j, k) + gather_fwd(P, S.dbarh[4], 0, i, j, k));
+  lam[0] = S.lam[0][id] + (gather_fwd(P, S.dbarh[2], 2, i, j, k) + gather_fwd(P, S.dbarh[5], 1, i, j, k));
+  const MatRec& M = P.mats[mat_of(P, id)];
+  const int bi = i - S.box[0], bj = j - S.box[1], bk = k - S.box[2];
+  const bool inbox = bi >= 0 && bi < S.box[3] && bj >= 0 && bj < S.box[4] && bk >= 0 &&
+                     bk < S.box[5];
+  const int64_t nb = (int64_t)S.box[3] * S.box[4] * S.box[5];
+  const int64_t t = inbox ? ((int64_t)bi * S.box[4] + bj) * S.box[5] + bk : 0;
+  // (axis a, psi slot) of the S_a and S_b terms of each component, d_bar index 2c and 2c+1
+  const int ax_a[3] = {1, 2, 0}, ax_b[3] = {2, 0, 1};
+  const int sl_a[3] = {0, 1, 1}, sl_b[3] = {0, 0, 1};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float ca = M.ca[c], cb = M.cb[c];
+    if (inbox && lam[c] != 0.f) {
+      const double e0 = en_box[c * nb + t], e1v = en1_box[c * nb + t];
+      S.gca[c][t] += (double)lam[c] * e0;
+      if (cb != 0.f) S.gcb[c][t] += (double)lam[c] * (e1v - (double)ca * e0) / (double)cb;
+    }
+    const float sa = cb * lam[c], sb = -cb * lam[c];
+    const int aa = ax_a[c], ab = ax_b[c];
+    const DevAxis& Aa = P.ax[aa];
+    const DevAxis& Ab = P.ax[ab];
+    const int qa = aa == 0 ? i : (aa == 1 ? j : k);
+    const int qb = ab == 0 ? i : (ab == 1 ? j : k);
+    S.dbare[2 * c][id] = dbar_of(sa, S.lpsie, aa, sl_a[c], Aa, Aa.ae, Aa.be, Aa.ke, qa, i, j, k,
+                                 P.ny, P.nzp);
+    S.dbare[2 * c + 1][id] = dbar_of(sb, S.lpsie, ab, sl_b[c], Ab, Ab.ae, Ab.be, Ab.ke, qb, i,
+                                     j, k, P.ny, P.nzp);
+    S.lam[c][id] = ca * lam[c];
+  }
+}
+
+// reverse step n, H side: lambda_H += transposed backward differences of the E-side d_bar, then
+// the adjoint psi and the six H-side d_bar (lambda_H passes through)
+__global__ void __launch_bounds__(128) k_adj_kb(YeeParams P, AdjState S) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= P.nz || j >= P.ny) return;
+  const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + k;
+  // Hz: Ex y-term (0), Ey x-term (3); Hy: Ex z-term (1), Ez x-term (4); Hx: Ey z-term (2),
+  // Ez y-term (5)
+  float lam[3];
+  lam[2] = S.lam[5][id] + (gather_bwd(P, S.dbare[0], 1, i, j, k) + gather_bwd(P, S.dbare[3], 0, i, j, k));
+  lam[1] = S.lam[4][id] + (gather_bwd(P, S.dbare[1], 2, i, j, k) + gather_bwd(P, S.dbare[4], 0, i, j, k));
+  lam[0] = S.lam[3][id] + (gather_bwd(P, S.dbare[2], 2, i, j, k) + gather_bwd(P, S.dbare[5], 1, i, j, k));
+  const int ax_a[3] = {1, 2, 0}, ax_b[3] = {2, 0, 1};
+  const int sl_a[3] = {0, 1, 1}, sl_b[3] = {0, 0, 1};
+#pragma unroll
+  for (int h = 0; h < 3; ++h) {
+    S.lam[3 + h][id] = lam[h];
+    const float sa = -P.ch * lam[h], sb = P.ch * lam[h];
+    const int aa = ax_a[h], ab = ax_b[h];
+    const DevAxis& Aa = P.ax[aa];
+    const DevAxis& Ab = P.ax[ab];
+    const int qa = aa == 0 ? i : (aa == 1 ? j : k);
+    const int qb = ab == 0 ? i : (ab == 1 ? j : k);
+    S.dbarh[2 * h][id] = dbar_of(sa, S.lpsih, aa, sl_a[h], Aa, Aa.ah, Aa.bh, Aa.kh, qa, i, j, k,
+                                 P.ny, P.nzp);
+    S.dbarh[2 * h + 1][id] = dbar_of(sb, S.lpsih, ab, sl_b[h], Ab, Ab.ah, Ab.bh, Ab.kh, qb, i,
+                                     j, k, P.ny, P.nzp);
+  }
+}
+
+// E of the box cells into a (3, box) buffer (the step's E for the gradient terms)
+__global__ void k_adj_snap(YeeParams P, AdjState S, float* dst) {
+  const int64_t nb = (int64_t)S.box[3] * S.box[4] * S.box[5];
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int bk = (int)(t % S.box[5]);
+    const int64_t r = t / S.box[5];
+    const int bj = (int)(r % S.box[4]), bi = (int)(r / S.box[4]);
+    const int64_t id = ((int64_t)(S.box[0] + bi) * P.ny + (S.box[1] + bj)) * P.nzp + (S.box[2] + bk);
+    dst[t] = P.f[0][id];
+    dst[nb + t] = P.f[1][id];
+    dst[2 * nb + t] = P.f[2][id];
+  }
 }
 
 }  // namespace
@@ -255,22 +264,20 @@ cudaError_t launch_adj_src(const YeeParams& P, const AdjFlux& a, const AdjState&
   return cudaGetLastError();
 }
 
-cudaError_t launch_adj_e(const YeeParams& P, const AdjState& S, const float* const en[3],
-                         const float* const en1[3], cudaStream_t s) {
+cudaError_t launch_adj_step(const YeeParams& P, const AdjState& S, const float* en_box,
+                            const float* en1_box, cudaStream_t s) {
   dim3 b(32, 4, 1), g((P.nzp + 31) / 32, (P.ny + 3) / 4, P.nx);
-  k_adj_e_a<<<g, b, 0, s>>>(P, S, en[0], en[1], en[2], en1[0], en1[1], en1[2]);
+  k_adj_ka<<<g, b, 0, s>>>(P, S, en_box, en1_box);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_adj_e_b<<<g, b, 0, s>>>(P, S);
+  k_adj_kb<<<g, b, 0, s>>>(P, S);
   return cudaGetLastError();
 }
 
-cudaError_t launch_adj_h(const YeeParams& P, const AdjState& S, cudaStream_t s) {
-  dim3 b(32, 4, 1), g((P.nzp + 31) / 32, (P.ny + 3) / 4, P.nx);
-  k_adj_h_a<<<g, b, 0, s>>>(P, S);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  k_adj_h_b<<<g, b, 0, s>>>(P, S);
+cudaError_t launch_adj_snap(const YeeParams& P, const AdjState& S, float* dst, cudaStream_t s) {
+  const int64_t nb = (int64_t)S.box[3] * S.box[4] * S.box[5];
+  const int blocks = (int)std::min<int64_t>((nb + 255) / 256, 148 * 8);
+  k_adj_snap<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(P, S, dst);
   return cudaGetLastError();
 }
 

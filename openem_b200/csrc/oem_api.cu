@@ -808,8 +808,19 @@ int oem_plan_enable_checkpoints(oem_plan* p, int k) {
 
 int oem_plan_adjoint_flux(oem_plan* p, int mon_id, const double* weights, const double* dA1,
                           const double* dA2, double* g_ca, double* g_cb, void* stream) {
+  if (!p) return set_error(OEM_ERR_INVALID, "null plan");
+  const int box[6] = {0, 0, 0, p->nx, p->ny, p->nz};
+  return oem_plan_adjoint_flux_box(p, mon_id, weights, dA1, dA2, box, g_ca, g_cb, stream);
+}
+
+int oem_plan_adjoint_flux_box(oem_plan* p, int mon_id, const double* weights, const double* dA1,
+                              const double* dA2, const int* box, double* g_ca, double* g_cb,
+                              void* stream) {
   int rc = check_plan(p, true);
   if (rc) return rc;
+  if (!box || box[3] < 1 || box[4] < 1 || box[5] < 1 || box[0] < 0 || box[1] < 0 ||
+      box[2] < 0 || box[0] + box[3] > p->nx || box[1] + box[4] > p->ny || box[2] + box[5] > p->nz)
+    return set_error(OEM_ERR_INVALID, "gradient box outside the grid");
   if (p->ckpt_k < 1) return set_error(OEM_ERR_STATE, "checkpoints were not enabled");
   if (p->steps != p->n_total) return set_error(OEM_ERR_STATE, "run the whole forward pass first");
   if (mon_id < 0 || mon_id >= (int)p->mons.size() || p->mons[mon_id].kind != 0)
@@ -872,11 +883,14 @@ int oem_plan_adjoint_flux(oem_plan* p, int mon_id, const double* weights, const 
   AdjFlux af{};
   double* dcoef = nullptr;
   float* seg = nullptr;
+  for (int q = 0; q < 6; ++q) S.box[q] = box[q];
+  const size_t nb = (size_t)box[3] * box[4] * box[5];
   rc = OEM_OK;
   for (int c = 0; c < 6 && !rc; ++c) rc = alloc(&S.lam[c], ncp);
-  for (int c = 0; c < 6 && !rc; ++c) rc = alloc(&S.dbar[c], ncp);
-  for (int c = 0; c < 3 && !rc; ++c) rc = alloc(&S.gca[c], ncp);
-  for (int c = 0; c < 3 && !rc; ++c) rc = alloc(&S.gcb[c], ncp);
+  for (int c = 0; c < 6 && !rc; ++c) rc = alloc(&S.dbare[c], ncp);
+  for (int c = 0; c < 6 && !rc; ++c) rc = alloc(&S.dbarh[c], ncp);
+  for (int c = 0; c < 3 && !rc; ++c) rc = alloc(&S.gca[c], nb);
+  for (int c = 0; c < 3 && !rc; ++c) rc = alloc(&S.gcb[c], nb);
   for (int a = 0; a < 3 && !rc; ++a)
     for (int side = 0; side < 2 && !rc; ++side) {
       const int L = side == 0 ? p->axh[a].lo : p->axh[a].hi;
@@ -889,7 +903,7 @@ int oem_plan_adjoint_flux(oem_plan* p, int mon_id, const double* weights, const 
       }
     }
   if (!rc) rc = alloc(&dcoef, coef.size());
-  if (!rc) rc = alloc(&seg, (size_t)(K + 1) * 3 * ncp);
+  if (!rc) rc = alloc(&seg, (size_t)(K + 1) * 3 * nb);
   if (rc) {
     release();
     return rc;
@@ -905,39 +919,28 @@ int oem_plan_adjoint_flux(oem_plan* p, int mon_id, const double* weights, const 
   cudaError_t e = cudaSuccess;
   for (int64_t sg = nseg - 1; sg >= 0 && !rc; --sg) {
     const int64_t n0 = sg * K, n1 = std::min<int64_t>(N, n0 + K);
-    // recompute the segment from its checkpoint, keeping E at every step
+    // recompute the segment from its checkpoint, keeping E of the box at every step
     if ((rc = load_state(p, (int)sg, s))) break;
     for (int64_t t = 0; t <= n1 - n0 && !rc; ++t) {
       if (t > 0) rc = enqueue_step(p, s, false);
-      for (int c = 0; c < 3 && !rc; ++c)
-        if ((e = cudaMemcpyAsync(seg + ((size_t)t * 3 + c) * ncp, P.f[c], ncp * sizeof(float),
-                                 cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
-          rc = cuda_error(e, "segment copy");
+      if (!rc && (e = launch_adj_snap(P, S, seg + (size_t)t * 3 * nb, s)) != cudaSuccess)
+        rc = cuda_error(e, "segment copy");
     }
     for (int64_t n = n1 - 1; n >= n0 && !rc; --n) {
-      const float* en[3];
-      const float* en1[3];
-      for (int c = 0; c < 3; ++c) {
-        en[c] = seg + ((size_t)(n - n0) * 3 + c) * ncp;
-        en1[c] = seg + ((size_t)(n - n0 + 1) * 3 + c) * ncp;
-      }
+      const float* en = seg + (size_t)(n - n0) * 3 * nb;
+      const float* en1 = seg + (size_t)(n - n0 + 1) * 3 * nb;
       if ((e = launch_adj_src(P, af, S, (int)n, s)) != cudaSuccess) rc = cuda_error(e, "adj_src");
-      if (!rc && (e = launch_adj_e(P, S, en, en1, s)) != cudaSuccess) rc = cuda_error(e, "adj_e");
-      if (!rc && (e = launch_adj_h(P, S, s)) != cudaSuccess) rc = cuda_error(e, "adj_h");
+      if (!rc && (e = launch_adj_step(P, S, en, en1, s)) != cudaSuccess)
+        rc = cuda_error(e, "adj_step");
     }
   }
-  if (!rc) {
-    for (int c = 0; c < 3 && !rc; ++c) {
-      const size_t plane_bytes = (size_t)p->nz * sizeof(double);
-      if ((e = cudaMemcpy2DAsync(g_ca + (size_t)c * p->nx * p->ny * p->nz, plane_bytes, S.gca[c],
-                                 (size_t)p->nzp * sizeof(double), plane_bytes,
-                                 (size_t)p->nx * p->ny, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-          (e = cudaMemcpy2DAsync(g_cb + (size_t)c * p->nx * p->ny * p->nz, plane_bytes, S.gcb[c],
-                                 (size_t)p->nzp * sizeof(double), plane_bytes,
-                                 (size_t)p->nx * p->ny, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+  if (!rc)
+    for (int c = 0; c < 3 && !rc; ++c)
+      if ((e = cudaMemcpyAsync(g_ca + (size_t)c * nb, S.gca[c], nb * sizeof(double),
+                               cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+          (e = cudaMemcpyAsync(g_cb + (size_t)c * nb, S.gcb[c], nb * sizeof(double),
+                               cudaMemcpyDeviceToHost, s)) != cudaSuccess)
         rc = cuda_error(e, "gradient readout");
-    }
-  }
   release();
   return rc;
 }

@@ -423,8 +423,10 @@ cudaError_t launch_tfsf(const YeeParams& P, const Tfsf& t, int is_e, const int* 
 struct AdjState {
   float* lam[6];      // adjoint of Ex Ey Ez Hx Hy Hz (padded)
   PsiSet lpsih, lpsie;  // adjoint psi
-  float* dbar[6];     // per-cell adjoint of the six differences of one half step
-  double* gca[3];     // sum over steps of lambda_E^{n+1} E^n
+  float* dbare[6];    // per-cell adjoint of the six differences of the E update
+  float* dbarh[6];    // ... and of the H update
+  int box[6];         // gradient box: i0, j0, k0, ni, nj, nk
+  double* gca[3];     // per box cell: sum over steps of lambda_E^{n+1} E^n
   double* gcb[3];     // sum over steps of lambda_E^{n+1} T^n, T^n = (E^{n+1} - ca E^n) / cb
 };
 struct AdjFlux {      // objective sources of one flux plane (see oem_adjoint.cu)
@@ -434,9 +436,9 @@ struct AdjFlux {      // objective sources of one flux plane (see oem_adjoint.cu
 };
 cudaError_t launch_adj_src(const YeeParams& P, const AdjFlux& a, const AdjState& S, int n,
                            cudaStream_t s);
-cudaError_t launch_adj_e(const YeeParams& P, const AdjState& S, const float* const en[3],
-                         const float* const en1[3], cudaStream_t s);
-cudaError_t launch_adj_h(const YeeParams& P, const AdjState& S, cudaStream_t s);
+cudaError_t launch_adj_step(const YeeParams& P, const AdjState& S, const float* en_box,
+                            const float* en1_box, cudaStream_t s);
+cudaError_t launch_adj_snap(const YeeParams& P, const AdjState& S, float* dst, cudaStream_t s);
 cudaError_t launch_mode_h(const YeeParams& P, const ModeSrc& m, const int* step, cudaStream_t s);
 cudaError_t launch_mode_e(const YeeParams& P, const ModeSrc& m, const int* step, cudaStream_t s);
 cudaError_t launch_energy(const YeeParams& P, double* const dl[3][2], double* part, int nblocks,

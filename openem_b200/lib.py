@@ -47,6 +47,7 @@ SIGNATURES = {
     "oem_plan_read_flux_time": (_I, [_P, _I, _P, _P]),
     "oem_plan_add_modulation": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _D]),
     "oem_plan_adjoint_flux": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
+    "oem_plan_adjoint_flux_box": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _P]),
     "oem_plan_add_flux_monitor": (_I, [_P, _I, _I, _I, _L, _P, _I, C.POINTER(_I)]),
     "oem_plan_add_box_monitor": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _L, _P, _I,
                                       C.POINTER(_I)]),

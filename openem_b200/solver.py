@@ -315,17 +315,20 @@ class Plan:
                 "read_monitor")
         return re + 1j * im
 
-    def adjoint_flux(self, mid: int, weights, dA1, dA2):
-        """dJ/dca and dJ/dcb, (3, nx, ny, nz) float64 each, of ``J = sum_f weights[f] P_f``
-        for the flux monitor ``mid`` (face elements ``dA1``, ``dA2`` of its two terms)."""
+    def adjoint_flux(self, mid: int, weights, dA1, dA2, box=None):
+        """dJ/dca and dJ/dcb, (3, ni, nj, nk) float64 each, of ``J = sum_f weights[f] P_f``
+        for the flux monitor ``mid`` (face elements ``dA1``, ``dA2`` of its two terms), over
+        ``box = (i0, j0, k0, ni, nj, nk)`` (default: the whole grid)."""
         w = np.ascontiguousarray(weights, dtype=np.float64)
         a1 = np.ascontiguousarray(dA1, dtype=np.float64)
         a2 = np.ascontiguousarray(dA2, dtype=np.float64)
-        g_ca = np.empty((3,) + self.shape, np.float64)
-        g_cb = np.empty((3,) + self.shape, np.float64)
-        L.check(self.lib.oem_plan_adjoint_flux(self.h, int(mid), L.ptr(w), L.ptr(a1), L.ptr(a2),
-                                               L.ptr(g_ca), L.ptr(g_cb), self._s),
-                "adjoint_flux")
+        b = np.asarray(box if box is not None else (0, 0, 0) + self.shape, dtype=np.int32)
+        b = np.ascontiguousarray(b)
+        g_ca = np.empty((3,) + tuple(int(v) for v in b[3:]), np.float64)
+        g_cb = np.empty_like(g_ca)
+        L.check(self.lib.oem_plan_adjoint_flux_box(self.h, int(mid), L.ptr(w), L.ptr(a1),
+                                                   L.ptr(a2), L.ptr(b), L.ptr(g_ca),
+                                                   L.ptr(g_cb), self._s), "adjoint_flux")
         return g_ca, g_cb
 
     def read_time_monitor(self, mid: int, shape) -> np.ndarray:
