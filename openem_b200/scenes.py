@@ -342,14 +342,54 @@ def tfsf_source(grid: Grid, dt: float, num_steps: int, eps_u: np.ndarray, box_lo
                       pol_u=float(pol[0]), pol_v=float(pol[1]), sigma1=sigma1)
 
 
+def tfsf_oblique_source(grid: Grid, dt: float, num_steps: int, box_lo, box_hi, k_hat, e_hat,
+                        axis: int = 2, eps_bg: float = 1.0, source_time=None,
+                        open_axes=()) -> TFSFSource:
+    """An oblique-incidence TFSF box source (``openem/scene/sources.py:928-997``): the 1D line
+    runs along +k_hat with the cell size matched to the grid's discrete dispersion at the pulse's
+    centre frequency, spans the box's projection on k_hat (two cells before it, three after)
+    plus a runway at both ends, and is injected two cells before the projection's start. The
+    amplitude is scaled by 1/sqrt(|k_axis|) (the same power per area of the injection plane as at
+    normal incidence)."""
+    from openem_b200 import tfsf as TF
+    k = np.asarray(k_hat, np.float64)
+    k = k / np.linalg.norm(k)
+    e = np.asarray(e_hat, np.float64)
+    e = e - (e @ k) * k
+    e = e / np.linalg.norm(e)
+    pulse = source_time or GaussianPulse(freq0=3e14, fwidth=1e14)
+    lo, hi = [int(x) for x in box_lo], [int(x) for x in box_hi]
+    dl_axes = [float(grid.axes[q].dl[min(lo[q], grid.axes[q].n - 1)]) for q in range(3)]
+    dl1v = TF.matched_dl(k, dl_axes, dt, float(pulse.freq0), eps_r=eps_bg)
+    pmin, pmax = TF.projection_range(grid, k, lo, hi)
+    proj0 = pmin - 2.0 * dl1v
+    n_col_e = int(np.ceil((pmax - proj0) / dl1v)) + 3
+    n_run = TF.runway_cells(num_steps, dt, dl1v)
+    dl1 = np.full(2 * n_run + n_col_e, dl1v)
+    eps1 = np.full(dl1.size, float(eps_bg))
+    col0 = n_run
+    inj = col0 - TF.GAP // 2
+    ex_inc, hy_inc = plane_wave_tables(pulse, dt, num_steps, 0.5 * dl1v, float(eps_bg), +1)
+    u, v = TF.cyclic_axes(axis)
+    return TFSFSource(direction=+1, box_lo=tuple(lo), box_hi=tuple(hi), dl1=dl1, eps1=eps1,
+                      inj=int(inj), col0=int(col0), ex_inc=ex_inc, hy_inc=hy_inc,
+                      waveform=sample_waveform(pulse, dt, num_steps), axis=axis,
+                      pol_u=float(e[u]), pol_v=float(e[v]), k_hat=tuple(float(x) for x in k),
+                      e_hat=tuple(float(x) for x in e), dl1_step=float(dl1v),
+                      proj0=float(proj0), n_col_e=int(n_col_e), open_axes=tuple(open_axes),
+                      amp_scale=float(1.0 / np.sqrt(abs(float(k[axis])))))
+
+
 def tfsf_box_scene(n: int = 40, n_pml: int = 8, dl: float = 0.02 * UM, axis: int = 2,
                    direction: int = 1, pol=(1.0, 0.0), margin: int = 5, sphere_eps: float = 0.0,
                    sphere_r: float = 0.1 * UM, substrate_eps: float = 0.0,
-                   num_steps: int = 300) -> Scene:
+                   num_steps: int = 300, k_hat=None, e_hat=None, freq0: float = 3e14,
+                   fwidth: float = 1e14) -> Scene:
     """An n^3 grid with CPML on every face and a TFSF box ``margin`` cells inside the CPML; a
     dielectric sphere at the centre (``sphere_eps`` > 0), a substrate filling the lower half
     along ``axis`` (``substrate_eps`` > 0, transversely uniform so it crosses the box), and a
-    normal-incidence pulse along ``axis`` with polarisation ``pol`` on (u, v)."""
+    normal-incidence pulse along ``axis`` with polarisation ``pol`` on (u, v) -- or, with
+    ``k_hat`` and ``e_hat``, an oblique one."""
     n_in = n - 2 * n_pml
     axes = [uniform_axis(n_in, dl, -0.5 * n_in * dl, "PML", n_pml) for _ in range(3)]
     grid = Grid(*axes)
@@ -371,8 +411,13 @@ def tfsf_box_scene(n: int = 40, n_pml: int = 8, dl: float = 0.02 * UM, axis: int
     lo = (n_pml + margin,) * 3
     hi = (n - n_pml - margin,) * 3
     u = (axis + 1) % 3
-    src = tfsf_source(grid, dt, num_steps, eps[u], lo, hi, axis=axis, direction=direction,
-                      pol=pol)
+    pulse = GaussianPulse(freq0=freq0, fwidth=fwidth)
+    if k_hat is not None:
+        src = tfsf_oblique_source(grid, dt, num_steps, lo, hi, k_hat, e_hat, axis=axis,
+                                  source_time=pulse)
+    else:
+        src = tfsf_source(grid, dt, num_steps, eps[u], lo, hi, axis=axis, direction=direction,
+                          pol=pol, source_time=pulse)
     return Scene(grid=grid, dt=dt, num_time_steps=num_steps, shutoff=1e-5, eps_ex=eps[0],
                  eps_ey=eps[1], eps_ez=eps[2], pml=pml_dict(grid, dt, n_pml),
                  tfsf_sources=[src])

@@ -31,8 +31,8 @@ def refuse_unsupported(sc) -> None:
     """Fail closed on scene features outside this engine's real-field path."""
     checks = [
         (T.dispersion_in_absorbers(sc), "dispersive media inside Absorber layers"),
-        (any(getattr(t, "k_hat", None) is not None or getattr(t, "open_axes", ())
-             for t in getattr(sc, "tfsf_sources", [])), "oblique or open-axis TFSF boxes"),
+        (any(getattr(t, "k_hat", None) is None and getattr(t, "open_axes", ())
+             for t in getattr(sc, "tfsf_sources", [])), "open-axis TFSF boxes at normal incidence"),
         (len(getattr(sc, "tfsf_sources", [])) > 1, "several TFSF boxes in one scene"),
         (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry > 0,
          "slanted-interface mixed dispersion"),

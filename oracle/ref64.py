@@ -205,11 +205,10 @@ class Oracle:
         if not getattr(sc, "tfsf_sources", None):
             return
         t = sc.tfsf_sources[0]
-        if getattr(t, "k_hat", None) is not None:
-            raise NotImplementedError("oracle: oblique TFSF not transcribed")
+        oblique = getattr(t, "k_hat", None) is not None
         a = int(t.axis)
         lo, hi = [int(x) for x in t.box_lo], [int(x) for x in t.box_hi]
-        nk = hi[a] - lo[a] + 1
+        nk = int(t.n_col_e) if oblique else hi[a] - lo[a] + 1
         dl1 = np.asarray(t.dl1, np.float64)
         eps1 = np.asarray(t.eps1, np.float64)
         n1 = dl1.size
@@ -238,7 +237,8 @@ class Oracle:
             e1[1:] = ca1[1:] * e1[1:] - cb1[1:] * (h1[1:] - h1[:-1])
             e1[inj] += ce_inj * scale * float(t.hy_inc[n])
             ex_tab[n + 1] = e1[col0:col0 + nk]
-        self.tfsf = {"t": t, "a": a, "lo": lo, "hi": hi, "nk": nk, "ex": ex_tab, "hy": hy_tab}
+        self.tfsf = {"t": t, "a": a, "lo": lo, "hi": hi, "nk": nk, "ex": ex_tab, "hy": hy_tab,
+                     "oblique": oblique}
 
     def inject_tfsf(self, side, n):
         """The box-face corrections of step n (the 16 terms of
@@ -246,6 +246,9 @@ class Oracle:
         H^{n+1/2}."""
         tf = getattr(self, "tfsf", None)  # the complex path has no TFSF box
         if tf is None:
+            return
+        if tf["oblique"]:
+            self._inject_tfsf_oblique(side, n)
             return
         t, a, lo, hi, nk = tf["t"], tf["a"], tf["lo"], tf["hi"], tf["nk"]
         u, v = (a + 1) % 3, (a + 2) % 3
@@ -306,6 +309,81 @@ class Oracle:
                 for idx, sg in ((lo[v], -1.0), (hi[v], 1.0)):
                     r = region(v, idx, u, hi[u] + 1, a, hi[a])
                     E[a][r] += cb[a][r] * sg * bv / dld[v][idx] * col_along_a(ra, a, u)
+
+    def _inject_tfsf_oblique(self, side, n):
+        """Oblique box (openem/tfsf_oblique.py): for each term s dF_r/dn of (curl F)_m in the
+        cyclic basis (u, v, a), the incident component r is evaluated at its own Yee points
+        beside the face by projecting them on k_hat and interpolating the 1D line (H values at
+        half cells); E_m gets -+ s h_r / dl*_n (times cb) on the total-field side of the n faces,
+        H_m gets +- ch s e_r / dl_n on the scattered-field side."""
+        tf = self.tfsf
+        t, lo, hi = tf["t"], tf["lo"], tf["hi"]
+        a = tf["a"]
+        uva = ((a + 1) % 3, (a + 2) % 3, a)
+        curl = {0: ((2, 1, 1.0), (1, 2, -1.0)), 1: ((0, 2, 1.0), (2, 0, -1.0)),
+                2: ((1, 0, 1.0), (0, 1, -1.0))}
+        k = np.asarray(t.k_hat, np.float64)
+        e_vec = np.asarray(t.e_hat, np.float64)
+        h_vec = np.cross(k, e_vec)
+        dl1, proj0 = float(t.dl1_step), float(t.proj0)
+        open_axes = tuple(getattr(t, "open_axes", ()))
+        axes = self.sc.grid.axes
+
+        def coords(comp, magnetic, w):
+            edge = (w == comp) if magnetic else (w != comp)
+            ax = axes[w]
+            return np.asarray(ax.edges[:-1] if edge else ax.centers, np.float64)
+
+        def span(comp, magnetic, w):
+            edge = (w == comp) if magnetic else (w != comp)
+            return slice(lo[w], hi[w] + (1 if edge else 0))
+
+        def interp(row, pos):
+            i0 = np.floor(pos).astype(np.int64)
+            w = pos - i0
+            bad_lo, bad_hi = i0 < 0, i0 >= row.size - 1
+            i0 = np.clip(i0, 0, row.size - 1)
+            w = np.where(bad_lo | bad_hi, 0.0, w)
+            i1 = np.minimum(i0 + 1, row.size - 1)
+            return row[i0] + w * (row[i1] - row[i0])
+
+        e_side = side == "e"
+        row = tf["hy"][n] if e_side else tf["ex"][n]
+        for m in range(3):
+            for (r, nn, sg) in curl[m]:
+                nax = uva[nn]
+                if nax in open_axes:
+                    continue
+                comp, inc = uva[m], uva[r]
+                dld = np.asarray(axes[nax].dl_dual, np.float64)
+                dl = np.asarray(axes[nax].dl, np.float64)
+                if e_side:
+                    sides = ((lo[nax], -sg * h_vec[inc] / dld[lo[nax]], lo[nax] - 1),
+                             (hi[nax], sg * h_vec[inc] / dld[hi[nax]], hi[nax]))
+                else:
+                    sides = ((lo[nax] - 1, self.ch * sg * e_vec[inc] / dl[lo[nax] - 1], lo[nax]),
+                             (hi[nax], -self.ch * sg * e_vec[inc] / dl[hi[nax]], hi[nax]))
+                for fx, cf, inc_n in sides:
+                    if cf == 0.0:
+                        continue
+                    sl = [None, None, None]
+                    grids = [None, None, None]
+                    for w in range(3):
+                        if w == nax:
+                            sl[w] = slice(fx, fx + 1)
+                            grids[w] = np.array([coords(inc, e_side, w)[inc_n]])
+                        else:
+                            sp = span(comp, not e_side, w)
+                            sl[w] = sp
+                            grids[w] = coords(inc, e_side, w)[sp]
+                    X, Y, Z = np.meshgrid(*grids, indexing="ij")
+                    pos = (k[0] * X + k[1] * Y + k[2] * Z - proj0) / dl1 + (0.5 if e_side else 0.0)
+                    val = interp(row, pos)
+                    sl = tuple(sl)
+                    if e_side:
+                        self.E[comp][sl] += self.cb[comp][sl] * cf * val
+                    else:
+                        self.H[comp][sl] += cf * val
 
     def _setup_dispersion(self):
         d = self.sc.dispersion

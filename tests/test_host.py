@@ -125,7 +125,7 @@ def test_unsupported_physics_fails_closed(feature):
     sd = scenes.small_dispersive(n=20, n_sph=1, n_pml=4, num_steps=10)
     bad = {
         "tfsf": replace(sc, tfsf_sources=[replace(
-            scenes.tfsf_box_scene(n=30, num_steps=10).tfsf_sources[0], k_hat=(0.0, 0.5, 0.87))]),
+            scenes.tfsf_box_scene(n=30, num_steps=10).tfsf_sources[0], open_axes=(0,))]),
         "disp_in_absorber": replace(sd, absorbers=scenes.absorber_slabs(sd.grid, 0, 10)),
         "modulation_pec": replace(sc, pec_ex=np.array([5]), modulation=M.TimeModulation(
             1e14, np.array([0]), np.array([0]), np.array([0.1]), np.array([0.0]))),
