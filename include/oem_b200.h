@@ -197,6 +197,16 @@ int oem_plan_add_tfsf(oem_plan* p, int n_e, const oem_tfsf_face* e_faces, int n_
                       const oem_tfsf_face* h_faces, int ex_rows, int ex_n, const double* ex_tab,
                       int hy_rows, int hy_n, const double* hy_tab);
 
+/* Fully anisotropic cells (openem/kernels/tensor.cu, openem/model.py:674-786): n_entry
+ * (comp, cell) entries, cell = (i ny + j) nz + k, with the rows of M1 = A^-1 B and
+ * M2 = (dt / eps0) A^-1 of their component (n x 3, A = eps + s, B = eps - s, s = sigma dt / 2eps0)
+ * and the PEC-wall factor of the written value. The cells' material records must pass the curl
+ * through (ca = 0, cb = 1); each step rhs = M1 <E^n> before the E update and
+ * E^{n+1} = rhs + M2 <curl H - J> after the E-side injection, the other two components averaged
+ * over four neighbours. The table must be closed under that stencil. */
+int oem_plan_add_tensor(oem_plan* p, int n_entry, const int* comp, const int64_t* cell,
+                        const float* m1, const float* m2, const float* pec);
+
 /* Absorber boundary slab (Tidy3D's Absorber; replaces absorb_slab / absorb_batch,
  * openem/kernels/absorber.cu:20-70, absorb_batch.cu:15-110, and the host tables of
  * openem/dispersion_setup.py:89-120): layers [g0, g0 + nlay) along `axis`. After the H-side

@@ -289,6 +289,8 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
   if (p->fused) {
     for (const Modulation& m : p->mods)
       if ((e = launch_modulate(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "modulate");
+    for (const TensorSet& t : p->tensors)
+      if ((e = launch_tensor_pre(P, t, s)) != cudaSuccess) return cuda_error(e, "tensor_pre");
     if (P.has_ade && (e = launch_ade_segments(P, p->d_ade_segs, p->n_ade_segs,
                                               (int64_t)p->nx * p->ny * p->nzp / 32, 0, s)) !=
                          cudaSuccess)
@@ -308,6 +310,8 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
   const bool fork = p->side_stream != nullptr;
   for (const Modulation& m : p->mods)
     if ((e = launch_modulate(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "modulate");
+  for (const TensorSet& t : p->tensors)
+    if ((e = launch_tensor_pre(P, t, s)) != cudaSuccess) return cuda_error(e, "tensor_pre");
   if (fork) {
     OEM_CUDA(cudaEventRecord(p->ev_fork, s));
     OEM_CUDA(cudaStreamWaitEvent(p->side_stream, p->ev_fork, 0));
@@ -355,6 +359,8 @@ static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors) {
   for (const DipoleSet& d : p->dipoles)
     if (!d.magnetic && (e = launch_dipoles(P, d, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "dipoles_e");
+  for (const TensorSet& t : p->tensors)
+    if ((e = launch_tensor_post(P, t, s)) != cudaSuccess) return cuda_error(e, "tensor_post");
   for (const Absorber& a : p->absorbers)
     if ((e = launch_absorb(P, a, 1, s)) != cudaSuccess) return cuda_error(e, "absorb_e");
   for (const TimeMon& m : p->tmons) {
@@ -1266,6 +1272,32 @@ int oem_plan_add_tfsf(oem_plan* p, int n_e, const oem_tfsf_face* e_faces, int n_
   return OEM_OK;
 }
 
+int oem_plan_add_tensor(oem_plan* p, int n_entry, const int* comp, const int64_t* cell,
+                        const float* m1, const float* m2, const float* pec) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (p->is_complex) return set_error(OEM_ERR_UNSUPPORTED, "tensor media on a complex plan");
+  if (n_entry < 1 || !comp || !cell || !m1 || !m2 || !pec)
+    return set_error(OEM_ERR_INVALID, "empty tensor table");
+  const int64_t ncell = (int64_t)p->nx * p->ny * p->nz;
+  std::vector<int64_t> padded(n_entry);
+  for (int e = 0; e < n_entry; ++e) {
+    if (comp[e] < 0 || comp[e] > 2 || cell[e] < 0 || cell[e] >= ncell)
+      return set_error(OEM_ERR_INVALID, "tensor entry outside the grid");
+    padded[e] = cell[e] / p->nz * p->nzp + cell[e] % p->nz;
+  }
+  if ((rc = use_device(p))) return rc;
+  TensorSet t;
+  t.n = n_entry;
+  if ((rc = dupload(p, &t.comp, comp, n_entry)) || (rc = dupload(p, &t.cell, padded.data(), n_entry)) ||
+      (rc = dupload(p, &t.m1, m1, 3 * (size_t)n_entry)) ||
+      (rc = dupload(p, &t.m2, m2, 3 * (size_t)n_entry)) || (rc = dupload(p, &t.pec, pec, n_entry)) ||
+      (rc = dalloc(p, &t.rhs, n_entry)) || (rc = dalloc(p, &t.enew, n_entry)))
+    return rc;
+  p->tensors.push_back(t);
+  return OEM_OK;
+}
+
 int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   int rc = check_plan(p, false);
   if (rc) return rc;
@@ -1517,6 +1549,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
         for (const Modulation& m : p->mods)
           if ((e = launch_modulate(p->yp, m, p->d_step, s)) != cudaSuccess)
             return cuda_error(e, "modulate");
+        for (const TensorSet& t : p->tensors)
+          if ((e = launch_tensor_pre(p->yp, t, s)) != cudaSuccess) return cuda_error(e, "tensor_pre");
         if (p->yp.has_ade &&
             (e = launch_ade_segments(p->yp, p->d_ade_segs, p->n_ade_segs,
                                      (int64_t)p->nx * p->ny * p->nzp / 32, 0, s)) != cudaSuccess)
@@ -1538,6 +1572,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       for (const Modulation& m : p->mods)
         if ((e = launch_modulate(p->yp, m, p->d_step, s)) != cudaSuccess)
           return cuda_error(e, "modulate");
+      for (const TensorSet& t : p->tensors)
+        if ((e = launch_tensor_pre(p->yp, t, s)) != cudaSuccess) return cuda_error(e, "tensor_pre");
       OEM_CUDA(cudaEventRecord(E[0], s));
       e = run_h(p, s);
       if (e != cudaSuccess) return cuda_error(e, "update_h");
@@ -1576,6 +1612,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       for (const DipoleSet& d : p->dipoles)
         if (!d.magnetic && (e = launch_dipoles(p->yp, d, p->d_step, s)) != cudaSuccess)
           return cuda_error(e, "dipoles_e");
+      for (const TensorSet& t : p->tensors)
+        if ((e = launch_tensor_post(p->yp, t, s)) != cudaSuccess) return cuda_error(e, "tensor_post");
       for (const Absorber& a : p->absorbers)
         if ((e = launch_absorb(p->yp, a, 1, s)) != cudaSuccess) return cuda_error(e, "absorb_e");
       for (const TimeMon& m : p->tmons) {
@@ -1679,6 +1717,7 @@ int oem_plan_launches_per_step(oem_plan* p, int* n) {
   c += 3 * (int)p->mons.size();  // snapshot, flush, flush mark
   c += 2 * (int)p->ftmons.size();
   for (const Tfsf& t : p->tfsfs) c += (int)(t.e_groups.size() + t.h_groups.size());
+  c += 3 * (int)p->tensors.size();
   *n = c;
   return OEM_OK;
 }

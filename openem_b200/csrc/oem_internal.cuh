@@ -236,6 +236,19 @@ struct Tfsf {
   int ex_rows = 0, ex_n = 0, hy_rows = 0, hy_n = 0;
 };
 
+// Fully anisotropic cells: per (component, cell) entry the rows of M1, M2 (n x 3) and the
+// PEC-wall factor; rhs / enew hold M1 <E^n> and the new value between the passes.
+struct TensorSet {
+  int n = 0;
+  int* comp = nullptr;
+  int64_t* cell = nullptr;  // padded index
+  float* m1 = nullptr;
+  float* m2 = nullptr;
+  float* pec = nullptr;
+  float* rhs = nullptr;
+  float* enew = nullptr;
+};
+
 struct TimeMon {
   int nc = 0;
   int comps[6] = {0, 0, 0, 0, 0, 0};
@@ -296,6 +309,7 @@ struct oem_plan {
   std::vector<oem::TimeMon> tmons;
   std::vector<oem::FluxTimeMon> ftmons;
   std::vector<oem::Tfsf> tfsfs;
+  std::vector<oem::TensorSet> tensors;
 
   // device state
   std::vector<void*> allocs;
@@ -417,6 +431,8 @@ cudaError_t launch_update_he_fused(const FusedMaps& maps, const YeeParams& P, co
                                    int xch, int n_mats, int* err, cudaStream_t s);
 cudaError_t launch_tfsf(const YeeParams& P, const Tfsf& t, int is_e, const int* step,
                         cudaStream_t s);
+cudaError_t launch_tensor_pre(const YeeParams& P, const TensorSet& t, cudaStream_t s);
+cudaError_t launch_tensor_post(const YeeParams& P, const TensorSet& t, cudaStream_t s);
 
 // Discrete adjoint (oem_adjoint.cu): adjoint fields, their CPML psi, scratch for the transposed
 // differences, and the gradient accumulators of ca and cb per component.

@@ -781,6 +781,63 @@ cudaError_t launch_tfsf(const YeeParams& P, const Tfsf& t, int is_e, const int* 
   return cudaSuccess;
 }
 
+// Fully anisotropic cells (openem/kernels/tensor.cu:49-135): out = wbase base + M_row <F>,
+// the other two components averaged over the 4 neighbours {cell, +1 along a} x {cell, -1 along
+// b} with the boundary masks. First pass: rhs = M1 <E^n> (before the E update); second pass:
+// enew = rhs + M2 <c>, c the curl the passthrough cells hold after the E-side injection.
+__global__ void k_tensor_dot(YeeParams P, TensorSet t, int second) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= t.n) return;
+  const int a = t.comp[e];
+  const int64_t id = t.cell[e];
+  const int64_t sj = P.nzp, si = (int64_t)P.ny * P.nzp;
+  const int c0[3] = {(int)(id / si), (int)((id / sj) % P.ny), (int)(id % sj)};
+  const float* m = (second ? t.m2 : t.m1) + 3 * (int64_t)e;
+  float acc = second ? t.rhs[e] : 0.0f;
+  acc = __fadd_rn(acc, __fmul_rn(m[a], P.f[a][id]));
+  for (int b = 0; b < 3; ++b) {
+    if (b == a) continue;
+    const DevAxis& A = P.ax[a];
+    const DevAxis& B = P.ax[b];
+    int ca[3] = {c0[0], c0[1], c0[2]};
+    ca[a] = A.nxt[c0[a]];
+    int cb[3] = {c0[0], c0[1], c0[2]};
+    cb[b] = B.prv[c0[b]];
+    int cab[3] = {ca[0], ca[1], ca[2]};
+    cab[b] = cb[b];
+    const float wa = A.mnx[c0[a]], wb = B.mpv[c0[b]];
+    const float* F = P.f[b];
+    auto at = [&](const int* c) { return F[c[0] * si + c[1] * sj + c[2]]; };
+    float sum = __fadd_rn(at(c0), __fmul_rn(wa, at(ca)));
+    sum = __fadd_rn(sum, __fmul_rn(wb, at(cb)));
+    sum = __fadd_rn(sum, __fmul_rn(__fmul_rn(wa, wb), at(cab)));
+    acc = __fadd_rn(acc, __fmul_rn(m[b], __fmul_rn(0.25f, sum)));
+  }
+  (second ? t.enew : t.rhs)[e] = acc;
+}
+
+// Write E^{n+1} of the entries (times the PEC-wall factor of the other two axes).
+__global__ void k_tensor_scatter(YeeParams P, TensorSet t) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= t.n) return;
+  P.f[t.comp[e]][t.cell[e]] = __fmul_rn(t.enew[e], t.pec[e]);
+}
+
+cudaError_t launch_tensor_pre(const YeeParams& P, const TensorSet& t, cudaStream_t s) {
+  if (t.n <= 0) return cudaSuccess;
+  k_tensor_dot<<<(t.n + 127) / 128, 128, 0, s>>>(P, t, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tensor_post(const YeeParams& P, const TensorSet& t, cudaStream_t s) {
+  if (t.n <= 0) return cudaSuccess;
+  k_tensor_dot<<<(t.n + 127) / 128, 128, 0, s>>>(P, t, 1);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_tensor_scatter<<<(t.n + 127) / 128, 128, 0, s>>>(P, t);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* step,
                             cudaStream_t s) {
   if (m.kind == 0) {

@@ -588,6 +588,12 @@ class TimeModulation:
 
 @dataclass(frozen=True)
 class TensorEps:
+    """Fully anisotropic cells (openem/model.py:674-786): per (component, cell) entry the 3x3
+    relative permittivity and conductivity at that component's Yee point. Entries with
+    off-diagonal coupling read the other two components as 4-neighbour averages, so the table
+    must be closed: every stencil point of a coupled entry is itself an entry (a ring of diagonal
+    halo entries around the anisotropic region)."""
+
     comp: np.ndarray
     cell: np.ndarray
     eps: np.ndarray
@@ -596,6 +602,64 @@ class TensorEps:
     @property
     def n_entry(self) -> int:
         return int(np.asarray(self.comp).size)
+
+    def rows(self, dt: float):
+        """Row ``comp`` of M1 = A^-1 B and of M2 = (dt/eps0) A^-1, A = eps + s, B = eps - s,
+        s = sigma dt / (2 eps0): the D-form update E^{n+1} = M1 E^n + M2 (curl H - J)."""
+        s = np.asarray(self.sigma, np.float64) * (dt / (2.0 * EPSILON_0))
+        eps = np.asarray(self.eps, np.float64)
+        a_inv = np.linalg.inv(eps + s)
+        m1 = a_inv @ (eps - s)
+        m2 = (dt / EPSILON_0) * a_inv
+        r = np.arange(self.n_entry)
+        comp = np.asarray(self.comp)
+        return m1[r, comp, :], m2[r, comp, :]
+
+    def coupled_mask(self) -> np.ndarray:
+        off = ~np.eye(3, dtype=bool)
+        return ((np.abs(np.asarray(self.eps)[:, off]).max(axis=1) > 0.0)
+                | (np.abs(np.asarray(self.sigma)[:, off]).max(axis=1) > 0.0))
+
+    def validate(self, shape, tables=None) -> None:
+        """Shapes, (comp, cell) uniqueness and, given the axis index tables, closure of the
+        4-neighbour stencils (component b of a coupled entry of component a is read at the cell,
+        one step forward along a and one step back along b)."""
+        n = self.n_entry
+        for name, arr in (("eps", self.eps), ("sigma", self.sigma)):
+            if np.asarray(arr).shape != (n, 3, 3):
+                raise ValueError(f"TensorEps.{name} has shape {np.asarray(arr).shape}, "
+                                 f"expected ({n}, 3, 3)")
+        key = check_csr("TensorEps", shape, self.comp, self.cell, [])
+        if n == 0 or tables is None:
+            return
+        ncell = int(np.prod(shape))
+        have = np.zeros(3 * ncell, dtype=bool)
+        have[key] = True
+        comp = np.asarray(self.comp)
+        c = unravel_cells(np.asarray(self.cell), shape)
+        eps, sig = np.asarray(self.eps), np.asarray(self.sigma)
+        cpl = self.coupled_mask()
+        missing = 0
+        for a in range(3):
+            for b in range(3):
+                if a == b:
+                    continue
+                m = cpl & (comp == a) & ((np.abs(eps[:, a, b]) > 0) | (np.abs(sig[:, a, b]) > 0))
+                if not m.any():
+                    continue
+                base = [np.asarray(c[w])[m] for w in range(3)]
+                for fa in (False, True):
+                    for fb in (False, True):
+                        q = [x.copy() for x in base]
+                        if fa:
+                            q[a] = np.asarray(tables[a]["nxt"])[q[a]]
+                        if fb:
+                            q[b] = np.asarray(tables[b]["prv"])[q[b]]
+                        flat = ravel_cells(q[0].astype(np.int64), q[1], q[2], shape)
+                        missing += int((~have[b * ncell + flat]).sum())
+        if missing:
+            raise ValueError(f"TensorEps closure is broken: {missing} stencil points of coupled "
+                             "entries are not entries themselves")
 
 
 @dataclass(frozen=True)

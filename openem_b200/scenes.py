@@ -21,7 +21,7 @@ import numpy as np
 from openem_b200.model import (
     C_0, EPSILON_0, ETA_0, Axis, Dispersion, FieldMonitor, FieldTimeMonitor, FluxMonitor,
     FluxTimeMonitor, GaussianPulse, Grid, ModeSource, PlaneWaveSource, PMLParams, PointDipole,
-    Scene, TFSFSource, TimeModulation, pml_build, sample_waveform)
+    Scene, TensorEps, TFSFSource, TimeModulation, pml_build, sample_waveform)
 
 UM = 1e-6
 
@@ -421,6 +421,54 @@ def tfsf_box_scene(n: int = 40, n_pml: int = 8, dl: float = 0.02 * UM, axis: int
     return Scene(grid=grid, dt=dt, num_time_steps=num_steps, shutoff=1e-5, eps_ex=eps[0],
                  eps_ey=eps[1], eps_ez=eps[2], pml=pml_dict(grid, dt, n_pml),
                  tfsf_sources=[src])
+
+
+def tensor_region(sc: Scene, lo, hi, eps_tensor, sigma_tensor=None) -> TensorEps:
+    """Entries of a fully anisotropic block over the cells [lo, hi) of every component (the
+    3x3 ``eps_tensor`` / ``sigma_tensor``, or a function of the flat cell index returning them)
+    plus a one-cell ring of diagonal halo entries around it carrying the scene's scalar eps and
+    sigma, which closes the table under the 4-neighbour stencil (the layout of
+    ``openem/scene/media.py``)."""
+    shape = sc.shape
+    ncell = int(np.prod(shape))
+    comps, cells, eps, sig = [], [], [], []
+    scal_e = (sc.eps_ex, sc.eps_ey, sc.eps_ez)
+    scal_s = (sc.sigma_ex, sc.sigma_ey, sc.sigma_ez)
+    glo = [max(lo[a] - 1, 0) for a in range(3)]
+    ghi = [min(hi[a] + 1, shape[a]) for a in range(3)]
+    for c in range(3):
+        I, J, K = np.meshgrid(*[np.arange(glo[a], ghi[a]) for a in range(3)], indexing="ij")
+        inner = ((I >= lo[0]) & (I < hi[0]) & (J >= lo[1]) & (J < hi[1]) & (K >= lo[2])
+                 & (K < hi[2])).ravel()
+        flat = ((I * shape[1] + J) * shape[2] + K).ravel()
+        for f, core in zip(flat, inner):
+            if core:
+                et = eps_tensor(f) if callable(eps_tensor) else eps_tensor
+                st = (sigma_tensor(f) if callable(sigma_tensor) else sigma_tensor)
+                eps.append(np.asarray(et, np.float64))
+                sig.append(np.zeros((3, 3)) if st is None else np.asarray(st, np.float64))
+            else:
+                d = np.eye(3)
+                d[c, c] = float(np.asarray(scal_e[c]).ravel()[f])
+                eps.append(d)
+                sd = np.zeros((3, 3))
+                if scal_s[c] is not None:
+                    sd[c, c] = float(np.asarray(scal_s[c]).ravel()[f])
+                sig.append(sd)
+            comps.append(c)
+            cells.append(f)
+    del ncell
+    return TensorEps(comp=np.asarray(comps, np.int32), cell=np.asarray(cells, np.int64),
+                     eps=np.stack(eps), sigma=np.stack(sig))
+
+
+def rotated_diag(e_diag, theta: float, axis: int = 2) -> np.ndarray:
+    """diag(e_diag) rotated by ``theta`` about coordinate axis ``axis``."""
+    c, s = np.cos(theta), np.sin(theta)
+    u, v = (axis + 1) % 3, (axis + 2) % 3
+    R = np.eye(3)
+    R[u, u], R[u, v], R[v, u], R[v, v] = c, -s, s, c
+    return R @ np.diag(np.asarray(e_diag, np.float64)) @ R.T
 
 
 def slab_transmission(res_slab, res_empty, name: str = "T") -> np.ndarray:

@@ -36,10 +36,13 @@ def refuse_unsupported(sc) -> None:
         (len(getattr(sc, "tfsf_sources", [])) > 1, "several TFSF boxes in one scene"),
         (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry > 0,
          "slanted-interface mixed dispersion"),
-        (sc.tensor is not None and sc.tensor.n_entry > 0, "fully anisotropic media"),
         (sc.modulation is not None and sc.modulation.n_entry > 0
          and (sc.pec_ex is not None or sc.tensor is not None or sc.dispersion_mix is not None),
          "time-modulated media together with PEC, tensor or mixed media"),
+        (sc.tensor is not None and sc.tensor.n_entry > 0
+         and ((sc.dispersion is not None and sc.dispersion.n_entry > 0) or sc.pec_ex is not None
+              or (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry > 0)),
+         "fully anisotropic media together with dispersion, PEC cells or mixed media"),
         (any(k != 0.0 for k in sc.bloch_k), "Bloch boundaries"),
     ]
     for bad, what in checks:
@@ -198,6 +201,13 @@ class Plan:
                 h, ps["pol"], ps["kh"], ps["ks"], ps["coef_h"], ps["coef_e"], int(ps["ex"].size),
                 L.ptr(self._arr(ps["ex"], np.float64)), L.ptr(self._arr(ps["hy"], np.float64))),
                 "add_plane_source")
+        tt = None if self.cplx else T.tensor_tables(sc, self.tabs)
+        if tt is not None:
+            L.check(lib.oem_plan_add_tensor(
+                h, int(tt["comp"].size), L.ptr(self._arr(tt["comp"], np.int32)),
+                L.ptr(self._arr(tt["cell"], np.int64)), L.ptr(self._arr(tt["m1"], np.float32)),
+                L.ptr(self._arr(tt["m2"], np.float32)), L.ptr(self._arr(tt["pec"], np.float32))),
+                "add_tensor")
         if getattr(sc, "tfsf_sources", None) and not self.cplx:
             from openem_b200 import tfsf as TF
             tb = TF.box_tables(sc, self.n_total)

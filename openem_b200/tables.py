@@ -220,7 +220,45 @@ def e_coefficients(sc, tabs):
             sl[a] = zero
             ca[c][tuple(sl)] = 0.0
             cb[c][tuple(sl)] = 0.0
+    # full-tensor entries pass the curl through (ca = 0, cb = 1; zero stays zero on a PEC-backed
+    # wall): the tensor passes turn it into E^{n+1} (openem/kernels/tensor.cu)
+    ten = sc.tensor
+    if ten is not None and ten.n_entry:
+        comp = np.asarray(ten.comp)
+        cell = np.asarray(ten.cell, np.int64)
+        for c in range(3):
+            idx = cell[comp == c]
+            ca[c].ravel()[idx] = 0.0
+            cb[c].ravel()[idx] = np.where(cb[c].ravel()[idx] != 0.0, 1.0, 0.0)
     return ca, cb
+
+
+def tensor_tables(sc, tabs) -> dict | None:
+    """Per entry of a fully anisotropic medium: component, cell, the rows of M1 and M2 in
+    float32 and the PEC-wall factor of the written value (the pec of the other two axes);
+    refused together with dispersion, mixed media, modulation or PEC cells (each rewrites the
+    same coefficients)."""
+    ten = sc.tensor
+    if ten is None or ten.n_entry == 0:
+        return None
+    if (sc.dispersion is not None and sc.dispersion.n_entry) or \
+            (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry) or \
+            (sc.modulation is not None and sc.modulation.n_entry) or sc.pec_ex is not None:
+        raise NotImplementedError("fully anisotropic media together with dispersion, mixed "
+                                  "media, modulation or PEC cells are not supported")
+    ten.validate(sc.shape, [{"nxt": t.nxt, "prv": t.prv} for t in tabs])
+    m1, m2 = ten.rows(sc.dt)
+    comp = np.asarray(ten.comp, np.int32)
+    cell = np.asarray(ten.cell, np.int64)
+    i, j, k = (np.asarray(x) for x in
+               (cell // (sc.shape[1] * sc.shape[2]), (cell // sc.shape[2]) % sc.shape[1],
+                cell % sc.shape[2]))
+    pec = [np.asarray(t.pec, np.float64) for t in tabs]
+    p = np.stack([pec[0][i], pec[1][j], pec[2][k]])
+    pf = p[(comp + 1) % 3, np.arange(comp.size)] * p[(comp + 2) % 3, np.arange(comp.size)]
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    return {"comp": np.ascontiguousarray(comp), "cell": np.ascontiguousarray(cell),
+            "m1": f32(m1), "m2": f32(m2), "pec": f32(pf)}
 
 
 def entry_pole_sets(sc):

@@ -105,6 +105,14 @@ def material_tables_device(sc, tabs, device: int = 0) -> DeviceTables:
             sl[a] = zd
             ca3[tuple(sl)] = 0.0
             cb3[tuple(sl)] = 0.0
+        ten = sc.tensor
+        if ten is not None and ten.n_entry:  # curl passthrough (tables.e_coefficients)
+            sel = np.asarray(ten.cell, np.int64)[np.asarray(ten.comp) == c]
+            if sel.size:
+                td = _to_dev(sel, torch, dev)
+                ca[td] = 0.0
+                cb[td] = torch.where(cb[td] != 0.0, torch.ones_like(cb[td]),
+                                     torch.zeros_like(cb[td]))
         ef = eps.to(torch.float32)
         del eps
         k1 = ((ca.view(torch.int32).to(torch.int64) & mask32) << 32) \

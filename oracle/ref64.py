@@ -125,8 +125,8 @@ class Oracle:
     def __init__(self, sc, n_total: int | None = None):
         if sc.any_bloch:
             raise ValueError("use BlochOracle for a scene with a non-zero Bloch vector")
-        if sc.any_dispersion_mix or sc.any_tensor:
-            raise NotImplementedError("oracle: mix / tensor not transcribed")
+        if sc.any_dispersion_mix:
+            raise NotImplementedError("oracle: mixed dispersion not transcribed")
         self.sc = sc
         self.n_total = int(n_total if n_total is not None else sc.num_time_steps)
         nx, ny, nz = self.shape = sc.shape
@@ -151,6 +151,7 @@ class Oracle:
         self.hist = [np.zeros(self.shape) for _ in range(3)]
         self._setup_dispersion()
         self._setup_modulation()
+        self._setup_tensor()
         self._setup_sources()
         self._setup_tfsf()
         self._setup_monitors()
@@ -180,6 +181,71 @@ class Oracle:
         self.mod = {"comp": comp, "cell": cell, "es": es, "sd": sd, "gg": gg,
                     "amp": np.asarray(mo.amp, np.float64),
                     "phase": np.asarray(mo.phase, np.float64), "om": 2 * np.pi * float(mo.freq)}
+
+    def _setup_tensor(self):
+        """Fully anisotropic cells (openem/kernels/tensor.cu): rows of M1 = A^-1 B and
+        M2 = (dt/eps0) A^-1 per entry; the entries' update coefficients pass the curl through
+        (ca = 0, cb = 1)."""
+        sc = self.sc
+        self.ten = None
+        t = sc.tensor
+        if t is None or t.n_entry == 0:
+            return
+        s = np.asarray(t.sigma, np.float64) * sc.dt / (2 * EPSILON_0)
+        eps = np.asarray(t.eps, np.float64)
+        ainv = np.linalg.inv(eps + s)
+        comp = np.asarray(t.comp, np.int64)
+        r = np.arange(comp.size)
+        m1 = (ainv @ (eps - s))[r, comp, :]
+        m2 = ((sc.dt / EPSILON_0) * ainv)[r, comp, :]
+        cell = np.asarray(t.cell, np.int64)
+        nx, ny, nz = self.shape
+        ijk = np.stack([cell // (ny * nz), (cell // nz) % ny, cell % nz])
+        for c in range(3):
+            m = comp == c
+            self.ca[c].ravel()[cell[m]] = 0.0
+            self.cb[c].ravel()[cell[m]] = 1.0
+        pec = [np.asarray(p, np.float64) for p in self.pec]
+        pf = np.array([pec[(a + 1) % 3][ijk[(a + 1) % 3, e]] * pec[(a + 2) % 3][ijk[(a + 2) % 3, e]]
+                       for e, a in enumerate(comp)])
+        self.ten = {"comp": comp, "ijk": ijk, "m1": m1, "m2": m2, "pec": pf, "rhs": None}
+
+    def _tensor_dot(self, m, F):
+        """m_row . <F> per entry, the off-position components averaged over the 4 neighbours
+        {cell, +1 along comp} x {cell, -1 along b} with the boundary masks."""
+        tn = self.ten
+        comp, ijk = tn["comp"], tn["ijk"]
+        out = np.empty(comp.size)
+        for e, a in enumerate(comp):
+            c0 = ijk[:, e]
+            acc = m[e, a] * F[a][tuple(c0)]
+            for b in range(3):
+                if b == a:
+                    continue
+                ca = c0.copy()
+                ca[a] = self.nxt[a][c0[a]]
+                cb = c0.copy()
+                cb[b] = self.prv[b][c0[b]]
+                cab = ca.copy()
+                cab[b] = cb[b]
+                wa, wb = self.mnx[a][c0[a]], self.mpv[b][c0[b]]
+                avg = 0.25 * (F[b][tuple(c0)] + wa * F[b][tuple(ca)] + wb * F[b][tuple(cb)]
+                              + wa * wb * F[b][tuple(cab)])
+                acc += m[e, b] * avg
+            out[e] = acc
+        return out
+
+    def tensor_pre(self):
+        if getattr(self, "ten", None) is not None:
+            self.ten["rhs"] = self._tensor_dot(self.ten["m1"], self.E)
+
+    def tensor_post(self):
+        tn = getattr(self, "ten", None)
+        if tn is None:
+            return
+        enew = tn["rhs"] + self._tensor_dot(tn["m2"], self.E)
+        for e, a in enumerate(tn["comp"]):
+            self.E[a][tuple(tn["ijk"][:, e])] = enew[e] * tn["pec"][e]
 
     def modulate(self, n):
         """D-form coefficients of step n on the modulated entries
@@ -755,8 +821,10 @@ class Oracle:
         self.absorb("H")
         self.disp_pre()
         self.modulate(n)
+        self.tensor_pre()
         self.update_e()
         self.inject_e(n)
+        self.tensor_post()
         self.disp_post()
         self.absorb("E")
         self._sample_time(n + 1)

@@ -162,3 +162,69 @@ def test_modulation_device_tables_match_host(monkeypatch):
     b = solver.run(sc, use_shutoff=False, return_fields=True, verbose=False)
     for nm in a.fields:
         np.testing.assert_array_equal(a.fields[nm], b.fields[nm])
+
+
+# ---- fully anisotropic media (openem/kernels/tensor.cu) ----------------------------------------
+
+def test_tensor_rotation_superposition_on_gpu():
+    """OpenEM's rotation identity (tests/test_tensor.py:247-288) on the transmitted-plane
+    phasors: the tensor run equals cos^2 / sin^2 / sin cos combinations of two scalar runs within
+    2e-5 of the largest phasor, the reference's own bound."""
+    import test_oracle_golden as tg
+    th = 0.37
+    sc_t, sc_a, sc_b = tg._tensor_slab(th)
+    run = lambda s: solver.run(s, use_shutoff=False, verbose=False)
+    rt, ra, rb = run(sc_t), run(sc_a), run(sc_b)
+    c, s = np.cos(th), np.sin(th)
+    for name in ("T", "R"):
+        pt, pa, pb = (r.phasors[name].data for r in (rt, ra, rb))
+        want_x = c * c * pa[0] + s * s * pb[0]
+        want_y = s * c * (pa[0] - pb[0])
+        scale = np.abs(pa[0]).max()
+        assert np.abs(pt[0] - want_x).max() < 2e-5 * scale, name
+        assert np.abs(pt[1] - want_y).max() < 2e-5 * scale, name
+        assert np.abs(want_y).max() > 1e-2 * scale  # the coupling is exercised
+
+
+def tensor_block_scene(diag=False):
+    sd = scenes.small_dispersive(n=30, n_sph=1, n_pml=6, num_steps=200)
+    sc = replace(sd, dispersion=None, sigma_ex=None, sigma_ey=None, sigma_ez=None)
+    rng = np.random.default_rng(4)
+    A = rng.normal(size=(3, 3))
+    eps = 3.0 * np.eye(3) + 0.4 * (A + A.T)
+    sig = np.zeros((3, 3)) if diag else np.array([[0, 150.0, 0], [-150.0, 0, 0], [0, 0, 20.0]])
+    if diag:
+        eps = np.diag(np.diag(eps))
+    ten = scenes.tensor_region(sc, (11, 9, 12), (19, 20, 17), eps, sig)
+    return sc, ten, eps
+
+
+def test_tensor_block_matches_oracle():
+    """A symmetric eps tensor with a gyrotropic (antisymmetric) sigma on a block beside a dipole:
+    every off-diagonal coupling and the 4-neighbour averages against the FP64 oracle."""
+    sc, ten, _ = tensor_block_scene()
+    sc = replace(sc, tensor=ten)
+    r = ref64.run(sc)
+    g = solver.run(sc, use_shutoff=False, return_fields=True, verbose=False)
+    floor = ref64.fp32_floor(sc, clean=r)
+    for nm in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        assert rel_l2(g.fields[nm], r.fields[nm]) < max(2e-5, 3.0 * floor[nm]), (nm, floor[nm])
+
+
+def test_diagonal_tensor_equals_scalar_path():
+    """OpenEM's degeneracy criterion (tests/test_tensor.py:93-116): a diagonal tensor block
+    equals the scalar update with the same eps to float32 rounding. The two runs round
+    differently where the point dipole sits inside the block (its current enters the pass-through
+    value and is scaled by the M2 row), so each component is held to the float32 floor of the
+    scene rather than to zero."""
+    sc, ten, eps = tensor_block_scene(diag=True)
+    e = [np.array(x) for x in (sc.eps_ex, sc.eps_ey, sc.eps_ez)]
+    for c in range(3):
+        e[c][11:19, 9:20, 12:17] = eps[c, c]
+    scal = replace(sc, eps_ex=e[0], eps_ey=e[1], eps_ez=e[2])
+    tens = replace(scal, tensor=ten)
+    a = solver.run(tens, use_shutoff=False, return_fields=True, verbose=False)
+    b = solver.run(scal, use_shutoff=False, return_fields=True, verbose=False)
+    floor = ref64.fp32_floor(scal)
+    for nm in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        assert rel_l2(a.fields[nm], b.fields[nm]) < max(2e-6, 3.0 * floor[nm]), (nm, floor[nm])

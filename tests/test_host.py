@@ -129,7 +129,7 @@ def test_unsupported_physics_fails_closed(feature):
         "disp_in_absorber": replace(sd, absorbers=scenes.absorber_slabs(sd.grid, 0, 10)),
         "modulation_pec": replace(sc, pec_ex=np.array([5]), modulation=M.TimeModulation(
             1e14, np.array([0]), np.array([0]), np.array([0.1]), np.array([0.0]))),
-        "tensor": replace(sc, tensor=M.TensorEps(np.array([0]), np.array([0]),
+        "tensor": replace(sd, tensor=M.TensorEps(np.array([0]), np.array([0]),
                                                   np.eye(3)[None], np.zeros((1, 3, 3)))),
     }[feature]
     with pytest.raises(NotImplementedError):

@@ -408,3 +408,55 @@ def test_oracle_oblique_tfsf_leakage(th, lo_, hi_):
     land on the same residual."""
     leak = _oblique_leak(th)
     assert lo_ <= leak < hi_, leak
+
+
+def _tensor_slab(th, e=(4.0, 2.25, 3.0), steps=1500):
+    base = scenes.slab_plane_wave(nxy=1, num_steps=steps, eps_slab=1.0)
+    z = np.asarray(base.grid.axes[2].edges[:-1])
+    kk = np.flatnonzero(np.abs(z) < 0.15e-6)
+    lo, hi = (0, 0, int(kk[0])), (1, 1, int(kk[-1]) + 1)
+    ten = scenes.tensor_region(base, lo, hi, scenes.rotated_diag(e, th, 2))
+
+    def scalar(ev):
+        eps = [np.array(x) for x in (base.eps_ex, base.eps_ey, base.eps_ez)]
+        for c in range(2):
+            eps[c][:, :, lo[2]:hi[2]] = ev
+        return replace(base, eps_ex=eps[0], eps_ey=eps[1], eps_ez=eps[2])
+    return replace(base, tensor=ten), scalar(e[0]), scalar(e[1])
+
+
+def test_oracle_tensor_rotation_superposition():
+    """OpenEM's rotation identity (tests/test_tensor.py test_rotation_superposition_identity): a
+    diagonal medium rotated about the propagation axis in a transversely uniform cell decouples
+    exactly, so the tensor run equals cos^2 / sin^2 / sin cos combinations of two scalar runs."""
+    th = 0.37
+    sc_t, sc_a, sc_b = _tensor_slab(th)
+    rt, ra, rb = ref64.run(sc_t), ref64.run(sc_a), ref64.run(sc_b)
+    c, s = np.cos(th), np.sin(th)
+    scale = np.abs(rt.fields["Ex"]).max()
+    assert np.abs(rt.fields["Ex"] - (c * c * ra.fields["Ex"] + s * s * rb.fields["Ex"])).max() \
+        < 1e-7 * scale
+    assert np.abs(rt.fields["Ey"] - s * c * (ra.fields["Ex"] - rb.fields["Ex"])).max() \
+        < 1e-7 * scale
+    assert np.abs(rt.fields["Ey"]).max() > 1e-2 * scale
+
+
+def test_tensor_closure_and_refusals():
+    """OpenEM's closure check (tests/test_tensor.py test_tensor_closure_validation): without its
+    halo ring a coupled block reads ordinary cells' E^{n+1} as curl, so the table is refused;
+    tensor media together with PEC cells fail closed."""
+    sd = scenes.small_dispersive(n=20, n_sph=1, n_pml=4, num_steps=10)
+    sc = replace(sd, dispersion=None, sigma_ex=None, sigma_ey=None, sigma_ez=None)
+    ten = scenes.tensor_region(sc, (8, 8, 8), (12, 12, 12),
+                               scenes.rotated_diag((4.0, 2.0, 3.0), 0.5, 1))
+    sc_t = replace(sc, tensor=ten)
+    tabs = [T.axis_tables(sc_t, a) for a in range(3)]
+    T.tensor_tables(sc_t, tabs)
+    t = sc_t.tensor
+    keep = t.coupled_mask()  # drop the halo ring
+    broken = M.TensorEps(comp=t.comp[keep], cell=t.cell[keep], eps=t.eps[keep],
+                         sigma=t.sigma[keep])
+    with pytest.raises(ValueError):
+        T.tensor_tables(replace(sc_t, tensor=broken), tabs)
+    with pytest.raises(NotImplementedError):
+        T.tensor_tables(replace(sc_t, pec_ex=np.array([0])), tabs)
