@@ -207,6 +207,20 @@ int oem_plan_add_tfsf(oem_plan* p, int n_e, const oem_tfsf_face* e_faces, int n_
 int oem_plan_add_tensor(oem_plan* p, int n_entry, const int* comp, const int64_t* cell,
                         const float* m1, const float* m2, const float* pec);
 
+/* Slanted-interface cells (openem/kernels/dispersion_mix.cu:41-135, openem/model.py:529-612,
+ * tables of openem/device_tables.py:291-321): n_entry (comp, cell) entries, cell =
+ * (i ny + j) nz + k, whose material records pass the curl through (ca = 0, cb = 1). Entry e owns
+ * arithmetic-branch poles p_ofs[e]..p_ofs[e+1] (poles of eps, conjugate pairs counted by
+ * 2 Re) and harmonic-branch poles q_ofs[e]..q_ofs[e+1] (poles of 1/eps, every root listed),
+ * each pole a row (Re(A-1), Im(A-1), Re(B), Im(B)) of p_coef / q_coef; k holds per entry
+ * (k1, k2, 1 - beta, 1 / (k1 k2 + beta)) with k1 = (1 - beta)(eps_inf + sum 2 Re(B_P)) and
+ * k2 = zeta_inf + sum Re(B_Q); dte = dt / eps0. Each step SP / SQ come from E^n and d_h^n
+ * before the E update; after the E-side injection d_tot += dte * E, d_h^{n+1} =
+ * (d_tot - k1 SQ - (1 - beta) SP) / (k1 k2 + beta) and E^{n+1} = k2 d_h + SQ. */
+int oem_plan_add_dispersion_mix(oem_plan* p, int n_entry, const int* comp, const int64_t* cell,
+                                const int* p_ofs, const float* p_coef, int n_p, const int* q_ofs,
+                                const float* q_coef, int n_q, const float* k, double dte);
+
 /* Absorber boundary slab (Tidy3D's Absorber; replaces absorb_slab / absorb_batch,
  * openem/kernels/absorber.cu:20-70, absorb_batch.cu:15-110, and the host tables of
  * openem/dispersion_setup.py:89-120): layers [g0, g0 + nlay) along `axis`. After the H-side

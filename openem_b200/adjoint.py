@@ -55,6 +55,9 @@ def _refuse(sc) -> None:
         raise NotImplementedError("the adjoint covers non-dispersive scenes")
     if sc.absorbers:
         raise NotImplementedError("the adjoint does not cover absorber slabs")
+    if (sc.tensor is not None and sc.tensor.n_entry) or \
+            (sc.modulation is not None and sc.modulation.n_entry):
+        raise NotImplementedError("the adjoint does not cover tensor media or time modulation")
     if sc.any_bloch:
         raise NotImplementedError("the adjoint covers real fields (no Bloch phase)")
 

@@ -287,6 +287,8 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
   const YeeParams& P = p->yp;
   cudaError_t e;
   if (p->fused) {
+    for (const MixSet& x : p->mixes)
+      if ((e = launch_mix_pre(P, x, s)) != cudaSuccess) return cuda_error(e, "mix_pre");
     for (const Modulation& m : p->mods)
       if ((e = launch_modulate(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "modulate");
     for (const TensorSet& t : p->tensors)
@@ -308,6 +310,8 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
   // the pole pass depends on E^n only: it runs on a branch beside the H update and joins
   // before the E update
   const bool fork = p->side_stream != nullptr;
+  for (const MixSet& x : p->mixes)
+    if ((e = launch_mix_pre(P, x, s)) != cudaSuccess) return cuda_error(e, "mix_pre");
   for (const Modulation& m : p->mods)
     if ((e = launch_modulate(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "modulate");
   for (const TensorSet& t : p->tensors)
@@ -359,6 +363,8 @@ static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors) {
   for (const DipoleSet& d : p->dipoles)
     if (!d.magnetic && (e = launch_dipoles(P, d, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "dipoles_e");
+  for (const MixSet& x : p->mixes)
+    if ((e = launch_mix_post(P, x, s)) != cudaSuccess) return cuda_error(e, "mix_post");
   for (const TensorSet& t : p->tensors)
     if ((e = launch_tensor_post(P, t, s)) != cudaSuccess) return cuda_error(e, "tensor_post");
   for (const Absorber& a : p->absorbers)
@@ -834,9 +840,11 @@ int oem_plan_adjoint_flux_box(oem_plan* p, int mon_id, const double* weights, co
   if (p->mons[mon_id].n_total < p->n_total)
     return set_error(OEM_ERR_INVALID, "the monitor's phase table is shorter than the run");
   if (!weights || !dA1 || !dA2 || !g_ca || !g_cb) return set_error(OEM_ERR_INVALID, "null argument");
-  if (p->is_complex || p->yp.has_ade || !p->absorbers.empty())
+  if (p->is_complex || p->yp.has_ade || !p->absorbers.empty() || !p->mixes.empty() ||
+      !p->tensors.empty() || !p->mods.empty())
     return set_error(OEM_ERR_UNSUPPORTED,
-                     "the adjoint covers real, non-dispersive plans without absorbers");
+                     "the adjoint covers real, non-dispersive plans without absorbers, tensor "
+                     "media or time modulation");
   for (int64_t q = 0; q < (int64_t)p->ckpt.size(); ++q)
     if (p->ckpt_step[q] != q * p->ckpt_k) return set_error(OEM_ERR_STATE, "missing checkpoint");
   if ((rc = use_device(p))) return rc;
@@ -1298,6 +1306,52 @@ int oem_plan_add_tensor(oem_plan* p, int n_entry, const int* comp, const int64_t
   return OEM_OK;
 }
 
+int oem_plan_add_dispersion_mix(oem_plan* p, int n_entry, const int* comp, const int64_t* cell,
+                                const int* p_ofs, const float* p_coef, int n_p, const int* q_ofs,
+                                const float* q_coef, int n_q, const float* k, double dte) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (p->is_complex) return set_error(OEM_ERR_UNSUPPORTED, "mixed dispersion on a complex plan");
+  if (n_entry < 1 || !comp || !cell || !p_ofs || !q_ofs || !k || n_p < 0 || n_q < 0 ||
+      (n_p > 0 && !p_coef) || (n_q > 0 && !q_coef))
+    return set_error(OEM_ERR_INVALID, "empty mixed-dispersion table");
+  if (!(dte > 0.0)) return set_error(OEM_ERR_INVALID, "dt / eps0 must be positive");
+  const int64_t ncell = (int64_t)p->nx * p->ny * p->nz;
+  std::vector<int64_t> padded(n_entry);
+  for (int e = 0; e < n_entry; ++e) {
+    if (comp[e] < 0 || comp[e] > 2 || cell[e] < 0 || cell[e] >= ncell)
+      return set_error(OEM_ERR_INVALID, "mixed-dispersion entry outside the grid");
+    padded[e] = cell[e] / p->nz * p->nzp + cell[e] % p->nz;
+  }
+  for (const int* ofs : {p_ofs, q_ofs}) {
+    const int last = ofs == p_ofs ? n_p : n_q;
+    if (ofs[0] != 0 || ofs[n_entry] != last)
+      return set_error(OEM_ERR_INVALID, "pole offsets do not span the pole table");
+    for (int e = 0; e < n_entry; ++e)
+      if (ofs[e + 1] < ofs[e]) return set_error(OEM_ERR_INVALID, "pole offsets not monotonic");
+  }
+  if ((rc = use_device(p))) return rc;
+  MixSet m;
+  m.n = n_entry;
+  m.dte = (float)dte;
+  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4* pc = n_p ? reinterpret_cast<const float4*>(p_coef) : &zero4;
+  const float4* qc = n_q ? reinterpret_cast<const float4*>(q_coef) : &zero4;
+  if ((rc = dupload(p, &m.comp, comp, n_entry)) ||
+      (rc = dupload(p, &m.cell, padded.data(), n_entry)) ||
+      (rc = dupload(p, &m.p_ofs, p_ofs, (size_t)n_entry + 1)) ||
+      (rc = dupload(p, &m.q_ofs, q_ofs, (size_t)n_entry + 1)) ||
+      (rc = dupload(p, &m.pc, pc, std::max(n_p, 1))) ||
+      (rc = dupload(p, &m.qc, qc, std::max(n_q, 1))) ||
+      (rc = dupload(p, &m.k, reinterpret_cast<const float4*>(k), n_entry)) ||
+      (rc = dalloc(p, &m.P, std::max(n_p, 1))) || (rc = dalloc(p, &m.Q, std::max(n_q, 1))) ||
+      (rc = dalloc(p, &m.sp, n_entry)) || (rc = dalloc(p, &m.sq, n_entry)) ||
+      (rc = dalloc(p, &m.dtot, n_entry)) || (rc = dalloc(p, &m.dh, n_entry)))
+    return rc;
+  p->mixes.push_back(m);
+  return OEM_OK;
+}
+
 int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   int rc = check_plan(p, false);
   if (rc) return rc;
@@ -1546,6 +1600,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       if (p->fused) {
         // E[0] ade E[5] fused E[1] ... E[4]: the pole pass and the fused kernel timed apart
         OEM_CUDA(cudaEventRecord(E[0], s));
+        for (const MixSet& x : p->mixes)
+          if ((e = launch_mix_pre(p->yp, x, s)) != cudaSuccess) return cuda_error(e, "mix_pre");
         for (const Modulation& m : p->mods)
           if ((e = launch_modulate(p->yp, m, p->d_step, s)) != cudaSuccess)
             return cuda_error(e, "modulate");
@@ -1569,6 +1625,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
         OEM_CUDA(cudaEventRecord(E[4], s));
         continue;
       }
+      for (const MixSet& x : p->mixes)
+        if ((e = launch_mix_pre(p->yp, x, s)) != cudaSuccess) return cuda_error(e, "mix_pre");
       for (const Modulation& m : p->mods)
         if ((e = launch_modulate(p->yp, m, p->d_step, s)) != cudaSuccess)
           return cuda_error(e, "modulate");
@@ -1612,6 +1670,8 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       for (const DipoleSet& d : p->dipoles)
         if (!d.magnetic && (e = launch_dipoles(p->yp, d, p->d_step, s)) != cudaSuccess)
           return cuda_error(e, "dipoles_e");
+      for (const MixSet& x : p->mixes)
+        if ((e = launch_mix_post(p->yp, x, s)) != cudaSuccess) return cuda_error(e, "mix_post");
       for (const TensorSet& t : p->tensors)
         if ((e = launch_tensor_post(p->yp, t, s)) != cudaSuccess) return cuda_error(e, "tensor_post");
       for (const Absorber& a : p->absorbers)
@@ -1718,6 +1778,7 @@ int oem_plan_launches_per_step(oem_plan* p, int* n) {
   c += 2 * (int)p->ftmons.size();
   for (const Tfsf& t : p->tfsfs) c += (int)(t.e_groups.size() + t.h_groups.size());
   c += 3 * (int)p->tensors.size();
+  c += 2 * (int)p->mixes.size();
   *n = c;
   return OEM_OK;
 }

@@ -249,6 +249,28 @@ struct TensorSet {
   float* enew = nullptr;
 };
 
+// Slanted-interface entries (openem/kernels/dispersion_mix.cu): per entry the component, the
+// padded cell, the pole ranges of the arithmetic (eps poles, P) and harmonic (1/eps poles, Q)
+// branches, (k1, k2, 1 - beta, 1 / (k1 k2 + beta)), and the per-step state: SP / SQ of the first
+// pass, the accumulated d_tot and the harmonic unknown d_h.
+struct MixSet {
+  int n = 0;
+  float dte = 0.0f;  // dt / eps0
+  int* comp = nullptr;
+  int64_t* cell = nullptr;  // padded index
+  int* p_ofs = nullptr;     // n + 1
+  int* q_ofs = nullptr;
+  float4* pc = nullptr;     // per pole (Re(A-1), Im(A-1), Re(B), Im(B))
+  float4* qc = nullptr;
+  float2* P = nullptr;      // pole states
+  float2* Q = nullptr;
+  float4* k = nullptr;
+  float* sp = nullptr;
+  float* sq = nullptr;
+  float* dtot = nullptr;
+  float* dh = nullptr;
+};
+
 struct TimeMon {
   int nc = 0;
   int comps[6] = {0, 0, 0, 0, 0, 0};
@@ -310,6 +332,7 @@ struct oem_plan {
   std::vector<oem::FluxTimeMon> ftmons;
   std::vector<oem::Tfsf> tfsfs;
   std::vector<oem::TensorSet> tensors;
+  std::vector<oem::MixSet> mixes;
 
   // device state
   std::vector<void*> allocs;
@@ -433,6 +456,8 @@ cudaError_t launch_tfsf(const YeeParams& P, const Tfsf& t, int is_e, const int* 
                         cudaStream_t s);
 cudaError_t launch_tensor_pre(const YeeParams& P, const TensorSet& t, cudaStream_t s);
 cudaError_t launch_tensor_post(const YeeParams& P, const TensorSet& t, cudaStream_t s);
+cudaError_t launch_mix_pre(const YeeParams& P, const MixSet& m, cudaStream_t s);
+cudaError_t launch_mix_post(const YeeParams& P, const MixSet& m, cudaStream_t s);
 
 // Discrete adjoint (oem_adjoint.cu): adjoint fields, their CPML psi, scratch for the transposed
 // differences, and the gradient accumulators of ca and cb per component.

@@ -838,6 +838,89 @@ cudaError_t launch_tensor_post(const YeeParams& P, const TensorSet& t, cudaStrea
   return cudaGetLastError();
 }
 
+// Slanted-interface cells, first pass (openem/kernels/dispersion_mix.cu:41-85): both pole
+// branches advance to the half step, the arithmetic one driven by E^n, the harmonic one by
+// d_h^n; SP = sum 2 Re(P_half), SQ = sum Re(Q_half).
+__global__ void k_mix_pre(YeeParams P, MixSet m) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.n) return;
+  const float en = P.f[m.comp[e]][m.cell[e]];
+  const float dh = m.dh[e];
+  float s = 0.0f;
+  for (int t = m.p_ofs[e]; t < m.p_ofs[e + 1]; ++t) {
+    const float4 c = m.pc[t];
+    float2 p = m.P[t];
+    const float dr = __fadd_rn(__fsub_rn(__fmul_rn(c.x, p.x), __fmul_rn(c.y, p.y)),
+                               __fmul_rn(c.z, en));
+    const float di = __fadd_rn(__fadd_rn(__fmul_rn(c.x, p.y), __fmul_rn(c.y, p.x)),
+                               __fmul_rn(c.w, en));
+    p.x = __fadd_rn(p.x, dr);
+    p.y = __fadd_rn(p.y, di);
+    m.P[t] = p;
+    s = __fadd_rn(s, __fmul_rn(2.0f, p.x));
+  }
+  m.sp[e] = s;
+  s = 0.0f;
+  for (int t = m.q_ofs[e]; t < m.q_ofs[e + 1]; ++t) {
+    const float4 c = m.qc[t];
+    float2 q = m.Q[t];
+    const float dr = __fadd_rn(__fsub_rn(__fmul_rn(c.x, q.x), __fmul_rn(c.y, q.y)),
+                               __fmul_rn(c.z, dh));
+    const float di = __fadd_rn(__fadd_rn(__fmul_rn(c.x, q.y), __fmul_rn(c.y, q.x)),
+                               __fmul_rn(c.w, dh));
+    q.x = __fadd_rn(q.x, dr);
+    q.y = __fadd_rn(q.y, di);
+    m.Q[t] = q;
+    s = __fadd_rn(s, q.x);
+  }
+  m.sq[e] = s;
+}
+
+// Second pass (openem/kernels/dispersion_mix.cu:87-135): the E array holds the pass-through
+// value (stretched curl, minus J, plus the E-side sources); d_tot advances by dt/eps0 times it,
+// the scalar equation gives d_h^{n+1} = (d_tot - k1 SQ - (1 - beta) SP) / (k1 k2 + beta),
+// E^{n+1} = k2 d_h + SQ, and both branches take their step-(n+1) terms.
+__global__ void k_mix_post(YeeParams P, MixSet m) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.n) return;
+  float* F = P.f[m.comp[e]];
+  const int64_t id = m.cell[e];
+  const float dt_new = __fadd_rn(m.dtot[e], __fmul_rn(m.dte, F[id]));
+  m.dtot[e] = dt_new;
+  const float4 k = m.k[e];
+  const float dh = __fmul_rn(
+      __fsub_rn(__fsub_rn(dt_new, __fmul_rn(k.x, m.sq[e])), __fmul_rn(k.z, m.sp[e])), k.w);
+  m.dh[e] = dh;
+  const float en = __fadd_rn(__fmul_rn(k.y, dh), m.sq[e]);
+  for (int t = m.p_ofs[e]; t < m.p_ofs[e + 1]; ++t) {
+    const float4 c = m.pc[t];
+    float2 p = m.P[t];
+    p.x = __fadd_rn(p.x, __fmul_rn(c.z, en));
+    p.y = __fadd_rn(p.y, __fmul_rn(c.w, en));
+    m.P[t] = p;
+  }
+  for (int t = m.q_ofs[e]; t < m.q_ofs[e + 1]; ++t) {
+    const float4 c = m.qc[t];
+    float2 q = m.Q[t];
+    q.x = __fadd_rn(q.x, __fmul_rn(c.z, dh));
+    q.y = __fadd_rn(q.y, __fmul_rn(c.w, dh));
+    m.Q[t] = q;
+  }
+  F[id] = en;
+}
+
+cudaError_t launch_mix_pre(const YeeParams& P, const MixSet& m, cudaStream_t s) {
+  if (m.n <= 0) return cudaSuccess;
+  k_mix_pre<<<(m.n + 127) / 128, 128, 0, s>>>(P, m);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mix_post(const YeeParams& P, const MixSet& m, cudaStream_t s) {
+  if (m.n <= 0) return cudaSuccess;
+  k_mix_post<<<(m.n + 127) / 128, 128, 0, s>>>(P, m);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* step,
                             cudaStream_t s) {
   if (m.kind == 0) {

@@ -542,6 +542,14 @@ class Dispersion:
 
 @dataclass(frozen=True)
 class DispersionMix:
+    """Slanted-interface cells (openem/model.py:529-612, openem/kernels/dispersion_mix.cu):
+    eps_eff = (1 - beta) sum f_i eps_i + beta / sum (f_i / eps_i), beta the squared normal
+    projection on the entry's component. The arithmetic branch carries poles of eps (``p_ofs``,
+    ``pa = A - 1``, ``pb = B``, conjugate pairs counted by 2 Re), the harmonic branch poles of
+    1/eps (``q_ofs``, ``qa``, ``qb``, every root listed, counted by Re) driven by its own
+    unknown d_h = D_h / eps0; per step one scalar linear equation gives d_h^{n+1} and E^{n+1}.
+    beta = 0 is the E form of :class:`Dispersion`, beta = 1 the pure harmonic (D) form."""
+
     comp: np.ndarray
     cell: np.ndarray
     p_ofs: np.ndarray
@@ -557,6 +565,63 @@ class DispersionMix:
     @property
     def n_entry(self) -> int:
         return int(np.asarray(self.comp).size)
+
+    def coefficients(self):
+        """Per entry ``(k1, k2, 1 - beta, 1 / (k1 k2 + beta))`` in float64 with
+        k1 = (1 - beta)(eps_inf + sum 2 Re(pb)) and k2 = zeta_inf + sum Re(qb): the implicit
+        couplings of the two branches to step n+1."""
+        n = self.n_entry
+        beta = np.asarray(self.beta, np.float64)
+
+        def seg_sum(ofs, vals):
+            ofs = np.asarray(ofs, np.int64)
+            out = np.zeros(n)
+            cnt = np.diff(ofs)
+            if vals.size:
+                np.add.at(out, np.repeat(np.arange(n), cnt), vals)
+            return out
+        gp = seg_sum(self.p_ofs, 2.0 * np.asarray(self.pb, np.complex128).real)
+        gq = seg_sum(self.q_ofs, np.asarray(self.qb, np.complex128).real)
+        one_mb = 1.0 - beta
+        k1 = one_mb * (np.asarray(self.eps_inf, np.float64) + gp)
+        k2 = np.asarray(self.zeta_inf, np.float64) + gq
+        den = k1 * k2 + beta
+        if np.any(np.abs(den) < 1e-30):
+            raise ValueError("mixed-cell denominator k1*k2 + beta is zero")
+        return k1, k2, one_mb, 1.0 / den
+
+    def validate(self, shape, *others) -> None:
+        """Shapes, CSR offsets, (comp, cell) uniqueness, beta in [0, 1] (1e-6 slack), no entry
+        shared with another dispersion table, a usable denominator."""
+        n = self.n_entry
+        for nm in ("beta", "eps_inf", "zeta_inf"):
+            a = np.asarray(getattr(self, nm))
+            if a.shape != (n,):
+                raise ValueError(f"DispersionMix.{nm} has shape {a.shape}, expected ({n},)")
+        for nm, ofs in (("pa", "p_ofs"), ("pb", "p_ofs"), ("qa", "q_ofs"), ("qb", "q_ofs")):
+            a = np.asarray(getattr(self, nm))
+            if a.ndim != 1:
+                raise ValueError(f"DispersionMix.{nm} must be one-dimensional")
+        if np.asarray(self.pa).size != np.asarray(self.pb).size or \
+                np.asarray(self.qa).size != np.asarray(self.qb).size:
+            raise ValueError("DispersionMix: pole coefficient lengths differ")
+        key = check_csr("DispersionMix", shape, self.comp, self.cell,
+                        [("p_ofs", self.p_ofs, int(np.asarray(self.pa).size)),
+                         ("q_ofs", self.q_ofs, int(np.asarray(self.qa).size))])
+        if n == 0:
+            return
+        beta = np.asarray(self.beta, np.float64)
+        if np.any((beta < -1e-6) | (beta > 1.0 + 1e-6)):
+            raise ValueError(f"beta outside [0,1]: {beta.min():.4f}..{beta.max():.4f} (the "
+                             "squared normal projection; out of range means an unreliable fit)")
+        ncell = int(np.prod(shape))
+        for o in others:
+            if o is None or o.n_entry == 0:
+                continue
+            ok = np.asarray(o.comp, np.int64) * ncell + np.asarray(o.cell, np.int64)
+            if np.intersect1d(key, ok).size:
+                raise ValueError("the same (comp, cell) appears in more than one dispersion table")
+        self.coefficients()
 
 
 @dataclass(frozen=True)

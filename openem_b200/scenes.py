@@ -19,7 +19,7 @@ from __future__ import annotations
 import numpy as np
 
 from openem_b200.model import (
-    C_0, EPSILON_0, ETA_0, Axis, Dispersion, FieldMonitor, FieldTimeMonitor, FluxMonitor,
+    C_0, EPSILON_0, ETA_0, Axis, Dispersion, DispersionMix, FieldMonitor, FieldTimeMonitor, FluxMonitor,
     FluxTimeMonitor, GaussianPulse, Grid, ModeSource, PlaneWaveSource, PMLParams, PointDipole,
     Scene, TensorEps, TFSFSource, TimeModulation, pml_build, sample_waveform)
 
@@ -149,6 +149,141 @@ def build_dispersion(masks, am1, b, shape) -> Dispersion | None:
     return Dispersion(comp=comp, cell=cell,
                       pole_ofs=(np.arange(n + 1, dtype=np.int64) * p).astype(np.int32),
                       am1=np.tile(am1, n), b=np.tile(b, n), g=np.full(n, g1))
+
+
+def zeta_poles(eps_inf: float, poles):
+    """Pole expansion of 1/eps: ``(zeta_inf, p, r)`` with
+    ``1/eps(s) = zeta_inf + sum_m r_m / (s - p_m)`` over every root (conjugates listed apart),
+    for ``eps(s) = eps_inf + sum c/(s-a) + c*/(s-a*)`` (the restatement of
+    ``openem/scene/poles.py:297-375``). With eps = N/D, the p_m are the zeros of N and
+    ``r_m = D(p_m) / N'(p_m)``; the polynomials are built in ``u = s / scale`` (scale the largest
+    |a|) so that their coefficients stay O(1). Roots within 1e-9 |u| of the imaginary axis are
+    put on it; a root strictly in the right half plane is refused."""
+    qs = []
+    for a, c in poles:
+        qs += [(complex(a), complex(c)), (np.conj(complex(a)), np.conj(complex(c)))]
+    scale = max((abs(a) for a, _ in qs if abs(a) > 0), default=1.0)
+    qu = [(a / scale, c / scale) for a, c in qs]
+    den = np.poly([a for a, _ in qu]) if qu else np.array([1.0 + 0j])
+    num = float(eps_inf) * den
+    for k, (_, c) in enumerate(qu):
+        rest = np.poly([a for j, (a, _) in enumerate(qu) if j != k])
+        num = num + np.concatenate([np.zeros(num.size - rest.size), c * rest])
+    pu = np.roots(num)
+    pu = np.where(np.abs(pu.real) <= 1e-9 * np.abs(pu), 1j * pu.imag, pu)
+    dnum = np.polyder(num)
+    ru = np.polyval(den, pu) / np.polyval(dnum, pu)
+    p, r = pu * scale, ru * scale
+    if p.size and float(np.max(p.real)) > 0.0:
+        raise ValueError(f"1/eps has a pole in the right half plane (max Re {np.max(p.real):.3e})")
+    return 1.0 / float(eps_inf), p, r
+
+
+def bulk_mix(shape, beta, pa, pb, qa, qb, eps_inf, zeta_inf, masks=None) -> DispersionMix:
+    """The same two branches on every (component, cell) inside ``masks`` (all cells when None)
+    with mixing weight ``beta`` (scalar or one value per entry)."""
+    comp, cell = [], []
+    for c in range(3):
+        m = np.ones(shape, bool) if masks is None else masks[c]
+        idx = np.flatnonzero(np.asarray(m).ravel())
+        comp.append(np.full(idx.size, c, np.int32))
+        cell.append(idx.astype(np.int64))
+    comp, cell = np.concatenate(comp), np.concatenate(cell)
+    n = comp.size
+    pa, pb, qa, qb = (np.asarray(x, np.complex128) for x in (pa, pb, qa, qb))
+    full = lambda v: np.broadcast_to(np.asarray(v, np.float64), (n,)).copy()
+    return DispersionMix(comp=comp, cell=cell,
+                         p_ofs=(np.arange(n + 1) * pa.size).astype(np.int64),
+                         pa=np.tile(pa, n), pb=np.tile(pb, n),
+                         q_ofs=(np.arange(n + 1) * qa.size).astype(np.int64),
+                         qa=np.tile(qa, n), qb=np.tile(qb, n),
+                         beta=full(beta), eps_inf=full(eps_inf), zeta_inf=full(zeta_inf))
+
+
+def mix_pieces(eps_inf1: float, poles, eps2: float, fill: float, dt: float):
+    """The two branches of a cell that holds the fraction ``fill`` of a pole-residue medium
+    (eps_inf1, poles) and the rest of a constant eps2 (the layout of OpenEM's mixed-form tests):
+    arithmetic eps_inf = f eps_inf1 + (1-f) eps2 with the residues times f; harmonic
+    zeta_inf = f / eps_inf1 + (1-f) / eps2 with the 1/eps residues times f. Returns
+    ``(eps_inf, zeta_inf, pa, pb, qa, qb)``."""
+    pa, pb = trap_coeffs(poles, dt)
+    z1, p1, r1 = zeta_poles(eps_inf1, poles)
+    qa, qb = trap_coeffs(list(zip(p1, r1)), dt)
+    return (fill * eps_inf1 + (1.0 - fill) * eps2, fill * z1 + (1.0 - fill) / eps2,
+            pa, pb * fill, qa, qb * fill)
+
+
+def mixed_sphere(n: int = 28, n_pml: int = 6, radius_cells: float = 5.3, num_steps: int = 300,
+                 eps2: float = 2.25, eps_inf1: float = 2.0, lorentz=(1.5, 3e14, 3e13),
+                 dip_freq0: float = 2.5e14, dip_fwidth: float = 1.5e14, seed: int = 5,
+                 probe: bool = True) -> Scene:
+    """A Lorentz sphere (eps_inf1 plus one Lorentz pair) in a constant eps2 background, with a
+    point dipole beside it. Component points well inside take the E form (:class:`Dispersion`);
+    points within half a cell of the surface take the mixed form with fill
+    f = clip(0.5 - d / dl, 0, 1) (d the signed distance to the surface) and beta the squared
+    normal projection on the component's axis, jittered by rng(seed) within [0, 1]."""
+    dl = 0.02 * UM
+    n_in = n - 2 * n_pml
+    lo = -0.5 * n_in * dl
+    axes = [uniform_axis(n_in, dl, lo, "PML", n_pml) for _ in range(3)]
+    grid = Grid(*axes)
+    dt = courant_dt([a.dl for a in axes])
+    shape = grid.shape
+    coords = yee_coords(grid)
+    poles = lorentz_poles(*lorentz)
+    R = radius_cells * dl
+    cen = np.array([0.1, -0.05, 0.0]) * dl
+    rng = np.random.default_rng(seed)
+    inner, eps = [], []
+    comp, cell, beta, fill = [], [], [], []
+    for c in range(3):
+        x, y, z = np.meshgrid(*coords[c], indexing="ij")
+        rel = np.stack([x - cen[0], y - cen[1], z - cen[2]])
+        r = np.sqrt((rel ** 2).sum(0))
+        d = r - R
+        ins = d < -0.5 * dl
+        shell = np.abs(d) <= 0.5 * dl
+        inner.append(ins)
+        idx = np.flatnonzero(shell.ravel())
+        nrm = rel[c].ravel()[idx] / np.maximum(r.ravel()[idx], 1e-30)
+        b = np.clip(nrm * nrm + rng.uniform(-0.05, 0.05, idx.size), 0.0, 1.0)
+        comp.append(np.full(idx.size, c, np.int32))
+        cell.append(idx.astype(np.int64))
+        beta.append(b)
+        fill.append(np.clip(0.5 - d.ravel()[idx] / dl, 0.0, 1.0))
+        e = np.full(shape, eps2)
+        e[ins] = eps_inf1
+        eps.append(e)
+    comp, cell = np.concatenate(comp), np.concatenate(cell)
+    beta, fill = np.concatenate(beta), np.concatenate(fill)
+    pa, pb = trap_coeffs(poles, dt)
+    z1, p1, r1 = zeta_poles(eps_inf1, poles)
+    qa, qb = trap_coeffs(list(zip(p1, r1)), dt)
+    ne, npp, nq = comp.size, pa.size, qa.size
+    mix = DispersionMix(
+        comp=comp, cell=cell,
+        p_ofs=(np.arange(ne + 1) * npp).astype(np.int64),
+        pa=np.tile(pa, ne), pb=(pb[None, :] * fill[:, None]).ravel(),
+        q_ofs=(np.arange(ne + 1) * nq).astype(np.int64),
+        qa=np.tile(qa, ne), qb=(qb[None, :] * fill[:, None]).ravel(),
+        beta=beta, eps_inf=fill * eps_inf1 + (1.0 - fill) * eps2,
+        zeta_inf=fill / eps_inf1 + (1.0 - fill) / eps2)
+    for c in range(3):
+        sel = comp == c
+        eps[c].ravel()[cell[sel]] = mix.eps_inf[sel]
+    disp = build_dispersion(inner, pa, pb, shape)
+    pulse = GaussianPulse(freq0=dip_freq0, fwidth=dip_fwidth)
+    wf = sample_waveform(pulse, dt, num_steps)
+    idx, coef = dipole_stencil(grid, 0, (R + 2.5 * dl, 0.0, 0.0))
+    dip = PointDipole(component=0, indices=idx, coef=coef, waveform=wf)
+    fmons = []
+    if probe:
+        h = n // 2
+        fmons.append(FieldMonitor(name="probe", freqs=np.array([dip_freq0]),
+                                  origin=(h - 3, h - 3, h - 1), box=(6, 6, 2)))
+    return Scene(grid=grid, dt=dt, num_time_steps=num_steps, shutoff=1e-5,
+                 eps_ex=eps[0], eps_ey=eps[1], eps_ez=eps[2], pml=pml_dict(grid, dt, n_pml),
+                 dispersion=disp, dispersion_mix=mix, dipoles=[dip], field_monitors=fmons)
 
 
 # ---------------------------------------------------------------------------

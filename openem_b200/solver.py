@@ -34,8 +34,6 @@ def refuse_unsupported(sc) -> None:
         (any(getattr(t, "k_hat", None) is None and getattr(t, "open_axes", ())
              for t in getattr(sc, "tfsf_sources", [])), "open-axis TFSF boxes at normal incidence"),
         (len(getattr(sc, "tfsf_sources", [])) > 1, "several TFSF boxes in one scene"),
-        (sc.dispersion_mix is not None and sc.dispersion_mix.n_entry > 0,
-         "slanted-interface mixed dispersion"),
         (sc.modulation is not None and sc.modulation.n_entry > 0
          and (sc.pec_ex is not None or sc.tensor is not None or sc.dispersion_mix is not None),
          "time-modulated media together with PEC, tensor or mixed media"),
@@ -208,6 +206,15 @@ class Plan:
                 L.ptr(self._arr(tt["cell"], np.int64)), L.ptr(self._arr(tt["m1"], np.float32)),
                 L.ptr(self._arr(tt["m2"], np.float32)), L.ptr(self._arr(tt["pec"], np.float32))),
                 "add_tensor")
+        mx = None if self.cplx else T.mix_tables(sc)
+        if mx is not None:
+            L.check(lib.oem_plan_add_dispersion_mix(
+                h, int(mx["comp"].size), L.ptr(self._arr(mx["comp"], np.int32)),
+                L.ptr(self._arr(mx["cell"], np.int64)), L.ptr(self._arr(mx["p_ofs"], np.int32)),
+                L.ptr(self._arr(mx["pc"], np.float32)), int(mx["n_p"]),
+                L.ptr(self._arr(mx["q_ofs"], np.int32)), L.ptr(self._arr(mx["qc"], np.float32)),
+                int(mx["n_q"]), L.ptr(self._arr(mx["k"], np.float32)), float(mx["dte"])),
+                "add_dispersion_mix")
         if getattr(sc, "tfsf_sources", None) and not self.cplx:
             from openem_b200 import tfsf as TF
             tb = TF.box_tables(sc, self.n_total)

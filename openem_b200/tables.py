@@ -220,17 +220,54 @@ def e_coefficients(sc, tabs):
             sl[a] = zero
             ca[c][tuple(sl)] = 0.0
             cb[c][tuple(sl)] = 0.0
-    # full-tensor entries pass the curl through (ca = 0, cb = 1; zero stays zero on a PEC-backed
-    # wall): the tensor passes turn it into E^{n+1} (openem/kernels/tensor.cu)
-    ten = sc.tensor
-    if ten is not None and ten.n_entry:
-        comp = np.asarray(ten.comp)
-        cell = np.asarray(ten.cell, np.int64)
+    # full-tensor and slanted-interface entries pass the curl through (ca = 0, cb = 1; zero stays
+    # zero on a PEC-backed wall): their own passes turn it into E^{n+1}
+    # (openem/kernels/tensor.cu, openem/kernels/dispersion_mix.cu, openem/coeffs.py:162-171)
+    for tab in passthrough_tables(sc):
+        comp = np.asarray(tab.comp)
+        cell = np.asarray(tab.cell, np.int64)
         for c in range(3):
             idx = cell[comp == c]
             ca[c].ravel()[idx] = 0.0
             cb[c].ravel()[idx] = np.where(cb[c].ravel()[idx] != 0.0, 1.0, 0.0)
     return ca, cb
+
+
+def passthrough_tables(sc) -> list:
+    """The entry tables whose cells take the D form (tensor media, mixed dispersion)."""
+    return [t for t in (sc.tensor, sc.dispersion_mix) if t is not None and t.n_entry]
+
+
+def mix_tables(sc) -> dict | None:
+    """Per entry of a slanted-interface table: component, cell, the pole CSR offsets of both
+    branches, float32 pole coefficients as (Re(A-1), Im(A-1), Re(B), Im(B)) rows, the float32
+    coefficients (k1, k2, 1 - beta, 1 / (k1 k2 + beta)) and dt / eps0
+    (openem/device_tables.py:291-321); refused together with modulation or tensor media (each
+    rewrites the same coefficients)."""
+    mm = sc.dispersion_mix
+    if mm is None or mm.n_entry == 0:
+        return None
+    if (sc.modulation is not None and sc.modulation.n_entry) or \
+            (sc.tensor is not None and sc.tensor.n_entry):
+        raise NotImplementedError("mixed dispersion together with modulation or tensor media is "
+                                  "not supported")
+    mm.validate(sc.shape, sc.dispersion)
+    k1, k2, omb, invd = mm.coefficients()
+
+    def rows(a, b):
+        a = np.asarray(a, np.complex128)
+        b = np.asarray(b, np.complex128)
+        if a.size == 0:
+            return np.zeros((1, 4), np.float32)
+        return np.ascontiguousarray(np.stack([a.real, a.imag, b.real, b.imag], 1), np.float32)
+    return {"comp": np.ascontiguousarray(mm.comp, np.int32),
+            "cell": np.ascontiguousarray(mm.cell, np.int64),
+            "p_ofs": np.ascontiguousarray(mm.p_ofs, np.int32),
+            "q_ofs": np.ascontiguousarray(mm.q_ofs, np.int32),
+            "pc": rows(mm.pa, mm.pb), "n_p": int(np.asarray(mm.pa).size),
+            "qc": rows(mm.qa, mm.qb), "n_q": int(np.asarray(mm.qa).size),
+            "k": np.ascontiguousarray(np.stack([k1, k2, omb, invd], 1), np.float32),
+            "dte": float(sc.dt / EPSILON_0)}
 
 
 def tensor_tables(sc, tabs) -> dict | None:
@@ -610,14 +647,17 @@ def absorber_tables(sc) -> list:
 
 
 def dispersion_in_absorbers(sc) -> bool:
-    """True when a dispersive (component, cell) entry lies inside an absorber's layers."""
-    d = sc.dispersion
-    if d is None or d.n_entry == 0 or not getattr(sc, "absorbers", None):
+    """True when a dispersive (component, cell) entry, of the E form or of the mixed form, lies
+    inside an absorber's layers."""
+    if not getattr(sc, "absorbers", None):
         return False
-    cells = np.asarray(d.cell, dtype=np.int64)
-    ijk = np.unravel_index(cells, tuple(int(v) for v in sc.shape))
-    for sl in sc.absorbers:
-        q = ijk[int(sl.axis)]
-        if np.any((q >= int(sl.g0)) & (q < int(sl.g0) + np.size(sl.decay_int))):
-            return True
+    for d in (sc.dispersion, sc.dispersion_mix):
+        if d is None or d.n_entry == 0:
+            continue
+        cells = np.asarray(d.cell, dtype=np.int64)
+        ijk = np.unravel_index(cells, tuple(int(v) for v in sc.shape))
+        for sl in sc.absorbers:
+            q = ijk[int(sl.axis)]
+            if np.any((q >= int(sl.g0)) & (q < int(sl.g0) + np.size(sl.decay_int))):
+                return True
     return False

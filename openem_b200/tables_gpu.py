@@ -105,8 +105,7 @@ def material_tables_device(sc, tabs, device: int = 0) -> DeviceTables:
             sl[a] = zd
             ca3[tuple(sl)] = 0.0
             cb3[tuple(sl)] = 0.0
-        ten = sc.tensor
-        if ten is not None and ten.n_entry:  # curl passthrough (tables.e_coefficients)
+        for ten in T.passthrough_tables(sc):  # curl passthrough (tables.e_coefficients)
             sel = np.asarray(ten.cell, np.int64)[np.asarray(ten.comp) == c]
             if sel.size:
                 td = _to_dev(sel, torch, dev)

@@ -125,8 +125,6 @@ class Oracle:
     def __init__(self, sc, n_total: int | None = None):
         if sc.any_bloch:
             raise ValueError("use BlochOracle for a scene with a non-zero Bloch vector")
-        if sc.any_dispersion_mix:
-            raise NotImplementedError("oracle: mixed dispersion not transcribed")
         self.sc = sc
         self.n_total = int(n_total if n_total is not None else sc.num_time_steps)
         nx, ny, nz = self.shape = sc.shape
@@ -150,6 +148,7 @@ class Oracle:
         self.ca, self.cb = e_coeffs(sc)
         self.hist = [np.zeros(self.shape) for _ in range(3)]
         self._setup_dispersion()
+        self._setup_mix()
         self._setup_modulation()
         self._setup_tensor()
         self._setup_sources()
@@ -468,6 +467,78 @@ class Oracle:
             "b": np.asarray(d.b, dtype=np.complex128),
             "P": np.zeros(int(ofs[-1]), dtype=np.complex128),
         }
+
+    def _setup_mix(self):
+        """Slanted-interface entries (openem/device_tables.py:291-321, openem/coeffs.py:162-171):
+        float64 coefficients ``k1, k2, 1 - beta, 1 / (k1 k2 + beta)``, complex pole states of
+        both branches, the accumulated d_tot and the harmonic unknown d_h; the entries' update
+        coefficients pass the curl through (ca = 0, cb = 1; a zeroed PEC cell stays zero)."""
+        sc = self.sc
+        self.mix = None
+        mm = sc.dispersion_mix
+        if mm is None or mm.n_entry == 0:
+            return
+        mm.validate(self.shape, sc.dispersion)
+        k1, k2, omb, invd = mm.coefficients()
+        comp = np.asarray(mm.comp, np.int64)
+        cell = np.asarray(mm.cell, np.int64)
+        n = comp.size
+        p_ofs = np.asarray(mm.p_ofs, np.int64)
+        q_ofs = np.asarray(mm.q_ofs, np.int64)
+        for c in range(3):
+            idx = cell[comp == c]
+            self.ca[c].ravel()[idx] = 0.0
+            self.cb[c].ravel()[idx] = np.where(self.cb[c].ravel()[idx] != 0.0, 1.0, 0.0)
+        self.mix = {"comp": comp, "cell": cell, "k1": k1, "k2": k2, "omb": omb, "invd": invd,
+                    "p_ent": np.repeat(np.arange(n), np.diff(p_ofs)),
+                    "q_ent": np.repeat(np.arange(n), np.diff(q_ofs)),
+                    "pa": np.asarray(mm.pa, np.complex128), "pb": np.asarray(mm.pb, np.complex128),
+                    "qa": np.asarray(mm.qa, np.complex128), "qb": np.asarray(mm.qb, np.complex128),
+                    "P": np.zeros(int(p_ofs[-1]), np.complex128),
+                    "Q": np.zeros(int(q_ofs[-1]), np.complex128),
+                    "dtot": np.zeros(n), "dh": np.zeros(n), "sp": np.zeros(n), "sq": np.zeros(n),
+                    "dte": sc.dt / EPSILON_0}
+
+    def _mix_field(self):
+        m = self.mix
+        out = np.empty(m["comp"].size)
+        for c in range(3):
+            sel = m["comp"] == c
+            out[sel] = self.E[c].ravel()[m["cell"][sel]]
+        return out
+
+    def mix_pre(self):
+        """Both branches advanced to the half step from E^n and d_h^n
+        (openem/kernels/dispersion_mix.cu:41-85): SP = sum 2 Re(P_half), SQ = sum Re(Q_half)."""
+        m = getattr(self, "mix", None)
+        if m is None:
+            return
+        en = self._mix_field()
+        n = en.size
+        m["P"] += m["pa"] * m["P"] + m["pb"] * en[m["p_ent"]]
+        m["Q"] += m["qa"] * m["Q"] + m["qb"] * m["dh"][m["q_ent"]]
+        m["sp"] = np.zeros(n)
+        np.add.at(m["sp"], m["p_ent"], 2.0 * m["P"].real)
+        m["sq"] = np.zeros(n)
+        np.add.at(m["sq"], m["q_ent"], m["Q"].real)
+
+    def mix_post(self):
+        """The pass-through value (stretched curl, minus J, plus the E-side sources) advances
+        d_tot; the scalar equation gives d_h^{n+1}, E^{n+1} = k2 d_h + SQ, and both branches
+        take their step-(n+1) terms (openem/kernels/dispersion_mix.cu:87-135)."""
+        m = getattr(self, "mix", None)
+        if m is None:
+            return
+        curl = self._mix_field()
+        m["dtot"] = m["dtot"] + m["dte"] * curl
+        dh = (m["dtot"] - m["k1"] * m["sq"] - m["omb"] * m["sp"]) * m["invd"]
+        m["dh"] = dh
+        en = m["k2"] * dh + m["sq"]
+        m["P"] += m["pb"] * en[m["p_ent"]]
+        m["Q"] += m["qb"] * dh[m["q_ent"]]
+        for c in range(3):
+            sel = m["comp"] == c
+            self.E[c].ravel()[m["cell"][sel]] = en[sel]
 
     def _entry_field(self, F):
         d = self.disp
@@ -820,10 +891,12 @@ class Oracle:
         self.inject_h(n)
         self.absorb("H")
         self.disp_pre()
+        self.mix_pre()
         self.modulate(n)
         self.tensor_pre()
         self.update_e()
         self.inject_e(n)
+        self.mix_post()
         self.tensor_post()
         self.disp_post()
         self.absorb("E")
@@ -871,22 +944,37 @@ def run(sc, num_steps: int | None = None) -> OracleResult:
 
 
 class PerturbedOracle(Oracle):
-    """The FP64 oracle with float32-sized rounding noise: after every step each field value
-    is multiplied by ``1 + u * U(-1, 1)`` with ``u = 2**-24`` (half an ulp of float32). The
-    distance of its result from the clean run is the rounding floor of a float32 engine on
-    that scene: how far one float32 rounding per value and step moves the fields. Resonant
-    dispersive scenes amplify it well above 2**-24; a float32 engine cannot be held closer
-    to the FP64 oracle than this floor."""
+    """The FP64 oracle with float32-sized rounding noise: after every step each stored value
+    (the fields, the pole states of the dispersive tables, and the accumulated d_tot and
+    harmonic d_h of the mixed-form entries; real and imaginary parts apart) is multiplied by
+    ``1 + u * U(-1, 1)`` with ``u = 2**-24`` (half an ulp of float32). The distance of its
+    result from the clean run is the rounding floor of a float32 engine on that scene: how far
+    one float32 rounding per stored value and step moves the fields. Resonant dispersive scenes
+    amplify it well above 2**-24; a float32 engine cannot be held closer to the FP64 oracle
+    than this floor."""
 
     def __init__(self, sc, n_total: int | None = None, seed: int = 0):
         super().__init__(sc, n_total)
         self._rng = np.random.default_rng(seed)
 
+    def _noise(self, shape):
+        return 1.0 + 2.0 ** -24 * self._rng.uniform(-1.0, 1.0, shape)
+
     def step(self):
         super().step()
-        u = 2.0 ** -24
         for F in (*self.E, *self.H):
-            F *= 1.0 + u * self._rng.uniform(-1.0, 1.0, F.shape)
+            F *= self._noise(F.shape)
+        states = []
+        if getattr(self, "disp", None) is not None:
+            states.append((self.disp, "P"))
+        if getattr(self, "mix", None) is not None:
+            states += [(self.mix, k) for k in ("P", "Q", "dtot", "dh")]
+        for d, k in states:
+            a = d[k]
+            if np.iscomplexobj(a):
+                d[k] = a.real * self._noise(a.shape) + 1j * a.imag * self._noise(a.shape)
+            else:
+                d[k] = a * self._noise(a.shape)
 
 
 def fp32_floor(sc, num_steps: int | None = None, seed: int = 1, clean=None) -> dict:

@@ -119,11 +119,20 @@ def test_phase_table():
     assert ph.dtype == np.float32 and ph.shape == (5, 2, 4)
 
 
-@pytest.mark.parametrize("feature", ["tfsf", "disp_in_absorber", "modulation_pec", "tensor"])
+@pytest.mark.parametrize("feature", ["tfsf", "disp_in_absorber", "modulation_pec", "tensor",
+                                     "mix_in_absorber", "mix_tensor", "mix_modulation"])
 def test_unsupported_physics_fails_closed(feature):
     sc = scenes.slab_plane_wave(nxy=1, num_steps=10)
     sd = scenes.small_dispersive(n=20, n_sph=1, n_pml=4, num_steps=10)
+    ms = replace(scenes.mixed_sphere(n=20, n_pml=4, radius_cells=3.3, num_steps=10),
+                 dispersion=None)
+    solver.refuse_unsupported(ms)
     bad = {
+        "mix_in_absorber": replace(ms, absorbers=scenes.absorber_slabs(ms.grid, 0, 10)),
+        "mix_tensor": replace(ms, tensor=M.TensorEps(np.array([0]), np.array([0]),
+                                                     np.eye(3)[None], np.zeros((1, 3, 3)))),
+        "mix_modulation": replace(ms, modulation=M.TimeModulation(
+            1e14, np.array([0]), np.array([0]), np.array([0.1]), np.array([0.0]))),
         "tfsf": replace(sc, tfsf_sources=[replace(
             scenes.tfsf_box_scene(n=30, num_steps=10).tfsf_sources[0], open_axes=(0,))]),
         "disp_in_absorber": replace(sd, absorbers=scenes.absorber_slabs(sd.grid, 0, 10)),
@@ -152,15 +161,22 @@ def test_bloch_subset_fails_closed(feature):
     solver.refuse_unsupported_bloch(plain)
 
 
-@pytest.mark.parametrize("feature", ["dispersion", "absorber", "bloch"])
+@pytest.mark.parametrize("feature", ["dispersion", "absorber", "bloch", "mix", "tensor",
+                                     "modulation"])
 def test_adjoint_fails_closed(feature):
-    """The discrete adjoint covers real, non-dispersive scenes without absorbers; the rest is
-    refused before anything reaches the device."""
+    """The discrete adjoint covers real, non-dispersive scenes without absorbers, tensor media or
+    time modulation; the rest is refused before anything reaches the device."""
     from openem_b200 import adjoint
     sd = scenes.small_dispersive(n=20, n_sph=1, n_pml=4, num_steps=10)
     plain = replace(sd, dispersion=None)
     bad = {
         "dispersion": sd,
+        "mix": replace(scenes.mixed_sphere(n=20, n_pml=4, radius_cells=3.3, num_steps=10),
+                       dispersion=None),
+        "tensor": replace(plain, tensor=M.TensorEps(np.array([0]), np.array([0]),
+                                                    np.eye(3)[None], np.zeros((1, 3, 3)))),
+        "modulation": replace(plain, modulation=M.TimeModulation(
+            1e14, np.array([0]), np.array([0]), np.array([0.1]), np.array([0.0]))),
         "absorber": replace(plain, absorbers=scenes.absorber_slabs(plain.grid, 0, 3)),
         "bloch": replace(plain, bloch_k=(0.1, 0.0, 0.0)),
     }[feature]

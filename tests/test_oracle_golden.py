@@ -460,3 +460,101 @@ def test_tensor_closure_and_refusals():
         T.tensor_tables(replace(sc_t, tensor=broken), tabs)
     with pytest.raises(NotImplementedError):
         T.tensor_tables(replace(sc_t, pec_ex=np.array([0])), tabs)
+
+
+# ---- slanted-interface mixed dispersion (openem/kernels/dispersion_mix.cu) ---------------------
+
+MIX_POLES = scenes.lorentz_poles(1.5, 3e14, 3e13)
+
+
+def _mix_bulk(kind, beta=0.0, fill=1.0, steps=300, n=16):
+    """Bulk medium over the whole grid of a dipole scene: ``kind`` "e" (E form, Dispersion),
+    "mix" (DispersionMix with weight beta) or "other" (eps_inf alone, no poles). The medium is
+    the fraction ``fill`` of eps_inf 2.0 plus one Lorentz pair, the rest eps 2.25."""
+    base = scenes.small_dispersive(n=n, n_sph=0, n_pml=4, num_steps=steps, monitors=False)
+    shape = base.shape
+    eps_inf, zinf, pa, pb, qa, qb = scenes.mix_pieces(2.0, MIX_POLES, 2.25, fill, base.dt)
+    eps = np.full(shape, eps_inf)
+    sc = replace(base, eps_ex=eps, eps_ey=eps.copy(), eps_ez=eps.copy(), sigma_ex=None,
+                 sigma_ey=None, sigma_ez=None, dispersion=None)
+    if kind == "e":
+        return replace(sc, dispersion=scenes.build_dispersion([np.ones(shape, bool)] * 3, pa, pb,
+                                                              shape))
+    if kind == "mix":
+        return replace(sc, dispersion_mix=scenes.bulk_mix(shape, beta, pa, pb, qa, qb, eps_inf,
+                                                          zinf))
+    return sc
+
+
+def _e_fields(r):
+    return np.concatenate([np.asarray(r.fields[c], float).ravel() for c in ("Ex", "Ey", "Ez")])
+
+
+def test_zeta_poles_reconstruct_inverse_eps():
+    """The pole expansion of 1/eps reproduces 1/eps(s) with every pole in the left half plane
+    (openem/scene/poles.py:339-375)."""
+    zi, p, r = scenes.zeta_poles(2.0, MIX_POLES)
+    assert np.all(p.real < 0)
+    for w in (3e13, 2.5e14, 3e14, 4e15):
+        s = -1j * 2 * np.pi * w
+        eps = 2.0 + sum(c / (s - a) + np.conj(c) / (s - np.conj(a)) for a, c in MIX_POLES)
+        zeta = zi + np.sum(r / (s - p))
+        assert abs(zeta * eps - 1.0) < 1e-12
+
+
+def test_oracle_mix_beta_zero_equals_e_form():
+    """OpenEM's first mixed-form criterion (tests/test_dispersion.py test_mix_beta_zero_equals_
+    e_form): at beta = 0 the accumulated d_tot and the scalar solve E = (d_tot - SP)/(eps_inf +
+    G_P) are the E form of the same poles by induction; in FP64 they agree to rounding."""
+    a = ref64.run(_mix_bulk("e", fill=0.5))
+    b = ref64.run(_mix_bulk("mix", beta=0.0, fill=0.5))
+    ea, eb = _e_fields(a), _e_fields(b)
+    assert np.abs(ea).max() > 0
+    assert np.linalg.norm(eb - ea) <= 1e-9 * np.linalg.norm(ea)
+
+
+def test_oracle_mix_harmonic_branch_is_the_same_material():
+    """OpenEM's second criterion (test_harmonic_and_arithmetic_branches_agree_on_same_material):
+    the pure harmonic branch (beta = 1, poles of 1/eps) and the E form (poles of eps) of one
+    material are two discretisations that agree to O(dt^2), far closer than eps_inf alone."""
+    e = _e_fields(ref64.run(_mix_bulk("e")))
+    d = _e_fields(ref64.run(_mix_bulk("mix", beta=1.0)))
+    o = _e_fields(ref64.run(_mix_bulk("other")))
+    same = np.linalg.norm(d - e) / np.linalg.norm(e)
+    diff = np.linalg.norm(o - e) / np.linalg.norm(e)
+    assert same < 0.02 and same < diff / 20, (same, diff)
+
+
+def test_oracle_mix_middle_beta_lies_between():
+    """OpenEM's discriminating-power criterion (test_mix_middle_beta_lies_between_and_is_
+    stable): with two materials in the cell, beta moves the result, and intermediate weights
+    stay inside the interval the two limits span."""
+    out = {b: _e_fields(ref64.run(_mix_bulk("mix", beta=b, fill=0.5)))
+           for b in (0.0, 0.35, 0.7, 1.0)}
+    span = np.abs(out[1.0] - out[0.0]).max()
+    assert span / np.abs(out[0.0]).max() > 0.05
+    for b in (0.35, 0.7):
+        assert np.isfinite(out[b]).all()
+        assert np.abs(out[b] - out[0.0]).max() < 1.05 * span
+        assert np.abs(out[b] - out[1.0]).max() < 1.05 * span
+
+
+def test_mix_validation():
+    """beta outside [0, 1], an entry shared with the E-form table and a zero denominator are
+    refused (openem/model.py:591-612)."""
+    z = np.zeros(0, complex)
+    one = dict(comp=np.array([0]), cell=np.array([3]), p_ofs=np.array([0, 0]), pa=z, pb=z,
+               q_ofs=np.array([0, 0]), qa=z, qb=z)
+    with pytest.raises(ValueError, match=r"\[0,1\]"):
+        M.DispersionMix(**one, beta=np.array([1.4]), eps_inf=np.array([2.0]),
+                        zeta_inf=np.array([0.5])).validate((4, 4, 4))
+    with pytest.raises(ValueError, match="zero"):
+        M.DispersionMix(**one, beta=np.array([0.0]), eps_inf=np.array([2.0]),
+                        zeta_inf=np.array([0.0])).validate((4, 4, 4))
+    ok = M.DispersionMix(**one, beta=np.array([0.3]), eps_inf=np.array([2.0]),
+                         zeta_inf=np.array([0.5]))
+    ok.validate((4, 4, 4))
+    d = M.Dispersion(comp=np.array([0]), cell=np.array([3]), pole_ofs=np.array([0, 0]), am1=z,
+                     b=z, g=np.zeros(1))
+    with pytest.raises(ValueError, match="more than one"):
+        ok.validate((4, 4, 4), d)
