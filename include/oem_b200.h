@@ -299,6 +299,12 @@ int oem_plan_read_time_monitor_complex(oem_plan* p, int id, float* re, float* im
  * imaginary parts; time samples (nc, nslots, ni, nj, nk) float32; one field component
  * (0..5) as an unpadded (nx, ny, nz) float32 array. */
 int oem_plan_read_monitor(oem_plan* p, int id, double* re, double* im, void* stream);
+
+/* The same phasors as oem_plan_read_monitor, written as interleaved (re, im) pairs into one
+ * host array of 2 x ncomp x nf x cells doubles: the memory layout of a complex128 array of the
+ * monitor's shape, so the host assembles nothing (interleaved on the device, copied out in
+ * chunks). */
+int oem_plan_read_monitor_interleaved(oem_plan* p, int mon_id, double* out, void* stream);
 int oem_plan_read_time_monitor(oem_plan* p, int id, float* out, void* stream);
 int oem_plan_read_field(oem_plan* p, int comp, float* out, void* stream);
 int oem_plan_write_field(oem_plan* p, int comp, const float* in, void* stream);

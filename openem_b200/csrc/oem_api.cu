@@ -1811,6 +1811,38 @@ int oem_plan_read_monitor(oem_plan* p, int id, double* re, double* im, void* str
   return check_device_error(p);
 }
 
+int oem_plan_read_monitor_interleaved(oem_plan* p, int id, double* out, void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (id < 0 || id >= (int)p->mons.size()) return set_error(OEM_ERR_INVALID, "monitor id out of range");
+  if (!out) return set_error(OEM_ERR_INVALID, "null output");
+  if ((rc = use_device(p))) return rc;
+  const Monitor& m = p->mons[id];
+  const int64_t n = (int64_t)m.ncomp * m.nf * m.cells;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // interleaved on the device in chunks through two buffers of at most 4M values (64 MB) the
+  // plan keeps after its first readout, each chunk copied out while the next is formed
+  if (!p->rd_scratch[0]) {  // sized for the plan's largest monitor, up to 4M values
+    int64_t most = 1;
+    for (const Monitor& q : p->mons) most = std::max(most, (int64_t)q.ncomp * q.nf * q.cells);
+    p->rd_chunk = std::min(most, (int64_t)1 << 22);
+    for (int b = 0; b < 2; ++b)
+      if ((rc = dalloc(p, &p->rd_scratch[b], (size_t)p->rd_chunk, false))) return rc;
+  }
+  const int64_t kChunk = p->rd_chunk;
+  cudaError_t e = cudaSuccess;
+  for (int64_t q0 = 0, b = 0; q0 < n && e == cudaSuccess; q0 += kChunk, b ^= 1) {
+    const int64_t c = std::min(kChunk, n - q0);
+    e = launch_interleave(m.d_re + q0, m.d_im + q0, p->rd_scratch[b], c, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(out + 2 * q0, p->rd_scratch[b], (size_t)c * sizeof(double2),
+                          cudaMemcpyDeviceToHost, s);
+  }
+  if (e != cudaSuccess) return cuda_error(e, "read_monitor_interleaved");
+  OEM_CUDA(cudaStreamSynchronize(s));
+  return check_device_error(p);
+}
+
 int oem_plan_read_time_monitor(oem_plan* p, int id, float* out, void* stream) {
   int rc = check_plan(p, true);
   if (rc) return rc;

@@ -333,6 +333,8 @@ struct oem_plan {
   std::vector<oem::Tfsf> tfsfs;
   std::vector<oem::TensorSet> tensors;
   std::vector<oem::MixSet> mixes;
+  double2* rd_scratch[2] = {nullptr, nullptr};  // readout interleave buffers (lazy)
+  int64_t rd_chunk = 0;
 
   // device state
   std::vector<void*> allocs;
@@ -457,6 +459,8 @@ cudaError_t launch_tfsf(const YeeParams& P, const Tfsf& t, int is_e, const int* 
 cudaError_t launch_tensor_pre(const YeeParams& P, const TensorSet& t, cudaStream_t s);
 cudaError_t launch_tensor_post(const YeeParams& P, const TensorSet& t, cudaStream_t s);
 cudaError_t launch_mix_pre(const YeeParams& P, const MixSet& m, cudaStream_t s);
+cudaError_t launch_interleave(const double* re, const double* im, double2* out, int64_t n,
+                              cudaStream_t s);
 cudaError_t launch_mix_post(const YeeParams& P, const MixSet& m, cudaStream_t s);
 
 // Discrete adjoint (oem_adjoint.cu): adjoint fields, their CPML psi, scratch for the transposed

@@ -953,6 +953,22 @@ cudaError_t launch_flush(const Monitor& m, const int* step, int forced, cudaStre
   return cudaGetLastError();
 }
 
+// (re, im) pairs of n values side by side: the layout of a host complex128 array.
+__global__ void k_interleave(const double* __restrict__ re, const double* __restrict__ im,
+                             double2* __restrict__ out, int64_t n) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x)
+    out[q] = make_double2(re[q], im[q]);
+}
+
+cudaError_t launch_interleave(const double* re, const double* im, double2* out, int64_t n,
+                              cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int64_t nb = std::min<int64_t>((n + 255) / 256, 148 * 16);
+  k_interleave<<<(unsigned)nb, 256, 0, s>>>(re, im, out, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_step_advance(int* step, cudaStream_t s) {
   k_step_advance<<<1, 32, 0, s>>>(step);
   return cudaGetLastError();

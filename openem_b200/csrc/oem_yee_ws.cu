@@ -851,8 +851,13 @@ constexpr int kF_EB = 0;                      // E^n box x3: rows j0-1 .. j0+4, 
 constexpr int kF_EN = kF_EB + 3 * kF_EBS;     // Ey, Ez of plane X.nxt[i]: rows j0-1 .. j0+3
 constexpr int kF_HO = kF_EN + 2 * kF_T5;      // H^{n-1/2} x3: rows j0-1 .. j0+3
 constexpr int kF_MT = kF_HO + 3 * kF_T5;      // material tile, rows j0 .. j0+3
-constexpr int kF_ZS = kF_MT + 512;            // Hx, Hy of H^{n+1/2} at (rows, k0 - 1) [c][row]
-constexpr int kFStage = kF_ZS + 32;
+constexpr int kFStage = kF_MT + 512;
+// Hx, Hy of H^{n+1/2} at (rows j0 .. j0+3, k0 - 1) of the main planes, a ring of kF_HRP planes
+// [plane % kF_HRP][c][row], filled kF_HB planes at a time by the 32 producer lanes
+constexpr int kF_HRP = 16;
+constexpr int kF_HB = 8;
+constexpr int kF_HR = kF_HRP * 2 * kTY;
+static_assert(kF_HB * kTY == 32 && kF_HRP >= kF_HB + kFS + 1, "halo ring covers the batches");
 constexpr uint32_t kF_EBBytes = 6 * kBZ * 4;
 constexpr uint32_t kF_T5Bytes = 5 * kTZ * 4;
 constexpr int kF_HN = 2 * 3 * 5 * kTZ;        // H^{n+1/2} of two planes [parity][comp][row][z]
@@ -1055,7 +1060,8 @@ __global__ void __launch_bounds__(192, 2) k_he_ws(const __grid_constant__ FusedM
   float* hn = smem + kFS * kFStage;
   float* zth = hn + kF_HN;
   float* zte = zth + kZTab;
-  MatRec* smats = reinterpret_cast<MatRec*>(zte + kZTab);
+  float* hring = zte + kZTab;
+  MatRec* smats = reinterpret_cast<MatRec*>(hring + kF_HR);
   uint64_t* full = reinterpret_cast<uint64_t*>(smats + kSmemMats);
   uint64_t* empty = full + kFS;
   const int lane = threadIdx.x, w = threadIdx.y;
@@ -1083,8 +1089,9 @@ __global__ void __launch_bounds__(192, 2) k_he_ws(const __grid_constant__ FusedM
   load_ztab(zte, Z, false, k0, P.nzp, tid, 192);
   if (w == 5 && lane == 0) {
     for (int s = 0; s < kFS; ++s) {
-      // lane 0's arrival with the transaction bytes, and one per halo-cell lane
-      mbar_init(&full[s], 1 + kTY);
+      // lane 0's arrival with the transaction bytes, and one per producer lane after its
+      // halo-ring writes
+      mbar_init(&full[s], 1 + 32);
       mbar_init(&empty[s], kTY + 1);
     }
     mbar_fence_init();
@@ -1092,16 +1099,16 @@ __global__ void __launch_bounds__(192, 2) k_he_ws(const __grid_constant__ FusedM
   __syncthreads();
 
   if (w == 5) {  // ------------------------------------------------------------ producer
-    // lane 0 issues the stage's copies; lanes 0..3 compute the halo cell (row j0 + lane,
-    // k0 - 1) of the stage's plane from global memory, stage depths ahead of the consumers
-    if (lane >= kTY) return;
+    // lane 0 issues the stage's copies; at every kF_HB-th main plane the 32 lanes compute the
+    // halo cells (row j0 + lane % 4, k0 - 1) of the next kF_HB main planes (plane lane / 4) from
+    // global memory at once, so their dependent loads overlap instead of serialising per plane
     int issued = 0;
     bool ok = true;
     const uint32_t mbytes = (uint32_t)(kTY * kTZ * (wide ? 4 : 2));
     for (int q = 0; q < nst && ok; ++q) {
       const int slot = q % kFS;
       if (q >= kFS) ok = mbar_wait(&empty[slot], (uint32_t)((q / kFS - 1) & 1), err);
-      if (!__all_sync(0xfu, ok)) break;
+      if (!__all_sync(kFull, ok)) break;
       float* st = smem + slot * kFStage;
       const bool main = !(pre && q == 0);
       const int i = main ? ib + q - (pre ? 1 : 0) : pp;
@@ -1116,11 +1123,16 @@ __global__ void __launch_bounds__(192, 2) k_he_ws(const __grid_constant__ FusedM
         tma3(st + kF_EN + kF_T5, &maps.e5[1], &full[slot], k0, j0 - 1, inext);
         tma3(st + kF_MT, &maps.m, &full[slot], k0, j0, i);
       }
-      if (main && k0 > 0 && j0 + lane < P.ny) {
-        float a, b;
-        fused_h_cell(P, i, j0 + lane, k0 - 1, &a, &b);
-        st[kF_ZS + lane] = a;
-        st[kF_ZS + kTY + lane] = b;
+      const int qm = q - (pre ? 1 : 0);  // main plane index
+      if (main && k0 > 0 && qm % kF_HB == 0) {
+        const int pm = qm + lane / kTY, r = lane % kTY;
+        if (pm < np && j0 + r < P.ny) {
+          float a, b;
+          fused_h_cell(P, ib + pm, j0 + r, k0 - 1, &a, &b);
+          float* hr = hring + (pm % kF_HRP) * 2 * kTY;
+          hr[r] = a;
+          hr[kTY + r] = b;
+        }
       }
       mbar_arrive(&full[slot]);
       issued = q + 1;
@@ -1225,8 +1237,9 @@ __global__ void __launch_bounds__(192, 2) k_he_ws(const __grid_constant__ FusedM
           hxm = hn_row(hn, par, 0, hr)[4 * lane - 1];
           hym = hn_row(hn, par, 1, hr)[4 * lane - 1];
         } else if (k0 > 0) {
-          hxm = st[kF_ZS + w];
-          hym = st[kF_ZS + kTY + w];
+          const float* hr = hring + ((t - (pre ? 1 : 0)) % kF_HRP) * 2 * kTY;
+          hxm = hr[w];
+          hym = hr[kTY + w];
         } else {  // k = 0: the clamped neighbour is the cell itself
           hxm = hx[0];
           hym = hy[0];
@@ -1324,7 +1337,7 @@ size_t ws_e_smem() {
 int ws_max_xchunk() { return kXMax; }
 
 size_t he_smem() {
-  return (size_t)kFS * kFStage * 4 + (size_t)(kF_HN + 2 * kZTab) * 4 +
+  return (size_t)kFS * kFStage * 4 + (size_t)(kF_HN + 2 * kZTab + kF_HR) * 4 +
          kSmemMats * sizeof(MatRec) + 2 * kFS * sizeof(uint64_t);
 }
 

@@ -494,7 +494,7 @@ def check_csr(name: str, shape, comp, cell, ofs_list) -> np.ndarray:
     key = comp.astype(np.int64) * ncell + cell.astype(np.int64)
     seen = np.zeros(3 * ncell, dtype=bool)
     seen[key] = True
-    nu = int(seen.sum())
+    nu = int(np.count_nonzero(seen))
     if nu != n:
         raise ValueError(f"{name}: {n - nu} duplicate (comp, cell) entries")
     return key

@@ -326,11 +326,10 @@ class Plan:
         return int(v.value)
 
     def read_monitor(self, mid: int, shape) -> np.ndarray:
-        re = np.empty(shape, np.float64)
-        im = np.empty(shape, np.float64)
-        L.check(self.lib.oem_plan_read_monitor(self.h, int(mid), L.ptr(re), L.ptr(im), self._s),
+        out = np.empty(shape, np.complex128)
+        L.check(self.lib.oem_plan_read_monitor_interleaved(self.h, int(mid), L.ptr(out), self._s),
                 "read_monitor")
-        return re + 1j * im
+        return out
 
     def adjoint_flux(self, mid: int, weights, dA1, dA2, box=None):
         """dJ/dca and dJ/dcb, (3, ni, nj, nk) float64 each, of ``J = sum_f weights[f] P_f``

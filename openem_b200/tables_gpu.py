@@ -50,9 +50,55 @@ def _to_dev(a, torch, dev, dtype=None):
     return t.to(dev, non_blocking=False)
 
 
+class _Uploads:
+    """The float64 eps and sigma arrays of each component copied to the device on a worker
+    thread, one component ahead of the caller: the first overlaps the host-side pole-set
+    deduplication, each later one the key building of the previous component, and at most two
+    components are resident at a time. The copies are synchronous on the worker's stream; the
+    caller's stream is recorded on each tensor before use."""
+
+    def __init__(self, sc, torch, dev):
+        from concurrent.futures import ThreadPoolExecutor
+        self.torch, self.dev = torch, dev
+        self.eps = (sc.eps_ex, sc.eps_ey, sc.eps_ez)
+        self.sig = (sc.sigma_ex, sc.sigma_ey, sc.sigma_ez)
+        self.pool = ThreadPoolExecutor(max_workers=1)
+        self.futs = [self.pool.submit(self._load, 0)]
+
+    def _load(self, c):
+        torch, dev = self.torch, self.dev
+        torch.cuda.set_device(dev)
+        eps = _to_dev(np.asarray(self.eps[c], np.float64), torch, dev).reshape(-1)
+        sig = (None if self.sig[c] is None
+               else _to_dev(np.asarray(self.sig[c], np.float64), torch, dev).reshape(-1))
+        return eps, sig
+
+    def get(self, c):
+        if c + 1 < 3:
+            self.futs.append(self.pool.submit(self._load, c + 1))
+        eps, sig = self.futs[c].result()
+        self.futs[c] = None
+        cur = self.torch.cuda.current_stream(self.dev)
+        for t in (eps, sig):
+            if t is not None:
+                t.record_stream(cur)
+        return eps, sig
+
+    def close(self):
+        self.pool.shutdown(wait=True, cancel_futures=True)
+
+
 def material_tables_device(sc, tabs, device: int = 0) -> DeviceTables:
     import torch
     dev = torch.device("cuda", device)
+    up = _Uploads(sc, torch, dev)
+    try:
+        return _material_tables_device(sc, tabs, torch, dev, up)
+    finally:
+        up.close()
+
+
+def _material_tables_device(sc, tabs, torch, dev, up) -> DeviceTables:
     shape = tuple(int(v) for v in sc.shape)
     nx, ny, nz = shape
     ncell = nx * ny * nz
@@ -65,16 +111,14 @@ def material_tables_device(sc, tabs, device: int = 0) -> DeviceTables:
         g_d = _to_dev(np.asarray(sc.dispersion.g, np.float64), torch, dev)
     else:
         set_ofs, coef, counts = np.zeros(1, np.int32), np.zeros((0, 4), np.float32), np.zeros(0, np.int32)
-    sig = (sc.sigma_ex, sc.sigma_ey, sc.sigma_ez)
     pecs = (sc.pec_ex, sc.pec_ey, sc.pec_ez)
     dt = float(sc.dt)
     keys, ca_l, cb_l, eps_l, ps_l = [], [], [], [], []
     mask32 = 0xFFFFFFFF
-    for c, eps_h in enumerate((sc.eps_ex, sc.eps_ey, sc.eps_ez)):
-        eps = _to_dev(np.asarray(eps_h, np.float64), torch, dev).reshape(-1)
-        s = (torch.zeros_like(eps) if sig[c] is None
-             else _to_dev(np.asarray(sig[c], np.float64), torch, dev).reshape(-1) * dt
-             / (2.0 * T.EPSILON_0))
+    for c in range(3):
+        eps, sg = up.get(c)
+        s = torch.zeros_like(eps) if sg is None else sg * dt / (2.0 * T.EPSILON_0)
+        del sg
         gg = torch.zeros_like(eps)
         ps = torch.full((ncell,), -1, dtype=torch.int64, device=dev)
         if ep is not None:
