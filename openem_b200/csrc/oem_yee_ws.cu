@@ -161,86 +161,62 @@ __device__ __forceinline__ bool zslab_staged(const DevAxis& Z, int side, int k0)
   return side ? (k0 + kTZ > Z.n - L && k0 < Z.n) : (k0 < L);
 }
 
-// Producer helper: issue the psi rows of plane i for one field family into a stage.
-// Returns the bytes issued.
-__device__ uint32_t stage_psi(const PsiSet& S, const YeeParams& P, float* px, float* py,
-                              float* pz, uint64_t* bar, int i, int j0, int k0) {
+// The psi rows a tile stages, fixed for all planes of a block: the y slab rows among its rows
+// and the staged z slab sides; only the x slab planes add rows (two per row and slot).
+struct PsiTile {
+  uint32_t rowb;     // bytes of one staged row (the tile's z extent)
+  int nrows;         // rows of the tile inside the grid
+  unsigned ymask;    // rows in a y slab
+  bool zs0, zs1;     // staged z slab sides
+  uint32_t yzbytes;  // bytes of the y and z rows
+  uint32_t xbytes;   // bytes of the x rows of a slab plane
+};
+
+__device__ __forceinline__ PsiTile psi_tile(const YeeParams& P, int j0, int k0) {
+  const DevAxis& Y = P.ax[1];
+  const DevAxis& Z = P.ax[2];
+  PsiTile t;
+  t.rowb = (uint32_t)min(kTZ, P.nzp - k0) * 4;
+  t.nrows = min(kTY, P.ny - j0);
+  t.ymask = 0;
+#pragma unroll
+  for (int r = 0; r < kTY; ++r) t.ymask |= (unsigned)(r < t.nrows && in_slab(Y, j0 + r)) << r;
+  t.zs0 = zslab_staged(Z, 0, k0);
+  t.zs1 = zslab_staged(Z, 1, k0);
+  t.yzbytes = 2u * t.rowb * (uint32_t)__popc(t.ymask) +
+              (t.zs0 ? 2u * (uint32_t)(t.nrows * Z.lo) * 4 : 0u) +
+              (t.zs1 ? 2u * (uint32_t)(t.nrows * Z.hi) * 4 : 0u);
+  t.xbytes = 2u * t.rowb * (uint32_t)t.nrows;
+  return t;
+}
+
+// Producer helper: issue the psi rows of plane i (x rows when `xsl`) for one field family into
+// a stage: x rows at px, y rows at py ([slot][row][z] each), z slab rows at pz
+// ([slot][side][row * depth]).
+__device__ __forceinline__ void stage_psi(const PsiTile& T, const PsiSet& S, const YeeParams& P,
+                                          float* px, float* py, float* pz, uint64_t* bar, int i,
+                                          int j0, int k0, bool xsl) {
   const DevAxis& X = P.ax[0];
   const DevAxis& Y = P.ax[1];
   const DevAxis& Z = P.ax[2];
-  const uint32_t rowb = (uint32_t)min(kTZ, P.nzp - k0) * 4;
-  uint32_t bytes = 0;
-  const bool xsl = in_slab(X, i);
-  for (int r = 0; r < kTY; ++r) {
-    const int j = j0 + r;
-    if (j >= P.ny) break;
+  for (int r = 0; r < T.nrows; ++r) {
     if (xsl)
-      for (int s = 0; s < 2; ++s) {
-        bulk(px + (s * 4 + r) * kTZ, psi_addr(S, 0, s, X, i, j, k0, P.ny, P.nzp), rowb, bar);
-        bytes += rowb;
-      }
-    if (in_slab(Y, j))
-      for (int s = 0; s < 2; ++s) {
-        bulk(py + (s * 4 + r) * kTZ, psi_addr(S, 1, s, Y, i, j, k0, P.ny, P.nzp), rowb, bar);
-        bytes += rowb;
-      }
+      for (int s = 0; s < 2; ++s)
+        bulk(px + (s * 4 + r) * kTZ, psi_addr(S, 0, s, X, i, j0 + r, k0, P.ny, P.nzp), T.rowb,
+             bar);
+    if ((T.ymask >> r) & 1u)
+      for (int s = 0; s < 2; ++s)
+        bulk(py + (s * 4 + r) * kTZ, psi_addr(S, 1, s, Y, i, j0 + r, k0, P.ny, P.nzp), T.rowb,
+             bar);
   }
-  // z slabs: the rows of the tile are adjacent in memory, one copy per (slot, side)
-  const int nrows = min(kTY, P.ny - j0);
   for (int side = 0; side < 2; ++side) {
-    if (!zslab_staged(Z, side, k0)) continue;
+    if (!(side ? T.zs1 : T.zs0)) continue;
     const int L = side ? Z.hi : Z.lo;
     const int kk = side ? Z.n - L : 0;
-    for (int s = 0; s < 2; ++s) {
+    for (int s = 0; s < 2; ++s)
       bulk(pz + (s * 2 + side) * kTY * kZMax, psi_addr(S, 2, s, Z, i, j0, kk, P.ny, P.nzp),
-           (uint32_t)(nrows * L) * 4, bar);
-      bytes += (uint32_t)(nrows * L) * 4;
-    }
+           (uint32_t)(T.nrows * L) * 4, bar);
   }
-  return bytes;
-}
-
-// Bytes stage_psi would issue (the producer arms the barrier before issuing).
-__device__ uint32_t psi_bytes(const YeeParams& P, int i, int j0, int k0) {
-  const DevAxis& X = P.ax[0];
-  const DevAxis& Y = P.ax[1];
-  const DevAxis& Z = P.ax[2];
-  const uint32_t rowb = (uint32_t)min(kTZ, P.nzp - k0) * 4;
-  uint32_t bytes = 0;
-  const bool xsl = in_slab(X, i);
-  for (int r = 0; r < kTY; ++r) {
-    const int j = j0 + r;
-    if (j >= P.ny) break;
-    if (xsl) bytes += 2 * rowb;
-    if (in_slab(Y, j)) bytes += 2 * rowb;
-  }
-  const int nrows = min(kTY, P.ny - j0);
-  for (int side = 0; side < 2; ++side)
-    if (zslab_staged(Z, side, k0)) bytes += 2u * (uint32_t)(nrows * (side ? Z.hi : Z.lo)) * 4;
-  return bytes;
-}
-
-// Offsets (floats) of the psi rows of plane i in the E kernel's pool, -1 where absent; returns
-// the floats they take (a multiple of 512, so the pole window after them stays aligned).
-__device__ int psi_pool_layout(const YeeParams& P, int i, int j0, int k0, int offs[3]) {
-  int cur = 0;
-  offs[0] = offs[1] = offs[2] = -1;
-  if (in_slab(P.ax[0], i)) {
-    offs[0] = cur;
-    cur += 1024;
-  }
-  bool y = false;
-#pragma unroll
-  for (int r = 0; r < kTY; ++r) y |= (j0 + r < P.ny) && in_slab(P.ax[1], j0 + r);
-  if (y) {
-    offs[1] = cur;
-    cur += 1024;
-  }
-  if (zslab_staged(P.ax[2], 0, k0) || zslab_staged(P.ax[2], 1, k0)) {
-    offs[2] = cur;
-    cur += 512;
-  }
-  return cur;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -373,14 +349,17 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_h_ws(const __grid_con
     if (lane != 0) return;
     int issued = 0;
     bool ok = true;
+    // the tile's y and z psi rows are fixed once; per plane only the x slab rows are added
+    const PsiTile pt = psi_tile(P, j0, k0);
     for (int q = 0; q < np && ok; ++q) {
       const int slot = q % kS;
       if (q >= kS) ok = mbar_wait(&empty[slot], (uint32_t)((q / kS - 1) & 1), err);
       if (!ok) break;
       float* st = smem + slot * kHStage;
       const int i = ib + q;
+      const bool xsl = in_slab(X, i);
       const int inext = (i + 1 < P.nx) ? i + 1 : X.nxt[P.nx - 1];
-      const uint32_t bytes = 3 * kWideBytes + 5 * kTileBytes + psi_bytes(P, i, j0, k0);
+      const uint32_t bytes = 3 * kWideBytes + 5 * kTileBytes + pt.yzbytes + (xsl ? pt.xbytes : 0u);
       mbar_expect_tx(&full[slot], bytes);
       for (int c = 0; c < 3; ++c) {
         tma3(st + kH_EB + c * kBoxW, &maps.e_wide[c], &full[slot], k0, j0, i);
@@ -389,7 +368,7 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_h_ws(const __grid_con
       // only Ey, Ez of the next plane enter the x derivatives
       tma3(st + kH_EN + 512, &maps.e_tile[1], &full[slot], k0, j0, inext);
       tma3(st + kH_EN + 1024, &maps.e_tile[2], &full[slot], k0, j0, inext);
-      stage_psi(P.psih, P, st + kH_PX, st + kH_PY, st + kH_PZ, &full[slot], i, j0, k0);
+      stage_psi(pt, P.psih, P, st + kH_PX, st + kH_PY, st + kH_PZ, &full[slot], i, j0, k0, xsl);
       issued = q + 1;
     }
     for (int q = max(0, issued - kS); q < issued; ++q)  // drain (no-op when consumed)
@@ -594,11 +573,19 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
     int issued = 0;
     bool ok = true;
     const uint32_t mbytes = (uint32_t)(kTY * kTZ * (wide ? 4 : 2));
+    // the tile's y and z psi rows are fixed once; per plane only the x slab rows are added.
+    // Pool layout per plane: x rows (1024 floats), y rows (1024), z rows (512) where present,
+    // then the pole-current window.
+    const PsiTile pt = psi_tile(P, j0, k0);
     for (int q = 0; q < np && ok; ++q) {
       const int slot = q % kS;
       const int i = ib + q;
-      int offs[3];
-      const int wbase = psi_pool_layout(P, i, j0, k0, offs);
+      const bool xsl = in_slab(X, i);
+      int offs[3] = {-1, -1, -1};
+      int wbase = 0;
+      if (xsl) { offs[0] = wbase; wbase += 1024; }
+      if (pt.ymask) { offs[1] = wbase; wbase += 1024; }
+      if (pt.zs0 || pt.zs1) { offs[2] = wbase; wbase += 512; }
       const int cap = kEPool - wbase;  // pole currents (floats) this plane can stage
       int pstart[kTY], poff[kTY], pcnt[kTY];
       int used = 0;
@@ -623,8 +610,8 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
       float* st = smem + slot * kEStage;
       int* tab = reinterpret_cast<int*>(st + kE_PT);
       const int iprev = (i > 0) ? i - 1 : X.prv[0];
-      uint32_t bytes = 3 * kWideBytes + 5 * kTileBytes + mbytes + psi_bytes(P, i, j0, k0) +
-                       (uint32_t)used * 4;
+      uint32_t bytes = 3 * kWideBytes + 5 * kTileBytes + mbytes + pt.yzbytes +
+                       (xsl ? pt.xbytes : 0u) + (uint32_t)used * 4;
 #pragma unroll
       for (int r = 0; r < kTY; ++r) {
         tab[2 * r] = pstart[r];
@@ -643,7 +630,8 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
       tma3(st + kE_HP + 512, &maps.h_tile[2], &full[slot], k0, j0, iprev);
       tma3(st + kE_MT, &maps.m_tile, &full[slot], k0, j0, i);
       float* pool = st + kE_POOL;
-      stage_psi(P.psie, P, pool + offs[0], pool + offs[1], pool + offs[2], &full[slot], i, j0, k0);
+      stage_psi(pt, P.psie, P, pool + offs[0], pool + offs[1], pool + offs[2], &full[slot], i, j0,
+                k0, xsl);
 #pragma unroll
       for (int r = 0; r < kTY; ++r)
         if (pcnt[r] > 0) {
