@@ -148,7 +148,29 @@ static int alloc_psi(oem_plan* p) {
   return OEM_OK;
 }
 
+// The imaginary part of a complex plan seen as a real plan: its field and psi arrays in place
+// of the real ones (the real kernels read only f, psih and psie).
+static YeeParams imag_part(const YeeParams& P) {
+  YeeParams Q = P;
+  for (int c = 0; c < 6; ++c) {
+    Q.f[c] = P.fi[c];
+    Q.fi[c] = P.f[c];
+  }
+  Q.psih = P.psih_i;
+  Q.psie = P.psie_i;
+  Q.psih_i = P.psih;
+  Q.psie_i = P.psie;
+  return Q;
+}
+
 static cudaError_t run_h(oem_plan* p, cudaStream_t s) {
+  if (p->is_complex && p->cplx_ws) {
+    cudaError_t e = launch_update_h_ws(p->tma, p->yp, p->xch, p->d_err, s);
+    if (e == cudaSuccess) e = launch_update_h_ws(p->tma_i, imag_part(p->yp), p->xch, p->d_err, s);
+    for (const SeamFace& f : p->seam_h)
+      if (e == cudaSuccess) e = launch_seam_h(p->yp, f, s);
+    return e;
+  }
   if (p->is_complex) return launch_update_h_c(p->yp, s);
   if (p->basic_kernels == 1) return launch_update_h(p->yp, s);
   if (p->basic_kernels == 2) return launch_update_h_stream(p->yp, p->xch, s);
@@ -157,6 +179,15 @@ static cudaError_t run_h(oem_plan* p, cudaStream_t s) {
 }
 
 static cudaError_t run_e(oem_plan* p, cudaStream_t s) {
+  if (p->is_complex && p->cplx_ws) {
+    const int nm = (int)p->mats.size();
+    cudaError_t e = launch_update_e_ws(p->tma, p->yp, p->xch, nm, p->d_err, s);
+    if (e == cudaSuccess)
+      e = launch_update_e_ws(p->tma_i, imag_part(p->yp), p->xch, nm, p->d_err, s);
+    for (const SeamFace& f : p->seam_e)
+      if (e == cudaSuccess) e = launch_seam_e(p->yp, f, s);
+    return e;
+  }
   if (p->is_complex) return launch_update_e_c(p->yp, s);
   if (p->basic_kernels == 1) return launch_update_e(p->yp, s);
   if (p->basic_kernels == 2) return launch_update_e_stream(p->yp, p->xch, (int)p->mats.size(), s);
@@ -210,18 +241,20 @@ static int encode_map(oem_plan* p, CUtensorMap* m, const void* base, bool u16, b
   return OEM_OK;
 }
 
-int make_tma_maps(oem_plan* p) {
+int make_tma_maps_of(oem_plan* p, TmaMaps& m, const YeeParams& P) {
   int rc;
-  const YeeParams& P = p->yp;
   for (int c = 0; c < 3; ++c) {
-    if ((rc = encode_map(p, &p->tma.e_wide[c], P.f[c], false, false, 136, 5))) return rc;
-    if ((rc = encode_map(p, &p->tma.e_tile[c], P.f[c], false, false, 128, 4))) return rc;
-    if ((rc = encode_map(p, &p->tma.h_wide[c], P.f[3 + c], false, false, 136, 5))) return rc;
-    if ((rc = encode_map(p, &p->tma.h_tile[c], P.f[3 + c], false, false, 128, 4))) return rc;
+    if ((rc = encode_map(p, &m.e_wide[c], P.f[c], false, false, 136, 5))) return rc;
+    if ((rc = encode_map(p, &m.e_tile[c], P.f[c], false, false, 128, 4))) return rc;
+    if ((rc = encode_map(p, &m.h_wide[c], P.f[3 + c], false, false, 136, 5))) return rc;
+    if ((rc = encode_map(p, &m.h_tile[c], P.f[3 + c], false, false, 128, 4))) return rc;
   }
-  if (P.mat16) return encode_map(p, &p->tma.m_tile, P.mat16, true, false, 128, 4);
-  return encode_map(p, &p->tma.m_tile, P.mat32, false, true, 128, 4);
+  if (P.mat16) return encode_map(p, &m.m_tile, P.mat16, true, false, 128, 4);
+  return encode_map(p, &m.m_tile, P.mat32, false, true, 128, 4);
 }
+
+int make_tma_maps(oem_plan* p) { return make_tma_maps_of(p, p->tma, p->yp); }
+
 
 // Tensor maps of the fused kernel reading bank b.
 static int make_fused_maps(oem_plan* p, int b) {
@@ -1409,7 +1442,27 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
     for (int c = 0; c < 6; ++c)
       if ((rc = dalloc(p, &P.fi[c], ncp))) return rc;
     P.cplx = 1;
-    p->basic_kernels = 1;  // the complex update kernels; no pipelined variant
+    // Large grids split the update: the warp-specialised real kernels on each part, then the
+    // seam faces (cells whose neighbour mask has an imaginary part) add the terms of the
+    // complex product. Needs the seam axes free of CPML slabs (their derivative enters
+    // unstretched) and at most a few seam faces; otherwise the complex one-thread-per-cell
+    // kernels.
+    p->seam_h.clear();
+    p->seam_e.clear();
+    bool split = p->basic_kernels == 3;
+    for (int a = 0; a < 3 && split; ++a) {
+      const AxisHost& h = p->axh[a];
+      const int n = a == 0 ? p->nx : a == 1 ? p->ny : p->nz;
+      bool any = false;
+      for (int q = 0; q < n; ++q) {
+        if (!h.mnx_i.empty() && h.mnx_i[q] != 0.0) { p->seam_h.push_back({a, q}); any = true; }
+        if (!h.mpv_i.empty() && h.mpv_i[q] != 0.0) { p->seam_e.push_back({a, q}); any = true; }
+      }
+      if (any && (h.lo > 0 || h.hi > 0)) split = false;
+    }
+    if (p->seam_h.size() + p->seam_e.size() > 12) split = false;
+    p->cplx_ws = split;
+    p->basic_kernels = split ? 3 : 1;
   }
   for (int a = 0; a < 3; ++a)
     if ((rc = upload_axis(p, a))) return rc;
@@ -1519,9 +1572,16 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
                                   : (p->basic_kernels == 3 ? ws_xchunk(P) : tma_xchunk(P));
   if (p->basic_kernels == 0 || p->basic_kernels == 3) {
     // grids the tensor-map encoder refuses run on the register-streaming kernels
-    if (make_tma_maps(p) != OEM_OK) {
-      p->basic_kernels = 2;
-      p->xch = stream_xchunk(P);
+    if (make_tma_maps(p) != OEM_OK ||
+        (p->cplx_ws && make_tma_maps_of(p, p->tma_i, imag_part(P)) != OEM_OK)) {
+      if (p->is_complex) {
+        p->cplx_ws = false;
+        p->basic_kernels = 1;
+        p->xch = tma_xchunk(P);
+      } else {
+        p->basic_kernels = 2;
+        p->xch = stream_xchunk(P);
+      }
     } else {
       cudaError_t e = p->basic_kernels == 3 ? ws_setup_kernels() : tma_setup_kernels();
       if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute");
@@ -1779,6 +1839,7 @@ int oem_plan_launches_per_step(oem_plan* p, int* n) {
   for (const Tfsf& t : p->tfsfs) c += (int)(t.e_groups.size() + t.h_groups.size());
   c += 3 * (int)p->tensors.size();
   c += 2 * (int)p->mixes.size();
+  if (p->cplx_ws) c += 2 + (int)(p->seam_h.size() + p->seam_e.size());
   *n = c;
   return OEM_OK;
 }

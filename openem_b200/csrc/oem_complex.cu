@@ -181,6 +181,73 @@ __global__ void __launch_bounds__(128) k_update_e_c(YeeParams P) {
   }
 }
 
+// Bloch seam terms of the split complex update. Away from a Bloch seam the real and the
+// imaginary parts follow the real update with the same (real) coefficients, so the
+// warp-specialised real kernels update each part with the real part m_re of the neighbour
+// masks. At a seam face the complex product n m adds -n_im m_im to the real part and
+// +n_re m_im to the imaginary part of a forward difference (the negatives for a backward one);
+// these kernels add those terms, times the update's coefficient, to the components whose
+// derivative along the seam axis they enter (a Bloch axis carries no CPML, so the derivative
+// enters unstretched). Per axis a, the (updated component, differentiated component, sign of
+// the coefficient) pairs follow the curl of k_update_h_c / k_update_e_c.
+__device__ __forceinline__ int64_t seam_cell(const YeeParams& P, int a, int q, int t, int* c) {
+  const int u = a == 0 ? 1 : 0, v = a == 2 ? 1 : 2;
+  const int nv = v == 1 ? P.ny : P.nz;
+  c[a] = q;
+  c[u] = t / nv;
+  c[v] = t - c[u] * nv;
+  return ((int64_t)c[0] * P.ny + c[1]) * P.nzp + c[2];
+}
+
+__global__ void k_seam_h(YeeParams P, int a, int q) {
+  const int u = a == 0 ? 1 : 0, v = a == 2 ? 1 : 2;
+  const int nu = u == 0 ? P.nx : P.ny, nv = v == 1 ? P.ny : P.nz;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nu * nv) return;
+  int c[3];
+  const int64_t id = seam_cell(P, a, q, t, c);
+  const DevAxis& A = P.ax[a];
+  c[a] = A.nxt[q];
+  const int64_t nb = ((int64_t)c[0] * P.ny + c[1]) * P.nzp + c[2];
+  const float mi = A.mnx_i[q], idl = A.idl_p[q];
+  // (H component, E component, sign of ch)
+  const int tab[3][2][3] = {{{4, 2, 1}, {5, 1, -1}}, {{3, 2, -1}, {5, 0, 1}}, {{3, 1, 1}, {4, 0, -1}}};
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int h = tab[a][r][0], e = tab[a][r][1];
+    const float g = tab[a][r][2] > 0 ? P.ch : -P.ch;
+    const float ddr = __fmul_rn(__fmul_rn(-P.fi[e][nb], mi), idl);
+    const float ddi = __fmul_rn(__fmul_rn(P.f[e][nb], mi), idl);
+    P.f[h][id] = __fmaf_rn(g, ddr, P.f[h][id]);
+    P.fi[h][id] = __fmaf_rn(g, ddi, P.fi[h][id]);
+  }
+}
+
+__global__ void k_seam_e(YeeParams P, int a, int q) {
+  const int u = a == 0 ? 1 : 0, v = a == 2 ? 1 : 2;
+  const int nu = u == 0 ? P.nx : P.ny, nv = v == 1 ? P.ny : P.nz;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nu * nv) return;
+  int c[3];
+  const int64_t id = seam_cell(P, a, q, t, c);
+  const DevAxis& A = P.ax[a];
+  c[a] = A.prv[q];
+  const int64_t nb = ((int64_t)c[0] * P.ny + c[1]) * P.nzp + c[2];
+  const float mi = A.mpv_i[q], idl = A.idl_d[q];
+  const MatRec& M = P.mats[mat_of(P, id)];
+  // (E component, H component, sign of cb)
+  const int tab[3][2][3] = {{{1, 5, -1}, {2, 4, 1}}, {{0, 5, 1}, {2, 3, -1}}, {{0, 4, -1}, {1, 3, 1}}};
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int e = tab[a][r][0], h = tab[a][r][1];
+    const float g = tab[a][r][2] > 0 ? M.cb[e] : -M.cb[e];
+    const float ddr = __fmul_rn(__fmul_rn(P.fi[h][nb], mi), idl);
+    const float ddi = __fmul_rn(__fmul_rn(-P.f[h][nb], mi), idl);
+    P.f[e][id] = __fmaf_rn(g, ddr, P.f[e][id]);
+    P.fi[e][id] = __fmaf_rn(g, ddi, P.fi[e][id]);
+  }
+}
+
 // Padded index of plane cell (o1, o2) of a mode plane along `axis` (tangential pair in cyclic
 // order: axis 0 -> (y, z), 1 -> (z, x), 2 -> (x, y)).
 __device__ __forceinline__ int64_t plane_cell(const YeeParams& P, int axis, int kp, int o1,
@@ -261,6 +328,22 @@ __global__ void k_mode_e(YeeParams P, ModeSrc m, const int* step) {
 }
 
 }  // namespace
+
+cudaError_t launch_seam_h(const YeeParams& P, const SeamFace& f, cudaStream_t s) {
+  const int a = f.axis;
+  const int64_t n = (int64_t)(a == 0 ? P.ny : P.nx) * (a == 2 ? P.ny : P.nz);
+  if (n <= 0 || n >= (1LL << 31)) return cudaErrorInvalidValue;
+  k_seam_h<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, a, f.q);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_seam_e(const YeeParams& P, const SeamFace& f, cudaStream_t s) {
+  const int a = f.axis;
+  const int64_t n = (int64_t)(a == 0 ? P.ny : P.nx) * (a == 2 ? P.ny : P.nz);
+  if (n <= 0 || n >= (1LL << 31)) return cudaErrorInvalidValue;
+  k_seam_e<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, a, f.q);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_update_h_c(const YeeParams& P, cudaStream_t s) {
   dim3 b(32, 4, 1), g((P.nzp + 31) / 32, (P.ny + 3) / 4, P.nx);

@@ -271,6 +271,14 @@ struct MixSet {
   float* dh = nullptr;
 };
 
+// One face of Bloch seam cells of the split complex update: the cells whose index along
+// `axis` is q, where the forward (H side) or backward (E side) neighbour mask has an
+// imaginary part.
+struct SeamFace {
+  int axis = 0;
+  int q = 0;
+};
+
 struct TimeMon {
   int nc = 0;
   int comps[6] = {0, 0, 0, 0, 0, 0};
@@ -333,6 +341,11 @@ struct oem_plan {
   std::vector<oem::Tfsf> tfsfs;
   std::vector<oem::TensorSet> tensors;
   std::vector<oem::MixSet> mixes;
+  // complex plans on large grids: the warp-specialised real kernels update the real and the
+  // imaginary parts (tma / tma_i), the seam faces add the imaginary-mask terms
+  bool cplx_ws = false;
+  oem::TmaMaps tma_i{};
+  std::vector<oem::SeamFace> seam_h, seam_e;
   double2* rd_scratch[2] = {nullptr, nullptr};  // readout interleave buffers (lazy)
   int64_t rd_chunk = 0;
 
@@ -429,6 +442,7 @@ cudaError_t launch_update_h_tma(const TmaMaps& maps, const YeeParams& P, int xch
 cudaError_t launch_update_e_tma(const TmaMaps& maps, const YeeParams& P, int xch, int n_mats,
                                 int* err, cudaStream_t s);
 int make_tma_maps(oem_plan* p);
+int make_tma_maps_of(oem_plan* p, TmaMaps& m, const YeeParams& P);
 cudaError_t launch_pad_index(const void* in, int in_bytes, uint16_t* out16, uint32_t* out32,
                              int nx, int ny, int nz, int nzp, uint32_t n_mat, unsigned* bad,
                              cudaStream_t s);
@@ -447,6 +461,8 @@ cudaError_t launch_ade_segments(const YeeParams& P, const int64_t* segs, int64_t
                                 int64_t nseg, int max_blocks, cudaStream_t s);
 cudaError_t launch_update_h_c(const YeeParams& P, cudaStream_t s);
 cudaError_t launch_update_e_c(const YeeParams& P, cudaStream_t s);
+cudaError_t launch_seam_h(const YeeParams& P, const SeamFace& f, cudaStream_t s);
+cudaError_t launch_seam_e(const YeeParams& P, const SeamFace& f, cudaStream_t s);
 cudaError_t launch_absorb(const YeeParams& P, const Absorber& a, int is_e, cudaStream_t s);
 cudaError_t launch_modulate(const YeeParams& P, const Modulation& m, const int* step,
                             cudaStream_t s);

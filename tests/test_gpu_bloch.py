@@ -67,8 +67,13 @@ def test_bloch_time_samples_match_oracle(bloch_runs):
         assert rel_l2(g.time_samples[name], data) < 1e-5, name
 
 
-def test_bloch_dipole_matches_oracle():
-    """A z dipole in the Bloch cell (no mode source): complex analytic amplitude injection."""
+@pytest.mark.parametrize("kind", [None, "ws"])
+def test_bloch_dipole_matches_oracle(monkeypatch, kind):
+    """A z dipole in the Bloch cell (no mode source): complex analytic amplitude injection, on
+    the complex one-thread-per-cell kernels and on the split update (the warp-specialised real
+    kernels on each part plus the seam terms)."""
+    if kind:
+        monkeypatch.setenv("OEM_B200_KERNELS", kind)
     sc = small_bloch(num_steps=250, k=(0.12, 0.0, 0.0))
     idx, coef = scenes.dipole_stencil(sc.grid, 2, (0.5 * 16 * 0.01e-6, 0.5 * 8 * 0.01e-6, 0.0))
     from openem_b200.model import GaussianPulse, sample_waveform
@@ -94,9 +99,13 @@ def test_gaussian_beam_real_path_matches_oracle():
     assert rel_l2(g.phasors["T"].data, r.phasors["T"]) < 1e-4
 
 
-def test_complex_at_zero_phase_is_two_real_runs():
+@pytest.mark.parametrize("kind", [None, "ws"])
+def test_complex_at_zero_phase_is_two_real_runs(monkeypatch, kind):
     """force_complex at k = 0: the real part is the real run driven by amp, the imaginary part
-    the real run driven by -i amp (Im(p a) = Re(p a (-i))), bit for bit."""
+    the real run driven by -i amp (Im(p a) = Re(p a (-i))), bit for bit, on both complex
+    update paths."""
+    if kind:
+        monkeypatch.setenv("OEM_B200_KERNELS", kind)
     sc = scenes.beam_slab(nx=24, ny=24, nz=36, n_pml=6, design=(6, 6), waist=0.15e-6,
                           slab_cells=4, num_steps=160)
     c = solver.run(sc, use_shutoff=False, return_fields=True, verbose=False, force_complex=True)
@@ -110,3 +119,32 @@ def test_complex_at_zero_phase_is_two_real_runs():
     np.testing.assert_allclose(c.phasors["T"].data,
                                a.phasors["T"].data + 1j * b.phasors["T"].data,
                                rtol=1e-6, atol=1e-12 * np.abs(c.phasors["T"].data).max())
+
+
+def test_split_complex_update_matches_oracle(bloch_runs, monkeypatch):
+    """The mode-source Bloch cell on the split complex update: fields, flux and field phasors
+    and time samples against the FP64 oracle with the bounds of the complex kernels."""
+    monkeypatch.setenv("OEM_B200_KERNELS", "ws")
+    r = bloch_runs["ref"]
+    g = solver.run(bloch_runs["sc"], use_shutoff=False, return_fields=True, verbose=False)
+    assert family_err(g.fields, r.fields, E3) < 1e-5
+    assert family_err(g.fields, r.fields, H3) < 1e-5
+    assert rel_l2(g.phasors["T"].data, r.phasors["T"]) < 1e-4
+    for name, data in r.time_samples.items():
+        assert rel_l2(g.time_samples[name], data) < 1e-5, name
+
+
+def test_split_complex_update_launches():
+    """The split update runs the real kernels twice per family plus one seam face per side."""
+    sc = small_bloch(num_steps=20, k=(0.12, 0.0, 0.0))
+    counts = {}
+    for kind in ("basic", "ws"):
+        import os
+        os.environ["OEM_B200_KERNELS"] = kind
+        try:
+            plan = solver.Plan(sc, 20, cplx=True)
+            counts[kind] = plan.launches_per_step()
+            plan.close()
+        finally:
+            del os.environ["OEM_B200_KERNELS"]
+    assert counts["ws"] - counts["basic"] == 4
