@@ -492,6 +492,8 @@ def check_csr(name: str, shape, comp, cell, ofs_list) -> np.ndarray:
         if np.any(np.diff(ofs) < 0):
             raise ValueError(f"{name}.{oname} is not monotonic")
     key = comp.astype(np.int64) * ncell + cell.astype(np.int64)
+    if n < 2 or bool(np.all(key[1:] > key[:-1])):  # tables ordered by (comp, cell): unique
+        return key
     seen = np.zeros(3 * ncell, dtype=bool)
     seen[key] = True
     nu = int(np.count_nonzero(seen))

@@ -298,7 +298,7 @@ def tensor_tables(sc, tabs) -> dict | None:
             "m1": f32(m1), "m2": f32(m2), "pec": f32(pf)}
 
 
-def entry_pole_sets(sc):
+def entry_pole_sets(sc, bulk_shortcut: bool = True):
     """Deduplicate ADE entries by their float32 coefficient lists.
 
     Returns ``(comp, cell, set_id, set_ofs, coef, counts)``: per entry its component, flat cell
@@ -316,6 +316,19 @@ def entry_pole_sets(sc):
         raise NotImplementedError("more than 15 poles on one component")
     am1 = np.asarray(d.am1, dtype=np.complex128)
     b = np.asarray(d.b, dtype=np.complex128)
+    k0 = int(npole[0])
+    if bulk_shortcut and k0 > 0 and np.all(npole == k0) and \
+            np.all(ofs[:-1] == np.arange(d.n_entry) * k0):
+        # every entry carries the same coefficient list (a bulk medium): one set, found without
+        # converting every pole (equal float64 values give equal float32 rows; anything else
+        # takes the general path below)
+        A = am1.reshape(d.n_entry, k0)
+        B = b.reshape(d.n_entry, k0)
+        if np.all(A == A[0]) and np.all(B == B[0]):
+            row = np.empty((k0, 4), dtype=np.float32)
+            row[:, 0], row[:, 1], row[:, 2], row[:, 3] = A[0].real, A[0].imag, B[0].real, B[0].imag
+            return (comp, cell, np.zeros(d.n_entry, dtype=np.int64),
+                    np.asarray([0, k0], dtype=np.int32), row, np.asarray([k0], dtype=np.int32))
     pc = np.empty((am1.size, 4), dtype=np.float32)
     pc[:, 0], pc[:, 1], pc[:, 2], pc[:, 3] = am1.real, am1.imag, b.real, b.imag
     set_id = np.full(d.n_entry, -1, dtype=np.int64)

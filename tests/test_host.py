@@ -279,3 +279,18 @@ def test_library_builds_loads_and_exports_header_symbols():
         assert hasattr(so, name), name
     assert set(lib.SIGNATURES) == declared
     assert lib.load().oem_version() >= 100
+
+
+def test_bulk_pole_set_shortcut_is_exact():
+    """One coefficient list on every entry takes a shortcut that converts one row; its output
+    equals the general deduplication's, and a single differing entry leaves the shortcut."""
+    from dataclasses import replace
+    from openem_b200 import tables as T
+    sd = scenes.small_dispersive(n=24, n_sph=2, n_pml=4, num_steps=10)
+    for sc in (sd, replace(sd, dispersion=replace(sd.dispersion, b=np.concatenate(
+            [sd.dispersion.b[:-1], sd.dispersion.b[-1:] * 1.5])))):
+        a = T.entry_pole_sets(sc)
+        b = T.entry_pole_sets(sc, bulk_shortcut=False)
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+    assert T.entry_pole_sets(sd)[3].size == 2
