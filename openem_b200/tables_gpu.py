@@ -52,18 +52,22 @@ def _to_dev(a, torch, dev, dtype=None):
 
 class _Uploads:
     """The float64 eps and sigma arrays of each component copied to the device on a worker
-    thread, one component ahead of the caller: the first overlaps the host-side pole-set
-    deduplication, each later one the key building of the previous component, and at most two
-    components are resident at a time. The copies are synchronous on the worker's stream; the
-    caller's stream is recorded on each tensor before use."""
+    thread while the caller deduplicates the pole sets and builds the keys: all three
+    components queued back to back when the six arrays take under a quarter of the free device
+    memory, otherwise one component ahead of the caller (at most two resident). The copies run
+    one at a time (pageable copies from several threads were slower) and are synchronous on the
+    worker's stream; the caller's stream is recorded on each tensor before use."""
 
     def __init__(self, sc, torch, dev):
         from concurrent.futures import ThreadPoolExecutor
         self.torch, self.dev = torch, dev
         self.eps = (sc.eps_ex, sc.eps_ey, sc.eps_ez)
         self.sig = (sc.sigma_ex, sc.sigma_ey, sc.sigma_ez)
+        nbytes = sum(np.asarray(a).size * 8 for a in (*self.eps, *self.sig) if a is not None)
+        free, _ = torch.cuda.mem_get_info(dev)
+        self.depth = 3 if nbytes < free // 4 else 1
         self.pool = ThreadPoolExecutor(max_workers=1)
-        self.futs = [self.pool.submit(self._load, 0)]
+        self.futs = [self.pool.submit(self._load, c) for c in range(self.depth)]
 
     def _load(self, c):
         torch, dev = self.torch, self.dev
@@ -74,8 +78,8 @@ class _Uploads:
         return eps, sig
 
     def get(self, c):
-        if c + 1 < 3:
-            self.futs.append(self.pool.submit(self._load, c + 1))
+        if c + self.depth < 3:
+            self.futs.append(self.pool.submit(self._load, c + self.depth))
         eps, sig = self.futs[c].result()
         self.futs[c] = None
         cur = self.torch.cuda.current_stream(self.dev)
