@@ -294,3 +294,37 @@ def test_bulk_pole_set_shortcut_is_exact():
         for x, y in zip(a, b):
             np.testing.assert_array_equal(x, y)
     assert T.entry_pole_sets(sd)[3].size == 2
+
+
+def test_ours_npz_round_trip(tmp_path, monkeypatch):
+    """The solve worker's ``ours.npz`` keys and contents (openem/nb/solve_worker.py:25-45): flux
+    phasors and frequencies, field phasors, time samples, flux time series and the run summary
+    round-trip; an output above the size cap leaves only the summary; a work directory asking
+    for the Tidy3D-convention readout is refused."""
+    from openem_b200 import results, solve_worker
+    rng = np.random.default_rng(0)
+    ph = rng.normal(size=(4, 3, 5, 6)) + 1j * rng.normal(size=(4, 3, 5, 6))
+    res = results.Result(
+        phasors={"T": results.Phasors(name="T", data=ph, freqs=np.array([1.0, 2.0, 3.0]))},
+        steps_run=123, shutoff_triggered=True, stop_reason="field decay", wall_seconds=1.5,
+        source_end=40, energy_trace=[(400, 1e-3)],
+        field_phasors={"box": rng.normal(size=(6, 2, 3, 3, 3)) + 0j},
+        time_samples={"tm": rng.normal(size=(6, 4, 2, 2, 2)).astype(np.float32)},
+        flux_time={"ft": rng.normal(size=7)})
+    mb = solve_worker.save_result(res, tmp_path / "ours.npz")
+    assert mb > 0
+    z = np.load(tmp_path / "ours.npz")
+    assert set(z.files) == {"__meta", "mon:T", "monf:T", "fld:box", "tim:tm", "ftm:ft"}
+    back = solve_worker.load_result(tmp_path / "ours.npz")
+    np.testing.assert_array_equal(back["phasors"]["T"][0], ph)
+    np.testing.assert_array_equal(back["field_phasors"]["box"], res.field_phasors["box"])
+    np.testing.assert_array_equal(back["time_samples"]["tm"], res.time_samples["tm"])
+    np.testing.assert_array_equal(back["flux_time"]["ft"], res.flux_time["ft"])
+    assert back["meta"] == {"steps_run": 123, "triggered": True, "stop": "field decay",
+                            "wall": 1.5, "source_end": 40, "energy_trace": [[400, 1e-3]]}
+    monkeypatch.setenv("OPENEM_OUT_MAX_GB", "1e-9")
+    assert solve_worker.save_result(res, tmp_path / "big.npz") < 0
+    assert (tmp_path / "big.TOOBIG").exists() and not (tmp_path / "big.npz").exists()
+    (tmp_path / "td_coords.npz").write_bytes(b"")
+    with pytest.raises(NotImplementedError):
+        solve_worker.solve_dir(tmp_path, tmp_path / "out")
