@@ -8,6 +8,7 @@
 // component; J of component c of a cell is written at the cell's first pole of component c.
 // The arithmetic and the summation order are those of the inline ADE of the other E kernels
 // (oem_arith.cuh), so every kernel variant produces the same bits.
+#include <algorithm>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -35,29 +36,28 @@ __global__ void k_list_pole_segments(const uint32_t* seg, int64_t nseg, uint32_t
 constexpr int kSegPoles = 256;  // pole states of one segment staged per warp
 
 // The pole update of one cell on states held in `st` (shared or global memory), J written to
-// the cell's first pole of each component.
+// the cell's first pole of each component; `en` holds the cell's E^n.
 __device__ __forceinline__ void ade_cell_poles(const YeeParams& P, const MatRec& M, float2* st,
-                                               uint32_t gp, int64_t cell) {
+                                               uint32_t gp, const float (&en)[3]) {
   int po = 0;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const int n = M.np[c];
     if (n == 0) continue;
-    const float en = P.f[c][cell];
     const float4* cf = P.pcoef + P.pset_ofs[M.pset[c]];
     float acc = 0.f;
     int tt = 0;
     for (; tt + 1 < n; tt += 2) {
       float2 s0 = st[po + tt], s1 = st[po + tt + 1];
-      const float d0 = ade_pole(s0, __ldg(cf + tt), en);
-      const float d1 = ade_pole(s1, __ldg(cf + tt + 1), en);
+      const float d0 = ade_pole(s0, __ldg(cf + tt), en[c]);
+      const float d1 = ade_pole(s1, __ldg(cf + tt + 1), en[c]);
       st[po + tt] = s0;
       st[po + tt + 1] = s1;
       acc = __fadd_rn(__fadd_rn(acc, d0), d1);
     }
     if (tt < n) {
       float2 s0 = st[po + tt];
-      acc = __fadd_rn(acc, ade_pole(s0, __ldg(cf + tt), en));
+      acc = __fadd_rn(acc, ade_pole(s0, __ldg(cf + tt), en[c]));
       st[po + tt] = s0;
     }
     P.J[gp + (uint32_t)po] = acc;
@@ -65,43 +65,75 @@ __device__ __forceinline__ void ade_cell_poles(const YeeParams& P, const MatRec&
   }
 }
 
+// What a segment needs before its pole states can be read: its pole range, and per lane the
+// cell's material and E^n. Loaded one segment ahead of the update.
+struct SegLoad {
+  int64_t s = -1;
+  uint32_t a = 0, b = 0, m = 0;
+  float e[3] = {0.f, 0.f, 0.f};
+};
+
+__device__ __forceinline__ SegLoad seg_load(const YeeParams& P, int64_t s, int64_t nseg,
+                                            int lane) {
+  SegLoad L;
+  if (s < 0) return L;
+  L.s = s;
+  const int64_t cell = s * 32 + lane;
+  L.a = P.seg_ofs[s];
+  L.b = (s + 1 < nseg) ? P.seg_ofs[s + 1] : P.n_pole_total;
+  L.m = P.mat16 ? (uint32_t)P.mat16[cell] : P.mat32[cell];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) L.e[c] = P.f[c][cell];
+  return L;
+}
+
 // One segment on one warp: its poles (contiguous in memory) are read into shared memory with
 // coalesced loads, updated there cell by cell, and written back coalesced; a segment with more
 // poles than the buffer holds is updated in place in global memory.
-__device__ __forceinline__ void ade_segment(const YeeParams& P, int64_t s, int64_t nseg,
-                                            float2* st, int lane) {
-  const int64_t cell = s * 32 + lane;
-  const uint32_t a = P.seg_ofs[s];
-  const uint32_t b = (s + 1 < nseg) ? P.seg_ofs[s + 1] : P.n_pole_total;
-  const int n = (int)(b - a);
-  const uint32_t m = P.mat16 ? (uint32_t)P.mat16[cell] : P.mat32[cell];
-  const MatRec& M = P.mats[m];
+__device__ __forceinline__ void ade_segment(const YeeParams& P, const SegLoad& L, float2* st,
+                                            int lane) {
+  const int n = (int)(L.b - L.a);
+  const MatRec& M = P.mats[L.m];
   const int npc = M.reserved;
   const unsigned lt = (1u << lane) - 1u;
   int pre = 0;
 #pragma unroll
   for (int bb = 0; bb < 6; ++bb) pre += __popc(__ballot_sync(kFull, (npc >> bb) & 1) & lt) << bb;
   if (n <= kSegPoles) {
-    for (int t = lane; t < n; t += 32) st[t] = P.P[a + t];
+    for (int t = lane; t < n; t += 32) st[t] = P.P[L.a + t];
     __syncwarp();
-    if (npc > 0) ade_cell_poles(P, M, st + pre, a + (uint32_t)pre, cell);
+    if (npc > 0) ade_cell_poles(P, M, st + pre, L.a + (uint32_t)pre, L.e);
     __syncwarp();
-    for (int t = lane; t < n; t += 32) P.P[a + t] = st[t];
+    for (int t = lane; t < n; t += 32) P.P[L.a + t] = st[t];
     __syncwarp();
   } else if (npc > 0) {
-    ade_cell_poles(P, M, P.P + a + pre, a + (uint32_t)pre, cell);
+    ade_cell_poles(P, M, P.P + L.a + pre, L.a + (uint32_t)pre, L.e);
   }
 }
 
-// One warp per listed segment (a grid-stride loop when the grid is capped). In the captured
-// step it runs on its own graph branch beside the H update.
+// Warps stride over the listed segments (the grid is about one resident wave): while a warp
+// updates segment q it has already loaded the pole range, materials and E^n of its next
+// segment and the index of the one after, so each segment waits on one dependent load (its
+// pole states) instead of three. In the captured step it runs on its own graph branch beside
+// the H update.
 __global__ void __launch_bounds__(256) k_ade_segments(YeeParams P, const int64_t* segs,
                                                       int64_t nsegs, int64_t nseg) {
   __shared__ float2 buf[8][kSegPoles];
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
-  for (int64_t q = (int64_t)blockIdx.x * 8 + w; q < nsegs; q += (int64_t)gridDim.x * 8)
-    ade_segment(P, segs[q], nseg, buf[w], lane);
+  const int64_t stride = (int64_t)gridDim.x * 8;
+  int64_t q = (int64_t)blockIdx.x * 8 + w;
+  SegLoad cur = seg_load(P, q < nsegs ? segs[q] : -1, nseg, lane);
+  int64_t s2 = q + stride < nsegs ? segs[q + stride] : -1;
+  while (cur.s >= 0) {
+    const int64_t q3 = q + 2 * stride;
+    const int64_t s3 = q3 < nsegs ? segs[q3] : -1;
+    const SegLoad nxt = seg_load(P, s2, nseg, lane);
+    ade_segment(P, cur, buf[w], lane);
+    cur = nxt;
+    s2 = s3;
+    q += stride;
+  }
 }
 
 }  // namespace
@@ -117,7 +149,8 @@ cudaError_t launch_list_pole_segments(const YeeParams& P, int64_t nseg, int64_t*
 cudaError_t launch_ade_segments(const YeeParams& P, const int64_t* segs, int64_t nsegs,
                                 int64_t nseg, int max_blocks, cudaStream_t s) {
   if (nsegs <= 0) return cudaSuccess;
-  int64_t blocks = (nsegs + 7) / 8;
+  // about one resident wave (5 blocks of 8 warps per SM); each warp strides over the list
+  int64_t blocks = std::min<int64_t>((nsegs + 7) / 8, 148 * 5);
   if (max_blocks > 0 && blocks > max_blocks) blocks = max_blocks;
   k_ade_segments<<<(unsigned)blocks, 256, 0, s>>>(P, segs, nsegs, nseg);
   return cudaGetLastError();
