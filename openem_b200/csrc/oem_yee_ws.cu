@@ -690,15 +690,17 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
         mid[0] = m.x & 0xffffu; mid[1] = m.x >> 16; mid[2] = m.y & 0xffffu; mid[3] = m.y >> 16;
       }
     }
+    // a row whose segments hold no poles (window offset -2) skips the pole bookkeeping
+    const bool row_poles = P.has_ade && tab[2 * w + 1] != -2;
     int lane_np = 0;
-    if (P.has_ade) {
+    if (row_poles) {
 #pragma unroll
       for (int e = 0; e < 4; ++e) lane_np += mats[mid[e]].reserved;
     }
     // poles of this lane: global index gp, window index wp (-1: read J from global memory)
     uint32_t gp = 0;
     int wp = -1;
-    if (P.has_ade && __any_sync(kFull, lane_np > 0)) {
+    if (row_poles && __any_sync(kFull, lane_np > 0)) {
       int pre = 0;
 #pragma unroll
       for (int b = 0; b < 8; ++b) pre += __popc(__ballot_sync(kFull, (lane_np >> b) & 1) & lt) << b;
