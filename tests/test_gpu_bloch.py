@@ -67,14 +67,15 @@ def test_bloch_time_samples_match_oracle(bloch_runs):
         assert rel_l2(g.time_samples[name], data) < 1e-5, name
 
 
+@pytest.mark.parametrize("k", [(0.12, 0.0, 0.0), (0.05, 0.03, 0.0)])
 @pytest.mark.parametrize("kind", [None, "ws"])
-def test_bloch_dipole_matches_oracle(monkeypatch, kind):
+def test_bloch_dipole_matches_oracle(monkeypatch, kind, k):
     """A z dipole in the Bloch cell (no mode source): complex analytic amplitude injection, on
     the complex one-thread-per-cell kernels and on the split update (the warp-specialised real
-    kernels on each part plus the seam terms)."""
+    kernels on each part plus the seam terms), with a Bloch phase on x and on x and y."""
     if kind:
         monkeypatch.setenv("OEM_B200_KERNELS", kind)
-    sc = small_bloch(num_steps=250, k=(0.12, 0.0, 0.0))
+    sc = small_bloch(num_steps=250, k=k)
     idx, coef = scenes.dipole_stencil(sc.grid, 2, (0.5 * 16 * 0.01e-6, 0.5 * 8 * 0.01e-6, 0.0))
     from openem_b200.model import GaussianPulse, sample_waveform
     wf = sample_waveform(GaussianPulse(freq0=3e14, fwidth=0.9e14), sc.dt, 250)
