@@ -134,6 +134,12 @@ __device__ __forceinline__ float gather_bwd(const YeeParams& P, const float* db,
   const DevAxis& A = P.ax[a];
   const int q = a == 0 ? i : (a == 1 ? j : k);
   float v = A.idl_d[q] * db[moved(P, a, i, j, k, q)];
+  // away from both ends the neighbour tables are q -+ 1 (wraps and clamps sit at the ends):
+  // exactly one cell, q + 1, names q as its backward neighbour
+  if (q > 0 && q < A.n - 1) {
+    v -= A.mpv[q + 1] * A.idl_d[q + 1] * db[moved(P, a, i, j, k, q + 1)];
+    return v;
+  }
   int cand[5];
   const int nc = neighbour_candidates(A, q, cand);
   for (int t = 0; t < nc; ++t) {
@@ -151,6 +157,11 @@ __device__ __forceinline__ float gather_fwd(const YeeParams& P, const float* db,
   const DevAxis& A = P.ax[a];
   const int q = a == 0 ? i : (a == 1 ? j : k);
   float v = -A.idl_p[q] * db[moved(P, a, i, j, k, q)];
+  // away from both ends exactly one cell, q - 1, names q as its forward neighbour
+  if (q > 0 && q < A.n - 1) {
+    v += A.mnx[q - 1] * A.idl_p[q - 1] * db[moved(P, a, i, j, k, q - 1)];
+    return v;
+  }
   int cand[5];
   const int nc = neighbour_candidates(A, q, cand);
   for (int t = 0; t < nc; ++t) {
