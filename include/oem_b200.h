@@ -137,6 +137,15 @@ int oem_plan_add_mode_source(oem_plan* p, int axis, int kh, int ks, int n1, int 
  * serving autotuner per grid-size class before oem_plan_finalize. */
 int oem_plan_set_xchunk(oem_plan* p, int xch);
 
+/* Declare, before oem_plan_finalize, the box (i0, j0, k0, ni, nj, nk) a later
+ * oem_plan_adjoint_flux_box will take gradients over. With checkpoints enabled the forward run
+ * then records E of the box after every step ((steps + 1) x 3 x box floats, when that is at most
+ * 8 GB and a quarter of the free memory), and the reverse pass over the same box reads it instead
+ * of recomputing each segment from its checkpoint (the reference recomputes nothing: its
+ * gradients come from a second solve, openem/nb/autograd_hook.py:184-221). The environment
+ * variable OEM_B200_ADJ_HISTORY=0 keeps the recompute. */
+int oem_plan_set_gradient_box(oem_plan* p, const int* box);
+
 /* Discrete adjoint of a flux objective (the reference computes gradients with forward and
  * adjoint solves through tidy3d's VJP, openem/nb/autograd_hook.py:184-221; this engine adds a
  * time-reversed discrete adjoint with K-step checkpoints). oem_plan_enable_checkpoints (before

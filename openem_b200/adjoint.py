@@ -108,7 +108,9 @@ def flux_gradient(sc, monitor: str | None = None, weights=None, num_steps: int |
     box = tuple(int(v) for v in (box if box is not None else (0, 0, 0) + tuple(sc.shape)))
     n = int(sc.num_time_steps if num_steps is None else num_steps)
     K = int(checkpoint_every or default_interval(n))
-    plan = Plan(sc, n, device=device, stream=stream, checkpoint_every=K)
+    # the box is declared before the run: the forward pass records its E every step and the
+    # reverse pass reads that instead of recomputing the segments
+    plan = Plan(sc, n, device=device, stream=stream, checkpoint_every=K, gradient_box=box)
     try:
         plan.run(n)
         plan.flush()

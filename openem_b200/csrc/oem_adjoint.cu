@@ -285,6 +285,33 @@ cudaError_t launch_adj_step(const YeeParams& P, const AdjState& S, const float* 
   return cudaGetLastError();
 }
 
+// E of the gradient box after the step the counter names (row step + 1 of the history), inside
+// the step graph of the forward run.
+__global__ void k_hist_snap(YeeParams P, int b0, int b1, int b2, int n0, int n1, int n2,
+                            float* hist, const int* step, int64_t n_total) {
+  const int64_t row = (int64_t)(*step) + 1;
+  if (row > n_total) return;
+  const int64_t nb = (int64_t)n0 * n1 * n2;
+  float* dst = hist + row * 3 * nb;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = t / ((int64_t)n1 * n2), r = t - a * n1 * n2;
+    const int64_t b = r / n2, c = r - b * n2;
+    const int64_t id = ((b0 + a) * P.ny + (b1 + b)) * P.nzp + (b2 + c);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) dst[q * nb + t] = P.f[q][id];
+  }
+}
+
+cudaError_t launch_hist_snap(const YeeParams& P, const int* box, float* hist, const int* step,
+                             int64_t n_total, cudaStream_t s) {
+  const int64_t nb = (int64_t)box[3] * box[4] * box[5];
+  const int blocks = (int)std::min<int64_t>((nb + 255) / 256, 148 * 8);
+  k_hist_snap<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(P, box[0], box[1], box[2], box[3], box[4],
+                                                      box[5], hist, step, n_total);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_adj_snap(const YeeParams& P, const AdjState& S, float* dst, cudaStream_t s) {
   const int64_t nb = (int64_t)S.box[3] * S.box[4] * S.box[5];
   const int blocks = (int)std::min<int64_t>((nb + 255) / 256, 148 * 8);

@@ -418,6 +418,9 @@ static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors) {
     if ((e = launch_snapshot(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "snapshot");
     if ((e = launch_flush(m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "flush");
   }
+  if (p->hist && (e = launch_hist_snap(P, p->gbox, p->hist, p->d_step, p->n_total, s)) !=
+                     cudaSuccess)
+    return cuda_error(e, "gradient box history");
   if ((e = launch_step_advance(p->d_step, s)) != cudaSuccess) return cuda_error(e, "step");
   return OEM_OK;
 }
@@ -843,6 +846,17 @@ int oem_plan_set_xchunk(oem_plan* p, int xch) {
   return OEM_OK;
 }
 
+int oem_plan_set_gradient_box(oem_plan* p, const int* box) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (!box || box[3] < 1 || box[4] < 1 || box[5] < 1 || box[0] < 0 || box[1] < 0 ||
+      box[2] < 0 || box[0] + box[3] > p->nx || box[1] + box[4] > p->ny || box[2] + box[5] > p->nz)
+    return set_error(OEM_ERR_INVALID, "gradient box outside the grid");
+  for (int q = 0; q < 6; ++q) p->gbox[q] = box[q];
+  p->gbox_set = true;
+  return OEM_OK;
+}
+
 int oem_plan_enable_checkpoints(oem_plan* p, int k) {
   int rc = check_plan(p, false);
   if (rc) return rc;
@@ -949,8 +963,12 @@ int oem_plan_adjoint_flux_box(oem_plan* p, int mon_id, const double* weights, co
         if (!rc) rc = alloc(&S.lpsie.p[a][slot][side], cnt);
       }
     }
+  // E of the box at every step: recorded during the forward run when this box was declared
+  // before it, else recomputed segment by segment from the checkpoints
+  bool use_hist = p->hist != nullptr;
+  for (int q = 0; q < 6; ++q) use_hist = use_hist && p->gbox[q] == box[q];
   if (!rc) rc = alloc(&dcoef, coef.size());
-  if (!rc) rc = alloc(&seg, (size_t)(K + 1) * 3 * nb);
+  if (!rc && !use_hist) rc = alloc(&seg, (size_t)(K + 1) * 3 * nb);
   if (rc) {
     release();
     return rc;
@@ -966,16 +984,19 @@ int oem_plan_adjoint_flux_box(oem_plan* p, int mon_id, const double* weights, co
   cudaError_t e = cudaSuccess;
   for (int64_t sg = nseg - 1; sg >= 0 && !rc; --sg) {
     const int64_t n0 = sg * K, n1 = std::min<int64_t>(N, n0 + K);
-    // recompute the segment from its checkpoint, keeping E of the box at every step
-    if ((rc = load_state(p, (int)sg, s))) break;
-    for (int64_t t = 0; t <= n1 - n0 && !rc; ++t) {
-      if (t > 0) rc = enqueue_step(p, s, false);
-      if (!rc && (e = launch_adj_snap(P, S, seg + (size_t)t * 3 * nb, s)) != cudaSuccess)
-        rc = cuda_error(e, "segment copy");
+    if (!use_hist) {
+      // recompute the segment from its checkpoint, keeping E of the box at every step
+      if ((rc = load_state(p, (int)sg, s))) break;
+      for (int64_t t = 0; t <= n1 - n0 && !rc; ++t) {
+        if (t > 0) rc = enqueue_step(p, s, false);
+        if (!rc && (e = launch_adj_snap(P, S, seg + (size_t)t * 3 * nb, s)) != cudaSuccess)
+          rc = cuda_error(e, "segment copy");
+      }
     }
     for (int64_t n = n1 - 1; n >= n0 && !rc; --n) {
-      const float* en = seg + (size_t)(n - n0) * 3 * nb;
-      const float* en1 = seg + (size_t)(n - n0 + 1) * 3 * nb;
+      const float* en = use_hist ? p->hist + (size_t)n * 3 * nb : seg + (size_t)(n - n0) * 3 * nb;
+      const float* en1 =
+          use_hist ? p->hist + (size_t)(n + 1) * 3 * nb : seg + (size_t)(n - n0 + 1) * 3 * nb;
       if ((e = launch_adj_src(P, af, S, (int)n, s)) != cudaSuccess) rc = cuda_error(e, "adj_src");
       if (!rc && (e = launch_adj_step(P, S, en, en1, s)) != cudaSuccess)
         rc = cuda_error(e, "adj_step");
@@ -1567,6 +1588,17 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
     P.has_ade = 1;
   }
   if ((rc = dalloc(p, &p->d_step, 1))) return rc;
+  if (p->gbox_set && p->ckpt_k > 0 && !p->is_complex) {
+    // the box history replaces the reverse pass's forward recompute when it fits: at most
+    // 8 GB and a quarter of the free memory
+    const char* hv = getenv("OEM_B200_ADJ_HISTORY");
+    const size_t nbx = (size_t)p->gbox[3] * p->gbox[4] * p->gbox[5];
+    const size_t bytes = ((size_t)n_total + 1) * 3 * nbx * sizeof(float);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { cudaGetLastError(); free_b = 0; }
+    if (!(hv && strcmp(hv, "0") == 0) && bytes <= ((size_t)8 << 30) && bytes <= free_b / 4)
+      if ((rc = dalloc(p, &p->hist, ((size_t)n_total + 1) * 3 * nbx))) return rc;
+  }
   if ((rc = dalloc(p, &p->d_err, 1))) return rc;
   p->xch = p->basic_kernels == 2 ? stream_xchunk(P)
                                   : (p->basic_kernels == 3 ? ws_xchunk(P) : tma_xchunk(P));
@@ -1840,6 +1872,7 @@ int oem_plan_launches_per_step(oem_plan* p, int* n) {
   c += 3 * (int)p->tensors.size();
   c += 2 * (int)p->mixes.size();
   if (p->cplx_ws) c += 2 + (int)(p->seam_h.size() + p->seam_e.size());
+  if (p->hist) c += 1;
   *n = c;
   return OEM_OK;
 }

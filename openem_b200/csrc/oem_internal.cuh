@@ -331,6 +331,11 @@ struct oem_plan {
   std::vector<std::vector<int64_t>> mod_cells;  // unpadded cells of each, kept until finalize
   // checkpoints of the state every ckpt_k steps (discrete adjoint): fields and CPML psi
   int ckpt_k = 0;
+  // gradient box declared before the run: E of its cells after every step (step-major, the
+  // three components, (steps + 1) rows), so the reverse pass needs no forward recompute
+  int gbox[6] = {0, 0, 0, 0, 0, 0};
+  bool gbox_set = false;
+  float* hist = nullptr;
   std::vector<float*> ckpt;        // one buffer per checkpoint, ckpt_floats floats each
   size_t ckpt_floats = 0;
   std::vector<int64_t> ckpt_step;  // step held by each buffer (-1: empty)
@@ -499,6 +504,8 @@ cudaError_t launch_adj_src(const YeeParams& P, const AdjFlux& a, const AdjState&
                            cudaStream_t s);
 cudaError_t launch_adj_step(const YeeParams& P, const AdjState& S, const float* en_box,
                             const float* en1_box, cudaStream_t s);
+cudaError_t launch_hist_snap(const YeeParams& P, const int* box, float* hist, const int* step,
+                             int64_t n_total, cudaStream_t s);
 cudaError_t launch_adj_snap(const YeeParams& P, const AdjState& S, float* dst, cudaStream_t s);
 cudaError_t launch_mode_h(const YeeParams& P, const ModeSrc& m, const int* step, cudaStream_t s);
 cudaError_t launch_mode_e(const YeeParams& P, const ModeSrc& m, const int* step, cudaStream_t s);

@@ -41,6 +41,7 @@ SIGNATURES = {
     "oem_plan_add_absorber": (_I, [_P, _I, _I, _I, _P, _P]),
     "oem_plan_set_xchunk": (_I, [_P, _I]),
     "oem_plan_enable_checkpoints": (_I, [_P, _I]),
+    "oem_plan_set_gradient_box": (_I, [_P, _P]),
     "oem_plan_add_tensor": (_I, [_P, _I, _P, _P, _P, _P, _P]),
     "oem_plan_add_dispersion_mix": (_I, [_P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _P, _D]),
     "oem_plan_add_tfsf": (_I, [_P, _I, _P, _I, _P, _I, _I, _P, _I, _I, _P]),

@@ -86,10 +86,12 @@ class Plan:
 
     def __init__(self, sc, n_total: int | None = None, device: int = 0, stream=None,
                  batch: int | None = None, cplx: bool = False, xchunk: int = 0,
-                 checkpoint_every: int = 0):
+                 checkpoint_every: int = 0, gradient_box=None):
         self.cplx = bool(cplx)
         self.xchunk = int(xchunk)
         self.checkpoint_every = int(checkpoint_every)
+        self.gradient_box = None if gradient_box is None else \
+            np.ascontiguousarray(gradient_box, dtype=np.int32)
         if self.cplx:
             refuse_unsupported_bloch(sc)
         else:
@@ -305,6 +307,8 @@ class Plan:
             L.check(lib.oem_plan_set_xchunk(h, self.xchunk), "set_xchunk")
         if self.checkpoint_every:
             L.check(lib.oem_plan_enable_checkpoints(h, self.checkpoint_every), "checkpoints")
+        if self.gradient_box is not None:
+            L.check(lib.oem_plan_set_gradient_box(h, L.ptr(self.gradient_box)), "gradient box")
         L.check(lib.oem_plan_finalize(h, self.n_total), "finalize")
         self._keep.clear()
 

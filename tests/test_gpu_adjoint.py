@@ -124,3 +124,16 @@ def test_c4_design_pixels_match_central_differences():
         cells = np.s_[i0 + a, j0 + b, box[2]:box[2] + box[5]]
         fd = (J(perturbed(sc, cells, (0, 1, 2), h)) - J(perturbed(sc, cells, (0, 1, 2), -h))) / (2 * h)
         assert abs(ad[q] - fd) <= 0.02 * abs(fd), (a, b, ad[q], fd)
+
+
+def test_box_history_equals_segment_recompute(monkeypatch):
+    """E of the gradient box recorded during the forward run gives the same gradient, bit for
+    bit, as recomputing every segment from its checkpoint (OEM_B200_ADJ_HISTORY=0)."""
+    sc = small_slab(num_steps=300)
+    box = (14, 15, 17, 11, 9, 7)
+    a = adjoint.flux_gradient(sc, checkpoint_every=50, box=box)
+    monkeypatch.setenv("OEM_B200_ADJ_HISTORY", "0")
+    b = adjoint.flux_gradient(sc, checkpoint_every=50, box=box)
+    assert a.value == b.value
+    np.testing.assert_array_equal(a.d_ca, b.d_ca)
+    np.testing.assert_array_equal(a.d_cb, b.d_cb)
