@@ -328,3 +328,27 @@ def test_ours_npz_round_trip(tmp_path, monkeypatch):
     (tmp_path / "td_coords.npz").write_bytes(b"")
     with pytest.raises(NotImplementedError):
         solve_worker.solve_dir(tmp_path, tmp_path / "out")
+
+
+def test_mix_tables_and_passthrough():
+    """The mixed-form tables the C-ABI receives: per entry (k1, k2, 1 - beta, 1/(k1 k2 + beta))
+    in float32, CSR pole rows (Re(A-1), Im(A-1), Re(B), Im(B)), and update coefficients that
+    pass the curl through on the mixed cells (ca = 0, cb = 1) while the E-form interior keeps its
+    own."""
+    from openem_b200 import tables as T
+    sc = scenes.mixed_sphere(n=20, n_pml=4, radius_cells=3.3, num_steps=10)
+    mm = sc.dispersion_mix
+    mx = T.mix_tables(sc)
+    k1, k2, omb, invd = mm.coefficients()
+    np.testing.assert_array_equal(mx["k"], np.stack([k1, k2, omb, invd], 1).astype(np.float32))
+    assert mx["pc"].shape == (mx["n_p"], 4) and mx["qc"].shape == (mx["n_q"], 4)
+    np.testing.assert_array_equal(mx["pc"][:, 2], np.asarray(mm.pb).real.astype(np.float32))
+    np.testing.assert_array_equal(mx["q_ofs"], np.asarray(mm.q_ofs, np.int32))
+    assert mx["dte"] == pytest.approx(sc.dt / 8.8541878128e-12)
+    tabs = [T.axis_tables(sc, a) for a in range(3)]
+    ca, cb = T.e_coefficients(sc, tabs)
+    for c in range(3):
+        cells = np.asarray(mm.cell)[np.asarray(mm.comp) == c]
+        assert np.all(ca[c].ravel()[cells] == 0.0) and np.all(cb[c].ravel()[cells] == 1.0)
+        inner = np.asarray(sc.dispersion.cell)[np.asarray(sc.dispersion.comp) == c]
+        assert np.all(cb[c].ravel()[inner] != 1.0)
