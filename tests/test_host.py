@@ -352,3 +352,26 @@ def test_mix_tables_and_passthrough():
         assert np.all(ca[c].ravel()[cells] == 0.0) and np.all(cb[c].ravel()[cells] == 1.0)
         inner = np.asarray(sc.dispersion.cell)[np.asarray(sc.dispersion.comp) == c]
         assert np.all(cb[c].ravel()[inner] != 1.0)
+
+
+def test_tensor_tables_and_passthrough():
+    """The tensor tables the C-ABI receives: per entry the float32 rows of M1 = A^-1 B and
+    M2 = (dt/eps0) A^-1 of its component and the PEC-wall factor of the two other axes; the
+    entries' update coefficients pass the curl through (ca = 0, cb = 1)."""
+    from openem_b200 import tables as T
+    sd = scenes.small_dispersive(n=20, n_sph=1, n_pml=4, num_steps=10)
+    sc = replace(sd, dispersion=None, sigma_ex=None, sigma_ey=None, sigma_ez=None)
+    ten = scenes.tensor_region(sc, (8, 8, 8), (12, 12, 12),
+                               scenes.rotated_diag((4.0, 2.0, 3.0), 0.5, 1),
+                               np.array([[0, 80.0, 0], [-80.0, 0, 0], [0, 0, 10.0]]))
+    sc = replace(sc, tensor=ten)
+    tabs = [T.axis_tables(sc, a) for a in range(3)]
+    tt = T.tensor_tables(sc, tabs)
+    m1, m2 = ten.rows(sc.dt)
+    np.testing.assert_array_equal(tt["m1"], m1.astype(np.float32))
+    np.testing.assert_array_equal(tt["m2"], m2.astype(np.float32))
+    assert np.all(tt["pec"] == 1.0)  # the block sits away from every wall
+    ca, cb = T.e_coefficients(sc, tabs)
+    for c in range(3):
+        cells = np.asarray(ten.cell)[np.asarray(ten.comp) == c]
+        assert np.all(ca[c].ravel()[cells] == 0.0) and np.all(cb[c].ravel()[cells] == 1.0)
