@@ -5,13 +5,23 @@ Drude + Lorentz spheres (seed 0), a z-polarised point dipole at the centre, thre
 field DFT monitors at 8 frequencies. A benchmark step is one FDTD time step of that grid.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload bulk|bloch] [--size N] [--no-e2e] [--no-cpu] [--no-secondary]
+                    [--precision]
 
 Prints one JSON line. ``value`` is device-timed (CUDA events on the run stream, max over
 ranks) with the scene resident in HBM; ``e2e`` times the public ``solver.run`` call with host
-arrays: table build and upload, the K steps, and the readout of every monitor.
-``--impl reference`` times the FP64 NumPy transcription of OpenEM's step on the host cores.
-Multi-GPU runs are independent replicas, one per GPU (the step has no exchange between
-independent simulations).
+arrays: table build and upload, the K steps, and the readout of every monitor, with the three
+phases' host times. ``--impl reference`` times the FP64 NumPy transcription of OpenEM's step on
+the host cores. Multi-GPU runs are independent replicas, one per GPU (the step has no exchange
+between independent simulations).
+
+``--workload bloch`` measures the Bloch metasurface cell instead (256 x 256 x 1024 complex
+cells, Bloch phase 0.15 on x, CPML 12 on z, a 40-cell pixelated anisotropic layer, an oblique
+plane wave, one flux plane at 200 frequencies); the default run reports a short measurement of
+it under ``secondary``. ``--precision`` adds the DFT accumulation study of the Bloch cell's
+32 x 32 x 1024 proxy (20,000 steps, 200 frequencies) to the Bloch line. ``--size`` scales the
+bulk workload (sphere count by volume) for profiling runs; per-kernel times are in
+``config.kernels_ms_per_launch``.
 """
 
 from __future__ import annotations
@@ -34,14 +44,24 @@ METRIC = "Gcell-updates/s"
 UNIT = "Gcell/s"
 
 
+def n_spheres(n: int) -> int:
+    """64 spheres at 512^3, the same density at other sizes."""
+    return 64 if n == 512 else max(2, int(round(64 * (n / 512) ** 3)))
+
+
 def workload_scene(n: int, steps: int):
     from openem_b200 import scenes
-    return scenes.dispersive_spheres(n=n, num_steps=steps)
+    return scenes.dispersive_spheres(n=n, n_sph=n_spheres(n), num_steps=steps)
 
 
 def workload_name(n: int) -> str:
-    return (f"dispersive_spheres {n}^3 (CPML 12 all faces, 64 Drude+Lorentz spheres seed 0, "
-            f"z-dipole, 3 mid-plane DFT monitors x 8 freqs)")
+    return (f"dispersive_spheres {n}^3 (CPML 12 all faces, {n_spheres(n)} Drude+Lorentz spheres "
+            f"seed 0, z-dipole, 3 mid-plane DFT monitors x 8 freqs)")
+
+
+BLOCH_NAME = ("bloch_metasurface 256x256x1024 complex (Bloch 0.15 on x, periodic y, CPML 12 on "
+              "z, 40-cell 64x64-pixel diagonal anisotropic layer seed 1, oblique s plane wave, "
+              "flux plane x 200 freqs)")
 
 
 # ---------------------------------------------------------------------------------------------
@@ -150,8 +170,7 @@ def dist_done(world: int):
 def cpu_oracle_rate(n: int, steps: int) -> tuple[float, float]:
     from openem_b200 import scenes
     from oracle import ref64
-    sc = scenes.small_dispersive(n=n, n_pml=12, n_sph=max(2, int(64 * (n / 512) ** 3)),
-                                 num_steps=steps + 1)
+    sc = scenes.small_dispersive(n=n, n_pml=12, n_sph=n_spheres(n), num_steps=steps + 1)
     o = ref64.Oracle(sc, steps + 1)
     o.step()
     t0 = time.perf_counter()
@@ -169,7 +188,7 @@ def run_reference(args):
     n = args.ref_size
     from openem_b200 import scenes
     from oracle import ref64
-    sc = scenes.small_dispersive(n=n, n_pml=12, n_sph=max(2, int(64 * (n / 512) ** 3)),
+    sc = scenes.small_dispersive(n=n, n_pml=12, n_sph=n_spheres(n),
                                  num_steps=args.warmup + args.steps + 1)
     o = ref64.Oracle(sc, args.warmup + args.steps + 1)
     for _ in range(args.warmup):
@@ -196,8 +215,185 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------------------------
+# the Bloch cell: throughput and the precision of its DFT accumulation
+# ---------------------------------------------------------------------------------------------
+def measure_bloch(steps: int, warmup: int, e2e: bool, device: int = 0) -> dict:
+    """Device-timed steps of the 256 x 256 x 1024 Bloch cell (value in complex cell-updates
+    per second), the roofline of its dominant kernel, and optionally the same steps end to end
+    through ``solver.run``."""
+    import torch
+
+    from openem_b200 import roofline, scenes, solver
+    KT = min(steps, 20)
+    sc = scenes.bloch_metasurface(num_steps=warmup + steps + KT)
+    stream = torch.cuda.current_stream()
+    plan = solver.Plan(sc, warmup + steps + KT, device=device, stream=stream, cplx=True)
+    plan.run(warmup)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    plan.run(steps)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    plan.status()
+    launches = plan.launches_per_step() * steps
+    plan.enable_timing(True)
+    plan.run(KT)
+    plan.status()
+    tm = plan.timing()
+    plan.close()
+    del plan
+    torch.cuda.empty_cache()
+    cells = int(np.prod(sc.shape))
+    value = cells * steps / (ms * 1e-3) / 1e9
+    peaks = roofline.measured_peaks(ROOT)
+    b_cell = roofline.step_bytes_per_cell_complex(sc)
+    kb = roofline.kernel_bytes_complex(sc)
+    dom = max((k for k in kb if k in tm), key=lambda k: tm[k][1])
+    t_launch = tm[dom][1] / tm[dom][0] * 1e-3
+    out = {"workload": BLOCH_NAME, "metric": METRIC + " (complex cells)", "value": value,
+           "unit": UNIT, "steps": steps, "warmup": warmup, "ms_per_step": ms / steps,
+           "dtype": "f32 (re, im)", "step_bytes_per_cell": b_cell,
+           "step_roofline_frac": value * b_cell / peaks["hbm_gbs"],
+           "roofline": {"bound": "hbm", "kernel": dom,
+                        "achieved": kb[dom] / t_launch / 1e9, "peak": peaks["hbm_gbs"],
+                        "unit": "GB/s", "frac": kb[dom] / t_launch / 1e9 / peaks["hbm_gbs"],
+                        "algorithmic_bytes_per_launch": kb[dom],
+                        "peak_source": peaks["source"]},
+           "kernels_ms_per_launch": {k: v[1] / v[0] for k, v in tm.items()},
+           "gpu_launches": launches}
+    if e2e:
+        torch.cuda.synchronize()
+        stats = {}
+        t0 = time.perf_counter()
+        solver.run(sc, num_steps=steps, use_shutoff=False, verbose=False, device=device,
+                   stream=stream, stats=stats)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out["e2e"] = {"value": cells * steps / dt / 1e9, "unit": UNIT,
+                      "h2d_bytes_per_step": stats["h2d_bytes"] / steps,
+                      "d2h_bytes_per_step": stats["d2h_bytes"] / steps, "seconds": dt,
+                      "setup_s": stats["setup_s"], "step_s": stats["step_s"],
+                      "readout_s": stats["readout_s"]}
+    return out
+
+
+def _accumulate_modes(samples: np.ndarray, phase: np.ndarray, batch: int) -> dict:
+    """The DFT of the E samples ``samples (S, C, P)`` (complex64) with the per-step E phases
+    ``phase (S, nf, 4)`` (columns 0, 1) summed four ways on the GPU: every product in float64;
+    float32 partials over ``batch`` steps added to float64 (the engine's scheme); one float32
+    running sum; a float32 running sum with Kahan's compensation."""
+    import torch
+    dev = torch.device("cuda")
+    S, C, P = samples.shape
+    nf = phase.shape[1]
+    v = torch.as_tensor(samples, device=dev)
+    ph = torch.as_tensor(phase, device=dev)
+    pe = torch.complex(ph[..., 0], ph[..., 1])
+    ref = torch.zeros((nf, C, P), dtype=torch.complex128, device=dev)
+    eng = torch.zeros_like(ref)
+    part = torch.zeros((nf, C, P), dtype=torch.complex64, device=dev)
+    f32 = torch.zeros_like(part)
+    kc = torch.zeros_like(part)
+    kahan = torch.zeros_like(part)
+    for s in range(S):
+        term = pe[s][:, None, None] * v[s][None]
+        ref += pe[s].to(torch.complex128)[:, None, None] * v[s].to(torch.complex128)[None]
+        part += term
+        f32 += term
+        y = term - kc
+        t = kahan + y
+        kc = (t - kahan) - y
+        kahan = t
+        if (s + 1) % batch == 0 or s == S - 1:
+            eng += part.to(torch.complex128)
+            part.zero_()
+    return {"fp64": ref.cpu().numpy(), "engine_scheme": eng.cpu().numpy(),
+            "fp32": f32.to(torch.complex128).cpu().numpy(),
+            "kahan": kahan.to(torch.complex128).cpu().numpy()}
+
+
+def dft_precision_study(nx: int = 32, ny: int = 32, nz: int = 1024, steps: int = 20000,
+                        nfreq: int = 200, npix: int = 8, oracle: bool = False) -> dict:
+    """Precision of the flux-plane DFT on a proxy of the Bloch cell (the same transverse
+    wavevector, ``npix`` x ``npix`` pixels). The plane's E is recorded every step by a field
+    time monitor; the DFT of those very samples is re-formed on the host four ways
+    (:func:`_accumulate_modes`), and each, with the device phasors, is compared with the
+    float64 sum of the samples (``vs_fp64_sum``: the accumulation error alone) and, with
+    ``oracle``, with the FP64 oracle's phasors of the same scene (``vs_oracle``: accumulation
+    plus the float32 field trajectory). Errors are max |X - ref| / max |ref| over points,
+    frequencies and the two tangential E components."""
+    from openem_b200 import scenes, solver, tables
+    sc = scenes.bloch_metasurface(nx=nx, ny=ny, nz=nz, npix=npix, nfreq=nfreq, num_steps=steps,
+                                  bloch_k=(0.15 * nx / 256, 0.0, 0.0))
+    mon = sc.flux_monitors[0]
+    km = int(mon.plane_index)
+    sc_rec = scenes.with_time_monitor(sc, name="plane", comps=(0, 1), origin=(0, 0, km),
+                                      box=(nx, ny, 1), interval=1)
+    t0 = time.perf_counter()
+    res = solver.run(sc_rec, use_shutoff=False, verbose=False, return_fields=True)
+    wall = time.perf_counter() - t0
+    # slot m of the time monitor holds E^m; the DFT term of step n is E^(n+1), the last one
+    # being the final field
+    ts = np.asarray(res.time_samples["plane"]).astype(np.complex64)[:, :, :, :, 0]
+    last = np.stack([np.asarray(res.fields[c])[:, :, km] for c in ("Ex", "Ey")])
+    e = np.concatenate([ts[:, 1:], last.astype(np.complex64)[:, None]], axis=1)
+    samples = np.ascontiguousarray(np.moveaxis(e, 1, 0)).reshape(steps, 2, nx * ny)
+    phase = tables.phase_table(mon.freqs, sc.dt, steps, mon.apodization)
+    batch = tables.batch_depth(nx * ny, 4)
+    sums = _accumulate_modes(samples, phase, batch)
+    dev = np.moveaxis(np.asarray(res.phasors["T"].data)[0:2].reshape(2, nfreq, nx * ny), 0, 1)
+    modes = (("engine", dev), ("engine_scheme_host", sums["engine_scheme"]),
+             ("fp32", sums["fp32"]), ("kahan", sums["kahan"]))
+    out = {"grid": [nx, ny, nz], "steps": steps, "nfreq": nfreq, "batch": batch,
+           "run_seconds": wall}
+    ref = sums["fp64"]
+    out["vs_fp64_sum"] = {k: float(np.abs(a - ref).max() / np.abs(ref).max()) for k, a in modes}
+    if oracle:
+        from oracle import ref64
+        r = ref64.run(sc)
+        oref = np.moveaxis(np.asarray(r.phasors["T"])[0:2].reshape(2, nfreq, nx * ny), 0, 1)
+        out["vs_oracle"] = {k: float(np.abs(a - oref).max() / np.abs(oref).max())
+                            for k, a in modes + (("fp64_sum", ref),)}
+    return out
+
+
+# ---------------------------------------------------------------------------------------------
 # the engine
 # ---------------------------------------------------------------------------------------------
+def run_bloch_line(args):
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+    torch.cuda.set_device(local)
+    barrier(world)
+    clocks = ClockSampler(local) if rank == 0 else None
+    if clocks:
+        clocks.start()
+    m = measure_bloch(args.steps, args.warmup, e2e=not args.no_e2e, device=local)
+    clk = clocks.stop() if clocks else None
+    ms_max = reduce_max(m["ms_per_step"] * args.steps, world)
+    if rank == 0:
+        cells = 256 * 256 * 1024
+        line = {"metric": METRIC, "value": world * cells * args.steps / (ms_max * 1e-3) / 1e9,
+                "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded scene factory)",
+                "config": {"workload": BLOCH_NAME, "cells": cells,
+                           "parallelism": f"replicas x{world}",
+                           "l2": "inputs larger than L2: 6.4 GB of complex fields per step",
+                           "step_bytes_per_cell": m["step_bytes_per_cell"],
+                           "step_roofline_frac": m["step_roofline_frac"],
+                           "kernels_ms_per_launch": m["kernels_ms_per_launch"]},
+                "roofline": m["roofline"], "cpu_baseline": None, "e2e": m.get("e2e"),
+                "gpu_launches": m["gpu_launches"], "clocks": clk}
+        if args.precision:
+            line["config"]["dft_precision"] = dft_precision_study()
+        print(json.dumps(line), flush=True)
+    dist_done(world)
+
+
 def run_ours(args):
     world, rank, local = dist_setup(args.gpus)
     import torch
@@ -273,7 +469,13 @@ def run_ours(args):
         e2e = {"value": world * cells * K / dt / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": stats["h2d_bytes"] / K,
                "d2h_bytes_per_step": stats["d2h_bytes"] / K,
-               "seconds": dt}
+               "seconds": dt, "setup_s": stats["setup_s"], "step_s": stats["step_s"],
+               "readout_s": stats["readout_s"]}
+
+    # a short device-timed run of the Bloch cell, reported beside the headline
+    secondary = None
+    if world == 1 and not args.no_secondary:
+        secondary = {"bloch": measure_bloch(max(K, 50), W, e2e=False, device=local)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -305,6 +507,7 @@ def run_ours(args):
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
+            "secondary": secondary,
         }
         print(json.dumps(line), flush=True)
     dist_done(world)
@@ -316,17 +519,22 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="bulk", choices=["bulk", "bloch"])
     ap.add_argument("--size", type=int, default=512)
-    ap.add_argument("--ref-size", type=int, default=64)
-    ap.add_argument("--cpu-size", type=int, default=96)
-    ap.add_argument("--cpu-steps", type=int, default=60)
+    ap.add_argument("--ref-size", type=int, default=128)
+    ap.add_argument("--cpu-size", type=int, default=128)
+    ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--precision", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "bloch":
+        run_bloch_line(args)
     else:
         run_ours(args)
 

@@ -317,10 +317,17 @@ int oem_plan_read_monitor_interleaved(oem_plan* p, int mon_id, double* out, void
 int oem_plan_read_time_monitor(oem_plan* p, int id, float* out, void* stream);
 int oem_plan_read_field(oem_plan* p, int comp, float* out, void* stream);
 int oem_plan_write_field(oem_plan* p, int comp, const float* in, void* stream);
+/* Complex plan: set both parts of one field component from unpadded (nx, ny, nz) float32
+ * arrays (the inverse of oem_plan_read_field_complex; OpenEM keeps re/im as separate arrays,
+ * openem/device_tables.py:87-104). Synchronous. */
+int oem_plan_write_field_complex(oem_plan* p, int comp, const float* re, const float* im,
+                                 void* stream);
 
 /* Volume-weighted float64 sums for the early-termination criteria
  * (openem/solver.py:107-121, :160-203): out[0] = sum V |E|^2, out[1] = sum V eps |E|^2,
- * out[2] = sum V |H|^2, with each component's own Yee dual volume. Synchronous. */
+ * out[2] = sum V |H|^2. V is the Yee dual volume of the E component of the same index
+ * (openem/grid.py:350-366), for H too, as OpenEM weights them (openem/solver.py:176); a complex
+ * plan sums re^2 + im^2. Synchronous. */
 int oem_plan_energy(oem_plan* p, double out[3], void* stream);
 
 /* Field sums for callers that cannot allocate device memory. This entry point has no
@@ -330,10 +337,14 @@ int oem_plan_energy(oem_plan* p, double out[3], void* stream);
  * z padded to nzp >= nz), three fp32 relative-permittivity arrays in the same layout (or NULL
  * for 1), and the host array `spacing` of 2*(nx+ny+nz) doubles: primal then dual spacing of x,
  * then of y, then of z. Output: out[0] = sum V|E|^2, out[1] = sum V eps|E|^2,
- * out[2] = sum V|H|^2 with each component's Yee dual volume; synchronous on `stream`.
+ * out[2] = sum V|H|^2 with the volumes of oem_plan_energy; synchronous on `stream`. Real
+ * fields only: the imaginary parts of a complex (Bloch) plan are not summed, so such callers
+ * use oem_plan_energy instead.
  * It allocates nothing: its only scratch is a file-scope device array of 581 KB (held on every
  * GPU that loads the library until exit), so nx + ny + nz is limited to 32768. The first call
- * on a device looks that array up (cudaGetSymbolAddress) and should come before any stream
+ * on a device looks that array up (cudaGetSymbolAddress); under CUDA's lazy module loading
+ * that first call also loads the library's module onto the device, which can allocate and
+ * synchronise. Make one warm-up call per device outside the step loop and before any stream
  * capture. All calls share the array: calls that overlap on the GPU race. */
 int oem_field_energy_noalloc(const float* const fields[6], const float* const eps[3], int nx,
                              int ny, int nz, int nzp, const double* spacing, double out[3],

@@ -2011,6 +2011,24 @@ int oem_plan_write_field(oem_plan* p, int comp, const float* in, void* stream) {
   return OEM_OK;
 }
 
+int oem_plan_write_field_complex(oem_plan* p, int comp, const float* re, const float* im,
+                                 void* stream) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (!p->is_complex) return set_error(OEM_ERR_STATE, "not a complex plan");
+  if (comp < 0 || comp > 5 || !re || !im) return set_error(OEM_ERR_INVALID, "component must be 0..5");
+  if ((rc = use_device(p))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  float* dst[2] = {p->yp.f[comp], p->yp.fi[comp]};
+  const float* src[2] = {re, im};
+  for (int q = 0; q < 2; ++q)
+    OEM_CUDA(cudaMemcpy2DAsync(dst[q], (size_t)p->nzp * sizeof(float), src[q],
+                               (size_t)p->nz * sizeof(float), (size_t)p->nz * sizeof(float),
+                               (size_t)p->nx * p->ny, cudaMemcpyHostToDevice, s));
+  OEM_CUDA(cudaStreamSynchronize(s));
+  return OEM_OK;
+}
+
 int oem_plan_energy(oem_plan* p, double out[3], void* stream) {
   int rc = check_plan(p, true);
   if (rc) return rc;

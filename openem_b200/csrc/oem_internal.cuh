@@ -511,6 +511,10 @@ cudaError_t launch_mode_h(const YeeParams& P, const ModeSrc& m, const int* step,
 cudaError_t launch_mode_e(const YeeParams& P, const ModeSrc& m, const int* step, cudaStream_t s);
 cudaError_t launch_energy(const YeeParams& P, double* const dl[3][2], double* part, int nblocks,
                           cudaStream_t s);
+// Block partials of the float64 energy sums: at most this many blocks of 256 threads, summed in
+// block order. oem_plan_energy and oem_field_energy_noalloc share it, so both add the same
+// partials in the same order.
+constexpr int kEnergyMaxBlocks = 148 * 16;
 int energy_block_count(const YeeParams& P);
 
 }  // namespace oem

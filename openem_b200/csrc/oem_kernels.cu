@@ -456,7 +456,9 @@ __global__ void k_step_advance(int* step) {
 }
 
 // Float64 volume-weighted sums for early termination (openem/solver.py:107-121, 160-203),
-// one partial per block: [sum V|E|^2, sum V eps |E|^2, sum V |H|^2].
+// one partial per block: [sum V|E|^2, sum V eps |E|^2, sum V |H|^2]. V is the Yee dual volume
+// of the E component of the same index (openem/grid.py:350-366); OpenEM weights Hx, Hy, Hz with
+// those same three volumes (openem/solver.py:176), and so does this sum.
 __global__ void __launch_bounds__(256) k_energy(YeeParams P, const double* dxp, const double* dxd,
                                                 const double* dyp, const double* dyd,
                                                 const double* dzp, const double* dzd,
@@ -475,9 +477,6 @@ __global__ void __launch_bounds__(256) k_energy(YeeParams P, const double* dxp, 
     const double vex = dxp[i] * dyd[j] * dzd[k];
     const double vey = dxd[i] * dyp[j] * dzd[k];
     const double vez = dxd[i] * dyd[j] * dzp[k];
-    const double vhx = dxd[i] * dyp[j] * dzp[k];
-    const double vhy = dxp[i] * dyd[j] * dzp[k];
-    const double vhz = dxp[i] * dyp[j] * dzd[k];
     const double ex = P.f[0][id], ey = P.f[1][id], ez = P.f[2][id];
     const double hx = P.f[3][id], hy = P.f[4][id], hz = P.f[5][id];
     double ax2 = ex * ex, ay2 = ey * ey, az2 = ez * ez;
@@ -491,7 +490,7 @@ __global__ void __launch_bounds__(256) k_energy(YeeParams P, const double* dxp, 
     const double e0 = vex * ax2, e1 = vey * ay2, e2 = vez * az2;
     s0 += e0 + e1 + e2;
     s1 += e0 * M.eps[0] + e1 * M.eps[1] + e2 * M.eps[2];
-    s2 += vhx * bx2 + vhy * by2 + vhz * bz2;
+    s2 += vex * bx2 + vey * by2 + vez * bz2;  // H weighted like E (openem/solver.py:176)
   }
   sh[0][threadIdx.x] = s0;
   sh[1][threadIdx.x] = s1;
@@ -977,7 +976,7 @@ cudaError_t launch_step_advance(int* step, cudaStream_t s) {
 int energy_block_count(const YeeParams& P) {
   const int64_t n = (int64_t)P.nx * P.ny * P.nz;
   int64_t nb = (n + 255) / 256;
-  if (nb > 148 * 16) nb = 148 * 16;
+  if (nb > kEnergyMaxBlocks) nb = kEnergyMaxBlocks;
   return (int)(nb < 1 ? 1 : nb);
 }
 

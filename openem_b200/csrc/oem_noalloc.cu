@@ -18,7 +18,12 @@
 //     cleared between calls; but two calls whose work overlaps on the GPU (different streams,
 //     or different host threads) race on it and return wrong sums.
 //   * The first call on each device looks up the array's device address with
-//     cudaGetSymbolAddress; make that first call before any stream capture.
+//     cudaGetSymbolAddress. With CUDA's lazy module loading (the default since CUDA 12) that
+//     first lookup is also what loads this library's module onto the device, which can itself
+//     allocate and synchronise the device. Make one warm-up call per device outside the step
+//     loop, before any stream capture; later calls only launch and copy.
+//   * Fields are real: a complex (Bloch) plan's imaginary parts are not read, so those
+//     callers must use oem_plan_energy.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -28,7 +33,7 @@
 
 namespace {
 
-constexpr int kMaxBlocks = 148 * 16;   // block partial sums per call
+constexpr int kMaxBlocks = oem::kEnergyMaxBlocks;  // block partial sums per call
 constexpr int kMaxAxisCells = 32768;   // nx + ny + nz
 constexpr int kPartials = 0;                       // [3 * kMaxBlocks] block partials
 constexpr int kTotals = 3 * kMaxBlocks;            // [3] final sums
@@ -68,9 +73,6 @@ __global__ void __launch_bounds__(256) k_energy_static(FieldSet F, int nx, int n
     const double vex = dxp[i] * dyd[j] * dzd[k];
     const double vey = dxd[i] * dyp[j] * dzd[k];
     const double vez = dxd[i] * dyd[j] * dzp[k];
-    const double vhx = dxd[i] * dyp[j] * dzp[k];
-    const double vhy = dxp[i] * dyd[j] * dzp[k];
-    const double vhz = dxp[i] * dyp[j] * dzd[k];
     const double ex = F.f[0][id], ey = F.f[1][id], ez = F.f[2][id];
     const double hx = F.f[3][id], hy = F.f[4][id], hz = F.f[5][id];
     const double e0 = vex * ex * ex, e1 = vey * ey * ey, e2 = vez * ez * ez;
@@ -79,7 +81,7 @@ __global__ void __launch_bounds__(256) k_energy_static(FieldSet F, int nx, int n
     const float p2 = F.eps[2] ? F.eps[2][id] : 1.0f;
     s0 += e0 + e1 + e2;
     s1 += e0 * p0 + e1 * p1 + e2 * p2;
-    s2 += vhx * hx * hx + vhy * hy * hy + vhz * hz * hz;
+    s2 += vex * hx * hx + vey * hy * hy + vez * hz * hz;  // H weighted like E
   }
   sh[0][threadIdx.x] = s0;
   sh[1][threadIdx.x] = s1;

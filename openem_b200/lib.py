@@ -69,6 +69,7 @@ SIGNATURES = {
     "oem_plan_read_field_complex": (_I, [_P, _I, _P, _P, _P]),
     "oem_plan_read_time_monitor_complex": (_I, [_P, _I, _P, _P, _P]),
     "oem_plan_write_field": (_I, [_P, _I, _P, _P]),
+    "oem_plan_write_field_complex": (_I, [_P, _I, _P, _P, _P]),
     "oem_plan_energy": (_I, [_P, _P, _P]),
     "oem_plan_field_ptrs": (_I, [_P, _P, C.POINTER(_I)]),
     "oem_field_energy_noalloc": (_I, [_P, _P, _I, _I, _I, _I, _P, _P, _P]),

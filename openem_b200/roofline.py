@@ -59,6 +59,18 @@ def step_bytes_per_cell(sc) -> float:
     return (48.0 + 6.0) + (psi + ade + mon) / n
 
 
+def step_bytes_per_cell_complex(sc) -> float:
+    """Algorithmic bytes per complex cell-update of the Bloch path: both parts of the six fields
+    read and written (96 B), the 6-byte material form, both parts of the slab psi (64 B per slab
+    cell and axis) and both parts of the four tangential components of every flux-plane point
+    read once per step (32 B per point)."""
+    c = counts(sc)
+    n = c["ncell"]
+    psi = 64.0 * sum(c["slab_cells"].values())
+    mon = 32.0 * c["monitor_points"]
+    return (96.0 + 6.0) + (psi + mon) / n
+
+
 def kernel_bytes(sc) -> dict:
     """Algorithmic bytes per launch of this engine's step kernels.
 
@@ -77,6 +89,13 @@ def kernel_bytes(sc) -> dict:
             "update_e": 38.0 * n + psi + 4.0 * n_entry,
             "ade": 16.0 * c["n_pole"] + 8.0 * n_entry,
             "update_he": 50.0 * n + 2.0 * psi + 4.0 * n_entry}
+
+
+def kernel_bytes_complex(sc) -> dict:
+    """Per launch of the complex split update, which runs the real update once on each part:
+    twice the real kernels' bytes (the seam-face terms are below 1% and not counted)."""
+    kb = kernel_bytes(sc)
+    return {"update_h": 2.0 * kb["update_h"], "update_e": 2.0 * kb["update_e"]}
 
 
 def measured_peaks(root=None) -> dict:

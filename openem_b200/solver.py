@@ -379,6 +379,16 @@ class Plan:
             raise ValueError(f"field shape {a.shape} != {self.shape}")
         L.check(self.lib.oem_plan_write_field(self.h, int(comp), L.ptr(a), self._s), "write_field")
 
+    def write_field_complex(self, comp: int, arr) -> None:
+        """Set both parts of one field component of a complex plan."""
+        arr = np.asarray(arr)
+        re = np.ascontiguousarray(arr.real, dtype=np.float32)
+        im = np.ascontiguousarray(arr.imag, dtype=np.float32)
+        if re.shape != self.shape:
+            raise ValueError(f"field shape {re.shape} != {self.shape}")
+        L.check(self.lib.oem_plan_write_field_complex(self.h, int(comp), L.ptr(re), L.ptr(im),
+                                                      self._s), "write_field_complex")
+
     def energy(self) -> np.ndarray:
         out = np.zeros(3, np.float64)
         L.check(self.lib.oem_plan_energy(self.h, L.ptr(out), self._s), "energy")
@@ -466,24 +476,31 @@ def run(sc, num_steps: int | None = None, use_shutoff: bool = True, kernels=None
     given, receives the host-to-device and device-to-host byte counts and the launches per
     step."""
     del kernels
-    if force_complex or any(k != 0.0 for k in sc.bloch_k):
-        from openem_b200 import bloch
-        return bloch.run(sc, num_steps=num_steps, use_shutoff=use_shutoff, verbose=verbose,
-                         return_fields=return_fields, policy=policy, device=device,
-                         stream=stream, stats=stats)
+    # the complex-field path (openem/solver.py:1263-1358, _run_bloch): fields and CPML psi as
+    # real and imaginary float32 arrays, the Bloch phase exp(+-i 2 pi k) only in the seam
+    # neighbour masks; with k = 0 (force_complex) the two parts are two independent real runs.
+    # Its subset is OpenEM's (refuse_unsupported_bloch).
+    cplx = bool(force_complex or any(k != 0.0 for k in sc.bloch_k))
     return run_plan(sc, num_steps, use_shutoff, verbose, return_fields, policy, device, stream,
-                    stats, cplx=False)
+                    stats, cplx=cplx)
 
 
 def run_plan(sc, num_steps, use_shutoff, verbose, return_fields, policy, device, stream, stats,
              cplx: bool) -> Result:
     """Build a plan (real or complex fields), step it with the shutoff cadence, read out."""
     n_total = int(num_steps if num_steps is not None else sc.num_time_steps)
+    t0 = time.perf_counter()
     plan = Plan(sc, n_total, device=device, stream=stream, cplx=cplx)
+    t1 = time.perf_counter()
     try:
         res = _loop(plan, sc, n_total, use_shutoff, verbose, return_fields, policy)
         plan.status()
+        t2 = time.perf_counter()
         if stats is not None:
+            # host wall time of the three phases: tables + upload + graph capture, the steps
+            # (with the shutoff checks), the readout of every monitor and field
+            stats.update(setup_s=t1 - t0, step_s=res.wall_seconds,
+                         readout_s=max(t2 - t1 - res.wall_seconds, 0.0))
             d2h = sum(np.asarray(p.data).size * 16 for p in res.phasors.values())
             d2h += sum(np.asarray(a).size * 16 for a in res.field_phasors.values())
             width = 8 if cplx else 4  # float32 parts read back per value
@@ -528,13 +545,14 @@ def _loop(plan: Plan, sc, n_total: int, use_shutoff: bool, verbose: bool, return
                                      for m, mid, shp in plan.flux_mons])
             stop = pol.check(steps, float(e[0]), float(m_u), fl) and steps > source_end \
                 and steps >= guard
-            trace.append((steps, pol.field_decay.ratio if pol.field_decay else float("nan")))
+            trace.append((steps, shutoff_mod.trace_ratio(pol)))
             if stop:
                 triggered = True
                 if verbose:
                     print(f"  early termination at step {steps}: {pol.reason}", flush=True)
                 break
     plan.flush()
+    plan.status()  # waits for the stream: the steps are done when the clock stops
     wall = time.time() - t0
     phasors = plan.flux_phasors()
     fphas = plan.field_phasors()
@@ -551,7 +569,7 @@ def _loop(plan: Plan, sc, n_total: int, use_shutoff: bool, verbose: bool, return
                       "field has most likely diverged", flush=True)
     return Result(phasors=phasors, steps_run=steps, shutoff_triggered=triggered,
                   decay_trace=trace,
-                  energy_trace=(pol.energy_decay.abs_history if pol.energy_decay else []),
+                  energy_trace=shutoff_mod.energy_trace(pol),
                   source_end=int(source_end), wall_seconds=wall,
                   stop_reason=pol.reason, shutoff_summary=pol.summary(), fields=fields,
                   field_phasors=fphas, time_samples=tsamp, time_slots=tslots,

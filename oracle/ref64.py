@@ -905,6 +905,18 @@ class Oracle:
         self._sample_flux_time(n + 1)
         self.n += 1
 
+    def load_fields(self, fields) -> None:
+        """Start from the given six fields (Ex, Ey, Ez, Hx, Hy, Hz) instead of zeros. CPML psi,
+        pole states and DFT accumulators still start at zero; the engine sets the same start
+        with ``Plan.write_field``. Scenes with time monitors are refused (their t = 0 sample
+        was taken on zero fields)."""
+        if self.n:
+            raise RuntimeError("load_fields must come before the first step")
+        if self.tmon or getattr(self, "ftmon", []):
+            raise ValueError("load_fields: scenes with time monitors are not supported")
+        for F, v in zip((*self.E, *self.H), fields):
+            F[...] = v
+
     def run(self, n_steps: int | None = None) -> OracleResult:
         n_steps = self.n_total if n_steps is None else int(n_steps)
         t0 = time.perf_counter()
@@ -1044,3 +1056,55 @@ class BlochOracle(Oracle):
             for (i, j, k), cf in zip(np.asarray(d.indices), np.asarray(d.coef)):
                 pts.append((int(d.component), int(i), int(j), int(k), float(cf), s))
         return {"pts": pts, "amp": np.stack([t[:n1] for t in tabs])}
+
+
+# ---- early termination on the oracle (openem/solver.py:107-203, :1165-1213) ------------------
+def shutoff_sums(o: Oracle) -> tuple:
+    """``(sum V |E|^2, sum V eps |E|^2, sum V |H|^2)`` of the oracle's current fields in float64.
+    V is the Yee dual volume of the E component of the same index (``openem/grid.py:350-366``),
+    used for H as well (``openem/solver.py:171-176``); eps the scene's relative permittivity."""
+    sc = o.sc
+    (xp, yp, zp) = (a.dl for a in sc.grid.axes)
+    (xd, yd, zd) = (a.dl_dual for a in sc.grid.axes)
+    vols = (xp[:, None, None] * yd[None, :, None] * zd[None, None, :],
+            xd[:, None, None] * yp[None, :, None] * zd[None, None, :],
+            xd[:, None, None] * yd[None, :, None] * zp[None, None, :])
+    eps = (sc.eps_ex, sc.eps_ey, sc.eps_ez)
+    e2 = [np.abs(F) ** 2 for F in o.E]
+    h2 = [np.abs(F) ** 2 for F in o.H]
+    m_e2 = float(sum((v * a).sum() for v, a in zip(vols, e2)))
+    w_e = float(sum((v * np.asarray(ep, dtype=np.float64) * a).sum()
+                    for v, ep, a in zip(vols, eps, e2)))
+    w_h = float(sum((v * a).sum() for v, a in zip(vols, h2)))
+    return m_e2, w_e, w_h
+
+
+def run_shutoff(sc, policy, num_steps: int | None = None):
+    """Run the oracle with early termination: every ``policy.interval`` steps feed the float64
+    sums and (real path only) the flux of every flux monitor to ``policy.check``, and stop once
+    it fires after the last source has finished and after the first time-monitor step
+    (``openem/solver.py:160-203``). Returns ``(OracleResult, steps_run, triggered, trace)``,
+    ``trace`` holding ``(step, m_e2, energy)`` per check."""
+    from openem_b200 import flux as flux_mod
+    from openem_b200 import shutoff as shutoff_mod
+    o = BlochOracle(sc, num_steps) if sc.any_bloch else Oracle(sc, num_steps)
+    source_end = shutoff_mod.source_end_step(sc)
+    tms = list(sc.field_time_monitors) + list(getattr(sc, "flux_time_monitors", []))
+    guard = max([int(m.step_begin) + 1 for m in tms] + [0])
+    interval = int(policy.interval)
+    trace, triggered = [], False
+    while o.n < o.n_total:
+        o.step()
+        if o.n % interval:
+            continue
+        m_e2, w_e, w_h = shutoff_sums(o)
+        m_u = 0.5 * (EPSILON_0 * w_e + MU_0 * w_h)
+        fl = np.zeros(0)
+        if o.fmon and not sc.any_bloch:
+            fl = np.concatenate([flux_mod.plane_flux(mon["acc"], sc.grid, axis=int(mon["m"].axis))
+                                 for mon in o.fmon])
+        trace.append((o.n, m_e2, m_u))
+        if policy.check(o.n, m_e2, m_u, fl) and o.n > source_end and o.n >= guard:
+            triggered = True
+            break
+    return o.result(), o.n, triggered, trace

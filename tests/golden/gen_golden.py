@@ -1,18 +1,18 @@
 """Generate the golden fixtures under ``tests/golden/`` from OpenEM's own CPU code.
 
-Run in a checkout that has the OpenEM sources (default ``/root/reference``; override with
-``OPENEM_SRC``). Only OpenEM's numpy modules are imported -- ``openem.cpml``, ``openem.grid``,
+Run with ``OPENEM_SRC`` set to a checkout of the OpenEM sources. Only OpenEM's numpy modules are imported -- ``openem.cpml``, ``openem.grid``,
 ``openem.model``, ``openem.serialize``, ``openem.tfsf1d`` (its numpy loop), ``openem.shutoff``,
 ``openem.apodization``, ``openem.flux`` -- none of which need cupy, tidy3d or a GPU. The engine's
 own scene factory supplies the scenes, converted field by field into OpenEM's classes.
 
-    python tests/golden/gen_golden.py
+    OPENEM_SRC=<openem checkout> python tests/golden/gen_golden.py [tables tfsf1d shutoff scenes]
 
 Outputs (all small):
     ref_tables.npz     CPML coefficients, axis index tables, dual spacings, apodisation windows,
                        plane flux of fixed phasors
     ref_tfsf1d.npz     the 1D Yee line with one-face injection (lossless slab and lossy profile)
-    ref_shutoff.npz    early-termination decisions on a fixed metric sequence
+    ref_shutoff.npz    early-termination decisions on two fixed metric sequences (the decay
+                       tests fire; the flux test fires while the energy decays slowly)
     ref_scene_slab.npz, ref_scene_disp.npz   scene.npz files written by OpenEM's serializer
 """
 
@@ -27,7 +27,9 @@ import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-SRC = os.environ.get("OPENEM_SRC", "/root/reference")
+SRC = os.environ.get("OPENEM_SRC")
+if not SRC:
+    sys.exit("set OPENEM_SRC to a checkout of the OpenEM sources")
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, SRC)
 
@@ -131,6 +133,20 @@ def gen_tfsf1d(out: dict) -> None:
     out["n_steps"] = np.array(n_steps)
 
 
+def _shutoff_sequence(steps, e2, energy, flux, prefix: str, out: dict) -> None:
+    pol = r_shut.default_policy(1e-5, interval=400)
+    fired, ratios, taus, rels = [], [], [], []
+    for s, a, b, f in zip(steps, e2, energy, flux):
+        fired.append(bool(pol.check(int(s), float(a), float(b), f)))
+        ratios.append(pol.field_decay.ratio)
+        taus.append(pol.energy_decay.tau)
+        rels.append(pol.phasor.rel)
+    out.update({prefix + "steps": steps, prefix + "e2": e2, prefix + "energy": energy,
+                prefix + "flux": flux, prefix + "fired": np.array(fired),
+                prefix + "ratio": np.array(ratios), prefix + "tau": np.array(taus),
+                prefix + "rel": np.array(rels), prefix + "reason": np.array(pol.reason)})
+
+
 def gen_shutoff(out: dict) -> None:
     rng = np.random.default_rng(11)
     steps = np.arange(1, 41) * 400
@@ -139,36 +155,40 @@ def gen_shutoff(out: dict) -> None:
     energy = env * 2e-3
     flux = np.stack([1.0 - np.exp(-steps / 4000.0), 0.5 - 0.4 * np.exp(-steps / 3000.0)], 1)
     flux += 1e-6 * rng.standard_normal(flux.shape)
-    pol = r_shut.default_policy(1e-5, interval=400)
-    fired, ratios, taus, rels = [], [], [], []
-    for s, a, b, f in zip(steps, e2, energy, flux):
-        fired.append(bool(pol.check(int(s), float(a), float(b), f)))
-        ratios.append(pol.field_decay.ratio)
-        taus.append(pol.energy_decay.tau)
-        rels.append(pol.phasor.rel)
-    out.update(steps=steps, e2=e2, energy=energy, flux=flux, fired=np.array(fired),
-               ratio=np.array(ratios), tau=np.array(taus), rel=np.array(rels),
-               reason=np.array(pol.reason))
+    _shutoff_sequence(steps, e2, energy, flux, "", out)
+    # a slowly ringing resonance: the energy decays by ~1e-3 over the run (no decay test
+    # fires) while the fluxes settle, so the flux test fires on its own
+    steps = np.arange(1, 61) * 400
+    ring = np.exp(-steps / 3500.0)
+    energy = 1e-3 * (np.minimum(steps / 2000.0, 1.0) * ring + 1e-4)
+    e2 = energy * (1.0 + 0.2 * np.sin(0.003 * steps))
+    flux = np.stack([0.8 - 0.3 * ring, 0.1 + 0.05 * ring, -0.2 + 0.1 * ring], 1)
+    flux += 1e-9 * rng.standard_normal(flux.shape)
+    _shutoff_sequence(steps, e2, energy, flux, "b_", out)
 
 
-def main() -> None:
-    d: dict = {}
-    gen_tables(d)
-    np.savez_compressed(HERE / "ref_tables.npz", **d)
-    d = {}
-    gen_tfsf1d(d)
-    np.savez_compressed(HERE / "ref_tfsf1d.npz", **d)
-    d = {}
-    gen_shutoff(d)
-    np.savez_compressed(HERE / "ref_shutoff.npz", **d)
-    slab = scenes.slab_plane_wave(nxy=2, num_steps=400)
-    r_ser.save(to_ref(slab), HERE / "ref_scene_slab.npz")
-    disp = scenes.with_time_monitor(scenes.small_dispersive(n=20, n_sph=2, num_steps=60,
-                                                            n_pml=6, nfreq=3), interval=7)
-    r_ser.save(to_ref(disp), HERE / "ref_scene_disp.npz")
+def main(which) -> None:
+    if "tables" in which:
+        d: dict = {}
+        gen_tables(d)
+        np.savez_compressed(HERE / "ref_tables.npz", **d)
+    if "tfsf1d" in which:
+        d = {}
+        gen_tfsf1d(d)
+        np.savez_compressed(HERE / "ref_tfsf1d.npz", **d)
+    if "shutoff" in which:
+        d = {}
+        gen_shutoff(d)
+        np.savez_compressed(HERE / "ref_shutoff.npz", **d)
+    if "scenes" in which:
+        slab = scenes.slab_plane_wave(nxy=2, num_steps=400)
+        r_ser.save(to_ref(slab), HERE / "ref_scene_slab.npz")
+        disp = scenes.with_time_monitor(scenes.small_dispersive(n=20, n_sph=2, num_steps=60,
+                                                                n_pml=6, nfreq=3), interval=7)
+        r_ser.save(to_ref(disp), HERE / "ref_scene_disp.npz")
     for p in sorted(HERE.glob("ref_*.npz")):
         print(p.name, p.stat().st_size)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or ("tables", "tfsf1d", "shutoff", "scenes"))

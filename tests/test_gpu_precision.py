@@ -1,17 +1,24 @@
 """Precision of the device DFT accumulation (float32 partials over a snapshot batch, each batch
-added once to a float64 accumulator) on a small Bloch cell: the E phasors of the flux plane
-against the float64 sum of the very samples the engine folded (recorded every step by a field
-time monitor), with a plain float32 running sum as the comparison that shows the difference."""
+added once to a float64 accumulator) on a small Bloch cell, 3000 steps x 16 frequencies.
+
+Against the float64 sum of the very samples the engine folded (recorded every step by a field
+time monitor) the engine's phasors carry the accumulation error alone: within 5e-7, like a
+Kahan-compensated float32 sum, while a plain float32 running sum is several times worse.
+Against the FP64 oracle's phasors of the same scene (its fields in float64 too) every mode is
+within the 1e-4 phasor tolerance, the float32 field trajectory included."""
 
 import pytest
 
-from openem_b200 import precision
+import bench
 
 pytestmark = pytest.mark.gpu
 
 
-def test_dft_accumulation_matches_float64_sum():
-    r = precision.study(nx=8, ny=8, nz=256, steps=3000, nfreq=16, npix=2)
-    assert r["engine"] < 5e-7, r
-    assert r["kahan"] < 5e-7, r
-    assert r["fp32"] > 5 * r["engine"], r
+def test_dft_accumulation_matches_float64_sum_and_oracle():
+    r = bench.dft_precision_study(nx=8, ny=8, nz=256, steps=3000, nfreq=16, npix=2, oracle=True)
+    s = r["vs_fp64_sum"]
+    assert s["engine"] < 5e-7, r
+    assert s["kahan"] < 5e-7, r
+    assert s["fp32"] > 5 * s["engine"], r
+    o = r["vs_oracle"]
+    assert all(v < 1e-4 for v in o.values()), r

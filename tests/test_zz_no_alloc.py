@@ -53,6 +53,19 @@ def test_noalloc_field_sums_match_plan_sums_twice():
             np.testing.assert_allclose(out, ref, rtol=1e-12, atol=0)
             outs.append(out)
         np.testing.assert_array_equal(outs[0], outs[1])
+        # eps = NULL means relative permittivity 1: the eps-weighted sum equals the plain one
+        out1 = np.zeros(3, np.float64)
+        L.check(lib.oem_field_energy_noalloc(fptr, None, nx, ny, nz, nzp.value, L.ptr(spacing),
+                                             L.ptr(out1), None), "field_energy_noalloc eps=NULL")
+        assert out1[1] == out1[0]
+        np.testing.assert_array_equal(out1[[0, 2]], outs[0][[0, 2]])
+        # on a caller's own (non-default) stream the sums are the same
+        side = torch.cuda.Stream(device="cuda:0")
+        out2 = np.zeros(3, np.float64)
+        L.check(lib.oem_field_energy_noalloc(fptr, eptr, nx, ny, nz, nzp.value, L.ptr(spacing),
+                                             L.ptr(out2), C.c_void_p(side.cuda_stream)),
+                "field_energy_noalloc on a side stream")
+        np.testing.assert_array_equal(out2, outs[0])
         # sizes beyond the fixed scratch are refused with a clear error
         big = np.zeros(2 * (40000 + 2), np.float64)
         rc = lib.oem_field_energy_noalloc(fptr, eptr, 40000, 1, 1, 32, L.ptr(big),
