@@ -7,7 +7,7 @@ on all faces, Drude+Lorentz spheres, the z dipole; the start is six seeded stand
 fields (``numpy.random.default_rng(21)``, Ex..Hz in order). The file holds the six final float32
 fields, which ``tests/test_oracle_golden.py`` compares with the FP64 oracle on the CPU.
 
-    python tests/golden/gen_ref_kernel_fields.py
+    python tests/golden/gen_ref_kernel_fields.py [output directory, default tests/golden]
 """
 
 from __future__ import annotations
@@ -36,9 +36,10 @@ def main() -> None:
     rk = ReferenceKernels(sc, STEPS)
     rk.load_fields(start_fields(sc.shape))
     out = rk.run(STEPS)
-    np.savez_compressed(HERE / "ref_kernels_disp.npz", steps=np.int32(STEPS),
+    dst = pathlib.Path(sys.argv[1]) if len(sys.argv) > 1 else HERE
+    np.savez_compressed(dst / "ref_kernels_disp.npz", steps=np.int32(STEPS),
                         seed=np.int32(SEED), **out)
-    print("ref_kernels_disp.npz", (HERE / "ref_kernels_disp.npz").stat().st_size)
+    print("ref_kernels_disp.npz", (dst / "ref_kernels_disp.npz").stat().st_size)
 
 
 if __name__ == "__main__":

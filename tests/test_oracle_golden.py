@@ -576,7 +576,8 @@ def test_oracle_matches_openem_kernel_fields():
     (update_h, dispersion_pre, update_e, inject_dipole, dispersion_post, compiled unchanged;
     ``tests/golden/gen_ref_kernel_fields.py``) on a 24^3 Drude+Lorentz scene with CPML 6 and the
     z dipole, from seeded random float32 fields. The FP64 oracle from the same start agrees
-    within 1e-5 of each field family's norm: float32 rounding, not a different update."""
+    within 2e-6 of each field family's norm (measured 3-4e-7): float32 rounding, not a
+    different update."""
     path = GOLD / "ref_kernels_disp.npz"
     if not path.exists():
         pytest.skip("fixture not generated yet")
@@ -591,4 +592,4 @@ def test_oracle_matches_openem_kernel_fields():
     for fam in (("Ex", "Ey", "Ez"), ("Hx", "Hy", "Hz")):
         den = np.sqrt(sum(float(np.linalg.norm(z[n])) ** 2 for n in fam))
         for n in fam:
-            assert np.linalg.norm(r.fields[n] - z[n]) / den < 1e-5, n
+            assert np.linalg.norm(r.fields[n] - z[n]) / den < 2e-6, n
