@@ -137,6 +137,15 @@ int oem_plan_add_mode_source(oem_plan* p, int axis, int kh, int ks, int n1, int 
  * serving autotuner per grid-size class before oem_plan_finalize. */
 int oem_plan_set_xchunk(oem_plan* p, int xch);
 
+/* Check of the failure path of the bounded device waits (no OpenEM counterpart; OpenEM's
+ * kernels have no waits). With polls > 0, before oem_plan_finalize, every consumer warp of the
+ * warp-specialised E update additionally waits on a shared-memory barrier that no thread ever
+ * arrives at, giving up after `polls` polls: the kernel records the expiry in the plan's error
+ * word, every warp leaves its pipeline, the producers first wait for their own copies, and the
+ * next oem_plan_status / readout returns OEM_ERR_TIMEOUT. The fields of such a run are invalid.
+ * Nothing faults or hangs; the device and other plans stay usable. 0 (the default) = off. */
+int oem_plan_set_wait_expiry_check(oem_plan* p, int polls);
+
 /* Declare, before oem_plan_finalize, the box (i0, j0, k0, ni, nj, nk) a later
  * oem_plan_adjoint_flux_box will take gradients over. With checkpoints enabled the forward run
  * then records E of the box after every step ((steps + 1) x 3 x box floats, when that is at most

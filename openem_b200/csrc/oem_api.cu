@@ -846,6 +846,15 @@ int oem_plan_set_xchunk(oem_plan* p, int xch) {
   return OEM_OK;
 }
 
+int oem_plan_set_wait_expiry_check(oem_plan* p, int polls) {
+  int rc = check_plan(p, false);
+  if (rc) return rc;
+  if (polls < 0 || polls > (1 << 20))
+    return set_error(OEM_ERR_INVALID, "polls must be 0..2^20");
+  p->yp.expire_polls = polls;
+  return OEM_OK;
+}
+
 int oem_plan_set_gradient_box(oem_plan* p, const int* box) {
   int rc = check_plan(p, false);
   if (rc) return rc;

@@ -94,6 +94,8 @@ struct YeeParams {
   int n_coef;              // entries of pcoef
   int n_sets;              // pole sets (pset_ofs holds n_sets + 1 entries)
   int has_ade;
+  int expire_polls;        // > 0: the E update's consumers wait on a barrier nothing arrives at
+                           // for this many polls (the check of the wait-expiry path)
 };
 
 // TMA descriptors of the field tiles the pipelined kernels load (see oem_yee_tma.cu):

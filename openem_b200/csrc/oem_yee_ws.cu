@@ -114,6 +114,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
   atomicExch(err, 1);
   return false;
 }
+// A wait of the pipeline itself: gives up after `limit` polls (setting *err), or early once
+// another warp of the grid has set *err (read every 4096 polls), so one failure ends every
+// block's pipeline quickly. A producer's final drain of its own copies uses mbar_wait, which
+// waits for them whatever happened elsewhere.
+constexpr uint32_t kPolls = 1u << 20;
+__device__ __forceinline__ bool mbar_wait_live(uint64_t* bar, uint32_t parity, int* err,
+                                               uint32_t limit) {
+  for (uint32_t it = 0; it < limit; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 4095u) == 4095u && *reinterpret_cast<volatile int*>(err) != 0) return false;
+  }
+  atomicExch(err, 1);
+  return false;
+}
 __device__ __forceinline__ void tma3(void* dst, const CUtensorMap* map, uint64_t* bar, int c0,
                                      int c1, int c2) {
   asm volatile(
@@ -353,7 +367,7 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_h_ws(const __grid_con
     const PsiTile pt = psi_tile(P, j0, k0);
     for (int q = 0; q < np && ok; ++q) {
       const int slot = q % kS;
-      if (q >= kS) ok = mbar_wait(&empty[slot], (uint32_t)((q / kS - 1) & 1), err);
+      if (q >= kS) ok = mbar_wait_live(&empty[slot], (uint32_t)((q / kS - 1) & 1), err, kPolls);
       if (!ok) break;
       float* st = smem + slot * kHStage;
       const int i = ib + q;
@@ -406,7 +420,7 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_h_ws(const __grid_con
   const int to = w * kTZ + 4 * lane;  // this quad in a tile
   for (int t = 0; t < np; ++t) {
     const int slot = t % kS;
-    const bool got = mbar_wait(&full[slot], (uint32_t)((t / kS) & 1), err);
+    bool got = mbar_wait_live(&full[slot], (uint32_t)((t / kS) & 1), err, kPolls);
     if (!__all_sync(kFull, got)) break;
     const float* st = smem + slot * kHStage;
     const int i = ib + t;
@@ -519,7 +533,8 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
   extern __shared__ __align__(128) float smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kS * kEStage);
   uint64_t* empty = full + kS;
-  float* zt = reinterpret_cast<float*>(empty + kS);
+  uint64_t* never = empty + kS;  // a barrier no thread arrives at (the wait-expiry check)
+  float* zt = reinterpret_cast<float*>(empty + kS + 2);
   MatRec* smats = reinterpret_cast<MatRec*>(zt + kZTab);
   uint32_t* segt = reinterpret_cast<uint32_t*>(smats + kSmemMats);  // [plane][row][start, end]
   const int lane = threadIdx.x, w = threadIdx.y;
@@ -546,6 +561,7 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], kTY);
     }
+    mbar_init(never, 1);
     mbar_fence_init();
   }
   __syncthreads();
@@ -605,7 +621,7 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
           poff[r] = -1;  // consumers read this row's poles from global memory
         }
       }
-      if (q >= kS) ok = mbar_wait(&empty[slot], (uint32_t)((q / kS - 1) & 1), err);
+      if (q >= kS) ok = mbar_wait_live(&empty[slot], (uint32_t)((q / kS - 1) & 1), err, kPolls);
       if (!ok) break;
       float* st = smem + slot * kEStage;
       int* tab = reinterpret_cast<int*>(st + kE_PT);
@@ -673,7 +689,10 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
   const int to = w * kTZ + 4 * lane;
   for (int t = 0; t < np; ++t) {
     const int slot = t % kS;
-    const bool got = mbar_wait(&full[slot], (uint32_t)((t / kS) & 1), err);
+    bool got = mbar_wait_live(&full[slot], (uint32_t)((t / kS) & 1), err, kPolls);
+    // the plan's wait-expiry check: wait on a barrier nothing arrives at, with its short bound,
+    // so that the expiry path (error word, early exit of every warp, the producer's drain) runs
+    if (P.expire_polls > 0 && got) got = mbar_wait_live(never, 0u, err, (uint32_t)P.expire_polls);
     if (!__all_sync(kFull, got)) break;
     const float* st = smem + slot * kEStage;
     const int* tab = reinterpret_cast<const int*>(st + kE_PT);
@@ -1097,7 +1116,7 @@ __global__ void __launch_bounds__(192, 2) k_he_ws(const __grid_constant__ FusedM
     const uint32_t mbytes = (uint32_t)(kTY * kTZ * (wide ? 4 : 2));
     for (int q = 0; q < nst && ok; ++q) {
       const int slot = q % kFS;
-      if (q >= kFS) ok = mbar_wait(&empty[slot], (uint32_t)((q / kFS - 1) & 1), err);
+      if (q >= kFS) ok = mbar_wait_live(&empty[slot], (uint32_t)((q / kFS - 1) & 1), err, kPolls);
       if (!__all_sync(kFull, ok)) break;
       float* st = smem + slot * kFStage;
       const bool main = !(pre && q == 0);
@@ -1146,7 +1165,7 @@ __global__ void __launch_bounds__(192, 2) k_he_ws(const __grid_constant__ FusedM
   bool alive = true;
   for (int t = 0; t < nst; ++t) {
     const int slot = t % kFS;
-    if (alive) alive = mbar_wait(&full[slot], (uint32_t)((t / kFS) & 1), err);
+    if (alive) alive = mbar_wait_live(&full[slot], (uint32_t)((t / kFS) & 1), err, kPolls);
     alive = __all_sync(kFull, alive);
     const float* st = smem + slot * kFStage;
     const bool main = !(pre && t == 0);
@@ -1320,7 +1339,7 @@ __global__ void __launch_bounds__(192, 2) k_he_ws(const __grid_constant__ FusedM
 
 size_t ws_h_smem() { return (size_t)kS * kHStage * 4 + 2 * kS * sizeof(uint64_t) + kZTab * 4; }
 size_t ws_e_smem() {
-  return (size_t)kS * kEStage * 4 + 2 * kS * sizeof(uint64_t) + kZTab * 4 +
+  return (size_t)kS * kEStage * 4 + (2 * kS + 2) * sizeof(uint64_t) + kZTab * 4 +
          kSmemMats * sizeof(MatRec) + kXMax * kTY * 2 * sizeof(uint32_t);
 }
 

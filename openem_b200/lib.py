@@ -40,6 +40,7 @@ SIGNATURES = {
     "oem_plan_set_axis_phase": (_I, [_P, _I, _P, _P]),
     "oem_plan_add_absorber": (_I, [_P, _I, _I, _I, _P, _P]),
     "oem_plan_set_xchunk": (_I, [_P, _I]),
+    "oem_plan_set_wait_expiry_check": (_I, [_P, _I]),
     "oem_plan_enable_checkpoints": (_I, [_P, _I]),
     "oem_plan_set_gradient_box": (_I, [_P, _P]),
     "oem_plan_add_tensor": (_I, [_P, _I, _P, _P, _P, _P, _P]),

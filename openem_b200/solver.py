@@ -86,9 +86,10 @@ class Plan:
 
     def __init__(self, sc, n_total: int | None = None, device: int = 0, stream=None,
                  batch: int | None = None, cplx: bool = False, xchunk: int = 0,
-                 checkpoint_every: int = 0, gradient_box=None):
+                 checkpoint_every: int = 0, gradient_box=None, wait_expiry_polls: int = 0):
         self.cplx = bool(cplx)
         self.xchunk = int(xchunk)
+        self.wait_expiry_polls = int(wait_expiry_polls)
         self.checkpoint_every = int(checkpoint_every)
         self.gradient_box = None if gradient_box is None else \
             np.ascontiguousarray(gradient_box, dtype=np.int32)
@@ -126,6 +127,17 @@ class Plan:
             return True
         return int(np.prod(self.shape)) >= 100_000 and tables_gpu.available()
 
+    @staticmethod
+    def _warn_nonfinite_materials(table) -> None:
+        """The deduplicated material records hold ca, cb and eps of every distinct cell: a NaN
+        or Inf in eps or sigma shows here at no cost. Like OpenEM (openem/solver.py:347-370)
+        the run goes ahead and the readout warns again; this names the cause up front."""
+        coef = np.ascontiguousarray(table, dtype=np.uint32)[:, :9].view(np.float32)
+        if not np.isfinite(coef).all():
+            print("[openem_b200] warning: eps or sigma holds non-finite values (NaN/Inf): the "
+                  "update coefficients of some cells are not finite and the fields will diverge",
+                  flush=True)
+
     def _arr(self, a, dtype):
         a = np.ascontiguousarray(a, dtype=dtype)
         self._keep.append(a)
@@ -161,6 +173,7 @@ class Plan:
                                   (sc.eps_ex, sc.eps_ey, sc.eps_ez))
             self.h2d_bytes += sum(np.asarray(a).nbytes for a in
                                   (sc.sigma_ex, sc.sigma_ey, sc.sigma_ez) if a is not None)
+            self._warn_nonfinite_materials(mt.table)
             L.check(lib.oem_plan_set_materials_device(
                 h, int(mt.n_mat), L.ptr(self._arr(mt.table, np.uint32)), int(mt.index_bytes),
                 C.c_void_p(mt.index.data_ptr())), "set_materials_device")
@@ -175,6 +188,7 @@ class Plan:
             table, index, n_mat = mt.table, mt.index, mt.n_mat
             if mod is not None:
                 table, index, n_mat = T.isolate_cells(table, index, mod["cell"])
+            self._warn_nonfinite_materials(table)
             L.check(lib.oem_plan_set_materials(h, int(n_mat),
                                                L.ptr(self._arr(table, np.uint32)),
                                                int(index.dtype.itemsize),
@@ -305,6 +319,9 @@ class Plan:
                 self.ft_mons.append((m, mid.value))
         if self.xchunk:
             L.check(lib.oem_plan_set_xchunk(h, self.xchunk), "set_xchunk")
+        if self.wait_expiry_polls:
+            L.check(lib.oem_plan_set_wait_expiry_check(h, self.wait_expiry_polls),
+                    "set_wait_expiry_check")
         if self.checkpoint_every:
             L.check(lib.oem_plan_enable_checkpoints(h, self.checkpoint_every), "checkpoints")
         if self.gradient_box is not None:

@@ -375,3 +375,20 @@ def test_tensor_tables_and_passthrough():
     for c in range(3):
         cells = np.asarray(ten.cell)[np.asarray(ten.comp) == c]
         assert np.all(ca[c].ravel()[cells] == 0.0) and np.all(cb[c].ravel()[cells] == 1.0)
+
+
+def test_nonfinite_material_coefficients_are_named(capsys):
+    """A NaN in eps reaches the deduplicated material records (ca, cb, eps); the plan names it
+    at set-up from that small table, before any device work."""
+    from dataclasses import replace
+    from openem_b200 import tables as T
+    from openem_b200.solver import Plan
+    sc = scenes.small_dispersive(n=20, n_sph=2, num_steps=10, n_pml=6, nfreq=2)
+    tabs = [T.axis_tables(sc, a) for a in range(3)]
+    Plan._warn_nonfinite_materials(T.material_tables(sc, tabs).table)
+    assert capsys.readouterr().out == ""
+    eps = np.array(sc.eps_ey)
+    eps[3, 4, 5] = np.inf
+    bad = replace(sc, eps_ey=eps)
+    Plan._warn_nonfinite_materials(T.material_tables(bad, [T.axis_tables(bad, a) for a in range(3)]).table)
+    assert "non-finite" in capsys.readouterr().out
