@@ -8,8 +8,9 @@ so OpenEM's notebook backend reads this engine's outputs unchanged.
 steps run, shutoff, stop reason, wall time, source end, energy trace).
 
 In-process: :func:`solve_dir`; as a subprocess: ``python -m openem_b200.solve_worker <work>
-<out> [--steps N]``. A work directory that asks for the Tidy3D-convention readout
-(``td_coords.npz``) is refused: that readout is not built here.
+<out> [--steps N]``. When the work directory holds ``td_coords.npz`` (target coordinates of the
+field monitors in Tidy3D's convention), ``ours.npz`` also carries the ``tdf:`` / ``tdc:`` entries
+of :func:`openem_b200.td_convention.to_tidy3d`, as OpenEM's worker writes them.
 """
 
 from __future__ import annotations
@@ -67,13 +68,16 @@ def solve_dir(work, out, steps: int | None = None) -> pathlib.Path:
     """Solve ``work/scene.npz`` (with the shutoff unless ``steps`` is given), write
     ``out/ours.npz`` and return its path."""
     work, out = pathlib.Path(work), pathlib.Path(out)
-    if (work / "td_coords.npz").exists():
-        raise NotImplementedError("the Tidy3D-convention field readout (td_coords.npz) is not "
-                                  "built in this engine")
     out.mkdir(parents=True, exist_ok=True)
     sc = serialize.load(work / "scene.npz")
     res = solver.run(sc, num_steps=steps, use_shutoff=steps is None, verbose=True)
-    mb = save_result(res, out / "ours.npz")
+    extra = {}
+    coords = work / "td_coords.npz"
+    if coords.exists() and res.field_phasors:
+        from openem_b200 import td_convention
+        with np.load(coords) as z:
+            extra = td_convention.to_tidy3d(sc, res.field_phasors, {k: z[k] for k in z.files})
+    mb = save_result(res, out / "ours.npz", extra=extra)
     print(f"SOLVE|{work.name}|{res.steps_run}|{int(res.shutoff_triggered)}|"
           f"{res.stop_reason or '-'}|{int(np.prod(sc.shape))}|{res.wall_seconds:.1f}|{mb:.1f}",
           flush=True)

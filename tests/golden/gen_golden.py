@@ -11,6 +11,8 @@ Outputs (all small):
     ref_tables.npz     CPML coefficients, axis index tables, dual spacings, apodisation windows,
                        plane flux of fixed phasors
     ref_tfsf1d.npz     the 1D Yee line with one-face injection (lossless slab and lossy profile)
+    ref_postprocess.npz  Tidy3D-convention divisors per source type, colocation and the field
+                       readout (openem.normalize, openem.colocate, openem.td_readout)
     ref_shutoff.npz    early-termination decisions on two fixed metric sequences (the decay
                        tests fire; the flux test fires while the energy decays slowly)
     ref_scene_slab.npz, ref_scene_disp.npz   scene.npz files written by OpenEM's serializer
@@ -34,6 +36,9 @@ sys.path.insert(0, str(ROOT))
 sys.path.insert(0, SRC)
 
 import openem.apodization as r_apod  # noqa: E402
+import openem.colocate as r_coloc  # noqa: E402
+import openem.normalize as r_norm  # noqa: E402
+import openem.td_readout as r_tdr  # noqa: E402
 import openem.cpml as r_cpml  # noqa: E402
 import openem.flux as r_flux  # noqa: E402
 import openem.grid as r_grid  # noqa: E402
@@ -167,6 +172,64 @@ def gen_shutoff(out: dict) -> None:
     _shutoff_sequence(steps, e2, energy, flux, "b_", out)
 
 
+def post_scenes():
+    """One scene per normalising source type, built by the engine's scene factory."""
+    return {
+        "dip": scenes.small_dispersive(n=20, n_sph=2, num_steps=300, n_pml=6, nfreq=3),
+        "pw": scenes.slab_plane_wave(nxy=3, num_steps=600),
+        "mode": scenes.bloch_metasurface(nx=8, ny=8, nz=64, n_pml=8, npix=2, layer_cells=8,
+                                         nfreq=5, num_steps=400, bloch_k=(0.05, 0.0, 0.0)),
+        "tfsf": scenes.tfsf_box_scene(n=24, n_pml=6, num_steps=300),
+    }
+
+
+def gen_postprocess(out: dict) -> None:
+    rng = np.random.default_rng(17)
+    for tag, sc in post_scenes().items():
+        rsc = to_ref(sc)
+        freqs = np.linspace(1.5e14, 3.5e14, 7)
+        out[f"{tag}_freqs"] = freqs
+        out[f"{tag}_D"] = r_norm.norm_spectrum(rsc, freqs)
+        out[f"{tag}_field"] = r_norm.field_norm(rsc, freqs)
+        out[f"{tag}_flux"] = r_norm.flux_norm(rsc, freqs)
+        if tag == "pw":
+            m = rsc.flux_monitors[0]
+            out["pw_bg"] = np.array(r_norm.background_index(rsc))
+            out["pw_area"] = np.array(r_norm.monitor_area(rsc, m))
+            out["pw_plane_div"] = r_norm.plane_flux_divisor(rsc, m, freqs)
+            pulse = GaussianPulse(freq0=2.998e14, fwidth=0.2 * 2.998e14)
+            out["pw_tscale"] = np.array(r_norm.time_scale(rsc, pulse, sc.dt, 600))
+    # colocation of random data from Yee positions to primal edges (and a single-point axis)
+    sc = post_scenes()["dip"]
+    rsc = to_ref(sc)
+    origin, box = (3, 4, 5), (6, 5, 4)
+    data = rng.standard_normal((2, 6, 5, 4)) + 1j * rng.standard_normal((2, 6, 5, 4))
+    out["col_data"] = data
+    for comp in ("Ex", "Hy", "Ez"):
+        src = r_coloc.sample_coords(rsc.grid, origin, box, comp)
+        dst = [np.asarray(rsc.grid.axes[a].edges)[origin[a]:origin[a] + box[a]] for a in range(3)]
+        dst[2] = dst[2][1:2]
+        out[f"col_{comp}"] = r_coloc.interp_to(data, src, dst)
+    out["col_snap"] = np.array([r_coloc.snap_floor(rsc.grid.axes[0].edges, c, 1e-15)
+                                for c in (-1e-6, 0.0, 3.3e-8, 1e-3)])
+    # the field readout of the dipole scene's mid-plane monitor with primal-edge targets
+    m = rsc.field_monitors[0]
+    nf = int(np.size(m.freqs))
+    raw = (rng.standard_normal((6, nf) + tuple(m.box))
+           + 1j * rng.standard_normal((6, nf) + tuple(m.box)))
+    plans = {}
+    for comp in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        for a, ax in enumerate("xyz"):
+            e = np.asarray(rsc.grid.axes[a].edges)[m.origin[a]:m.origin[a] + m.box[a]] / 1e-6
+            plans[f"{m.name}|{comp}:{ax}"] = e if m.box[a] > 2 else e[:1]
+    fin = r_tdr.finalize(rsc, {m.name: raw}, plans)
+    out["tdr_raw"] = raw
+    for k, v in plans.items():
+        out["plan|" + k] = v
+    for k, v in fin.items():
+        out["fin|" + k] = v
+
+
 def main(which) -> None:
     if "tables" in which:
         d: dict = {}
@@ -180,6 +243,10 @@ def main(which) -> None:
         d = {}
         gen_shutoff(d)
         np.savez_compressed(HERE / "ref_shutoff.npz", **d)
+    if "postprocess" in which:
+        d = {}
+        gen_postprocess(d)
+        np.savez_compressed(HERE / "ref_postprocess.npz", **d)
     if "scenes" in which:
         slab = scenes.slab_plane_wave(nxy=2, num_steps=400)
         r_ser.save(to_ref(slab), HERE / "ref_scene_slab.npz")
@@ -191,4 +258,4 @@ def main(which) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ("tables", "tfsf1d", "shutoff", "scenes"))
+    main(sys.argv[1:] or ("tables", "tfsf1d", "shutoff", "postprocess", "scenes"))

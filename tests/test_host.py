@@ -325,9 +325,13 @@ def test_ours_npz_round_trip(tmp_path, monkeypatch):
     monkeypatch.setenv("OPENEM_OUT_MAX_GB", "1e-9")
     assert solve_worker.save_result(res, tmp_path / "big.npz") < 0
     assert (tmp_path / "big.TOOBIG").exists() and not (tmp_path / "big.npz").exists()
-    (tmp_path / "td_coords.npz").write_bytes(b"")
-    with pytest.raises(NotImplementedError):
-        solve_worker.solve_dir(tmp_path, tmp_path / "out")
+    # extra entries (the Tidy3D-convention readout) travel next to the solver's own keys
+    monkeypatch.setenv("OPENEM_OUT_MAX_GB", "20")
+    mb = solve_worker.save_result(res, tmp_path / "extra.npz",
+                                  extra={"tdf:box|Ex": np.ones((2, 1, 1, 3), complex)})
+    assert mb > 0
+    with np.load(tmp_path / "extra.npz") as z:
+        assert "tdf:box|Ex" in z.files and "__meta" in z.files
 
 
 def test_mix_tables_and_passthrough():
