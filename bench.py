@@ -394,6 +394,28 @@ def run_bloch_line(args):
     dist_done(world)
 
 
+def run_serve_line(args):
+    """The serving stream (``openem_b200.serve.measure_stream``): ``--requests`` requests of the
+    N^3 stream, served with continuous batching against the same requests run serially; one
+    replica per rank."""
+    world, rank, local = dist_setup(args.gpus)
+    from openem_b200 import serve
+    m = serve.measure_stream(args.requests, device=local)
+    value = reduce_max(-m["sims_per_s"], world)  # the slowest replica sets the whole job
+    if rank == 0:
+        line = {"metric": "served sims/s", "value": -value * world, "unit": "sims/s",
+                "n_gpus": world, "steps": m["requests"], "warmup": 1,
+                "ms_per_step": 1e3 * m["serve_seconds"] / m["requests"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded request stream)",
+                "config": {"workload": "serving stream: N^3 grids, N log-uniform in [64, 384], "
+                                       "1000-6000 steps, Poisson arrivals at 1.2x the serial "
+                                       "capacity", **m},
+                "cpu_baseline": None, "e2e": None, "gpu_launches": None, "clocks": None}
+        print(json.dumps(line), flush=True)
+    dist_done(world)
+
+
 def run_ours(args):
     world, rank, local = dist_setup(args.gpus)
     import torch
@@ -519,7 +541,8 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="bulk", choices=["bulk", "bloch"])
+    ap.add_argument("--workload", default="bulk", choices=["bulk", "bloch", "serve"])
+    ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--ref-size", type=int, default=128)
     ap.add_argument("--cpu-size", type=int, default=128)
@@ -535,6 +558,8 @@ def main():
         run_reference(args)
     elif args.workload == "bloch":
         run_bloch_line(args)
+    elif args.workload == "serve":
+        run_serve_line(args)
     else:
         run_ours(args)
 

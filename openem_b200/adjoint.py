@@ -51,8 +51,8 @@ class FluxGradient:
 
 
 def _refuse(sc) -> None:
-    if sc.any_dispersion or getattr(sc, "any_dispersion_mix", False):
-        raise NotImplementedError("the adjoint covers non-dispersive scenes")
+    if getattr(sc, "dispersion_mix", None) is not None and sc.dispersion_mix.n_entry > 0:
+        raise NotImplementedError("the adjoint does not cover slanted-interface mixed media")
     if sc.absorbers:
         raise NotImplementedError("the adjoint does not cover absorber slabs")
     if (sc.tensor is not None and sc.tensor.n_entry) or \

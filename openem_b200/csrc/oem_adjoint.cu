@@ -18,6 +18,13 @@
 // source), dJ/dca = sum_n lambda_E^{n+1} E^n and dJ/dcb = sum_n lambda_E^{n+1} T^n per
 // component and cell, accumulated in float64.
 //
+// Dispersive cells. The pole pass of step n (oem_arith.cuh ade_pole, per pole of a component)
+//   p = s + B E^n,  d = (A - 1) p + B E^n,  s' = p + d,  J = sum 2 Re(d)
+// feeds E^{n+1} = ... - cb cw J. Its transpose, with the adjoint pole state lambda_s (complex,
+// zero after the last step since the states are no output) and lambda_J = -cb cw lambda_E^{n+1}:
+//   lambda_d = lambda_s + 2 lambda_J (real part),  lambda_p = lambda_s + conj(A - 1) lambda_d,
+//   lambda_E^n += Re(conj(B) (lambda_d + lambda_p)),  lambda_s <- lambda_p.
+//
 // The transposed differences are gathers (one thread per cell): a cell receives its own term
 // and the terms of the cells whose neighbour it is; at a clamped wall or a PMC / symmetry plane a
 // cell can be its own neighbour, so the inverse neighbour relation is checked explicitly.
@@ -180,8 +187,21 @@ __global__ void __launch_bounds__(128) k_adj_ka(YeeParams P, AdjState S, const f
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
-  if (k >= P.nz || j >= P.ny) return;
+  if (j >= P.ny) return;  // warp-uniform: a warp is one aligned 32-cell z segment of a row
   const int64_t id = ((int64_t)i * P.ny + j) * P.nzp + k;
+  // first pole of this cell: the segment's offset plus the poles of the lanes before it (the
+  // padding cells past nz hold the pole-free material 0)
+  uint32_t poff = 0;
+  if (S.lps) {
+    const MatRec& Mp = P.mats[mat_of(P, id)];
+    const int npc = Mp.np[0] + Mp.np[1] + Mp.np[2];
+    const unsigned lt = (1u << (threadIdx.x & 31)) - 1u;
+    int pre = 0;
+#pragma unroll
+    for (int b = 0; b < 6; ++b) pre += __popc(__ballot_sync(0xffffffffu, (npc >> b) & 1) & lt) << b;
+    poff = P.seg_ofs[id >> 5] + (uint32_t)pre;
+  }
+  if (k >= P.nz) return;
   // Ez: Hx y-term (0), Hy x-term (3); Ey: Hx z-term (1), Hz x-term (4); Ex: Hy z-term (2),
   // Hz y-term (5)
   float lam[3];
@@ -215,7 +235,22 @@ __global__ void __launch_bounds__(128) k_adj_ka(YeeParams P, AdjState S, const f
                                  P.ny, P.nzp);
     S.dbare[2 * c + 1][id] = dbar_of(sb, S.lpsie, ab, sl_b[c], Ab, Ab.ae, Ab.be, Ab.ke, qb, i,
                                      j, k, P.ny, P.nzp);
-    S.lam[c][id] = ca * lam[c];
+    float lam_n = ca * lam[c];
+    if (S.lps && M.np[c] > 0) {  // the transposed pole pass of this component
+      const float lj = -cb * P.cw * lam[c];
+      const float4* cf = P.pcoef + P.pset_ofs[M.pset[c]];
+      for (int t = 0; t < M.np[c]; ++t) {
+        const float4 q = cf[t];  // (Re(A-1), Im(A-1), Re B, Im B)
+        float2& ls = S.lps[poff + t];
+        const float ldr = ls.x + 2.0f * lj, ldi = ls.y;
+        const float lpr = ls.x + (q.x * ldr + q.y * ldi);
+        const float lpi = ls.y + (q.x * ldi - q.y * ldr);
+        lam_n += q.z * (ldr + lpr) + q.w * (ldi + lpi);
+        ls = make_float2(lpr, lpi);
+      }
+    }
+    if (S.lps) poff += (uint32_t)M.np[c];
+    S.lam[c][id] = lam_n;
   }
 }
 

@@ -442,6 +442,10 @@ static void state_arrays(oem_plan* p, std::vector<std::pair<float*, size_t>>& v)
       }
     }
   }
+  // ADE pole states (a segment recomputed from a checkpoint needs them; the pole currents are
+  // recomputed from them)
+  if (p->yp.P && p->n_pole_total > 0)
+    v.push_back({reinterpret_cast<float*>(p->yp.P), 2 * (size_t)p->n_pole_total});
 }
 
 static int save_state(oem_plan* p, int slot, cudaStream_t s) {
@@ -896,11 +900,11 @@ int oem_plan_adjoint_flux_box(oem_plan* p, int mon_id, const double* weights, co
   if (p->mons[mon_id].n_total < p->n_total)
     return set_error(OEM_ERR_INVALID, "the monitor's phase table is shorter than the run");
   if (!weights || !dA1 || !dA2 || !g_ca || !g_cb) return set_error(OEM_ERR_INVALID, "null argument");
-  if (p->is_complex || p->yp.has_ade || !p->absorbers.empty() || !p->mixes.empty() ||
-      !p->tensors.empty() || !p->mods.empty())
+  if (p->is_complex || !p->absorbers.empty() || !p->mixes.empty() || !p->tensors.empty() ||
+      !p->mods.empty())
     return set_error(OEM_ERR_UNSUPPORTED,
-                     "the adjoint covers real, non-dispersive plans without absorbers, tensor "
-                     "media or time modulation");
+                     "the adjoint covers real plans without absorbers, mixed or tensor media or "
+                     "time modulation");
   for (int64_t q = 0; q < (int64_t)p->ckpt.size(); ++q)
     if (p->ckpt_step[q] != q * p->ckpt_k) return set_error(OEM_ERR_STATE, "missing checkpoint");
   if ((rc = use_device(p))) return rc;
@@ -961,6 +965,7 @@ int oem_plan_adjoint_flux_box(oem_plan* p, int mon_id, const double* weights, co
   for (int c = 0; c < 6 && !rc; ++c) rc = alloc(&S.dbarh[c], ncp);
   for (int c = 0; c < 3 && !rc; ++c) rc = alloc(&S.gca[c], nb);
   for (int c = 0; c < 3 && !rc; ++c) rc = alloc(&S.gcb[c], nb);
+  if (!rc && p->yp.has_ade) rc = alloc(&S.lps, (size_t)std::max<int64_t>(p->n_pole_total, 1));
   for (int a = 0; a < 3 && !rc; ++a)
     for (int side = 0; side < 2 && !rc; ++side) {
       const int L = side == 0 ? p->axh[a].lo : p->axh[a].hi;
@@ -1497,17 +1502,6 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   for (int a = 0; a < 3; ++a)
     if ((rc = upload_axis(p, a))) return rc;
   if ((rc = alloc_psi(p))) return rc;
-  if (p->ckpt_k > 0) {
-    std::vector<std::pair<float*, size_t>> v;
-    state_arrays(p, v);
-    p->ckpt_floats = 0;
-    for (auto& a : v) p->ckpt_floats += a.second;
-    const int64_t nslot = (n_total + p->ckpt_k - 1) / p->ckpt_k;
-    p->ckpt.assign((size_t)std::max<int64_t>(nslot, 1), nullptr);
-    p->ckpt_step.assign(p->ckpt.size(), -1);
-    for (float*& b : p->ckpt)
-      if ((rc = dalloc(p, &b, p->ckpt_floats, false))) return rc;
-  }
   // materials: table with the padding material at 0, padded index shifted by one
   MatRec* dm;
   if ((rc = dupload(p, &dm, p->mats.data(), p->mats.size()))) return rc;
@@ -1595,6 +1589,17 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
       OEM_CUDA(cudaStreamSynchronize(0));
     }
     P.has_ade = 1;
+  }
+  if (p->ckpt_k > 0) {  // fields, psi and pole states of every K-th step
+    std::vector<std::pair<float*, size_t>> v;
+    state_arrays(p, v);
+    p->ckpt_floats = 0;
+    for (auto& a : v) p->ckpt_floats += a.second;
+    const int64_t nslot = (n_total + p->ckpt_k - 1) / p->ckpt_k;
+    p->ckpt.assign((size_t)std::max<int64_t>(nslot, 1), nullptr);
+    p->ckpt_step.assign(p->ckpt.size(), -1);
+    for (float*& b : p->ckpt)
+      if ((rc = dalloc(p, &b, p->ckpt_floats, false))) return rc;
   }
   if ((rc = dalloc(p, &p->d_step, 1))) return rc;
   if (p->gbox_set && p->ckpt_k > 0 && !p->is_complex) {

@@ -496,6 +496,7 @@ struct AdjState {
   int box[6];         // gradient box: i0, j0, k0, ni, nj, nk
   double* gca[3];     // per box cell: sum over steps of lambda_E^{n+1} E^n
   double* gcb[3];     // sum over steps of lambda_E^{n+1} T^n, T^n = (E^{n+1} - ca E^n) / cb
+  float2* lps;        // adjoint of the ADE pole states (pole-indexed), nullptr without poles
 };
 struct AdjFlux {      // objective sources of one flux plane (see oem_adjoint.cu)
   int axis, km, n1, n2, nf;

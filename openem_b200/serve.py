@@ -15,11 +15,13 @@ and the server builds every plan of that class with the winner.
 
 Each request's result is exactly what it would be alone: plans share nothing but the device.
 
-    python -m openem_b200.serve --requests 48 --min-n 48 --max-n 192 --min-steps 500 \\
-        --max-steps 1500 --load 4.0
+    python -m openem_b200.serve [--requests 256 --min-n 64 --max-n 384 --min-steps 1000
+                                 --max-steps 6000 --load 1.2]
 
-prints one JSON line with sims/s and p50/p99 latency of the served stream against the same
-requests run one at a time through :func:`openem_b200.solver.run`.
+(the defaults are the 256-request stream with N^3 grids, N log-uniform in [64, 384], 1000 to
+6000 steps) prints one JSON line with sims/s and p50/p99 latency of the served stream against the
+same requests run one at a time through :func:`openem_b200.solver.run`, and whether every served
+result equals the serial one bit for bit. Scenes are built when their request is admitted.
 """
 
 from __future__ import annotations
@@ -38,10 +40,25 @@ from openem_b200.results import Result
 
 @dataclass
 class Request:
+    """A simulation to serve. ``scene`` is a ``Scene``, or a callable that builds it: a stream of
+    large requests then holds only the requests in flight on the host, each built on a plan
+    worker when admitted. ``footprint`` (bytes) is the admission estimate; by default it is
+    computed from the scene."""
+
     rid: int
     scene: object
     num_steps: int
     arrival: float = 0.0  # seconds after the start of serving
+    footprint: int | None = None
+
+    def build(self):
+        """The request's Scene (built on each call when ``scene`` is a factory)."""
+        return self.scene() if callable(self.scene) else self.scene
+
+    def need(self) -> int:
+        if self.footprint is None:
+            self.footprint = footprint(self.build(), self.num_steps)
+        return int(self.footprint)
 
 
 @dataclass
@@ -87,10 +104,12 @@ class Tuner:
     CPML on all faces, timed over ``steps`` steps per candidate with CUDA events."""
 
     def __init__(self, device: int = 0, candidates=(8, 16, 32, 64), steps: int = 30):
+        import threading
         self.device = int(device)
         self.candidates = tuple(int(c) for c in candidates)
         self.steps = int(steps)
         self.cache: dict = {}
+        self._lock = threading.Lock()  # plan workers tune one class at a time
 
     @staticmethod
     def size_class(sc) -> tuple:
@@ -99,9 +118,10 @@ class Tuner:
 
     def xchunk(self, sc) -> int:
         key = self.size_class(sc)
-        if key not in self.cache:
-            self.cache[key] = self._tune(sc)
-        return self.cache[key]
+        with self._lock:
+            if key not in self.cache:
+                self.cache[key] = self._tune(sc)
+            return self.cache[key]
 
     def _tune(self, sc) -> int:
         from dataclasses import replace
@@ -128,8 +148,9 @@ class Tuner:
 
 
 def _plan_factory(req: Request, device: int, stream, tuner: Tuner | None):
-    xch = tuner.xchunk(req.scene) if tuner is not None else 0
-    return solver.Plan(req.scene, req.num_steps, device=device, stream=stream, xchunk=xch)
+    sc = req.build()
+    xch = tuner.xchunk(sc) if tuner is not None else 0
+    return solver.Plan(sc, req.num_steps, device=device, stream=stream, xchunk=xch)
 
 
 class Server:
@@ -141,8 +162,9 @@ class Server:
     def __init__(self, device: int = 0, max_slots: int = 16, mem_budget: int | None = None,
                  chunk: int = 256, tuner: Tuner | None = None, plan_factory=None,
                  clock=time.perf_counter, stream_factory=None, event_factory=None,
-                 build_workers: int = 4):
+                 build_workers: int = 4, keep=None):
         self.device = int(device)
+        self.keep = keep  # applied to each Result as it completes (None: keep the Result)
         self.build_workers = int(build_workers)
         self.max_slots = int(max_slots)
         self.chunk = int(chunk)
@@ -198,7 +220,7 @@ class Server:
             # admission: arrived requests, while a slot and the memory budget allow
             while pending and pending[0].arrival <= now and len(active) < self.max_slots:
                 req = pending[0]
-                need = footprint(req.scene, req.num_steps)
+                need = req.need()
                 if used + dead_bytes + need > self.mem_budget and graveyard:
                     for p in graveyard:
                         p.close()
@@ -232,6 +254,8 @@ class Server:
                     progressed = True
                     continue
                 res = self._readout(ent)
+                if self.keep is not None:
+                    res = self.keep(res)
                 fin = self.clock() - t0
                 done.append(Done(req.rid, res, req.arrival, ent["start"], fin))
                 self.log.append((fin, "done", req.rid))
@@ -271,32 +295,68 @@ class Server:
                       time_samples=tsamp, time_slots=tslots)
 
 
-def serial(requests, device: int = 0) -> list:
+def serial(requests, device: int = 0, keep=None) -> list:
     """The same requests one at a time through the plain engine (``solver.run``), back to back
-    from t = 0; returns Done records with the serial completion times."""
+    from t = 0, each scene built just before its run; returns Done records with the serial
+    completion times. ``keep`` (a function of the Result) replaces each Result by what it
+    returns, so that a long stream need not hold every result."""
     import torch
     out = []
     t0 = time.perf_counter()
     for req in sorted(requests, key=lambda r: r.rid):
         start = time.perf_counter() - t0
-        res = solver.run(req.scene, num_steps=req.num_steps, use_shutoff=False, verbose=False,
+        res = solver.run(req.build(), num_steps=req.num_steps, use_shutoff=False, verbose=False,
                          device=device)
         torch.cuda.synchronize(device)
-        out.append(Done(req.rid, res, 0.0, start, time.perf_counter() - t0))
+        out.append(Done(req.rid, keep(res) if keep else res, 0.0, start,
+                        time.perf_counter() - t0))
     return out
 
 
+def stream_footprint(n: int, num_steps: int, max_freqs: int = 32) -> int:
+    """Admission estimate of a serving request before its scene exists: fields and index of an
+    n^3 grid, CPML psi of 12-layer slabs, two poles per component in half the cells, one flux
+    plane at ``max_freqs`` frequencies."""
+    nzp = (n + 31) // 32 * 32
+    ncp = n * n * nzp
+    b = 26 * ncp + 3 * 16 * 2 * min(12, max(4, n // 8)) * n * nzp
+    b += 12 * 2 * 3 * ncp // 2 + ncp // 8
+    b += 32 * 4 * 4 * n * n + 2 * 4 * max_freqs * n * n * 8 + num_steps * max_freqs * 16
+    return int(b + (32 << 20))
+
+
 def make_stream(n_requests: int, seed: int = 3, n_range=(64, 384), step_range=(1000, 6000)):
-    """The request stream: N log-uniform in ``n_range``, steps uniform in ``step_range``, each
-    scene from :func:`openem_b200.scenes.serving_request` (seeded)."""
+    """The request stream: N log-uniform in ``n_range``, steps uniform in ``step_range``
+    (``numpy.random.default_rng(seed)``), each scene from
+    :func:`openem_b200.scenes.serving_request` with its own generator
+    ``default_rng([seed, rid])``, built when the request is admitted."""
+    from functools import partial
+
     from openem_b200 import scenes
     rng = np.random.default_rng(seed)
     reqs = []
     for q in range(n_requests):
         n = int(round(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1])))))
         steps = int(rng.integers(step_range[0], step_range[1] + 1))
-        reqs.append(Request(q, scenes.serving_request(n, rng, steps), steps))
+        build = partial(_stream_scene, n, seed, q, steps)
+        reqs.append(Request(q, build, steps, footprint=stream_footprint(n, steps)))
     return reqs
+
+
+def _stream_scene(n: int, seed: int, rid: int, steps: int):
+    from openem_b200 import scenes
+    return scenes.serving_request(n, np.random.default_rng([seed, rid]), steps)
+
+
+def digest(res) -> str:
+    """A bit-exact fingerprint of a Result's flux phasors (served and serial runs compare
+    these instead of holding every phasor array)."""
+    import hashlib
+    h = hashlib.sha1()
+    for name in sorted(res.phasors):
+        h.update(name.encode())
+        h.update(np.ascontiguousarray(res.phasors[name].data).tobytes())
+    return h.hexdigest()
 
 
 def poisson_arrivals(requests, rate: float, seed: int = 3) -> None:
@@ -313,52 +373,59 @@ def _percentiles(lat):
     return float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
 
 
+def measure_stream(n_requests: int = 256, seed: int = 3, n_range=(64, 384),
+                   step_range=(1000, 6000), load: float = 1.2, slots: int = 16,
+                   workers: int = 4, tune: bool = False, device: int = 0) -> dict:
+    """Serve a stream and run the same requests serially on the plain engine: sims/s of both,
+    p50 / p99 latency, and whether every served result equals its serial one bit for bit
+    (compared through :func:`digest`). ``load`` is the offered Poisson arrival rate as a multiple
+    of the serial capacity measured first."""
+    import torch
+    torch.cuda.set_device(device)
+    reqs = make_stream(n_requests, seed, n_range, step_range)
+    tuner = Tuner(device) if tune else None
+    # warm-up: the library and a first graph capture
+    solver.run(reqs[0].build(), num_steps=10, use_shutoff=False, verbose=False, device=device)
+    ser = serial(reqs, device, keep=digest)
+    t_ser = ser[-1].finish
+    rate = load * len(reqs) / t_ser
+    poisson_arrivals(reqs, rate, seed)
+    srv = Server(device, max_slots=slots, tuner=tuner, build_workers=workers, keep=digest)
+    got = srv.serve(reqs)
+    t_srv = max(d.finish for d in got) - min(r.arrival for r in reqs)
+    same = all(g.result == s.result for g, s in zip(got, ser))
+    p50, p99 = _percentiles([d.latency for d in got])
+    s50, s99 = _percentiles([d.finish for d in ser])
+    return {
+        "metric": "served sims/s", "requests": len(reqs),
+        "sims_per_s": len(reqs) / t_srv, "serial_sims_per_s": len(reqs) / t_ser,
+        "ratio": t_ser / t_srv, "serve_seconds": t_srv, "serial_seconds": t_ser,
+        "p50_latency_s": p50, "p99_latency_s": p99,
+        "serial_p50_completion_s": s50, "serial_p99_completion_s": s99,
+        "offered_load_x_serial": load, "arrival_rate_per_s": rate,
+        "identical_to_alone": bool(same),
+        "config": {"n_range": list(n_range), "step_range": list(step_range), "slots": slots,
+                   "build_workers": workers, "seed": seed, "tuned": bool(tune)}}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--requests", type=int, default=48)
-    ap.add_argument("--min-n", type=int, default=48)
-    ap.add_argument("--max-n", type=int, default=192)
-    ap.add_argument("--min-steps", type=int, default=500)
-    ap.add_argument("--max-steps", type=int, default=1500)
-    ap.add_argument("--load", type=float, default=4.0,
+    ap.add_argument("--requests", type=int, default=256)
+    ap.add_argument("--min-n", type=int, default=64)
+    ap.add_argument("--max-n", type=int, default=384)
+    ap.add_argument("--min-steps", type=int, default=1000)
+    ap.add_argument("--max-steps", type=int, default=6000)
+    ap.add_argument("--load", type=float, default=1.2,
                     help="offered load as a multiple of the serial capacity")
     ap.add_argument("--slots", type=int, default=16)
     ap.add_argument("--workers", type=int, default=4, help="plan-building threads")
+    ap.add_argument("--tune", action="store_true", help="time the x-chunk per grid size")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--device", type=int, default=0)
     a = ap.parse_args()
-    import torch
-    torch.cuda.set_device(a.device)
-    reqs = make_stream(a.requests, a.seed, (a.min_n, a.max_n), (a.min_steps, a.max_steps))
-    # warm-up: the library, the first graph capture and the tuner's probes
-    tuner = Tuner(a.device)
-    for r in reqs:
-        tuner.xchunk(r.scene)
-    solver.run(reqs[0].scene, num_steps=10, use_shutoff=False, verbose=False, device=a.device)
-    ser = serial(reqs, a.device)
-    t_ser = ser[-1].finish
-    rate = a.load * len(reqs) / t_ser
-    poisson_arrivals(reqs, rate, a.seed)
-    srv = Server(a.device, max_slots=a.slots, tuner=tuner, build_workers=a.workers)
-    got = srv.serve(reqs)
-    t_srv = max(d.finish for d in got) - min(r.arrival for r in reqs)
-    same = all(np.array_equal(g.result.phasors["T"].data, s.result.phasors["T"].data)
-               for g, s in zip(got, ser))
-    p50, p99 = _percentiles([d.latency for d in got])
-    s50, s99 = _percentiles([d.finish for d in ser])
-    cells = sum(int(np.prod(r.scene.shape)) * r.num_steps for r in reqs)
-    print(json.dumps({
-        "metric": "served sims/s", "requests": len(reqs),
-        "sims_per_s": len(reqs) / t_srv, "serial_sims_per_s": len(reqs) / t_ser,
-        "ratio": t_ser / t_srv, "p50_latency_s": p50, "p99_latency_s": p99,
-        "serial_p50_completion_s": s50, "serial_p99_completion_s": s99,
-        "offered_load_x_serial": a.load, "arrival_rate_per_s": rate,
-        "gcell_updates": cells / 1e9, "identical_to_alone": bool(same),
-        "config": {"n_range": [a.min_n, a.max_n], "step_range": [a.min_steps, a.max_steps],
-                   "slots": a.slots, "build_workers": a.workers, "seed": a.seed,
-                   "tuned_xchunk": {
-                       "x".join(str(v) for v in k): c for k, c in tuner.cache.items()}}}),
-          flush=True)
+    print(json.dumps(measure_stream(a.requests, a.seed, (a.min_n, a.max_n),
+                                    (a.min_steps, a.max_steps), a.load, a.slots, a.workers,
+                                    a.tune, a.device)), flush=True)
 
 
 if __name__ == "__main__":

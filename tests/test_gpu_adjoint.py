@@ -163,3 +163,60 @@ def test_box_history_equals_segment_recompute(monkeypatch):
     assert a.value == b.value
     np.testing.assert_array_equal(a.d_ca, b.d_ca)
     np.testing.assert_array_equal(a.d_cb, b.d_cb)
+
+
+def dispersive_slab(**kw):
+    """The small slab scene with its slab made of a Drude + Lorentz medium (the DC part of the
+    Drude pole folded into a conductivity, as the scene factory does): the adjoint runs the
+    transposed pole pass in every slab cell."""
+    sc = small_slab(**kw)
+    poles, sigma = scenes.split_dc(scenes.drude_poles(2.0e15, 1e14)
+                                   + scenes.lorentz_poles(1.0, 2.6e14, 2e13), sc.dt)
+    am1, b = scenes.trap_coeffs(poles, sc.dt)
+    masks = [np.asarray(e) > 2.2 for e in (sc.eps_ex, sc.eps_ey, sc.eps_ez)]
+    disp = scenes.build_dispersion(masks, am1, b, sc.shape)
+    sig = [np.where(m, sigma, 0.0) for m in masks]
+    return replace(sc, dispersion=disp, sigma_ex=sig[0], sigma_ey=sig[1], sigma_ez=sig[2])
+
+
+def test_dispersive_adjoint_matches_central_differences():
+    """Gradient of a block of Drude + Lorentz slab cells against central differences of the GPU
+    forward run (h = 2e-2 on the block's eps_inf), within 2%."""
+    sc = dispersive_slab()
+    assert sc.dispersion.n_entry > 0
+    g = adjoint.flux_gradient(sc, checkpoint_every=64)
+    cells = slab_block(sc, 18, 18)
+    h = 2e-2
+    fd = (objective(perturbed(sc, cells, (0, 1, 2), h))
+          - objective(perturbed(sc, cells, (0, 1, 2), -h))) / (2 * h)
+    ad = float(sum(g.d_eps[c][cells].sum() for c in range(3)))
+    assert abs(fd) * h > 1e-5 * abs(g.value)
+    assert abs(ad - fd) <= 0.02 * abs(fd), (ad, fd)
+
+
+@pytest.mark.parametrize("block", [(18, 18), (15, 21)])
+def test_dispersive_adjoint_matches_fp64_central_differences(block):
+    """The same against central differences of the FP64 oracle (h = 1e-3): within 1e-4."""
+    sc = dispersive_slab()
+    g = adjoint.flux_gradient(sc, checkpoint_every=64)
+    cells = slab_block(sc, *block)
+    h = 1e-3
+    fd = (objective_fp64(perturbed(sc, cells, (0, 1, 2), h))
+          - objective_fp64(perturbed(sc, cells, (0, 1, 2), -h))) / (2 * h)
+    ad = float(sum(g.d_eps[c][cells].sum() for c in range(3)))
+    print(f"dispersive block {block}: adjoint {ad:.9e}, FP64 central difference {fd:.9e}, "
+          f"relative {abs(ad - fd) / abs(fd):.2e}")
+    assert abs(ad - fd) <= 1e-4 * abs(fd), (ad, fd, abs(ad - fd) / abs(fd))
+
+
+def test_dispersive_checkpoints_hold_the_pole_states(monkeypatch):
+    """Recomputing every segment from its checkpoint (fields, psi and pole states) gives the
+    gradient bit for bit as the recorded box history does."""
+    sc = dispersive_slab(num_steps=300)
+    box = (14, 15, 17, 11, 9, 7)
+    a = adjoint.flux_gradient(sc, checkpoint_every=50, box=box)
+    monkeypatch.setenv("OEM_B200_ADJ_HISTORY", "0")
+    b = adjoint.flux_gradient(sc, checkpoint_every=37, box=box)
+    assert a.value == b.value
+    np.testing.assert_array_equal(a.d_ca, b.d_ca)
+    np.testing.assert_array_equal(a.d_cb, b.d_cb)

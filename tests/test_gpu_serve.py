@@ -21,5 +21,5 @@ def test_served_results_equal_alone():
     ev = [e for _t, e, _r in srv.log]
     assert ev.count("admit") == 5 and ev.count("done") == 5
     for d, r in zip(got, reqs):
-        alone = solver.run(r.scene, num_steps=r.num_steps, use_shutoff=False, verbose=False)
+        alone = solver.run(r.build(), num_steps=r.num_steps, use_shutoff=False, verbose=False)
         np.testing.assert_array_equal(d.result.phasors["T"].data, alone.phasors["T"].data)

@@ -161,16 +161,16 @@ def test_bloch_subset_fails_closed(feature):
     solver.refuse_unsupported_bloch(plain)
 
 
-@pytest.mark.parametrize("feature", ["dispersion", "absorber", "bloch", "mix", "tensor",
-                                     "modulation"])
+@pytest.mark.parametrize("feature", ["absorber", "bloch", "mix", "tensor", "modulation"])
 def test_adjoint_fails_closed(feature):
-    """The discrete adjoint covers real, non-dispersive scenes without absorbers, tensor media or
-    time modulation; the rest is refused before anything reaches the device."""
+    """The discrete adjoint covers real scenes with pole-residue dispersion, without absorbers,
+    slanted-interface mixed media, tensor media or time modulation; the rest is refused before
+    anything reaches the device."""
     from openem_b200 import adjoint
     sd = scenes.small_dispersive(n=20, n_sph=1, n_pml=4, num_steps=10)
     plain = replace(sd, dispersion=None)
+    adjoint._refuse(sd)  # pole-residue dispersion is covered
     bad = {
-        "dispersion": sd,
         "mix": replace(scenes.mixed_sphere(n=20, n_pml=4, radius_cells=3.3, num_steps=10),
                        dispersion=None),
         "tensor": replace(plain, tensor=M.TensorEps(np.array([0]), np.array([0]),

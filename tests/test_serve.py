@@ -88,7 +88,7 @@ def test_slots_bound_the_simulations_in_flight():
 
 def test_memory_budget_admits_by_footprint():
     reqs = _reqs(4)
-    one = S.footprint(reqs[0].scene, reqs[0].num_steps)
+    one = reqs[0].need()
     srv, _ = _server(max_slots=8, mem_budget=int(1.5 * one), chunk=400)
     srv.serve(reqs)
     assert _max_in_flight(srv.log) == 1
@@ -107,7 +107,11 @@ def test_footprint_grows_with_the_grid():
 
 def test_make_stream_and_arrivals():
     reqs = S.make_stream(5, seed=3, n_range=(32, 48), step_range=(100, 200))
-    assert all(32 <= r.scene.shape[0] <= 48 and 100 <= r.num_steps <= 200 for r in reqs)
+    assert all(32 <= r.build().shape[0] <= 48 and 100 <= r.num_steps <= 200 for r in reqs)
+    # scenes are built on demand, the same each time, and the admission estimate bounds them
+    a, b = reqs[2].build(), reqs[2].build()
+    np.testing.assert_array_equal(a.eps_ex, b.eps_ex)
+    assert all(r.footprint >= S.footprint(r.build(), r.num_steps) for r in reqs)
     S.poisson_arrivals(reqs, rate=10.0)
     t = [r.arrival for r in reqs]
     assert t[0] == 0.0 and all(b > a for a, b in zip(t, t[1:]))
