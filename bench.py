@@ -148,12 +148,13 @@ def barrier(world: int):
         dist.barrier()
 
 
-def reduce_max(x: float, world: int) -> float:
+def reduce_max(x: float, world: int, device: str = "cuda") -> float:
+    """The largest ``x`` over the ranks (the slowest replica's time sets the whole job's)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -346,11 +346,16 @@ __global__ void __launch_bounds__(128) k_flush(Monitor m, const int* step, int f
   const int s_lo = *m.d_done + 1;
   if (s_lo > s_now) return;
   constexpr int NE = NC / 2;  // E components come first
-  // grid-stride over the points: a few blocks per SM, so that the launch of a step without a
-  // batch boundary costs little
-  for (int64_t pt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pt < m.cells;
-       pt += (int64_t)gridDim.x * blockDim.x)
-  for (int f0 = 0; f0 < m.nf; f0 += 8) {
+  // grid-stride over the (frequency group, point) items, points fastest: each thread sums one
+  // point's rows for one group of 8 frequencies, so a plane with many frequencies spreads over
+  // many threads (the rows of a point come from L2 for every group after the first); at most a
+  // few blocks per SM, so that the launch of a step without a batch boundary costs little
+  const int64_t items = (int64_t)((m.nf + 7) / 8) * m.cells;
+  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items;
+       it += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t grp = it / m.cells;
+    const int64_t pt = it - grp * m.cells;
+    const int f0 = (int)grp * 8;
     const int nfc = min(8, m.nf - f0);
     float aR[8][NC], aI[8][NC];
 #pragma unroll
@@ -398,9 +403,14 @@ __global__ void __launch_bounds__(128) k_flush_c(Monitor m, const int* step, int
   const int s_lo = *m.d_done + 1;
   if (s_lo > s_now) return;
   constexpr int NE = NC / 2;
-  for (int64_t pt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pt < m.cells;
-       pt += (int64_t)gridDim.x * blockDim.x) {
-    for (int f0 = 0; f0 < m.nf; f0 += 4) {
+  // grid-stride over (frequency group of 4, point) items, as in k_flush
+  const int64_t items = (int64_t)((m.nf + 3) / 4) * m.cells;
+  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items;
+       it += (int64_t)gridDim.x * blockDim.x) {
+    {
+      const int64_t grp = it / m.cells;
+      const int64_t pt = it - grp * m.cells;
+      const int f0 = (int)grp * 4;
       const int nfc = min(4, m.nf - f0);
       float aR[4][NC], aI[4][NC];
 #pragma unroll
@@ -935,7 +945,8 @@ cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* ste
 }
 
 cudaError_t launch_flush(const Monitor& m, const int* step, int forced, cudaStream_t s) {
-  const int64_t nb = std::min<int64_t>((m.cells + 127) / 128, 148 * 8);
+  const int64_t groups = m.cplx ? (m.nf + 3) / 4 : (m.nf + 7) / 8;
+  const int64_t nb = std::min<int64_t>((groups * m.cells + 127) / 128, 148 * 8);
   if (m.cplx) {
     if (m.ncomp == 4)
       k_flush_c<4><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);

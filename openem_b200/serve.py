@@ -201,40 +201,67 @@ class Server:
         self.device_ctx()
         # device-side table builds run on a high-priority stream, so that their small kernels
         # are scheduled ahead of the pending blocks of the simulations in flight
-        with torch.cuda.stream(torch.cuda.Stream(device=self.device, priority=-1)):
-            return self.plan_factory(req, stream)
+        try:
+            with torch.cuda.stream(torch.cuda.Stream(device=self.device, priority=-1)):
+                return self.plan_factory(req, stream)
+        finally:
+            # the table build's temporaries stay in torch's cache otherwise, where the engine's
+            # own allocations cannot reach them
+            torch.cuda.empty_cache()
 
     device_ctx = None
+
+    @staticmethod
+    def _out_of_memory(exc) -> bool:
+        return "out of memory" in str(exc) or "do not fit" in str(exc)
+
+    @staticmethod
+    def build_bytes(req) -> int:
+        """Device memory a plan build needs on top of the plan while it runs (the float64 eps
+        and sigma copies, keys and sort buffers of the device table build): 160 B per cell."""
+        sc = req.scene if not callable(req.scene) else None
+        if sc is not None:
+            n = int(np.prod(sc.shape))
+        else:
+            n = int(req.need() // 26)  # the footprint is at least 26 B per cell
+        return 160 * n
 
     def _serve(self, requests, pool) -> list:
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
         active = []       # dicts: req, plan (or its future), stream, event, steps, start, bytes
         graveyard = []    # finished plans whose memory is released in batches
         used = 0
+        hold = -1         # after a failed build: admit nothing until this many have finished
+        building = 0      # transient bytes of the builds in flight
         dead_bytes = 0
         done = []
         t0 = self.clock()
         while pending or active:
             now = self.clock() - t0
             progressed = False
-            # admission: arrived requests, while a slot and the memory budget allow
+            # admission: arrived requests, while a slot and the memory budget allow (the plan
+            # itself and, while it is being built, its build's transient buffers)
             while pending and pending[0].arrival <= now and len(active) < self.max_slots:
+                if hold >= 0 and len(done) <= hold and active:
+                    break
                 req = pending[0]
                 need = req.need()
-                if used + dead_bytes + need > self.mem_budget and graveyard:
+                extra = self.build_bytes(req)
+                if used + building + dead_bytes + need + extra > self.mem_budget and graveyard:
                     for p in graveyard:
                         p.close()
                     graveyard.clear()
                     dead_bytes = 0
-                if used + need > self.mem_budget and active:
+                if used + building + need + extra > self.mem_budget and active:
                     break  # wait for a simulation to finish and free its memory
                 pending.pop(0)
                 stream = self.stream_factory()
                 ent = {"req": req, "plan": None, "stream": stream, "event": self.event_factory(),
-                       "steps": 0, "start": self.clock() - t0, "bytes": need,
+                       "steps": 0, "start": self.clock() - t0, "bytes": need, "extra": extra,
                        "future": pool.submit(self._build, req, stream)}
                 active.append(ent)
                 used += need
+                building += extra
                 self.log.append((ent["start"], "admit", req.rid))
                 progressed = True
             # step: a built plan whose previous chunk has drained gets the next one
@@ -242,7 +269,25 @@ class Server:
                 if ent["plan"] is None:
                     if not ent["future"].done():
                         continue
-                    ent["plan"] = ent["future"].result()  # re-raises a failed build
+                    building -= ent["extra"]
+                    try:
+                        ent["plan"] = ent["future"].result()  # re-raises a failed build
+                    except RuntimeError as exc:
+                        # the device was fuller than the estimates said: release what can be
+                        # released and admit this request again once others have finished
+                        if not self._out_of_memory(exc) or len(active) == 1:
+                            raise
+                        active.remove(ent)
+                        used -= ent["bytes"]
+                        for p in graveyard:
+                            p.close()
+                        graveyard.clear()
+                        dead_bytes = 0
+                        pending.insert(0, ent["req"])
+                        hold = len(done)
+                        self.log.append((self.clock() - t0, "retry", ent["req"].rid))
+                        progressed = True
+                        continue
                     self._issue(ent)
                     progressed = True
                     continue
@@ -390,6 +435,7 @@ def measure_stream(n_requests: int = 256, seed: int = 3, n_range=(64, 384),
     t_ser = ser[-1].finish
     rate = load * len(reqs) / t_ser
     poisson_arrivals(reqs, rate, seed)
+    torch.cuda.empty_cache()  # the admission budget is measured from the free memory
     srv = Server(device, max_slots=slots, tuner=tuner, build_workers=workers, keep=digest)
     got = srv.serve(reqs)
     t_srv = max(d.finish for d in got) - min(r.arrival for r in reqs)

@@ -127,10 +127,12 @@ def test_box_gradient_equals_full_gradient_inside_the_box():
 
 def test_c4_design_pixels_match_central_differences():
     """The 200 x 200 x 120 slab-and-beam configuration (2000 steps, K = 64, gradients kept for
-    the 80 x 80 x 9 design box): of 16 design pixels drawn with rng(2), the four with the largest
-    gradients agree with central differences (h = 1e-2 on the pixel's column of cells) within 2%.
-    Pixels with far smaller gradients are limited by the float32 forward noise of the
-    differences themselves."""
+    the 80 x 80 x 9 design box), all 16 design pixels drawn with rng(2), against central
+    differences of the float32 forward run (h = 1e-2 on the pixel's column of cells) with one
+    bound: |adjoint - FD| <= 5% of |FD| + 0.5% of the largest |FD| of the 16 (the second term is
+    the float32 noise of a difference of two forward runs; at h = 1e-3 that noise exceeds the
+    smaller pixels' signal, which is why the transpose itself is pinned by FP64-oracle
+    differences in the tests above). The four largest are also held to 2%."""
     from openem_b200 import flux
     sc = scenes.beam_slab()
     nx, ny, _ = sc.shape
@@ -145,11 +147,19 @@ def test_c4_design_pixels_match_central_differences():
     def J(s):
         r = solver.run(s, use_shutoff=False, verbose=False)
         return float(flux.plane_flux(r.phasors["T"].data, s.grid, axis=2).sum())
-    for q in np.argsort(-np.abs(ad))[:4]:
+    fd = np.zeros(16)
+    for q in range(16):
         a, b = pix[q]
         cells = np.s_[i0 + a, j0 + b, box[2]:box[2] + box[5]]
-        fd = (J(perturbed(sc, cells, (0, 1, 2), h)) - J(perturbed(sc, cells, (0, 1, 2), -h))) / (2 * h)
-        assert abs(ad[q] - fd) <= 0.02 * abs(fd), (a, b, ad[q], fd)
+        fd[q] = (J(perturbed(sc, cells, (0, 1, 2), h))
+                 - J(perturbed(sc, cells, (0, 1, 2), -h))) / (2 * h)
+    for q in range(16):
+        print(f"pixel {tuple(pix[q])}: adjoint {ad[q]:.6e}, FD {fd[q]:.6e}, "
+              f"relative {abs(ad[q] - fd[q]) / abs(fd[q]):.2e}")
+    big = np.abs(fd).max()
+    assert np.all(np.abs(ad - fd) <= 0.05 * np.abs(fd) + 0.005 * big), (ad, fd)
+    for q in np.argsort(-np.abs(ad))[:4]:
+        assert abs(ad[q] - fd[q]) <= 0.02 * abs(fd[q]), (pix[q], ad[q], fd[q])
 
 
 def test_box_history_equals_segment_recompute(monkeypatch):

@@ -115,3 +115,28 @@ def test_make_stream_and_arrivals():
     S.poisson_arrivals(reqs, rate=10.0)
     t = [r.arrival for r in reqs]
     assert t[0] == 0.0 and all(b > a for a, b in zip(t, t[1:]))
+
+
+def test_a_build_that_runs_out_of_memory_is_admitted_again():
+    """A plan build that finds the device fuller than the admission estimates (the engine reports
+    an out-of-memory status) is put back at the head of the queue and built again once another
+    request has finished; every request still completes."""
+    plans, failed = [], []
+
+    def factory(req, stream):
+        if req.rid == 2 and not failed:
+            failed.append(req.rid)
+            raise RuntimeError("[oem status -6] finalize: cudaMalloc of 1 bytes failed: out of "
+                               "memory")
+        plans.append(FakePlan(req))
+        return plans[-1]
+
+    srv = S.Server(plan_factory=factory, stream_factory=lambda: object(),
+                   event_factory=FakeEvent, max_slots=4, mem_budget=1 << 40, chunk=300)
+    done = srv.serve(_reqs(5))
+    assert [d.rid for d in done] == list(range(5))
+    ev = [(e, r) for _t, e, r in srv.log]
+    assert ("retry", 2) in ev
+    assert [e for e, r in ev if r == 2].count("admit") == 2
+    retry_at = ev.index(("retry", 2))
+    assert any(e == "done" for e, _r in ev[:ev.index(("admit", 2), retry_at)])
