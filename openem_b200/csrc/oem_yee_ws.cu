@@ -114,10 +114,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
   atomicExch(err, 1);
   return false;
 }
-// A wait of the pipeline itself: gives up after `limit` polls (setting *err), or early once
-// another warp of the grid has set *err (read every 4096 polls), so one failure ends every
-// block's pipeline quickly. A producer's final drain of its own copies uses mbar_wait, which
-// waits for them whatever happened elsewhere.
+// A producer's wait for a free stage: gives up after `limit` polls (setting *err), or early once
+// another warp of the grid has set *err (read every 4096 polls), so a block whose consumers have
+// left does not run out its own bound. Consumers wait with mbar_wait (the extra check in their
+// per-plane wait cost the E update 1.5%), and so does a producer's final drain of its own
+// copies, which must complete whatever happened elsewhere.
 constexpr uint32_t kPolls = 1u << 20;
 __device__ __forceinline__ bool mbar_wait_live(uint64_t* bar, uint32_t parity, int* err,
                                                uint32_t limit) {
@@ -420,7 +421,7 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_h_ws(const __grid_con
   const int to = w * kTZ + 4 * lane;  // this quad in a tile
   for (int t = 0; t < np; ++t) {
     const int slot = t % kS;
-    bool got = mbar_wait_live(&full[slot], (uint32_t)((t / kS) & 1), err, kPolls);
+    bool got = mbar_wait(&full[slot], (uint32_t)((t / kS) & 1), err);
     if (!__all_sync(kFull, got)) break;
     const float* st = smem + slot * kHStage;
     const int i = ib + t;
@@ -533,10 +534,11 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
   extern __shared__ __align__(128) float smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kS * kEStage);
   uint64_t* empty = full + kS;
-  uint64_t* never = empty + kS;  // a barrier no thread arrives at (the wait-expiry check)
-  float* zt = reinterpret_cast<float*>(empty + kS + 2);
+  float* zt = reinterpret_cast<float*>(empty + kS);
   MatRec* smats = reinterpret_cast<MatRec*>(zt + kZTab);
   uint32_t* segt = reinterpret_cast<uint32_t*>(smats + kSmemMats);  // [plane][row][start, end]
+  // a barrier no thread arrives at (the wait-expiry check), after everything else
+  uint64_t* never = reinterpret_cast<uint64_t*>(segt + kXMax * kTY * 2);
   const int lane = threadIdx.x, w = threadIdx.y;
   const int tid = w * 32 + lane;
   const int k0 = blockIdx.x * kTZ;
@@ -689,7 +691,7 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
   const int to = w * kTZ + 4 * lane;
   for (int t = 0; t < np; ++t) {
     const int slot = t % kS;
-    bool got = mbar_wait_live(&full[slot], (uint32_t)((t / kS) & 1), err, kPolls);
+    bool got = mbar_wait(&full[slot], (uint32_t)((t / kS) & 1), err);
     // the plan's wait-expiry check: wait on a barrier nothing arrives at, with its short bound,
     // so that the expiry path (error word, early exit of every warp, the producer's drain) runs
     if (P.expire_polls > 0 && got) got = mbar_wait_live(never, 0u, err, (uint32_t)P.expire_polls);
@@ -1339,7 +1341,7 @@ __global__ void __launch_bounds__(192, 2) k_he_ws(const __grid_constant__ FusedM
 
 size_t ws_h_smem() { return (size_t)kS * kHStage * 4 + 2 * kS * sizeof(uint64_t) + kZTab * 4; }
 size_t ws_e_smem() {
-  return (size_t)kS * kEStage * 4 + (2 * kS + 2) * sizeof(uint64_t) + kZTab * 4 +
+  return (size_t)kS * kEStage * 4 + (2 * kS + 1) * sizeof(uint64_t) + kZTab * 4 +
          kSmemMats * sizeof(MatRec) + kXMax * kTY * 2 * sizeof(uint32_t);
 }
 

@@ -26,6 +26,26 @@ from openem_b200.results import Phasors, Result
 SHUTOFF_INTERVAL = 400
 COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 
+_TOUCH_POOL = None
+
+
+def host_array(shape, dtype) -> np.ndarray:
+    """An output array for a device readout. A large one has its pages touched by eight threads
+    first: a copy into fresh pages spends most of its time in page faults (a 403 MB phasor
+    readout: 81 ms into fresh pages, 20 ms into touched ones), and the faults of separate
+    threads run in parallel."""
+    global _TOUCH_POOL
+    out = np.empty(shape, dtype)
+    flat = out.reshape(-1).view(np.uint8)
+    if flat.size < (64 << 20):
+        return out
+    if _TOUCH_POOL is None:
+        from concurrent.futures import ThreadPoolExecutor
+        _TOUCH_POOL = ThreadPoolExecutor(max_workers=8)
+    step = -(-flat.size // 8)
+    list(_TOUCH_POOL.map(lambda q: flat[q * step:(q + 1) * step].fill(0), range(8)))
+    return out
+
 
 def refuse_unsupported(sc) -> None:
     """Fail closed on scene features outside this engine's real-field path."""
@@ -347,7 +367,7 @@ class Plan:
         return int(v.value)
 
     def read_monitor(self, mid: int, shape) -> np.ndarray:
-        out = np.empty(shape, np.complex128)
+        out = host_array(shape, np.complex128)
         L.check(self.lib.oem_plan_read_monitor_interleaved(self.h, int(mid), L.ptr(out), self._s),
                 "read_monitor")
         return out
@@ -381,7 +401,7 @@ class Plan:
         return out
 
     def read_field(self, comp: int) -> np.ndarray:
-        out = np.empty(self.shape, np.float32)
+        out = host_array(self.shape, np.float32)
         if self.cplx:
             im = np.empty(self.shape, np.float32)
             L.check(self.lib.oem_plan_read_field_complex(self.h, int(comp), L.ptr(out),

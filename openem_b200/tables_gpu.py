@@ -50,6 +50,42 @@ def _to_dev(a, torch, dev, dtype=None):
     return t.to(dev, non_blocking=False)
 
 
+class _PinnedStager:
+    """Host-to-device copies of large arrays through two halves of one pinned buffer: the host
+    copies chunk q into one half (torch's multi-threaded memcpy) while the DMA of chunk q - 1
+    drains the other, so the transfer runs near the link rate instead of through the driver's
+    pageable staging. One buffer per process, made on first use; used by one thread at a time."""
+
+    CHUNK = 64 << 20
+    _buf = None
+
+    @classmethod
+    def copy(cls, a: np.ndarray, torch, dev):
+        a = np.ascontiguousarray(a)
+        if a.nbytes < 2 * cls.CHUNK:
+            return torch.from_numpy(a).to(dev)
+        if cls._buf is None:
+            cls._buf = torch.empty(2 * cls.CHUNK, dtype=torch.uint8, pin_memory=True)
+        dst = torch.empty(a.shape, dtype=torch.from_numpy(a[:0]).dtype, device=dev)
+        src = torch.from_numpy(a.reshape(-1).view(np.uint8))
+        out = dst.view(-1).view(torch.uint8)
+        stream = torch.cuda.current_stream(dev)
+        done = [None, None]
+        for q, off in enumerate(range(0, a.nbytes, cls.CHUNK)):
+            half = q % 2
+            n = min(cls.CHUNK, a.nbytes - off)
+            if done[half] is not None:
+                done[half].synchronize()  # the DMA out of this half has finished
+            stage = cls._buf[half * cls.CHUNK: half * cls.CHUNK + n]
+            stage.copy_(src[off:off + n])
+            out[off:off + n].copy_(stage, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            done[half] = ev
+        stream.synchronize()
+        return dst
+
+
 class _Uploads:
     """The float64 eps and sigma arrays of each component copied to the device on a worker
     thread while the caller deduplicates the pole sets and builds the keys: all three
@@ -66,15 +102,17 @@ class _Uploads:
         nbytes = sum(np.asarray(a).size * 8 for a in (*self.eps, *self.sig) if a is not None)
         free, _ = torch.cuda.mem_get_info(dev)
         self.depth = 3 if nbytes < free // 4 else 1
+        self.stream = torch.cuda.Stream(device=dev)
         self.pool = ThreadPoolExecutor(max_workers=1)
         self.futs = [self.pool.submit(self._load, c) for c in range(self.depth)]
 
     def _load(self, c):
         torch, dev = self.torch, self.dev
         torch.cuda.set_device(dev)
-        eps = _to_dev(np.asarray(self.eps[c], np.float64), torch, dev).reshape(-1)
-        sig = (None if self.sig[c] is None
-               else _to_dev(np.asarray(self.sig[c], np.float64), torch, dev).reshape(-1))
+        with torch.cuda.stream(self.stream):
+            eps = _PinnedStager.copy(np.asarray(self.eps[c], np.float64), torch, dev).reshape(-1)
+            sig = (None if self.sig[c] is None else
+                   _PinnedStager.copy(np.asarray(self.sig[c], np.float64), torch, dev).reshape(-1))
         return eps, sig
 
     def get(self, c):

@@ -155,12 +155,17 @@ def test_pipelined_kernels_periodic_slab(monkeypatch, kind):
         assert rel_l2(b.fields[nm], a.fields[nm]) < 1e-6, nm
 
 
-def test_device_tables_match_host_tables():
-    """Material index and pole offsets built on the GPU equal the numpy build cell for cell."""
+@pytest.mark.parametrize("chunk", [None, 64 << 10])
+def test_device_tables_match_host_tables(monkeypatch, chunk):
+    """Material index and pole offsets built on the GPU equal the numpy build cell for cell; with
+    a small staging chunk the eps / sigma uploads go through the pinned double buffer."""
     from openem_b200 import tables as T
     from openem_b200 import tables_gpu
     if not tables_gpu.available():
         pytest.skip("torch with CUDA is not available")
+    if chunk:
+        monkeypatch.setattr(tables_gpu._PinnedStager, "CHUNK", chunk)
+        monkeypatch.setattr(tables_gpu._PinnedStager, "_buf", None)
     sc = scenes.small_dispersive(n=48, n_sph=6, num_steps=10, n_pml=8, nfreq=2)
     tabs = [T.axis_tables(sc, a) for a in range(3)]
     h = T.material_tables(sc, tabs)
