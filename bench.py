@@ -448,6 +448,7 @@ def run_ours(args):
     clk = clocks.stop() if clocks else None
     plan.status()
     launches = plan.launches_per_step() * K
+    snap_in_e = plan.box_snapshots_in_update() > 0
     # per-kernel CUDA-event times (direct launches) for the roofline of the dominant kernel
     plan.enable_timing(True)
     plan.run(KT)
@@ -461,7 +462,7 @@ def run_ours(args):
     value = world * cells * K / (ms_max * 1e-3) / 1e9
 
     # roofline of the dominant kernel
-    kb = roofline.kernel_bytes(sc)
+    kb = roofline.kernel_bytes(sc, box_snapshots_in_e=snap_in_e)
     peaks = roofline.measured_peaks(ROOT)
     dom = max((k for k in ("update_he", "update_h", "update_e") if k in tm),
               key=lambda k: tm[k][1])

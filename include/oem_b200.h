@@ -301,8 +301,15 @@ int oem_plan_flush(oem_plan* p, void* stream);
  * since the last check (the readout calls report it too). */
 int oem_plan_status(oem_plan* p, void* stream);
 
-/* Number of kernel launches one time step of this plan makes (its captured step graph). */
+/* Number of kernel launches one time step of this plan makes (the kernel nodes of its
+ * captured one-step graph). */
 int oem_plan_launches_per_step(oem_plan* p, int* n);
+
+/* Number of box DFT monitors whose per-step snapshot the E update kernel writes itself (0: each
+ * box has its own snapshot launch, the default). Decided at finalize when OEM_B200_SNAP=update
+ * is set in the environment: a real plan on the warp-specialised kernels whose only E-side
+ * work after the update is electric dipoles, with at most four box monitors. */
+int oem_plan_box_snapshots_in_update(oem_plan* p, int* n);
 
 /* Steps taken so far (host-side count). */
 int oem_plan_steps(oem_plan* p, int64_t* steps);
@@ -323,6 +330,12 @@ int oem_plan_read_monitor(oem_plan* p, int id, double* re, double* im, void* str
  * monitor's shape, so the host assembles nothing (interleaved on the device, copied out in
  * chunks). */
 int oem_plan_read_monitor_interleaved(oem_plan* p, int mon_id, double* out, void* stream);
+
+/* Phasor values with a NaN or infinite part that oem_plan_read_monitor_interleaved has read out
+ * since the previous call of this function (counted on the device while interleaving); the
+ * count is reset. A caller warns of a diverged field from it without scanning the readout
+ * (openem/solver.py:347-370 scans the host arrays). */
+int oem_plan_readout_nonfinite(oem_plan* p, int64_t* count);
 int oem_plan_read_time_monitor(oem_plan* p, int id, float* out, void* stream);
 int oem_plan_read_field(oem_plan* p, int comp, float* out, void* stream);
 int oem_plan_write_field(oem_plan* p, int comp, const float* in, void* stream);

@@ -10,7 +10,9 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -19,6 +21,44 @@
 namespace oem {
 
 static thread_local std::string g_last_error;
+
+// Host side of the phasor readout, one per device per process: two pinned halves of a staging
+// buffer. The DMA of chunk q fills one half while host threads copy chunk q - 1 out of the other
+// into the caller's (pageable) array, so the copy-out runs near the link rate instead of
+// through the driver's single-threaded pageable staging. Readouts on one device take turns.
+struct ReadStage {
+  std::mutex mu;
+  char* half[2] = {nullptr, nullptr};
+  size_t bytes = 0;  // of each half
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+static std::mutex g_stage_mu;
+static std::map<int, ReadStage*> g_stages;
+
+static ReadStage* read_stage(int device) {
+  std::lock_guard<std::mutex> g(g_stage_mu);
+  ReadStage*& r = g_stages[device];
+  if (!r) r = new ReadStage();
+  return r;
+}
+
+// Copy n bytes with up to 8 host threads (pieces of at least 4 MB).
+static void par_memcpy(char* dst, const char* src, size_t n) {
+  const size_t kMin = (size_t)4 << 20;
+  const int nt = (int)std::min<size_t>(8, std::max<size_t>(1, n / kMin));
+  if (nt == 1) {
+    memcpy(dst, src, n);
+    return;
+  }
+  const size_t per = (n + nt - 1) / nt;
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t) {
+    const size_t a = t * per, b = std::min(n, a + per);
+    if (a < b) th.emplace_back([=] { memcpy(dst + a, src + a, b - a); });
+  }
+  memcpy(dst, src, std::min(n, per));
+  for (std::thread& x : th) x.join();
+}
 
 int set_error(int code, const std::string& msg) {
   g_last_error = msg;
@@ -178,7 +218,7 @@ static cudaError_t run_h(oem_plan* p, cudaStream_t s) {
   return launch_update_h_tma(p->tma, p->yp, p->xch, p->d_err, s);
 }
 
-static cudaError_t run_e(oem_plan* p, cudaStream_t s) {
+static cudaError_t run_e(oem_plan* p, cudaStream_t s, const SnapBoxes* sb = nullptr) {
   if (p->is_complex && p->cplx_ws) {
     const int nm = (int)p->mats.size();
     cudaError_t e = launch_update_e_ws(p->tma, p->yp, p->xch, nm, p->d_err, s);
@@ -197,7 +237,7 @@ static cudaError_t run_e(oem_plan* p, cudaStream_t s) {
                                           (int64_t)p->nx * p->ny * p->nzp / 32, 0, s);
       if (e != cudaSuccess) return e;
     }
-    return launch_update_e_ws(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s);
+    return launch_update_e_ws(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s, sb);
   }
   return launch_update_e_tma(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s);
 }
@@ -308,6 +348,12 @@ static int check_device_error(oem_plan* p) {
 // One time step (openem/solver.py:1145-1162).
 static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors);
 
+// The box monitors whose snapshots the E update of this step writes, or null: only on a step
+// that records monitors.
+static const SnapBoxes* snap_boxes(const oem_plan* p, bool monitors) {
+  return (monitors && p->snapk.n > 0) ? &p->snapk : nullptr;
+}
+
 // The current field bank becomes b: every kernel enqueued afterwards (sources, monitors,
 // readouts) reads and writes that bank.
 static void set_bank(oem_plan* p, int b) {
@@ -371,11 +417,12 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
     if ((e = launch_mode_h(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_h");
   for (const Absorber& a : p->absorbers)
     if ((e = launch_absorb(P, a, 0, s)) != cudaSuccess) return cuda_error(e, "absorb_h");
+  const SnapBoxes* sb = snap_boxes(p, monitors);
   if (fork) {
     OEM_CUDA(cudaStreamWaitEvent(s, p->ev_join, 0));
-    e = launch_update_e_ws(p->tma, P, p->xch, (int)p->mats.size(), p->d_err, s);
+    e = launch_update_e_ws(p->tma, P, p->xch, (int)p->mats.size(), p->d_err, s, sb);
   } else {
-    e = run_e(p, s);
+    e = run_e(p, s, sb);
   }
   if (e != cudaSuccess) return cuda_error(e, "update_e");
   return enqueue_e_side(p, s, monitors);
@@ -393,8 +440,9 @@ static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors) {
     if ((e = launch_tfsf(P, t, 1, p->d_step, s)) != cudaSuccess) return cuda_error(e, "tfsf_e");
   for (const ModeSrc& m : p->modesrcs)
     if ((e = launch_mode_e(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_e");
+  const SnapBoxes* sb = snap_boxes(p, monitors);
   for (const DipoleSet& d : p->dipoles)
-    if (!d.magnetic && (e = launch_dipoles(P, d, p->d_step, s)) != cudaSuccess)
+    if (!d.magnetic && (e = launch_dipoles(P, d, p->d_step, s, sb)) != cudaSuccess)
       return cuda_error(e, "dipoles_e");
   for (const MixSet& x : p->mixes)
     if ((e = launch_mix_post(P, x, s)) != cudaSuccess) return cuda_error(e, "mix_post");
@@ -415,7 +463,9 @@ static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors) {
   }
   for (const Monitor& m : p->mons) {
     if (!monitors) break;
-    if ((e = launch_snapshot(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "snapshot");
+    // box rows already written by the E update (and the E dipoles) when sb is set
+    if (!(sb && m.kind == 1) && (e = launch_snapshot(P, m, p->d_step, s)) != cudaSuccess)
+      return cuda_error(e, "snapshot");
     if ((e = launch_flush(m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "flush");
   }
   if (p->hist && (e = launch_hist_snap(P, p->gbox, p->hist, p->d_step, p->n_total, s)) !=
@@ -488,6 +538,24 @@ static int capture(oem_plan* p, int nsteps, cudaGraphExec_t* out) {
     return rc;
   }
   if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");
+  if (nsteps == 1) {
+    // the kernels one step launches: the kernel nodes of the one-step graph
+    size_t nn = 0;
+    e = cudaGraphGetNodes(g, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (e == cudaSuccess && nn) e = cudaGraphGetNodes(g, nodes.data(), &nn);
+    int kernels = 0;
+    for (size_t q = 0; q < nn && e == cudaSuccess; ++q) {
+      cudaGraphNodeType t;
+      e = cudaGraphNodeGetType(nodes[q], &t);
+      kernels += (e == cudaSuccess && t == cudaGraphNodeTypeKernel) ? 1 : 0;
+    }
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return cuda_error(e, "cudaGraphGetNodes");
+    }
+    p->step_kernels = kernels;
+  }
   e = cudaGraphInstantiate(out, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return cuda_error(e, "cudaGraphInstantiate");
@@ -1153,6 +1221,7 @@ static int add_monitor_common(oem_plan* p, Monitor& m, int nf, int64_t n_total, 
   if ((rc = dalloc(p, &m.d_im, (size_t)m.ncomp * nf * m.cells))) return rc;
   int minus1 = -1;
   if ((rc = dupload(p, &m.d_done, &minus1, 1))) return rc;
+  if ((rc = dalloc(p, &m.d_count, 1))) return rc;
   *id = (int)p->mons.size();
   p->mons.push_back(m);
   return OEM_OK;
@@ -1420,6 +1489,34 @@ int oem_plan_add_dispersion_mix(oem_plan* p, int n_entry, const int* comp, const
   return OEM_OK;
 }
 
+// Box snapshots written by the warp-specialised E update (k_e_ws<true>) instead of k_snap_box,
+// when OEM_B200_SNAP=update asks for it: a real plan on those kernels whose only E-side work
+// after the update is E dipoles (they rewrite the rows of their targets), with one to
+// kMaxSnapBoxes box monitors. Exact, but slower on the 512^3 workload (the E update 1.228 against
+// 1.085 ms, the step 2.255 against 2.207 ms): the one lane per warp that holds a z-normal box's
+// cells delays its warp's release of every stage, in half the blocks.
+static void plan_snap_boxes(oem_plan* p) {
+  p->snapk = SnapBoxes{};
+  const char* ev = getenv("OEM_B200_SNAP");
+  if (!ev || strcmp(ev, "update") != 0) return;
+  if (p->is_complex || p->fused || p->basic_kernels != 3) return;
+  if (!p->planes.empty() || !p->tfsfs.empty() || !p->modesrcs.empty() || !p->mixes.empty() ||
+      !p->tensors.empty() || !p->absorbers.empty())
+    return;
+  int nb = 0;
+  for (const Monitor& m : p->mons) nb += m.kind == 1;
+  if (nb == 0 || nb > kMaxSnapBoxes) return;
+  for (const Monitor& m : p->mons) {
+    if (m.kind != 1) continue;
+    SnapBox& b = p->snapk.b[p->snapk.n++];
+    b.i0 = m.i0; b.ni = m.ni; b.j0 = m.j0; b.nj = m.nj; b.k0 = m.k0; b.nk = m.nk;
+    b.T = m.T;
+    b.cells = m.cells;
+    b.snap = m.d_snap;
+  }
+  p->snapk.step = p->d_step;
+}
+
 int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   int rc = check_plan(p, false);
   if (rc) return rc;
@@ -1657,6 +1754,7 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
     p->fused = true;
     set_bank(p, 0);
   }
+  plan_snap_boxes(p);
   p->energy_blocks = energy_block_count(P);
   if ((rc = dalloc(p, &p->d_energy_part, 3 * (size_t)p->energy_blocks))) return rc;
   // capture: G steps per graph for small grids (launch overhead), 1 for large ones
@@ -1761,38 +1859,14 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
                                      (int64_t)p->nx * p->ny * p->nzp / 32, 0, s)) != cudaSuccess)
           return cuda_error(e, "ade");
         OEM_CUDA(cudaEventRecord(E[5], s));
-        e = launch_update_e_ws(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s);
+        e = launch_update_e_ws(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s,
+                               snap_boxes(p, true));
       } else {
-        e = run_e(p, s);
+        e = run_e(p, s, snap_boxes(p, true));
       }
       if (e != cudaSuccess) return cuda_error(e, "update_e");
       OEM_CUDA(cudaEventRecord(E[3], s));
-      for (const PlaneSrc& src : p->planes)
-        if ((e = launch_plane_e(p->yp, src, p->d_step, s)) != cudaSuccess) return cuda_error(e, "plane_e");
-      for (const Tfsf& t : p->tfsfs)
-        if ((e = launch_tfsf(p->yp, t, 1, p->d_step, s)) != cudaSuccess) return cuda_error(e, "tfsf_e");
-      for (const ModeSrc& m : p->modesrcs)
-        if ((e = launch_mode_e(p->yp, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "mode_e");
-      for (const DipoleSet& d : p->dipoles)
-        if (!d.magnetic && (e = launch_dipoles(p->yp, d, p->d_step, s)) != cudaSuccess)
-          return cuda_error(e, "dipoles_e");
-      for (const MixSet& x : p->mixes)
-        if ((e = launch_mix_post(p->yp, x, s)) != cudaSuccess) return cuda_error(e, "mix_post");
-      for (const TensorSet& t : p->tensors)
-        if ((e = launch_tensor_post(p->yp, t, s)) != cudaSuccess) return cuda_error(e, "tensor_post");
-      for (const Absorber& a : p->absorbers)
-        if ((e = launch_absorb(p->yp, a, 1, s)) != cudaSuccess) return cuda_error(e, "absorb_e");
-      for (const TimeMon& m : p->tmons) {
-        if ((e = launch_time_sample(p->yp, m, p->d_step, 1, s)) != cudaSuccess) return cuda_error(e, "ts");
-        if ((e = launch_time_sample(p->yp, m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "ts");
-      }
-      for (const FluxTimeMon& m : p->ftmons)
-        if ((e = launch_flux_time(p->yp, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "ft");
-      for (const Monitor& m : p->mons) {
-        if ((e = launch_snapshot(p->yp, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "snap");
-        if ((e = launch_flush(m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "flush");
-      }
-      if ((e = launch_step_advance(p->d_step, s)) != cudaSuccess) return cuda_error(e, "step");
+      if ((rc = enqueue_e_side(p, s, true))) return rc;
       OEM_CUDA(cudaEventRecord(E[4], s));
     }
     if (n > 0) OEM_CUDA(cudaEventSynchronize(ev[(size_t)n * 6 - 2]));
@@ -1872,22 +1946,16 @@ int oem_plan_launches_per_step(oem_plan* p, int* n) {
   int rc = check_plan(p, true);
   if (rc) return rc;
   if (!n) return set_error(OEM_ERR_INVALID, "null output");
-  int c = p->fused ? 1 + 1 : 2 + 1;  // update_h, update_e (or the fused pair), step counter
-  if (p->basic_kernels == 3 && p->yp.has_ade) c += 1;  // separate pole pass
-  c += 2 * (int)p->planes.size();
-  c += 2 * (int)p->modesrcs.size();
-  c += 2 * (int)p->absorbers.size();
-  c += (int)p->mods.size();
-  for (const DipoleSet& d : p->dipoles) c += d.n_targets > 0 ? 1 : 0;
-  c += 2 * (int)p->tmons.size();
-  c += 3 * (int)p->mons.size();  // snapshot, flush, flush mark
-  c += 2 * (int)p->ftmons.size();
-  for (const Tfsf& t : p->tfsfs) c += (int)(t.e_groups.size() + t.h_groups.size());
-  c += 3 * (int)p->tensors.size();
-  c += 2 * (int)p->mixes.size();
-  if (p->cplx_ws) c += 2 + (int)(p->seam_h.size() + p->seam_e.size());
-  if (p->hist) c += 1;
-  *n = c;
+  // counted from the kernel nodes of the captured one-step graph
+  *n = p->step_kernels;
+  return OEM_OK;
+}
+
+int oem_plan_box_snapshots_in_update(oem_plan* p, int* n) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (!n) return set_error(OEM_ERR_INVALID, "null output");
+  *n = p->snapk.n;
   return OEM_OK;
 }
 
@@ -1936,19 +2004,88 @@ int oem_plan_read_monitor_interleaved(oem_plan* p, int id, double* out, void* st
     p->rd_chunk = std::min(most, (int64_t)1 << 22);
     for (int b = 0; b < 2; ++b)
       if ((rc = dalloc(p, &p->rd_scratch[b], (size_t)p->rd_chunk, false))) return rc;
+    if ((rc = dalloc(p, &p->d_rd_bad, 1))) return rc;
   }
   const int64_t kChunk = p->rd_chunk;
-  cudaError_t e = cudaSuccess;
-  for (int64_t q0 = 0, b = 0; q0 < n && e == cudaSuccess; q0 += kChunk, b ^= 1) {
-    const int64_t c = std::min(kChunk, n - q0);
-    e = launch_interleave(m.d_re + q0, m.d_im + q0, p->rd_scratch[b], c, s);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(out + 2 * q0, p->rd_scratch[b], (size_t)c * sizeof(double2),
-                          cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaMemsetAsync(p->d_rd_bad, 0, sizeof(unsigned long long), s);
+  const size_t cbytes = (size_t)kChunk * sizeof(double2);
+  // readouts of 16 MB and more go through the pinned halves (their copy-out threads also take
+  // the page faults of a fresh output array in parallel)
+  ReadStage* rs = (size_t)n * sizeof(double2) >= ((size_t)16 << 20) ? read_stage(p->device)
+                                                                      : nullptr;
+  std::unique_lock<std::mutex> lk;
+  if (rs) {
+    lk = std::unique_lock<std::mutex>(rs->mu);
+    if (rs->bytes < cbytes) {
+      for (int b = 0; b < 2; ++b) {
+        if (rs->half[b]) cudaFreeHost(rs->half[b]);
+        rs->half[b] = nullptr;
+        if (!rs->ev[b]) cudaEventCreateWithFlags(&rs->ev[b], cudaEventDisableTiming);
+      }
+      rs->bytes = 0;
+      if (cudaHostAlloc((void**)&rs->half[0], cbytes, cudaHostAllocDefault) == cudaSuccess &&
+          cudaHostAlloc((void**)&rs->half[1], cbytes, cudaHostAllocDefault) == cudaSuccess &&
+          rs->ev[0] && rs->ev[1]) {
+        rs->bytes = cbytes;
+      } else {
+        cudaGetLastError();
+        for (int b = 0; b < 2; ++b) {
+          if (rs->half[b]) cudaFreeHost(rs->half[b]);
+          rs->half[b] = nullptr;
+        }
+      }
+    }
+    if (rs->bytes < cbytes) {  // no pinned memory: the driver's pageable copies
+      lk.unlock();
+      rs = nullptr;
+    }
   }
+  if (rs) {
+    // chunk q: interleave, DMA into half q % 2; then copy chunk q - 1 out of the other half
+    int64_t prev0 = -1, prevc = 0;
+    for (int64_t q0 = 0, b = 0; e == cudaSuccess && (q0 < n || prev0 >= 0); q0 += kChunk, b ^= 1) {
+      const int64_t c = q0 < n ? std::min(kChunk, n - q0) : 0;
+      if (c > 0) {
+        e = launch_interleave(m.d_re + q0, m.d_im + q0, p->rd_scratch[b], c, p->d_rd_bad, s);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(rs->half[b], p->rd_scratch[b], (size_t)c * sizeof(double2),
+                              cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaEventRecord(rs->ev[b], s);
+      }
+      if (e == cudaSuccess && prev0 >= 0) {
+        e = cudaEventSynchronize(rs->ev[b ^ 1]);
+        if (e == cudaSuccess)
+          par_memcpy(reinterpret_cast<char*>(out + 2 * prev0), rs->half[b ^ 1],
+                     (size_t)prevc * sizeof(double2));
+      }
+      prev0 = c > 0 ? q0 : -1;
+      prevc = c;
+    }
+  } else {
+    for (int64_t q0 = 0, b = 0; q0 < n && e == cudaSuccess; q0 += kChunk, b ^= 1) {
+      const int64_t c = std::min(kChunk, n - q0);
+      e = launch_interleave(m.d_re + q0, m.d_im + q0, p->rd_scratch[b], c, p->d_rd_bad, s);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out + 2 * q0, p->rd_scratch[b], (size_t)c * sizeof(double2),
+                            cudaMemcpyDeviceToHost, s);
+    }
+  }
+  unsigned long long bad = 0;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&bad, p->d_rd_bad, sizeof(bad), cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return cuda_error(e, "read_monitor_interleaved");
   OEM_CUDA(cudaStreamSynchronize(s));
+  p->rd_nonfinite += (int64_t)bad;
   return check_device_error(p);
+}
+
+int oem_plan_readout_nonfinite(oem_plan* p, int64_t* count) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (!count) return set_error(OEM_ERR_INVALID, "null output");
+  *count = p->rd_nonfinite;
+  p->rd_nonfinite = 0;
+  return OEM_OK;
 }
 
 int oem_plan_read_time_monitor(oem_plan* p, int id, float* out, void* stream) {

@@ -170,7 +170,24 @@ struct Monitor {
   double* d_re = nullptr;    // (ncomp, nf, cells)
   double* d_im = nullptr;
   int* d_done = nullptr;     // last step already folded into the accumulators
+  unsigned* d_count = nullptr;  // blocks of the running flush that have finished
   int cplx = 0;              // complex fields: the ring holds ncomp real then ncomp imaginary rows
+};
+
+// Box DFT monitors whose snapshot rows the warp-specialised E update writes itself: E^{n+1}
+// from its registers, H^{n+1/2} from its staged tile, at the same positions and in the same
+// ring row as k_snap_box (the ring holds six rows per step, components in order). The E-side
+// dipole update then rewrites the rows of its few target cells that lie in a box.
+constexpr int kMaxSnapBoxes = 4;
+struct SnapBox {
+  int i0 = 0, ni = 0, j0 = 0, nj = 0, k0 = 0, nk = 0, T = 1;
+  int64_t cells = 0;
+  float* snap = nullptr;  // (T, 6, cells)
+};
+struct SnapBoxes {
+  int n = 0;
+  const int* step = nullptr;
+  SnapBox b[kMaxSnapBoxes];
 };
 
 // One absorber slab (Tidy3D's Absorber): the layers [g0, g0 + nlay) along `axis`, whole- and
@@ -354,6 +371,8 @@ struct oem_plan {
   oem::TmaMaps tma_i{};
   std::vector<oem::SeamFace> seam_h, seam_e;
   double2* rd_scratch[2] = {nullptr, nullptr};  // readout interleave buffers (lazy)
+  unsigned long long* d_rd_bad = nullptr;        // non-finite values seen by one readout
+  int64_t rd_nonfinite = 0;                      // since the last oem_plan_readout_nonfinite
   int64_t rd_chunk = 0;
 
   // device state
@@ -368,6 +387,7 @@ struct oem_plan {
   cudaGraphExec_t graph_many[2] = {nullptr, nullptr};  // per starting field bank
   cudaGraphExec_t graph_one[2] = {nullptr, nullptr};
   int graph_steps = 1;
+  int step_kernels = 0;  // kernel nodes of the one-step graph
 
   bool timing = false;
   std::vector<oem::TimingRec> trecs;
@@ -382,6 +402,7 @@ struct oem_plan {
   int* d_err = nullptr;   // set by a kernel whose bounded wait gave up
   int64_t* d_ade_segs = nullptr;  // segments with poles (separate pole pass)
   int64_t n_ade_segs = 0;
+  oem::SnapBoxes snapk{};  // box monitors whose snapshots the E update writes (n = 0: none)
   cudaStream_t side_stream = nullptr;  // branch of the captured step that runs the pole pass
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int xch = 8;            // x planes per thread in the streaming kernels
@@ -434,7 +455,7 @@ cudaError_t launch_plane_h(const YeeParams& P, const PlaneSrc& src, const int* s
 cudaError_t launch_plane_e(const YeeParams& P, const PlaneSrc& src, const int* step,
                            cudaStream_t s);
 cudaError_t launch_dipoles(const YeeParams& P, const DipoleSet& d, const int* step,
-                           cudaStream_t s);
+                           cudaStream_t s, const SnapBoxes* sb = nullptr);
 cudaError_t launch_time_sample(const YeeParams& P, const TimeMon& m, const int* step, int add,
                                cudaStream_t s);
 cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* step,
@@ -460,7 +481,7 @@ cudaError_t ws_setup_kernels();
 cudaError_t launch_update_h_ws(const TmaMaps& maps, const YeeParams& P, int xch, int* err,
                                cudaStream_t s);
 cudaError_t launch_update_e_ws(const TmaMaps& maps, const YeeParams& P, int xch, int n_mats,
-                               int* err, cudaStream_t s);
+                               int* err, cudaStream_t s, const SnapBoxes* sb = nullptr);
 cudaError_t launch_update_e_stream(const YeeParams& P, int xch, int n_mats, cudaStream_t s);
 cudaError_t launch_list_pole_segments(const YeeParams& P, int64_t nseg, int64_t* list,
                                       unsigned long long* count, cudaStream_t s);
@@ -483,7 +504,7 @@ cudaError_t launch_tensor_pre(const YeeParams& P, const TensorSet& t, cudaStream
 cudaError_t launch_tensor_post(const YeeParams& P, const TensorSet& t, cudaStream_t s);
 cudaError_t launch_mix_pre(const YeeParams& P, const MixSet& m, cudaStream_t s);
 cudaError_t launch_interleave(const double* re, const double* im, double2* out, int64_t n,
-                              cudaStream_t s);
+                              unsigned long long* bad, cudaStream_t s);
 cudaError_t launch_mix_post(const YeeParams& P, const MixSet& m, cudaStream_t s);
 
 // Discrete adjoint (oem_adjoint.cu): adjoint fields, their CPML psi, scratch for the transposed

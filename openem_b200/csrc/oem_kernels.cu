@@ -206,7 +206,7 @@ __global__ void k_plane_e(YeeParams P, PlaneSrc s, const int* step) {
 // Point dipoles, one thread per distinct (component, cell); its stencil points are added in a
 // fixed order, so the result is deterministic (openem/kernels/source_dft.cu:147-206 uses
 // atomicAdd instead).
-__global__ void k_dipoles(YeeParams P, DipoleSet d, const int* step) {
+__global__ void k_dipoles(YeeParams P, DipoleSet d, const int* step, SnapBoxes sb) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = *step;
   if (t >= d.n_targets || n < 0 || n >= d.nsteps1) return;
@@ -220,6 +220,19 @@ __global__ void k_dipoles(YeeParams P, DipoleSet d, const int* step) {
     v += -cc * d.d_coef[q] * a;
   }
   F[id] = v;
+  // E dipoles after an E update that wrote the box snapshots itself: the target's row in each
+  // box that holds it takes the injected value, as a snapshot taken after this kernel would
+  for (int m = 0; m < sb.n; ++m) {
+    const SnapBox& b = sb.b[m];
+    const int k = (int)(id % P.nzp);
+    const int j = (int)((id / P.nzp) % P.ny);
+    const int i = (int)(id / ((int64_t)P.nzp * P.ny));
+    if ((unsigned)(i - b.i0) >= (unsigned)b.ni || (unsigned)(j - b.j0) >= (unsigned)b.nj ||
+        (unsigned)(k - b.k0) >= (unsigned)b.nk)
+      continue;
+    const int64_t o = ((int64_t)(i - b.i0) * b.nj + (j - b.j0)) * b.nk + (k - b.k0);
+    b.snap[(int64_t)(n % b.T) * 6 * b.cells + (int64_t)c * b.cells + o] = v;
+  }
   if (d.d_amp_im) {  // complex plan: the imaginary part of the amplitude drives the im field
     float* Fi = P.fi[d.magnetic ? 3 + c : c];
     float w = Fi[id];
@@ -335,129 +348,124 @@ __global__ void k_snap_box(YeeParams P, Monitor m, const int* step) {
   }
 }
 
-// Batched DFT flush (openem/kernels/source_dft.cu:440-530): at a batch boundary, or when
-// forced, fold the not-yet-folded snapshot rows into the float64 accumulators. Per
-// (point, frequency) the rows are summed in step order into an fp32 partial, which is then
-// added to the float64 accumulator once. done[0] holds the last step already folded.
-template <int NC>
-__global__ void __launch_bounds__(128) k_flush(Monitor m, const int* step, int forced) {
+// Batched DFT flush (openem/kernels/source_dft.cu:440-530 real fields,
+// openem/kernels/bloch.cu:389-481 complex fields): at a batch boundary, or when forced, fold the
+// not-yet-folded snapshot rows into the float64 accumulators. Per (component, point, frequency)
+// the rows are summed in step order into an fp32 partial, which is then added to the float64
+// accumulator once; a complex ring holds NC real rows then NC imaginary rows per step and the
+// product is (u_re + i u_im)(cos + i sin). done[0] holds the last step already folded.
+//
+// One thread per (component, point), points fastest: it holds the batch's (at most 32)
+// snapshot values of its entry in registers, so the ring is read from memory once, and walks
+// every frequency; the phase rows of the batch are staged in shared memory a chunk of
+// frequencies at a time (the same float4 for every thread of a warp). Each accumulator is read
+// and written once per flush, coalesced over the points. A grid of a few blocks per SM strides
+// over tiles of 128 entries, so that the launch of a step without a batch boundary costs little.
+constexpr int kFlushF = 16;  // frequencies per staged phase chunk
+constexpr int kFlushG = 4;   // frequencies whose sums a thread forms together
+static_assert(kFlushF % kFlushG == 0, "whole groups per chunk");
+template <int NC, bool CPLX>
+__global__ void __launch_bounds__(128, 4) k_flush(Monitor m, const int* step, int forced) {
   const int s_now = forced ? (*step - 1) : *step;
   if (!forced && ((s_now + 1) % m.T) != 0) return;
-  const int s_lo = *m.d_done + 1;
+  // the ring holds the last T <= 32 steps: older unfolded rows (steps run without monitors)
+  // are gone and are not folded
+  const int s_lo = max(*m.d_done + 1, s_now - m.T + 1);
   if (s_lo > s_now) return;
-  constexpr int NE = NC / 2;  // E components come first
-  // grid-stride over the (frequency group, point) items, points fastest: each thread sums one
-  // point's rows for one group of 8 frequencies, so a plane with many frequencies spreads over
-  // many threads (the rows of a point come from L2 for every group after the first); at most a
-  // few blocks per SM, so that the launch of a step without a batch boundary costs little
-  const int64_t items = (int64_t)((m.nf + 7) / 8) * m.cells;
-  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items;
-       it += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t grp = it / m.cells;
-    const int64_t pt = it - grp * m.cells;
-    const int f0 = (int)grp * 8;
-    const int nfc = min(8, m.nf - f0);
-    float aR[8][NC], aI[8][NC];
+  const int ns = s_now - s_lo + 1;  // rows to fold, 1..T
+  constexpr int NE = NC / 2;        // E components come first
+  __shared__ float4 sph[32][kFlushF];
+  const int64_t cells = m.cells;
+  const int64_t items = (int64_t)NC * cells;
+  for (int64_t base = (int64_t)blockIdx.x * 128; base < items; base += (int64_t)gridDim.x * 128) {
+    const int64_t it = base + threadIdx.x;
+    const bool act = it < items;
+    const int c = act ? (int)(it / cells) : 0;
+    const int64_t pt = act ? it - (int64_t)c * cells : 0;
+    const bool isE = c < NE;
+    float vr[32], vi[32];
 #pragma unroll
-    for (int ff = 0; ff < 8; ++ff)
+    for (int q = 0; q < 32; ++q) {
+      vr[q] = 0.f;
+      vi[q] = 0.f;
+      if (act && q < ns) {
+        const int s = s_lo + q;
+        const float* row = m.d_snap + (int64_t)(s % m.T) * (CPLX ? 2 : 1) * NC * cells;
+        vr[q] = row[(int64_t)c * cells + pt];
+        if (CPLX) vi[q] = row[(int64_t)(NC + c) * cells + pt];
+      }
+    }
+    for (int f0 = 0; f0 < m.nf; f0 += kFlushF) {
+      const int nfc = min(kFlushF, m.nf - f0);
+      __syncthreads();  // the previous chunk's rows are no longer read
+      for (int e = threadIdx.x; e < ns * kFlushF; e += 128) {
+        const int q = e / kFlushF, ff = e - q * kFlushF;
+        if (ff < nfc)
+          sph[q][ff] = __ldg(reinterpret_cast<const float4*>(m.d_phase) +
+                             ((int64_t)(s_lo + q) * m.nf + f0 + ff));
+      }
+      __syncthreads();
+      // groups of kFlushG frequencies: the group's accumulators are loaded before its partial
+      // sums are formed, so their DRAM latency overlaps the arithmetic, and the group's
+      // independent sums interleave
+      for (int g = 0; g < nfc; g += kFlushG) {
+        const int ng = min(kFlushG, nfc - g);
+        double accR[kFlushG], accI[kFlushG];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) { aR[ff][c] = 0.f; aI[ff][c] = 0.f; }
-    for (int s = s_lo; s <= s_now; ++s) {
-      const float* row = m.d_snap + (int64_t)(s % m.T) * NC * m.cells;
-      float v[NC];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) v[c] = row[c * m.cells + pt];
-      const float4* ph = reinterpret_cast<const float4*>(m.d_phase) + ((int64_t)s * m.nf + f0);
-#pragma unroll
-      for (int ff = 0; ff < 8; ++ff) {
-        if (ff < nfc) {
-          const float4 q = __ldg(ph + ff);
-#pragma unroll
-          for (int c = 0; c < NC; ++c) {
-            aR[ff][c] = fmaf(v[c], c < NE ? q.x : q.z, aR[ff][c]);
-            aI[ff][c] = fmaf(v[c], c < NE ? q.y : q.w, aI[ff][c]);
+        for (int u = 0; u < kFlushG; ++u) {
+          accR[u] = 0.0;
+          accI[u] = 0.0;
+          if (act && u < ng) {
+            const int64_t o = ((int64_t)c * m.nf + f0 + g + u) * cells + pt;
+            accR[u] = m.d_re[o];
+            accI[u] = m.d_im[o];
           }
         }
-      }
-    }
+        float aR[kFlushG], aI[kFlushG];
 #pragma unroll
-    for (int ff = 0; ff < 8; ++ff) {
-      if (ff < nfc) {
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          const int64_t o = ((int64_t)c * m.nf + f0 + ff) * m.cells + pt;
-          m.d_re[o] += (double)aR[ff][c];
-          m.d_im[o] += (double)aI[ff][c];
+        for (int u = 0; u < kFlushG; ++u) {
+          aR[u] = 0.f;
+          aI[u] = 0.f;
         }
-      }
-    }
-  }
-}
-
-// Complex-field variant (openem/kernels/bloch.cu:389-481): the ring holds NC real rows then
-// NC imaginary rows; phasor += (u_re + i u_im)(cos + i sin) with the apodised phase.
-template <int NC>
-__global__ void __launch_bounds__(128) k_flush_c(Monitor m, const int* step, int forced) {
-  const int s_now = forced ? (*step - 1) : *step;
-  if (!forced && ((s_now + 1) % m.T) != 0) return;
-  const int s_lo = *m.d_done + 1;
-  if (s_lo > s_now) return;
-  constexpr int NE = NC / 2;
-  // grid-stride over (frequency group of 4, point) items, as in k_flush
-  const int64_t items = (int64_t)((m.nf + 3) / 4) * m.cells;
-  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items;
-       it += (int64_t)gridDim.x * blockDim.x) {
-    {
-      const int64_t grp = it / m.cells;
-      const int64_t pt = it - grp * m.cells;
-      const int f0 = (int)grp * 4;
-      const int nfc = min(4, m.nf - f0);
-      float aR[4][NC], aI[4][NC];
 #pragma unroll
-      for (int ff = 0; ff < 4; ++ff)
+        for (int q = 0; q < 32; ++q) {
+          if (q < ns) {
 #pragma unroll
-        for (int c = 0; c < NC; ++c) { aR[ff][c] = 0.f; aI[ff][c] = 0.f; }
-      for (int s = s_lo; s <= s_now; ++s) {
-        const float* row = m.d_snap + (int64_t)(s % m.T) * 2 * NC * m.cells;
-        float vr[NC], vi[NC];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          vr[c] = row[c * m.cells + pt];
-          vi[c] = row[(NC + c) * m.cells + pt];
-        }
-        const float4* ph = reinterpret_cast<const float4*>(m.d_phase) + ((int64_t)s * m.nf + f0);
-#pragma unroll
-        for (int ff = 0; ff < 4; ++ff) {
-          if (ff < nfc) {
-            const float4 q = __ldg(ph + ff);
-#pragma unroll
-            for (int c = 0; c < NC; ++c) {
-              const float co = c < NE ? q.x : q.z, si = c < NE ? q.y : q.w;
-              aR[ff][c] = fmaf(-vi[c], si, fmaf(vr[c], co, aR[ff][c]));
-              aI[ff][c] = fmaf(vi[c], co, fmaf(vr[c], si, aI[ff][c]));
+            for (int u = 0; u < kFlushG; ++u) {
+              const float4 ph = sph[q][g + u];
+              const float co = isE ? ph.x : ph.z, si = isE ? ph.y : ph.w;
+              if (CPLX) {
+                aR[u] = fmaf(-vi[q], si, fmaf(vr[q], co, aR[u]));
+                aI[u] = fmaf(vi[q], co, fmaf(vr[q], si, aI[u]));
+              } else {
+                aR[u] = fmaf(vr[q], co, aR[u]);
+                aI[u] = fmaf(vr[q], si, aI[u]);
+              }
             }
           }
         }
-      }
 #pragma unroll
-      for (int ff = 0; ff < 4; ++ff) {
-        if (ff < nfc) {
-#pragma unroll
-          for (int c = 0; c < NC; ++c) {
-            const int64_t o = ((int64_t)c * m.nf + f0 + ff) * m.cells + pt;
-            m.d_re[o] += (double)aR[ff][c];
-            m.d_im[o] += (double)aI[ff][c];
+        for (int u = 0; u < kFlushG; ++u) {
+          if (act && u < ng) {
+            const int64_t o = ((int64_t)c * m.nf + f0 + g + u) * cells + pt;
+            m.d_re[o] = accR[u] + (double)aR[u];
+            m.d_im[o] = accI[u] + (double)aI[u];
           }
         }
       }
     }
   }
-}
-
-__global__ void k_flush_mark(int T, const int* step, int* done, int forced) {
-  const int s_now = forced ? (*step - 1) : *step;
-  if (forced || ((s_now + 1) % T) == 0) {
-    if (s_now > *done) *done = s_now;
+  // the last block to finish records the folded step: every block read done[0] at its start
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(m.d_count, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    if (s_now > *m.d_done) *m.d_done = s_now;
+    *m.d_count = 0u;
   }
 }
 
@@ -593,9 +601,11 @@ cudaError_t launch_plane_e(const YeeParams& P, const PlaneSrc& src, const int* s
 }
 
 cudaError_t launch_dipoles(const YeeParams& P, const DipoleSet& d, const int* step,
-                           cudaStream_t s) {
+                           cudaStream_t s, const SnapBoxes* sb) {
   if (d.n_targets == 0) return cudaSuccess;
-  k_dipoles<<<(d.n_targets + 63) / 64, 64, 0, s>>>(P, d, step);
+  SnapBoxes none{};
+  const SnapBoxes& b = (sb && !d.magnetic && !d.d_amp_im) ? *sb : none;
+  k_dipoles<<<(d.n_targets + 63) / 64, 64, 0, s>>>(P, d, step, b);
   return cudaGetLastError();
 }
 
@@ -945,37 +955,42 @@ cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* ste
 }
 
 cudaError_t launch_flush(const Monitor& m, const int* step, int forced, cudaStream_t s) {
-  const int64_t groups = m.cplx ? (m.nf + 3) / 4 : (m.nf + 7) / 8;
-  const int64_t nb = std::min<int64_t>((groups * m.cells + 127) / 128, 148 * 8);
+  const int64_t nb = std::min<int64_t>(((int64_t)m.ncomp * m.cells + 127) / 128, 148 * 4);
+  if (m.T > 32) return cudaErrorInvalidValue;  // a thread holds at most 32 rows
   if (m.cplx) {
     if (m.ncomp == 4)
-      k_flush_c<4><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
+      k_flush<4, true><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
     else
-      k_flush_c<6><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
+      k_flush<6, true><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
   } else if (m.ncomp == 4) {
-    k_flush<4><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
+    k_flush<4, false><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
   } else {
-    k_flush<6><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
+    k_flush<6, false><<<(unsigned)nb, 128, 0, s>>>(m, step, forced);
   }
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  k_flush_mark<<<1, 1, 0, s>>>(m.T, step, m.d_done, forced);
   return cudaGetLastError();
 }
 
-// (re, im) pairs of n values side by side: the layout of a host complex128 array.
+// (re, im) pairs of n values side by side: the layout of a host complex128 array. Values with
+// a non-finite part are counted into *bad (one atomic per warp that saw any), so the host need
+// not scan the readout for them.
 __global__ void k_interleave(const double* __restrict__ re, const double* __restrict__ im,
-                             double2* __restrict__ out, int64_t n) {
+                             double2* __restrict__ out, int64_t n, unsigned long long* bad) {
+  unsigned cnt = 0;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
-       q += (int64_t)gridDim.x * blockDim.x)
-    out[q] = make_double2(re[q], im[q]);
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const double a = re[q], b = im[q];
+    cnt += (isfinite(a) && isfinite(b)) ? 0u : 1u;
+    out[q] = make_double2(a, b);
+  }
+  cnt = __reduce_add_sync(0xffffffffu, cnt);
+  if (cnt && (threadIdx.x & 31) == 0) atomicAdd(bad, (unsigned long long)cnt);
 }
 
 cudaError_t launch_interleave(const double* re, const double* im, double2* out, int64_t n,
-                              cudaStream_t s) {
+                              unsigned long long* bad, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   const int64_t nb = std::min<int64_t>((n + 255) / 256, 148 * 16);
-  k_interleave<<<(unsigned)nb, 256, 0, s>>>(re, im, out, n);
+  k_interleave<<<(unsigned)nb, 256, 0, s>>>(re, im, out, n, bad);
   return cudaGetLastError();
 }
 

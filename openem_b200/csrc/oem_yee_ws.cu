@@ -421,12 +421,15 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_h_ws(const __grid_con
   const int to = w * kTZ + 4 * lane;  // this quad in a tile
   for (int t = 0; t < np; ++t) {
     const int slot = t % kS;
-    bool got = mbar_wait(&full[slot], (uint32_t)((t / kS) & 1), err);
-    if (!__all_sync(kFull, got)) break;
-    const float* st = smem + slot * kHStage;
+    // the plane's axis values do not depend on the stage: their loads are issued before the
+    // wait, which hides their latency
     const int i = ib + t;
     const bool xsl = in_slab(X, i);
     const float mi = X.mnx[i], idx_ = X.idl_p[i];
+    const bool xfast = !xsl && i + 1 < P.nx && X.nxt[i] == i + 1 && mi == 1.0f;
+    bool got = mbar_wait(&full[slot], (uint32_t)((t / kS) & 1), err);
+    if (!__all_sync(kFull, got)) break;
+    const float* st = smem + slot * kHStage;
     const int64_t row = i * si + (int64_t)j * sj;
     if (kvm) {
       float ex[4], ey[4], ez[4], yex[4], yez[4], ney[4], nez[4], hx[4], hy[4], hz[4];
@@ -466,7 +469,7 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_h_ws(const __grid_con
         dxz[e] = fdiff(zex, mkz[e], ex[e], idz[e]);
       }
       if (zslm) z_cpml(dyz, dxz, zslm, st + kH_PZ, zt, P.psih, P, Z, i, j, kq, k0, w, lane);
-      if (yplain && !xsl && i + 1 < P.nx && X.nxt[i] == i + 1 && mi == 1.0f) {
+      if (yplain && xfast) {
         // x and y interior: unit masks, no x/y CPML (the same bits as below, n * 1 == n)
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
@@ -529,8 +532,44 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_h_ws(const __grid_con
 // ---------------------------------------------------------------------------------------------
 // E full step with the deferred ADE
 // ---------------------------------------------------------------------------------------------
+// Snapshot rows of the box monitors that hold cells of this quad (plane i, row j, cells kq ..
+// kq + 3): the six components at the cells' own Yee positions, E^{n+1} as just computed and
+// H^{n+1/2} from the staged halo box (hb: this quad's Hx; Hy, Hz follow at kBoxW strides),
+// into ring row step % T (srow: that row of each box, set once per block in shared memory),
+// the layout and values of k_snap_box. sbm: the boxes whose rows and z range hold cells of this
+// quad (fixed per lane), so that a lane with none skips the call.
+__device__ __forceinline__ void snap_quad(const SnapBoxes& sb, float* const* srow, unsigned sbm,
+                                          int i, int j, int kq, const float* ex, const float* ey,
+                                          const float* ez, const float* hb) {
+#pragma unroll
+  for (int m = 0; m < kMaxSnapBoxes; ++m) {
+    const SnapBox& b = sb.b[m];
+    if (!((sbm >> m) & 1u) || (unsigned)(i - b.i0) >= (unsigned)b.ni) continue;
+    float hx[4], hy[4], hz[4];
+    unpack4(lds4(hb), hx);
+    unpack4(lds4(hb + kBoxW), hy);
+    unpack4(lds4(hb + 2 * kBoxW), hz);
+    float* row = srow[m];
+    const int64_t base = ((int64_t)(i - b.i0) * b.nj + (j - b.j0)) * b.nk - b.k0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int k = kq + e;
+      if ((unsigned)(k - b.k0) >= (unsigned)b.nk) continue;
+      const int64_t o = base + k;
+      row[o] = ex[e];
+      row[b.cells + o] = ey[e];
+      row[2 * b.cells + o] = ez[e];
+      row[3 * b.cells + o] = hx[e];
+      row[4 * b.cells + o] = hy[e];
+      row[5 * b.cells + o] = hz[e];
+    }
+  }
+}
+
+template <bool SNAP>
 __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_constant__ TmaMaps maps, YeeParams P,
-                                                 int xch, int n_mats, int* err) {
+                                                 int xch, int n_mats, int* err,
+                                                 const __grid_constant__ SnapBoxes sb) {
   extern __shared__ __align__(128) float smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kS * kEStage);
   uint64_t* empty = full + kS;
@@ -539,6 +578,7 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
   uint32_t* segt = reinterpret_cast<uint32_t*>(smats + kSmemMats);  // [plane][row][start, end]
   // a barrier no thread arrives at (the wait-expiry check), after everything else
   uint64_t* never = reinterpret_cast<uint64_t*>(segt + kXMax * kTY * 2);
+  float** srow = reinterpret_cast<float**>(never + 1);  // this step's snapshot row of each box
   const int lane = threadIdx.x, w = threadIdx.y;
   const int tid = w * 32 + lane;
   const int k0 = blockIdx.x * kTZ;
@@ -558,6 +598,8 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
     mats = smats;
   }
   load_ztab(zt, Z, false, k0, P.nzp, tid, 160);
+  if (SNAP && tid < sb.n)
+    srow[tid] = sb.b[tid].snap + (int64_t)(*sb.step % sb.b[tid].T) * 6 * sb.b[tid].cells;
   if (w == 4 && lane == 0) {
     for (int s = 0; s < kS; ++s) {
       mbar_init(&full[s], 1);
@@ -689,8 +731,22 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
   const float cw = P.cw;
   const int ro = (w + 1) * kBZ + 4 + 4 * lane;  // this quad in the H halo box
   const int to = w * kTZ + 4 * lane;
+  unsigned sbm = 0;  // boxes with cells in this lane's row and z range
+  if (SNAP) {
+#pragma unroll
+    for (int m = 0; m < kMaxSnapBoxes; ++m) {
+      const SnapBox& b = sb.b[m];
+      if (m < sb.n && row_ok && (unsigned)(j - b.j0) < (unsigned)b.nj && kq < b.k0 + b.nk &&
+          kq + 4 > b.k0)
+        sbm |= 1u << m;
+    }
+  }
   for (int t = 0; t < np; ++t) {
     const int slot = t % kS;
+    // the plane's axis values, loaded before the wait as in the H update
+    const int i = ib + t;
+    const bool xsl = in_slab(X, i);
+    const float mi = X.mpv[i], idx_ = X.idl_d[i];
     bool got = mbar_wait(&full[slot], (uint32_t)((t / kS) & 1), err);
     // the plan's wait-expiry check: wait on a barrier nothing arrives at, with its short bound,
     // so that the expiry path (error word, early exit of every warp, the producer's drain) runs
@@ -700,7 +756,6 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
     const int* tab = reinterpret_cast<const int*>(st + kE_PT);
     const float* pool = st + kE_POOL;
     const float* jw = pool + tab[11];  // pole currents of the plane's rows
-    const int i = ib + t;
     uint32_t mid[4] = {0u, 0u, 0u, 0u};
     if (row_ok) {
       if (wide) {
@@ -728,8 +783,6 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
       gp = (uint32_t)tab[2 * w] + (uint32_t)pre;
       if (tab[2 * w + 1] >= 0) wp = tab[2 * w + 1] + pre;
     }
-    const bool xsl = in_slab(X, i);
-    const float mi = X.mpv[i], idx_ = X.idl_d[i];
     const int64_t row = i * si + (int64_t)j * sj;
     if (kvm) {
       float ex[4], ey[4], ez[4], hx[4], hy[4], hz[4], yhx[4], yhz[4], phy[4], phz[4];
@@ -833,6 +886,9 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
       *reinterpret_cast<float4*>(P.f[0] + row + kq) = make_float4(ex[0], ex[1], ex[2], ex[3]);
       *reinterpret_cast<float4*>(P.f[1] + row + kq) = make_float4(ey[0], ey[1], ey[2], ey[3]);
       *reinterpret_cast<float4*>(P.f[2] + row + kq) = make_float4(ez[0], ez[1], ez[2], ez[3]);
+      if constexpr (SNAP) {
+        if (sbm) snap_quad(sb, srow, sbm, i, j, kq, ex, ey, ez, st + kE_HB + ro);
+      }
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[slot]);
@@ -1342,7 +1398,8 @@ __global__ void __launch_bounds__(192, 2) k_he_ws(const __grid_constant__ FusedM
 size_t ws_h_smem() { return (size_t)kS * kHStage * 4 + 2 * kS * sizeof(uint64_t) + kZTab * 4; }
 size_t ws_e_smem() {
   return (size_t)kS * kEStage * 4 + (2 * kS + 1) * sizeof(uint64_t) + kZTab * 4 +
-         kSmemMats * sizeof(MatRec) + kXMax * kTY * 2 * sizeof(uint32_t);
+         kSmemMats * sizeof(MatRec) + kXMax * kTY * 2 * sizeof(uint32_t) +
+         kMaxSnapBoxes * sizeof(float*);
 }
 
 int ws_max_xchunk() { return kXMax; }
@@ -1388,12 +1445,13 @@ cudaError_t ws_setup_kernels() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_h_ws, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_e_ws, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)ws_e_smem());
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_e_ws, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared);
+  for (auto* k : {k_e_ws<false>, k_e_ws<true>}) {
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_e_smem());
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               cudaSharedmemCarveoutMaxShared);
+  }
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_he_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)he_smem());
   if (e == cudaSuccess)
@@ -1410,9 +1468,12 @@ cudaError_t launch_update_h_ws(const TmaMaps& maps, const YeeParams& P, int xch,
 }
 
 cudaError_t launch_update_e_ws(const TmaMaps& maps, const YeeParams& P, int xch, int n_mats,
-                               int* err, cudaStream_t s) {
+                               int* err, cudaStream_t s, const SnapBoxes* sb) {
   dim3 b(32, kTY + 1, 1), g((P.nzp + kTZ - 1) / kTZ, (P.ny + kTY - 1) / kTY, (P.nx + xch - 1) / xch);
-  k_e_ws<<<g, b, ws_e_smem(), s>>>(maps, P, xch, n_mats, err);
+  if (sb && sb->n > 0)
+    k_e_ws<true><<<g, b, ws_e_smem(), s>>>(maps, P, xch, n_mats, err, *sb);
+  else
+    k_e_ws<false><<<g, b, ws_e_smem(), s>>>(maps, P, xch, n_mats, err, SnapBoxes{});
   return cudaGetLastError();
 }
 

@@ -523,13 +523,16 @@ class Dispersion:
     def n_pole(self) -> int:
         return int(np.asarray(self.am1).size)
 
-    def validate(self, shape) -> None:
+    def validate_shapes(self) -> None:
         n = self.n_entry
         for nm, arr, want in (("g", self.g, n), ("am1", self.am1, self.n_pole),
                               ("b", self.b, self.n_pole)):
             if np.asarray(arr).shape != (want,):
                 raise ValueError(f"Dispersion.{nm} has shape {np.asarray(arr).shape}, "
                                  f"expected ({want},)")
+
+    def validate(self, shape) -> None:
+        self.validate_shapes()
         check_csr("Dispersion", shape, self.comp, self.cell,
                   [("pole_ofs", self.pole_ofs, self.n_pole)])
 

@@ -71,12 +71,13 @@ def step_bytes_per_cell_complex(sc) -> float:
     return (96.0 + 6.0) + (psi + mon) / n
 
 
-def kernel_bytes(sc) -> dict:
+def kernel_bytes(sc, box_snapshots_in_e: bool = False) -> dict:
     """Algorithmic bytes per launch of this engine's step kernels.
 
     ``update_h``: E read, H read and written (36 B per cell) plus the H-side psi of the slab
     cells. ``update_e``: H read, E read and written, the material index (38 B per cell), the
-    E-side psi, and one float32 polarisation current per dispersive (component, cell) entry.
+    E-side psi, one float32 polarisation current per dispersive (component, cell) entry, and,
+    when the E update writes the box monitors' snapshots itself, six float32 per box point.
     ``ade`` (the separate pole pass): each pole state read and written (16 B), and per entry
     E^n read and the current written (8 B). ``update_he`` (the fused step over two field banks):
     E and H each read once and written once (48 B per cell), the material index, both families'
@@ -85,8 +86,10 @@ def kernel_bytes(sc) -> dict:
     n = c["ncell"]
     psi = 16.0 * sum(c["slab_cells"].values())
     n_entry = 0 if sc.dispersion is None else int(sc.dispersion.n_entry)
+    snap = 24.0 * sum(int(np.prod(m.box)) for m in sc.field_monitors) if box_snapshots_in_e \
+        else 0.0
     return {"update_h": 36.0 * n + psi,
-            "update_e": 38.0 * n + psi + 4.0 * n_entry,
+            "update_e": 38.0 * n + psi + 4.0 * n_entry + snap,
             "ade": 16.0 * c["n_pole"] + 8.0 * n_entry,
             "update_he": 50.0 * n + 2.0 * psi + 4.0 * n_entry}
 

@@ -367,10 +367,18 @@ class Plan:
         return int(v.value)
 
     def read_monitor(self, mid: int, shape) -> np.ndarray:
-        out = host_array(shape, np.complex128)
+        # not pre-touched: the library's copy-out threads fault the pages in parallel
+        out = np.empty(shape, np.complex128)
         L.check(self.lib.oem_plan_read_monitor_interleaved(self.h, int(mid), L.ptr(out), self._s),
                 "read_monitor")
         return out
+
+    def readout_nonfinite(self) -> int:
+        """Phasor values with a non-finite part read out since the previous call (counted on
+        the device)."""
+        n = C.c_int64(0)
+        L.check(self.lib.oem_plan_readout_nonfinite(self.h, C.byref(n)), "readout_nonfinite")
+        return int(n.value)
 
     def adjoint_flux(self, mid: int, weights, dA1, dA2, box=None):
         """dJ/dca and dJ/dcb, (3, ni, nj, nk) float64 each, of ``J = sum_f weights[f] P_f``
@@ -431,6 +439,12 @@ class Plan:
         L.check(self.lib.oem_plan_energy(self.h, L.ptr(out), self._s), "energy")
         return out
 
+    def box_snapshots_in_update(self) -> int:
+        """Box monitors whose snapshots the E update kernel writes (no launch of their own)."""
+        n = C.c_int(0)
+        L.check(self.lib.oem_plan_box_snapshots_in_update(self.h, C.byref(n)))
+        return int(n.value)
+
     def launches_per_step(self) -> int:
         n = C.c_int()
         L.check(self.lib.oem_plan_launches_per_step(self.h, C.byref(n)))
@@ -467,13 +481,18 @@ class Plan:
             pass
 
     # ---- results -----------------------------------------------------------------------
+    def flux_phasor(self, m, mid: int, shp) -> Phasors:
+        return Phasors(name=m.name, data=self.read_monitor(mid, shp),
+                       freqs=np.asarray(m.freqs, dtype=np.float64))
+
+    def field_phasor(self, m, mid: int, shp) -> np.ndarray:
+        return self.read_monitor(mid, shp)
+
     def flux_phasors(self) -> dict:
-        return {m.name: Phasors(name=m.name, data=self.read_monitor(mid, shp),
-                                freqs=np.asarray(m.freqs, dtype=np.float64))
-                for m, mid, shp in self.flux_mons}
+        return {m.name: self.flux_phasor(m, mid, shp) for m, mid, shp in self.flux_mons}
 
     def field_phasors(self) -> dict:
-        return {m.name: self.read_monitor(mid, shp) for m, mid, shp in self.box_mons}
+        return {m.name: self.field_phasor(m, mid, shp) for m, mid, shp in self.box_mons}
 
     def flux_time(self, steps_run: int) -> dict:
         """``{name: (filled,) float64}`` of the flux time monitors after ``steps_run`` steps."""
@@ -591,19 +610,20 @@ def _loop(plan: Plan, sc, n_total: int, use_shutoff: bool, verbose: bool, return
     plan.flush()
     plan.status()  # waits for the stream: the steps are done when the clock stops
     wall = time.time() - t0
-    phasors = plan.flux_phasors()
-    fphas = plan.field_phasors()
+    # every monitor's readout counts its non-finite phasors on the device (no host scan)
+    plan.readout_nonfinite()
+    phasors, fphas = {}, {}
+    for tag, d, read in (("mon", phasors, plan.flux_phasor), ("fld", fphas, plan.field_phasor)):
+        for m, mid, shp in (plan.flux_mons if tag == "mon" else plan.box_mons):
+            d[m.name] = read(m, mid, shp)
+            if plan.readout_nonfinite():
+                print(f"[openem_b200] warning: monitor {tag}:{m.name} holds non-finite values; "
+                      "the field has most likely diverged", flush=True)
     tsamp, tslots = plan.time_samples(steps)
     fields = {}
     if return_fields:
         for c, nm in enumerate(COMPONENTS):
             fields[nm] = plan.read_field(c)
-    for tag, d in (("mon", phasors), ("fld", fphas)):
-        for nm, obj in d.items():
-            a = np.asarray(obj.data if hasattr(obj, "data") else obj)
-            if a.size and not np.isfinite(a).all():
-                print(f"[openem_b200] warning: monitor {tag}:{nm} holds non-finite values; the "
-                      "field has most likely diverged", flush=True)
     return Result(phasors=phasors, steps_run=steps, shutoff_triggered=triggered,
                   decay_trace=trace,
                   energy_trace=shutoff_mod.energy_trace(pol),

@@ -298,37 +298,63 @@ def tensor_tables(sc, tabs) -> dict | None:
             "m1": f32(m1), "m2": f32(m2), "pec": f32(pf)}
 
 
-def entry_pole_sets(sc, bulk_shortcut: bool = True):
+_POOL = None
+
+
+def _par_all(test, n: int, parts: int = 8) -> bool:
+    """``all(test(lo, hi))`` over ``parts`` slices of range(n), on worker threads (numpy's
+    elementwise work releases the GIL, so large scans run in parallel)."""
+    global _POOL
+    if n < (1 << 20):
+        return bool(test(0, n))
+    if _POOL is None:
+        from concurrent.futures import ThreadPoolExecutor
+        _POOL = ThreadPoolExecutor(max_workers=parts)
+    step = -(-n // parts)
+    return all(_POOL.map(lambda lo: bool(test(lo, min(lo + step, n))), range(0, n, step)))
+
+
+def _rows_equal_first(a: np.ndarray) -> bool:
+    """Every row of a 2D array equal to the first, bit for bit."""
+    v = np.ascontiguousarray(a).view(np.uint64).reshape(a.shape[0], -1)
+    return _par_all(lambda lo, hi: np.all(v[lo:hi] == v[0]), v.shape[0])
+
+
+def entry_pole_sets(sc, bulk_shortcut: bool = True, validate: bool = True):
     """Deduplicate ADE entries by their float32 coefficient lists.
 
     Returns ``(comp, cell, set_id, set_ofs, coef, counts)``: per entry its component, flat cell
     and pole-set id; per set its first pole in ``coef`` ((n, 4) float32 rows
-    ``Re(A-1), Im(A-1), Re(B), Im(B)``) and its pole count. ``None`` without dispersion."""
+    ``Re(A-1), Im(A-1), Re(B), Im(B)``) and its pole count. ``None`` without dispersion.
+    ``validate=False`` skips the table checks, for a caller that has made them."""
     d = sc.dispersion
     if d is None or d.n_entry == 0:
         return None
-    d.validate(sc.shape)
-    comp = np.asarray(d.comp, dtype=np.int64)
-    cell = np.asarray(d.cell, dtype=np.int64)
-    ofs = np.asarray(d.pole_ofs, dtype=np.int64)
+    if validate:
+        d.validate(sc.shape)
+    comp = np.asarray(d.comp)
+    cell = np.asarray(d.cell)
+    ofs = np.asarray(d.pole_ofs)
+    am1 = np.asarray(d.am1, dtype=np.complex128)
+    b = np.asarray(d.b, dtype=np.complex128)
+    n = d.n_entry
+    k0 = int(ofs[1] - ofs[0])
+    if bulk_shortcut and 0 < k0 <= 15 and int(ofs[0]) == 0 and \
+            _par_all(lambda lo, hi: np.all(np.diff(ofs[lo:hi + 1]) == k0), n):
+        # every entry carries k0 poles (offsets i * k0) and, when their float64 bits agree, the
+        # same coefficient list (a bulk medium): one set, found without converting every pole
+        # (equal float64 values give equal float32 rows; anything else takes the general path)
+        A = am1.reshape(n, k0)
+        B = b.reshape(n, k0)
+        if _rows_equal_first(A) and _rows_equal_first(B):
+            row = np.empty((k0, 4), dtype=np.float32)
+            row[:, 0], row[:, 1], row[:, 2], row[:, 3] = A[0].real, A[0].imag, B[0].real, B[0].imag
+            return (comp, cell, np.zeros(n, dtype=np.int64),
+                    np.asarray([0, k0], dtype=np.int32), row, np.asarray([k0], dtype=np.int32))
+    ofs = ofs.astype(np.int64)
     npole = np.diff(ofs)
     if npole.max() > 15:
         raise NotImplementedError("more than 15 poles on one component")
-    am1 = np.asarray(d.am1, dtype=np.complex128)
-    b = np.asarray(d.b, dtype=np.complex128)
-    k0 = int(npole[0])
-    if bulk_shortcut and k0 > 0 and np.all(npole == k0) and \
-            np.all(ofs[:-1] == np.arange(d.n_entry) * k0):
-        # every entry carries the same coefficient list (a bulk medium): one set, found without
-        # converting every pole (equal float64 values give equal float32 rows; anything else
-        # takes the general path below)
-        A = am1.reshape(d.n_entry, k0)
-        B = b.reshape(d.n_entry, k0)
-        if np.all(A == A[0]) and np.all(B == B[0]):
-            row = np.empty((k0, 4), dtype=np.float32)
-            row[:, 0], row[:, 1], row[:, 2], row[:, 3] = A[0].real, A[0].imag, B[0].real, B[0].imag
-            return (comp, cell, np.zeros(d.n_entry, dtype=np.int64),
-                    np.asarray([0, k0], dtype=np.int32), row, np.asarray([k0], dtype=np.int32))
     pc = np.empty((am1.size, 4), dtype=np.float32)
     pc[:, 0], pc[:, 1], pc[:, 2], pc[:, 3] = am1.real, am1.imag, b.real, b.imag
     set_id = np.full(d.n_entry, -1, dtype=np.int64)

@@ -51,23 +51,30 @@ def _to_dev(a, torch, dev, dtype=None):
 
 
 class _PinnedStager:
-    """Host-to-device copies of large arrays through two halves of one pinned buffer: the host
-    copies chunk q into one half (torch's multi-threaded memcpy) while the DMA of chunk q - 1
-    drains the other, so the transfer runs near the link rate instead of through the driver's
-    pageable staging. One buffer per process, made on first use; used by one thread at a time."""
+    """Host-to-device copies of large arrays through two halves of one pinned buffer: host
+    threads copy chunk q into one half (numpy copies release the GIL, so the threads run in
+    parallel) while the DMA of chunk q - 1 drains the other, so the transfer runs near the link
+    rate instead of through the driver's single-threaded pageable staging. One buffer per
+    process, made on first use; used by one thread at a time."""
 
     CHUNK = 64 << 20
+    THREADS = 8
     _buf = None
+    _pool = None
 
     @classmethod
     def copy(cls, a: np.ndarray, torch, dev):
         a = np.ascontiguousarray(a)
         if a.nbytes < 2 * cls.CHUNK:
             return torch.from_numpy(a).to(dev)
-        if cls._buf is None:
+        if cls._buf is None or cls._buf.numel() < 2 * cls.CHUNK:
             cls._buf = torch.empty(2 * cls.CHUNK, dtype=torch.uint8, pin_memory=True)
+        if cls.THREADS > 1 and cls._pool is None:
+            from concurrent.futures import ThreadPoolExecutor
+            cls._pool = ThreadPoolExecutor(max_workers=cls.THREADS)
         dst = torch.empty(a.shape, dtype=torch.from_numpy(a[:0]).dtype, device=dev)
-        src = torch.from_numpy(a.reshape(-1).view(np.uint8))
+        src = a.reshape(-1).view(np.uint8)
+        buf = cls._buf.numpy()
         out = dst.view(-1).view(torch.uint8)
         stream = torch.cuda.current_stream(dev)
         done = [None, None]
@@ -76,9 +83,17 @@ class _PinnedStager:
             n = min(cls.CHUNK, a.nbytes - off)
             if done[half] is not None:
                 done[half].synchronize()  # the DMA out of this half has finished
-            stage = cls._buf[half * cls.CHUNK: half * cls.CHUNK + n]
-            stage.copy_(src[off:off + n])
-            out[off:off + n].copy_(stage, non_blocking=True)
+            base = half * cls.CHUNK
+            if cls.THREADS > 1:
+                per = -(-n // cls.THREADS)  # bytes per thread, rounded up to whole pages
+                step = (per + 4095) // 4096 * 4096
+                list(cls._pool.map(
+                    lambda r: np.copyto(buf[base + r:base + min(r + step, n)],
+                                        src[off + r:off + min(r + step, n)]),
+                    range(0, n, step)))
+            else:
+                np.copyto(buf[base:base + n], src[off:off + n])
+            out[off:off + n].copy_(cls._buf[base:base + n], non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(stream)
             done[half] = ev
@@ -140,33 +155,86 @@ def material_tables_device(sc, tabs, device: int = 0) -> DeviceTables:
         up.close()
 
 
+def _check_entries_device(name, shape, comp, cell, ofs_list, torch, dev):
+    """The checks of ``model.check_csr`` (ranges, monotone offsets, (comp, cell) uniqueness, the
+    same messages) made on the device; returns the entries' components and cells there."""
+    comp = np.asarray(comp)
+    cell = np.asarray(cell)
+    n = int(comp.size)
+    ncell = int(np.prod(shape))
+    if comp.shape != (n,) or cell.shape != (n,):
+        raise ValueError(f"{name}: comp/cell lengths differ")
+    comp_d = _to_dev(comp, torch, dev, torch.int64)
+    cell_d = _to_dev(cell, torch, dev, torch.int64)
+    if n == 0:
+        return comp_d, cell_d
+    lo_c, hi_c, lo_k, hi_k = (int(v) for v in torch.stack(
+        [comp_d.min(), comp_d.max(), cell_d.min(), cell_d.max()]).cpu())
+    if lo_c < 0 or hi_c > 2:
+        raise ValueError(f"{name}: comp out of range {lo_c}..{hi_c}")
+    if lo_k < 0 or hi_k >= ncell:
+        raise ValueError(f"{name}: cell out of range {hi_k} >= {ncell}")
+    for oname, ofs, npole in ofs_list:
+        ofs = np.asarray(ofs)
+        if ofs.shape != (n + 1,):
+            raise ValueError(f"{name}.{oname} has shape {ofs.shape}, expected ({n + 1},)")
+        if ofs[0] != 0 or ofs[-1] != npole:
+            raise ValueError(f"{name}.{oname} endpoints {ofs[0]}..{ofs[-1]}, expected 0..{npole}")
+        od = _to_dev(ofs, torch, dev, torch.int64)
+        if bool((od[1:] < od[:-1]).any()):
+            raise ValueError(f"{name}.{oname} is not monotonic")
+    key = comp_d * ncell + cell_d
+    if n >= 2 and not bool((key[1:] > key[:-1]).all()):  # unordered: count the distinct keys
+        nu = int(torch.unique(key).numel())
+        if nu != n:
+            raise ValueError(f"{name}: {n - nu} duplicate (comp, cell) entries")
+    return comp_d, cell_d
+
+
 def _material_tables_device(sc, tabs, torch, dev, up) -> DeviceTables:
     shape = tuple(int(v) for v in sc.shape)
     nx, ny, nz = shape
     ncell = nx * ny * nz
-    ep = T.entry_pole_sets(sc)
-    if ep is not None:
-        comp_e, cell_e, set_e, set_ofs, coef, counts = ep
-        comp_d = _to_dev(comp_e, torch, dev)
-        cell_d = _to_dev(cell_e, torch, dev)
-        set_d = _to_dev(set_e, torch, dev)
-        g_d = _to_dev(np.asarray(sc.dispersion.g, np.float64), torch, dev)
-    else:
-        set_ofs, coef, counts = np.zeros(1, np.int32), np.zeros((0, 4), np.float32), np.zeros(0, np.int32)
+    d = sc.dispersion
+    disp = d is not None and d.n_entry > 0
+    pole_fut = pole_pool = None
+    if disp:
+        # the entry table checked on the device before any device indexing with it; the host
+        # deduplicates the pole sets on a worker thread meanwhile (they are needed only for the
+        # second key of each component, after the coefficients of all three)
+        d.validate_shapes()
+        comp_d, cell_d = _check_entries_device("Dispersion", shape, d.comp, d.cell,
+                                               [("pole_ofs", d.pole_ofs, d.n_pole)], torch, dev)
+        from concurrent.futures import ThreadPoolExecutor
+        pole_pool = ThreadPoolExecutor(max_workers=1)
+        pole_fut = pole_pool.submit(T.entry_pole_sets, sc, True, False)
+        g_d = _to_dev(np.asarray(d.g, np.float64), torch, dev)
+        sel = [torch.nonzero(comp_d == c).squeeze(1) for c in range(3)]  # entries per component
+    try:
+        return _material_tables_from(sc, tabs, torch, dev, up, shape, disp,
+                                     (comp_d, cell_d, g_d, sel) if disp else None, pole_fut)
+    finally:
+        if pole_pool is not None:
+            pole_pool.shutdown(wait=True)
+
+
+def _material_tables_from(sc, tabs, torch, dev, up, shape, disp, ent, pole_fut) -> DeviceTables:
+    nx, ny, nz = shape
+    ncell = nx * ny * nz
     pecs = (sc.pec_ex, sc.pec_ey, sc.pec_ez)
     dt = float(sc.dt)
-    keys, ca_l, cb_l, eps_l, ps_l = [], [], [], [], []
+    # each key's rank among its distinct values: the coefficient key of a component while the
+    # next one uploads, the (eps, pole set) key once the pole sets are known
+    inv1, card1, inv2, card2, ca_l, cb_l, eps_l, ps_l = [], [], [], [], [], [], [], []
     mask32 = 0xFFFFFFFF
     for c in range(3):
         eps, sg = up.get(c)
         s = torch.zeros_like(eps) if sg is None else sg * dt / (2.0 * T.EPSILON_0)
         del sg
         gg = torch.zeros_like(eps)
-        ps = torch.full((ncell,), -1, dtype=torch.int64, device=dev)
-        if ep is not None:
-            m = comp_d == c
-            gg[cell_d[m]] = g_d[m]
-            ps[cell_d[m]] = set_d[m]
+        if disp:
+            _, cell_d, g_d, sel = ent
+            gg[cell_d[sel[c]]] = g_d[sel[c]]
         den = eps + s + gg
         ca = ((eps - s) / den).to(torch.float32)
         cb = ((dt / T.EPSILON_0) / den).to(torch.float32)
@@ -202,22 +270,50 @@ def _material_tables_device(sc, tabs, torch, dev, up) -> DeviceTables:
         del eps
         k1 = ((ca.view(torch.int32).to(torch.int64) & mask32) << 32) \
             | (cb.view(torch.int32).to(torch.int64) & mask32)
-        k2 = ((ef.view(torch.int32).to(torch.int64) & mask32) << 32) | (ps + 1)
-        keys += [k1, k2]
+        u, inv = torch.unique(k1, return_inverse=True)
+        inv1.append(inv)
+        card1.append(int(u.numel()))
+        del k1, u
         ca_l.append(ca)
         cb_l.append(cb)
         eps_l.append(ef)
+    ep = pole_fut.result() if disp else None
+    if ep is not None:
+        _, _, set_e, set_ofs, coef, counts = ep
+        set_d = _to_dev(set_e, torch, dev)
+    else:
+        set_ofs, coef, counts = np.zeros(1, np.int32), np.zeros((0, 4), np.float32), np.zeros(0, np.int32)
+    for c in range(3):
+        ps = torch.full((ncell,), -1, dtype=torch.int64, device=dev)
+        if ep is not None:
+            _, cell_d, _, sel = ent
+            ps[cell_d[sel[c]]] = set_d[sel[c]]
+        k2 = ((eps_l[c].view(torch.int32).to(torch.int64) & mask32) << 32) | (ps + 1)
+        u, inv = torch.unique(k2, return_inverse=True)
+        inv2.append(inv)
+        card2.append(int(u.numel()))
+        del k2, u
         ps_l.append(ps)
-    # running code = inverse of the unique of (previous code, next key code)
-    code = None
-    n = 1
-    for k in keys:
-        u, inv = torch.unique(k, return_inverse=True)
-        comb = inv if code is None else code * int(u.numel()) + inv
+    # the keys in component order, coefficient key first: (x1, x2, y1, y2, z1, z2)
+    invs = [v for c in range(3) for v in (inv1[c], inv2[c])]
+    card = [v for c in range(3) for v in (card1[c], card2[c])]
+    del inv1, inv2
+    # material code = rank of the cell's six key ranks in lexicographic order: one unique of
+    # their mixed-radix number when it fits in 62 bits, else a running code (the inverse of the
+    # unique of (previous code, next key rank)) -- the same codes either way
+    if float(np.prod(np.asarray(card, dtype=np.float64))) < 2.0 ** 62:
+        comb = invs[0]
+        for inv, nk in zip(invs[1:], card[1:]):
+            comb = comb * nk + inv
         uu, code = torch.unique(comb, return_inverse=True)
-        n = int(uu.numel())
-    del keys
-    n_mat = n
+        del comb
+    else:
+        code = None
+        for inv, nk in zip(invs, card):
+            comb = inv if code is None else code * nk + inv
+            uu, code = torch.unique(comb, return_inverse=True)
+    del invs
+    n_mat = int(uu.numel())
     rep = torch.empty(n_mat, dtype=torch.int64, device=dev)
     rep.scatter_(0, code, torch.arange(ncell, device=dev))
     rec = np.zeros((n_mat, 16), dtype=np.uint32)

@@ -142,6 +142,34 @@ def test_pipelined_kernels_equal_basic_kernels(monkeypatch, kind, n, n_pml):
         assert rel_l2(b.field_phasors[name], a.field_phasors[name]) < 1e-6, name
 
 
+@pytest.mark.parametrize("n", [42, 48])
+def test_box_snapshots_in_e_update_equal_snapshot_kernel(monkeypatch, n):
+    """With OEM_B200_SNAP=update the E update writes the box monitors' snapshot rows itself (E
+    from its registers, H from its staged tile) and the E dipoles rewrite the rows of their
+    targets: the phasors equal, bit for bit, those of the separate snapshot kernel (the
+    default). The centre dipole lies inside all three boxes; 42 cells leave partial tiles in y
+    and z."""
+    monkeypatch.setenv("OEM_B200_KERNELS", "ws")
+    sc = scenes.dispersive_spheres(n=n, n_sph=3, num_steps=150, nfreq=3,
+                                   rmin=0.05 * scenes.UM, rmax=0.1 * scenes.UM)
+    dip = sc.dipoles[0]
+    h = n // 2
+    idx = np.asarray(dip.indices)
+    assert ((idx >= h - 1) & (idx <= h)).all()  # the dipole's cells lie in every box
+    a = solver.run(sc, use_shutoff=False, return_fields=True, verbose=False)
+    monkeypatch.setenv("OEM_B200_SNAP", "update")
+    b = solver.run(sc, use_shutoff=False, return_fields=True, verbose=False)
+    plan = solver.Plan(sc, 10)
+    assert plan.box_snapshots_in_update() == 3
+    plan.close()
+    assert set(a.field_phasors) == {"mid_x", "mid_y", "mid_z"}
+    for name in a.field_phasors:
+        np.testing.assert_array_equal(b.field_phasors[name], a.field_phasors[name])
+    for nm in a.fields:
+        np.testing.assert_array_equal(b.fields[nm], a.fields[nm])
+    assert float(np.abs(a.field_phasors["mid_z"]).max()) > 0.0
+
+
 @pytest.mark.parametrize("kind", ["stream", "tma", "ws"])
 def test_pipelined_kernels_periodic_slab(monkeypatch, kind):
     """Periodic x/y walls of a one-cell-wide column (every neighbour wraps) and a plane-wave

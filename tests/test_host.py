@@ -396,3 +396,39 @@ def test_nonfinite_material_coefficients_are_named(capsys):
     bad = replace(sc, eps_ey=eps)
     Plan._warn_nonfinite_materials(T.material_tables(bad, [T.axis_tables(bad, a) for a in range(3)]).table)
     assert "non-finite" in capsys.readouterr().out
+
+
+def test_device_entry_checks_match_host_checks():
+    """The device table builder checks the dispersion entry table on the device before indexing
+    with it; on torch CPU tensors here, every failure gives check_csr's message and a valid
+    table passes."""
+    import torch
+    from openem_b200 import tables_gpu as TG
+    shape = (4, 5, 6)
+    ncell = 120
+    comp = np.array([0, 0, 1, 2], np.int64)
+    cell = np.array([3, 7, 7, 119], np.int64)
+    ofs = np.array([0, 2, 4, 4, 6], np.int64)
+    cases = [
+        (comp, cell, ofs, None),
+        (np.array([0, 3, 1, 2]), cell, ofs, "comp out of range"),
+        (comp, np.array([3, 7, 7, 120]), ofs, "cell out of range"),
+        (comp, cell, np.array([0, 2, 1, 4, 6]), "not monotonic"),
+        (comp, cell, np.array([0, 2, 4, 4, 5]), "endpoints"),
+        (comp[:3], cell, ofs, "lengths differ"),
+        (np.array([1, 0, 1, 2]), np.array([7, 3, 7, 119]), ofs, "duplicate"),
+        (np.array([1, 0, 0, 2]), np.array([7, 3, 5, 119]), ofs, None),  # unordered, unique
+    ]
+    for cc, kk, oo, msg in cases:
+        host_err = dev_err = None
+        try:
+            M.check_csr("Dispersion", shape, cc, kk, [("pole_ofs", oo, 6)])
+        except ValueError as e:
+            host_err = str(e)
+        try:
+            TG._check_entries_device("Dispersion", shape, cc, kk, [("pole_ofs", oo, 6)], torch,
+                                     torch.device("cpu"))
+        except ValueError as e:
+            dev_err = str(e)
+        assert host_err == dev_err, (msg, host_err, dev_err)
+        assert (msg is None) == (host_err is None) and (msg is None or msg in host_err)
