@@ -566,6 +566,109 @@ __device__ __forceinline__ void snap_quad(const SnapBoxes& sb, float* const* sro
   }
 }
 
+// The E update's producer warp: per plane of the chunk it waits for a free stage and stages the
+// H halo box, the Hy/Hz tiles of the previous plane, the E and material tiles (TMA), the plane's
+// psi rows and the window of pole currents of its dispersive rows (bulk copies), then drains its
+// own copies before it returns. Lane 0 issues; the warp first reads the chunk's pole ranges.
+__device__ __forceinline__ void e_producer(const TmaMaps& maps, const YeeParams& P, float* smem,
+                                           uint64_t* full, uint64_t* empty, uint32_t* segt,
+                                           int* err, int ib, int np, int j0, int k0, int lane) {
+  const DevAxis& X = P.ax[0];
+  const bool wide = P.mat32 != nullptr;
+  // pole ranges of every (plane, row) of the chunk: the first pole of the tile row and the
+  // end of its last segment, all fetched at once by the producer warp
+  const int64_t nseg = (int64_t)P.nx * P.ny * P.nzp / 32;
+  const int nst = min(4, (P.nzp - k0) / 32);
+  if (P.has_ade) {
+    for (int t = lane; t < np * kTY; t += 32) {
+      const int i = ib + t / kTY, j = j0 + t % kTY;
+      uint32_t a = 0u, b = 0u;
+      if (j < P.ny) {
+        const int64_t s0 = (((int64_t)i * P.ny + j) * P.nzp + k0) >> 5;
+        a = __ldg(P.seg_ofs + s0);
+        b = (s0 + nst < nseg) ? __ldg(P.seg_ofs + s0 + nst) : P.n_pole_total;
+      }
+      segt[2 * t] = a;
+      segt[2 * t + 1] = b;
+    }
+    __syncwarp();
+  }
+  if (lane != 0) return;
+  int issued = 0;
+  bool ok = true;
+  const uint32_t mbytes = (uint32_t)(kTY * kTZ * (wide ? 4 : 2));
+  // the tile's y and z psi rows are fixed once; per plane only the x slab rows are added.
+  // Pool layout per plane: x rows (1024 floats), y rows (1024), z rows (512) where present,
+  // then the pole-current window.
+  const PsiTile pt = psi_tile(P, j0, k0);
+  for (int q = 0; q < np && ok; ++q) {
+    const int slot = q % kS;
+    const int i = ib + q;
+    const bool xsl = in_slab(X, i);
+    int offs[3] = {-1, -1, -1};
+    int wbase = 0;
+    if (xsl) { offs[0] = wbase; wbase += 1024; }
+    if (pt.ymask) { offs[1] = wbase; wbase += 1024; }
+    if (pt.zs0 || pt.zs1) { offs[2] = wbase; wbase += 512; }
+    const int cap = kEPool - wbase;  // pole currents (floats) this plane can stage
+    int pstart[kTY], poff[kTY], pcnt[kTY];
+    int used = 0;
+#pragma unroll
+    for (int r = 0; r < kTY; ++r) {
+      const uint32_t a = P.has_ade ? segt[2 * (q * kTY + r)] : 0u;
+      const uint32_t b = P.has_ade ? segt[2 * (q * kTY + r) + 1] : 0u;
+      pstart[r] = (int)a; poff[r] = -2; pcnt[r] = 0;
+      if (b <= a) continue;
+      const int a16 = (int)(a & ~3u);  // 16-byte aligned start
+      const int n4 = (int)(((b - (uint32_t)a16) + 3u) & ~3u);
+      if (used + n4 <= cap) {
+        poff[r] = used + ((int)a - a16);
+        pcnt[r] = n4;
+        used += n4;
+      } else {
+        poff[r] = -1;  // consumers read this row's poles from global memory
+      }
+    }
+    if (q >= kS) ok = mbar_wait_live(&empty[slot], (uint32_t)((q / kS - 1) & 1), err, kPolls);
+    if (!ok) break;
+    float* st = smem + slot * kEStage;
+    int* tab = reinterpret_cast<int*>(st + kE_PT);
+    const int iprev = (i > 0) ? i - 1 : X.prv[0];
+    uint32_t bytes = 3 * kWideBytes + 5 * kTileBytes + mbytes + pt.yzbytes +
+                     (xsl ? pt.xbytes : 0u) + (uint32_t)used * 4;
+#pragma unroll
+    for (int r = 0; r < kTY; ++r) {
+      tab[2 * r] = pstart[r];
+      tab[2 * r + 1] = poff[r];
+    }
+    tab[8] = offs[0];
+    tab[9] = offs[1];
+    tab[10] = offs[2];
+    tab[11] = wbase;
+    mbar_expect_tx(&full[slot], bytes);
+    for (int c = 0; c < 3; ++c) {
+      tma3(st + kE_HB + c * kBoxW, &maps.h_wide[c], &full[slot], k0 - 4, j0 - 1, i);
+      tma3(st + kE_ET + c * 512, &maps.e_tile[c], &full[slot], k0, j0, i);
+    }
+    tma3(st + kE_HP, &maps.h_tile[1], &full[slot], k0, j0, iprev);
+    tma3(st + kE_HP + 512, &maps.h_tile[2], &full[slot], k0, j0, iprev);
+    tma3(st + kE_MT, &maps.m_tile, &full[slot], k0, j0, i);
+    float* pool = st + kE_POOL;
+    stage_psi(pt, P.psie, P, pool + offs[0], pool + offs[1], pool + offs[2], &full[slot], i, j0,
+              k0, xsl);
+#pragma unroll
+    for (int r = 0; r < kTY; ++r)
+      if (pcnt[r] > 0) {
+        const int a16 = pstart[r] & ~3;
+        bulk(pool + wbase + (poff[r] - (pstart[r] - a16)), P.J + a16, (uint32_t)pcnt[r] * 4,
+             &full[slot]);
+      }
+    issued = q + 1;
+  }
+  for (int q = max(0, issued - kS); q < issued; ++q)
+    mbar_wait(&full[q % kS], (uint32_t)((q / kS) & 1), err);
+}
+
 template <bool SNAP>
 __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_constant__ TmaMaps maps, YeeParams P,
                                                  int xch, int n_mats, int* err,
@@ -611,98 +714,7 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
   __syncthreads();
 
   if (w == 4) {  // ------------------------------------------------------------ producer
-    // pole ranges of every (plane, row) of the chunk: the first pole of the tile row and the
-    // end of its last segment, all fetched at once by the producer warp
-    const int64_t nseg = (int64_t)P.nx * P.ny * P.nzp / 32;
-    const int nst = min(4, (P.nzp - k0) / 32);
-    if (P.has_ade) {
-      for (int t = lane; t < np * kTY; t += 32) {
-        const int i = ib + t / kTY, j = j0 + t % kTY;
-        uint32_t a = 0u, b = 0u;
-        if (j < P.ny) {
-          const int64_t s0 = (((int64_t)i * P.ny + j) * P.nzp + k0) >> 5;
-          a = __ldg(P.seg_ofs + s0);
-          b = (s0 + nst < nseg) ? __ldg(P.seg_ofs + s0 + nst) : P.n_pole_total;
-        }
-        segt[2 * t] = a;
-        segt[2 * t + 1] = b;
-      }
-      __syncwarp();
-    }
-    if (lane != 0) return;
-    int issued = 0;
-    bool ok = true;
-    const uint32_t mbytes = (uint32_t)(kTY * kTZ * (wide ? 4 : 2));
-    // the tile's y and z psi rows are fixed once; per plane only the x slab rows are added.
-    // Pool layout per plane: x rows (1024 floats), y rows (1024), z rows (512) where present,
-    // then the pole-current window.
-    const PsiTile pt = psi_tile(P, j0, k0);
-    for (int q = 0; q < np && ok; ++q) {
-      const int slot = q % kS;
-      const int i = ib + q;
-      const bool xsl = in_slab(X, i);
-      int offs[3] = {-1, -1, -1};
-      int wbase = 0;
-      if (xsl) { offs[0] = wbase; wbase += 1024; }
-      if (pt.ymask) { offs[1] = wbase; wbase += 1024; }
-      if (pt.zs0 || pt.zs1) { offs[2] = wbase; wbase += 512; }
-      const int cap = kEPool - wbase;  // pole currents (floats) this plane can stage
-      int pstart[kTY], poff[kTY], pcnt[kTY];
-      int used = 0;
-#pragma unroll
-      for (int r = 0; r < kTY; ++r) {
-        const uint32_t a = P.has_ade ? segt[2 * (q * kTY + r)] : 0u;
-        const uint32_t b = P.has_ade ? segt[2 * (q * kTY + r) + 1] : 0u;
-        pstart[r] = (int)a; poff[r] = -2; pcnt[r] = 0;
-        if (b <= a) continue;
-        const int a16 = (int)(a & ~3u);  // 16-byte aligned start
-        const int n4 = (int)(((b - (uint32_t)a16) + 3u) & ~3u);
-        if (used + n4 <= cap) {
-          poff[r] = used + ((int)a - a16);
-          pcnt[r] = n4;
-          used += n4;
-        } else {
-          poff[r] = -1;  // consumers read this row's poles from global memory
-        }
-      }
-      if (q >= kS) ok = mbar_wait_live(&empty[slot], (uint32_t)((q / kS - 1) & 1), err, kPolls);
-      if (!ok) break;
-      float* st = smem + slot * kEStage;
-      int* tab = reinterpret_cast<int*>(st + kE_PT);
-      const int iprev = (i > 0) ? i - 1 : X.prv[0];
-      uint32_t bytes = 3 * kWideBytes + 5 * kTileBytes + mbytes + pt.yzbytes +
-                       (xsl ? pt.xbytes : 0u) + (uint32_t)used * 4;
-#pragma unroll
-      for (int r = 0; r < kTY; ++r) {
-        tab[2 * r] = pstart[r];
-        tab[2 * r + 1] = poff[r];
-      }
-      tab[8] = offs[0];
-      tab[9] = offs[1];
-      tab[10] = offs[2];
-      tab[11] = wbase;
-      mbar_expect_tx(&full[slot], bytes);
-      for (int c = 0; c < 3; ++c) {
-        tma3(st + kE_HB + c * kBoxW, &maps.h_wide[c], &full[slot], k0 - 4, j0 - 1, i);
-        tma3(st + kE_ET + c * 512, &maps.e_tile[c], &full[slot], k0, j0, i);
-      }
-      tma3(st + kE_HP, &maps.h_tile[1], &full[slot], k0, j0, iprev);
-      tma3(st + kE_HP + 512, &maps.h_tile[2], &full[slot], k0, j0, iprev);
-      tma3(st + kE_MT, &maps.m_tile, &full[slot], k0, j0, i);
-      float* pool = st + kE_POOL;
-      stage_psi(pt, P.psie, P, pool + offs[0], pool + offs[1], pool + offs[2], &full[slot], i, j0,
-                k0, xsl);
-#pragma unroll
-      for (int r = 0; r < kTY; ++r)
-        if (pcnt[r] > 0) {
-          const int a16 = pstart[r] & ~3;
-          bulk(pool + wbase + (poff[r] - (pstart[r] - a16)), P.J + a16, (uint32_t)pcnt[r] * 4,
-               &full[slot]);
-        }
-      issued = q + 1;
-    }
-    for (int q = max(0, issued - kS); q < issued; ++q)
-      mbar_wait(&full[q % kS], (uint32_t)((q / kS) & 1), err);
+    e_producer(maps, P, smem, full, empty, segt, err, ib, np, j0, k0, lane);
     return;
   }
 
