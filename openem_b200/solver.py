@@ -189,10 +189,7 @@ class Plan:
             mt = tables_gpu.material_tables_device(sc, self.tabs, self.device)
             if mod is not None:
                 tables_gpu.isolate_cells_device(mt, mod["cell"])
-            self.h2d_bytes += sum(np.asarray(a).nbytes for a in
-                                  (sc.eps_ex, sc.eps_ey, sc.eps_ez))
-            self.h2d_bytes += sum(np.asarray(a).nbytes for a in
-                                  (sc.sigma_ex, sc.sigma_ey, sc.sigma_ez) if a is not None)
+            self.h2d_bytes += int(mt.h2d_bytes)  # eps and sigma as copied (dense or sparse)
             self._warn_nonfinite_materials(mt.table)
             L.check(lib.oem_plan_set_materials_device(
                 h, int(mt.n_mat), L.ptr(self._arr(mt.table, np.uint32)), int(mt.index_bytes),

@@ -301,17 +301,22 @@ def tensor_tables(sc, tabs) -> dict | None:
 _POOL = None
 
 
-def _par_all(test, n: int, parts: int = 8) -> bool:
-    """``all(test(lo, hi))`` over ``parts`` slices of range(n), on worker threads (numpy's
-    elementwise work releases the GIL, so large scans run in parallel)."""
+def par_map(fn, n: int, parts: int = 8) -> list:
+    """``[fn(lo, hi)]`` over ``parts`` consecutive slices of range(n), on worker threads
+    (numpy's elementwise work releases the GIL, so large scans run in parallel)."""
     global _POOL
     if n < (1 << 20):
-        return bool(test(0, n))
+        return [fn(0, n)]
     if _POOL is None:
         from concurrent.futures import ThreadPoolExecutor
         _POOL = ThreadPoolExecutor(max_workers=parts)
     step = -(-n // parts)
-    return all(_POOL.map(lambda lo: bool(test(lo, min(lo + step, n))), range(0, n, step)))
+    return list(_POOL.map(lambda lo: fn(lo, min(lo + step, n)), range(0, n, step)))
+
+
+def _par_all(test, n: int, parts: int = 8) -> bool:
+    """``all(test(lo, hi))`` over slices of range(n), on worker threads."""
+    return all(bool(r) for r in par_map(test, n, parts))
 
 
 def _rows_equal_first(a: np.ndarray) -> bool:

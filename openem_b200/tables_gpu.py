@@ -13,6 +13,8 @@ The index and the segment offsets stay in device memory and are handed to the pl
 
 from __future__ import annotations
 
+import threading
+
 import numpy as np
 
 from openem_b200 import tables as T
@@ -37,6 +39,7 @@ class DeviceTables:
         self.coef = coef
         self.seg_ofs = seg_ofs      # torch int32 (uint32 bits), (n_seg,), on the device
         self.n_pole_total = n_pole_total
+        self.h2d_bytes = 0          # eps and sigma bytes copied to the device
 
     @property
     def index_bytes(self) -> int:
@@ -101,6 +104,52 @@ class _PinnedStager:
         return dst
 
 
+_SCAN = threading.local()
+
+
+def _differing(v: np.ndarray, v0, lo: int, hi: int, piece: int = 1 << 20) -> np.ndarray:
+    """Indices in [lo, hi) where v differs from v0, scanned a piece at a time through one
+    reused mask per thread (no fresh pages per piece); pieces with no differing cell, the bulk of
+    a background, cost one comparison and one any()."""
+    b = getattr(_SCAN, "mask", None)
+    if b is None:
+        b = _SCAN.mask = np.empty(piece, dtype=bool)
+    out = []
+    for q in range(lo, hi, piece):
+        m = min(piece, hi - q)
+        np.not_equal(v[q:q + m], v0, out=b[:m])
+        if b[:m].any():
+            out.append(np.flatnonzero(b[:m]) + q)
+    return np.concatenate(out) if out else np.zeros(0, dtype=np.int64)
+
+
+def _upload_material(a: np.ndarray, torch, dev):
+    """One float64 per-cell array on the device, and the bytes that crossed the link. A scene's eps and sigma are mostly one
+    background value with objects in it: when at most an eighth of the cells differ from the
+    first cell's value (compared bit for bit, so NaN and signed zeros count as different), only
+    those cells' indices and values cross the link and the array is filled on the device;
+    otherwise the whole array is copied. A sample of the first 1/64 decides which path is tried,
+    and a scan that finds too many differing cells copies the whole array after all."""
+    a = np.ascontiguousarray(a, np.float64).reshape(-1)
+    n = a.size
+    if n < (1 << 22):
+        return _PinnedStager.copy(a, torch, dev), a.nbytes
+    v = a.view(np.uint64)
+    v0 = v[0]
+    m = n // 64
+    if np.count_nonzero(v[:m] != v0) > m // 8:
+        return _PinnedStager.copy(a, torch, dev), a.nbytes
+    parts = T.par_map(lambda lo, hi: _differing(v, v0, lo, hi), n)
+    cnt = sum(int(p.size) for p in parts)
+    if cnt > n // 8:
+        return _PinnedStager.copy(a, torch, dev), a.nbytes
+    out = torch.full((n,), float(a[0]), dtype=torch.float64, device=dev)
+    if cnt:
+        idx = np.concatenate(parts)
+        out[torch.from_numpy(idx).to(dev)] = torch.from_numpy(a[idx]).to(dev)
+    return out, 16 * cnt
+
+
 class _Uploads:
     """The float64 eps and sigma arrays of each component copied to the device on a worker
     thread while the caller deduplicates the pole sets and builds the keys: all three
@@ -118,6 +167,7 @@ class _Uploads:
         free, _ = torch.cuda.mem_get_info(dev)
         self.depth = 3 if nbytes < free // 4 else 1
         self.stream = torch.cuda.Stream(device=dev)
+        self.h2d = 0  # bytes copied to the device
         self.pool = ThreadPoolExecutor(max_workers=1)
         self.futs = [self.pool.submit(self._load, c) for c in range(self.depth)]
 
@@ -125,9 +175,13 @@ class _Uploads:
         torch, dev = self.torch, self.dev
         torch.cuda.set_device(dev)
         with torch.cuda.stream(self.stream):
-            eps = _PinnedStager.copy(np.asarray(self.eps[c], np.float64), torch, dev).reshape(-1)
-            sig = (None if self.sig[c] is None else
-                   _PinnedStager.copy(np.asarray(self.sig[c], np.float64), torch, dev).reshape(-1))
+            eps, nb = _upload_material(self.eps[c], torch, dev)
+            sig = None
+            if self.sig[c] is not None:
+                sig, nb2 = _upload_material(self.sig[c], torch, dev)
+                nb += nb2
+            self.stream.synchronize()
+        self.h2d += nb
         return eps, sig
 
     def get(self, c):
@@ -150,9 +204,11 @@ def material_tables_device(sc, tabs, device: int = 0) -> DeviceTables:
     dev = torch.device("cuda", device)
     up = _Uploads(sc, torch, dev)
     try:
-        return _material_tables_device(sc, tabs, torch, dev, up)
+        mt = _material_tables_device(sc, tabs, torch, dev, up)
     finally:
         up.close()
+    mt.h2d_bytes = up.h2d
+    return mt
 
 
 def _check_entries_device(name, shape, comp, cell, ofs_list, torch, dev):

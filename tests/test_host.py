@@ -432,3 +432,27 @@ def test_device_entry_checks_match_host_checks():
             dev_err = str(e)
         assert host_err == dev_err, (msg, host_err, dev_err)
         assert (msg is None) == (host_err is None) and (msg is None or msg in host_err)
+
+
+def test_sparse_material_upload_is_exact():
+    """A per-cell float64 array that is mostly one value crosses as (index, value) pairs and is
+    filled on the device (torch CPU tensors here), bit for bit, NaN and -0.0 included; a varied
+    array is copied whole. The byte counts are what was sent."""
+    import torch
+    from openem_b200 import tables_gpu as TG
+    rng = np.random.default_rng(3)
+    n = 1 << 23
+    a = np.zeros(n)
+    a[rng.integers(0, n, 5000)] = rng.random(5000)
+    a[11] = -0.0
+    a[12] = np.nan
+    t, nb = TG._upload_material(a, torch, torch.device("cpu"))
+    assert np.array_equal(t.numpy().view(np.uint64), a.view(np.uint64))
+    assert nb == 16 * int(np.count_nonzero(a.view(np.uint64) != a.view(np.uint64)[0]))
+    b = rng.random(n)
+    t, nb = TG._upload_material(b, torch, torch.device("cpu"))
+    assert np.array_equal(t.numpy(), b) and nb == b.nbytes
+    c = np.ones(n)
+    c[n // 2:] = 2.0  # the sample looks uniform, the full scan finds half the cells differ
+    t, nb = TG._upload_material(c, torch, torch.device("cpu"))
+    assert np.array_equal(t.numpy(), c) and nb == c.nbytes
