@@ -6,6 +6,7 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/mman.h>
 
 #include <algorithm>
 #include <cmath>
@@ -40,6 +41,15 @@ static ReadStage* read_stage(int device) {
   ReadStage*& r = g_stages[device];
   if (!r) r = new ReadStage();
   return r;
+}
+
+// Ask for transparent huge pages on the page-aligned interior of a large output range before
+// its first touch: a fresh 1.2 GB readout array otherwise takes 300k page faults. A hint only
+// (no effect where huge pages are disabled).
+static void advise_huge_pages(void* p, size_t n) {
+  const uintptr_t a = ((uintptr_t)p + 4095) & ~(uintptr_t)4095;
+  const uintptr_t b = ((uintptr_t)p + n) & ~(uintptr_t)4095;
+  if (b > a + ((uintptr_t)4 << 20)) madvise((void*)a, b - a, MADV_HUGEPAGE);
 }
 
 // Copy n bytes with up to 8 host threads (pieces of at least 4 MB).
@@ -2041,6 +2051,7 @@ int oem_plan_read_monitor_interleaved(oem_plan* p, int id, double* out, void* st
     }
   }
   if (rs) {
+    advise_huge_pages(out, (size_t)n * sizeof(double2));
     // chunk q: interleave, DMA into half q % 2; then copy chunk q - 1 out of the other half
     int64_t prev0 = -1, prevc = 0;
     for (int64_t q0 = 0, b = 0; e == cudaSuccess && (q0 < n || prev0 >= 0); q0 += kChunk, b ^= 1) {

@@ -308,8 +308,9 @@ def par_map(fn, n: int, parts: int = 8) -> list:
     if n < (1 << 20):
         return [fn(0, n)]
     if _POOL is None:
+        import os
         from concurrent.futures import ThreadPoolExecutor
-        _POOL = ThreadPoolExecutor(max_workers=parts)
+        _POOL = ThreadPoolExecutor(max_workers=max(8, min(16, os.cpu_count() or 8)))
     step = -(-n // parts)
     return list(_POOL.map(lambda lo: fn(lo, min(lo + step, n)), range(0, n, step)))
 

@@ -139,7 +139,7 @@ def _upload_material(a: np.ndarray, torch, dev):
     m = n // 64
     if np.count_nonzero(v[:m] != v0) > m // 8:
         return _PinnedStager.copy(a, torch, dev), a.nbytes
-    parts = T.par_map(lambda lo, hi: _differing(v, v0, lo, hi), n)
+    parts = T.par_map(lambda lo, hi: _differing(v, v0, lo, hi), n, parts=16)
     cnt = sum(int(p.size) for p in parts)
     if cnt > n // 8:
         return _PinnedStager.copy(a, torch, dev), a.nbytes
@@ -274,6 +274,54 @@ def _material_tables_device(sc, tabs, torch, dev, up) -> DeviceTables:
             pole_pool.shutdown(wait=True)
 
 
+def _lex_codes_hashed(keys, torch, dev):
+    """Material codes from one sort: a 64-bit mix of each cell's key tuple is made unique, the
+    distinct tuples (one representative cell each) are put in lexicographic order on the host,
+    and every cell is checked against its code's tuple. Returns (n_mat, code), the same codes as
+    the exact ranking, or None after a hash collision (the caller then ranks exactly)."""
+    h = torch.zeros_like(keys[0])
+    for k in keys:  # int64 arithmetic wraps; any deterministic mix will do, the check is exact
+        h = (h ^ k) * -7046029254386353131
+        h = h ^ (h >> 29)
+    uu, code = torch.unique(h, return_inverse=True)
+    del h
+    n = int(uu.numel())
+    rep = torch.empty(n, dtype=torch.int64, device=dev)
+    rep.scatter_(0, code, torch.arange(code.numel(), device=dev))
+    tup = []
+    for k in keys:
+        kr = k[rep]
+        if bool((k != kr[code]).any()):
+            return None
+        tup.append(kr.cpu().numpy())
+    order = np.lexsort(tuple(tup[::-1]))  # the first key is the primary one
+    rank = np.empty(n, dtype=np.int64)
+    rank[order] = np.arange(n, dtype=np.int64)
+    return n, torch.from_numpy(rank).to(dev)[code]
+
+
+def _lex_codes_exact(keys, torch):
+    """Material codes as the rank of each cell's six key ranks in lexicographic order: one
+    unique of their mixed-radix number when it fits in 62 bits, else a running code (the inverse
+    of the unique of (previous code, next key rank)) -- the same codes either way."""
+    invs, card = [], []
+    for k in keys:
+        u, inv = torch.unique(k, return_inverse=True)
+        invs.append(inv)
+        card.append(int(u.numel()))
+    if float(np.prod(np.asarray(card, dtype=np.float64))) < 2.0 ** 62:
+        comb = invs[0]
+        for inv, nk in zip(invs[1:], card[1:]):
+            comb = comb * nk + inv
+        uu, code = torch.unique(comb, return_inverse=True)
+    else:
+        code = None
+        for inv, nk in zip(invs, card):
+            comb = inv if code is None else code * nk + inv
+            uu, code = torch.unique(comb, return_inverse=True)
+    return int(uu.numel()), code
+
+
 def _material_tables_from(sc, tabs, torch, dev, up, shape, disp, ent, pole_fut) -> DeviceTables:
     nx, ny, nz = shape
     ncell = nx * ny * nz
@@ -281,7 +329,7 @@ def _material_tables_from(sc, tabs, torch, dev, up, shape, disp, ent, pole_fut) 
     dt = float(sc.dt)
     # each key's rank among its distinct values: the coefficient key of a component while the
     # next one uploads, the (eps, pole set) key once the pole sets are known
-    inv1, card1, inv2, card2, ca_l, cb_l, eps_l, ps_l = [], [], [], [], [], [], [], []
+    key1, key2, ca_l, cb_l, eps_l, ps_l = [], [], [], [], [], []
     mask32 = 0xFFFFFFFF
     for c in range(3):
         eps, sg = up.get(c)
@@ -324,12 +372,8 @@ def _material_tables_from(sc, tabs, torch, dev, up, shape, disp, ent, pole_fut) 
                                      torch.zeros_like(cb[td]))
         ef = eps.to(torch.float32)
         del eps
-        k1 = ((ca.view(torch.int32).to(torch.int64) & mask32) << 32) \
-            | (cb.view(torch.int32).to(torch.int64) & mask32)
-        u, inv = torch.unique(k1, return_inverse=True)
-        inv1.append(inv)
-        card1.append(int(u.numel()))
-        del k1, u
+        key1.append(((ca.view(torch.int32).to(torch.int64) & mask32) << 32)
+                    | (cb.view(torch.int32).to(torch.int64) & mask32))
         ca_l.append(ca)
         cb_l.append(cb)
         eps_l.append(ef)
@@ -344,32 +388,19 @@ def _material_tables_from(sc, tabs, torch, dev, up, shape, disp, ent, pole_fut) 
         if ep is not None:
             _, cell_d, _, sel = ent
             ps[cell_d[sel[c]]] = set_d[sel[c]]
-        k2 = ((eps_l[c].view(torch.int32).to(torch.int64) & mask32) << 32) | (ps + 1)
-        u, inv = torch.unique(k2, return_inverse=True)
-        inv2.append(inv)
-        card2.append(int(u.numel()))
-        del k2, u
+        key2.append(((eps_l[c].view(torch.int32).to(torch.int64) & mask32) << 32) | (ps + 1))
         ps_l.append(ps)
-    # the keys in component order, coefficient key first: (x1, x2, y1, y2, z1, z2)
-    invs = [v for c in range(3) for v in (inv1[c], inv2[c])]
-    card = [v for c in range(3) for v in (card1[c], card2[c])]
-    del inv1, inv2
-    # material code = rank of the cell's six key ranks in lexicographic order: one unique of
-    # their mixed-radix number when it fits in 62 bits, else a running code (the inverse of the
-    # unique of (previous code, next key rank)) -- the same codes either way
-    if float(np.prod(np.asarray(card, dtype=np.float64))) < 2.0 ** 62:
-        comb = invs[0]
-        for inv, nk in zip(invs[1:], card[1:]):
-            comb = comb * nk + inv
-        uu, code = torch.unique(comb, return_inverse=True)
-        del comb
+    # the keys in component order, coefficient key first: (x1, x2, y1, y2, z1, z2); the material
+    # code of a cell is the rank of its key tuple in lexicographic order
+    keys = [k for c in range(3) for k in (key1[c], key2[c])]
+    del key1, key2
+    found = _lex_codes_hashed(keys, torch, dev)
+    if found is not None:
+        n_mat, code = found
+        del keys
     else:
-        code = None
-        for inv, nk in zip(invs, card):
-            comb = inv if code is None else code * nk + inv
-            uu, code = torch.unique(comb, return_inverse=True)
-    del invs
-    n_mat = int(uu.numel())
+        n_mat, code = _lex_codes_exact(keys, torch)
+        del keys
     rep = torch.empty(n_mat, dtype=torch.int64, device=dev)
     rep.scatter_(0, code, torch.arange(ncell, device=dev))
     rec = np.zeros((n_mat, 16), dtype=np.uint32)

@@ -456,3 +456,25 @@ def test_sparse_material_upload_is_exact():
     c[n // 2:] = 2.0  # the sample looks uniform, the full scan finds half the cells differ
     t, nb = TG._upload_material(c, torch, torch.device("cpu"))
     assert np.array_equal(t.numpy(), c) and nb == c.nbytes
+
+
+def test_hashed_material_codes_equal_exact_ranking():
+    """The device table builder's one-sort material codes (a 64-bit mix of each cell's six keys,
+    the distinct tuples put in lexicographic order) equal the exact ranking of the key tuples;
+    torch CPU tensors here."""
+    import torch
+    from openem_b200 import tables_gpu as TG
+    g = torch.Generator().manual_seed(1)
+    n = 300_000
+    keys = [(torch.randint(-3, 4, (n,), generator=g) << 40) + torch.randint(0, 3, (n,), generator=g)
+            for _ in range(6)]
+    keys[2][::7] = torch.iinfo(torch.int64).min  # extreme key values sort first
+    n1, c1 = TG._lex_codes_hashed(keys, torch, torch.device("cpu"))
+    n2, c2 = TG._lex_codes_exact(keys, torch)
+    assert n1 == n2 and torch.equal(c1, c2)
+    tup = torch.stack(keys, 1).numpy()
+    order = np.lexsort(tup.T[::-1])
+    ranks = np.empty(n, np.int64)
+    ranks[order] = np.arange(n)
+    first = np.unique(c2.numpy(), return_index=True)[1]
+    assert (np.diff(ranks[first]) > 0).all()  # codes ascend with the tuples
