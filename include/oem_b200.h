@@ -305,8 +305,8 @@ int oem_plan_status(oem_plan* p, void* stream);
  * captured one-step graph). */
 int oem_plan_launches_per_step(oem_plan* p, int* n);
 
-/* Number of box DFT monitors whose per-step snapshot the E update kernel writes itself (0: each
- * box has its own snapshot launch, the default). Decided at finalize when OEM_B200_SNAP=update
+/* Number of box DFT monitors whose per-step snapshot the E update kernel writes itself (0: one
+ * snapshot launch covers every box monitor, the default). Decided at finalize when OEM_B200_SNAP=update
  * is set in the environment: a real plan on the warp-specialised kernels whose only E-side
  * work after the update is electric dipoles, with at most four box monitors. */
 int oem_plan_box_snapshots_in_update(oem_plan* p, int* n);

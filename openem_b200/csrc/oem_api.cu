@@ -471,12 +471,28 @@ static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors) {
     if (!monitors) break;
     if ((e = launch_flux_time(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "flux_time");
   }
-  for (const Monitor& m : p->mons) {
-    if (!monitors) break;
-    // box rows already written by the E update (and the E dipoles) when sb is set
-    if (!(sb && m.kind == 1) && (e = launch_snapshot(P, m, p->d_step, s)) != cudaSuccess)
+  if (monitors) {
+    // plane monitors one launch each, every box monitor in one launch (box rows are already
+    // written by the E update and the E dipoles when sb is set), then the flushes
+    const Monitor* boxes[64];
+    int nb = 0;
+    for (const Monitor& m : p->mons) {
+      if (m.kind != 1) {
+        if ((e = launch_snapshot(P, m, p->d_step, s)) != cudaSuccess)
+          return cuda_error(e, "snapshot");
+      } else if (!sb) {
+        boxes[nb++] = &m;
+        if (nb == 64) {
+          if ((e = launch_snapshot_boxes(P, boxes, nb, p->d_step, s)) != cudaSuccess)
+            return cuda_error(e, "snapshot");
+          nb = 0;
+        }
+      }
+    }
+    if (nb && (e = launch_snapshot_boxes(P, boxes, nb, p->d_step, s)) != cudaSuccess)
       return cuda_error(e, "snapshot");
-    if ((e = launch_flush(m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "flush");
+    for (const Monitor& m : p->mons)
+      if ((e = launch_flush(m, p->d_step, 0, s)) != cudaSuccess) return cuda_error(e, "flush");
   }
   if (p->hist && (e = launch_hist_snap(P, p->gbox, p->hist, p->d_step, p->n_total, s)) !=
                      cudaSuccess)
@@ -1499,7 +1515,7 @@ int oem_plan_add_dispersion_mix(oem_plan* p, int n_entry, const int* comp, const
   return OEM_OK;
 }
 
-// Box snapshots written by the warp-specialised E update (k_e_ws<true>) instead of k_snap_box,
+// Box snapshots written by the warp-specialised E update (k_e_ws<true>) instead of k_snap_boxes,
 // when OEM_B200_SNAP=update asks for it: a real plan on those kernels whose only E-side work
 // after the update is E dipoles (they rewrite the rows of their targets), with one to
 // kMaxSnapBoxes box monitors. Exact, but slower on the 512^3 workload (the E update 1.228 against

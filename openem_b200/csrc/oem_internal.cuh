@@ -174,9 +174,18 @@ struct Monitor {
   int cplx = 0;              // complex fields: the ring holds ncomp real then ncomp imaginary rows
 };
 
+// Box DFT monitors snapshotted by one launch (k_snap_boxes): block ranges per box.
+constexpr int kMaxBoxSnap = 8;
+struct BoxSnapSet {
+  int n = 0;
+  Monitor m[kMaxBoxSnap];
+  uint32_t blk0[kMaxBoxSnap + 1] = {};  // first block of each box; blk0[n]: all blocks
+  uint32_t cb[kMaxBoxSnap] = {};        // blocks of 256 points per plane of each box
+};
+
 // Box DFT monitors whose snapshot rows the warp-specialised E update writes itself: E^{n+1}
 // from its registers, H^{n+1/2} from its staged tile, at the same positions and in the same
-// ring row as k_snap_box (the ring holds six rows per step, components in order). The E-side
+// ring row as k_snap_boxes (the ring holds six rows per step, components in order). The E-side
 // dipole update then rewrites the rows of its few target cells that lie in a box.
 constexpr int kMaxSnapBoxes = 4;
 struct SnapBox {
@@ -460,6 +469,8 @@ cudaError_t launch_time_sample(const YeeParams& P, const TimeMon& m, const int* 
                                cudaStream_t s);
 cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* step,
                             cudaStream_t s);
+cudaError_t launch_snapshot_boxes(const YeeParams& P, const Monitor* const* boxes, int n,
+                                  const int* step, cudaStream_t s);
 cudaError_t launch_flush(const Monitor& m, const int* step, int forced, cudaStream_t s);
 cudaError_t launch_step_advance(int* step, cudaStream_t s);
 int stream_xchunk(const YeeParams& P);

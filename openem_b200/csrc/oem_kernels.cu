@@ -326,25 +326,31 @@ __global__ void k_snap_plane(YeeParams P, Monitor m, const int* step) {
   }
 }
 
-// DFT snapshot of a box: the six components at their Yee positions
-// (openem/kernels/source_dft.cu:453-478). Threads cover one (j, k) plane of the box with a
-// 32-bit index; blockIdx.y walks the x planes.
-__global__ void k_snap_box(YeeParams P, Monitor m, const int* step) {
+// DFT snapshot of box monitors (openem/kernels/source_dft.cu:453-478): the six components at
+// their Yee positions into ring row step % T, every box of the plan in one launch: block ranges
+// per box (blk0), cb blocks of 256 points per plane of a box, so that the boxes' reads overlap (a thin box across rows reads 8
+// bytes of every 64 it fetches and is latency-bound; the others stream beside it).
+__global__ void __launch_bounds__(256) k_snap_boxes(YeeParams P,
+                                                    const __grid_constant__ BoxSnapSet S,
+                                                    const int* step) {
+  int q = 0;
+  while (q + 1 < S.n && blockIdx.x >= S.blk0[q + 1]) ++q;
+  const Monitor& m = S.m[q];
+  const uint32_t bl = blockIdx.x - S.blk0[q];
+  const uint32_t a = bl / S.cb[q];  // plane of the box
+  const uint32_t t = (bl - a * S.cb[q]) * 256u + threadIdx.x;
   const uint32_t njk = (uint32_t)m.nj * (uint32_t)m.nk;
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= njk) return;
   const uint32_t b = t / (uint32_t)m.nk;
   const uint32_t cc = t - b * (uint32_t)m.nk;
   float* row = m.d_snap + (int64_t)((*step) % m.T) * (m.cplx ? 12 : 6) * m.cells;
-  for (int a = blockIdx.y; a < m.ni; a += gridDim.y) {
-    const int64_t id = ((int64_t)(m.i0 + a) * P.ny + (m.j0 + (int)b)) * P.nzp + (m.k0 + (int)cc);
-    const int64_t o = (int64_t)a * njk + t;
+  const int64_t id = ((int64_t)(m.i0 + (int)a) * P.ny + (m.j0 + (int)b)) * P.nzp + (m.k0 + (int)cc);
+  const int64_t o = (int64_t)a * njk + t;
 #pragma unroll
-    for (int q = 0; q < 6; ++q) row[q * m.cells + o] = P.f[q][id];
-    if (m.cplx) {
+  for (int c = 0; c < 6; ++c) row[c * m.cells + o] = P.f[c][id];
+  if (m.cplx) {
 #pragma unroll
-      for (int q = 0; q < 6; ++q) row[(6 + q) * m.cells + o] = P.fi[q][id];
-    }
+    for (int c = 0; c < 6; ++c) row[(6 + c) * m.cells + o] = P.fi[c][id];
   }
 }
 
@@ -942,16 +948,34 @@ cudaError_t launch_mix_post(const YeeParams& P, const MixSet& m, cudaStream_t s)
 
 cudaError_t launch_snapshot(const YeeParams& P, const Monitor& m, const int* step,
                             cudaStream_t s) {
-  if (m.kind == 0) {
-    dim3 b(32, 4, 1), g((m.n2 + 31) / 32, (m.n1 + 3) / 4, 1);
-    k_snap_plane<<<g, b, 0, s>>>(P, m, step);
-  } else {
-    const int64_t njk = (int64_t)m.nj * m.nk;
-    if (njk >= (1LL << 31)) return cudaErrorInvalidValue;  // one box plane per 32-bit index
-    dim3 g((unsigned)((njk + 255) / 256), (unsigned)std::min(m.ni, 65535), 1);
-    k_snap_box<<<g, 256, 0, s>>>(P, m, step);
-  }
+  if (m.kind != 0) return cudaErrorInvalidValue;  // boxes: launch_snapshot_boxes
+  dim3 b(32, 4, 1), g((m.n2 + 31) / 32, (m.n1 + 3) / 4, 1);
+  k_snap_plane<<<g, b, 0, s>>>(P, m, step);
   return cudaGetLastError();
+}
+
+cudaError_t launch_snapshot_boxes(const YeeParams& P, const Monitor* const* boxes, int n,
+                                  const int* step, cudaStream_t s) {
+  for (int g0 = 0; g0 < n; g0 += kMaxBoxSnap) {
+    BoxSnapSet S;
+    S.n = std::min(kMaxBoxSnap, n - g0);
+    int64_t total = 0;
+    for (int q = 0; q < S.n; ++q) {
+      const Monitor& m = *boxes[g0 + q];
+      const int64_t njk = (int64_t)m.nj * m.nk;
+      if (njk >= (1LL << 31)) return cudaErrorInvalidValue;  // one box plane per 32-bit index
+      S.m[q] = m;
+      S.cb[q] = (uint32_t)((njk + 255) / 256);
+      S.blk0[q] = (uint32_t)total;
+      total += (int64_t)m.ni * S.cb[q];
+      if (total >= (1LL << 31)) return cudaErrorInvalidValue;
+    }
+    S.blk0[S.n] = (uint32_t)total;
+    k_snap_boxes<<<(unsigned)total, 256, 0, s>>>(P, S, step);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_flush(const Monitor& m, const int* step, int forced, cudaStream_t s) {

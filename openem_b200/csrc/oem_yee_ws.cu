@@ -536,7 +536,7 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_h_ws(const __grid_con
 // kq + 3): the six components at the cells' own Yee positions, E^{n+1} as just computed and
 // H^{n+1/2} from the staged halo box (hb: this quad's Hx; Hy, Hz follow at kBoxW strides),
 // into ring row step % T (srow: that row of each box, set once per block in shared memory),
-// the layout and values of k_snap_box. sbm: the boxes whose rows and z range hold cells of this
+// the layout and values of k_snap_boxes. sbm: the boxes whose rows and z range hold cells of this
 // quad (fixed per lane), so that a lane with none skips the call.
 __device__ __forceinline__ void snap_quad(const SnapBoxes& sb, float* const* srow, unsigned sbm,
                                           int i, int j, int kq, const float* ex, const float* ey,
