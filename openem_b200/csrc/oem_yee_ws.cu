@@ -669,7 +669,7 @@ __device__ __forceinline__ void e_producer(const TmaMaps& maps, const YeeParams&
     mbar_wait(&full[q % kS], (uint32_t)((q / kS) & 1), err);
 }
 
-template <bool SNAP>
+template <bool SNAP, bool SMATS>
 __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_constant__ TmaMaps maps, YeeParams P,
                                                  int xch, int n_mats, int* err,
                                                  const __grid_constant__ SnapBoxes sb) {
@@ -693,12 +693,13 @@ __global__ void __launch_bounds__(160, OEM_WS_MINBLOCKS) k_e_ws(const __grid_con
   const DevAxis& Y = P.ax[1];
   const DevAxis& Z = P.ax[2];
   const bool wide = P.mat32 != nullptr;
-  const MatRec* mats = P.mats;
-  if (n_mats <= kSmemMats) {
+  // SMATS: the plan's material records fit in shared memory (n_mats <= kSmemMats), so the
+  // per-cell record loads are shared-memory loads the compiler knows as such
+  const MatRec* mats = SMATS ? smats : P.mats;
+  if (SMATS) {
     const uint4* src = reinterpret_cast<const uint4*>(P.mats);
     uint4* dst = reinterpret_cast<uint4*>(smats);
     for (int q = tid; q < n_mats * 4; q += 160) dst[q] = src[q];
-    mats = smats;
   }
   load_ztab(zt, Z, false, k0, P.nzp, tid, 160);
   if (SNAP && tid < sb.n)
@@ -1457,7 +1458,8 @@ cudaError_t ws_setup_kernels() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_h_ws, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared);
-  for (auto* k : {k_e_ws<false>, k_e_ws<true>}) {
+  for (auto* k : {k_e_ws<false, false>, k_e_ws<true, false>, k_e_ws<false, true>,
+                  k_e_ws<true, true>}) {
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_e_smem());
     if (e == cudaSuccess)
@@ -1483,9 +1485,11 @@ cudaError_t launch_update_e_ws(const TmaMaps& maps, const YeeParams& P, int xch,
                                int* err, cudaStream_t s, const SnapBoxes* sb) {
   dim3 b(32, kTY + 1, 1), g((P.nzp + kTZ - 1) / kTZ, (P.ny + kTY - 1) / kTY, (P.nx + xch - 1) / xch);
   if (sb && sb->n > 0)
-    k_e_ws<true><<<g, b, ws_e_smem(), s>>>(maps, P, xch, n_mats, err, *sb);
+    (n_mats <= kSmemMats ? k_e_ws<true, true> : k_e_ws<true, false>)<<<g, b, ws_e_smem(), s>>>(
+        maps, P, xch, n_mats, err, *sb);
   else
-    k_e_ws<false><<<g, b, ws_e_smem(), s>>>(maps, P, xch, n_mats, err, SnapBoxes{});
+    (n_mats <= kSmemMats ? k_e_ws<false, true> : k_e_ws<false, false>)<<<g, b, ws_e_smem(), s>>>(
+        maps, P, xch, n_mats, err, SnapBoxes{});
   return cudaGetLastError();
 }
 
