@@ -38,26 +38,27 @@ constexpr int kSegPoles = 256;  // pole states of one segment staged per warp
 // The pole update of one cell on states held in `st` (shared or global memory), J written to
 // the cell's first pole of each component; `en` holds the cell's E^n.
 __device__ __forceinline__ void ade_cell_poles(const YeeParams& P, const MatRec& M, float2* st,
-                                               uint32_t gp, const float (&en)[3]) {
+                                               uint32_t gp, const float (&en)[3],
+                                               const float4* pcoef, const int* pset_ofs) {
   int po = 0;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const int n = M.np[c];
     if (n == 0) continue;
-    const float4* cf = P.pcoef + P.pset_ofs[M.pset[c]];
+    const float4* cf = pcoef + pset_ofs[M.pset[c]];
     float acc = 0.f;
     int tt = 0;
     for (; tt + 1 < n; tt += 2) {
       float2 s0 = st[po + tt], s1 = st[po + tt + 1];
-      const float d0 = ade_pole(s0, __ldg(cf + tt), en[c]);
-      const float d1 = ade_pole(s1, __ldg(cf + tt + 1), en[c]);
+      const float d0 = ade_pole(s0, cf[tt], en[c]);
+      const float d1 = ade_pole(s1, cf[tt + 1], en[c]);
       st[po + tt] = s0;
       st[po + tt + 1] = s1;
       acc = __fadd_rn(__fadd_rn(acc, d0), d1);
     }
     if (tt < n) {
       float2 s0 = st[po + tt];
-      acc = __fadd_rn(acc, ade_pole(s0, __ldg(cf + tt), en[c]));
+      acc = __fadd_rn(acc, ade_pole(s0, cf[tt], en[c]));
       st[po + tt] = s0;
     }
     P.J[gp + (uint32_t)po] = acc;
@@ -91,9 +92,10 @@ __device__ __forceinline__ SegLoad seg_load(const YeeParams& P, int64_t s, int64
 // coalesced loads, updated there cell by cell, and written back coalesced; a segment with more
 // poles than the buffer holds is updated in place in global memory.
 __device__ __forceinline__ void ade_segment(const YeeParams& P, const SegLoad& L, float2* st,
-                                            int lane) {
+                                            int lane, const MatRec* mats, const float4* pcoef,
+                                            const int* pset_ofs) {
   const int n = (int)(L.b - L.a);
-  const MatRec& M = P.mats[L.m];
+  const MatRec& M = mats[L.m];
   const int npc = M.reserved;
   const unsigned lt = (1u << lane) - 1u;
   int pre = 0;
@@ -102,12 +104,12 @@ __device__ __forceinline__ void ade_segment(const YeeParams& P, const SegLoad& L
   if (n <= kSegPoles) {
     for (int t = lane; t < n; t += 32) st[t] = P.P[L.a + t];
     __syncwarp();
-    if (npc > 0) ade_cell_poles(P, M, st + pre, L.a + (uint32_t)pre, L.e);
+    if (npc > 0) ade_cell_poles(P, M, st + pre, L.a + (uint32_t)pre, L.e, pcoef, pset_ofs);
     __syncwarp();
     for (int t = lane; t < n; t += 32) P.P[L.a + t] = st[t];
     __syncwarp();
   } else if (npc > 0) {
-    ade_cell_poles(P, M, P.P + L.a + pre, L.a + (uint32_t)pre, L.e);
+    ade_cell_poles(P, M, P.P + L.a + pre, L.a + (uint32_t)pre, L.e, pcoef, pset_ofs);
   }
 }
 
@@ -116,9 +118,29 @@ __device__ __forceinline__ void ade_segment(const YeeParams& P, const SegLoad& L
 // segment and the index of the one after, so each segment waits on one dependent load (its
 // pole states) instead of three. In the captured step it runs on its own graph branch beside
 // the H update.
+constexpr int kAdeMats = 64;    // material records staged in shared memory when they fit
+constexpr int kAdeCoefs = 256;  // pole coefficient rows staged likewise
+constexpr int kAdeSets = 64;
+
+template <bool SMEM>
 __global__ void __launch_bounds__(256) k_ade_segments(YeeParams P, const int64_t* segs,
-                                                      int64_t nsegs, int64_t nseg) {
+                                                      int64_t nsegs, int64_t nseg, int n_mats) {
   __shared__ float2 buf[8][kSegPoles];
+  // SMEM: the material records, pole sets and coefficients fit here, read as shared memory
+  __shared__ MatRec smats[SMEM ? kAdeMats : 1];
+  __shared__ float4 scoef[SMEM ? kAdeCoefs : 1];
+  __shared__ int sofs[SMEM ? kAdeSets + 1 : 1];
+  const MatRec* mats = SMEM ? smats : P.mats;
+  const float4* pcoef = SMEM ? scoef : P.pcoef;
+  const int* pset_ofs = SMEM ? sofs : P.pset_ofs;
+  if (SMEM) {
+    const uint4* src = reinterpret_cast<const uint4*>(P.mats);
+    uint4* dst = reinterpret_cast<uint4*>(smats);
+    for (int q = threadIdx.x; q < n_mats * 4; q += blockDim.x) dst[q] = src[q];
+    for (int q = threadIdx.x; q < P.n_coef; q += blockDim.x) scoef[q] = P.pcoef[q];
+    for (int q = threadIdx.x; q <= P.n_sets; q += blockDim.x) sofs[q] = P.pset_ofs[q];
+    __syncthreads();
+  }
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
   const int64_t stride = (int64_t)gridDim.x * 8;
@@ -129,7 +151,7 @@ __global__ void __launch_bounds__(256) k_ade_segments(YeeParams P, const int64_t
     const int64_t q3 = q + 2 * stride;
     const int64_t s3 = q3 < nsegs ? segs[q3] : -1;
     const SegLoad nxt = seg_load(P, s2, nseg, lane);
-    ade_segment(P, cur, buf[w], lane);
+    ade_segment(P, cur, buf[w], lane, mats, pcoef, pset_ofs);
     cur = nxt;
     s2 = s3;
     q += stride;
@@ -147,12 +169,15 @@ cudaError_t launch_list_pole_segments(const YeeParams& P, int64_t nseg, int64_t*
 }
 
 cudaError_t launch_ade_segments(const YeeParams& P, const int64_t* segs, int64_t nsegs,
-                                int64_t nseg, int max_blocks, cudaStream_t s) {
+                                int64_t nseg, int max_blocks, int n_mats, cudaStream_t s) {
   if (nsegs <= 0) return cudaSuccess;
   // about one resident wave (5 blocks of 8 warps per SM); each warp strides over the list
   int64_t blocks = std::min<int64_t>((nsegs + 7) / 8, 148 * 5);
   if (max_blocks > 0 && blocks > max_blocks) blocks = max_blocks;
-  k_ade_segments<<<(unsigned)blocks, 256, 0, s>>>(P, segs, nsegs, nseg);
+  if (n_mats <= kAdeMats && P.n_coef <= kAdeCoefs && P.n_sets <= kAdeSets)
+    k_ade_segments<true><<<(unsigned)blocks, 256, 0, s>>>(P, segs, nsegs, nseg, n_mats);
+  else
+    k_ade_segments<false><<<(unsigned)blocks, 256, 0, s>>>(P, segs, nsegs, nseg, n_mats);
   return cudaGetLastError();
 }
 

@@ -244,7 +244,7 @@ static cudaError_t run_e(oem_plan* p, cudaStream_t s, const SnapBoxes* sb = null
   if (p->basic_kernels == 3) {
     if (p->yp.has_ade) {
       cudaError_t e = launch_ade_segments(p->yp, p->d_ade_segs, p->n_ade_segs,
-                                          (int64_t)p->nx * p->ny * p->nzp / 32, 0, s);
+                                          (int64_t)p->nx * p->ny * p->nzp / 32, 0, (int)p->mats.size(), s);
       if (e != cudaSuccess) return e;
     }
     return launch_update_e_ws(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s, sb);
@@ -383,7 +383,7 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
     for (const TensorSet& t : p->tensors)
       if ((e = launch_tensor_pre(P, t, s)) != cudaSuccess) return cuda_error(e, "tensor_pre");
     if (P.has_ade && (e = launch_ade_segments(P, p->d_ade_segs, p->n_ade_segs,
-                                              (int64_t)p->nx * p->ny * p->nzp / 32, 0, s)) !=
+                                              (int64_t)p->nx * p->ny * p->nzp / 32, 0, (int)p->mats.size(), s)) !=
                          cudaSuccess)
       return cuda_error(e, "ade");
     const int nb = p->bank ^ 1;
@@ -409,7 +409,7 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
     OEM_CUDA(cudaEventRecord(p->ev_fork, s));
     OEM_CUDA(cudaStreamWaitEvent(p->side_stream, p->ev_fork, 0));
     if ((e = launch_ade_segments(P, p->d_ade_segs, p->n_ade_segs,
-                                 (int64_t)p->nx * p->ny * p->nzp / 32, 0, p->side_stream)) !=
+                                 (int64_t)p->nx * p->ny * p->nzp / 32, 0, (int)p->mats.size(), p->side_stream)) !=
         cudaSuccess)
       return cuda_error(e, "ade");
     OEM_CUDA(cudaEventRecord(p->ev_join, p->side_stream));
@@ -1839,7 +1839,7 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
           if ((e = launch_tensor_pre(p->yp, t, s)) != cudaSuccess) return cuda_error(e, "tensor_pre");
         if (p->yp.has_ade &&
             (e = launch_ade_segments(p->yp, p->d_ade_segs, p->n_ade_segs,
-                                     (int64_t)p->nx * p->ny * p->nzp / 32, 0, s)) != cudaSuccess)
+                                     (int64_t)p->nx * p->ny * p->nzp / 32, 0, (int)p->mats.size(), s)) != cudaSuccess)
           return cuda_error(e, "ade");
         OEM_CUDA(cudaEventRecord(E[5], s));
         const int nb = p->bank ^ 1;
@@ -1882,7 +1882,7 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       if (split) {
         // the pole pass and the E kernel timed apart
         if ((e = launch_ade_segments(p->yp, p->d_ade_segs, p->n_ade_segs,
-                                     (int64_t)p->nx * p->ny * p->nzp / 32, 0, s)) != cudaSuccess)
+                                     (int64_t)p->nx * p->ny * p->nzp / 32, 0, (int)p->mats.size(), s)) != cudaSuccess)
           return cuda_error(e, "ade");
         OEM_CUDA(cudaEventRecord(E[5], s));
         e = launch_update_e_ws(p->tma, p->yp, p->xch, (int)p->mats.size(), p->d_err, s,

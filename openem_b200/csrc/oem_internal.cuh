@@ -497,7 +497,7 @@ cudaError_t launch_update_e_stream(const YeeParams& P, int xch, int n_mats, cuda
 cudaError_t launch_list_pole_segments(const YeeParams& P, int64_t nseg, int64_t* list,
                                       unsigned long long* count, cudaStream_t s);
 cudaError_t launch_ade_segments(const YeeParams& P, const int64_t* segs, int64_t nsegs,
-                                int64_t nseg, int max_blocks, cudaStream_t s);
+                                int64_t nseg, int max_blocks, int n_mats, cudaStream_t s);
 cudaError_t launch_update_h_c(const YeeParams& P, cudaStream_t s);
 cudaError_t launch_update_e_c(const YeeParams& P, cudaStream_t s);
 cudaError_t launch_seam_h(const YeeParams& P, const SeamFace& f, cudaStream_t s);
