@@ -124,12 +124,14 @@ def _differing(v: np.ndarray, v0, lo: int, hi: int, piece: int = 1 << 20) -> np.
 
 
 def _upload_material(a: np.ndarray, torch, dev):
-    """One float64 per-cell array on the device, and the bytes that crossed the link. A scene's eps and sigma are mostly one
-    background value with objects in it: when at most an eighth of the cells differ from the
-    first cell's value (compared bit for bit, so NaN and signed zeros count as different), only
-    those cells' indices and values cross the link and the array is filled on the device;
-    otherwise the whole array is copied. A sample of the first 1/64 decides which path is tried,
-    and a scan that finds too many differing cells copies the whole array after all."""
+    """One float64 per-cell array on the device, and the bytes that crossed the link.
+
+    A scene's eps and sigma are mostly one background value with objects in it: when at most an
+    eighth of the cells differ from the first cell's value (compared bit for bit, so NaN and
+    signed zeros count as different), only those cells' indices and values cross the link and
+    the array is filled on the device; otherwise the whole array is copied. A sample of the
+    first 1/64 decides which path is tried, and a scan that finds too many differing cells
+    copies the whole array after all."""
     a = np.ascontiguousarray(a, np.float64).reshape(-1)
     n = a.size
     if n < (1 << 22):
@@ -151,12 +153,13 @@ def _upload_material(a: np.ndarray, torch, dev):
 
 
 class _Uploads:
-    """The float64 eps and sigma arrays of each component copied to the device on a worker
-    thread while the caller deduplicates the pole sets and builds the keys: all three
-    components queued back to back when the six arrays take under a quarter of the free device
-    memory, otherwise one component ahead of the caller (at most two resident). The copies run
-    one at a time (pageable copies from several threads were slower) and are synchronous on the
-    worker's stream; the caller's stream is recorded on each tensor before use."""
+    """The float64 eps and sigma arrays of each component put on the device by a worker thread
+    (`_upload_material`: sparse or whole) while the caller turns the previous component into
+    coefficients and keys: all three components queued back to back when the six arrays take
+    under a quarter of the free device memory, otherwise one component ahead of the caller (at
+    most two resident). The uploads run one at a time, each with its own host threads, and are
+    synchronous on the worker's stream; the caller's stream is recorded on each tensor before
+    use; `h2d` counts the bytes that crossed the link."""
 
     def __init__(self, sc, torch, dev):
         from concurrent.futures import ThreadPoolExecutor
