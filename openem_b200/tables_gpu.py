@@ -58,18 +58,25 @@ class _PinnedStager:
     threads copy chunk q into one half (numpy copies release the GIL, so the threads run in
     parallel) while the DMA of chunk q - 1 drains the other, so the transfer runs near the link
     rate instead of through the driver's single-threaded pageable staging. One buffer per
-    process, made on first use; used by one thread at a time."""
+    process, made on first use; copies from several threads (a server building plans on
+    worker threads) take turns through a lock."""
 
     CHUNK = 64 << 20
     THREADS = 8
     _buf = None
     _pool = None
+    _lock = threading.Lock()
 
     @classmethod
     def copy(cls, a: np.ndarray, torch, dev):
         a = np.ascontiguousarray(a)
         if a.nbytes < 2 * cls.CHUNK:
             return torch.from_numpy(a).to(dev)
+        with cls._lock:
+            return cls._copy(a, torch, dev)
+
+    @classmethod
+    def _copy(cls, a: np.ndarray, torch, dev):
         if cls._buf is None or cls._buf.numel() < 2 * cls.CHUNK:
             cls._buf = torch.empty(2 * cls.CHUNK, dtype=torch.uint8, pin_memory=True)
         if cls.THREADS > 1 and cls._pool is None:

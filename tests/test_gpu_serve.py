@@ -23,3 +23,28 @@ def test_served_results_equal_alone():
     for d, r in zip(got, reqs):
         alone = solver.run(r.build(), num_steps=r.num_steps, use_shutoff=False, verbose=False)
         np.testing.assert_array_equal(d.result.phasors["T"].data, alone.phasors["T"].data)
+
+
+def test_pinned_stager_copies_from_several_threads():
+    """Plans built on several worker threads share one pinned staging buffer: concurrent large
+    copies take turns and every array arrives intact."""
+    import threading
+    import torch
+    from openem_b200 import tables_gpu as TG
+    dev = torch.device("cuda", 0)
+    arrays = [np.random.default_rng(q).random((1 << 25) + 1000 * q) for q in range(4)]
+    out = [None] * 4
+
+    def run(q):
+        torch.cuda.set_device(0)
+        with torch.cuda.stream(torch.cuda.Stream()):
+            out[q] = TG._PinnedStager.copy(arrays[q], torch, dev)
+            torch.cuda.current_stream().synchronize()
+
+    ts = [threading.Thread(target=run, args=(q,)) for q in range(4)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    for a, t in zip(arrays, out):
+        np.testing.assert_array_equal(t.cpu().numpy(), a)
