@@ -68,7 +68,10 @@ BLOCH_NAME = ("bloch_metasurface 256x256x1024 complex (Bloch 0.15 on x, periodic
 # clocks
 # ---------------------------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi samples of the SM clock and throttle reasons while the timed region runs."""
+    """SM clock and throttle reasons sampled while the timed steps run: NVML queried every few
+    milliseconds from a thread (started once the steps are queued, stopped when the device has
+    finished them), so that a timed region of a few tens of milliseconds still gets samples;
+    nvidia-smi at 200 ms intervals when NVML is unavailable. Reads only; changes no setting."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -79,8 +82,36 @@ class ClockSampler:
         self.proc = None
         self.lines = []
         self.thread = None
+        self.nv = None
+        self.handle = None
+        self.samples = []
+        self.smax = None
+        self.stopping = False
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            # the CUDA device's PCI address as NVML's "dddddddd:bb:dd.0" string (bytes: NVML
+            # reads it through a char pointer)
+            pr = torch.cuda.get_device_properties(index)
+            ids = (getattr(pr, "pci_domain_id", None), getattr(pr, "pci_bus_id", None),
+                   getattr(pr, "pci_device_id", None))
+            if all(isinstance(v, int) for v in ids):
+                busid = "{:08X}:{:02X}:{:02X}.0".format(*ids).encode("ascii")
+                self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(busid)
+            else:
+                self.handle = pynvml.nvmlDeviceGetHandleByIndex(int(index))
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
+            self.nv = pynvml
+        except Exception:
+            self.nv = None
 
     def start(self):
+        if self.nv is not None:
+            self.stopping = False
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
@@ -92,11 +123,34 @@ class ClockSampler:
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
 
+    def _poll(self):
+        nv = self.nv
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        while not self.stopping:
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM))
+                mask = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle))
+            except Exception:
+                break
+            self.samples.append((sm, {k for k, b in bits.items() if mask & b}))
+            time.sleep(0.002)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self) -> dict:
+        if self.nv is not None:
+            self.stopping = True
+            if self.thread:
+                self.thread.join(timeout=2)
+            sm = [v for v, _ in self.samples]
+            reasons = set().union(*[r for _, r in self.samples]) if self.samples else set()
+            return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.smax,
+                    "reasons": sorted(reasons), "samples": len(sm), "source": "nvml"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -121,7 +175,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -218,10 +272,11 @@ def run_reference(args):
 # ---------------------------------------------------------------------------------------------
 # the Bloch cell: throughput and the precision of its DFT accumulation
 # ---------------------------------------------------------------------------------------------
-def measure_bloch(steps: int, warmup: int, e2e: bool, device: int = 0) -> dict:
+def measure_bloch(steps: int, warmup: int, e2e: bool, device: int = 0, clocks=None) -> dict:
     """Device-timed steps of the 256 x 256 x 1024 Bloch cell (value in complex cell-updates
     per second), the roofline of its dominant kernel, and optionally the same steps end to end
-    through ``solver.run``."""
+    through ``solver.run``; ``clocks`` (a ClockSampler) samples while the timed steps run and its
+    record is returned under "clocks"."""
     import torch
 
     from openem_b200 import roofline, scenes, solver
@@ -235,7 +290,10 @@ def measure_bloch(steps: int, warmup: int, e2e: bool, device: int = 0) -> dict:
     a.record(stream)
     plan.run(steps)
     b.record(stream)
+    if clocks:
+        clocks.start()
     torch.cuda.synchronize()
+    clk = clocks.stop() if clocks else None
     ms = a.elapsed_time(b)
     plan.status()
     launches = plan.launches_per_step() * steps
@@ -263,7 +321,7 @@ def measure_bloch(steps: int, warmup: int, e2e: bool, device: int = 0) -> dict:
                         "algorithmic_bytes_per_launch": kb[dom],
                         "peak_source": peaks["source"]},
            "kernels_ms_per_launch": {k: v[1] / v[0] for k, v in tm.items()},
-           "gpu_launches": launches}
+           "gpu_launches": launches, "clocks": clk}
     if e2e:
         torch.cuda.synchronize()
         stats = {}
@@ -369,10 +427,8 @@ def run_bloch_line(args):
     torch.cuda.set_device(local)
     barrier(world)
     clocks = ClockSampler(local) if rank == 0 else None
-    if clocks:
-        clocks.start()
-    m = measure_bloch(args.steps, args.warmup, e2e=not args.no_e2e, device=local)
-    clk = clocks.stop() if clocks else None
+    m = measure_bloch(args.steps, args.warmup, e2e=not args.no_e2e, device=local, clocks=clocks)
+    clk = m.pop("clocks")
     ms_max = reduce_max(m["ms_per_step"] * args.steps, world)
     if rank == 0:
         cells = 256 * 256 * 1024
@@ -433,19 +489,20 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier(world)
     clocks = ClockSampler(local) if rank == 0 else None
-    if clocks:
-        clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     barrier(world)
-    # the timed region: the captured step graph, as solver.run launches it
+    # the timed region: the captured step graph, as solver.run launches it; the clocks are
+    # sampled from when the steps are queued until the device has finished them
     ev0.record(stream)
     plan.run(K)
     ev1.record(stream)
+    if clocks:
+        clocks.start()
     torch.cuda.synchronize()
+    clk = clocks.stop() if clocks else None
     barrier(world)
     ms = ev0.elapsed_time(ev1)
-    clk = clocks.stop() if clocks else None
     plan.status()
     launches = plan.launches_per_step() * K
     snap_in_e = plan.box_snapshots_in_update() > 0
@@ -499,7 +556,8 @@ def run_ours(args):
     # a short device-timed run of the Bloch cell, reported beside the headline
     secondary = None
     if world == 1 and not args.no_secondary:
-        secondary = {"bloch": measure_bloch(max(K, 50), W, e2e=False, device=local)}
+        secondary = {"bloch": measure_bloch(max(K, 50), W, e2e=False, device=local,
+                                            clocks=ClockSampler(local))}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
