@@ -380,7 +380,9 @@ __global__ void __launch_bounds__(128, 4) k_flush(Monitor m, const int* step, in
   if (s_lo > s_now) return;
   const int ns = s_now - s_lo + 1;  // rows to fold, 1..T
   constexpr int NE = NC / 2;        // E components come first
-  __shared__ float4 sph[32][kFlushF];
+  // the phase rows of the chunk, split by field family: [0] (cos, sin) at the E times, [1] at
+  // the H times, so that a thread reads the pair of its component with one load
+  __shared__ float2 sph[2][32][kFlushF];
   const int64_t cells = m.cells;
   const int64_t items = (int64_t)NC * cells;
   for (int64_t base = (int64_t)blockIdx.x * 128; base < items; base += (int64_t)gridDim.x * 128) {
@@ -406,9 +408,12 @@ __global__ void __launch_bounds__(128, 4) k_flush(Monitor m, const int* step, in
       __syncthreads();  // the previous chunk's rows are no longer read
       for (int e = threadIdx.x; e < ns * kFlushF; e += 128) {
         const int q = e / kFlushF, ff = e - q * kFlushF;
-        if (ff < nfc)
-          sph[q][ff] = __ldg(reinterpret_cast<const float4*>(m.d_phase) +
-                             ((int64_t)(s_lo + q) * m.nf + f0 + ff));
+        if (ff < nfc) {
+          const float4 ph = __ldg(reinterpret_cast<const float4*>(m.d_phase) +
+                                  ((int64_t)(s_lo + q) * m.nf + f0 + ff));
+          sph[0][q][ff] = make_float2(ph.x, ph.y);
+          sph[1][q][ff] = make_float2(ph.z, ph.w);
+        }
       }
       __syncthreads();
       // groups of kFlushG frequencies: the group's accumulators are loaded before its partial
@@ -433,13 +438,14 @@ __global__ void __launch_bounds__(128, 4) k_flush(Monitor m, const int* step, in
           aR[u] = 0.f;
           aI[u] = 0.f;
         }
+        const float2 (*fam)[kFlushF] = sph[isE ? 0 : 1];
 #pragma unroll
         for (int q = 0; q < 32; ++q) {
           if (q < ns) {
 #pragma unroll
             for (int u = 0; u < kFlushG; ++u) {
-              const float4 ph = sph[q][g + u];
-              const float co = isE ? ph.x : ph.z, si = isE ? ph.y : ph.w;
+              const float2 ph = fam[q][g + u];
+              const float co = ph.x, si = ph.y;
               if (CPLX) {
                 aR[u] = fmaf(-vi[q], si, fmaf(vr[q], co, aR[u]));
                 aI[u] = fmaf(vi[q], co, fmaf(vr[q], si, aI[u]));
