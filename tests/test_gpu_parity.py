@@ -218,3 +218,30 @@ def test_device_table_run_equals_host_table_run(monkeypatch):
     b = solver.run(sc, use_shutoff=False, return_fields=True, verbose=False)
     for nm in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
         np.testing.assert_array_equal(a.fields[nm], b.fields[nm])
+
+
+@pytest.mark.parametrize("kind", ["basic", "ws"])
+def test_many_box_monitors_match_oracle(monkeypatch, kind):
+    """Ten box monitors of assorted shapes (one launch snapshots at most eight, so two launches
+    per step; thin and ragged boxes, one touching the grid's faces) against the FP64 oracle."""
+    from dataclasses import replace
+    from openem_b200.model import FieldMonitor
+    monkeypatch.setenv("OEM_B200_KERNELS", kind)
+    sc = scenes.small_dispersive(n=36, n_sph=3, num_steps=90, n_pml=6, nfreq=2)
+    freqs = np.asarray(sc.field_monitors[0].freqs)
+    shapes = [((0, 0, 0), (36, 36, 36)), ((3, 5, 7), (1, 9, 2)), ((10, 2, 17), (5, 1, 3)),
+              ((17, 17, 17), (2, 2, 2)), ((0, 20, 30), (36, 3, 6)), ((35, 35, 35), (1, 1, 1)),
+              ((8, 8, 0), (7, 11, 36)), ((12, 0, 11), (4, 36, 1)), ((20, 21, 22), (3, 4, 5)),
+              ((1, 2, 3), (33, 31, 29))]
+    mons = [FieldMonitor(name=f"b{q}", freqs=freqs, origin=o, box=b)
+            for q, (o, b) in enumerate(shapes)]
+    sc = replace(sc, field_monitors=mons)
+    ref = ref64.run(sc)
+    got = solver.run(sc, use_shutoff=False, verbose=False)
+    scale = float(np.abs(ref.field_phasors["b0"]).max())  # the whole-grid box
+    for name, data in ref.field_phasors.items():
+        g = got.field_phasors[name]
+        assert g.shape == data.shape, name
+        # relative L2 within 1e-4, or, for a box where the field is still weak, every value
+        # within 1e-6 of the largest phasor anywhere
+        assert rel_l2(g, data) < 1e-4 or float(np.abs(g - data).max()) < 1e-6 * scale, name
