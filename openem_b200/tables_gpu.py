@@ -133,18 +133,21 @@ def _differing(v: np.ndarray, v0, lo: int, hi: int, piece: int = 1 << 20) -> np.
 def _upload_material(a: np.ndarray, torch, dev):
     """One float64 per-cell array on the device, and the bytes that crossed the link.
 
-    A scene's eps and sigma are mostly one background value with objects in it: when at most an
-    eighth of the cells differ from the first cell's value (compared bit for bit, so NaN and
-    signed zeros count as different), only those cells' indices and values cross the link and
-    the array is filled on the device; otherwise the whole array is copied. A sample of the
-    first 1/64 decides which path is tried, and a scan that finds too many differing cells
-    copies the whole array after all."""
+    A scene's eps and sigma are mostly one background value with objects in it: the most
+    common value among 4096 cells spread over the array is taken as the background, and when at
+    most an eighth of the cells differ from it (compared bit for bit, so NaN and signed zeros
+    count as different), only those cells' indices and values cross the link and the array is
+    filled on the device; otherwise the whole array is copied. The first 1/64 of the cells
+    decides which path is tried, and a scan that finds too many differing cells copies the
+    whole array after all."""
     a = np.ascontiguousarray(a, np.float64).reshape(-1)
     n = a.size
     if n < (1 << 22):
         return _PinnedStager.copy(a, torch, dev), a.nbytes
     v = a.view(np.uint64)
-    v0 = v[0]
+    # the background: the most common value among 4096 cells spread over the array
+    u, cnt_u = np.unique(v[::max(1, n // 4096)], return_counts=True)
+    v0 = u[int(np.argmax(cnt_u))]
     m = n // 64
     if np.count_nonzero(v[:m] != v0) > m // 8:
         return _PinnedStager.copy(a, torch, dev), a.nbytes
@@ -152,7 +155,9 @@ def _upload_material(a: np.ndarray, torch, dev):
     cnt = sum(int(p.size) for p in parts)
     if cnt > n // 8:
         return _PinnedStager.copy(a, torch, dev), a.nbytes
-    out = torch.full((n,), float(a[0]), dtype=torch.float64, device=dev)
+    # filled with the background's bits (a NaN keeps its payload, -0.0 its sign)
+    out = torch.full((n,), int(np.array([v0], np.uint64).view(np.int64)[0]), dtype=torch.int64,
+                     device=dev).view(torch.float64)
     if cnt:
         idx = np.concatenate(parts)
         out[torch.from_numpy(idx).to(dev)] = torch.from_numpy(a[idx]).to(dev)

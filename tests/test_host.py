@@ -453,9 +453,18 @@ def test_sparse_material_upload_is_exact():
     t, nb = TG._upload_material(b, torch, torch.device("cpu"))
     assert np.array_equal(t.numpy(), b) and nb == b.nbytes
     c = np.ones(n)
-    c[n // 2:] = 2.0  # the sample looks uniform, the full scan finds half the cells differ
+    c[n // 2:] = 2.0  # the first 1/64 looks uniform, the full scan finds half the cells differ
     t, nb = TG._upload_material(c, torch, torch.device("cpu"))
     assert np.array_equal(t.numpy(), c) and nb == c.nbytes
+    nanp = np.array([0x7FF8000000000123], np.uint64).view(np.float64)[0]  # a NaN with payload
+    dd = np.full(n, nanp)
+    dd[5] = -0.0
+    t, nb = TG._upload_material(dd, torch, torch.device("cpu"))
+    assert np.array_equal(t.numpy().view(np.uint64), dd.view(np.uint64)) and nb == 16
+    d = np.full(n, 2.25)
+    d[:1000] = 1.0  # the first cell lies in an object: the background is the common value
+    t, nb = TG._upload_material(d, torch, torch.device("cpu"))
+    assert np.array_equal(t.numpy(), d) and nb == 16 * 1000
 
 
 def test_hashed_material_codes_equal_exact_ranking():
