@@ -311,6 +311,15 @@ int oem_plan_launches_per_step(oem_plan* p, int* n);
  * work after the update is electric dipoles, with at most four box monitors. */
 int oem_plan_box_snapshots_in_update(oem_plan* p, int* n);
 
+/* 1 when this plan runs each step's pole pass one step early: a run of c >= 2 steps launches
+ * the first step's pole pass, then every step but the last runs the next step's pole pass
+ * beside its DFT snapshots and flushes (it reads E^{n+1} once every E-side source is in); the
+ * last step runs none, so the pole states are those of the run's last step when the call
+ * returns. Decided at finalize: a dispersive plan on the warp-specialised kernels without time
+ * modulation, mixed-form or tensor entries; OEM_B200_ADE=inline in the environment turns it
+ * off. The results are the same bit for bit either way. */
+int oem_plan_pole_pass_ahead(oem_plan* p, int* on);
+
 /* Steps taken so far (host-side count). */
 int oem_plan_steps(oem_plan* p, int64_t* steps);
 

@@ -356,7 +356,7 @@ static int check_device_error(oem_plan* p) {
 }
 
 // One time step (openem/solver.py:1145-1162).
-static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors);
+static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors, bool ade_next = false);
 
 // The box monitors whose snapshots the E update of this step writes, or null: only on a step
 // that records monitors.
@@ -372,7 +372,18 @@ static void set_bank(oem_plan* p, int b) {
   p->yp.psih = p->bank_psih[b];
 }
 
-static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
+static int launch_ade(oem_plan* p, cudaStream_t s, int max_blocks = 0) {
+  cudaError_t e = launch_ade_segments(p->yp, p->d_ade_segs, p->n_ade_segs,
+                                      (int64_t)p->nx * p->ny * p->nzp / 32, max_blocks,
+                                      (int)p->mats.size(), s);
+  return e == cudaSuccess ? OEM_OK : cuda_error(e, "ade");
+}
+
+// One step. ade_here: the step runs its own pole pass (beside the H update when the plan has a
+// side stream); otherwise the previous step ran it (ade_next there). ade_next: the pole pass of
+// the following step runs on the side stream once this step's E-side sources are in.
+static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true, bool ade_here = true,
+                        bool ade_next = false) {
   const YeeParams& P = p->yp;
   cudaError_t e;
   if (p->fused) {
@@ -405,13 +416,11 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
     if ((e = launch_modulate(P, m, p->d_step, s)) != cudaSuccess) return cuda_error(e, "modulate");
   for (const TensorSet& t : p->tensors)
     if ((e = launch_tensor_pre(P, t, s)) != cudaSuccess) return cuda_error(e, "tensor_pre");
-  if (fork) {
+  if (fork && ade_here) {
     OEM_CUDA(cudaEventRecord(p->ev_fork, s));
     OEM_CUDA(cudaStreamWaitEvent(p->side_stream, p->ev_fork, 0));
-    if ((e = launch_ade_segments(P, p->d_ade_segs, p->n_ade_segs,
-                                 (int64_t)p->nx * p->ny * p->nzp / 32, 0, (int)p->mats.size(), p->side_stream)) !=
-        cudaSuccess)
-      return cuda_error(e, "ade");
+    int rc = launch_ade(p, p->side_stream);
+    if (rc) return rc;
     OEM_CUDA(cudaEventRecord(p->ev_join, p->side_stream));
   }
   if ((e = run_h(p, s)) != cudaSuccess) return cuda_error(e, "update_h");
@@ -429,18 +438,19 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true) {
     if ((e = launch_absorb(P, a, 0, s)) != cudaSuccess) return cuda_error(e, "absorb_h");
   const SnapBoxes* sb = snap_boxes(p, monitors);
   if (fork) {
-    OEM_CUDA(cudaStreamWaitEvent(s, p->ev_join, 0));
+    if (ade_here) OEM_CUDA(cudaStreamWaitEvent(s, p->ev_join, 0));
     e = launch_update_e_ws(p->tma, P, p->xch, (int)p->mats.size(), p->d_err, s, sb);
   } else {
     e = run_e(p, s, sb);
   }
   if (e != cudaSuccess) return cuda_error(e, "update_e");
-  return enqueue_e_side(p, s, monitors);
+  return enqueue_e_side(p, s, monitors, fork && ade_next);
 }
 
 // After the E update: E-side injection, absorber, time / flux-time samples, DFT snapshots and
-// flushes, the step counter.
-static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors) {
+// flushes, the step counter. ade_next: the next step's pole pass (it reads E^{n+1} with every
+// E-side source in) runs on the side stream beside the monitors and joins at the end.
+static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors, bool ade_next) {
   const YeeParams& P = p->yp;
   cudaError_t e;
   for (const PlaneSrc& src : p->planes)
@@ -460,6 +470,14 @@ static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors) {
     if ((e = launch_tensor_post(P, t, s)) != cudaSuccess) return cuda_error(e, "tensor_post");
   for (const Absorber& a : p->absorbers)
     if ((e = launch_absorb(P, a, 1, s)) != cudaSuccess) return cuda_error(e, "absorb_e");
+  if (ade_next) {
+    OEM_CUDA(cudaEventRecord(p->ev_fork, s));
+    OEM_CUDA(cudaStreamWaitEvent(p->side_stream, p->ev_fork, 0));
+    // four blocks per SM instead of five: the snapshot blocks find room beside them
+    int rc = launch_ade(p, p->side_stream, 148 * 4);
+    if (rc) return rc;
+    OEM_CUDA(cudaEventRecord(p->ev_join, p->side_stream));
+  }
   for (const TimeMon& m : p->tmons) {
     if (!monitors) break;
     if ((e = launch_time_sample(P, m, p->d_step, 1, s)) != cudaSuccess)
@@ -498,6 +516,7 @@ static int enqueue_e_side(oem_plan* p, cudaStream_t s, bool monitors) {
                      cudaSuccess)
     return cuda_error(e, "gradient box history");
   if ((e = launch_step_advance(p->d_step, s)) != cudaSuccess) return cuda_error(e, "step");
+  if (ade_next) OEM_CUDA(cudaStreamWaitEvent(s, p->ev_join, 0));
   return OEM_OK;
 }
 
@@ -551,12 +570,19 @@ static int load_state(oem_plan* p, int slot, cudaStream_t s) {
   return OEM_OK;
 }
 
-static int capture(oem_plan* p, int nsteps, cudaGraphExec_t* out) {
+// mode 0: nsteps self-contained steps (the first runs its own pole pass; with ade_ahead each
+// later one has it run by the step before); 1: one step whose pole pass ran before it and
+// which runs the next one's (graph_mid); 2: one step whose pole pass ran before it (graph_last).
+static int capture(oem_plan* p, int nsteps, cudaGraphExec_t* out, int mode = 0) {
   cudaGraph_t g = nullptr;
   const int bank0 = p->bank;
   OEM_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
   int rc = OEM_OK;
-  for (int q = 0; q < nsteps && rc == OEM_OK; ++q) rc = enqueue_step(p, p->cap_stream);
+  for (int q = 0; q < nsteps && rc == OEM_OK; ++q) {
+    const bool here = mode == 0 && (q == 0 || !p->ade_ahead);
+    const bool next = mode == 1 || (mode == 0 && p->ade_ahead && q + 1 < nsteps);
+    rc = enqueue_step(p, p->cap_stream, true, here, next);
+  }
   if (p->fused) set_bank(p, bank0);  // capturing ran nothing: the fields are still in bank0
   cudaError_t e = cudaStreamEndCapture(p->cap_stream, &g);
   if (rc) {
@@ -564,7 +590,7 @@ static int capture(oem_plan* p, int nsteps, cudaGraphExec_t* out) {
     return rc;
   }
   if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");
-  if (nsteps == 1) {
+  if (nsteps == 1 && mode == 0) {
     // the kernels one step launches: the kernel nodes of the one-step graph
     size_t nn = 0;
     e = cudaGraphGetNodes(g, nullptr, &nn);
@@ -644,6 +670,8 @@ int oem_plan_destroy(oem_plan* p) {
     if (p->graph_many[b]) cudaGraphExecDestroy(p->graph_many[b]);
     if (p->graph_one[b]) cudaGraphExecDestroy(p->graph_one[b]);
   }
+  if (p->graph_mid) cudaGraphExecDestroy(p->graph_mid);
+  if (p->graph_last) cudaGraphExecDestroy(p->graph_last);
   if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
   if (p->side_stream) cudaStreamDestroy(p->side_stream);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
@@ -1793,10 +1821,21 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   const double cells = (double)ncp;
   int G = (int)std::min(32.0, std::max(1.0, 4.0e6 / cells));
   p->graph_steps = G;
+  {
+    // the pole pass runs a step ahead only where nothing of the step before the E update
+    // (modulation, the mixed-form and tensor pre-passes) changes what it reads
+    const char* ade = getenv("OEM_B200_ADE");
+    p->ade_ahead = p->side_stream != nullptr && p->mods.empty() && p->mixes.empty() &&
+                   p->tensors.empty() && !(ade && strcmp(ade, "inline") == 0);
+  }
   for (int b = 0; b < (p->fused ? 2 : 1); ++b) {
     if (p->fused) set_bank(p, b);
     if ((rc = capture(p, 1, &p->graph_one[b]))) return rc;
     if (G > 1 && (rc = capture(p, G, &p->graph_many[b]))) return rc;
+  }
+  if (p->ade_ahead) {
+    if ((rc = capture(p, 1, &p->graph_mid, 1))) return rc;
+    if ((rc = capture(p, 1, &p->graph_last, 2))) return rc;
   }
   if (p->fused) set_bank(p, 0);
   // setup work runs on the legacy default stream; waiting for it alone leaves other plans'
@@ -1945,6 +1984,14 @@ int oem_plan_run(oem_plan* p, int64_t nsteps, void* stream) {
       if (p->fused && (p->graph_steps & 1)) set_bank(p, p->bank ^ 1);
       c -= p->graph_steps;
     }
+    if (p->ade_ahead && c >= 2) {
+      // this step's pole pass, then each step runs the next one's beside its monitors; the
+      // last step of the run runs none, so the pole states end at the run's last step
+      if ((rc = launch_ade(p, s))) return rc;
+      for (; c > 1; --c) OEM_CUDA(cudaGraphLaunch(p->graph_mid, s));
+      OEM_CUDA(cudaGraphLaunch(p->graph_last, s));
+      --c;
+    }
     while (c > 0) {
       OEM_CUDA(cudaGraphLaunch(p->graph_one[p->bank], s));
       if (p->fused) set_bank(p, p->bank ^ 1);
@@ -1982,6 +2029,14 @@ int oem_plan_box_snapshots_in_update(oem_plan* p, int* n) {
   if (rc) return rc;
   if (!n) return set_error(OEM_ERR_INVALID, "null output");
   *n = p->snapk.n;
+  return OEM_OK;
+}
+
+int oem_plan_pole_pass_ahead(oem_plan* p, int* on) {
+  int rc = check_plan(p, true);
+  if (rc) return rc;
+  if (!on) return set_error(OEM_ERR_INVALID, "null output");
+  *on = p->ade_ahead ? 1 : 0;
   return OEM_OK;
 }
 

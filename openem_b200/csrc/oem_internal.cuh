@@ -395,6 +395,11 @@ struct oem_plan {
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t graph_many[2] = {nullptr, nullptr};  // per starting field bank
   cudaGraphExec_t graph_one[2] = {nullptr, nullptr};
+  // pole pass one step ahead: a run of c >= 2 steps is one pole pass, c - 1 replays of
+  // graph_mid (whose last branch runs the next step's pole pass beside the snapshots) and one
+  // of graph_last (no pole pass), so no pole state is advanced past the run's last step
+  bool ade_ahead = false;
+  cudaGraphExec_t graph_mid = nullptr, graph_last = nullptr;
   int graph_steps = 1;
   int step_kernels = 0;  // kernel nodes of the one-step graph
 

@@ -63,6 +63,7 @@ SIGNATURES = {
     "oem_plan_status": (_I, [_P, _P]),
     "oem_plan_launches_per_step": (_I, [_P, C.POINTER(_I)]),
     "oem_plan_box_snapshots_in_update": (_I, [_P, C.POINTER(_I)]),
+    "oem_plan_pole_pass_ahead": (_I, [_P, C.POINTER(_I)]),
     "oem_plan_steps": (_I, [_P, C.POINTER(_L)]),
     "oem_plan_read_monitor": (_I, [_P, _I, _P, _P, _P]),
     "oem_plan_read_monitor_interleaved": (_I, [_P, _I, _P, _P]),

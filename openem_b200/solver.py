@@ -442,6 +442,13 @@ class Plan:
         L.check(self.lib.oem_plan_box_snapshots_in_update(self.h, C.byref(n)))
         return int(n.value)
 
+    def pole_pass_ahead(self) -> bool:
+        """Whether each step's pole pass runs at the end of the step before it (beside the DFT
+        snapshots), within one ``run`` call."""
+        n = C.c_int(0)
+        L.check(self.lib.oem_plan_pole_pass_ahead(self.h, C.byref(n)))
+        return bool(n.value)
+
     def launches_per_step(self) -> int:
         n = C.c_int()
         L.check(self.lib.oem_plan_launches_per_step(self.h, C.byref(n)))

@@ -114,20 +114,25 @@ class _PinnedStager:
 _SCAN = threading.local()
 
 
-def _differing(v: np.ndarray, v0, lo: int, hi: int, piece: int = 1 << 20) -> np.ndarray:
-    """Indices in [lo, hi) where v differs from v0, scanned a piece at a time through one
-    reused mask per thread (no fresh pages per piece); pieces with no differing cell, the bulk of
-    a background, cost one comparison and one any()."""
+def _differing(v: np.ndarray, v0, lo: int, hi: int, piece: int = 1 << 20):
+    """Indices in [lo, hi) where v differs from v0 (int32) and v's values there, scanned a piece
+    at a time through one reused mask per thread (no fresh pages per piece); pieces with no
+    differing cell, the bulk of a background, cost one comparison and one any(). The values are
+    gathered from the piece just compared, on the scanning thread."""
     b = getattr(_SCAN, "mask", None)
     if b is None:
         b = _SCAN.mask = np.empty(piece, dtype=bool)
-    out = []
+    idx, val = [], []
     for q in range(lo, hi, piece):
         m = min(piece, hi - q)
         np.not_equal(v[q:q + m], v0, out=b[:m])
         if b[:m].any():
-            out.append(np.flatnonzero(b[:m]) + q)
-    return np.concatenate(out) if out else np.zeros(0, dtype=np.int64)
+            k = np.flatnonzero(b[:m])
+            val.append(v[q:q + m][k])
+            idx.append((k + q).astype(np.int32))
+    if not idx:
+        return np.zeros(0, np.int32), np.zeros(0, v.dtype)
+    return np.concatenate(idx), np.concatenate(val)
 
 
 def _upload_material(a: np.ndarray, torch, dev):
@@ -136,32 +141,34 @@ def _upload_material(a: np.ndarray, torch, dev):
     A scene's eps and sigma are mostly one background value with objects in it: the most
     common value among 4096 cells spread over the array is taken as the background, and when at
     most an eighth of the cells differ from it (compared bit for bit, so NaN and signed zeros
-    count as different), only those cells' indices and values cross the link and the array is
-    filled on the device; otherwise the whole array is copied. The first 1/64 of the cells
-    decides which path is tried, and a scan that finds too many differing cells copies the
-    whole array after all."""
+    count as different), only those cells' indices (int32) and values cross the link and the
+    array is filled on the device; otherwise the whole array is copied. The same sample decides
+    which path is tried (more than a quarter of it off the background: the whole array), and a
+    scan that finds too many differing cells copies the whole array after all."""
     a = np.ascontiguousarray(a, np.float64).reshape(-1)
     n = a.size
-    if n < (1 << 22):
+    if n < (1 << 22) or n >= (1 << 31):
         return _PinnedStager.copy(a, torch, dev), a.nbytes
     v = a.view(np.uint64)
     # the background: the most common value among 4096 cells spread over the array
     u, cnt_u = np.unique(v[::max(1, n // 4096)], return_counts=True)
-    v0 = u[int(np.argmax(cnt_u))]
-    m = n // 64
-    if np.count_nonzero(v[:m] != v0) > m // 8:
+    top = int(np.argmax(cnt_u))
+    v0 = u[top]
+    if 4 * (int(cnt_u.sum()) - int(cnt_u[top])) > int(cnt_u.sum()):
         return _PinnedStager.copy(a, torch, dev), a.nbytes
-    parts = T.par_map(lambda lo, hi: _differing(v, v0, lo, hi), n, parts=16)
-    cnt = sum(int(p.size) for p in parts)
+    # four slices per pool thread: a slice that finds objects takes longer than a background one
+    parts = T.par_map(lambda lo, hi: _differing(v, v0, lo, hi), n, parts=64)
+    cnt = sum(int(p[0].size) for p in parts)
     if cnt > n // 8:
         return _PinnedStager.copy(a, torch, dev), a.nbytes
     # filled with the background's bits (a NaN keeps its payload, -0.0 its sign)
     out = torch.full((n,), int(np.array([v0], np.uint64).view(np.int64)[0]), dtype=torch.int64,
-                     device=dev).view(torch.float64)
+                     device=dev)
     if cnt:
-        idx = np.concatenate(parts)
-        out[torch.from_numpy(idx).to(dev)] = torch.from_numpy(a[idx]).to(dev)
-    return out, 16 * cnt
+        idx = np.concatenate([p[0] for p in parts])
+        val = np.concatenate([p[1] for p in parts]).view(np.int64)
+        out[torch.from_numpy(idx).to(dev).long()] = torch.from_numpy(val).to(dev)
+    return out.view(torch.float64), 12 * cnt
 
 
 class _Uploads:

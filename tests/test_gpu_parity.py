@@ -170,6 +170,47 @@ def test_box_snapshots_in_e_update_equal_snapshot_kernel(monkeypatch, n):
     assert float(np.abs(a.field_phasors["mid_z"]).max()) > 0.0
 
 
+@pytest.mark.parametrize("n", [42, 128])
+def test_pole_pass_ahead_equals_inline(monkeypatch, n):
+    """Each step's pole pass run at the end of the step before it, beside the DFT snapshots
+    (the default on the warp-specialised kernels), gives the same fields and phasors, bit for
+    bit, as the pole pass beside the H update of its own step (OEM_B200_ADE=inline), over runs
+    of 1, 2, 3 and 40 steps whose boundaries end and restart the early pole pass, and as one run
+    of all 46 steps. At 42 cells the plan also replays its 32-step graphs."""
+    monkeypatch.setenv("OEM_B200_KERNELS", "ws")
+    r = (0.05, 0.1) if n < 64 else (0.1, 0.3)
+    sc = scenes.dispersive_spheres(n=n, n_sph=4, num_steps=60, nfreq=3,
+                                   rmin=r[0] * scenes.UM, rmax=r[1] * scenes.UM)
+    chunks = [1, 2, 3, 40]
+
+    def go(ahead, parts):
+        if ahead:
+            monkeypatch.delenv("OEM_B200_ADE", raising=False)
+        else:
+            monkeypatch.setenv("OEM_B200_ADE", "inline")
+        plan = solver.Plan(sc, sum(parts))
+        try:
+            assert plan.pole_pass_ahead() == ahead
+            for c in parts:
+                plan.run(c)
+            plan.flush()
+            fields = [plan.read_field(c) for c in range(6)]
+            ph = plan.field_phasors()
+        finally:
+            plan.close()
+        return fields, ph
+
+    f0, p0 = go(False, chunks)
+    for parts in (chunks, [sum(chunks)]):
+        f1, p1 = go(True, parts)
+        for c in range(6):
+            np.testing.assert_array_equal(f1[c], f0[c])
+        assert set(p1) == set(p0) == {"mid_x", "mid_y", "mid_z"}
+        for name in p0:
+            np.testing.assert_array_equal(p1[name], p0[name])
+    assert float(np.abs(f0[2]).max()) > 0.0
+
+
 @pytest.mark.parametrize("kind", ["stream", "tma", "ws"])
 def test_pipelined_kernels_periodic_slab(monkeypatch, kind):
     """Periodic x/y walls of a one-cell-wide column (every neighbour wraps) and a plane-wave

@@ -435,9 +435,9 @@ def test_device_entry_checks_match_host_checks():
 
 
 def test_sparse_material_upload_is_exact():
-    """A per-cell float64 array that is mostly one value crosses as (index, value) pairs and is
-    filled on the device (torch CPU tensors here), bit for bit, NaN and -0.0 included; a varied
-    array is copied whole. The byte counts are what was sent."""
+    """A per-cell float64 array that is mostly one value crosses as (int32 index, value) pairs
+    and is filled on the device (torch CPU tensors here), bit for bit, NaN and -0.0 included; a
+    varied array is copied whole. The byte counts are what was sent."""
     import torch
     from openem_b200 import tables_gpu as TG
     rng = np.random.default_rng(3)
@@ -448,23 +448,27 @@ def test_sparse_material_upload_is_exact():
     a[12] = np.nan
     t, nb = TG._upload_material(a, torch, torch.device("cpu"))
     assert np.array_equal(t.numpy().view(np.uint64), a.view(np.uint64))
-    assert nb == 16 * int(np.count_nonzero(a.view(np.uint64) != a.view(np.uint64)[0]))
+    assert nb == 12 * int(np.count_nonzero(a.view(np.uint64) != a.view(np.uint64)[0]))
     b = rng.random(n)
     t, nb = TG._upload_material(b, torch, torch.device("cpu"))
     assert np.array_equal(t.numpy(), b) and nb == b.nbytes
     c = np.ones(n)
-    c[n // 2:] = 2.0  # the first 1/64 looks uniform, the full scan finds half the cells differ
+    c[n // 2:] = 2.0  # half the sample is off the background: copied whole without a scan
     t, nb = TG._upload_material(c, torch, torch.device("cpu"))
+    assert np.array_equal(t.numpy(), c) and nb == c.nbytes
+    c = np.ones(n)
+    c[rng.random(n) < 0.2] = 2.0  # a fifth of the sample off (under a quarter): the scan
+    t, nb = TG._upload_material(c, torch, torch.device("cpu"))  # finds > 1/8 and copies whole
     assert np.array_equal(t.numpy(), c) and nb == c.nbytes
     nanp = np.array([0x7FF8000000000123], np.uint64).view(np.float64)[0]  # a NaN with payload
     dd = np.full(n, nanp)
     dd[5] = -0.0
     t, nb = TG._upload_material(dd, torch, torch.device("cpu"))
-    assert np.array_equal(t.numpy().view(np.uint64), dd.view(np.uint64)) and nb == 16
+    assert np.array_equal(t.numpy().view(np.uint64), dd.view(np.uint64)) and nb == 12
     d = np.full(n, 2.25)
     d[:1000] = 1.0  # the first cell lies in an object: the background is the common value
     t, nb = TG._upload_material(d, torch, torch.device("cpu"))
-    assert np.array_equal(t.numpy(), d) and nb == 16 * 1000
+    assert np.array_equal(t.numpy(), d) and nb == 12 * 1000
 
 
 def test_hashed_material_codes_equal_exact_ranking():
