@@ -235,33 +235,76 @@ def cpu_oracle_rate(n: int, steps: int) -> tuple[float, float]:
     return n ** 3 * steps / dt / 1e9, dt
 
 
+def _ref_replica(n: int, warmup: int, steps: int, barrier, out) -> None:
+    """One process of the reference arm: the oracle's step on its own copy of the proxy scene,
+    timed after every replica has finished its warm-up."""
+    from openem_b200 import scenes
+    from oracle import ref64
+    sc = scenes.small_dispersive(n=n, n_pml=12, n_sph=n_spheres(n), num_steps=warmup + steps + 1)
+    o = ref64.Oracle(sc, warmup + steps + 1)
+    for _ in range(warmup):
+        o.step()
+    barrier.wait(timeout=600)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step()
+    out.put(time.perf_counter() - t0)
+
+
+def reference_procs(requested: int) -> int:
+    """Processes for the reference arm: every host core this process may run on, fewer when
+    the available memory would not hold a replica (about 1 GB at 128^3) on each."""
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    r = requested if requested > 0 else int(cores or 1)
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+        r = min(r, max(1, int(avail // (2 << 30))))
+    except (ValueError, OSError):
+        pass
+    return max(1, r)
+
+
 def run_reference(args):
+    """The reference's CPU implementation of the step on all the host's cores: one process per
+    core (spawned, single-threaded numpy), each stepping its own copy of the proxy scene; the
+    K steps of all replicas timed together (max over replicas), throughput summed."""
     world, rank, _ = dist_setup(args.gpus)
     if rank != 0:
         dist_done(world)
         return
+    import multiprocessing as mp
     n = args.ref_size
-    from openem_b200 import scenes
-    from oracle import ref64
-    sc = scenes.small_dispersive(n=n, n_pml=12, n_sph=n_spheres(n),
-                                 num_steps=args.warmup + args.steps + 1)
-    o = ref64.Oracle(sc, args.warmup + args.steps + 1)
-    for _ in range(args.warmup):
-        o.step()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        o.step()
-    dt = time.perf_counter() - t0
-    value = n ** 3 * args.steps / dt / 1e9
-    sample = (f"FP64 NumPy transcription of OpenEM's step (oracle/ref64.py), {n}^3 proxy of the "
-              f"workload's construction, {args.steps} steps, 1 thread of {os.cpu_count()}")
+    R = reference_procs(args.ref_procs)
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[k] = "1"  # inherited by the spawned replicas: one thread each
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(R)
+    out = ctx.Queue()
+    procs = [ctx.Process(target=_ref_replica, args=(n, args.warmup, args.steps, barrier, out))
+             for _ in range(R)]
+    for p in procs:
+        p.start()
+    try:
+        dts = [out.get(timeout=1800) for _ in range(R)]
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    dt = max(dts)
+    value = R * n ** 3 * args.steps / dt / 1e9
+    sample = (f"FP64 NumPy transcription of OpenEM's step (oracle/ref64.py), {R} single-threaded "
+              f"processes of {os.cpu_count()} cores, each a {n}^3 proxy of the workload's "
+              f"construction, {args.steps} steps after {args.warmup} warm-up steps "
+              f"(max over replicas {dt:.1f} s)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene factory)",
-            "config": {"workload": workload_name(args.size) + f"; measured on a {n}^3 proxy",
-                       "parallelism": "replicas"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+            "config": {"workload": workload_name(args.size) + f"; measured on {R} replicas of a "
+                                                              f"{n}^3 proxy",
+                       "parallelism": f"replicas x{R} (host processes)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": R, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -605,6 +648,8 @@ def main():
     ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--ref-size", type=int, default=128)
+    ap.add_argument("--ref-procs", type=int, default=0,
+                    help="processes of the reference arm (0: one per host core)")
     ap.add_argument("--cpu-size", type=int, default=128)
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-e2e", action="store_true")
