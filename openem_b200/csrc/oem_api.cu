@@ -43,6 +43,30 @@ static ReadStage* read_stage(int device) {
   return r;
 }
 
+// Grow the stage to halves of at least cbytes; false when no pinned memory could be had (the
+// stage is then empty). The caller holds rs->mu and has made the device current.
+static bool grow_stage(ReadStage* rs, size_t cbytes) {
+  if (rs->bytes >= cbytes) return true;
+  for (int b = 0; b < 2; ++b) {
+    if (rs->half[b]) cudaFreeHost(rs->half[b]);
+    rs->half[b] = nullptr;
+    if (!rs->ev[b]) cudaEventCreateWithFlags(&rs->ev[b], cudaEventDisableTiming);
+  }
+  rs->bytes = 0;
+  if (cudaHostAlloc((void**)&rs->half[0], cbytes, cudaHostAllocDefault) == cudaSuccess &&
+      cudaHostAlloc((void**)&rs->half[1], cbytes, cudaHostAllocDefault) == cudaSuccess &&
+      rs->ev[0] && rs->ev[1]) {
+    rs->bytes = cbytes;
+    return true;
+  }
+  cudaGetLastError();
+  for (int b = 0; b < 2; ++b) {
+    if (rs->half[b]) cudaFreeHost(rs->half[b]);
+    rs->half[b] = nullptr;
+  }
+  return false;
+}
+
 // Ask for transparent huge pages on the page-aligned interior of a large output range before
 // its first touch: a fresh 1.2 GB readout array otherwise takes 300k page faults. A hint only
 // (no effect where huge pages are disabled).
@@ -52,10 +76,11 @@ static void advise_huge_pages(void* p, size_t n) {
   if (b > a + ((uintptr_t)4 << 20)) madvise((void*)a, b - a, MADV_HUGEPAGE);
 }
 
-// Copy n bytes with up to 8 host threads (pieces of at least 4 MB).
+// Copy n bytes with up to 16 host threads (pieces of at least 4 MB).
 static void par_memcpy(char* dst, const char* src, size_t n) {
   const size_t kMin = (size_t)4 << 20;
-  const int nt = (int)std::min<size_t>(8, std::max<size_t>(1, n / kMin));
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const int nt = (int)std::min<size_t>(std::min<size_t>(16, hw), std::max<size_t>(1, n / kMin));
   if (nt == 1) {
     memcpy(dst, src, n);
     return;
@@ -665,6 +690,7 @@ int oem_plan_create(int device, int nx, int ny, int nz, double ch, double cw, oe
 
 int oem_plan_destroy(oem_plan* p) {
   if (!p) return OEM_OK;
+  if (p->stage_thread.joinable()) p->stage_thread.join();
   cudaSetDevice(p->device);
   for (int b = 0; b < 2; ++b) {
     if (p->graph_many[b]) cudaGraphExecDestroy(p->graph_many[b]);
@@ -1842,6 +1868,23 @@ int oem_plan_finalize(oem_plan* p, int64_t n_total) {
   // (non-blocking) streams running, which a server with several plans in flight relies on
   OEM_CUDA(cudaStreamSynchronize(0));
   p->finalized = true;
+  {
+    // the pinned readout stage of a plan whose largest phasor readout takes 16 MB or more is
+    // grown on a host thread now (page locking of up to 128 MB takes tens of milliseconds,
+    // hidden behind the steps); the first readout joins it
+    int64_t most = 0;
+    for (const Monitor& q : p->mons) most = std::max(most, (int64_t)q.ncomp * q.nf * q.cells);
+    const size_t cbytes = (size_t)std::min(most, (int64_t)1 << 22) * sizeof(double2);
+    if ((size_t)most * sizeof(double2) >= ((size_t)16 << 20)) {
+      ReadStage* rs = read_stage(p->device);
+      const int dev = p->device;
+      p->stage_thread = std::thread([rs, dev, cbytes] {
+        std::lock_guard<std::mutex> g(rs->mu);
+        if (rs->bytes >= cbytes || cudaSetDevice(dev) != cudaSuccess) return;
+        grow_stage(rs, cbytes);
+      });
+    }
+  }
   return OEM_OK;
 }
 
@@ -2096,27 +2139,9 @@ int oem_plan_read_monitor_interleaved(oem_plan* p, int id, double* out, void* st
                                                                       : nullptr;
   std::unique_lock<std::mutex> lk;
   if (rs) {
+    if (p->stage_thread.joinable()) p->stage_thread.join();  // started at finalize
     lk = std::unique_lock<std::mutex>(rs->mu);
-    if (rs->bytes < cbytes) {
-      for (int b = 0; b < 2; ++b) {
-        if (rs->half[b]) cudaFreeHost(rs->half[b]);
-        rs->half[b] = nullptr;
-        if (!rs->ev[b]) cudaEventCreateWithFlags(&rs->ev[b], cudaEventDisableTiming);
-      }
-      rs->bytes = 0;
-      if (cudaHostAlloc((void**)&rs->half[0], cbytes, cudaHostAllocDefault) == cudaSuccess &&
-          cudaHostAlloc((void**)&rs->half[1], cbytes, cudaHostAllocDefault) == cudaSuccess &&
-          rs->ev[0] && rs->ev[1]) {
-        rs->bytes = cbytes;
-      } else {
-        cudaGetLastError();
-        for (int b = 0; b < 2; ++b) {
-          if (rs->half[b]) cudaFreeHost(rs->half[b]);
-          rs->half[b] = nullptr;
-        }
-      }
-    }
-    if (rs->bytes < cbytes) {  // no pinned memory: the driver's pageable copies
+    if (!grow_stage(rs, cbytes)) {  // no pinned memory: the driver's pageable copies
       lk.unlock();
       rs = nullptr;
     }

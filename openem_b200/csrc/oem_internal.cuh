@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/oem_b200.h"
@@ -383,6 +384,7 @@ struct oem_plan {
   unsigned long long* d_rd_bad = nullptr;        // non-finite values seen by one readout
   int64_t rd_nonfinite = 0;                      // since the last oem_plan_readout_nonfinite
   int64_t rd_chunk = 0;
+  std::thread stage_thread;  // grows the pinned readout stage after finalize (joined on use)
 
   // device state
   std::vector<void*> allocs;
