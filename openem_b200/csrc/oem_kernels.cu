@@ -314,16 +314,23 @@ __global__ void k_snap_plane(YeeParams P, Monitor m, const int* step) {
   const int64_t idm = ((int64_t)c[0] * P.ny + c[1]) * P.nzp + c[2];
   const int64_t off = (int64_t)p1 * m.n2 + p2;
   float* row = m.d_snap + (int64_t)((*step) % m.T) * (m.cplx ? 8 : 4) * m.cells;
-  row[off] = P.f[t1][id];
-  row[m.cells + off] = P.f[t2][id];
-  row[2 * m.cells + off] = 0.5f * (P.f[3 + t1][id] + P.f[3 + t1][idm]);
-  row[3 * m.cells + off] = 0.5f * (P.f[3 + t2][id] + P.f[3 + t2][idm]);
+  // loads first (see k_snap_boxes)
+  const float e1 = P.f[t1][id], e2 = P.f[t2][id];
+  const float h1 = P.f[3 + t1][id], h1m = P.f[3 + t1][idm];
+  const float h2 = P.f[3 + t2][id], h2m = P.f[3 + t2][idm];
   if (m.cplx) {
-    row[4 * m.cells + off] = P.fi[t1][id];
-    row[5 * m.cells + off] = P.fi[t2][id];
-    row[6 * m.cells + off] = 0.5f * (P.fi[3 + t1][id] + P.fi[3 + t1][idm]);
-    row[7 * m.cells + off] = 0.5f * (P.fi[3 + t2][id] + P.fi[3 + t2][idm]);
+    const float e1i = P.fi[t1][id], e2i = P.fi[t2][id];
+    const float h1i = P.fi[3 + t1][id], h1mi = P.fi[3 + t1][idm];
+    const float h2i = P.fi[3 + t2][id], h2mi = P.fi[3 + t2][idm];
+    row[4 * m.cells + off] = e1i;
+    row[5 * m.cells + off] = e2i;
+    row[6 * m.cells + off] = 0.5f * (h1i + h1mi);
+    row[7 * m.cells + off] = 0.5f * (h2i + h2mi);
   }
+  row[off] = e1;
+  row[m.cells + off] = e2;
+  row[2 * m.cells + off] = 0.5f * (h1 + h1m);
+  row[3 * m.cells + off] = 0.5f * (h2 + h2m);
 }
 
 // DFT snapshot of box monitors (openem/kernels/source_dft.cu:453-478): the six components at
@@ -346,12 +353,20 @@ __global__ void __launch_bounds__(256) k_snap_boxes(YeeParams P,
   float* row = m.d_snap + (int64_t)((*step) % m.T) * (m.cplx ? 12 : 6) * m.cells;
   const int64_t id = ((int64_t)(m.i0 + (int)a) * P.ny + (m.j0 + (int)b)) * P.nzp + (m.k0 + (int)cc);
   const int64_t o = (int64_t)a * njk + t;
+  // every load before the first store: the compiler cannot move a load above a store to a
+  // pointer that may alias it, and a thin box's reads are latency-bound
+  float v[6];
 #pragma unroll
-  for (int c = 0; c < 6; ++c) row[c * m.cells + o] = P.f[c][id];
+  for (int c = 0; c < 6; ++c) v[c] = P.f[c][id];
   if (m.cplx) {
+    float vi[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) row[(6 + c) * m.cells + o] = P.fi[c][id];
+    for (int c = 0; c < 6; ++c) vi[c] = P.fi[c][id];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) row[(6 + c) * m.cells + o] = vi[c];
   }
+#pragma unroll
+  for (int c = 0; c < 6; ++c) row[c * m.cells + o] = v[c];
 }
 
 // Batched DFT flush (openem/kernels/source_dft.cu:440-530 real fields,
