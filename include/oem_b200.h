@@ -285,7 +285,10 @@ int oem_plan_add_time_monitor(oem_plan* p, int nc, const int32_t* comps, int i0,
                               int* id);
 
 /* Allocate the fields and auxiliary state, upload everything, capture the step graph.
- * n_total is the nominal number of steps (bounds the source and phase tables). */
+ * n_total is the nominal number of steps (bounds the source and phase tables). When the plan's
+ * largest phasor readout takes 16 MB or more, a host thread started here grows the process's
+ * pinned readout stage for this device (page locking of up to 128 MB); the first readout of
+ * the plan, or oem_plan_destroy, joins it. */
 int oem_plan_finalize(oem_plan* p, int64_t n_total);
 
 /* Advance nsteps full time steps on `stream` (asynchronous). One step is
