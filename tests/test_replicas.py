@@ -40,3 +40,21 @@ def test_two_replicas_report_the_slowest_rank():
     out = mgr.dict()
     mp.start_processes(_rank, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
     assert dict(out) == {0: 17.25, 1: 17.25}
+
+
+def test_reference_arm_runs_one_oracle_process_per_core():
+    """``bench.py --impl reference``: the oracle's step in spawned single-threaded processes,
+    one per requested core, timed together; the line reports their number and sums their
+    throughput (CPU only, a 24^3 proxy here)."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference",
+                        "--steps", "3", "--warmup", "3", "--ref-size", "24", "--ref-procs", "2"],
+                       capture_output=True, text=True, timeout=300, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["cpu_baseline"]["cores"] == 2
+    assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
+    assert "replicas x2" in line["config"]["parallelism"]
