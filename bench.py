@@ -256,11 +256,16 @@ def reference_procs(requested: int) -> int:
     the available memory would not hold a replica (about 1 GB at 128^3) on each."""
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     r = requested if requested > 0 else int(cores or 1)
-    try:
-        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
-        r = min(r, max(1, int(avail // (2 << 30))))
-    except (ValueError, OSError):
+    avail = None
+    try:  # MemAvailable counts the reclaimable page cache, unlike the free pages
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable:"):
+                    avail = int(ln.split()[1]) * 1024
+    except OSError:
         pass
+    if avail:
+        r = min(r, max(1, int(avail // (2 << 30))))
     return max(1, r)
 
 
