@@ -116,8 +116,8 @@ __device__ __forceinline__ void ade_segment(const YeeParams& P, const SegLoad& L
 // Warps stride over the listed segments (the grid is about one resident wave): while a warp
 // updates segment q it has already loaded the pole range, materials and E^n of its next
 // segment and the index of the one after, so each segment waits on one dependent load (its
-// pole states) instead of three. In the captured step it runs on its own graph branch beside
-// the H update.
+// pole states) instead of three. In the captured step it runs on a graph branch of its own:
+// beside the snapshots of the step before (within one run call), or beside the H update.
 constexpr int kAdeMats = 64;    // material records staged in shared memory when they fit
 constexpr int kAdeCoefs = 256;  // pole coefficient rows staged likewise
 constexpr int kAdeSets = 64;

@@ -432,8 +432,8 @@ static int enqueue_step(oem_plan* p, cudaStream_t s, bool monitors = true, bool 
     set_bank(p, nb);
     return enqueue_e_side(p, s, monitors);
   }
-  // the pole pass depends on E^n only: it runs on a branch beside the H update and joins
-  // before the E update
+  // the pole pass depends on E^n only: when the step runs its own (ade_here) it goes on a
+  // branch beside the H update and joins before the E update
   const bool fork = p->side_stream != nullptr;
   for (const MixSet& x : p->mixes)
     if ((e = launch_mix_pre(P, x, s)) != cudaSuccess) return cuda_error(e, "mix_pre");
