@@ -282,11 +282,14 @@ def run_reference(args):
     R = reference_procs(args.ref_procs)
     for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
         os.environ[k] = "1"  # inherited by the spawned replicas: one thread each
+    # each K-step run stays within a few minutes: at most 60 timed steps per replica (about
+    # 0.8 s each at 128^3 with every core busy); the line reports the steps it timed
+    K = min(args.steps, 60)
+    W = min(args.warmup, 5)
     ctx = mp.get_context("spawn")
     barrier = ctx.Barrier(R)
     out = ctx.Queue()
-    procs = [ctx.Process(target=_ref_replica, args=(n, args.warmup, args.steps, barrier, out))
-             for _ in range(R)]
+    procs = [ctx.Process(target=_ref_replica, args=(n, W, K, barrier, out)) for _ in range(R)]
     for p in procs:
         p.start()
     try:
@@ -297,14 +300,14 @@ def run_reference(args):
             if p.is_alive():
                 p.kill()
     dt = max(dts)
-    value = R * n ** 3 * args.steps / dt / 1e9
+    value = R * n ** 3 * K / dt / 1e9
     sample = (f"FP64 NumPy transcription of OpenEM's step (oracle/ref64.py), {R} single-threaded "
               f"processes of {os.cpu_count()} cores, each a {n}^3 proxy of the workload's "
-              f"construction, {args.steps} steps after {args.warmup} warm-up steps "
+              f"construction, {K} timed steps after {W} warm-up steps "
               f"(max over replicas {dt:.1f} s)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "n_gpus": args.gpus, "steps": K, "warmup": W,
+            "ms_per_step": dt / K * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene factory)",
             "config": {"workload": workload_name(args.size) + f"; measured on {R} replicas of a "
                                                               f"{n}^3 proxy",
